@@ -1,0 +1,698 @@
+// api.cpp -- host side of the C ABI declared in include/curast_b200.h.
+//
+// Built with -ffp-contract=off: the per-instance world_view = view * world and
+// the mirrored-instance determinant are formed here in glm's float order
+// (libs/glm/glm/detail/type_mat4x4.inl:601-618, func_geometric.inl:53-85),
+// exactly as the reference's render host does (src/CuRast_render.h:406-410)
+// and its stage-1 kernel does (src/kernels/triangles_visbuffer.cu:179-185).
+#include "curast_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "cr_device.h"
+
+namespace {
+
+thread_local std::string g_error;
+
+cr_status fail(cr_status s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_error = buf;
+    return s;
+}
+
+cr_status cuda_fail(cudaError_t e, const char* what) {
+    return fail(e == cudaErrorMemoryAllocation ? CR_ERR_OOM : CR_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CR_CUDA(call, what)                      \
+    do {                                         \
+        cudaError_t _e = (call);                 \
+        if (_e != cudaSuccess) return cuda_fail(_e, what); \
+    } while (0)
+
+struct MeshRec {
+    bool live = false;
+    bool owned = false;
+    float* positions = nullptr;
+    uint32_t* indices = nullptr;
+    uint32_t* colors = nullptr;
+    uint32_t numVertices = 0;
+    uint32_t numTriangles = 0;
+    size_t bytes = 0;
+};
+
+// glm mat4 * mat4: column j = ((A0*B[j][0] + A1*B[j][1]) + A2*B[j][2]) + A3*B[j][3]
+void mat4_mul(const float* a, const float* b, float* out) {
+    float r[16];
+    for (int j = 0; j < 4; j++)
+        for (int i = 0; i < 4; i++) {
+            float s = a[0 * 4 + i] * b[j * 4 + 0];
+            s = s + a[1 * 4 + i] * b[j * 4 + 1];
+            s = s + a[2 * 4 + i] * b[j * 4 + 2];
+            s = s + a[3 * 4 + i] * b[j * 4 + 3];
+            r[j * 4 + i] = s;
+        }
+    memcpy(out, r, sizeof(r));
+}
+
+// dot(cross(c0, c1), c2) over the first three columns (tv.cu:179-182)
+float det3_glm(const float* m) {
+    const float c0[3] = {m[0], m[1], m[2]}, c1[3] = {m[4], m[5], m[6]}, c2[3] = {m[8], m[9], m[10]};
+    const float x = c0[1] * c1[2] - c1[1] * c0[2];
+    const float y = c0[2] * c1[0] - c1[2] * c0[0];
+    const float z = c0[0] * c1[1] - c1[0] * c0[1];
+    return (x * c2[0] + y * c2[1]) + z * c2[2];
+}
+
+// glm::inverse for mat4 (libs/glm/glm/detail/func_matrix.inl:296-360)
+void mat4_inverse(const float* m, float* out) {
+#define M(c, r) m[(c) * 4 + (r)]
+    const float C00 = M(2, 2) * M(3, 3) - M(3, 2) * M(2, 3), C02 = M(1, 2) * M(3, 3) - M(3, 2) * M(1, 3),
+                C03 = M(1, 2) * M(2, 3) - M(2, 2) * M(1, 3), C04 = M(2, 1) * M(3, 3) - M(3, 1) * M(2, 3),
+                C06 = M(1, 1) * M(3, 3) - M(3, 1) * M(1, 3), C07 = M(1, 1) * M(2, 3) - M(2, 1) * M(1, 3),
+                C08 = M(2, 1) * M(3, 2) - M(3, 1) * M(2, 2), C10 = M(1, 1) * M(3, 2) - M(3, 1) * M(1, 2),
+                C11 = M(1, 1) * M(2, 2) - M(2, 1) * M(1, 2), C12 = M(2, 0) * M(3, 3) - M(3, 0) * M(2, 3),
+                C14 = M(1, 0) * M(3, 3) - M(3, 0) * M(1, 3), C15 = M(1, 0) * M(2, 3) - M(2, 0) * M(1, 3),
+                C16 = M(2, 0) * M(3, 2) - M(3, 0) * M(2, 2), C18 = M(1, 0) * M(3, 2) - M(3, 0) * M(1, 2),
+                C19 = M(1, 0) * M(2, 2) - M(2, 0) * M(1, 2), C20 = M(2, 0) * M(3, 1) - M(3, 0) * M(2, 1),
+                C22 = M(1, 0) * M(3, 1) - M(3, 0) * M(1, 1), C23 = M(1, 0) * M(2, 1) - M(2, 0) * M(1, 1);
+    const float F0[4] = {C00, C00, C02, C03}, F1[4] = {C04, C04, C06, C07}, F2[4] = {C08, C08, C10, C11},
+                F3[4] = {C12, C12, C14, C15}, F4[4] = {C16, C16, C18, C19}, F5[4] = {C20, C20, C22, C23};
+    const float V0[4] = {M(1, 0), M(0, 0), M(0, 0), M(0, 0)}, V1[4] = {M(1, 1), M(0, 1), M(0, 1), M(0, 1)},
+                V2[4] = {M(1, 2), M(0, 2), M(0, 2), M(0, 2)}, V3[4] = {M(1, 3), M(0, 3), M(0, 3), M(0, 3)};
+    const float SA[4] = {+1, -1, +1, -1}, SB[4] = {-1, +1, -1, +1};
+    float inv[16];
+    for (int k = 0; k < 4; k++) {
+        inv[0 * 4 + k] = (V1[k] * F0[k] - V2[k] * F1[k] + V3[k] * F2[k]) * SA[k];
+        inv[1 * 4 + k] = (V0[k] * F0[k] - V2[k] * F3[k] + V3[k] * F4[k]) * SB[k];
+        inv[2 * 4 + k] = (V0[k] * F1[k] - V1[k] * F3[k] + V3[k] * F5[k]) * SA[k];
+        inv[3 * 4 + k] = (V0[k] * F2[k] - V1[k] * F4[k] + V2[k] * F5[k]) * SB[k];
+    }
+    const float d0 = M(0, 0) * inv[0], d1 = M(0, 1) * inv[4], d2 = M(0, 2) * inv[8], d3 = M(0, 3) * inv[12];
+    const float one_over_det = 1.0f / ((d0 + d1) + (d2 + d3));
+    for (int k = 0; k < 16; k++) out[k] = inv[k] * one_over_det;
+#undef M
+}
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+struct Assembled {
+    std::vector<uint32_t> order;
+    std::vector<CrInstance> inst;
+    std::vector<float> worldView;   // 16 per instance
+    std::vector<float> world;       // 16 per instance
+    std::vector<CrSegment> seg;
+    uint64_t totalTriangles = 0;
+    uint64_t numItems = 0;
+};
+
+}  // namespace
+
+struct cr_context {
+    cr_config cfg{};
+    int device = 0;
+    CrLaunchShape shape{};
+    std::vector<MeshRec> meshes;
+    size_t bytesInUse = 0;
+
+    // frame table: device copy + pinned staging
+    void* dFrame = nullptr;
+    size_t dFrameCap = 0;
+    void* hFrame = nullptr;
+    size_t hFrameCap = 0;
+    cudaEvent_t frameCopied = nullptr;
+    cudaEvent_t frameDone = nullptr;  // last kernel of the previous frame
+
+    // queues
+    uint64_t* ntList = nullptr;
+    uint64_t ntCap = 0;
+    CrTile* hugeList = nullptr;
+    uint64_t hugeCap = 0;
+    unsigned long long* counters = nullptr;
+    unsigned long long* hCounters = nullptr;  // pinned
+
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    // CR_RENDER_TIMING: a ring of event sets (6 per frame) drained on demand
+    static constexpr int kRing = 128;
+    std::vector<cudaEvent_t> ring;
+    int ringHead = 0, ringCount = 0;
+    cr_frame_stats last{};
+    bool pendingStats = false;
+    cudaStream_t lastStream = nullptr;
+
+    cr_status dev_alloc(void** p, size_t bytes, const char* what) {
+        if (cfg.memory_budget && bytesInUse + bytes > cfg.memory_budget)
+            return fail(CR_ERR_OOM, "%s: %zu bytes would exceed the memory budget (%zu in use of %llu)", what, bytes,
+                        bytesInUse, (unsigned long long)cfg.memory_budget);
+        cudaError_t e = cudaMalloc(p, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return cuda_fail(e, what);
+        }
+        bytesInUse += bytes;
+        return CR_OK;
+    }
+    void dev_free(void* p, size_t bytes) {
+        if (!p) return;
+        cudaFree(p);
+        bytesInUse -= std::min(bytesInUse, bytes);
+    }
+};
+
+namespace {
+
+// CuRast_render.h:338-345: triangle count descending, then mesh; ties keep
+// submission order (the reference's std::sort leaves them unspecified).
+template <typename MeshOf, typename TrisOf>
+void order_instances(uint32_t count, uint32_t flags, MeshOf meshOf, TrisOf trisOf, std::vector<uint32_t>& order) {
+    order.resize(count);
+    std::iota(order.begin(), order.end(), 0u);
+    if (flags & CR_RENDER_KEEP_ORDER) return;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+        const uint32_t ta = trisOf(a), tb = trisOf(b);
+        if (ta != tb) return ta > tb;
+        return meshOf(a) < meshOf(b);
+    });
+}
+
+cr_status assemble(cr_context* ctx, const cr_instance* instances, uint32_t count, const float* view, uint32_t flags,
+                   Assembled& A) {
+    for (uint32_t i = 0; i < count; i++) {
+        const uint32_t m = instances[i].mesh;
+        if (m >= ctx->meshes.size() || !ctx->meshes[m].live) return fail(CR_ERR_NOT_FOUND, "instance %u: unknown mesh %u", i, m);
+    }
+    order_instances(
+        count, flags, [&](uint32_t i) { return instances[i].mesh; },
+        [&](uint32_t i) { return ctx->meshes[instances[i].mesh].numTriangles; }, A.order);
+    A.inst.assign(count, CrInstance{});
+    A.worldView.resize(16ull * count);
+    A.world.resize(16ull * count);
+    A.seg.clear();
+    uint64_t sum = 0;
+    uint64_t items = 0;
+    for (uint32_t r = 0; r < count; r++) {
+        const cr_instance& in = instances[A.order[r]];
+        const MeshRec& m = ctx->meshes[in.mesh];
+        CrInstance& ci = A.inst[r];
+        ci.indices = m.indices;
+        ci.positions = m.positions;
+        ci.colors = m.colors;
+        ci.cum = sum;
+        ci.numTriangles = m.numTriangles;
+        ci.numVertices = m.numVertices;
+        float* wv = &A.worldView[16ull * r];
+        mat4_mul(view, in.world, wv);  // CuRast_render.h:409
+        ci.flip = det3_glm(wv) < 0.0f ? 1u : 0u;
+        memcpy(&A.world[16ull * r], in.world, 64);
+        // CuRast_render.h:425-433: consecutive instances of one mesh form a segment
+        if (A.seg.empty() || A.seg.back().positions != m.positions || A.seg.back().indices != m.indices ||
+            A.seg.back().numTriangles != m.numTriangles) {
+            CrSegment s{};
+            s.indices = m.indices;
+            s.positions = m.positions;
+            s.numTriangles = m.numTriangles;
+            s.firstInstance = r;
+            s.instanceCount = 0;
+            s.flags = (m.indices && ((uintptr_t)m.indices & 15u) == 0) ? 1u : 0u;
+            A.seg.push_back(s);
+        }
+        A.seg.back().instanceCount++;
+        sum += m.numTriangles;
+    }
+    if (sum >= (1ull << 36)) return fail(CR_ERR_INVALID, "scene has %llu triangles; ids hold 36 bits", (unsigned long long)sum);
+    for (CrSegment& s : A.seg) {
+        s.numBatches = (s.numTriangles + CR_BATCH - 1) / CR_BATCH;
+        s.numChunks = (s.instanceCount + CR_INST_CHUNK - 1) / CR_INST_CHUNK;
+        s.itemBase = items;
+        items += (uint64_t)s.numBatches * s.numChunks;
+    }
+    A.totalTriangles = sum;
+    A.numItems = items;
+    return CR_OK;
+}
+
+cr_status ensure_queues(cr_context* ctx, uint64_t ntWant, uint64_t hugeWant) {
+    if (ntWant > ctx->ntCap) {
+        ctx->dev_free(ctx->ntList, ctx->ntCap * 8);
+        ctx->ntList = nullptr;
+        ctx->ntCap = 0;
+        cr_status s = ctx->dev_alloc((void**)&ctx->ntList, ntWant * 8, "stage-2 queue");
+        if (s) return s;
+        ctx->ntCap = ntWant;
+    }
+    if (hugeWant > ctx->hugeCap) {
+        ctx->dev_free(ctx->hugeList, ctx->hugeCap * sizeof(CrTile));
+        ctx->hugeList = nullptr;
+        ctx->hugeCap = 0;
+        cr_status s = ctx->dev_alloc((void**)&ctx->hugeList, hugeWant * sizeof(CrTile), "stage-3 queue");
+        if (s) return s;
+        ctx->hugeCap = hugeWant;
+    }
+    return CR_OK;
+}
+
+// Packs the assembled frame into pinned memory and copies it to the device.
+cr_status upload_frame(cr_context* ctx, const Assembled& A, cudaStream_t stream, CrFrameParams& fp,
+                       CrResolveParams& rp) {
+    const size_t n = A.inst.size(), m = A.seg.size();
+    const size_t oInst = 0;
+    const size_t oWV = align_up(oInst + n * sizeof(CrInstance), 256);
+    const size_t oW = align_up(oWV + n * 64, 256);
+    const size_t oSeg = align_up(oW + n * 64, 256);
+    const size_t total = align_up(oSeg + m * sizeof(CrSegment), 256);
+    // the previous frame's copy must have left the staging buffer
+    CR_CUDA(cudaEventSynchronize(ctx->frameCopied), "frame staging");
+    if (total > ctx->hFrameCap) {
+        if (ctx->hFrame) cudaFreeHost(ctx->hFrame);
+        ctx->hFrame = nullptr;
+        ctx->hFrameCap = 0;
+        CR_CUDA(cudaMallocHost(&ctx->hFrame, total * 2), "pinned frame table");
+        ctx->hFrameCap = total * 2;
+    }
+    if (total > ctx->dFrameCap) {
+        // the device table may still be read by queued work on another stream
+        CR_CUDA(cudaDeviceSynchronize(), "frame table resize");
+        ctx->dev_free(ctx->dFrame, ctx->dFrameCap);
+        ctx->dFrame = nullptr;
+        ctx->dFrameCap = 0;
+        cr_status s = ctx->dev_alloc(&ctx->dFrame, total * 2, "frame table");
+        if (s) return s;
+        ctx->dFrameCap = total * 2;
+    }
+    char* h = (char*)ctx->hFrame;
+    memcpy(h + oInst, A.inst.data(), n * sizeof(CrInstance));
+    memcpy(h + oWV, A.worldView.data(), n * 64);
+    memcpy(h + oW, A.world.data(), n * 64);
+    memcpy(h + oSeg, A.seg.data(), m * sizeof(CrSegment));
+    CR_CUDA(cudaMemcpyAsync(ctx->dFrame, h, total, cudaMemcpyHostToDevice, stream), "frame table upload");
+    CR_CUDA(cudaEventRecord(ctx->frameCopied, stream), "frame event");
+    char* d = (char*)ctx->dFrame;
+    fp.instances = (const CrInstance*)(d + oInst);
+    fp.world_view = (const float4*)(d + oWV);
+    fp.world = (const float4*)(d + oW);
+    fp.segments = (const CrSegment*)(d + oSeg);
+    fp.numInstances = (uint32_t)n;
+    fp.numSegments = (uint32_t)m;
+    fp.numItems = A.numItems;
+    rp.instances = fp.instances;
+    rp.world = fp.world;
+    rp.numInstances = (uint32_t)n;
+    return CR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cr_abi_version(void) { return CR_ABI_VERSION; }
+
+const char* cr_last_error(void) { return g_error.c_str(); }
+
+void cr_mat4_mul(const float* a, const float* b, float* out) { mat4_mul(a, b, out); }
+
+void cr_config_default(cr_config* cfg) {
+    if (!cfg) return;
+    memset(cfg, 0, sizeof(*cfg));
+    cfg->device = 0;
+    cfg->threshold_small = 128;
+    cfg->threshold_large = 4096;
+    cfg->grow_on_overflow = 1;
+    cfg->wait_timeout_ms = 1000;
+}
+
+cr_status cr_create(const cr_config* cfg, cr_context** out) {
+    if (!out) return fail(CR_ERR_INVALID, "cr_create: out is NULL");
+    *out = nullptr;
+    cr_config c;
+    if (cfg) c = *cfg;
+    else cr_config_default(&c);
+    if (c.threshold_small == 0) c.threshold_small = 128;
+    if (c.threshold_large == 0) c.threshold_large = 4096;
+    if (c.wait_timeout_ms == 0) c.wait_timeout_ms = 1000;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(CR_ERR_UNSUPPORTED, "no CUDA device: %s", cudaGetErrorString(e));
+    }
+    if (c.device < 0 || c.device >= ndev) return fail(CR_ERR_INVALID, "device %d out of range", c.device);
+    CR_CUDA(cudaSetDevice(c.device), "cudaSetDevice");
+    cudaDeviceProp prop;
+    CR_CUDA(cudaGetDeviceProperties(&prop, c.device), "cudaGetDeviceProperties");
+    if (prop.major != 10)
+        return fail(CR_ERR_UNSUPPORTED, "device %d is sm_%d%d; this library is built for sm_100a", c.device, prop.major,
+                    prop.minor);
+    cr_context* ctx = new cr_context();
+    ctx->cfg = c;
+    ctx->device = c.device;
+    if (cr_query_launch_shape(c.device, &ctx->shape) != 0) {
+        delete ctx;
+        return fail(CR_ERR_CUDA, "occupancy query failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    cr_status s = ctx->dev_alloc((void**)&ctx->counters, CR_CTR_COUNT * sizeof(unsigned long long), "counters");
+    if (s) {
+        delete ctx;
+        return s;
+    }
+    if (cudaMallocHost(&ctx->hCounters, CR_CTR_COUNT * sizeof(unsigned long long)) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->frameCopied, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->frameDone, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreate(&ctx->ev[0]) != cudaSuccess || cudaEventCreate(&ctx->ev[1]) != cudaSuccess ||
+        cudaEventCreate(&ctx->ev[2]) != cudaSuccess) {
+        cr_destroy(ctx);
+        return fail(CR_ERR_CUDA, "context setup failed");
+    }
+    cudaEventRecord(ctx->frameCopied, 0);
+    cudaEventRecord(ctx->frameDone, 0);
+    const uint64_t nt0 = c.max_nontrivial ? c.max_nontrivial : (1ull << 20);
+    const uint64_t hu0 = c.max_huge ? c.max_huge : (1ull << 20);
+    s = ensure_queues(ctx, nt0, hu0);
+    if (s) {
+        cr_destroy(ctx);
+        return s;
+    }
+    *out = ctx;
+    return CR_OK;
+}
+
+cr_status cr_destroy(cr_context* ctx) {
+    if (!ctx) return CR_OK;
+    cudaSetDevice(ctx->device);
+    cudaDeviceSynchronize();
+    for (MeshRec& m : ctx->meshes)
+        if (m.live && m.owned) {
+            cudaFree(m.positions);
+            cudaFree(m.indices);
+            cudaFree(m.colors);
+        }
+    if (ctx->ntList) cudaFree(ctx->ntList);
+    if (ctx->hugeList) cudaFree(ctx->hugeList);
+    if (ctx->counters) cudaFree(ctx->counters);
+    if (ctx->dFrame) cudaFree(ctx->dFrame);
+    if (ctx->hFrame) cudaFreeHost(ctx->hFrame);
+    if (ctx->hCounters) cudaFreeHost(ctx->hCounters);
+    if (ctx->frameCopied) cudaEventDestroy(ctx->frameCopied);
+    if (ctx->frameDone) cudaEventDestroy(ctx->frameDone);
+    for (cudaEvent_t& e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t& e : ctx->ring)
+        if (e) cudaEventDestroy(e);
+    delete ctx;
+    return CR_OK;
+}
+
+cr_status cr_mesh_create(cr_context* ctx, const cr_mesh_desc* d, uint32_t* mesh_out) {
+    if (!ctx || !d || !mesh_out) return fail(CR_ERR_INVALID, "cr_mesh_create: NULL argument");
+    if (!d->positions || d->num_vertices == 0) return fail(CR_ERR_INVALID, "cr_mesh_create: no positions");
+    if (!d->indices && (uint64_t)d->num_triangles * 3 > d->num_vertices)
+        return fail(CR_ERR_INVALID, "cr_mesh_create: non-indexed mesh needs 3 vertices per triangle");
+    cudaSetDevice(ctx->device);
+    MeshRec m;
+    m.live = true;
+    m.numVertices = d->num_vertices;
+    m.numTriangles = d->num_triangles;
+    if (d->memory == CR_MEM_DEVICE) {
+        m.owned = false;
+        m.positions = const_cast<float*>(d->positions);
+        m.indices = const_cast<uint32_t*>(d->indices);
+        m.colors = const_cast<uint32_t*>(d->colors);
+    } else if (d->memory == CR_MEM_HOST) {
+        m.owned = true;
+        const size_t pb = align_up((size_t)d->num_vertices * 12, 256) + 256;
+        // index tiles are fetched in 384-byte bursts; pad to whole tiles
+        const size_t ib = d->indices ? align_up((size_t)d->num_triangles * 12, 384) + 256 : 0;
+        const size_t cb = d->colors ? align_up((size_t)d->num_vertices * 4, 256) : 0;
+        cr_status s = ctx->dev_alloc((void**)&m.positions, pb, "mesh positions");
+        if (s) return s;
+        m.bytes += pb;
+        CR_CUDA(cudaMemcpy(m.positions, d->positions, (size_t)d->num_vertices * 12, cudaMemcpyHostToDevice),
+                "mesh positions upload");
+        if (ib) {
+            s = ctx->dev_alloc((void**)&m.indices, ib, "mesh indices");
+            if (s) {
+                ctx->dev_free(m.positions, pb);
+                return s;
+            }
+            m.bytes += ib;
+            CR_CUDA(cudaMemset(m.indices, 0, ib), "mesh index padding");
+            CR_CUDA(cudaMemcpy(m.indices, d->indices, (size_t)d->num_triangles * 12, cudaMemcpyHostToDevice),
+                    "mesh indices upload");
+        }
+        if (cb) {
+            s = ctx->dev_alloc((void**)&m.colors, cb, "mesh colours");
+            if (s) {
+                ctx->dev_free(m.positions, pb);
+                ctx->dev_free(m.indices, ib);
+                return s;
+            }
+            m.bytes += cb;
+            CR_CUDA(cudaMemcpy(m.colors, d->colors, (size_t)d->num_vertices * 4, cudaMemcpyHostToDevice),
+                    "mesh colours upload");
+        }
+    } else {
+        return fail(CR_ERR_INVALID, "cr_mesh_create: unknown memory kind %d", d->memory);
+    }
+    ctx->meshes.push_back(m);
+    *mesh_out = (uint32_t)(ctx->meshes.size() - 1);
+    return CR_OK;
+}
+
+cr_status cr_mesh_destroy(cr_context* ctx, uint32_t mesh) {
+    if (!ctx || mesh >= ctx->meshes.size() || !ctx->meshes[mesh].live) return fail(CR_ERR_NOT_FOUND, "unknown mesh %u", mesh);
+    MeshRec& m = ctx->meshes[mesh];
+    cudaSetDevice(ctx->device);
+    cudaDeviceSynchronize();
+    if (m.owned) {
+        cudaFree(m.positions);
+        cudaFree(m.indices);
+        cudaFree(m.colors);
+        ctx->bytesInUse -= std::min(ctx->bytesInUse, m.bytes);
+    }
+    m = MeshRec{};
+    return CR_OK;
+}
+
+cr_status cr_mesh_device_arrays(cr_context* ctx, uint32_t mesh, uint64_t* d_positions, uint64_t* d_indices,
+                                uint64_t* d_colors) {
+    if (!ctx || mesh >= ctx->meshes.size() || !ctx->meshes[mesh].live) return fail(CR_ERR_NOT_FOUND, "unknown mesh %u", mesh);
+    const MeshRec& m = ctx->meshes[mesh];
+    if (d_positions) *d_positions = (uint64_t)(uintptr_t)m.positions;
+    if (d_indices) *d_indices = (uint64_t)(uintptr_t)m.indices;
+    if (d_colors) *d_colors = (uint64_t)(uintptr_t)m.colors;
+    return CR_OK;
+}
+
+cr_status cr_frame_assemble(cr_context* ctx, const cr_instance* instances, uint32_t count, const float* view,
+                            uint32_t flags, uint32_t* order, uint64_t* first_id, float* world_view) {
+    if (!ctx || (!instances && count) || !view) return fail(CR_ERR_INVALID, "cr_frame_assemble: NULL argument");
+    Assembled A;
+    cr_status s = assemble(ctx, instances, count, view, flags, A);
+    if (s) return s;
+    for (uint32_t i = 0; i < count; i++) {
+        if (order) order[i] = A.order[i];
+        if (first_id) first_id[i] = A.inst[i].cum;
+    }
+    if (world_view) memcpy(world_view, A.worldView.data(), A.worldView.size() * sizeof(float));
+    return CR_OK;
+}
+
+cr_status cr_order_instances(const uint32_t* mesh, const uint32_t* triangles, uint32_t count, uint32_t flags,
+                             uint32_t* order, uint64_t* first_id) {
+    if (count && (!mesh || !triangles || !order)) return fail(CR_ERR_INVALID, "cr_order_instances: NULL argument");
+    std::vector<uint32_t> o;
+    order_instances(
+        count, flags, [&](uint32_t i) { return mesh[i]; }, [&](uint32_t i) { return triangles[i]; }, o);
+    uint64_t sum = 0;
+    for (uint32_t r = 0; r < count; r++) {
+        order[r] = o[r];
+        if (first_id) first_id[r] = sum;
+        sum += triangles[o[r]];
+    }
+    return CR_OK;
+}
+
+cr_status cr_render(cr_context* ctx, const cr_instance* instances, uint32_t count, const cr_camera* cam,
+                    uint64_t d_visbuffer, uint64_t d_rgba, uint64_t d_colorbuffer, int32_t display, uint32_t flags,
+                    void* stream_) {
+    if (!ctx || !cam || (!instances && count)) return fail(CR_ERR_INVALID, "cr_render: NULL argument");
+    if (cam->width <= 0 || cam->height <= 0 || (uint64_t)cam->width * cam->height >= (1ull << 31))
+        return fail(CR_ERR_INVALID, "cr_render: bad resolution %dx%d", cam->width, cam->height);
+    if (!d_visbuffer || (d_visbuffer & 15)) return fail(CR_ERR_INVALID, "cr_render: visbuffer must be 16-byte aligned");
+    if (!(flags & CR_RENDER_NO_RESOLVE) && !d_rgba && !d_colorbuffer)
+        return fail(CR_ERR_INVALID, "cr_render: resolve needs an RGBA8 or colour buffer");
+    cudaStream_t stream = (cudaStream_t)stream_;
+    CR_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+
+    Assembled A;
+    cr_status s = assemble(ctx, instances, count, cam->view, flags, A);
+    if (s) return s;
+    // frame tables, queues and counters are shared by consecutive frames,
+    // which may be issued on different streams
+    CR_CUDA(cudaStreamWaitEvent(stream, ctx->frameDone, 0), "stream wait");
+    const uint64_t numPixels = (uint64_t)cam->width * (uint64_t)cam->height;
+
+    CrFrameParams fp{};
+    CrResolveParams rp{};
+    if (count) {
+        s = upload_frame(ctx, A, stream, fp, rp);
+        if (s) return s;
+    }
+    fp.fb = (uint64_t*)d_visbuffer;
+    fp.W = cam->width;
+    fp.H = cam->height;
+    fp.f = cam->proj[5];
+    fp.aspect = (float)cam->width / (float)cam->height;
+    fp.thrSmall = ctx->cfg.threshold_small;
+    fp.thrLarge = ctx->cfg.threshold_large;
+    fp.counters = ctx->counters;
+    fp.waitTimeoutNs = (uint64_t)ctx->cfg.wait_timeout_ms * 1000000ull;
+    fp.debugFlags = ctx->cfg.debug_flags;
+
+    rp.display = display;
+    rp.fb = (const uint64_t*)d_visbuffer;
+    rp.colorbuffer = (uint64_t*)d_colorbuffer;
+    rp.rgba = (uint32_t*)d_rgba;
+    rp.W = cam->width;
+    rp.H = cam->height;
+    mat4_inverse(cam->view, rp.viewI);
+    for (int r = 0; r < 3; r++)  // viewI * (0,0,0,1)
+        rp.origin[r] = (rp.viewI[0 + r] * 0.0f + rp.viewI[4 + r] * 0.0f) + (rp.viewI[8 + r] * 0.0f + rp.viewI[12 + r] * 1.0f);
+    rp.p00 = cam->proj[0];
+    rp.p11 = cam->proj[5];
+    rp.background = 0xffffffffu;  // HostDeviceInterface.h:37 BACKGROUND_COLOR
+
+    const bool sync = (flags & CR_RENDER_SYNC) != 0;
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        fp.ntList = ctx->ntList;
+        fp.ntCap = ctx->ntCap;
+        fp.hugeList = ctx->hugeList;
+        fp.hugeCap = ctx->hugeCap;
+        cudaEvent_t* tev = nullptr;  // 6 timing events of this frame, or none
+        if (flags & CR_RENDER_TIMING) {
+            if (ctx->ring.empty()) {
+                ctx->ring.resize(6 * cr_context::kRing, nullptr);
+                for (cudaEvent_t& e : ctx->ring) CR_CUDA(cudaEventCreate(&e), "timing events");
+            }
+            if (ctx->ringCount == cr_context::kRing) {  // full: fold the oldest frame first
+                cr_stage_times tmp;
+                cr_status ds = cr_drain_stage_times(ctx, &tmp);
+                if (ds) return ds;
+            }
+            tev = &ctx->ring[6 * ((ctx->ringHead + ctx->ringCount) % cr_context::kRing)];
+            ctx->ringCount++;
+        }
+        auto mark = [&](int i) -> cudaError_t { return tev ? cudaEventRecord(tev[i], stream) : cudaSuccess; };
+        if (sync) CR_CUDA(cudaEventRecord(ctx->ev[0], stream), "event");
+        CR_CUDA(mark(0), "event");
+        if (flags & CR_RENDER_NO_CLEAR) {
+            CR_CUDA(cudaMemsetAsync(ctx->counters, 0, CR_CTR_COUNT * sizeof(unsigned long long), stream), "counters");
+        } else if (cr_launch_clear(fp.fb, numPixels, ctx->counters, stream)) {
+            return fail(CR_ERR_CUDA, "clear launch: %s", cudaGetErrorString(cudaGetLastError()));
+        }
+        CR_CUDA(mark(1), "event");
+        if (count && cr_launch_stage1(fp, ctx->shape, stream))
+            return fail(CR_ERR_CUDA, "stage-1 launch: %s", cudaGetErrorString(cudaGetLastError()));
+        CR_CUDA(mark(2), "event");
+        if (count && cr_launch_stage2(fp, ctx->shape, stream))
+            return fail(CR_ERR_CUDA, "stage-2 launch: %s", cudaGetErrorString(cudaGetLastError()));
+        CR_CUDA(mark(3), "event");
+        if (count && cr_launch_stage3(fp, ctx->shape, stream))
+            return fail(CR_ERR_CUDA, "stage-3 launch: %s", cudaGetErrorString(cudaGetLastError()));
+        CR_CUDA(mark(4), "event");
+        if (sync) CR_CUDA(cudaEventRecord(ctx->ev[1], stream), "event");
+        if (!(flags & CR_RENDER_NO_RESOLVE) && count && cr_launch_resolve(rp, stream))
+            return fail(CR_ERR_CUDA, "resolve launch: %s", cudaGetErrorString(cudaGetLastError()));
+        CR_CUDA(mark(5), "event");
+        CR_CUDA(cudaMemcpyAsync(ctx->hCounters, ctx->counters, CR_CTR_COUNT * sizeof(unsigned long long),
+                                cudaMemcpyDeviceToHost, stream),
+                "counters readback");
+        ctx->last = cr_frame_stats{};
+        ctx->last.instances = count;
+        ctx->last.triangles = A.totalTriangles;
+        ctx->pendingStats = true;
+        ctx->lastStream = stream;
+        CR_CUDA(cudaEventRecord(ctx->frameDone, stream), "frame event");
+        if (!sync) return CR_OK;
+        CR_CUDA(cudaEventRecord(ctx->ev[2], stream), "event");
+        CR_CUDA(cudaEventSynchronize(ctx->ev[2]), "frame");
+        cudaEventElapsedTime(&ctx->last.ms_total, ctx->ev[0], ctx->ev[2]);
+        cudaEventElapsedTime(&ctx->last.ms_raster, ctx->ev[0], ctx->ev[1]);
+        cudaEventElapsedTime(&ctx->last.ms_resolve, ctx->ev[1], ctx->ev[2]);
+        ctx->pendingStats = false;
+        ctx->last.nontrivial = ctx->hCounters[CR_CTR_NONTRIVIAL];
+        ctx->last.huge_tiles = ctx->hCounters[CR_CTR_HUGE];
+        ctx->last.overflow = ctx->hCounters[CR_CTR_OVERFLOW];
+        if (ctx->hCounters[CR_CTR_TIMEOUT]) return fail(CR_ERR_TIMEOUT, "a device-side wait timed out");
+        if (!ctx->last.overflow) return CR_OK;
+        if (!ctx->cfg.grow_on_overflow || (flags & CR_RENDER_NO_CLEAR))
+            return fail(CR_ERR_QUEUE_OVERFLOW, "queue overflow: nontrivial %llu/%llu, tiles %llu/%llu",
+                        (unsigned long long)ctx->last.nontrivial, (unsigned long long)ctx->ntCap,
+                        (unsigned long long)ctx->last.huge_tiles, (unsigned long long)ctx->hugeCap);
+        // the counters hold the exact demand of every queue that was fed in full
+        const uint64_t ntWant = std::max<uint64_t>(ctx->ntCap, ctx->last.nontrivial + ctx->last.nontrivial / 8 + 1024);
+        const uint64_t huWant = (ctx->last.overflow & 1)
+                                    ? ctx->hugeCap
+                                    : std::max<uint64_t>(ctx->hugeCap, ctx->last.huge_tiles + ctx->last.huge_tiles / 8 + 1024);
+        s = ensure_queues(ctx, ntWant, huWant);
+        if (s) return s;
+    }
+    return fail(CR_ERR_QUEUE_OVERFLOW, "queue overflow persisted after growing the queues");
+}
+
+cr_status cr_sync(cr_context* ctx) {
+    if (!ctx) return fail(CR_ERR_INVALID, "cr_sync: NULL context");
+    CR_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    if (ctx->pendingStats) {
+        CR_CUDA(cudaStreamSynchronize(ctx->lastStream), "sync");
+        ctx->last.nontrivial = ctx->hCounters[CR_CTR_NONTRIVIAL];
+        ctx->last.huge_tiles = ctx->hCounters[CR_CTR_HUGE];
+        ctx->last.overflow = ctx->hCounters[CR_CTR_OVERFLOW];
+        ctx->pendingStats = false;
+        if (ctx->hCounters[CR_CTR_TIMEOUT]) return fail(CR_ERR_TIMEOUT, "a device-side wait timed out");
+        if (ctx->last.overflow)
+            return fail(CR_ERR_QUEUE_OVERFLOW, "the last frame overflowed its queues; render it with CR_RENDER_SYNC");
+    }
+    return CR_OK;
+}
+
+cr_status cr_drain_stage_times(cr_context* ctx, cr_stage_times* out) {
+    if (!ctx || !out) return fail(CR_ERR_INVALID, "cr_drain_stage_times: NULL argument");
+    memset(out, 0, sizeof(*out));
+    CR_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    while (ctx->ringCount > 0) {
+        cudaEvent_t* e = &ctx->ring[6 * ctx->ringHead];
+        CR_CUDA(cudaEventSynchronize(e[5]), "timing sync");
+        for (int i = 0; i < 5; i++) {
+            float ms = 0.0f;
+            CR_CUDA(cudaEventElapsedTime(&ms, e[i], e[i + 1]), "timing");
+            out->ms[i] += ms;
+        }
+        out->frames++;
+        ctx->ringHead = (ctx->ringHead + 1) % cr_context::kRing;
+        ctx->ringCount--;
+    }
+    return CR_OK;
+}
+
+cr_status cr_last_frame_stats(cr_context* ctx, cr_frame_stats* out) {
+    if (!ctx || !out) return fail(CR_ERR_INVALID, "cr_last_frame_stats: NULL argument");
+    cr_status s = cr_sync(ctx);
+    *out = ctx->last;
+    return s;
+}
+
+}  // extern "C"

@@ -1,0 +1,111 @@
+// cr_device.h -- records shared by the host library and the sm_100a kernels.
+//
+// HBM layout of one frame (all arrays 16-byte aligned, written once per frame
+// by one host->device copy of a packed frame table):
+//   CrInstance  instances[n]      64 B each, render order
+//   float4      world_view[n][4]  view * world, column-major (glm order)
+//   float4      world[n][4]       object -> world, for the resolve
+//   CrSegment   segments[m]       runs of consecutive instances of one mesh
+// Work queues (library-owned, grown on demand):
+//   uint64_t    nontrivial[cap]   (instance << 32 | triangle), tv.cu:192-197
+//   CrTile      huge[cap]         {instance, triangle, tile_x, tile_y}, HostDeviceInterface.h:254-259
+//   unsigned long long counters[8]  see CR_CTR_*
+#pragma once
+#include <cstdint>
+
+#define CR_TILE_SIZE 64         // HostDeviceInterface.h:261
+#define CR_BATCH 32             // triangles per stage-1 warp item
+#define CR_INST_CHUNK 16        // instances per stage-1 warp item
+
+// counters[] slots
+#define CR_CTR_NONTRIVIAL 0     // entries appended to the stage-2 queue
+#define CR_CTR_HUGE 1           // tiles appended to the stage-3 queue
+#define CR_CTR_OVERFLOW 2       // bit 0: stage-2 queue, bit 1: stage-3 queue
+#define CR_CTR_TIMEOUT 3        // nonzero if a bounded device wait gave up
+#define CR_CTR_COUNT 8
+
+struct alignas(16) CrInstance {
+    const uint32_t* indices;    // nullptr -> vertex index 3*t+k
+    const float* positions;     // xyz, 12-byte stride
+    const uint32_t* colors;     // RGBA8 per vertex, may be nullptr
+    uint64_t cum;               // first global triangle id of this instance
+    uint32_t numTriangles;
+    uint32_t flip;              // det(world_view 3x3) < 0, tv.cu:179-185
+    uint32_t numVertices;
+    uint32_t pad0;
+    uint64_t pad1[2];
+};
+static_assert(sizeof(CrInstance) == 64, "CrInstance layout");
+
+struct alignas(16) CrSegment {
+    const uint32_t* indices;
+    const float* positions;
+    uint32_t numTriangles;
+    uint32_t firstInstance;
+    uint32_t instanceCount;
+    uint32_t numBatches;        // ceil(numTriangles / CR_BATCH)
+    uint32_t numChunks;         // ceil(instanceCount / CR_INST_CHUNK)
+    uint32_t flags;             // bit 0: index array 16-byte aligned (TMA tiles)
+    uint64_t itemBase;          // first stage-1 work item of this segment
+};
+static_assert(sizeof(CrSegment) == 48, "CrSegment layout");
+
+struct alignas(16) CrTile {     // HugeTriangle, HostDeviceInterface.h:254-259
+    int32_t instance;
+    int32_t triangle;
+    int32_t tile_x;
+    int32_t tile_y;
+};
+
+struct CrFrameParams {
+    const CrInstance* instances;
+    const float4* world_view;   // 4 per instance
+    const float4* world;        // 4 per instance
+    const CrSegment* segments;
+    uint32_t numInstances;
+    uint32_t numSegments;
+    uint64_t numItems;          // stage-1 work items
+    uint64_t* fb;               // visbuffer, W*H
+    int32_t W, H;
+    float f;                    // proj[1][1]
+    float aspect;               // float(W) / float(H)
+    uint32_t thrSmall, thrLarge;
+    uint64_t* ntList;
+    uint64_t ntCap;
+    CrTile* hugeList;
+    uint64_t hugeCap;
+    unsigned long long* counters;
+    uint64_t waitTimeoutNs;     // bound of every device-side wait
+    uint32_t debugFlags;        // CR_DEBUG_* (failure-detection tests)
+    uint32_t pad;
+};
+
+struct CrResolveParams {
+    const CrInstance* instances;
+    const float4* world;
+    uint32_t numInstances;
+    int32_t display;
+    const uint64_t* fb;
+    uint64_t* colorbuffer;      // may be nullptr
+    uint32_t* rgba;             // may be nullptr
+    int32_t W, H;
+    float viewI[16];            // inverse(view), glm::inverse float order
+    float origin[3];            // viewI * (0,0,0,1)
+    float p00, p11;             // proj[0][0], proj[1][1]
+    uint32_t background;
+};
+
+// Launch helpers implemented in raster.cu / resolve.cu.
+struct CrLaunchShape {
+    int numSMs;
+    int stage1Blocks;
+    int stage2Blocks;
+    int stage3Blocks;
+};
+
+int cr_query_launch_shape(int device, CrLaunchShape* out);
+int cr_launch_clear(uint64_t* fb, uint64_t numPixels, unsigned long long* counters, void* stream);
+int cr_launch_stage1(const CrFrameParams& p, const CrLaunchShape& s, void* stream);
+int cr_launch_stage2(const CrFrameParams& p, const CrLaunchShape& s, void* stream);
+int cr_launch_stage3(const CrFrameParams& p, const CrLaunchShape& s, void* stream);
+int cr_launch_resolve(const CrResolveParams& p, void* stream);

@@ -1,0 +1,172 @@
+// resolve.cu -- visbuffer -> colour for sm_100a.
+//
+// One thread per pixel, 32x8 blocks so each warp reads 32 consecutive
+// visbuffer entries (256 B) and writes 32 consecutive RGBA8 values.  It fuses
+// the reference's two passes, kernel_resolve_visbuffer_to_colorbuffer2D
+// (src/kernels/resolve.cu:640-1141, DisplayAttribute NONE / TRIANGLE_ID /
+// VERTEX_COLORS) and kernel_resolve_colorbuffer_to_screenshot
+// (resolve.cu:1264-1313 with EDL and SSAO off), so the 64-bit colorbuffer is
+// written only when the caller asks for it and never read back.
+// inverse(view) is formed once on the host instead of once per pixel.
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "cr_device.h"
+
+namespace {
+
+struct V3 {
+    float x, y, z;
+};
+
+__device__ __forceinline__ V3 sub3(V3 a, V3 b) { return V3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ float dot3(V3 a, V3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+__device__ __forceinline__ V3 cross3(V3 x, V3 y) {
+    return V3{x.y * y.z - y.y * x.z, x.z * y.x - y.z * x.x, x.x * y.y - y.x * x.y};
+}
+// glm::normalize: v * inversesqrt(dot(v, v)), inversesqrt(x) = 1 / sqrt(x)
+__device__ __forceinline__ V3 normalize3(V3 v) {
+    const float inv = 1.0f / sqrtf(dot3(v, v));
+    return V3{v.x * inv, v.y * inv, v.z * inv};
+}
+
+__device__ __forceinline__ V3 xform_m(const float* m, V3 p) {  // m column-major, w = 1
+    return V3{(m[0] * p.x + m[4] * p.y) + (m[8] * p.z + m[12] * 1.0f),
+              (m[1] * p.x + m[5] * p.y) + (m[9] * p.z + m[13] * 1.0f),
+              (m[2] * p.x + m[6] * p.y) + (m[10] * p.z + m[14] * 1.0f)};
+}
+
+__device__ __forceinline__ V3 xform_f4(const float4* m, V3 p) {
+    const float4 c0 = __ldg(m), c1 = __ldg(m + 1), c2 = __ldg(m + 2), c3 = __ldg(m + 3);
+    return V3{(c0.x * p.x + c1.x * p.y) + (c2.x * p.z + c3.x * 1.0f),
+              (c0.y * p.x + c1.y * p.y) + (c2.y * p.z + c3.y * 1.0f),
+              (c0.z * p.x + c1.z * p.y) + (c2.z * p.z + c3.z * 1.0f)};
+}
+
+__device__ __forceinline__ float clamp_ref(float v, float lo, float hi) {
+    if (v < lo) return lo;
+    if (v > hi) return hi;
+    return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T* ldg_ptr(T* const* p) {
+    return reinterpret_cast<T*>(__ldg(reinterpret_cast<const unsigned long long*>(p)));
+}
+
+__device__ __forceinline__ V3 load_pos(const float* pos, uint32_t idx) {
+    const float* q = pos + 3ull * idx;
+    return V3{__ldg(q), __ldg(q + 1), __ldg(q + 2)};
+}
+
+__global__ void __launch_bounds__(256) k_resolve(const CrResolveParams p) {
+    const int x = blockIdx.x * 32 + threadIdx.x;
+    const int y = blockIdx.y * 8 + threadIdx.y;
+    if (x >= p.W || y >= p.H) return;
+    const int pid = x + p.W * y;
+    const uint64_t pixel = __ldcs(reinterpret_cast<const unsigned long long*>(p.fb) + pid);
+
+    // unpack_pixel, helpers:54-66
+    const uint32_t ud = (uint32_t)(pixel >> 33) & 0x7FFFFFF8u;
+    const float depth = (ud == 0x7FFFFFF8u) ? INFINITY : __uint_as_float(ud);
+    const uint64_t tid = pixel & 0xFFFFFFFFFull;
+
+    uint32_t color = 0;
+    if (!isinf(depth)) {
+        // instance whose [cum, next cum) holds tid (resolve.cu:697-721)
+        uint32_t lo = 0, hi = p.numInstances - 1;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (__ldg(&p.instances[mid].cum) <= tid) lo = mid;
+            else hi = mid - 1;
+        }
+        const CrInstance* I = p.instances + lo;
+        const uint32_t nT = __ldg(&I->numTriangles);
+        uint32_t tri = (uint32_t)(tid - __ldg(&I->cum));
+        tri = min(tri, nT - 1u);
+        const uint32_t* colors = ldg_ptr(&I->colors);
+        if (p.display == 0) {  // DisplayAttribute::NONE
+            color = 0xffffffffu;
+        } else if (p.display == 5) {  // DisplayAttribute::TRIANGLE_ID
+            color = tri * 12345678u;
+        } else if (p.display == 4 && colors) {  // DisplayAttribute::VERTEX_COLORS
+            const uint32_t* ix = ldg_ptr(&I->indices);
+            uint32_t i0, i1, i2;
+            if (ix) {
+                i0 = __ldg(ix + 3ull * tri + 0);
+                i1 = __ldg(ix + 3ull * tri + 1);
+                i2 = __ldg(ix + 3ull * tri + 2);
+            } else {
+                i0 = 3 * tri + 0;
+                i1 = 3 * tri + 1;
+                i2 = 3 * tri + 2;
+            }
+            const float* pos = ldg_ptr(&I->positions);
+            const float4* W4 = p.world + 4ull * lo;
+            const V3 aw = xform_f4(W4, load_pos(pos, i0));
+            const V3 bw = xform_f4(W4, load_pos(pos, i1));
+            const V3 cw = xform_f4(W4, load_pos(pos, i2));
+
+            // computeRayDir, resolve.cu:662-676
+            const V3 origin = {p.origin[0], p.origin[1], p.origin[2]};
+            const float u = 2.0f * ((float)x + 0.5f) / (float)p.W - 1.0f;
+            const float v = 2.0f * ((float)y + 0.5f) / (float)p.H - 1.0f;
+            const V3 rdv = normalize3(V3{1.0f / p.p00 * u, 1.0f / p.p11 * v, -1.0f});
+            const V3 rayDir = normalize3(sub3(xform_m(p.viewI, rdv), origin));
+
+            // intersectPlane (helpers:318-348) and barycentrics (resolve.cu:790-834)
+            const V3 e1 = sub3(bw, aw);
+            const V3 e2 = sub3(cw, aw);
+            const V3 normal = normalize3(cross3(e1, e2));
+            const float d = dot3(aw, normal);
+            const float den = dot3(normal, rayDir);
+            float t = INFINITY;
+            if (den != 0.0f) {
+                const float tt = -(dot3(origin, normal) + -d) / den;
+                t = tt >= 0.0f ? tt : INFINITY;
+            }
+            const float d00 = dot3(e1, e1);
+            const float d01 = dot3(e1, e2);
+            const float d11 = dot3(e2, e2);
+            const float denomI = 1.0f / (d00 * d11 - d01 * d01);
+            const V3 ph = {origin.x + t * rayDir.x, origin.y + t * rayDir.y, origin.z + t * rayDir.z};
+            const V3 v2 = sub3(ph, aw);
+            const float d20 = dot3(v2, e1);
+            const float d21 = dot3(v2, e2);
+            const float sx = (d11 * d20 - d01 * d21) * denomI;
+            const float sy = (d00 * d21 - d01 * d20) * denomI;
+            const float w0 = 1.0f - sx - sy;
+
+            const uint32_t Ca = __ldg(colors + i0), Cb = __ldg(colors + i1), Cc = __ldg(colors + i2);
+            color = Ca;
+#pragma unroll
+            for (int ch = 0; ch < 3; ++ch) {
+                const float ca = (float)((Ca >> (8 * ch)) & 0xffu);
+                const float cb = (float)((Cb >> (8 * ch)) & 0xffu);
+                const float cc = (float)((Cc >> (8 * ch)) & 0xffu);
+                const float c = ca * w0 + cb * sx + cc * sy;
+                const uint32_t b8 = __float2uint_rz(clamp_ref(c, 0.0f, 255.0f)) & 0xffu;
+                color = (color & ~(0xffu << (8 * ch))) | (b8 << (8 * ch));
+            }
+        } else {
+            color = 0xff0000ffu;
+        }
+        color |= 0xff000000u;
+    }
+    if (p.colorbuffer) {
+        const uint64_t v = (depth != INFINITY) ? (((uint64_t)__float_as_uint(depth) << 32) | color)
+                                               : ((uint64_t)0x7f800000u << 32);
+        __stcs(reinterpret_cast<unsigned long long*>(p.colorbuffer) + pid, (unsigned long long)v);
+    }
+    if (p.rgba) __stcs(p.rgba + pid, isinf(depth) ? p.background : color);
+}
+
+}  // namespace
+
+int cr_launch_resolve(const CrResolveParams& p, void* stream) {
+    if (p.W <= 0 || p.H <= 0 || p.numInstances == 0) return 0;
+    dim3 block(32, 8);
+    dim3 grid((p.W + 31) / 32, (p.H + 7) / 8);
+    k_resolve<<<grid, block, 0, (cudaStream_t)stream>>>(p);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}

@@ -1,0 +1,303 @@
+"""ctypes binding of libcurast_b200.so (include/curast_b200.h).
+
+A thin host-side wrapper used by the tests and the benchmark; the product is
+the C ABI itself.  Device buffers are passed as integer addresses (for
+example ``tensor.data_ptr()``), streams as ``cudaStream_t`` integers.  If the
+shared library is missing this module raises instead of falling back to
+anything else.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcurast_b200.so")
+
+CR_OK = 0
+CR_ERR_INVALID = 1
+CR_ERR_OOM = 2
+CR_ERR_QUEUE_OVERFLOW = 3
+CR_ERR_TIMEOUT = 4
+CR_ERR_CUDA = 5
+CR_ERR_BUSY = 6
+CR_ERR_NOT_FOUND = 7
+CR_ERR_UNSUPPORTED = 8
+
+CR_MEM_HOST = 0
+CR_MEM_DEVICE = 1
+
+CR_DISPLAY_NONE = 0
+CR_DISPLAY_VERTEX_COLORS = 4
+CR_DISPLAY_TRIANGLE_ID = 5
+
+CR_RENDER_SYNC = 1 << 0
+CR_RENDER_KEEP_ORDER = 1 << 1
+CR_RENDER_NO_RESOLVE = 1 << 2
+CR_RENDER_NO_CLEAR = 1 << 3
+CR_RENDER_TIMING = 1 << 4
+STAGES = ("clear", "stage1", "stage2", "stage3", "resolve")
+
+CLEAR_PIXEL = 0xFFFFFFF000000000
+BACKGROUND = 0xFFFFFFFF
+
+_u32, _i32, _u64, _f32 = ctypes.c_uint32, ctypes.c_int32, ctypes.c_uint64, ctypes.c_float
+
+
+class CrConfig(ctypes.Structure):
+    _fields_ = [
+        ("device", _i32),
+        ("threshold_small", _u32),
+        ("threshold_large", _u32),
+        ("stage1_warps", _u32),
+        ("max_nontrivial", _u64),
+        ("max_huge", _u64),
+        ("memory_budget", _u64),
+        ("grow_on_overflow", _u32),
+        ("wait_timeout_ms", _u32),
+        ("debug_flags", _u32),
+        ("reserved", _u32 * 5),
+    ]
+
+
+CR_DEBUG_DROP_FIRST_TILE_COPY = 1
+
+
+class CrMeshDesc(ctypes.Structure):
+    _fields_ = [
+        ("positions", ctypes.c_void_p),
+        ("indices", ctypes.c_void_p),
+        ("colors", ctypes.c_void_p),
+        ("num_vertices", _u32),
+        ("num_triangles", _u32),
+        ("memory", _i32),
+        ("reserved", _u32),
+    ]
+
+
+class CrInstance(ctypes.Structure):
+    _fields_ = [("mesh", _u32), ("reserved", _u32), ("world", _f32 * 16)]
+
+
+class CrCamera(ctypes.Structure):
+    _fields_ = [("view", _f32 * 16), ("proj", _f32 * 16), ("width", _i32), ("height", _i32)]
+
+
+class CrFrameStats(ctypes.Structure):
+    _fields_ = [
+        ("nontrivial", _u64),
+        ("huge_tiles", _u64),
+        ("overflow", _u64),
+        ("instances", _u64),
+        ("triangles", _u64),
+        ("ms_total", _f32),
+        ("ms_raster", _f32),
+        ("ms_resolve", _f32),
+        ("reserved", _f32),
+    ]
+
+
+class CrStageTimes(ctypes.Structure):
+    _fields_ = [("ms", _f32 * 5), ("frames", _u32)]
+
+
+EXPORTS = {
+    "cr_drain_stage_times": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrStageTimes)]),
+    "cr_config_default": (None, [ctypes.POINTER(CrConfig)]),
+    "cr_create": (_i32, [ctypes.POINTER(CrConfig), ctypes.POINTER(ctypes.c_void_p)]),
+    "cr_destroy": (_i32, [ctypes.c_void_p]),
+    "cr_last_error": (ctypes.c_char_p, []),
+    "cr_abi_version": (_i32, []),
+    "cr_mesh_create": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrMeshDesc), ctypes.POINTER(_u32)]),
+    "cr_mesh_destroy": (_i32, [ctypes.c_void_p, _u32]),
+    "cr_mesh_device_arrays": (_i32, [ctypes.c_void_p, _u32, ctypes.POINTER(_u64), ctypes.POINTER(_u64),
+                                     ctypes.POINTER(_u64)]),
+    "cr_frame_assemble": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrInstance), _u32, ctypes.c_void_p, _u32,
+                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "cr_render": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrInstance), _u32, ctypes.POINTER(CrCamera), _u64, _u64,
+                         _u64, _i32, _u32, ctypes.c_void_p]),
+    "cr_last_frame_stats": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrFrameStats)]),
+    "cr_sync": (_i32, [ctypes.c_void_p]),
+    "cr_mat4_mul": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "cr_order_instances": (_i32, [ctypes.c_void_p, ctypes.c_void_p, _u32, _u32, ctypes.c_void_p, ctypes.c_void_p]),
+}
+
+
+def order_instances(mesh, triangles, keep_order=False):
+    """The frame-assembly ordering rule (host only)."""
+    mesh = np.ascontiguousarray(mesh, np.uint32)
+    tris = np.ascontiguousarray(triangles, np.uint32)
+    n = mesh.size
+    order = np.zeros(max(n, 1), np.uint32)
+    first = np.zeros(max(n, 1), np.uint64)
+    _check(load().cr_order_instances(mesh.ctypes.data, tris.ctypes.data, n,
+                                     CR_RENDER_KEEP_ORDER if keep_order else 0, order.ctypes.data, first.ctypes.data))
+    return order[:n], first[:n]
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Loads the shared library (raises if it is missing or incomplete)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `make -C {HERE}` (sm_100a CUDA path only)")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in EXPORTS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class CurastError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"status {status}: {msg}")
+        self.status = status
+
+
+def _check(st):
+    if st != CR_OK:
+        raise CurastError(st, load().cr_last_error().decode(errors="replace"))
+
+
+def _f16(m):
+    a = np.ascontiguousarray(np.asarray(m, dtype=np.float32).reshape(16))
+    return (_f32 * 16)(*a.tolist())
+
+
+def mat4_mul(a, b):
+    """glm-order float product a * b of two column-major 4x4 matrices."""
+    lib = load()
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.float32).reshape(16))
+    b = np.ascontiguousarray(np.asarray(b, dtype=np.float32).reshape(16))
+    out = np.empty(16, dtype=np.float32)
+    lib.cr_mat4_mul(a.ctypes.data, b.ctypes.data, out.ctypes.data)
+    return out
+
+
+def make_camera(view, proj, width, height):
+    return CrCamera(_f16(view), _f16(proj), int(width), int(height))
+
+
+def make_instances(pairs):
+    """pairs: iterable of (mesh_handle, world 4x4 column-major (16 floats))."""
+    pairs = list(pairs)
+    arr = (CrInstance * max(len(pairs), 1))()
+    for i, (m, w) in enumerate(pairs):
+        arr[i].mesh = int(m)
+        arr[i].world = _f16(w)
+    return arr, len(pairs)
+
+
+class Context:
+    """Owns one cr_context (device geometry, work queues)."""
+
+    def __init__(self, device=0, threshold_small=128, threshold_large=4096, max_nontrivial=0, max_huge=0,
+                 memory_budget=0, grow_on_overflow=1, wait_timeout_ms=1000, debug_flags=0):
+        lib = load()
+        cfg = CrConfig()
+        lib.cr_config_default(ctypes.byref(cfg))
+        cfg.device = device
+        cfg.wait_timeout_ms = wait_timeout_ms
+        cfg.debug_flags = debug_flags
+        cfg.threshold_small = threshold_small
+        cfg.threshold_large = threshold_large
+        cfg.max_nontrivial = max_nontrivial
+        cfg.max_huge = max_huge
+        cfg.memory_budget = memory_budget
+        cfg.grow_on_overflow = grow_on_overflow
+        h = ctypes.c_void_p()
+        _check(lib.cr_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self.h = h
+        self._keep = []
+
+    def close(self):
+        if self.h:
+            load().cr_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def mesh_from_host(self, positions, indices, colors=None):
+        """positions (V,3) float32, indices (T,3) uint32 or None, colors (V,) uint32 or None."""
+        pos = np.ascontiguousarray(positions, dtype=np.float32)
+        idx = None if indices is None else np.ascontiguousarray(indices, dtype=np.uint32)
+        col = None if colors is None else np.ascontiguousarray(colors, dtype=np.uint32)
+        d = CrMeshDesc()
+        d.positions = pos.ctypes.data
+        d.indices = idx.ctypes.data if idx is not None else None
+        d.colors = col.ctypes.data if col is not None else None
+        d.num_vertices = pos.shape[0]
+        d.num_triangles = (idx.shape[0] if idx is not None else pos.shape[0] // 3)
+        d.memory = CR_MEM_HOST
+        out = _u32()
+        _check(load().cr_mesh_create(self.h, ctypes.byref(d), ctypes.byref(out)))
+        return out.value
+
+    def mesh_from_device(self, d_positions, num_vertices, d_indices, num_triangles, d_colors=0):
+        """Borrows device arrays (addresses); they must outlive the mesh."""
+        d = CrMeshDesc()
+        d.positions = int(d_positions)
+        d.indices = int(d_indices) if d_indices else None
+        d.colors = int(d_colors) if d_colors else None
+        d.num_vertices = int(num_vertices)
+        d.num_triangles = int(num_triangles)
+        d.memory = CR_MEM_DEVICE
+        out = _u32()
+        _check(load().cr_mesh_create(self.h, ctypes.byref(d), ctypes.byref(out)))
+        return out.value
+
+    def mesh_device_arrays(self, mesh):
+        p, i, c = _u64(), _u64(), _u64()
+        _check(load().cr_mesh_device_arrays(self.h, mesh, ctypes.byref(p), ctypes.byref(i), ctypes.byref(c)))
+        return p.value, i.value, c.value
+
+    def frame_assemble(self, instances, view, keep_order=False):
+        arr, n = make_instances(instances) if not isinstance(instances, tuple) else instances
+        order = np.zeros(max(n, 1), dtype=np.uint32)
+        first = np.zeros(max(n, 1), dtype=np.uint64)
+        wv = np.zeros((max(n, 1), 16), dtype=np.float32)
+        v = np.ascontiguousarray(np.asarray(view, dtype=np.float32).reshape(16))
+        _check(load().cr_frame_assemble(self.h, arr, n, v.ctypes.data, CR_RENDER_KEEP_ORDER if keep_order else 0,
+                                        order.ctypes.data, first.ctypes.data, wv.ctypes.data))
+        return order[:n], first[:n], wv[:n]
+
+    def render(self, instances, camera, d_visbuffer, d_rgba=0, d_colorbuffer=0,
+               display=CR_DISPLAY_VERTEX_COLORS, flags=CR_RENDER_SYNC, stream=0):
+        arr, n = make_instances(instances) if not isinstance(instances, tuple) else instances
+        _check(load().cr_render(self.h, arr, n, ctypes.byref(camera), int(d_visbuffer), int(d_rgba),
+                                int(d_colorbuffer), int(display), int(flags), ctypes.c_void_p(int(stream))))
+
+    def render_status(self, instances, camera, d_visbuffer, d_rgba=0, d_colorbuffer=0,
+                      display=CR_DISPLAY_VERTEX_COLORS, flags=CR_RENDER_SYNC, stream=0):
+        arr, n = make_instances(instances) if not isinstance(instances, tuple) else instances
+        return load().cr_render(self.h, arr, n, ctypes.byref(camera), int(d_visbuffer), int(d_rgba),
+                                int(d_colorbuffer), int(display), int(flags), ctypes.c_void_p(int(stream)))
+
+    def stats(self):
+        s = CrFrameStats()
+        st = load().cr_last_frame_stats(self.h, ctypes.byref(s))
+        return st, s
+
+    def sync(self):
+        _check(load().cr_sync(self.h))
+
+    def drain_stage_times(self):
+        """{stage: summed ms}, frame count -- for frames rendered with CR_RENDER_TIMING."""
+        t = CrStageTimes()
+        _check(load().cr_drain_stage_times(self.h, ctypes.byref(t)))
+        return {k: float(t.ms[i]) for i, k in enumerate(STAGES)}, int(t.frames)

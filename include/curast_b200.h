@@ -1,0 +1,192 @@
+/*
+ * curast_b200.h -- C ABI of the B200-native CuRast visibility-buffer
+ * rasterizer.
+ *
+ * The library replaces the CUDA rasterization path of CuRast
+ * (MrBigoudi/CuRast-OOC).  Each entry point names the reference interface it
+ * stands in for (paths inside the reference project):
+ *
+ *   cr_render        CuRast::draw's CUDA visbuffer branch
+ *                    (src/CuRast_render.h:356-592): frame assembly, clear,
+ *                    drawTrianglesVisbuffer (src/CuRast_render.h:211-264,
+ *                    the three kernel_stage{1,2,3}_* launches of
+ *                    src/kernels/triangles_visbuffer.cu:755-835) and
+ *                    kernel_resolve_visbuffer_to_colorbuffer2D +
+ *                    kernel_resolve_colorbuffer_to_screenshot
+ *                    (src/kernels/resolve.cu:640-1141,1264-1313).
+ *   cr_mesh_create   the loader's device upload of one mesh
+ *                    (src/LargeGlbLoader.h:504-521, CMesh::indices/positions/
+ *                    colors at src/kernels/HostDeviceInterface.h:196-234).
+ *
+ * Conventions
+ *   - Plain pointers and sizes only.  Pointers named d_* are device pointers
+ *     on the context's device; all others are host pointers.
+ *   - Every call returns a cr_status; nothing exits the process.  The text of
+ *     the last error of the calling thread is available from cr_last_error().
+ *   - A context owns its geometry and its work queues and is used from one
+ *     host thread at a time.  Output buffers belong to the caller.
+ *   - Matrices are column-major float[16] (glm layout).
+ *   - The visbuffer holds, per pixel, (bits(depth) & 0x7FFFFFF8) << 33 |
+ *     36-bit global triangle id, reduced with a 64-bit atomic minimum; a
+ *     cleared pixel is 0xFFFFFFF000000000 (src/kernels/rasterization_helpers.cuh:35-66,
+ *     src/kernels/resolve.cu:228).
+ */
+#ifndef CURAST_B200_H
+#define CURAST_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CR_ABI_VERSION 1
+
+typedef enum cr_status {
+    CR_OK = 0,
+    CR_ERR_INVALID = 1,        /* bad argument or handle                         */
+    CR_ERR_OOM = 2,            /* device/host allocation failed or over budget   */
+    CR_ERR_QUEUE_OVERFLOW = 3, /* a stage queue was too small; frame incomplete  */
+    CR_ERR_TIMEOUT = 4,        /* a bounded device-side wait gave up             */
+    CR_ERR_CUDA = 5,           /* CUDA runtime error                             */
+    CR_ERR_BUSY = 6,           /* admission refused for now (memory budget)      */
+    CR_ERR_NOT_FOUND = 7,      /* unknown mesh / ticket                          */
+    CR_ERR_UNSUPPORTED = 8     /* no usable sm_100 device                        */
+} cr_status;
+
+typedef struct cr_context cr_context;
+
+/* Stage thresholds and queue sizes.  The defaults are the reference's
+ * (src/kernels/HostDeviceInterface.h:261-266); the visbuffer depends on
+ * threshold_small / threshold_large, so changing them changes the output. */
+typedef struct cr_config {
+    int32_t device;            /* CUDA device ordinal                              */
+    uint32_t threshold_small;  /* stage 1 -> 2 fragment-box threshold (128)       */
+    uint32_t threshold_large;  /* stage 2 -> 3 fragment threshold (4096)          */
+    uint32_t stage1_warps;     /* warps per stage-1 block (0 = default)           */
+    uint64_t max_nontrivial;   /* stage-2 queue entries (0 = sized per frame)     */
+    uint64_t max_huge;         /* stage-3 tile entries (0 = sized per frame)      */
+    uint64_t memory_budget;    /* bytes the context may allocate (0 = no cap)     */
+    uint32_t grow_on_overflow; /* re-render once with larger queues (default 1)   */
+    uint32_t wait_timeout_ms;  /* bound of every device-side wait (default 1000)  */
+    uint32_t debug_flags;      /* CR_DEBUG_* below; 0 in normal use               */
+    uint32_t reserved[5];
+} cr_config;
+
+/* Failure-detection test hook: stage 1 never issues its first index-tile
+ * copy, so the bounded wait for it runs out; the frame then reports
+ * CR_ERR_TIMEOUT and the context stays usable. */
+#define CR_DEBUG_DROP_FIRST_TILE_COPY 1u
+
+typedef enum cr_memory { CR_MEM_HOST = 0, CR_MEM_DEVICE = 1 } cr_memory;
+
+typedef struct cr_mesh_desc {
+    const float* positions;    /* xyz per vertex (12-byte stride)                  */
+    const uint32_t* indices;   /* 3 per triangle; NULL = vertex 3t+k              */
+    const uint32_t* colors;    /* RGBA8 per vertex; may be NULL                    */
+    uint32_t num_vertices;
+    uint32_t num_triangles;
+    int32_t memory;            /* CR_MEM_HOST: copied; CR_MEM_DEVICE: borrowed    */
+    uint32_t reserved;
+} cr_mesh_desc;
+
+typedef struct cr_instance {
+    uint32_t mesh;             /* handle from cr_mesh_create                       */
+    uint32_t reserved;
+    float world[16];           /* object -> world                                  */
+} cr_instance;
+
+typedef struct cr_camera {
+    float view[16];            /* world -> view                                    */
+    float proj[16];            /* only proj[5] (= f) and proj[0] reach the output  */
+    int32_t width;
+    int32_t height;
+} cr_camera;
+
+typedef enum cr_display {
+    CR_DISPLAY_NONE = 0,          /* DisplayAttribute::NONE: white                 */
+    CR_DISPLAY_VERTEX_COLORS = 4, /* DisplayAttribute::VERTEX_COLORS               */
+    CR_DISPLAY_TRIANGLE_ID = 5    /* DisplayAttribute::TRIANGLE_ID                 */
+} cr_display;
+
+enum cr_render_flags {
+    CR_RENDER_SYNC = 1u << 0,          /* wait for the frame and report overflow   */
+    CR_RENDER_KEEP_ORDER = 1u << 1,    /* do not sort instances (ids follow input) */
+    CR_RENDER_NO_RESOLVE = 1u << 2,    /* visbuffer only                            */
+    CR_RENDER_NO_CLEAR = 1u << 3,      /* accumulate into an existing visbuffer     */
+    CR_RENDER_TIMING = 1u << 4         /* record per-stage device times             */
+};
+
+/* Per-stage device time summed over the frames rendered with
+ * CR_RENDER_TIMING since the last call (waits for them).  ms[0..4]: clear,
+ * stage 1, stage 2, stage 3, resolve.  Returns the frame count in *frames. */
+typedef struct cr_stage_times {
+    float ms[5];
+    uint32_t frames;
+} cr_stage_times;
+
+typedef struct cr_frame_stats {
+    uint64_t nontrivial;       /* triangles queued for stage 2                     */
+    uint64_t huge_tiles;       /* 64x64 tiles queued for stage 3                   */
+    uint64_t overflow;         /* nonzero if a queue overflowed                     */
+    uint64_t instances;
+    uint64_t triangles;        /* triangle x instance work items                   */
+    float ms_total;            /* device time of the last frame (SYNC renders)     */
+    float ms_raster;
+    float ms_resolve;
+    float reserved;
+} cr_frame_stats;
+
+/* ---- context ---------------------------------------------------------- */
+void cr_config_default(cr_config* cfg);
+cr_status cr_create(const cr_config* cfg, cr_context** out);
+cr_status cr_destroy(cr_context* ctx);
+const char* cr_last_error(void);
+int cr_abi_version(void);
+
+/* ---- geometry ----------------------------------------------------------- */
+cr_status cr_mesh_create(cr_context* ctx, const cr_mesh_desc* desc, uint32_t* mesh_out);
+cr_status cr_mesh_destroy(cr_context* ctx, uint32_t mesh);
+/* Device pointers of a mesh's arrays (for callers that share them). */
+cr_status cr_mesh_device_arrays(cr_context* ctx, uint32_t mesh, uint64_t* d_positions,
+                                uint64_t* d_indices, uint64_t* d_colors);
+
+/* ---- frame assembly (host only; CuRast_render.h:337-435) -------------------
+ * Orders instances as the reference does (triangle count descending, then
+ * mesh), groups consecutive instances of one mesh and assigns each instance
+ * its first global triangle id.  order[i] = input index of the i-th
+ * instance in render order; first_id[i] = its first triangle id;
+ * world_view[16*i] = view * world of that instance in glm's float order. */
+cr_status cr_frame_assemble(cr_context* ctx, const cr_instance* instances, uint32_t count,
+                            const float* view, uint32_t flags, uint32_t* order,
+                            uint64_t* first_id, float* world_view);
+
+/* The ordering rule of cr_frame_assemble on plain arrays (no context, no
+ * GPU): mesh[i] and triangles[i] describe instance i. */
+cr_status cr_order_instances(const uint32_t* mesh, const uint32_t* triangles, uint32_t count,
+                             uint32_t flags, uint32_t* order, uint64_t* first_id);
+
+/* ---- rendering ---------------------------------------------------------
+ * Renders one view.  d_visbuffer: W*H uint64; d_rgba: W*H uint32 (may be 0
+ * with CR_RENDER_NO_RESOLVE); d_colorbuffer: optional W*H uint64
+ * (depth << 32 | RGBA8 as the reference's colorbuffer).  stream: a
+ * cudaStream_t (0 = legacy default stream). */
+cr_status cr_render(cr_context* ctx, const cr_instance* instances, uint32_t count,
+                    const cr_camera* camera, uint64_t d_visbuffer, uint64_t d_rgba,
+                    uint64_t d_colorbuffer, int32_t display, uint32_t flags, void* stream);
+
+/* Statistics of the last frame rendered with CR_RENDER_SYNC (or after
+ * cr_sync). */
+cr_status cr_last_frame_stats(cr_context* ctx, cr_frame_stats* out);
+cr_status cr_sync(cr_context* ctx);
+cr_status cr_drain_stage_times(cr_context* ctx, cr_stage_times* out);
+
+/* 4x4 helpers in glm's float operation order (host). */
+void cr_mat4_mul(const float* a, const float* b, float* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CURAST_B200_H */

@@ -1,0 +1,263 @@
+"""GPU parity tests: the CUDA path, called through the C ABI, against the CPU
+oracle and against the reference's own kernels (IEEE-mode build) on the same
+seeded inputs.  Visbuffers must match bit for bit; resolved colours within
+1/255 per channel."""
+import os
+
+import numpy as np
+import pytest
+
+import golden_cases
+import oracle_lib as ol
+import pycurast as pc
+import scenes
+
+pytestmark = pytest.mark.gpu
+CLEAR = pc.CLEAR_PIXEL
+COLOR_TOL = 1  # per 8-bit channel
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def render_ours(ctx, meshes, instances, view, proj, W, H, flags=pc.CR_RENDER_SYNC | pc.CR_RENDER_KEEP_ORDER,
+                display=pc.CR_DISPLAY_VERTEX_COLORS, handles=None):
+    torch = _torch()
+    if handles is None:
+        handles = [ctx.mesh_from_host(p, i, c) for (p, i, c) in meshes]
+    inst = [(handles[m], w) for m, w in instances]
+    vis = torch.empty(W * H, dtype=torch.int64, device="cuda")
+    rgba = torch.empty(W * H, dtype=torch.int32, device="cuda")
+    cb = torch.empty(W * H, dtype=torch.int64, device="cuda")
+    cam = pc.make_camera(view, proj, W, H)
+    ctx.render(inst, cam, vis.data_ptr(), rgba.data_ptr(), cb.data_ptr(), display, flags)
+    torch.cuda.synchronize()
+    st, stats = ctx.stats()
+    assert st == pc.CR_OK
+    return (vis.cpu().numpy().view(np.uint64), rgba.cpu().numpy().view(np.uint32),
+            cb.cpu().numpy().view(np.uint64), stats)
+
+
+def render_oracle(meshes, instances, view, proj, W, H, display=4):
+    items = [(meshes[m][0], meshes[m][1], meshes[m][2], w) for m, w in instances]
+    fr = ol.Frame(items, view)
+    fb, st = ol.raster(fr, W, H, proj[5])
+    cb, rgba = ol.resolve(fr, view, proj, W, H, fb, display=display)
+    return fb, rgba, cb, st
+
+
+_REF = None
+
+
+def reference():
+    global _REF
+    if _REF is None:
+        if not os.path.exists(ol.HARNESS_SO):
+            pytest.skip("reference harness not built")
+        _REF = ol.Reference("ieee")
+    return _REF
+
+
+def render_reference(meshes, instances, view, proj, W, H, instanced=True, cap=1 << 22):
+    ref = reference()
+    ref.reset()
+    hs = [ref.mesh_host(p, i, c) for (p, i, c) in meshes]
+    ids = [hs[m] for m, _ in instances]
+    worlds = np.stack([np.asarray(w, np.float32).reshape(16) for _, w in instances])
+    vis, cb, rgba, ms, counts = ref.frame(ids, worlds, view, proj, W, H, instanced=instanced, display=4,
+                                          cap_nontrivial=cap, cap_huge=cap)
+    return vis, rgba, cb, counts
+
+
+def channel_diff(a, b):
+    a = a.view(np.uint8).reshape(-1, 4).astype(np.int16)
+    b = b.view(np.uint8).reshape(-1, 4).astype(np.int16)
+    return int(np.abs(a - b).max()) if a.size else 0
+
+
+def assert_same_vis(a, b, what):
+    bad = np.nonzero(a != b)[0]
+    assert bad.size == 0, f"{what}: {bad.size} of {a.size} pixels differ; first {bad[:8]}"
+
+
+@pytest.fixture
+def ctx(gpu):
+    c = pc.Context()
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("name", golden_cases.CASES)
+def test_golden_cases(ctx, name):
+    c = golden_cases.case(name)
+    args = (c["meshes"], c["instances"], c["view"], c["proj"], c["W"], c["H"])
+    vis, rgba, cb, stats = render_ours(ctx, *args)
+    ovis, orgba, ocb, ost = render_oracle(*args)
+    assert_same_vis(vis, ovis, "ours vs oracle")
+    assert stats.nontrivial == ost.nontrivial and stats.huge_tiles == ost.huge_tiles
+    assert channel_diff(rgba, orgba) <= COLOR_TOL
+    assert np.array_equal(cb >> np.uint64(32), ocb >> np.uint64(32))  # colorbuffer depth bits
+    rvis, rrgba, rcb, counts = render_reference(*args)
+    assert_same_vis(vis, rvis, "ours vs reference kernels")
+    assert int(counts[0]) == stats.nontrivial and int(counts[1]) == stats.huge_tiles
+    assert channel_diff(rgba, rrgba) <= COLOR_TOL
+    assert np.array_equal(cb >> np.uint64(32), rcb >> np.uint64(32))
+
+
+def test_heightfield_1m_1080p(ctx):
+    """The benchmark scene: 1,048,576 triangles at 1920x1080."""
+    m = scenes.heightfield()
+    view, proj = scenes.heightfield_camera(1920, 1080)
+    args = ([m], [(0, scenes.identity())], view, proj, 1920, 1080)
+    vis, rgba, cb, stats = render_ours(ctx, *args)
+    ovis, orgba, ocb, ost = render_oracle(*args)
+    assert_same_vis(vis, ovis, "ours vs oracle")
+    assert channel_diff(rgba, orgba) <= COLOR_TOL
+    rvis, rrgba, _, counts = render_reference(*args)
+    assert_same_vis(vis, rvis, "ours vs reference kernels")
+    assert channel_diff(rgba, rrgba) <= COLOR_TOL
+    assert (vis != CLEAR).mean() > 0.3
+
+
+@pytest.mark.parametrize("W,H", [(640, 360), (333, 197)])
+def test_soup_all_stages(ctx, W, H):
+    """Sub-pixel to screen-filling and near-plane-crossing triangles; odd sizes."""
+    m = scenes.triangle_soup(60000, seed=101, near_fraction=0.01)
+    view = scenes.identity()
+    proj = scenes.perspective(60.0, W / H)
+    args = ([m], [(0, scenes.identity())], view, proj, W, H)
+    vis, rgba, cb, stats = render_ours(ctx, *args)
+    ovis, orgba, _, ost = render_oracle(*args)
+    assert ost.stage1_direct > 0 and ost.stage2_direct > 0 and ost.huge_tiles > 0
+    assert_same_vis(vis, ovis, "ours vs oracle")
+    assert channel_diff(rgba, orgba) <= COLOR_TOL
+    rvis, _, _, _ = render_reference(*args)
+    assert_same_vis(vis, rvis, "ours vs reference kernels")
+
+
+def test_many_instances_sorted(ctx):
+    """cr_render's own ordering (triangle count, then mesh) with instanced
+    segments and mirrored instances; compared in the order it reports."""
+    rng = np.random.default_rng(9)
+    meshes = [scenes.heightfield(nx=24, nz=12, seed=41), scenes.triangle_soup(300, seed=43),
+              scenes.heightfield(nx=8, nz=8, seed=47)]
+    hs = [ctx.mesh_from_host(p, i, c) for (p, i, c) in meshes]
+    inst = []
+    for k in range(40):
+        mi = int(rng.integers(0, 3))
+        inst.append((mi, scenes.random_affine(rng, pos_box=4.0, smin=0.3, smax=1.2, mirror=(k % 5 == 0))))
+    W, H = 400, 240
+    view = scenes.look_at((2.0, 5.0, 9.0), (2.0, 1.0, 2.0))
+    proj = scenes.perspective(60.0, W / H)
+    order, first, _ = ctx.frame_assemble([(hs[m], w) for m, w in inst], view)
+    vis, rgba, _, stats = render_ours(ctx, meshes, inst, view, proj, W, H, flags=pc.CR_RENDER_SYNC, handles=hs)
+    ordered = [inst[i] for i in order]
+    ovis, orgba, _, _ = render_oracle(meshes, ordered, view, proj, W, H)
+    assert_same_vis(vis, ovis, "ours vs oracle")
+    assert channel_diff(rgba, orgba) <= COLOR_TOL
+    rvis, _, _, _ = render_reference(meshes, ordered, view, proj, W, H, instanced=True)
+    assert_same_vis(vis, rvis, "ours vs reference (instanced stage 1)")
+    rvis2, _, _, _ = render_reference(meshes, ordered, view, proj, W, H, instanced=False)
+    assert_same_vis(vis, rvis2, "ours vs reference (per-instance stage 1)")
+
+
+def test_non_indexed_mesh(ctx):
+    p, _, c = scenes.triangle_soup(5000, seed=55, indexed=False)
+    W, H = 256, 144
+    args = ([(p, None, c)], [(0, scenes.identity())], scenes.identity(), scenes.perspective(60.0, W / H), W, H)
+    vis, rgba, _, _ = render_ours(ctx, *args)
+    ovis, orgba, _, _ = render_oracle(*args)
+    assert_same_vis(vis, ovis, "ours vs oracle")
+    assert channel_diff(rgba, orgba) <= COLOR_TOL
+
+
+def test_borrowed_device_mesh_matches_host_mesh(ctx):
+    torch = _torch()
+    p, i, c = scenes.triangle_soup(8000, seed=61)
+    dp = torch.from_numpy(p.copy()).cuda()
+    di = torch.from_numpy(i.astype(np.int32).copy()).cuda()
+    dc = torch.from_numpy(c.view(np.int32).copy()).cuda()
+    h_dev = ctx.mesh_from_device(dp.data_ptr(), p.shape[0], di.data_ptr(), i.shape[0], dc.data_ptr())
+    h_host = ctx.mesh_from_host(p, i, c)
+    W, H = 320, 200
+    view, proj = scenes.identity(), scenes.perspective(60.0, W / H)
+    a = render_ours(ctx, None, [(0, scenes.identity())], view, proj, W, H, handles=[h_dev])
+    b = render_ours(ctx, None, [(0, scenes.identity())], view, proj, W, H, handles=[h_host])
+    assert_same_vis(a[0], b[0], "device vs host mesh")
+    assert np.array_equal(a[1], b[1])
+
+
+def test_queue_overflow_grows_and_matches(gpu):
+    m = scenes.triangle_soup(20000, seed=71, near_fraction=0.05)
+    W, H = 320, 180
+    args = ([m], [(0, scenes.identity())], scenes.identity(), scenes.perspective(60.0, W / H), W, H)
+    with pc.Context() as big:
+        ref_vis = render_ours(big, *args)[0]
+    with pc.Context(max_nontrivial=16, max_huge=16) as small:
+        vis, _, _, stats = render_ours(small, *args)
+        assert stats.overflow == 0
+        assert_same_vis(vis, ref_vis, "after growing the queues")
+
+
+def test_queue_overflow_reported_when_growth_disabled(gpu):
+    m = scenes.triangle_soup(20000, seed=71, near_fraction=0.05)
+    W, H = 320, 180
+    with pc.Context(max_nontrivial=16, max_huge=16, grow_on_overflow=0) as small:
+        with pytest.raises(pc.CurastError) as e:
+            render_ours(small, [m], [(0, scenes.identity())], scenes.identity(), scenes.perspective(60.0, W / H),
+                        W, H)
+        assert e.value.status == pc.CR_ERR_QUEUE_OVERFLOW
+
+
+def test_empty_frame_clears(ctx):
+    torch = _torch()
+    W, H = 130, 70
+    vis = torch.zeros(W * H, dtype=torch.int64, device="cuda")
+    rgba = torch.zeros(W * H, dtype=torch.int32, device="cuda")
+    cam = pc.make_camera(scenes.identity(), scenes.perspective(60.0, W / H), W, H)
+    ctx.render(pc.make_instances([]), cam, vis.data_ptr(), rgba.data_ptr())
+    torch.cuda.synchronize()
+    assert (vis.cpu().numpy().view(np.uint64) == CLEAR).all()
+
+
+def test_bounded_wait_timeout_is_reported_and_context_survives(gpu):
+    """Failure detection without a GPU fault: the first index-tile copy is
+    never issued, its bounded wait runs out, the frame reports
+    CR_ERR_TIMEOUT, and the next frame on the same context is correct."""
+    torch = _torch()
+    m = scenes.heightfield(nx=64, nz=32, seed=3)
+    W, H = 320, 180
+    view, proj = scenes.heightfield_camera(W, H)
+    with pc.Context(debug_flags=pc.CR_DEBUG_DROP_FIRST_TILE_COPY, wait_timeout_ms=20) as bad:
+        h = bad.mesh_from_host(*m)
+        vis = torch.empty(W * H, dtype=torch.int64, device="cuda")
+        rgba = torch.empty(W * H, dtype=torch.int32, device="cuda")
+        cam = pc.make_camera(view, proj, W, H)
+        st = bad.render_status([(h, scenes.identity())], cam, vis.data_ptr(), rgba.data_ptr())
+        assert st == pc.CR_ERR_TIMEOUT
+    torch.cuda.synchronize()
+    with pc.Context() as good:
+        a = render_ours(good, [m], [(0, scenes.identity())], view, proj, W, H)[0]
+    o = render_oracle([m], [(0, scenes.identity())], view, proj, W, H)[0]
+    assert_same_vis(a, o, "after a timed-out frame")
+
+
+def test_async_render_on_torch_stream(ctx):
+    torch = _torch()
+    m = scenes.heightfield(nx=64, nz=32, seed=3)
+    W, H = 320, 180
+    view, proj = scenes.heightfield_camera(W, H)
+    h = ctx.mesh_from_host(*m)
+    s = torch.cuda.Stream()
+    vis = torch.empty(W * H, dtype=torch.int64, device="cuda")
+    rgba = torch.empty(W * H, dtype=torch.int32, device="cuda")
+    cam = pc.make_camera(view, proj, W, H)
+    for _ in range(3):
+        ctx.render([(h, scenes.identity())], cam, vis.data_ptr(), rgba.data_ptr(), flags=0, stream=s.cuda_stream)
+    ctx.sync()
+    s.synchronize()
+    o = render_oracle([m], [(0, scenes.identity())], view, proj, W, H)[0]
+    assert_same_vis(vis.cpu().numpy().view(np.uint64), o, "async render")
