@@ -48,6 +48,8 @@ def load_peaks():
 # workloads
 # ---------------------------------------------------------------------------
 def build_workload(name):
+    """Seeded synthetic stand-ins for the reference's benchmark scenes.
+    Host workloads hold numpy arrays, device workloads torch CUDA tensors."""
     import scenes
 
     if name == "heightfield_1m_1080p":
@@ -55,17 +57,40 @@ def build_workload(name):
         pos, idx, col = scenes.heightfield()
         view, proj = scenes.heightfield_camera(W, H)
         return dict(name=name, W=W, H=H, meshes=[(pos, idx, col)], instances=[(0, scenes.identity())],
-                    view=view, proj=proj,
+                    view=view, proj=proj, device=False,
                     desc="1024x512-quad displaced heightfield (1,048,576 triangles, 525,825 vertices), 1920x1080")
+    if name.startswith("planet_"):
+        # planet_<N>m_1080p: the dense subdivided-sphere scene with N million triangles
+        count = int(name.split("_")[1].rstrip("m")) * 1_000_000
+        W, H = 1920, 1080
+        pos, idx, col = scenes.planet(count, device="cuda", width=W, height=H)
+        view, proj = scenes.planet_camera(W, H)
+        return dict(name=name, W=W, H=H, meshes=[(pos, idx, col)], instances=[(0, scenes.identity())],
+                    view=view, proj=proj, device=True,
+                    desc=f"seeded displaced icosphere, {count:,} triangles, per-patch subdivision levels giving a "
+                         f"lognormal pre-clip projected-area histogram, 1920x1080")
     raise SystemExit(f"unknown workload {name}")
 
 
 def scene_counts(wl):
-    T = sum(wl["meshes"][m][1].shape[0] if wl["meshes"][m][1] is not None else wl["meshes"][m][0].shape[0] // 3
-            for m, _ in wl["instances"])
+    def ntri(m):
+        p, i, _ = wl["meshes"][m]
+        return i.shape[0] if i is not None else p.shape[0] // 3
+
+    T = sum(ntri(m) for m, _ in wl["instances"])
     V = sum(p.shape[0] for p, _, _ in wl["meshes"])
-    Tunique = sum(i.shape[0] if i is not None else p.shape[0] // 3 for p, i, _ in wl["meshes"])
+    Tunique = sum(ntri(m) for m in range(len(wl["meshes"])))
     return T, V, Tunique
+
+
+def host_mesh(mesh):
+    """numpy (positions, uint32 indices, uint32 colours) of a workload mesh."""
+    p, i, c = mesh
+    if hasattr(p, "cpu"):
+        p = p.cpu().numpy()
+        i = None if i is None else i.cpu().numpy().view(np.uint32)
+        c = None if c is None else c.cpu().numpy().view(np.uint32)
+    return p, i, c
 
 
 # ---------------------------------------------------------------------------
@@ -168,7 +193,7 @@ def cpu_baseline(wl, budget_s=20.0):
     import oracle_lib as ol
 
     ncores = os.cpu_count() or 1
-    pos, idx, col = wl["meshes"][0]
+    pos, idx, col = host_mesh(wl["meshes"][0])
     T = idx.shape[0]
     sample = T
     t_used = 0.0
@@ -206,7 +231,11 @@ def run_ours(args, rank, world, local):
     T, V, Tu = scene_counts(wl)
     W, H = wl["W"], wl["H"]
     ctx = pc.Context(device=local)
-    handles = [ctx.mesh_from_host(p, i, c) for (p, i, c) in wl["meshes"]]
+    if wl["device"]:
+        handles = [ctx.mesh_from_device(p.data_ptr(), p.shape[0], i.data_ptr(), i.shape[0], c.data_ptr())
+                   for (p, i, c) in wl["meshes"]]
+    else:
+        handles = [ctx.mesh_from_host(p, i, c) for (p, i, c) in wl["meshes"]]
     inst = pc.make_instances([(handles[m], w) for m, w in wl["instances"]])
     cam = pc.make_camera(wl["view"], wl["proj"], W, H)
     vis = torch.empty(W * H, dtype=torch.int64, device="cuda")
@@ -323,13 +352,24 @@ def run_reference(args, rank, world, local):
         ref = ol.Reference("native", device=local)
     except Exception as e:  # noqa: BLE001
         return {"impl": "reference", "unavailable": f"reference kernels not loadable: {e}"}
-    ids = [ref.mesh_host(p, i, c) for (p, i, c) in wl["meshes"]]
+    if wl["device"]:
+        ids = [ref.mesh_device(p.data_ptr(), p.shape[0], i.data_ptr(), i.shape[0], c.data_ptr())
+               for (p, i, c) in wl["meshes"]]
+    else:
+        ids = [ref.mesh_host(p, i, c) for (p, i, c) in wl["meshes"]]
     mids = [ids[m] for m, _ in wl["instances"]]
     worlds = np.stack([np.asarray(w, np.float32).reshape(16) for _, w in wl["instances"]])
-    # The reference never checks its queue capacities; give it the exact upper
-    # bound for stage 2 and a wide margin for stage 3.
-    cap_nt = T
-    cap_huge = 1 << 26
+    # The reference never checks its queue capacities: size them from the CPU
+    # oracle's exact counts for this frame, with a wide margin (the fast-math
+    # build decides a handful of edge triangles differently).
+    items = []
+    for m, w in wl["instances"]:
+        p, i, c = host_mesh(wl["meshes"][m])
+        items.append((p, i, c, w))
+    _, ost = ol.raster(ol.Frame(items, wl["view"]), W, H, wl["proj"][5], nthreads=os.cpu_count() or 1)
+    del items
+    cap_nt = min(T, 2 * int(ost.nontrivial) + (1 << 20))
+    cap_huge = 2 * int(ost.huge_tiles) + (1 << 20)
     ref.frame(mids, worlds, wl["view"], wl["proj"], W, H, instanced=True, cap_nontrivial=cap_nt,
               cap_huge=cap_huge, frames=max(args.warmup, 1), want_color=False)
     _, _, _, ms, counts = ref.frame(mids, worlds, wl["view"], wl["proj"], W, H, instanced=True,
@@ -368,7 +408,8 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="heightfield_1m_1080p")
+    ap.add_argument("--workload", default="planet_400m_1080p",
+                    help="planet_400m_1080p (the 400M-triangle dense mesh), planet_<N>m_1080p, heightfield_1m_1080p")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)

@@ -599,6 +599,70 @@ __device__ __forceinline__ int stage2_setup(const CrFrameParams& p, const float 
     return S2_RASTER;
 }
 
+// Narrows one bounding-box row (pixel row py, columns start_x + [0, size_x))
+// to [xlo, xlo + len): every column outside it provably fails the float test
+// of tv.cu:539-547, so skipping it cannot change the visbuffer.
+//
+// With u = 2^-24 and the setup values taken as exact inputs, the float
+// results of
+//     s = (fl(fl(px - asx) + .5) * acy - fl(fl(py - asy) + .5) * acx) * inv_det
+// (and t, v = 1 - (s + t) likewise) differ from the real-valued affine
+// functions S, T, V = 1 - S - T by at most
+//     |s_f - S| <= u |inv_det| (|acy| (5.1|ax| + 2.4) + |acx| (5.1|ay| + 2.4)) * 1.001
+// (ax = px - asx, ay = py - asy; a standard first-order bound on the two
+// roundings of sx, the two products, the difference and the final product),
+// and |v_f - V| <= |s_f - S| + |t_f - T| + 2u (1 + |S| + |T|).  The margins
+// below over-cover these by 3x, in double precision, over the whole row; a
+// column whose S, T or V is below minus its margin cannot pass.  Non-finite
+// setups keep the whole row.
+__device__ __forceinline__ void row_span(float start_x, float py, int size_x, float asx, float asy, float abx,
+                                         float aby, float acx, float acy, float inv_det, int& xlo, int& len) {
+    xlo = 0;
+    len = size_x;
+    const double u = 5.9604644775390625e-08;
+    const double di = (double)inv_det;
+    const double px0 = (double)start_x, px1 = (double)start_x + (double)(size_x - 1);
+    const double c0 = 0.5 - (double)asx;  // sx = px + c0 (exactly, in reals)
+    const double ay = (double)py - (double)asy;
+    const double sy = ay + 0.5;
+    const double AX = fmax(fabs(px0 - (double)asx), fabs(px1 - (double)asx)) + 1.0;
+    const double AY = fabs(ay) + 1.0;
+    const double aS = (double)acy * di, bS = (c0 * (double)acy - sy * (double)acx) * di;
+    const double aT = -(double)aby * di, bT = ((double)abx * sy - (double)aby * c0) * di;
+    const double aV = -(aS + aT), bV = 1.0 - bS - bT;
+    const double Smax = fmax(fabs(aS * px0 + bS), fabs(aS * px1 + bS));
+    const double Tmax = fmax(fabs(aT * px0 + bT), fabs(aT * px1 + bT));
+    const double adi = fabs(di);
+    const double Es = 16.0 * u * adi * (fabs((double)acy) * AX + fabs((double)acx) * AY) + 4.0 * u * Smax + 1e-37;
+    const double Et = 16.0 * u * adi * (fabs((double)abx) * AY + fabs((double)aby) * AX) + 4.0 * u * Tmax + 1e-37;
+    const double Ev = 2.0 * (Es + Et) + 4.0 * u * (Smax + Tmax + 1.0) + 1e-37;
+    double lo = px0, hi = px1;
+    bool empty = false;
+    // keep px with a*px + b >= -E; NaN bounds leave lo/hi unchanged
+    auto keep = [&](double a, double b, double E) {
+        if (a > 0.0) lo = fmax(lo, (-E - b) / a);
+        else if (a < 0.0) hi = fmin(hi, (-E - b) / a);
+        else if (b < -E) empty = true;
+    };
+    keep(aS, bS, Es);
+    keep(aT, bT, Et);
+    keep(aV, bV, Ev);
+    if (empty) {
+        len = 0;
+        return;
+    }
+    double flo = floor(lo - px0) - 1.0;
+    double fhi = ceil(hi - px0) + 1.0;
+    flo = fmax(flo, 0.0);
+    fhi = fmin(fhi, (double)(size_x - 1));
+    if (!(flo <= fhi)) {
+        if (flo > fhi) len = 0;  // NaN keeps the whole row
+        return;
+    }
+    xlo = (int)flo;
+    len = (int)(fhi - flo) + 1;
+}
+
 template <int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) k_stage2(const CrFrameParams p) {
     const int lane = threadIdx.x & 31;
@@ -685,24 +749,55 @@ __global__ void __launch_bounds__(WARPS * 32) k_stage2(const CrFrameParams p) {
             const uint64_t id = (uint64_t)__shfl_sync(FULL, su.id32, j);
             const float start_x = floorf(min_x);
             const float start_y = floorf(min_y);
-            for (int off = lane; off < nf; off += 32) {
-                const int fx = off % size_x;
-                const int fy = off / size_x;
-                const float px = start_x + (float)fx;
-                const float py = start_y + (float)fy;
-                const float sx = px - asx + 0.5f;
-                const float sy = py - asy + 0.5f;
-                const float s = (sx * acy - sy * acx) * inv_det;
-                const float t = (abx * sy - aby * sx) * inv_det;
-                const float v = 1.0f - (s + t);
-                if (s >= 0.0f && t >= 0.0f && v >= 0.0f) {
-                    // The reference only tests pid < W*H and writes negative
-                    // indices in front of the buffer; they are dropped here.
-                    const int pid = (int)px + p.W * (int)py;
-                    if (pid >= 0 && pid < numPixels) {
-                        const float inv_depth = v * iza + s * izb + t * izc;
-                        const float depth = 1.0f / inv_depth;
-                        fb_min(p.fb, (uint32_t)pid, pack_pixel(depth, id));
+            const int size_y = nf / size_x;
+            // The reference tests every fragment of the bounding box.  Here each
+            // row is first narrowed to the columns whose exact float test can
+            // still pass (row_span), the surviving spans of 32 rows are packed
+            // across the lanes, and each fragment then runs the reference's
+            // test unchanged -- so the same fragments are written.
+            for (int r0 = 0; r0 < size_y; r0 += 32) {
+                int xlo = 0, len = 0;
+                if (r0 + lane < size_y)
+                    row_span(start_x, start_y + (float)(r0 + lane), size_x, asx, asy, abx, aby, acx, acy, inv_det,
+                             xlo, len);
+                int incl = len;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const int v = __shfl_up_sync(FULL, incl, d);
+                    if (lane >= d) incl += v;
+                }
+                const int total = __shfl_sync(FULL, incl, 31);
+                for (int base = 0; base < total; base += 32) {
+                    const int k = base + lane;
+                    // first row of the group whose inclusive span sum exceeds k
+                    int r = 0;
+#pragma unroll
+                    for (int step = 16; step >= 1; step >>= 1) {
+                        const int c = __shfl_sync(FULL, incl, r + step - 1);
+                        if (c <= k) r += step;
+                    }
+                    const int rx = __shfl_sync(FULL, xlo, r);
+                    const int rend = __shfl_sync(FULL, incl, r);
+                    const int rlen = __shfl_sync(FULL, len, r);
+                    if (k >= total) continue;
+                    const int fx = rx + (k - (rend - rlen));
+                    const int fy = r0 + r;
+                    const float px = start_x + (float)fx;
+                    const float py = start_y + (float)fy;
+                    const float sx = px - asx + 0.5f;
+                    const float sy = py - asy + 0.5f;
+                    const float s = (sx * acy - sy * acx) * inv_det;
+                    const float t = (abx * sy - aby * sx) * inv_det;
+                    const float v = 1.0f - (s + t);
+                    if (s >= 0.0f && t >= 0.0f && v >= 0.0f) {
+                        // The reference only tests pid < W*H and writes negative
+                        // indices in front of the buffer; they are dropped here.
+                        const int pid = (int)px + p.W * (int)py;
+                        if (pid >= 0 && pid < numPixels) {
+                            const float inv_depth = v * iza + s * izb + t * izc;
+                            const float depth = 1.0f / inv_depth;
+                            fb_min(p.fb, (uint32_t)pid, pack_pixel(depth, id));
+                        }
                     }
                 }
             }

@@ -112,6 +112,173 @@ def heightfield_camera(width=1920, height=1080):
     return view, proj
 
 
+# ---------------------------------------------------------------------------
+# the dense-planet scene: a subdivided icosphere with fractal displacement
+# ---------------------------------------------------------------------------
+def _icosahedron():
+    t = (1 + 5 ** 0.5) / 2
+    v = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t], [0, -1, -t], [0, 1, -t],
+                  [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], np.float64)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    f = np.array([[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4], [11, 10, 2],
+                  [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8], [3, 8, 9], [4, 9, 5], [2, 4, 11],
+                  [6, 2, 10], [8, 6, 7], [9, 8, 1]])
+    return v, f
+
+
+def icosphere_patches(level):
+    """Corners (A, B, C) of the 20*4^level spherical triangles of a subdivided
+    icosahedron, counter-clockwise seen from outside."""
+    v, f = _icosahedron()
+    A, B, C = v[f[:, 0]], v[f[:, 1]], v[f[:, 2]]
+    for _ in range(level):
+        AB = A + B
+        AB /= np.linalg.norm(AB, axis=1, keepdims=True)
+        BC = B + C
+        BC /= np.linalg.norm(BC, axis=1, keepdims=True)
+        CA = C + A
+        CA /= np.linalg.norm(CA, axis=1, keepdims=True)
+        A, B, C = (np.concatenate([A, AB, CA, AB]), np.concatenate([AB, B, BC, BC]), np.concatenate([CA, BC, C, CA]))
+    return A, B, C
+
+
+PLANET = dict(base_level=7, height=0.035, look=(0.0, -0.3, -1.0), sigma=2.5, max_level=14, disp_amp=0.004,
+              fovy=60.0)
+
+
+def _planet_waves(seed):
+    rng = np.random.default_rng(seed + 1000)
+    waves = []
+    for o in range(6):
+        for _ in range(3):
+            d = rng.normal(size=3)
+            d /= np.linalg.norm(d)
+            waves.append((d, float(4 * 2 ** o), float(PLANET["disp_amp"] * 0.55 ** o), float(rng.uniform(0, 2 * np.pi))))
+    return waves
+
+
+def planet_camera(width=1920, height=1080):
+    eye = np.array([0.0, 1.0 + PLANET["height"], 0.0])
+    view = look_at(eye, eye + np.asarray(PLANET["look"]))
+    proj = perspective(PLANET["fovy"], width / height, 0.001, 10.0)
+    return view, proj
+
+
+def _planet_levels(num_triangles, seed, width, height):
+    """Per-patch subdivision levels: each patch's triangles get a projected
+    area drawn from a lognormal around a common median, so the triangle-
+    weighted area histogram is a wide lognormal; the median is solved so the
+    levels hold >= num_triangles triangles."""
+    A, B, C = icosphere_patches(PLANET["base_level"])
+    view = planet_camera(width, height)[0].astype(np.float64).reshape(4, 4)
+    fpx = 1.0 / math.tan(math.radians(PLANET["fovy"] / 2)) * height / 2
+    cen = A + B + C
+    cen /= np.linalg.norm(cen, axis=1, keepdims=True)
+    area_w = 0.5 * np.linalg.norm(np.cross(B - A, C - A), axis=1)
+    vc = cen @ view[:3, :3] + view[3, :3]
+    z = -vc[:, 2]
+    nv = cen @ view[:3, :3]
+    cosang = np.abs(np.einsum("ij,ij->i", nv, vc) / np.linalg.norm(vc, axis=1))
+    scale = area_w * fpx ** 2 * np.maximum(cosang, 0.02) / np.maximum(z, 1e-3) ** 2
+    draw = np.random.default_rng(seed).normal(0.0, PLANET["sigma"], A.shape[0])
+
+    def levels(med):
+        target = np.exp(math.log(med) + draw)
+        L = np.clip(np.round(np.log(np.maximum(scale / target, 1.0)) / math.log(4)), 0, PLANET["max_level"])
+        return np.where(z <= 0.02, 0, L).astype(np.int64)
+
+    lo, hi = 1e-3, 1e6
+    for _ in range(60):
+        mid = math.sqrt(lo * hi)
+        if (4 ** levels(mid)).sum() >= num_triangles:
+            lo = mid
+        else:
+            hi = mid
+    L = levels(lo)
+    order = np.random.default_rng(seed + 1).permutation(A.shape[0])
+    tris = 4 ** L[order]
+    cum = np.cumsum(tris)
+    k = int(np.searchsorted(cum, num_triangles))
+    used = order[:k + 1]
+    ntri = tris[:k + 1].copy()
+    ntri[-1] -= int(cum[k] - num_triangles)  # trim the last patch
+    return A[used], B[used], C[used], L[used], ntri
+
+
+def planet(num_triangles=400_000_000, seed=17, device="cuda", width=1920, height=1080):
+    """Seeded dense planet: base-level-7 icosphere patches each subdivided to
+    its own level (0..14), radially displaced by 18 seeded sine waves over 6
+    octaves (fractal, amplitude 0.004 * 0.55^octave), trimmed to exactly
+    num_triangles triangles.  Returns torch tensors on `device`: positions
+    (V, 3) float32, indices (T, 3) int32 (uint32 bit patterns), colors (V,)
+    int32 (RGBA8 bit patterns)."""
+    import torch
+
+    A, B, C, L, ntri = _planet_levels(num_triangles, seed, width, height)
+    n = 2 ** L
+    nv = (n + 1) * (n + 2) // 2
+    vbase = np.concatenate([[0], np.cumsum(nv)])
+    tbase = np.concatenate([[0], np.cumsum(ntri)])
+    V, T = int(vbase[-1]), int(tbase[-1])
+    dev = lambda a, dt: torch.as_tensor(a, dtype=dt, device=device)  # noqa: E731
+    tA, tB, tC = dev(A, torch.float64), dev(B, torch.float64), dev(C, torch.float64)
+    tm = dev(n, torch.int64)
+    tvb, ttb = dev(vbase, torch.int64), dev(tbase, torch.int64)
+    waves = _planet_waves(seed)
+    pos = torch.empty((V, 3), dtype=torch.float32, device=device)
+    idx = torch.empty((T, 3), dtype=torch.int32, device=device)
+
+    def row_of(k, b):
+        # largest j with (j*b - j*j) / 2 <= k, i.e. the row holding item k of a
+        # triangular layout whose row j holds (b - 1)/2 - j ... items
+        j = torch.floor((b.double() - torch.sqrt(b.double() ** 2 - 8.0 * k.double())) / 2.0).long()
+        j = torch.where((j + 1) * b - (j + 1) * (j + 1) <= 2 * k, j + 1, j)
+        return torch.where(j * b - j * j > 2 * k, j - 1, j)
+
+    def vid(i, j, m):  # vertex (i, j) of a level with m segments, rows by j
+        return j * (m + 1) - (j * (j - 1)) // 2 + i
+
+    chunk = 1 << 24
+    # vertices: flat barycentric grids, one per patch (i + j <= m)
+    for v0 in range(0, V, chunk):
+        g = torch.arange(v0, min(V, v0 + chunk), device=device)
+        p = torch.searchsorted(tvb, g, right=True) - 1
+        m = tm[p]
+        k = g - tvb[p]
+        j = row_of(k, 2 * m + 3)
+        i = k - (j * (2 * m + 3) - j * j) // 2
+        md = m.double()
+        q = tA[p] + (tB[p] - tA[p]) * (i.double() / md)[:, None] + (tC[p] - tA[p]) * (j.double() / md)[:, None]
+        q = (q / torch.linalg.norm(q, dim=1, keepdim=True)).float()
+        r = torch.ones(q.shape[0], dtype=torch.float32, device=device)
+        for d, fr, amp, ph in waves:
+            r += amp * torch.sin(fr * (q[:, 0] * float(d[0]) + q[:, 1] * float(d[1]) + q[:, 2] * float(d[2])) + ph)
+        pos[v0:v0 + q.shape[0]] = q * r[:, None]
+    # triangles: all upward ones row by row, then the downward ones
+    for t0 in range(0, T, chunk):
+        g = torch.arange(t0, min(T, t0 + chunk), device=device)
+        p = torch.searchsorted(ttb, g, right=True) - 1
+        m = tm[p]
+        k = g - ttb[p]
+        nup = m * (m + 1) // 2
+        up = k < nup
+        ku = torch.where(up, k, torch.zeros_like(k))
+        kd = torch.where(up, torch.zeros_like(k), k - nup)
+        ju = row_of(ku, 2 * m + 1)
+        iu = ku - (ju * (2 * m + 1) - ju * ju) // 2
+        jd = row_of(kd, 2 * m - 1)
+        id_ = kd - (jd * (2 * m - 1) - jd * jd) // 2
+        a = torch.where(up, vid(iu, ju, m), vid(id_ + 1, jd, m))
+        b = torch.where(up, vid(iu + 1, ju, m), vid(id_ + 1, jd + 1, m))
+        c = torch.where(up, vid(iu, ju + 1, m), vid(id_, jd + 1, m))
+        base = tvb[p]
+        idx[t0:t0 + g.shape[0]] = (torch.stack([a, b, c], 1) + base[:, None]).to(torch.int32)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    colors = torch.randint(-2**31, 2**31 - 1, (V,), dtype=torch.int32, device=device, generator=g)
+    return pos, idx, colors
+
+
 def triangle_soup(n, seed=7, spread=4.0, near_fraction=0.02, size_sigma=1.5, indexed=True):
     """Random triangles in front of a camera at the origin looking down -z,
     with lognormal sizes so that every stage is exercised: sub-pixel and small

@@ -164,6 +164,53 @@ def test_many_instances_sorted(ctx):
     assert_same_vis(vis, rvis2, "ours vs reference (per-instance stage 1)")
 
 
+@pytest.mark.parametrize("count", [8_000_000, 40_000_000])
+def test_planet_device_mesh(ctx, count):
+    """The dense-planet scene generated in HBM and borrowed by the library:
+    bit-exact against the oracle (and the reference kernels at 8M)."""
+    torch = _torch()
+    pos, idx, col = scenes.planet(count, device="cuda")
+    W, H = 1920, 1080
+    view, proj = scenes.planet_camera(W, H)
+    h = ctx.mesh_from_device(pos.data_ptr(), pos.shape[0], idx.data_ptr(), idx.shape[0], col.data_ptr())
+    vis, rgba, _, stats = render_ours(ctx, None, [(0, scenes.identity())], view, proj, W, H, handles=[h])
+    m = (pos.cpu().numpy(), idx.cpu().numpy().view(np.uint32), col.cpu().numpy().view(np.uint32))
+    del pos, idx, col
+    torch.cuda.empty_cache()
+    ovis, orgba, _, ost = render_oracle([m], [(0, scenes.identity())], view, proj, W, H)
+    assert ost.nontrivial > 0 and ost.huge_tiles > 0
+    assert stats.nontrivial == ost.nontrivial and stats.huge_tiles == ost.huge_tiles
+    assert_same_vis(vis, ovis, "ours vs oracle")
+    assert channel_diff(rgba, orgba) <= COLOR_TOL
+    if count <= 8_000_000:
+        rvis, _, _, counts = render_reference([m], [(0, scenes.identity())], view, proj, W, H,
+                                              cap=2 * int(ost.nontrivial) + 2 * int(ost.huge_tiles) + (1 << 20))
+        assert_same_vis(vis, rvis, "ours vs reference kernels")
+
+
+def test_stage2_span_narrowing_on_slivers(ctx):
+    """Long thin and nearly degenerate triangles, where the rounding of the
+    per-fragment test is largest relative to the triangle: the rows narrowed
+    by the error bound must keep every fragment the full scan would write."""
+    rng = np.random.default_rng(123)
+    n = 20000
+    c = np.stack([rng.uniform(-3, 3, n), rng.uniform(-2, 2, n), -rng.uniform(2, 6, n)], 1)
+    d1 = rng.normal(size=(n, 3)) * rng.uniform(0.2, 1.5, (n, 1))
+    d2 = d1 * (1 + rng.normal(size=(n, 1)) * 10.0 ** rng.uniform(-7, -1, (n, 1))) + rng.normal(size=(n, 3)) * 1e-4
+    tri = np.stack([c, c + d1, c + d2], 1).astype(np.float32)
+    flip = rng.uniform(size=n) < 0.5
+    tri[flip] = tri[flip][:, [0, 2, 1]]
+    pos = tri.reshape(-1, 3)
+    idx = np.arange(pos.shape[0], dtype=np.uint32).reshape(-1, 3)
+    col = rng.integers(0, 2**32, pos.shape[0], dtype=np.uint64).astype(np.uint32)
+    W, H = 800, 600
+    args = ([(pos, idx, col)], [(0, scenes.identity())], scenes.identity(), scenes.perspective(60.0, W / H), W, H)
+    vis, _, _, stats = render_ours(ctx, *args)
+    ovis, _, _, ost = render_oracle(*args)
+    assert ost.stage2_direct > 1000
+    assert_same_vis(vis, ovis, "ours vs oracle")
+
+
 def test_non_indexed_mesh(ctx):
     p, _, c = scenes.triangle_soup(5000, seed=55, indexed=False)
     W, H = 256, 144
