@@ -172,6 +172,17 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 // ---------------------------------------------------------------------------
 enum : int { S1_CULL = 0, S1_DONE = 1, S1_QUEUE = 2 };
 
+// fl(X / d) > 1 for d > 0 without the division.  With round-to-nearest-even,
+// fl(q) > 1 iff q > 1 + 2^-24, i.e. X - d > d * 2^-24.  Outside (d/2, 2d) the
+// answer is plain; inside, X - d is exact (Sterbenz) and d * 2^-24 is exact
+// for d >= 1e-30, so the comparison is exact.  Tiny, huge or NaN d divide.
+__device__ __forceinline__ bool ndc_beyond(float X, float d) {
+    if (!(d >= 1e-30f && d <= 1e30f)) return X / d > 1.0f;
+    if (X >= 2.0f * d) return true;
+    if (X <= 0.5f * d) return false;
+    return (X - d) > d * 5.9604644775390625e-8f;
+}
+
 __device__ __forceinline__ int stage1_triangle(const CrFrameParams& p, const float fa, const Mat& M,
                                                const uint32_t flip, const V3 pa, const V3 pb, const V3 pc,
                                                const uint64_t id) {
@@ -179,18 +190,29 @@ __device__ __forceinline__ int stage1_triangle(const CrFrameParams& p, const flo
     const V3 av = xform(M, pa);
     const V3 bv = xform(M, pb);
     const V3 cv = xform(M, pc);
-    const V3 an = to_ndc(av, fa, f);
-    const V3 bn = to_ndc(bv, fa, f);
-    const V3 cn = to_ndc(cv, fa, f);
-
-    bool nontrivial = (an.z <= 0.0f || bn.z <= 0.0f || cn.z <= 0.0f);
-    if (!nontrivial) {
-        if (an.x > +1.0f && bn.x > +1.0f && cn.x > +1.0f) return S1_CULL;
-        if (an.x < -1.0f && bn.x < -1.0f && cn.x < -1.0f) return S1_CULL;
-        if (an.y > +1.0f && bn.y > +1.0f && cn.y > +1.0f) return S1_CULL;
-        if (an.y < -1.0f && bn.y < -1.0f && cn.y < -1.0f) return S1_CULL;
+    // The reference's culls (all behind, frustum sides, sample miss, back
+    // face) have no side effects, so any order gives the same outcome; the
+    // ones that need no division run first.
+    const float da = -av.z, db = -bv.z, dc = -cv.z;
+    if (da <= 0.0f && db <= 0.0f && dc <= 0.0f) return S1_CULL;  // tv.cu:119
+    {  // tv.cu:168-188
+        const V3 N = cross3(sub3(bv, av), sub3(cv, av));
+        float res = dot3(av, N);
+        if (flip) res = -res;
+        if (res >= 0.0f) return S1_CULL;
     }
-    if (an.z <= 0.0f && bn.z <= 0.0f && cn.z <= 0.0f) return S1_CULL;
+    bool nontrivial = (da <= 0.0f || db <= 0.0f || dc <= 0.0f);
+    const float Xa = fa * av.x, Xb = fa * bv.x, Xc = fa * cv.x;
+    const float Ya = f * av.y, Yb = f * bv.y, Yc = f * cv.y;
+    if (!nontrivial) {  // tv.cu:113-118, on fl(X/d) without dividing
+        if (ndc_beyond(Xa, da) && ndc_beyond(Xb, db) && ndc_beyond(Xc, dc)) return S1_CULL;
+        if (ndc_beyond(-Xa, da) && ndc_beyond(-Xb, db) && ndc_beyond(-Xc, dc)) return S1_CULL;
+        if (ndc_beyond(Ya, da) && ndc_beyond(Yb, db) && ndc_beyond(Yc, dc)) return S1_CULL;
+        if (ndc_beyond(-Ya, da) && ndc_beyond(-Yb, db) && ndc_beyond(-Yc, dc)) return S1_CULL;
+    }
+    const V3 an = {Xa / da, Ya / da, da};  // viewToNDC, helpers:95-101
+    const V3 bn = {Xb / db, Yb / db, db};
+    const V3 cn = {Xc / dc, Yc / dc, dc};
 
     const float Wf = (float)p.W, Hf = (float)p.H;
     V2 as = to_screen(an, Wf, Hf);
@@ -221,13 +243,6 @@ __device__ __forceinline__ int stage1_triangle(const CrFrameParams& p, const flo
     const int size_y = (int)(ceilf(max_y) - ceilf(min_y));
     const uint32_t numFragments = (uint32_t)size_x * (uint32_t)size_y;
     if (numFragments > p.thrSmall) nontrivial = true;
-
-    {  // tv.cu:168-188
-        const V3 N = cross3(sub3(bv, av), sub3(cv, av));
-        float res = dot3(av, N);
-        if (flip) res = -res;
-        if (res >= 0.0f) return S1_CULL;
-    }
     if (nontrivial) return S1_QUEUE;
 
     const V2 v_ab = {bs.x - as.x, bs.y - as.y};
@@ -336,38 +351,50 @@ __global__ void __launch_bounds__(WARPS * 32) k_stage1(const CrFrameParams p) {
 
     const float fa = p.f / p.aspect;
     uint32_t parity = 0;
-    uint32_t k = 0;
-    for (uint64_t item = gw; item < p.numItems; item += nw, ++k) {
+
+    // Fetch of one work item: wait for its index tile (or read the indices
+    // directly), hand the slot to the item S1_STAGES ahead, and issue the
+    // position gathers.  The loop below fetches item k+1 before it processes
+    // item k, so the gathers of the next item overlap this item's math.
+    struct Fetched {
+        uint64_t item;
+        Item it;
+        const CrSegment* sg;
+        uint32_t tri;
+        bool active;
+        V3 pa, pb, pc;
+    };
+    auto fetch = [&](uint64_t item, uint32_t k, Fetched& f) -> bool {
         const int slot = (int)(k & (S1_STAGES - 1));
         const uint32_t bit = 1u << slot;
-        const Item it = decode_item(p, item);
-        const CrSegment* sg = p.segments + it.seg;
-        const uint32_t numTri = __ldg(&sg->numTriangles);
-        const uint32_t tri = it.batch * CR_BATCH + lane;
-        const bool active = tri < numTri;
+        f.item = item;
+        f.it = decode_item(p, item);
+        f.sg = p.segments + f.it.seg;
+        f.tri = f.it.batch * CR_BATCH + lane;
+        f.active = f.tri < __ldg(&f.sg->numTriangles);
         uint32_t i0 = 0, i1 = 0, i2 = 0;
-        if (item_uses_tma(sg, it.batch)) {
+        if (item_uses_tma(f.sg, f.it.batch)) {
             const bool ok =
                 __all_sync(FULL, mbar_wait_bounded(&s_bar[w][slot], (parity & bit) ? 1u : 0u, p.waitTimeoutNs));
-            if (!ok) {  // record, stop this warp, drain its copies below
+            if (!ok) {  // record; the caller stops this warp and drains its copies
                 if (lane == 0) atomicOr(&p.counters[CR_CTR_TIMEOUT], 1ull);
-                break;
+                return false;
             }
             parity ^= bit;
             pending &= ~bit;
             i0 = s_idx[w][slot][3 * lane + 0];
             i1 = s_idx[w][slot][3 * lane + 1];
             i2 = s_idx[w][slot][3 * lane + 2];
-        } else if (active) {
-            const uint32_t* ix = ldg_ptr(&sg->indices);
+        } else if (f.active) {
+            const uint32_t* ix = ldg_ptr(&f.sg->indices);
             if (ix) {
-                i0 = __ldg(ix + 3ull * tri + 0);
-                i1 = __ldg(ix + 3ull * tri + 1);
-                i2 = __ldg(ix + 3ull * tri + 2);
+                i0 = __ldg(ix + 3ull * f.tri + 0);
+                i1 = __ldg(ix + 3ull * f.tri + 1);
+                i2 = __ldg(ix + 3ull * f.tri + 2);
             } else {
-                i0 = 3 * tri + 0;
-                i1 = 3 * tri + 1;
-                i2 = 3 * tri + 2;
+                i0 = 3 * f.tri + 0;
+                i1 = 3 * f.tri + 1;
+                i2 = 3 * f.tri + 2;
             }
         }
         __syncwarp();
@@ -386,14 +413,27 @@ __global__ void __launch_bounds__(WARPS * 32) k_stage1(const CrFrameParams p) {
                 }
             }
         }
-
-        V3 pa = {0, 0, 0}, pb = {0, 0, 0}, pc = {0, 0, 0};
-        if (active) {
-            const float* pos = ldg_ptr(&sg->positions);
-            pa = load_pos(pos, i0);
-            pb = load_pos(pos, i1);
-            pc = load_pos(pos, i2);
+        f.pa = f.pb = f.pc = V3{0.0f, 0.0f, 0.0f};
+        if (f.active) {
+            const float* pos = ldg_ptr(&f.sg->positions);
+            f.pa = load_pos(pos, i0);
+            f.pb = load_pos(pos, i1);
+            f.pc = load_pos(pos, i2);
         }
+        return true;
+    };
+
+    Fetched cur, nxt;
+    uint32_t k = 0;
+    bool ok = gw < p.numItems && fetch(gw, 0, cur);
+    while (ok) {
+        const bool more = cur.item + nw < p.numItems;
+        const bool nextOk = more && fetch(cur.item + nw, k + 1, nxt);
+        const Item it = cur.it;
+        const CrSegment* sg = cur.sg;
+        const uint32_t tri = cur.tri;
+        const bool active = cur.active;
+        const V3 pa = cur.pa, pb = cur.pb, pc = cur.pc;
         const uint32_t first = __ldg(&sg->firstInstance);
         const uint32_t count = __ldg(&sg->instanceCount);
         const uint32_t ib = first + it.chunk * CR_INST_CHUNK;
@@ -416,6 +456,9 @@ __global__ void __launch_bounds__(WARPS * 32) k_stage1(const CrFrameParams p) {
                 }
             }
         }
+        if (!nextOk) break;
+        cur = nxt;
+        ++k;
     }
     // only after a timeout can copies still be in flight: wait for them
     // (bounded) so none lands in shared memory after the block has exited
@@ -672,12 +715,16 @@ __global__ void __launch_bounds__(WARPS * 32) k_stage2(const CrFrameParams p) {
     const float fa = p.f / p.aspect;
     const int numPixels = p.W * p.H;
 
-    for (uint64_t g = gw; g * 32 < count; g += nw) {
-        const uint64_t e = g * 32 + lane;
-        const uint64_t packed = e < count ? p.ntList[e] : 0ull;
+    // group size: 32 queued triangles per warp step when the queue is long,
+    // fewer when it is short so that every warp gets work
+    const uint64_t G = max(1ull, min(32ull, (count + nw - 1) / nw));
+    for (uint64_t g = gw; g * G < count; g += nw) {
+        const uint64_t e = g * G + lane;
+        const bool mine = lane < (int)G && e < count;
+        const uint64_t packed = mine ? p.ntList[e] : 0ull;
         S2Setup su;
         int kind = S2_SKIP;
-        if (e < count) kind = stage2_setup(p, fa, packed, su);
+        if (mine) kind = stage2_setup(p, fa, packed, su);
 
         // ---- tiles: tv.cu:494-514, one atomic per warp --------------------
         int tile_x = 0, tile_y = 0, tiles_x = 1;

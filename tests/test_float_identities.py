@@ -1,0 +1,40 @@
+"""CPU checks of the exact float identities the CUDA kernels rely on to skip
+work without changing results (numpy float32 arithmetic is IEEE-754 with
+round-to-nearest-even, like the kernels built with -fmad=false)."""
+import numpy as np
+
+F32 = np.float32
+
+
+def ndc_beyond(X, d):
+    """Restatement of raster.cu ndc_beyond: fl(X / d) > 1 without dividing."""
+    X, d = F32(X), F32(d)
+    if not (d >= F32(1e-30) and d <= F32(1e30)):
+        return bool(X / d > F32(1.0))
+    if X >= F32(2.0) * d:
+        return True
+    if X <= F32(0.5) * d:
+        return False
+    return bool((X - d) > d * F32(5.9604644775390625e-8))
+
+
+def test_ndc_beyond_matches_division():
+    rng = np.random.default_rng(0)
+    d = (10.0 ** rng.uniform(-29, 29, 200000)).astype(np.float32)
+    # ratios clustered around the rounding boundary 1 + 2^-24 and around 1
+    k = rng.integers(-40, 40, d.size)
+    ratio = 1.0 + k * 2.0 ** -25
+    X = (d.astype(np.float64) * ratio).astype(np.float32)
+    X = np.where(rng.uniform(size=d.size) < 0.1, -X, X)
+    X = np.where(rng.uniform(size=d.size) < 0.05, X * F32(1.9), X)
+    with np.errstate(all="ignore"):
+        want = (X / d) > F32(1.0)
+    got = np.array([ndc_beyond(x, y) for x, y in zip(X, d)])
+    assert np.array_equal(got, want)
+
+
+def test_ndc_beyond_special_values():
+    with np.errstate(all="ignore"):
+        for X in [np.inf, -np.inf, np.nan, 0.0, -0.0, 1e-38, 3e38]:
+            for d in [1e-45, 1e-31, 1e-30, 1.0, 1e30, 2e30, 3e38, np.inf, np.nan]:
+                assert ndc_beyond(X, d) == bool(F32(X) / F32(d) > F32(1.0)), (X, d)
