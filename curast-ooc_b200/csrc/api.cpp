@@ -118,6 +118,8 @@ struct Assembled {
     std::vector<CrSegment> seg;
     uint64_t totalTriangles = 0;
     uint64_t numItems = 0;
+    uint64_t outBytes = 0;     // vertex-pass outcode bytes of all instances
+    uint64_t numVChunks = 0;   // vertex-pass chunks of all instances
 };
 
 }  // namespace
@@ -138,6 +140,8 @@ struct cr_context {
     cudaEvent_t frameDone = nullptr;  // last kernel of the previous frame
 
     // queues
+    uint8_t* outcodes = nullptr;  // vertex-pass output
+    uint64_t outCap = 0;
     uint64_t* ntList = nullptr;
     uint64_t ntCap = 0;
     CrTile* hugeList = nullptr;
@@ -146,7 +150,7 @@ struct cr_context {
     unsigned long long* hCounters = nullptr;  // pinned
 
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
-    // CR_RENDER_TIMING: a ring of event sets (6 per frame) drained on demand
+    // CR_RENDER_TIMING: a ring of event sets (7 per frame) drained on demand
     static constexpr int kRing = 128;
     std::vector<cudaEvent_t> ring;
     int ringHead = 0, ringCount = 0;
@@ -214,6 +218,10 @@ cr_status assemble(cr_context* ctx, const cr_instance* instances, uint32_t count
         ci.cum = sum;
         ci.numTriangles = m.numTriangles;
         ci.numVertices = m.numVertices;
+        ci.outBase = A.outBytes;
+        ci.vchunkBase = A.numVChunks;
+        A.outBytes += align_up(m.numVertices, 16);
+        A.numVChunks += (m.numVertices + CR_VCHUNK - 1) / CR_VCHUNK;
         float* wv = &A.worldView[16ull * r];
         mat4_mul(view, in.world, wv);  // CuRast_render.h:409
         ci.flip = det3_glm(wv) < 0.0f ? 1u : 0u;
@@ -308,6 +316,7 @@ cr_status upload_frame(cr_context* ctx, const Assembled& A, cudaStream_t stream,
     fp.numInstances = (uint32_t)n;
     fp.numSegments = (uint32_t)m;
     fp.numItems = A.numItems;
+    fp.numVChunks = A.numVChunks;
     rp.instances = fp.instances;
     rp.world = fp.world;
     rp.numInstances = (uint32_t)n;
@@ -399,6 +408,7 @@ cr_status cr_destroy(cr_context* ctx) {
             cudaFree(m.indices);
             cudaFree(m.colors);
         }
+    if (ctx->outcodes) cudaFree(ctx->outcodes);
     if (ctx->ntList) cudaFree(ctx->ntList);
     if (ctx->hugeList) cudaFree(ctx->hugeList);
     if (ctx->counters) cudaFree(ctx->counters);
@@ -545,12 +555,23 @@ cr_status cr_render(cr_context* ctx, const cr_instance* instances, uint32_t coun
     CR_CUDA(cudaStreamWaitEvent(stream, ctx->frameDone, 0), "stream wait");
     const uint64_t numPixels = (uint64_t)cam->width * (uint64_t)cam->height;
 
+    if (A.outBytes > ctx->outCap) {  // vertex-pass outcodes: one byte per (instance, vertex)
+        CR_CUDA(cudaDeviceSynchronize(), "outcode resize");
+        ctx->dev_free(ctx->outcodes, ctx->outCap);
+        ctx->outcodes = nullptr;
+        ctx->outCap = 0;
+        const uint64_t want = A.outBytes + A.outBytes / 8;
+        s = ctx->dev_alloc((void**)&ctx->outcodes, want, "vertex outcodes");
+        if (s) return s;
+        ctx->outCap = want;
+    }
     CrFrameParams fp{};
     CrResolveParams rp{};
     if (count) {
         s = upload_frame(ctx, A, stream, fp, rp);
         if (s) return s;
     }
+    fp.outcodes = ctx->outcodes;
     fp.fb = (uint64_t*)d_visbuffer;
     fp.W = cam->width;
     fp.H = cam->height;
@@ -584,7 +605,7 @@ cr_status cr_render(cr_context* ctx, const cr_instance* instances, uint32_t coun
         cudaEvent_t* tev = nullptr;  // 6 timing events of this frame, or none
         if (flags & CR_RENDER_TIMING) {
             if (ctx->ring.empty()) {
-                ctx->ring.resize(6 * cr_context::kRing, nullptr);
+                ctx->ring.resize(7 * cr_context::kRing, nullptr);
                 for (cudaEvent_t& e : ctx->ring) CR_CUDA(cudaEventCreate(&e), "timing events");
             }
             if (ctx->ringCount == cr_context::kRing) {  // full: fold the oldest frame first
@@ -592,7 +613,7 @@ cr_status cr_render(cr_context* ctx, const cr_instance* instances, uint32_t coun
                 cr_status ds = cr_drain_stage_times(ctx, &tmp);
                 if (ds) return ds;
             }
-            tev = &ctx->ring[6 * ((ctx->ringHead + ctx->ringCount) % cr_context::kRing)];
+            tev = &ctx->ring[7 * ((ctx->ringHead + ctx->ringCount) % cr_context::kRing)];
             ctx->ringCount++;
         }
         auto mark = [&](int i) -> cudaError_t { return tev ? cudaEventRecord(tev[i], stream) : cudaSuccess; };
@@ -604,19 +625,22 @@ cr_status cr_render(cr_context* ctx, const cr_instance* instances, uint32_t coun
             return fail(CR_ERR_CUDA, "clear launch: %s", cudaGetErrorString(cudaGetLastError()));
         }
         CR_CUDA(mark(1), "event");
+        if (count && cr_launch_vertex(fp, ctx->shape, stream))
+            return fail(CR_ERR_CUDA, "vertex-pass launch: %s", cudaGetErrorString(cudaGetLastError()));
+        CR_CUDA(mark(2), "event");
         if (count && cr_launch_stage1(fp, ctx->shape, stream))
             return fail(CR_ERR_CUDA, "stage-1 launch: %s", cudaGetErrorString(cudaGetLastError()));
-        CR_CUDA(mark(2), "event");
+        CR_CUDA(mark(3), "event");
         if (count && cr_launch_stage2(fp, ctx->shape, stream))
             return fail(CR_ERR_CUDA, "stage-2 launch: %s", cudaGetErrorString(cudaGetLastError()));
-        CR_CUDA(mark(3), "event");
+        CR_CUDA(mark(4), "event");
         if (count && cr_launch_stage3(fp, ctx->shape, stream))
             return fail(CR_ERR_CUDA, "stage-3 launch: %s", cudaGetErrorString(cudaGetLastError()));
-        CR_CUDA(mark(4), "event");
+        CR_CUDA(mark(5), "event");
         if (sync) CR_CUDA(cudaEventRecord(ctx->ev[1], stream), "event");
         if (!(flags & CR_RENDER_NO_RESOLVE) && count && cr_launch_resolve(rp, stream))
             return fail(CR_ERR_CUDA, "resolve launch: %s", cudaGetErrorString(cudaGetLastError()));
-        CR_CUDA(mark(5), "event");
+        CR_CUDA(mark(6), "event");
         CR_CUDA(cudaMemcpyAsync(ctx->hCounters, ctx->counters, CR_CTR_COUNT * sizeof(unsigned long long),
                                 cudaMemcpyDeviceToHost, stream),
                 "counters readback");
@@ -674,9 +698,9 @@ cr_status cr_drain_stage_times(cr_context* ctx, cr_stage_times* out) {
     memset(out, 0, sizeof(*out));
     CR_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
     while (ctx->ringCount > 0) {
-        cudaEvent_t* e = &ctx->ring[6 * ctx->ringHead];
-        CR_CUDA(cudaEventSynchronize(e[5]), "timing sync");
-        for (int i = 0; i < 5; i++) {
+        cudaEvent_t* e = &ctx->ring[7 * ctx->ringHead];
+        CR_CUDA(cudaEventSynchronize(e[6]), "timing sync");
+        for (int i = 0; i < 6; i++) {
             float ms = 0.0f;
             CR_CUDA(cudaEventElapsedTime(&ms, e[i], e[i + 1]), "timing");
             out->ms[i] += ms;

@@ -14,7 +14,7 @@
 #include <cstdint>
 
 #define CR_TILE_SIZE 64         // HostDeviceInterface.h:261
-#define CR_BATCH 32             // triangles per stage-1 warp item
+#define CR_BATCH 128            // triangles per stage-1 warp item (4 per lane)
 #define CR_INST_CHUNK 16        // instances per stage-1 warp item
 
 // counters[] slots
@@ -33,8 +33,20 @@ struct alignas(16) CrInstance {
     uint32_t flip;              // det(world_view 3x3) < 0, tv.cu:179-185
     uint32_t numVertices;
     uint32_t pad0;
-    uint64_t pad1[2];
+    uint64_t outBase;           // first outcode byte of this instance
+    uint64_t vchunkBase;        // first vertex-pass chunk of this instance
 };
+
+// Per-(instance, vertex) outcode bits written by the vertex pass.  They are
+// the reference's per-vertex frustum predicates on fl(X / depth), evaluated
+// exactly without dividing.
+#define CR_OC_BEHIND 1u         // depth <= 0                      (tv.cu:110,119)
+#define CR_OC_RIGHT 2u          // ndc.x > +1                      (tv.cu:114)
+#define CR_OC_LEFT 4u           // ndc.x < -1                      (tv.cu:115)
+#define CR_OC_TOP 8u            // ndc.y > +1                      (tv.cu:116)
+#define CR_OC_BOTTOM 16u        // ndc.y < -1                      (tv.cu:117)
+#define CR_OC_SIDES 30u
+#define CR_VCHUNK 1024          // vertices per vertex-pass chunk
 static_assert(sizeof(CrInstance) == 64, "CrInstance layout");
 
 struct alignas(16) CrSegment {
@@ -78,6 +90,8 @@ struct CrFrameParams {
     uint64_t waitTimeoutNs;     // bound of every device-side wait
     uint32_t debugFlags;        // CR_DEBUG_* (failure-detection tests)
     uint32_t pad;
+    uint8_t* outcodes;          // vertex-pass output, CrInstance::outBase + vertex
+    uint64_t numVChunks;        // vertex-pass chunks of all instances
 };
 
 struct CrResolveParams {
@@ -98,6 +112,7 @@ struct CrResolveParams {
 // Launch helpers implemented in raster.cu / resolve.cu.
 struct CrLaunchShape {
     int numSMs;
+    int vertexBlocks;
     int stage1Blocks;
     int stage2Blocks;
     int stage3Blocks;
@@ -105,6 +120,7 @@ struct CrLaunchShape {
 
 int cr_query_launch_shape(int device, CrLaunchShape* out);
 int cr_launch_clear(uint64_t* fb, uint64_t numPixels, unsigned long long* counters, void* stream);
+int cr_launch_vertex(const CrFrameParams& p, const CrLaunchShape& s, void* stream);
 int cr_launch_stage1(const CrFrameParams& p, const CrLaunchShape& s, void* stream);
 int cr_launch_stage2(const CrFrameParams& p, const CrLaunchShape& s, void* stream);
 int cr_launch_stage3(const CrFrameParams& p, const CrLaunchShape& s, void* stream);

@@ -11,11 +11,15 @@
 // the reference's work freely and still match it bit for bit.
 //
 // Work decomposition (differs from the reference, same fragment set):
-//   stage 1  persistent warps; a work item is 32 consecutive triangles of one
-//            mesh x up to 16 of its instances.  The item's 384-byte index tile
-//            is fetched by a 1D bulk TMA copy (cp.async.bulk) into a 4-deep
-//            per-warp shared-memory ring, signalled by an mbarrier, so index
-//            loads are coalesced 384-byte bursts issued ahead of use.
+//   vertex   one thread per (instance, vertex): transform + exact per-vertex
+//            cull predicates (behind / beyond each frustum side) into a byte.
+//   stage 1  persistent warps; a work item is 128 consecutive triangles of
+//            one mesh x up to 16 of its instances.  The item's 1536-byte index
+//            tile is fetched by a 1D bulk TMA copy (cp.async.bulk) into a
+//            4-deep per-warp shared-memory ring, signalled by an mbarrier, so
+//            index loads are coalesced bursts issued ahead of use.  Triangles
+//            whose three outcodes prove them culled stop there; survivors are
+//            packed across the lanes and run the reference's full path.
 //            Nontrivial triangles are appended with one atomic per warp
 //            (ballot / popc).                         reference: tv.cu:274-384
 //   stage 2  persistent warps; every lane sets up one queued triangle at once
@@ -285,6 +289,46 @@ __device__ __forceinline__ int stage1_triangle(const CrFrameParams& p, const flo
     return S1_DONE;
 }
 
+// ---------------------------------------------------------------------------
+// Vertex pass: one thread per (instance, vertex).  It evaluates the per-vertex
+// halves of stage 1's culls -- "behind the camera" and the four frustum sides
+// on fl(X / depth), the latter exactly without dividing -- into one byte, so
+// stage 1 can drop the (typically many) triangles all of whose vertices lie
+// behind one side from three gathered bytes, without fetching positions.
+// The transform is stage 1's own (same function, same M), so the predicates
+// are bit-identical to the ones the reference evaluates per triangle.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t vertex_outcode(const Mat& M, V3 p, float fa, float f) {
+    const V3 q = xform(M, p);
+    const float d = -q.z;
+    if (d <= 0.0f) return CR_OC_BEHIND;
+    const float X = fa * q.x, Y = f * q.y;
+    return (ndc_beyond(X, d) ? CR_OC_RIGHT : 0u) | (ndc_beyond(-X, d) ? CR_OC_LEFT : 0u) |
+           (ndc_beyond(Y, d) ? CR_OC_TOP : 0u) | (ndc_beyond(-Y, d) ? CR_OC_BOTTOM : 0u);
+}
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) k_vertex(const CrFrameParams p) {
+    const float fa = p.f / p.aspect;
+    for (uint64_t c = blockIdx.x; c < p.numVChunks; c += gridDim.x) {
+        uint32_t lo = 0, hi = p.numInstances - 1;  // instance holding chunk c
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (__ldg(&p.instances[mid].vchunkBase) <= c) lo = mid;
+            else hi = mid - 1;
+        }
+        const CrInstance* I = p.instances + lo;
+        const uint32_t v0 = (uint32_t)(c - __ldg(&I->vchunkBase)) * CR_VCHUNK;
+        const uint32_t nV = __ldg(&I->numVertices);
+        const uint32_t v1 = min(v0 + (uint32_t)CR_VCHUNK, nV);
+        const float* pos = ldg_ptr(&I->positions);
+        uint8_t* out = p.outcodes + __ldg(&I->outBase);
+        const Mat M = load_mat(p.world_view + 4ull * lo);
+        for (uint32_t v = v0 + threadIdx.x; v < v1; v += THREADS)
+            out[v] = (uint8_t)vertex_outcode(M, load_pos(pos, v), fa, p.f);
+    }
+}
+
 struct Item {
     uint32_t seg;
     uint32_t batch;
@@ -302,8 +346,16 @@ __device__ __forceinline__ Item decode_item(const CrFrameParams& p, uint64_t ite
     it.seg = lo;
     const uint64_t rem = item - __ldg(&p.segments[lo].itemBase);
     const uint32_t nb = __ldg(&p.segments[lo].numBatches);
-    it.chunk = (uint32_t)(rem / nb);
-    it.batch = (uint32_t)(rem - (uint64_t)it.chunk * nb);
+    if (rem < nb) {  // first (often only) instance chunk: no division
+        it.chunk = 0;
+        it.batch = (uint32_t)rem;
+    } else if (rem <= 0xffffffffull) {
+        it.chunk = (uint32_t)rem / nb;
+        it.batch = (uint32_t)rem - it.chunk * nb;
+    } else {
+        it.chunk = (uint32_t)(rem / nb);
+        it.batch = (uint32_t)(rem - (uint64_t)it.chunk * nb);
+    }
     return it;
 }
 
@@ -313,12 +365,21 @@ __device__ __forceinline__ bool item_uses_tma(const CrSegment* sg, uint32_t batc
     return (__ldg(&sg->flags) & 1u) && (uint64_t)(batch + 1) * CR_BATCH <= __ldg(&sg->numTriangles);
 }
 
-constexpr int S1_STAGES = 4;
+constexpr int S1_STAGES = 3;
+constexpr int S1_R = CR_BATCH / 32;  // triangles per lane per work item
 
+// A work item is CR_BATCH (128) consecutive triangles of one mesh x up to
+// CR_INST_CHUNK of its instances.  Per item a warp: waits for the item's
+// 1536-byte index tile (TMA ring), gathers the 3 x 4 vertex outcodes of its
+// four triangles per lane at once, culls all-behind / all-beyond-one-side
+// triangles from them, packs the survivors across the lanes and runs the
+// reference's full per-triangle path (stage1_triangle) on those, then hands
+// the ring slot to the item S1_STAGES ahead.
 template <int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) k_stage1(const CrFrameParams p) {
+__global__ void __launch_bounds__(WARPS * 32, 3) k_stage1(const CrFrameParams p) {
     __shared__ __align__(128) uint32_t s_idx[WARPS][S1_STAGES][CR_BATCH * 3];
     __shared__ __align__(8) uint64_t s_bar[WARPS][S1_STAGES];
+    __shared__ uint8_t s_surv[WARPS][CR_BATCH];
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
     const uint64_t gw = (uint64_t)blockIdx.x * WARPS + w;
@@ -351,54 +412,104 @@ __global__ void __launch_bounds__(WARPS * 32) k_stage1(const CrFrameParams p) {
 
     const float fa = p.f / p.aspect;
     uint32_t parity = 0;
-
-    // Fetch of one work item: wait for its index tile (or read the indices
-    // directly), hand the slot to the item S1_STAGES ahead, and issue the
-    // position gathers.  The loop below fetches item k+1 before it processes
-    // item k, so the gathers of the next item overlap this item's math.
-    struct Fetched {
-        uint64_t item;
-        Item it;
-        const CrSegment* sg;
-        uint32_t tri;
-        bool active;
-        V3 pa, pb, pc;
-    };
-    auto fetch = [&](uint64_t item, uint32_t k, Fetched& f) -> bool {
-        const int slot = (int)(k & (S1_STAGES - 1));
+    uint32_t k = 0;
+    for (uint64_t item = gw; item < p.numItems; item += nw, ++k) {
+        const int slot = (int)(k % S1_STAGES);
         const uint32_t bit = 1u << slot;
-        f.item = item;
-        f.it = decode_item(p, item);
-        f.sg = p.segments + f.it.seg;
-        f.tri = f.it.batch * CR_BATCH + lane;
-        f.active = f.tri < __ldg(&f.sg->numTriangles);
-        uint32_t i0 = 0, i1 = 0, i2 = 0;
-        if (item_uses_tma(f.sg, f.it.batch)) {
+        const Item it = decode_item(p, item);
+        const CrSegment* sg = p.segments + it.seg;
+        const uint32_t numTri = __ldg(&sg->numTriangles);
+        const uint32_t* gix = ldg_ptr(&sg->indices);
+        const bool tma = item_uses_tma(sg, it.batch);
+        const uint32_t tri0 = it.batch * CR_BATCH;
+        if (tma) {
             const bool ok =
                 __all_sync(FULL, mbar_wait_bounded(&s_bar[w][slot], (parity & bit) ? 1u : 0u, p.waitTimeoutNs));
-            if (!ok) {  // record; the caller stops this warp and drains its copies
+            if (!ok) {  // record, stop this warp, drain its copies below
                 if (lane == 0) atomicOr(&p.counters[CR_CTR_TIMEOUT], 1ull);
-                return false;
+                break;
             }
             parity ^= bit;
             pending &= ~bit;
-            i0 = s_idx[w][slot][3 * lane + 0];
-            i1 = s_idx[w][slot][3 * lane + 1];
-            i2 = s_idx[w][slot][3 * lane + 2];
-        } else if (f.active) {
-            const uint32_t* ix = ldg_ptr(&f.sg->indices);
-            if (ix) {
-                i0 = __ldg(ix + 3ull * f.tri + 0);
-                i1 = __ldg(ix + 3ull * f.tri + 1);
-                i2 = __ldg(ix + 3ull * f.tri + 2);
-            } else {
-                i0 = 3 * f.tri + 0;
-                i1 = 3 * f.tri + 1;
-                i2 = 3 * f.tri + 2;
-            }
         }
+        // vertex indices of this lane's triangles (tile position r*32 + lane)
+        auto index_of = [&](uint32_t pos, int c) -> uint32_t {
+            if (tma) return s_idx[w][slot][3 * pos + c];
+            const uint32_t t = tri0 + pos;
+            return gix ? __ldg(gix + 3ull * t + c) : 3 * t + c;
+        };
+        uint32_t ix[S1_R][3];
+        bool act[S1_R];
+#pragma unroll
+        for (int r = 0; r < S1_R; ++r) {
+            const uint32_t pos = r * 32 + lane;
+            act[r] = tri0 + pos < numTri;
+            ix[r][0] = act[r] ? index_of(pos, 0) : 0;
+            ix[r][1] = act[r] ? index_of(pos, 1) : 0;
+            ix[r][2] = act[r] ? index_of(pos, 2) : 0;
+        }
+
+        const uint32_t first = __ldg(&sg->firstInstance);
+        const uint32_t count = __ldg(&sg->instanceCount);
+        const uint32_t ib = first + it.chunk * CR_INST_CHUNK;
+        const uint32_t ie = min(ib + CR_INST_CHUNK, first + count);
+        for (uint32_t inst = ib; inst < ie; ++inst) {
+            const uint8_t* oc = p.outcodes + __ldg(&p.instances[inst].outBase);
+            uint32_t o[S1_R][3];
+#pragma unroll
+            for (int r = 0; r < S1_R; ++r) {
+                o[r][0] = act[r] ? __ldg(oc + ix[r][0]) : 0u;
+                o[r][1] = act[r] ? __ldg(oc + ix[r][1]) : 0u;
+                o[r][2] = act[r] ? __ldg(oc + ix[r][2]) : 0u;
+            }
+            // all behind (tv.cu:119) or all beyond one side with none behind
+            // (tv.cu:110-118): culled from the outcodes alone
+            int nsurv = 0;
+#pragma unroll
+            for (int r = 0; r < S1_R; ++r) {
+                const uint32_t all = o[r][0] & o[r][1] & o[r][2];
+                const uint32_t any = o[r][0] | o[r][1] | o[r][2];
+                const bool culled = (all & CR_OC_BEHIND) || (!(any & CR_OC_BEHIND) && (all & CR_OC_SIDES));
+                const unsigned m = __ballot_sync(FULL, act[r] && !culled);
+                if (act[r] && !culled) s_surv[w][nsurv + __popc(m & ((1u << lane) - 1u))] = (uint8_t)(r * 32 + lane);
+                nsurv += __popc(m);
+            }
+            __syncwarp();
+            if (nsurv == 0) continue;
+            const Mat M = load_mat(p.world_view + 4ull * inst);
+            const uint32_t flip = __ldg(&p.instances[inst].flip);
+            const uint64_t cum = __ldg(&p.instances[inst].cum);
+            const float* pos = ldg_ptr(&sg->positions);
+            for (int base = 0; base < nsurv; base += 32) {
+                const int j = base + lane;
+                int res = S1_CULL;
+                uint32_t tri = 0;
+                if (j < nsurv) {
+                    const uint32_t tp = s_surv[w][j];
+                    tri = tri0 + tp;
+                    const V3 pa = load_pos(pos, index_of(tp, 0));
+                    const V3 pb = load_pos(pos, index_of(tp, 1));
+                    const V3 pc = load_pos(pos, index_of(tp, 2));
+                    res = stage1_triangle(p, fa, M, flip, pa, pb, pc, cum + tri);
+                }
+                const unsigned qmask = __ballot_sync(FULL, res == S1_QUEUE);
+                if (qmask) {  // warp-aggregated append, tv.cu:190-197
+                    const int leader = __ffs(qmask) - 1;
+                    unsigned long long b = 0;
+                    if (lane == leader) b = atomicAdd(&p.counters[CR_CTR_NONTRIVIAL], (unsigned long long)__popc(qmask));
+                    b = __shfl_sync(FULL, b, leader);
+                    if (res == S1_QUEUE) {
+                        const uint64_t q = b + __popc(qmask & ((1u << lane) - 1u));
+                        if (q < p.ntCap) p.ntList[q] = ((uint64_t)inst << 32) | (uint64_t)tri;
+                        else atomicOr(&p.counters[CR_CTR_OVERFLOW], 1ull);
+                    }
+                }
+            }
+            __syncwarp();
+        }
+
         __syncwarp();
-        {  // refill this slot with the item S1_STAGES ahead
+        {  // every read of this slot is done: refill it with the item S1_STAGES ahead
             const uint64_t nxt = item + (uint64_t)S1_STAGES * nw;
             if (nxt < p.numItems) {
                 const Item nt = decode_item(p, nxt);
@@ -413,52 +524,6 @@ __global__ void __launch_bounds__(WARPS * 32) k_stage1(const CrFrameParams p) {
                 }
             }
         }
-        f.pa = f.pb = f.pc = V3{0.0f, 0.0f, 0.0f};
-        if (f.active) {
-            const float* pos = ldg_ptr(&f.sg->positions);
-            f.pa = load_pos(pos, i0);
-            f.pb = load_pos(pos, i1);
-            f.pc = load_pos(pos, i2);
-        }
-        return true;
-    };
-
-    Fetched cur, nxt;
-    uint32_t k = 0;
-    bool ok = gw < p.numItems && fetch(gw, 0, cur);
-    while (ok) {
-        const bool more = cur.item + nw < p.numItems;
-        const bool nextOk = more && fetch(cur.item + nw, k + 1, nxt);
-        const Item it = cur.it;
-        const CrSegment* sg = cur.sg;
-        const uint32_t tri = cur.tri;
-        const bool active = cur.active;
-        const V3 pa = cur.pa, pb = cur.pb, pc = cur.pc;
-        const uint32_t first = __ldg(&sg->firstInstance);
-        const uint32_t count = __ldg(&sg->instanceCount);
-        const uint32_t ib = first + it.chunk * CR_INST_CHUNK;
-        const uint32_t ie = min(ib + CR_INST_CHUNK, first + count);
-        for (uint32_t inst = ib; inst < ie; ++inst) {
-            const Mat M = load_mat(p.world_view + 4ull * inst);
-            const uint32_t flip = __ldg(&p.instances[inst].flip);
-            const uint64_t cum = __ldg(&p.instances[inst].cum);
-            const int r = active ? stage1_triangle(p, fa, M, flip, pa, pb, pc, cum + tri) : S1_CULL;
-            const unsigned qmask = __ballot_sync(FULL, r == S1_QUEUE);
-            if (qmask) {  // warp-aggregated append, tv.cu:190-197
-                const int leader = __ffs(qmask) - 1;
-                unsigned long long base = 0;
-                if (lane == leader) base = atomicAdd(&p.counters[CR_CTR_NONTRIVIAL], (unsigned long long)__popc(qmask));
-                base = __shfl_sync(FULL, base, leader);
-                if (r == S1_QUEUE) {
-                    const uint64_t pos = base + __popc(qmask & ((1u << lane) - 1u));
-                    if (pos < p.ntCap) p.ntList[pos] = ((uint64_t)inst << 32) | (uint64_t)tri;
-                    else atomicOr(&p.counters[CR_CTR_OVERFLOW], 1ull);
-                }
-            }
-        }
-        if (!nextOk) break;
-        cur = nxt;
-        ++k;
     }
     // only after a timeout can copies still be in flight: wait for them
     // (bounded) so none lands in shared memory after the block has exited
@@ -717,7 +782,8 @@ __global__ void __launch_bounds__(WARPS * 32) k_stage2(const CrFrameParams p) {
 
     // group size: 32 queued triangles per warp step when the queue is long,
     // fewer when it is short so that every warp gets work
-    const uint64_t G = max(1ull, min(32ull, (count + nw - 1) / nw));
+    uint64_t G = (count + nw - 1) / nw;
+    G = G < 1 ? 1 : (G > 32 ? 32 : G);
     for (uint64_t g = gw; g * G < count; g += nw) {
         const uint64_t e = g * G + lane;
         const bool mine = lane < (int)G && e < count;
@@ -956,13 +1022,17 @@ __global__ void __launch_bounds__(256) k_clear(uint64_t* fb, uint64_t n, unsigne
 constexpr int S1_WARPS = 8;
 constexpr int S2_WARPS = 8;
 constexpr int S3_WARPS = 8;
+constexpr int VX_THREADS = 256;
 
 int cr_query_launch_shape(int device, CrLaunchShape* out) {
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return -1;
-    int b1 = 0, b2 = 0, b3 = 0;
+    int b1 = 0, b2 = 0, b3 = 0, bv = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_stage1<S1_WARPS>, S1_WARPS * 32, 0) != cudaSuccess)
         return -1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bv, k_vertex<VX_THREADS>, VX_THREADS, 0) != cudaSuccess)
+        return -1;
+    out->vertexBlocks = sms * (bv > 0 ? bv : 1);
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_stage2<S2_WARPS>, S2_WARPS * 32, 0) != cudaSuccess)
         return -1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b3, k_stage3<S3_WARPS>, S3_WARPS * 32, 0) != cudaSuccess)
@@ -978,6 +1048,14 @@ int cr_launch_clear(uint64_t* fb, uint64_t numPixels, unsigned long long* counte
     const uint64_t want = (numPixels / 2 + 255) / 256;
     const unsigned grid = (unsigned)(want < 1 ? 1 : (want > 148 * 16 ? 148 * 16 : want));
     k_clear<<<grid, 256, 0, (cudaStream_t)stream>>>(fb, numPixels, counters);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int cr_launch_vertex(const CrFrameParams& p, const CrLaunchShape& s, void* stream) {
+    if (p.numVChunks == 0) return 0;
+    uint64_t blocks = p.numVChunks;
+    if (blocks > (uint64_t)s.vertexBlocks) blocks = (uint64_t)s.vertexBlocks;
+    k_vertex<VX_THREADS><<<(unsigned)blocks, VX_THREADS, 0, (cudaStream_t)stream>>>(p);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

@@ -36,7 +36,7 @@ CR_RENDER_KEEP_ORDER = 1 << 1
 CR_RENDER_NO_RESOLVE = 1 << 2
 CR_RENDER_NO_CLEAR = 1 << 3
 CR_RENDER_TIMING = 1 << 4
-STAGES = ("clear", "stage1", "stage2", "stage3", "resolve")
+STAGES = ("clear", "vertex", "stage1", "stage2", "stage3", "resolve")
 
 CLEAR_PIXEL = 0xFFFFFFF000000000
 BACKGROUND = 0xFFFFFFFF
@@ -98,7 +98,7 @@ class CrFrameStats(ctypes.Structure):
 
 
 class CrStageTimes(ctypes.Structure):
-    _fields_ = [("ms", _f32 * 5), ("frames", _u32)]
+    _fields_ = [("ms", _f32 * 6), ("frames", _u32)]
 
 
 EXPORTS = {

@@ -119,10 +119,11 @@ enum cr_render_flags {
 };
 
 /* Per-stage device time summed over the frames rendered with
- * CR_RENDER_TIMING since the last call (waits for them).  ms[0..4]: clear,
- * stage 1, stage 2, stage 3, resolve.  Returns the frame count in *frames. */
+ * CR_RENDER_TIMING since the last call (waits for them).  ms[0..5]: clear,
+ * vertex pass, stage 1, stage 2, stage 3, resolve.  Returns the frame count
+ * in *frames. */
 typedef struct cr_stage_times {
-    float ms[5];
+    float ms[6];
     uint32_t frames;
 } cr_stage_times;
 
