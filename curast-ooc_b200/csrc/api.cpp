@@ -325,6 +325,11 @@ cr_status upload_frame(cr_context* ctx, const Assembled& A, cudaStream_t stream,
 
 }  // namespace
 
+// Internal helpers shared with noalloc.cu (declared in cr_device.h).
+void cr_internal_set_error(const char* msg) { g_error = msg; }
+void cr_internal_mat4_inverse(const float* m, float* out) { mat4_inverse(m, out); }
+float cr_internal_det3(const float* m) { return det3_glm(m); }
+
 extern "C" {
 
 int cr_abi_version(void) { return CR_ABI_VERSION; }

@@ -125,3 +125,8 @@ int cr_launch_stage1(const CrFrameParams& p, const CrLaunchShape& s, void* strea
 int cr_launch_stage2(const CrFrameParams& p, const CrLaunchShape& s, void* stream);
 int cr_launch_stage3(const CrFrameParams& p, const CrLaunchShape& s, void* stream);
 int cr_launch_resolve(const CrResolveParams& p, void* stream);
+
+// Host helpers implemented in api.cpp.
+void cr_internal_set_error(const char* msg);
+void cr_internal_mat4_inverse(const float* m, float* out);  // glm::inverse order
+float cr_internal_det3(const float* m);                     // dot(cross(c0, c1), c2)

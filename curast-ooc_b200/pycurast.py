@@ -101,6 +101,21 @@ class CrStageTimes(ctypes.Structure):
     _fields_ = [("ms", _f32 * 6), ("frames", _u32)]
 
 
+class CrNoallocInstance(ctypes.Structure):
+    _fields_ = [
+        ("d_positions", ctypes.c_void_p),
+        ("d_indices", ctypes.c_void_p),
+        ("d_colors", ctypes.c_void_p),
+        ("num_vertices", _u32),
+        ("num_triangles", _u32),
+        ("world", _f32 * 16),
+    ]
+
+
+CR_NOALLOC_MAX_INSTANCES = 16
+CR_NOALLOC_MAX_VERTICES = 4 << 20
+
+
 EXPORTS = {
     "cr_drain_stage_times": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrStageTimes)]),
     "cr_config_default": (None, [ctypes.POINTER(CrConfig)]),
@@ -120,7 +135,25 @@ EXPORTS = {
     "cr_sync": (_i32, [ctypes.c_void_p]),
     "cr_mat4_mul": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "cr_order_instances": (_i32, [ctypes.c_void_p, ctypes.c_void_p, _u32, _u32, ctypes.c_void_p, ctypes.c_void_p]),
+    "cr_render_noalloc": (_i32, [_i32, ctypes.POINTER(CrNoallocInstance), _u32, ctypes.POINTER(CrCamera), _u64, _u64,
+                                 _i32, ctypes.c_void_p]),
 }
+
+
+def render_noalloc(device, instances, camera, d_visbuffer, d_rgba=0, display=CR_DISPLAY_VERTEX_COLORS, stream=0):
+    """cr_render_noalloc: instances are (d_positions, d_indices, d_colors,
+    num_vertices, num_triangles, world) tuples of device addresses.  Returns
+    the status code (the binding does not raise, so callers can test limits)."""
+    arr = (CrNoallocInstance * max(len(instances), 1))()
+    for i, (dp, di, dc, nv, nt, world) in enumerate(instances):
+        arr[i].d_positions = int(dp)
+        arr[i].d_indices = int(di) if di else None
+        arr[i].d_colors = int(dc) if dc else None
+        arr[i].num_vertices = int(nv)
+        arr[i].num_triangles = int(nt)
+        arr[i].world = _f16(world)
+    return load().cr_render_noalloc(int(device), arr, len(instances), ctypes.byref(camera), int(d_visbuffer),
+                                    int(d_rgba), int(display), ctypes.c_void_p(int(stream)))
 
 
 def order_instances(mesh, triangles, keep_order=False):

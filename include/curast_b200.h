@@ -186,6 +186,48 @@ cr_status cr_drain_stage_times(cr_context* ctx, cr_stage_times* out);
 /* 4x4 helpers in glm's float operation order (host). */
 void cr_mat4_mul(const float* a, const float* b, float* out);
 
+/* ---- rendering without allocating ----------------------------------------
+ * No counterpart in the reference (CuRast allocates its queues and buffers
+ * itself).  For callers that must not allocate device memory while they
+ * render -- a plug-in whose host owns every byte of device memory through its
+ * own pool or gives it a fixed cap, or a frame loop that cannot take the
+ * device-wide synchronisation cudaMalloc/cudaFree imply in the middle of a
+ * frame -- cr_render_noalloc renders one view without any context and calls
+ * no allocating routine.  Its work queues, counters, outcodes and frame table
+ * live in one static device array of CR_NOALLOC_SCRATCH_BYTES (about 12 MiB)
+ * that every GPU which loads the library holds until the process exits.
+ *
+ *   - instances[i] is one instance with its mesh's device arrays; ids follow
+ *     the given order (as CR_RENDER_KEEP_ORDER); at most
+ *     CR_NOALLOC_MAX_INSTANCES instances and CR_NOALLOC_MAX_VERTICES vertices
+ *     summed over them, else CR_ERR_INVALID.  A frame needing more than
+ *     CR_NOALLOC_MAX_NONTRIVIAL stage-2 or CR_NOALLOC_MAX_TILES stage-3
+ *     entries returns CR_ERR_QUEUE_OVERFLOW (output incomplete).
+ *   - The call is synchronous on `stream` (it reads back the queue counters).
+ *   - The first call on a device looks up the array's device address (once
+ *     per device); make that first call before any stream capture.
+ *   - Every call shares the one array: calls that overlap on the GPU (other
+ *     streams, other host threads) race and must be serialised by the caller.
+ *     Each call resets the counters it needs; nothing else carries over. */
+#define CR_NOALLOC_MAX_INSTANCES 16u
+#define CR_NOALLOC_MAX_VERTICES (4u << 20)
+#define CR_NOALLOC_MAX_NONTRIVIAL (512u << 10)
+#define CR_NOALLOC_MAX_TILES (256u << 10)
+#define CR_NOALLOC_SCRATCH_BYTES (12u * 1024u * 1024u + 20u * 1024u)
+
+typedef struct cr_noalloc_instance {
+    const float* d_positions;   /* xyz per vertex, device                      */
+    const uint32_t* d_indices;  /* 3 per triangle, device; NULL = vertex 3t+k  */
+    const uint32_t* d_colors;   /* RGBA8 per vertex, device; may be NULL       */
+    uint32_t num_vertices;
+    uint32_t num_triangles;
+    float world[16];            /* object -> world                             */
+} cr_noalloc_instance;
+
+cr_status cr_render_noalloc(int32_t device, const cr_noalloc_instance* instances, uint32_t count,
+                            const cr_camera* camera, uint64_t d_visbuffer, uint64_t d_rgba,
+                            int32_t display, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
