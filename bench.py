@@ -59,6 +59,17 @@ def build_workload(name):
         return dict(name=name, W=W, H=H, meshes=[(pos, idx, col)], instances=[(0, scenes.identity())],
                     view=view, proj=proj, device=False,
                     desc="1024x512-quad displaced heightfield (1,048,576 triangles, 525,825 vertices), 1920x1080")
+    if name.startswith("instanced_"):
+        # instanced_<K>x<N>m_1080p: one N-million-triangle mesh drawn as K instances
+        k, n = name.split("_")[1].split("x")
+        count, tris = int(k), int(n.rstrip("m")) * 1_000_000
+        W, H = 1920, 1080
+        pos, idx, col = scenes.asteroid(tris, device="cuda")
+        view, proj = scenes.instanced_camera(W, H)
+        return dict(name=name, W=W, H=H, meshes=[(pos, idx, col)],
+                    instances=[(0, w) for w in scenes.instanced_field(count)], view=view, proj=proj, device=True,
+                    desc=f"one seeded {tris:,}-triangle displaced icosphere drawn as {count} instances (uniform "
+                         f"rotation, scale 0.5-2, positions uniform in a 100^3 box), 1920x1080")
     if name.startswith("planet_"):
         # planet_<N>m_1080p: the dense subdivided-sphere scene with N million triangles
         count = int(name.split("_")[1].rstrip("m")) * 1_000_000

@@ -560,12 +560,19 @@ cr_status cr_render(cr_context* ctx, const cr_instance* instances, uint32_t coun
     CR_CUDA(cudaStreamWaitEvent(stream, ctx->frameDone, 0), "stream wait");
     const uint64_t numPixels = (uint64_t)cam->width * (uint64_t)cam->height;
 
-    if (A.outBytes > ctx->outCap) {  // vertex-pass outcodes: one byte per (instance, vertex)
+    // vertex-pass records: one outcode byte, or one 8-byte cell record, per
+    // (instance, vertex); the choice changes speed only, never the output
+    uint32_t cellMode = ctx->cfg.cull_records == CR_CULL_CELLS ? 1u
+                        : ctx->cfg.cull_records == CR_CULL_OUTCODES ? 0u
+                                                                    : (count > 1 ? 1u : 0u);
+    if (cam->width > 65535 || cam->height > 65535) cellMode = 0;  // cells hold 16-bit coordinates
+    const uint64_t recBytes = A.outBytes * (cellMode ? 8 : 1);
+    if (recBytes > ctx->outCap) {
         CR_CUDA(cudaDeviceSynchronize(), "outcode resize");
         ctx->dev_free(ctx->outcodes, ctx->outCap);
         ctx->outcodes = nullptr;
         ctx->outCap = 0;
-        const uint64_t want = A.outBytes + A.outBytes / 8;
+        const uint64_t want = recBytes + recBytes / 8;
         s = ctx->dev_alloc((void**)&ctx->outcodes, want, "vertex outcodes");
         if (s) return s;
         ctx->outCap = want;
@@ -577,6 +584,7 @@ cr_status cr_render(cr_context* ctx, const cr_instance* instances, uint32_t coun
         if (s) return s;
     }
     fp.outcodes = ctx->outcodes;
+    fp.cellMode = cellMode;
     fp.fb = (uint64_t*)d_visbuffer;
     fp.W = cam->width;
     fp.H = cam->height;

@@ -47,6 +47,18 @@ struct alignas(16) CrInstance {
 #define CR_OC_BOTTOM 16u        // ndc.y < -1                      (tv.cu:117)
 #define CR_OC_SIDES 30u
 #define CR_VCHUNK 1024          // vertices per vertex-pass chunk
+
+// Cell records (8 bytes per (instance, vertex), CrFrameParams::cellMode):
+// the outcode byte plus the vertex's exact stage-1 screen position reduced to
+// its pixel cell, so stage 1 can also decide the reference's sample-miss cull
+// (tv.cu:153-158) from three records.
+//   bits  0..7   outcode
+//   bit   8      inside: screen x in [0, W-1] and y in [0, H-1] (and depth > 0)
+//   bit   9      x is not an integer      bit 10  y is not an integer
+//   bits 16..31  floor(x)                 bits 32..47  floor(y)
+#define CR_CELL_INSIDE (1ull << 8)
+#define CR_CELL_FRACX (1ull << 9)
+#define CR_CELL_FRACY (1ull << 10)
 static_assert(sizeof(CrInstance) == 64, "CrInstance layout");
 
 struct alignas(16) CrSegment {
@@ -63,10 +75,35 @@ struct alignas(16) CrSegment {
 static_assert(sizeof(CrSegment) == 48, "CrSegment layout");
 
 struct alignas(16) CrTile {     // HugeTriangle, HostDeviceInterface.h:254-259
-    int32_t instance;
+    int32_t instance;           // instance | view << 26 (view 0 in single-view frames)
     int32_t triangle;
     int32_t tile_x;
     int32_t tile_y;
+};
+
+// Stage-2 queue entry: (view << 58) | (instance << 32) | triangle; single-view
+// frames use view 0, i.e. the reference's packing (tv.cu:192-197).
+#define CR_ENTRY_VIEW_SHIFT 58
+#define CR_ENTRY_INST_MASK 0x3ffffffull  // 26 bits of instance
+#define CR_MAX_VIEWS 64                  // views per batched frame (one bit each)
+
+// One view of a batched frame (single-view frames fill one).
+struct alignas(16) CrView {
+    uint64_t* fb;               // visbuffer, W*H
+    uint32_t* rgba;             // may be nullptr
+    uint64_t* colorbuffer;      // may be nullptr
+    int32_t W, H;
+    float f;                    // proj[1][1]
+    float aspect;               // float(W) / float(H)
+    float viewI[16];            // inverse(view), for the resolve
+    float origin[3];
+    float p00, p11;
+    uint32_t pad[3];
+};
+
+// Multi-view vertex record: per frustum predicate one bit per view.
+struct alignas(8) CrViewMasks {
+    unsigned long long behind, right, left, top, bottom;
 };
 
 struct CrFrameParams {
@@ -92,6 +129,12 @@ struct CrFrameParams {
     uint32_t pad;
     uint8_t* outcodes;          // vertex-pass output, CrInstance::outBase + vertex
     uint64_t numVChunks;        // vertex-pass chunks of all instances
+    // batched frames: world_view holds numViews * numInstances matrices,
+    // view-major; the vertex pass writes CrViewMasks records instead of bytes
+    const CrView* views;
+    uint32_t numViews;
+    uint32_t cellMode;          // 1: the vertex pass writes 8-byte cell records
+    CrViewMasks* viewMasks;     // CrInstance::outBase + vertex
 };
 
 struct CrResolveParams {
@@ -125,6 +168,18 @@ int cr_launch_stage1(const CrFrameParams& p, const CrLaunchShape& s, void* strea
 int cr_launch_stage2(const CrFrameParams& p, const CrLaunchShape& s, void* stream);
 int cr_launch_stage3(const CrFrameParams& p, const CrLaunchShape& s, void* stream);
 int cr_launch_resolve(const CrResolveParams& p, void* stream);
+
+// Batched (multi-view) frame: one launch per stage over all views.
+struct CrBatchShape {
+    int vertexBlocks, stage1Blocks, stage2Blocks, stage3Blocks;  // persistent grids
+};
+int cr_launch_clear_views(const CrFrameParams& p, int maxPixels, void* stream);
+int cr_launch_vertex_views(const CrFrameParams& p, const CrBatchShape& s, void* stream);
+int cr_launch_stage1_views(const CrFrameParams& p, const CrBatchShape& s, void* stream);
+int cr_launch_stage2_views(const CrFrameParams& p, const CrBatchShape& s, void* stream);
+int cr_launch_stage3_views(const CrFrameParams& p, const CrBatchShape& s, void* stream);
+int cr_launch_resolve_views(const CrFrameParams& p, int32_t display, int maxW, int maxH, void* stream);
+int cr_query_batch_shape(int device, CrBatchShape* out);
 
 // Host helpers implemented in api.cpp.
 void cr_internal_set_error(const char* msg);

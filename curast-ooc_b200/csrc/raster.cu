@@ -187,7 +187,25 @@ __device__ __forceinline__ bool ndc_beyond(float X, float d) {
     return (X - d) > d * 5.9604644775390625e-8f;
 }
 
-__device__ __forceinline__ int stage1_triangle(const CrFrameParams& p, const float fa, const Mat& M,
+// The render target of one view: visbuffer, size and projection.
+struct Target {
+    uint64_t* fb;
+    int32_t W, H;
+    float f, fa;  // proj[1][1] and f / aspect
+    uint32_t thrSmall;
+};
+
+__device__ __forceinline__ Target target_of(const CrFrameParams& p) {
+    return Target{p.fb, p.W, p.H, p.f, p.f / p.aspect, p.thrSmall};
+}
+
+__device__ __forceinline__ Target target_of(const CrFrameParams& p, uint32_t view) {
+    const CrView* v = p.views + view;
+    const float f = __ldg(&v->f);
+    return Target{ldg_ptr(&v->fb), __ldg(&v->W), __ldg(&v->H), f, f / __ldg(&v->aspect), p.thrSmall};
+}
+
+__device__ __forceinline__ int stage1_triangle(const Target& p, const float fa, const Mat& M,
                                                const uint32_t flip, const V3 pa, const V3 pb, const V3 pc,
                                                const uint64_t id) {
     const float f = p.f;
@@ -307,9 +325,31 @@ __device__ __forceinline__ uint32_t vertex_outcode(const Mat& M, V3 p, float fa,
            (ndc_beyond(Y, d) ? CR_OC_TOP : 0u) | (ndc_beyond(-Y, d) ? CR_OC_BOTTOM : 0u);
 }
 
+// Cell record of one vertex: the outcode plus stage 1's own screen position
+// (viewToNDC, ndcToScreen, -0.5: tv.cu:106-108,121-134, same operations in
+// the same order) reduced to its pixel cell.
+__device__ __forceinline__ uint64_t vertex_cell_record(const Mat& M, V3 p, float fa, float f, float Wf, float Hf,
+                                                       int W, int H) {
+    const V3 q = xform(M, p);
+    const float d = -q.z;
+    if (d <= 0.0f) return CR_OC_BEHIND;
+    const float X = fa * q.x, Y = f * q.y;
+    uint64_t rec = (ndc_beyond(X, d) ? CR_OC_RIGHT : 0u) | (ndc_beyond(-X, d) ? CR_OC_LEFT : 0u) |
+                   (ndc_beyond(Y, d) ? CR_OC_TOP : 0u) | (ndc_beyond(-Y, d) ? CR_OC_BOTTOM : 0u);
+    const V2 s = to_screen(V3{X / d, Y / d, d}, Wf, Hf);
+    const float sx = s.x - 0.5f, sy = s.y - 0.5f;
+    if (sx >= 0.0f && sx <= (float)(W - 1) && sy >= 0.0f && sy <= (float)(H - 1)) {
+        const float fx = floorf(sx), fy = floorf(sy);
+        rec |= CR_CELL_INSIDE | (sx > fx ? CR_CELL_FRACX : 0ull) | (sy > fy ? CR_CELL_FRACY : 0ull) |
+               ((uint64_t)(uint32_t)(int)fx << 16) | ((uint64_t)(uint32_t)(int)fy << 32);
+    }
+    return rec;
+}
+
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS) k_vertex(const CrFrameParams p) {
     const float fa = p.f / p.aspect;
+    const float Wf = (float)p.W, Hf = (float)p.H;
     for (uint64_t c = blockIdx.x; c < p.numVChunks; c += gridDim.x) {
         uint32_t lo = 0, hi = p.numInstances - 1;  // instance holding chunk c
         while (lo < hi) {
@@ -322,10 +362,16 @@ __global__ void __launch_bounds__(THREADS) k_vertex(const CrFrameParams p) {
         const uint32_t nV = __ldg(&I->numVertices);
         const uint32_t v1 = min(v0 + (uint32_t)CR_VCHUNK, nV);
         const float* pos = ldg_ptr(&I->positions);
-        uint8_t* out = p.outcodes + __ldg(&I->outBase);
         const Mat M = load_mat(p.world_view + 4ull * lo);
-        for (uint32_t v = v0 + threadIdx.x; v < v1; v += THREADS)
-            out[v] = (uint8_t)vertex_outcode(M, load_pos(pos, v), fa, p.f);
+        if (p.cellMode) {
+            uint64_t* out = reinterpret_cast<uint64_t*>(p.outcodes) + __ldg(&I->outBase);
+            for (uint32_t v = v0 + threadIdx.x; v < v1; v += THREADS)
+                out[v] = vertex_cell_record(M, load_pos(pos, v), fa, p.f, Wf, Hf, p.W, p.H);
+        } else {
+            uint8_t* out = p.outcodes + __ldg(&I->outBase);
+            for (uint32_t v = v0 + threadIdx.x; v < v1; v += THREADS)
+                out[v] = (uint8_t)vertex_outcode(M, load_pos(pos, v), fa, p.f);
+        }
     }
 }
 
@@ -454,22 +500,56 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_stage1(const CrFrameParams p)
         const uint32_t ib = first + it.chunk * CR_INST_CHUNK;
         const uint32_t ie = min(ib + CR_INST_CHUNK, first + count);
         for (uint32_t inst = ib; inst < ie; ++inst) {
-            const uint8_t* oc = p.outcodes + __ldg(&p.instances[inst].outBase);
-            uint32_t o[S1_R][3];
+            const uint64_t ob = __ldg(&p.instances[inst].outBase);
+            bool culledR[S1_R];
+            if (p.cellMode) {
+                const uint64_t* rec = reinterpret_cast<const uint64_t*>(p.outcodes) + ob;
+                uint64_t o[S1_R][3];
 #pragma unroll
-            for (int r = 0; r < S1_R; ++r) {
-                o[r][0] = act[r] ? __ldg(oc + ix[r][0]) : 0u;
-                o[r][1] = act[r] ? __ldg(oc + ix[r][1]) : 0u;
-                o[r][2] = act[r] ? __ldg(oc + ix[r][2]) : 0u;
+                for (int r = 0; r < S1_R; ++r) {
+                    o[r][0] = act[r] ? __ldg(rec + ix[r][0]) : 0ull;
+                    o[r][1] = act[r] ? __ldg(rec + ix[r][1]) : 0ull;
+                    o[r][2] = act[r] ? __ldg(rec + ix[r][2]) : 0ull;
+                }
+#pragma unroll
+                for (int r = 0; r < S1_R; ++r) {
+                    const uint64_t all = o[r][0] & o[r][1] & o[r][2];
+                    const uint64_t any = o[r][0] | o[r][1] | o[r][2];
+                    bool c = (all & CR_OC_BEHIND) || (!(any & CR_OC_BEHIND) && (all & CR_OC_SIDES));
+                    // sample miss (tv.cu:153-158): with every vertex on screen
+                    // (so the bbox clamps change nothing), the box misses all
+                    // samples in x (y) iff all three x (y) lie strictly inside
+                    // one pixel cell
+                    if (!c && !(any & CR_OC_BEHIND) && (all & CR_CELL_INSIDE)) {
+                        const uint64_t diff = (o[r][0] ^ o[r][1]) | (o[r][0] ^ o[r][2]);
+                        const bool missX = (all & CR_CELL_FRACX) && !(diff & 0x00000000ffff0000ull);
+                        const bool missY = (all & CR_CELL_FRACY) && !(diff & 0x0000ffff00000000ull);
+                        c = missX || missY;
+                    }
+                    culledR[r] = c;
+                }
+            } else {
+                const uint8_t* oc = p.outcodes + ob;
+                uint32_t o[S1_R][3];
+#pragma unroll
+                for (int r = 0; r < S1_R; ++r) {
+                    o[r][0] = act[r] ? __ldg(oc + ix[r][0]) : 0u;
+                    o[r][1] = act[r] ? __ldg(oc + ix[r][1]) : 0u;
+                    o[r][2] = act[r] ? __ldg(oc + ix[r][2]) : 0u;
+                }
+#pragma unroll
+                for (int r = 0; r < S1_R; ++r) {
+                    const uint32_t all = o[r][0] & o[r][1] & o[r][2];
+                    const uint32_t any = o[r][0] | o[r][1] | o[r][2];
+                    culledR[r] = (all & CR_OC_BEHIND) || (!(any & CR_OC_BEHIND) && (all & CR_OC_SIDES));
+                }
             }
             // all behind (tv.cu:119) or all beyond one side with none behind
             // (tv.cu:110-118): culled from the outcodes alone
             int nsurv = 0;
 #pragma unroll
             for (int r = 0; r < S1_R; ++r) {
-                const uint32_t all = o[r][0] & o[r][1] & o[r][2];
-                const uint32_t any = o[r][0] | o[r][1] | o[r][2];
-                const bool culled = (all & CR_OC_BEHIND) || (!(any & CR_OC_BEHIND) && (all & CR_OC_SIDES));
+                const bool culled = culledR[r];
                 const unsigned m = __ballot_sync(FULL, act[r] && !culled);
                 if (act[r] && !culled) s_surv[w][nsurv + __popc(m & ((1u << lane) - 1u))] = (uint8_t)(r * 32 + lane);
                 nsurv += __popc(m);
@@ -490,7 +570,7 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_stage1(const CrFrameParams p)
                     const V3 pa = load_pos(pos, index_of(tp, 0));
                     const V3 pb = load_pos(pos, index_of(tp, 1));
                     const V3 pc = load_pos(pos, index_of(tp, 2));
-                    res = stage1_triangle(p, fa, M, flip, pa, pb, pc, cum + tri);
+                    res = stage1_triangle(target_of(p), fa, M, flip, pa, pb, pc, cum + tri);
                 }
                 const unsigned qmask = __ballot_sync(FULL, res == S1_QUEUE);
                 if (qmask) {  // warp-aggregated append, tv.cu:190-197
@@ -648,13 +728,15 @@ struct S2Setup {
     uint32_t id32;
 };
 
-__device__ __forceinline__ int stage2_setup(const CrFrameParams& p, const float fa, uint64_t packed, S2Setup& o) {
-    const uint32_t inst = (uint32_t)(packed >> 32);
+__device__ __forceinline__ int stage2_setup(const CrFrameParams& p, const Target& t, uint64_t packed, S2Setup& o) {
+    const uint32_t view = (uint32_t)(packed >> CR_ENTRY_VIEW_SHIFT);
+    const uint32_t inst = (uint32_t)((packed >> 32) & CR_ENTRY_INST_MASK);
     const uint32_t tri = (uint32_t)(packed & 0xffffffffu);
     const CrInstance* I = p.instances + inst;
     // tv.cu:414,424,519: the cumulative count is held in 32 bits
     const uint32_t cum32 = (uint32_t)__ldg(&I->cum);
-    const Mat M = load_mat(p.world_view + 4ull * inst);
+    const Mat M = load_mat(p.world_view + 4ull * ((uint64_t)view * p.numInstances + inst));
+    const float fa = t.fa;
     const uint32_t* ix = ldg_ptr(&I->indices);
     const float* pos = ldg_ptr(&I->positions);
     uint32_t i0, i1, i2;
@@ -667,14 +749,14 @@ __device__ __forceinline__ int stage2_setup(const CrFrameParams& p, const float 
         i1 = 3 * tri + 1;
         i2 = 3 * tri + 2;
     }
-    const float f = p.f;
+    const float f = t.f;
     const V3 av = xform(M, load_pos(pos, i0));
     const V3 bv = xform(M, load_pos(pos, i1));
     const V3 cv = xform(M, load_pos(pos, i2));
     const V3 an = to_ndc(av, fa, f);
     const V3 bn = to_ndc(bv, fa, f);
     const V3 cn = to_ndc(cv, fa, f);
-    const float Wf = (float)p.W, Hf = (float)p.H;
+    const float Wf = (float)t.W, Hf = (float)t.H;
     float min_x, max_x, min_y, max_y;
     if (!screen_bbox(an, bn, cn, av, bv, cv, fa, f, Wf, Hf, min_x, max_x, min_y, max_y)) return S2_SKIP;
     min_x -= 0.5f;
@@ -771,14 +853,14 @@ __device__ __forceinline__ void row_span(float start_x, float py, int size_x, fl
     len = (int)(fhi - flo) + 1;
 }
 
-template <int WARPS>
+// MULTI: entries carry their view (batched frames); otherwise view 0 is the
+// frame's single target.
+template <int WARPS, bool MULTI>
 __global__ void __launch_bounds__(WARPS * 32) k_stage2(const CrFrameParams p) {
     const int lane = threadIdx.x & 31;
     const uint64_t gw = (uint64_t)blockIdx.x * WARPS + (threadIdx.x >> 5);
     const uint64_t nw = (uint64_t)gridDim.x * WARPS;
     const uint64_t count = min((uint64_t)p.counters[CR_CTR_NONTRIVIAL], p.ntCap);
-    const float fa = p.f / p.aspect;
-    const int numPixels = p.W * p.H;
 
     // group size: 32 queued triangles per warp step when the queue is long,
     // fewer when it is short so that every warp gets work
@@ -788,9 +870,11 @@ __global__ void __launch_bounds__(WARPS * 32) k_stage2(const CrFrameParams p) {
         const uint64_t e = g * G + lane;
         const bool mine = lane < (int)G && e < count;
         const uint64_t packed = mine ? p.ntList[e] : 0ull;
+        const uint32_t view = MULTI ? (uint32_t)(packed >> CR_ENTRY_VIEW_SHIFT) : 0u;
+        const Target tg = MULTI ? target_of(p, view) : target_of(p);
         S2Setup su;
         int kind = S2_SKIP;
-        if (mine) kind = stage2_setup(p, fa, packed, su);
+        if (mine) kind = stage2_setup(p, tg, packed, su);
 
         // ---- tiles: tv.cu:494-514, one atomic per warp --------------------
         int tile_x = 0, tile_y = 0, tiles_x = 1;
@@ -828,7 +912,8 @@ __global__ void __launch_bounds__(WARPS * 32) k_stage2(const CrFrameParams p) {
                     const uint64_t slot = b + i;
                     if (slot < p.hugeCap) {
                         CrTile t;
-                        t.instance = (int32_t)(pk >> 32);
+                        t.instance = (int32_t)(((pk >> 32) & CR_ENTRY_INST_MASK) |
+                                               ((pk >> CR_ENTRY_VIEW_SHIFT) << 26));
                         t.triangle = (int32_t)(pk & 0xffffffffu);
                         t.tile_x = tx + (int)(i % (uint32_t)tsx);
                         t.tile_y = ty + (int)(i / (uint32_t)tsx);
@@ -860,6 +945,9 @@ __global__ void __launch_bounds__(WARPS * 32) k_stage2(const CrFrameParams p) {
             const int size_x = __shfl_sync(FULL, su.size_x, j);
             const int nf = __shfl_sync(FULL, su.numFragments, j);
             const uint64_t id = (uint64_t)__shfl_sync(FULL, su.id32, j);
+            uint64_t* const fbj = MULTI ? (uint64_t*)__shfl_sync(FULL, (unsigned long long)tg.fb, j) : p.fb;
+            const int Wj = MULTI ? __shfl_sync(FULL, tg.W, j) : p.W;
+            const int numPixels = Wj * (MULTI ? __shfl_sync(FULL, tg.H, j) : p.H);
             const float start_x = floorf(min_x);
             const float start_y = floorf(min_y);
             const int size_y = nf / size_x;
@@ -905,11 +993,11 @@ __global__ void __launch_bounds__(WARPS * 32) k_stage2(const CrFrameParams p) {
                     if (s >= 0.0f && t >= 0.0f && v >= 0.0f) {
                         // The reference only tests pid < W*H and writes negative
                         // indices in front of the buffer; they are dropped here.
-                        const int pid = (int)px + p.W * (int)py;
+                        const int pid = (int)px + Wj * (int)py;
                         if (pid >= 0 && pid < numPixels) {
                             const float inv_depth = v * iza + s * izb + t * izc;
                             const float depth = 1.0f / inv_depth;
-                            fb_min(p.fb, (uint32_t)pid, pack_pixel(depth, id));
+                            fb_min(fbj, (uint32_t)pid, pack_pixel(depth, id));
                         }
                     }
                 }
@@ -937,21 +1025,24 @@ __device__ __forceinline__ float intersect_mt(V3 dir, V3 v0, V3 e1, V3 e2) {
     return t > 0.0f ? t : INFINITY;
 }
 
-template <int WARPS>
+template <int WARPS, bool MULTI>
 __global__ void __launch_bounds__(WARPS * 32) k_stage3(const CrFrameParams p) {
     const int lane = threadIdx.x & 31;
     const uint64_t gw = (uint64_t)blockIdx.x * WARPS + (threadIdx.x >> 5);
     const uint64_t nw = (uint64_t)gridDim.x * WARPS;
     const uint64_t count = min((uint64_t)p.counters[CR_CTR_HUGE], p.hugeCap);
-    const float f = p.f;
-    const float fa = f / p.aspect;
-    const float Wf = (float)p.W, Hf = (float)p.H;
-    const int numPixels = p.W * p.H;
 
     for (uint64_t ti = gw; ti < count; ti += nw) {
         const CrTile tile = p.hugeList[ti];
-        const CrInstance* I = p.instances + tile.instance;
-        const Mat M = load_mat(p.world_view + 4ull * (uint32_t)tile.instance);
+        const uint32_t inst = (uint32_t)tile.instance & (uint32_t)CR_ENTRY_INST_MASK;
+        const uint32_t view = MULTI ? ((uint32_t)tile.instance >> 26) : 0u;
+        const Target tg = MULTI ? target_of(p, view) : target_of(p);
+        const float f = tg.f;
+        const float fa = tg.fa;
+        const float Wf = (float)tg.W, Hf = (float)tg.H;
+        const int numPixels = tg.W * tg.H;
+        const CrInstance* I = p.instances + inst;
+        const Mat M = load_mat(p.world_view + 4ull * ((uint64_t)view * p.numInstances + inst));
         const uint32_t tri = (uint32_t)tile.triangle;
         const uint32_t* ix = ldg_ptr(&I->indices);
         const float* pos = ldg_ptr(&I->positions);
@@ -991,14 +1082,14 @@ __global__ void __launch_bounds__(WARPS * 32) k_stage3(const CrFrameParams p) {
             const float ry = (1.0f / f) * v;
 #pragma unroll
             for (int c = 0; c < 2; ++c) {
-                const int pid = px[c] + p.W * py;
+                const int pid = px[c] + tg.W * py;
                 const V3 d = {rx[c], ry, -1.0f};
                 const float inv = 1.0f / sqrtf(dot3(d, d));
                 const V3 dir = {d.x * inv, d.y * inv, d.z * inv};
                 const float t = intersect_mt(dir, av, e1, e2);
                 if (t == INFINITY || pid >= numPixels) continue;
                 const float depth = ((t * dir.x) * 0.0f + (t * dir.y) * 0.0f) + (t * dir.z) * -1.0f;
-                fb_min(p.fb, (uint32_t)pid, pack_pixel(depth, id));
+                fb_min(tg.fb, (uint32_t)pid, pack_pixel(depth, id));
             }
         }
     }
@@ -1033,9 +1124,9 @@ int cr_query_launch_shape(int device, CrLaunchShape* out) {
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bv, k_vertex<VX_THREADS>, VX_THREADS, 0) != cudaSuccess)
         return -1;
     out->vertexBlocks = sms * (bv > 0 ? bv : 1);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_stage2<S2_WARPS>, S2_WARPS * 32, 0) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_stage2<S2_WARPS, false>, S2_WARPS * 32, 0) != cudaSuccess)
         return -1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b3, k_stage3<S3_WARPS>, S3_WARPS * 32, 0) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b3, k_stage3<S3_WARPS, false>, S3_WARPS * 32, 0) != cudaSuccess)
         return -1;
     out->numSMs = sms;
     out->stage1Blocks = sms * (b1 > 0 ? b1 : 1);
@@ -1069,11 +1160,11 @@ int cr_launch_stage1(const CrFrameParams& p, const CrLaunchShape& s, void* strea
 }
 
 int cr_launch_stage2(const CrFrameParams& p, const CrLaunchShape& s, void* stream) {
-    k_stage2<S2_WARPS><<<(unsigned)s.stage2Blocks, S2_WARPS * 32, 0, (cudaStream_t)stream>>>(p);
+    k_stage2<S2_WARPS, false><<<(unsigned)s.stage2Blocks, S2_WARPS * 32, 0, (cudaStream_t)stream>>>(p);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 int cr_launch_stage3(const CrFrameParams& p, const CrLaunchShape& s, void* stream) {
-    k_stage3<S3_WARPS><<<(unsigned)s.stage3Blocks, S3_WARPS * 32, 0, (cudaStream_t)stream>>>(p);
+    k_stage3<S3_WARPS, false><<<(unsigned)s.stage3Blocks, S3_WARPS * 32, 0, (cudaStream_t)stream>>>(p);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

@@ -56,8 +56,14 @@ class CrConfig(ctypes.Structure):
         ("grow_on_overflow", _u32),
         ("wait_timeout_ms", _u32),
         ("debug_flags", _u32),
-        ("reserved", _u32 * 5),
+        ("cull_records", _u32),
+        ("reserved", _u32 * 4),
     ]
+
+
+CR_CULL_AUTO = 0
+CR_CULL_OUTCODES = 1
+CR_CULL_CELLS = 2
 
 
 CR_DEBUG_DROP_FIRST_TILE_COPY = 1
@@ -230,11 +236,13 @@ class Context:
     """Owns one cr_context (device geometry, work queues)."""
 
     def __init__(self, device=0, threshold_small=128, threshold_large=4096, max_nontrivial=0, max_huge=0,
-                 memory_budget=0, grow_on_overflow=1, wait_timeout_ms=1000, debug_flags=0):
+                 memory_budget=0, grow_on_overflow=1, wait_timeout_ms=1000, debug_flags=0,
+                 cull_records=CR_CULL_AUTO):
         lib = load()
         cfg = CrConfig()
         lib.cr_config_default(ctypes.byref(cfg))
         cfg.device = device
+        cfg.cull_records = cull_records
         cfg.wait_timeout_ms = wait_timeout_ms
         cfg.debug_flags = debug_flags
         cfg.threshold_small = threshold_small

@@ -212,9 +212,33 @@ def planet(num_triangles=400_000_000, seed=17, device="cuda", width=1920, height
     num_triangles triangles.  Returns torch tensors on `device`: positions
     (V, 3) float32, indices (T, 3) int32 (uint32 bit patterns), colors (V,)
     int32 (RGBA8 bit patterns)."""
+    A, B, C, L, ntri = _planet_levels(num_triangles, seed, width, height)
+    return _patch_mesh(A, B, C, L, ntri, seed, device)
+
+
+def asteroid(num_triangles=1_000_000, seed=23, device="cuda", amp=0.03):
+    """Seeded displaced unit icosphere: the 20*4^3 base patches uniformly
+    subdivided to the level that reaches num_triangles, trimmed to exactly
+    that many, with the planet's fractal displacement scaled to `amp`."""
+    A, B, C = icosphere_patches(3)
+    lev = 0
+    while A.shape[0] * 4 ** lev < num_triangles:
+        lev += 1
+    L = np.full(A.shape[0], lev, np.int64)
+    ntri = np.full(A.shape[0], 4 ** lev, np.int64)
+    cum = np.cumsum(ntri)
+    k = int(np.searchsorted(cum, num_triangles))
+    ntri = ntri[:k + 1].copy()
+    ntri[-1] -= int(cum[k] - num_triangles)
+    return _patch_mesh(A[:k + 1], B[:k + 1], C[:k + 1], L[:k + 1], ntri, seed, device,
+                       amp_scale=amp / PLANET["disp_amp"])
+
+
+def _patch_mesh(A, B, C, L, ntri, seed, device, amp_scale=1.0):
+    """Vertices and triangles of patches subdivided to levels L (ntri of each
+    patch's 4^L triangles kept), built on `device` in 16M-element chunks."""
     import torch
 
-    A, B, C, L, ntri = _planet_levels(num_triangles, seed, width, height)
     n = 2 ** L
     nv = (n + 1) * (n + 2) // 2
     vbase = np.concatenate([[0], np.cumsum(nv)])
@@ -252,7 +276,8 @@ def planet(num_triangles=400_000_000, seed=17, device="cuda", width=1920, height
         q = (q / torch.linalg.norm(q, dim=1, keepdim=True)).float()
         r = torch.ones(q.shape[0], dtype=torch.float32, device=device)
         for d, fr, amp, ph in waves:
-            r += amp * torch.sin(fr * (q[:, 0] * float(d[0]) + q[:, 1] * float(d[1]) + q[:, 2] * float(d[2])) + ph)
+            r += (amp * amp_scale) * torch.sin(
+                fr * (q[:, 0] * float(d[0]) + q[:, 1] * float(d[1]) + q[:, 2] * float(d[2])) + ph)
         pos[v0:v0 + q.shape[0]] = q * r[:, None]
     # triangles: all upward ones row by row, then the downward ones
     for t0 in range(0, T, chunk):
@@ -307,3 +332,18 @@ def triangle_soup(n, seed=7, spread=4.0, near_fraction=0.02, size_sigma=1.5, ind
     col2 = colors[perm]
     idx = inv.reshape(-1, 3)
     return pos2, idx, col2
+
+
+def instanced_field(count=3000, seed=29, box=100.0):
+    """World transforms of `count` instances: uniform random rotations, scale
+    U(0.5, 2), translations uniform in [0, box]^3 (float32, column-major)."""
+    rng = np.random.default_rng(seed)
+    return [random_affine(rng, pos_box=box, smin=0.5, smax=2.0) for _ in range(count)]
+
+
+def instanced_camera(width=1920, height=1080, box=100.0):
+    """Looks at the instance box from outside, framing all of it."""
+    c = box / 2.0
+    view = look_at((c, c + 0.35 * box, c + 2.1 * box), (c, c, c))
+    proj = perspective(60.0, width / height, 0.1, 10.0 * box)
+    return view, proj

@@ -71,8 +71,20 @@ typedef struct cr_config {
     uint32_t grow_on_overflow; /* re-render once with larger queues (default 1)   */
     uint32_t wait_timeout_ms;  /* bound of every device-side wait (default 1000)  */
     uint32_t debug_flags;      /* CR_DEBUG_* below; 0 in normal use               */
-    uint32_t reserved[5];
+    uint32_t cull_records;     /* CR_CULL_* below: per-vertex records of the
+                                  vertex pass (output-neutral; speed only)        */
+    uint32_t reserved[4];
 } cr_config;
+
+/* Per-vertex records written before stage 1.  Both give bit-identical
+ * output; they differ in what stage 1 can cull without fetching positions:
+ * OUTCODES (1 byte: behind / beyond a frustum side) suits scenes whose
+ * triangles are mostly off-screen, CELLS (8 bytes: also the exact pixel cell)
+ * additionally culls sub-pixel triangles that miss every sample.  AUTO picks
+ * CELLS for frames with more than one instance. */
+#define CR_CULL_AUTO 0u
+#define CR_CULL_OUTCODES 1u
+#define CR_CULL_CELLS 2u
 
 /* Failure-detection test hook: stage 1 never issues its first index-tile
  * copy, so the bounded wait for it runs out; the frame then reports

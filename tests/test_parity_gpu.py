@@ -188,6 +188,53 @@ def test_planet_device_mesh(ctx, count):
         assert_same_vis(vis, rvis, "ours vs reference kernels")
 
 
+def test_instanced_field(ctx):
+    """One mesh drawn as many instances in one launch (instance chunks of the
+    stage-1 work items), against the oracle and the reference's instanced
+    stage-1 kernel."""
+    torch = _torch()
+    pos, idx, col = scenes.asteroid(50_000, device="cuda")
+    worlds = scenes.instanced_field(200, box=20.0)
+    W, H = 640, 360
+    view, proj = scenes.instanced_camera(W, H, box=20.0)
+    h = ctx.mesh_from_device(pos.data_ptr(), pos.shape[0], idx.data_ptr(), idx.shape[0], col.data_ptr())
+    inst = [(0, w) for w in worlds]
+    vis, rgba, _, stats = render_ours(ctx, None, inst, view, proj, W, H, handles=[h])
+    m = (pos.cpu().numpy(), idx.cpu().numpy().view(np.uint32), col.cpu().numpy().view(np.uint32))
+    ovis, orgba, _, ost = render_oracle([m], inst, view, proj, W, H)
+    assert (ovis != CLEAR).mean() > 0.05
+    assert_same_vis(vis, ovis, "ours vs oracle")
+    assert channel_diff(rgba, orgba) <= COLOR_TOL
+    rvis, _, _, _ = render_reference([m], inst, view, proj, W, H, instanced=True,
+                                     cap=2 * int(ost.nontrivial) + 2 * int(ost.huge_tiles) + (1 << 20))
+    assert_same_vis(vis, rvis, "ours vs reference (instanced stage 1)")
+
+
+@pytest.mark.parametrize("records", [pc.CR_CULL_OUTCODES, pc.CR_CULL_CELLS])
+def test_cull_records_do_not_change_output(gpu, records):
+    """Both kinds of per-vertex records (outcode bytes, cell records that
+    also decide the sample-miss cull) give the oracle's visbuffer, on a
+    sub-pixel-heavy instanced scene and on a planet."""
+    torch = _torch()
+    with pc.Context(cull_records=records) as c:
+        pos, idx, col = scenes.asteroid(20_000, device="cuda")
+        worlds = scenes.instanced_field(300, box=30.0)
+        W, H = 500, 300
+        view, proj = scenes.instanced_camera(W, H, box=30.0)
+        h = c.mesh_from_device(pos.data_ptr(), pos.shape[0], idx.data_ptr(), idx.shape[0], col.data_ptr())
+        inst = [(0, w) for w in worlds]
+        vis = render_ours(c, None, inst, view, proj, W, H, handles=[h])[0]
+        m = (pos.cpu().numpy(), idx.cpu().numpy().view(np.uint32), col.cpu().numpy().view(np.uint32))
+        assert_same_vis(vis, render_oracle([m], inst, view, proj, W, H)[0], "instanced field")
+        pos, idx, col = scenes.planet(4_000_000, device="cuda")
+        W, H = 1280, 720
+        view, proj = scenes.planet_camera(W, H)
+        h = c.mesh_from_device(pos.data_ptr(), pos.shape[0], idx.data_ptr(), idx.shape[0], col.data_ptr())
+        vis = render_ours(c, None, [(0, scenes.identity())], view, proj, W, H, handles=[h])[0]
+        m = (pos.cpu().numpy(), idx.cpu().numpy().view(np.uint32), col.cpu().numpy().view(np.uint32))
+        assert_same_vis(vis, render_oracle([m], [(0, scenes.identity())], view, proj, W, H)[0], "planet")
+
+
 def test_stage2_span_narrowing_on_slivers(ctx):
     """Long thin and nearly degenerate triangles, where the rounding of the
     per-fragment test is largest relative to the triangle: the rows narrowed
