@@ -80,6 +80,19 @@ def build_workload(name):
                     view=view, proj=proj, device=True,
                     desc=f"seeded displaced icosphere, {count:,} triangles, per-patch subdivision levels giving a "
                          f"lognormal pre-clip projected-area histogram, 1920x1080")
+    if name.startswith("batched_"):
+        # batched_<V>v_<N>m: N-million-triangle terrain seen by V seeded cameras
+        nv_s, n_s = name.split("_")[1:3]
+        nv = int(nv_s.rstrip("v"))
+        tris = int(n_s.rstrip("m")) * 1_000_000
+        quads = int(round((tris / 2) ** 0.5))
+        pos, idx, col = scenes.terrain(n=quads, device="cuda")
+        cams = scenes.batch_cameras(nv)
+        return dict(name=name, meshes=[(pos, idx, col)], instances=[(0, scenes.identity())], cams=cams,
+                    device=True, batched=True,
+                    desc=f"seeded fractal-displaced grid of {quads}x{quads} quads ({idx.shape[0]:,} triangles) seen "
+                         f"by {nv} seeded cameras, resolutions uniform among 512x512, 1280x720, 1920x1080, "
+                         f"3840x2160")
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -239,6 +252,8 @@ def run_ours(args, rank, world, local):
     import pycurast as pc
 
     wl = build_workload(args.workload)
+    if wl.get("batched"):
+        return run_batched(args, rank, world, local, wl)
     T, V, Tu = scene_counts(wl)
     W, H = wl["W"], wl["H"]
     ctx = pc.Context(device=local)
@@ -359,6 +374,152 @@ def run_ours(args, rank, world, local):
     return line
 
 
+def run_batched(args, rank, world, local, wl):
+    """One step = one batched frame of all views (the autotuned plan replayed
+    as a CUDA graph: table upload, clear, vertex pass, stages 1-3, resolve).
+    The same views rendered one cr_render at a time are timed beside it."""
+    import torch
+
+    import pycurast as pc
+
+    T, V, Tu = scene_counts(wl)
+    cams = wl["cams"]
+    nv = len(cams)
+    P = sum(W * H for _, _, W, H in cams)
+    ctx = pc.Context(device=local)
+    p, i, c = wl["meshes"][0]
+    h = ctx.mesh_from_device(p.data_ptr(), p.shape[0], i.data_ptr(), i.shape[0], c.data_ptr())
+    inst = pc.make_instances([(h, scenes_identity())])
+    ccams = [pc.make_camera(*cam) for cam in cams]
+    vis = [torch.empty(W * H, dtype=torch.int64, device="cuda") for _, _, W, H in cams]
+    rgba = [torch.empty(W * H, dtype=torch.int32, device="cuda") for _, _, W, H in cams]
+    host_rgba = [torch.empty(W * H, dtype=torch.int32, pin_memory=True) for _, _, W, H in cams]
+    views = [(ccams[k], vis[k].data_ptr(), rgba[k].data_ptr(), 0) for k in range(nv)]
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+
+    # autotune this scene class, then capture the frame as a graph
+    t0 = time.perf_counter()
+    tuning = ctx.autotune_batch(inst, views)
+    tune_s = time.perf_counter() - t0
+    plan = pc.BatchPlan(ctx, inst, views)
+    for _ in range(args.warmup):
+        plan.launch(sh)
+    fstats = plan.wait()
+
+    def timed(fn, steps):
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for k in range(steps):
+            evs[k][0].record(stream)
+            fn(k)
+            evs[k][1].record(stream)
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in evs]
+
+    # ---- device-timed region (visbuffers + images are ~2 GB: inputs and
+    # outputs far larger than L2) ------------------------------------------
+    clocks = ClockSampler(local) if rank == 0 else None
+    if clocks:
+        clocks.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    ms_steps = timed(lambda k: plan.launch(sh), args.steps)
+    barrier(world)
+    clk = clocks.stop() if clocks else None
+    plan.wait()
+    ms = max_over_ranks(float(np.mean(ms_steps)), world)
+
+    # per-stage device times of the batched frame (eager, same shapes)
+    ctx.drain_stage_times()
+    for _ in range(3):
+        ctx.render_batch(inst, views, pc.CR_DISPLAY_VERTEX_COLORS, pc.CR_RENDER_TIMING, sh)
+    stage_ms, nfr = ctx.drain_stage_times()
+    stage_ms = {k: v / max(nfr, 1) for k, v in stage_ms.items()}
+
+    # ---- the plain per-view loop on the same GPU ---------------------------
+    def plain(k, flags=0):
+        for j in range(nv):
+            ctx.render(inst, ccams[j], vis[j].data_ptr(), rgba[j].data_ptr(), 0, pc.CR_DISPLAY_VERTEX_COLORS,
+                       flags, sh)
+
+    plain(0, pc.CR_RENDER_SYNC)
+    plain_steps = max(3, min(args.steps, 5))
+    plain_ms = max_over_ranks(float(np.mean(timed(plain, plain_steps))), world)
+
+    # ---- end to end: cameras in (graph's table upload), 64 RGBA8 images out
+    barrier(world)
+    torch.cuda.synchronize()
+
+    def e2e_step(k):
+        plan.launch(sh)
+        for j in range(nv):
+            host_rgba[j].copy_(rgba[j], non_blocking=True)
+
+    e2e_ms = timed(e2e_step, max(3, min(args.steps, 5)))
+    plan.wait()
+    e2e = max_over_ranks(float(np.mean(e2e_ms)), world)
+    plan.close()
+    if rank != 0:
+        ctx.close()
+        return None
+    peak, peak_kind = load_peaks()
+    # algorithmic bytes: vertex pass 12 B position read + 48 B record write per
+    # vertex; stage 1 12 B index tile per triangle + each 48 B record once;
+    # whole frame 12T + 12V (geometry once for all views) + 28 B per pixel of
+    # every view (visbuffer clear and write-back, resolve read + RGBA8 write)
+    algo = {"vertex": 60 * V, "stage1": 12 * T + 48 * V}
+    dominant = max(("vertex", "stage1", "stage2", "stage3", "resolve", "clear"), key=lambda s: stage_ms[s])
+    rk = "stage1" if dominant not in algo else dominant
+    t_k = stage_ms[rk]
+    achieved = algo[rk] / (t_k * 1e-3) / 1e9
+    frame_bytes = 12 * T + 12 * V + 28 * P
+    line = {
+        "metric": "views/s (batched frame of 64 views of uneven resolution, one CUDA-graph launch per step)",
+        "value": world * nv / (ms * 1e-3),
+        "unit": "views/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": wl["name"], "desc": wl["desc"], "triangles": T, "vertices": V, "views": nv,
+                   "pixels": P, "parallelism": f"replicas x{world}",
+                   "l2": "per-step visbuffers and images ({:.1f} GB) exceed L2".format(28 * P / 1e9),
+                   "stage_ms": stage_ms, "dominant_stage": dominant,
+                   "nontrivial": int(fstats.nontrivial), "huge_tiles": int(fstats.huge_tiles),
+                   "plain_loop": {"ms_per_step": plain_ms, "views_per_s": world * nv / (plain_ms * 1e-3),
+                                  "note": f"{nv} cr_render calls per step, same GPU, same outputs"},
+                   "speedup_vs_plain_loop": plain_ms / ms,
+                   "tuning": {"seconds": tune_s, "candidates": int(tuning.candidates),
+                              "ms_default_shapes": float(tuning.ms_before), "ms_tuned": float(tuning.ms_after),
+                              "vertex_blocks": int(tuning.vertex_blocks), "stage1": [int(tuning.stage1_blocks),
+                                                                                    int(tuning.stage1_warps)],
+                              "stage2": [int(tuning.stage2_blocks), int(tuning.stage2_warps)],
+                              "stage3_blocks": int(tuning.stage3_blocks)},
+                   "frame_roofline": {"bytes": frame_bytes, "achieved_gbs": frame_bytes / (ms * 1e-3) / 1e9,
+                                      "frac": frame_bytes / (ms * 1e-3) / 1e9 / peak}},
+        "e2e": {"value": world * nv / (e2e * 1e-3), "unit": "views/s", "ms_per_step": e2e,
+                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 4 * P},
+        "roofline": {"kernel": f"k_{rk}_views", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "algorithmic_bytes": algo[rk],
+                     "kernel_ms": t_k, "traffic": read_traffic(rk + "_views", wl["name"])},
+        "gpu_launches": 6 * args.steps,
+        "clocks": clk,
+    }
+    ctx.close()
+    return line
+
+
+def scenes_identity():
+    import scenes
+
+    return scenes.identity()
+
+
 # ---------------------------------------------------------------------------
 # the reference's own kernels
 # ---------------------------------------------------------------------------
@@ -368,6 +529,8 @@ def run_reference(args, rank, world, local):
     import oracle_lib as ol
 
     wl = build_workload(args.workload)
+    if wl.get("batched"):
+        return run_reference_batched(args, wl, local)
     T, V, Tu = scene_counts(wl)
     W, H = wl["W"], wl["H"]
     try:
@@ -424,6 +587,58 @@ def run_reference(args, rank, world, local):
     }
 
 
+def run_reference_batched(args, wl, local):
+    """The reference renders one view per CuRast::draw: its own kernels run
+    once per view (same cameras, resolutions and mesh); a step is all views."""
+    import oracle_lib as ol
+
+    T, V, Tu = scene_counts(wl)
+    cams = wl["cams"]
+    try:
+        ref = ol.Reference("native", device=local)
+    except Exception as e:  # noqa: BLE001
+        return {"impl": "reference", "unavailable": f"reference kernels not loadable: {e}"}
+    p, i, c = wl["meshes"][0]
+    mid = ref.mesh_device(p.data_ptr(), p.shape[0], i.data_ptr(), i.shape[0], c.data_ptr())
+    hp, hi, hc = host_mesh(wl["meshes"][0])
+    world = np.asarray(wl["instances"][0][1], np.float32).reshape(1, 16)
+    total_ms = 0.0
+    steps = max(1, min(args.steps, 5))
+    for view, proj, W, H in cams:
+        # the reference never checks its queue capacities: size them from the
+        # CPU oracle's exact counts for this view, with a wide margin
+        _, ost = ol.raster(ol.Frame([(hp, hi, hc, world[0])], view), W, H, proj[5], nthreads=os.cpu_count() or 1)
+        cap_nt = min(T, 2 * int(ost.nontrivial) + (1 << 20))
+        cap_huge = 2 * int(ost.huge_tiles) + (1 << 20)
+        ref.frame([mid], world, view, proj, W, H, instanced=True, cap_nontrivial=cap_nt, cap_huge=cap_huge,
+                  frames=1, want_color=False)
+        _, _, _, ms, _ = ref.frame([mid], world, view, proj, W, H, instanced=True, cap_nontrivial=cap_nt,
+                                   cap_huge=cap_huge, frames=steps, want_color=False)
+        total_ms += float(ms[0] + ms[1])
+    v = len(cams) / (total_ms * 1e-3)
+    return {
+        "impl": "reference",
+        "metric": "views/s (batched frame of 64 views of uneven resolution, one CUDA-graph launch per step)",
+        "value": v,
+        "unit": "views/s",
+        "n_gpus": 1,
+        "steps": steps,
+        "warmup": 1,
+        "ms_per_step": total_ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": wl["name"], "desc": wl["desc"], "triangles": T, "vertices": V, "views": len(cams),
+                   "parallelism": "single GPU",
+                   "build": "CuRast NVRTC recipe (--use_fast_math, LTO) for sm_100a; one frame per view"},
+        "cpu_baseline": {"kind": "reference", "value": v, "unit": "views/s", "cores": 0,
+                         "sample": "not a CPU run: the reference's own CUDA kernels, one frame per view"},
+        "e2e": {"value": v, "unit": "views/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -431,7 +646,9 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="planet_400m_1080p",
-                    help="planet_400m_1080p (the 400M-triangle dense mesh), planet_<N>m_1080p, heightfield_1m_1080p")
+                    help="planet_400m_1080p (the 400M-triangle dense mesh), planet_<N>m_1080p, heightfield_1m_1080p, "
+                         "instanced_<K>x<N>m_1080p, batched_<V>v_<N>m (V cameras over an N-million-triangle "
+                         "terrain)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)

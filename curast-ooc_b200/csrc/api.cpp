@@ -1,10 +1,7 @@
-// api.cpp -- host side of the C ABI declared in include/curast_b200.h.
+// api.cpp -- host side of the single-view C ABI declared in
+// include/curast_b200.h (context, meshes, frame assembly, cr_render).
 //
-// Built with -ffp-contract=off: the per-instance world_view = view * world and
-// the mirrored-instance determinant are formed here in glm's float order
-// (libs/glm/glm/detail/type_mat4x4.inl:601-618, func_geometric.inl:53-85),
-// exactly as the reference's render host does (src/CuRast_render.h:406-410)
-// and its stage-1 kernel does (src/kernels/triangles_visbuffer.cu:179-185).
+// Built with -ffp-contract=off; see context.h for why.
 #include "curast_b200.h"
 
 #include <cuda_runtime.h>
@@ -18,11 +15,13 @@
 #include <string>
 #include <vector>
 
-#include "cr_device.h"
+#include "context.h"
+
+namespace cr {
 
 namespace {
-
 thread_local std::string g_error;
+}  // namespace
 
 cr_status fail(cr_status s, const char* fmt, ...) {
     char buf[512];
@@ -37,23 +36,6 @@ cr_status fail(cr_status s, const char* fmt, ...) {
 cr_status cuda_fail(cudaError_t e, const char* what) {
     return fail(e == cudaErrorMemoryAllocation ? CR_ERR_OOM : CR_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
-
-#define CR_CUDA(call, what)                      \
-    do {                                         \
-        cudaError_t _e = (call);                 \
-        if (_e != cudaSuccess) return cuda_fail(_e, what); \
-    } while (0)
-
-struct MeshRec {
-    bool live = false;
-    bool owned = false;
-    float* positions = nullptr;
-    uint32_t* indices = nullptr;
-    uint32_t* colors = nullptr;
-    uint32_t numVertices = 0;
-    uint32_t numTriangles = 0;
-    size_t bytes = 0;
-};
 
 // glm mat4 * mat4: column j = ((A0*B[j][0] + A1*B[j][1]) + A2*B[j][2]) + A3*B[j][3]
 void mat4_mul(const float* a, const float* b, float* out) {
@@ -108,76 +90,29 @@ void mat4_inverse(const float* m, float* out) {
 #undef M
 }
 
-size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+}  // namespace cr
 
-struct Assembled {
-    std::vector<uint32_t> order;
-    std::vector<CrInstance> inst;
-    std::vector<float> worldView;   // 16 per instance
-    std::vector<float> world;       // 16 per instance
-    std::vector<CrSegment> seg;
-    uint64_t totalTriangles = 0;
-    uint64_t numItems = 0;
-    uint64_t outBytes = 0;     // vertex-pass outcode bytes of all instances
-    uint64_t numVChunks = 0;   // vertex-pass chunks of all instances
-};
+using namespace cr;
 
-}  // namespace
-
-struct cr_context {
-    cr_config cfg{};
-    int device = 0;
-    CrLaunchShape shape{};
-    std::vector<MeshRec> meshes;
-    size_t bytesInUse = 0;
-
-    // frame table: device copy + pinned staging
-    void* dFrame = nullptr;
-    size_t dFrameCap = 0;
-    void* hFrame = nullptr;
-    size_t hFrameCap = 0;
-    cudaEvent_t frameCopied = nullptr;
-    cudaEvent_t frameDone = nullptr;  // last kernel of the previous frame
-
-    // queues
-    uint8_t* outcodes = nullptr;  // vertex-pass output
-    uint64_t outCap = 0;
-    uint64_t* ntList = nullptr;
-    uint64_t ntCap = 0;
-    CrTile* hugeList = nullptr;
-    uint64_t hugeCap = 0;
-    unsigned long long* counters = nullptr;
-    unsigned long long* hCounters = nullptr;  // pinned
-
-    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
-    // CR_RENDER_TIMING: a ring of event sets (7 per frame) drained on demand
-    static constexpr int kRing = 128;
-    std::vector<cudaEvent_t> ring;
-    int ringHead = 0, ringCount = 0;
-    cr_frame_stats last{};
-    bool pendingStats = false;
-    cudaStream_t lastStream = nullptr;
-
-    cr_status dev_alloc(void** p, size_t bytes, const char* what) {
-        if (cfg.memory_budget && bytesInUse + bytes > cfg.memory_budget)
-            return fail(CR_ERR_OOM, "%s: %zu bytes would exceed the memory budget (%zu in use of %llu)", what, bytes,
-                        bytesInUse, (unsigned long long)cfg.memory_budget);
-        cudaError_t e = cudaMalloc(p, bytes);
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            return cuda_fail(e, what);
-        }
-        bytesInUse += bytes;
-        return CR_OK;
+cr_status cr_context::dev_alloc(void** p, size_t bytes, const char* what) {
+    if (cfg.memory_budget && bytesInUse + bytes > cfg.memory_budget)
+        return fail(CR_ERR_OOM, "%s: %zu bytes would exceed the memory budget (%zu in use of %llu)", what, bytes,
+                    bytesInUse, (unsigned long long)cfg.memory_budget);
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return cuda_fail(e, what);
     }
-    void dev_free(void* p, size_t bytes) {
-        if (!p) return;
-        cudaFree(p);
-        bytesInUse -= std::min(bytesInUse, bytes);
-    }
-};
+    bytesInUse += bytes;
+    return CR_OK;
+}
+void cr_context::dev_free(void* p, size_t bytes) {
+    if (!p) return;
+    cudaFree(p);
+    bytesInUse -= std::min(bytesInUse, bytes);
+}
 
-namespace {
+namespace cr {
 
 // CuRast_render.h:338-345: triangle count descending, then mesh; ties keep
 // submission order (the reference's std::sort leaves them unspecified).
@@ -323,7 +258,97 @@ cr_status upload_frame(cr_context* ctx, const Assembled& A, cudaStream_t stream,
     return CR_OK;
 }
 
-}  // namespace
+cr_status ensure_records(cr_context* ctx, uint64_t bytes) {
+    if (bytes <= ctx->outCap) return CR_OK;
+    CR_CUDA(cudaDeviceSynchronize(), "record buffer resize");
+    ctx->dev_free(ctx->outcodes, ctx->outCap);
+    ctx->outcodes = nullptr;
+    ctx->outCap = 0;
+    const uint64_t want = align_up(bytes + bytes / 8, 256);
+    cr_status s = ctx->dev_alloc((void**)&ctx->outcodes, want, "vertex records");
+    if (s) return s;
+    ctx->outCap = want;
+    return CR_OK;
+}
+
+// Adds the oldest frame of the timing ring to ctx->folded (waits for it).
+cr_status fold_oldest(cr_context* ctx) {
+    cudaEvent_t* e = &ctx->ring[7 * ctx->ringHead];
+    CR_CUDA(cudaEventSynchronize(e[6]), "timing sync");
+    for (int i = 0; i < 6; i++) {
+        float ms = 0.0f;
+        CR_CUDA(cudaEventElapsedTime(&ms, e[i], e[i + 1]), "timing");
+        ctx->folded.ms[i] += ms;
+    }
+    ctx->folded.frames++;
+    ctx->ringHead = (ctx->ringHead + 1) % cr_context::kRing;
+    ctx->ringCount--;
+    return CR_OK;
+}
+
+cr_status run_frame(cr_context* ctx, uint32_t flags, cudaStream_t stream, uint64_t instances, uint64_t triangles,
+                    const IssueFn& issue) {
+    const bool sync = (flags & CR_RENDER_SYNC) != 0;
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        cudaEvent_t* tev = nullptr;  // 7 timing events of this frame, or none
+        if (flags & CR_RENDER_TIMING) {
+            if (ctx->ring.empty()) {
+                ctx->ring.resize(7 * cr_context::kRing, nullptr);
+                for (cudaEvent_t& e : ctx->ring) CR_CUDA(cudaEventCreate(&e), "timing events");
+            }
+            if (ctx->ringCount == cr_context::kRing) {  // full: fold the oldest frame first
+                cr_status ds = fold_oldest(ctx);
+                if (ds) return ds;
+            }
+            tev = &ctx->ring[7 * ((ctx->ringHead + ctx->ringCount) % cr_context::kRing)];
+            ctx->ringCount++;
+        }
+        if (sync) CR_CUDA(cudaEventRecord(ctx->ev[0], stream), "event");
+        cr_status s = issue(tev, sync ? ctx->ev[1] : nullptr);
+        if (s) return s;
+        CR_CUDA(cudaMemcpyAsync(ctx->hCounters, ctx->counters, CR_CTR_COUNT * sizeof(unsigned long long),
+                                cudaMemcpyDeviceToHost, stream),
+                "counters readback");
+        ctx->last = cr_frame_stats{};
+        ctx->last.instances = instances;
+        ctx->last.triangles = triangles;
+        ctx->pendingStats = true;
+        ctx->lastStream = stream;
+        CR_CUDA(cudaEventRecord(ctx->frameDone, stream), "frame event");
+        if (!sync) return CR_OK;
+        CR_CUDA(cudaEventRecord(ctx->ev[2], stream), "event");
+        CR_CUDA(cudaEventSynchronize(ctx->ev[2]), "frame");
+        cudaEventElapsedTime(&ctx->last.ms_total, ctx->ev[0], ctx->ev[2]);
+        cudaEventElapsedTime(&ctx->last.ms_raster, ctx->ev[0], ctx->ev[1]);
+        cudaEventElapsedTime(&ctx->last.ms_resolve, ctx->ev[1], ctx->ev[2]);
+        ctx->pendingStats = false;
+        ctx->last.nontrivial = ctx->hCounters[CR_CTR_NONTRIVIAL];
+        ctx->last.huge_tiles = ctx->hCounters[CR_CTR_HUGE];
+        ctx->last.overflow = ctx->hCounters[CR_CTR_OVERFLOW];
+        if (ctx->hCounters[CR_CTR_TIMEOUT]) return fail(CR_ERR_TIMEOUT, "a device-side wait timed out");
+        if (!ctx->last.overflow) return CR_OK;
+        if (!ctx->cfg.grow_on_overflow || (flags & CR_RENDER_NO_CLEAR))
+            return fail(CR_ERR_QUEUE_OVERFLOW, "queue overflow: nontrivial %llu/%llu, tiles %llu/%llu",
+                        (unsigned long long)ctx->last.nontrivial, (unsigned long long)ctx->ntCap,
+                        (unsigned long long)ctx->last.huge_tiles, (unsigned long long)ctx->hugeCap);
+        // the counters hold the exact demand of every queue that was fed in full
+        const uint64_t ntWant = std::max<uint64_t>(ctx->ntCap, ctx->last.nontrivial + ctx->last.nontrivial / 8 + 1024);
+        const uint64_t huWant = (ctx->last.overflow & 1)
+                                    ? ctx->hugeCap
+                                    : std::max<uint64_t>(ctx->hugeCap, ctx->last.huge_tiles + ctx->last.huge_tiles / 8 + 1024);
+        s = ensure_queues(ctx, ntWant, huWant);
+        if (s) return s;
+    }
+    return fail(CR_ERR_QUEUE_OVERFLOW, "queue overflow persisted after growing the queues");
+}
+
+const cr_tuning* find_tuning(const cr_context* ctx, uint32_t sceneClass) {
+    for (const cr_tuning& t : ctx->tunings)
+        if (t.scene_class == sceneClass) return &t;
+    return nullptr;
+}
+
+}  // namespace cr
 
 // Internal helpers shared with noalloc.cu (declared in cr_device.h).
 void cr_internal_set_error(const char* msg) { g_error = msg; }
@@ -373,7 +398,7 @@ cr_status cr_create(const cr_config* cfg, cr_context** out) {
     cr_context* ctx = new cr_context();
     ctx->cfg = c;
     ctx->device = c.device;
-    if (cr_query_launch_shape(c.device, &ctx->shape) != 0) {
+    if (cr_query_launch_shape(c.device, &ctx->shape) != 0 || cr_query_batch_shape(c.device, &ctx->bshape) != 0) {
         delete ctx;
         return fail(CR_ERR_CUDA, "occupancy query failed: %s", cudaGetErrorString(cudaGetLastError()));
     }
@@ -566,17 +591,8 @@ cr_status cr_render(cr_context* ctx, const cr_instance* instances, uint32_t coun
                         : ctx->cfg.cull_records == CR_CULL_OUTCODES ? 0u
                                                                     : (count > 1 ? 1u : 0u);
     if (cam->width > 65535 || cam->height > 65535) cellMode = 0;  // cells hold 16-bit coordinates
-    const uint64_t recBytes = A.outBytes * (cellMode ? 8 : 1);
-    if (recBytes > ctx->outCap) {
-        CR_CUDA(cudaDeviceSynchronize(), "outcode resize");
-        ctx->dev_free(ctx->outcodes, ctx->outCap);
-        ctx->outcodes = nullptr;
-        ctx->outCap = 0;
-        const uint64_t want = recBytes + recBytes / 8;
-        s = ctx->dev_alloc((void**)&ctx->outcodes, want, "vertex outcodes");
-        if (s) return s;
-        ctx->outCap = want;
-    }
+    s = ensure_records(ctx, A.outBytes * (cellMode ? 8 : 1));
+    if (s) return s;
     CrFrameParams fp{};
     CrResolveParams rp{};
     if (count) {
@@ -609,28 +625,12 @@ cr_status cr_render(cr_context* ctx, const cr_instance* instances, uint32_t coun
     rp.p11 = cam->proj[5];
     rp.background = 0xffffffffu;  // HostDeviceInterface.h:37 BACKGROUND_COLOR
 
-    const bool sync = (flags & CR_RENDER_SYNC) != 0;
-    for (int attempt = 0; attempt < 3; ++attempt) {
+    auto issue = [&](cudaEvent_t* tev, cudaEvent_t rasterEnd) -> cr_status {
         fp.ntList = ctx->ntList;
         fp.ntCap = ctx->ntCap;
         fp.hugeList = ctx->hugeList;
         fp.hugeCap = ctx->hugeCap;
-        cudaEvent_t* tev = nullptr;  // 6 timing events of this frame, or none
-        if (flags & CR_RENDER_TIMING) {
-            if (ctx->ring.empty()) {
-                ctx->ring.resize(7 * cr_context::kRing, nullptr);
-                for (cudaEvent_t& e : ctx->ring) CR_CUDA(cudaEventCreate(&e), "timing events");
-            }
-            if (ctx->ringCount == cr_context::kRing) {  // full: fold the oldest frame first
-                cr_stage_times tmp;
-                cr_status ds = cr_drain_stage_times(ctx, &tmp);
-                if (ds) return ds;
-            }
-            tev = &ctx->ring[7 * ((ctx->ringHead + ctx->ringCount) % cr_context::kRing)];
-            ctx->ringCount++;
-        }
         auto mark = [&](int i) -> cudaError_t { return tev ? cudaEventRecord(tev[i], stream) : cudaSuccess; };
-        if (sync) CR_CUDA(cudaEventRecord(ctx->ev[0], stream), "event");
         CR_CUDA(mark(0), "event");
         if (flags & CR_RENDER_NO_CLEAR) {
             CR_CUDA(cudaMemsetAsync(ctx->counters, 0, CR_CTR_COUNT * sizeof(unsigned long long), stream), "counters");
@@ -650,44 +650,13 @@ cr_status cr_render(cr_context* ctx, const cr_instance* instances, uint32_t coun
         if (count && cr_launch_stage3(fp, ctx->shape, stream))
             return fail(CR_ERR_CUDA, "stage-3 launch: %s", cudaGetErrorString(cudaGetLastError()));
         CR_CUDA(mark(5), "event");
-        if (sync) CR_CUDA(cudaEventRecord(ctx->ev[1], stream), "event");
+        if (rasterEnd) CR_CUDA(cudaEventRecord(rasterEnd, stream), "event");
         if (!(flags & CR_RENDER_NO_RESOLVE) && count && cr_launch_resolve(rp, stream))
             return fail(CR_ERR_CUDA, "resolve launch: %s", cudaGetErrorString(cudaGetLastError()));
         CR_CUDA(mark(6), "event");
-        CR_CUDA(cudaMemcpyAsync(ctx->hCounters, ctx->counters, CR_CTR_COUNT * sizeof(unsigned long long),
-                                cudaMemcpyDeviceToHost, stream),
-                "counters readback");
-        ctx->last = cr_frame_stats{};
-        ctx->last.instances = count;
-        ctx->last.triangles = A.totalTriangles;
-        ctx->pendingStats = true;
-        ctx->lastStream = stream;
-        CR_CUDA(cudaEventRecord(ctx->frameDone, stream), "frame event");
-        if (!sync) return CR_OK;
-        CR_CUDA(cudaEventRecord(ctx->ev[2], stream), "event");
-        CR_CUDA(cudaEventSynchronize(ctx->ev[2]), "frame");
-        cudaEventElapsedTime(&ctx->last.ms_total, ctx->ev[0], ctx->ev[2]);
-        cudaEventElapsedTime(&ctx->last.ms_raster, ctx->ev[0], ctx->ev[1]);
-        cudaEventElapsedTime(&ctx->last.ms_resolve, ctx->ev[1], ctx->ev[2]);
-        ctx->pendingStats = false;
-        ctx->last.nontrivial = ctx->hCounters[CR_CTR_NONTRIVIAL];
-        ctx->last.huge_tiles = ctx->hCounters[CR_CTR_HUGE];
-        ctx->last.overflow = ctx->hCounters[CR_CTR_OVERFLOW];
-        if (ctx->hCounters[CR_CTR_TIMEOUT]) return fail(CR_ERR_TIMEOUT, "a device-side wait timed out");
-        if (!ctx->last.overflow) return CR_OK;
-        if (!ctx->cfg.grow_on_overflow || (flags & CR_RENDER_NO_CLEAR))
-            return fail(CR_ERR_QUEUE_OVERFLOW, "queue overflow: nontrivial %llu/%llu, tiles %llu/%llu",
-                        (unsigned long long)ctx->last.nontrivial, (unsigned long long)ctx->ntCap,
-                        (unsigned long long)ctx->last.huge_tiles, (unsigned long long)ctx->hugeCap);
-        // the counters hold the exact demand of every queue that was fed in full
-        const uint64_t ntWant = std::max<uint64_t>(ctx->ntCap, ctx->last.nontrivial + ctx->last.nontrivial / 8 + 1024);
-        const uint64_t huWant = (ctx->last.overflow & 1)
-                                    ? ctx->hugeCap
-                                    : std::max<uint64_t>(ctx->hugeCap, ctx->last.huge_tiles + ctx->last.huge_tiles / 8 + 1024);
-        s = ensure_queues(ctx, ntWant, huWant);
-        if (s) return s;
-    }
-    return fail(CR_ERR_QUEUE_OVERFLOW, "queue overflow persisted after growing the queues");
+        return CR_OK;
+    };
+    return run_frame(ctx, flags, stream, count, A.totalTriangles, issue);
 }
 
 cr_status cr_sync(cr_context* ctx) {
@@ -708,20 +677,13 @@ cr_status cr_sync(cr_context* ctx) {
 
 cr_status cr_drain_stage_times(cr_context* ctx, cr_stage_times* out) {
     if (!ctx || !out) return fail(CR_ERR_INVALID, "cr_drain_stage_times: NULL argument");
-    memset(out, 0, sizeof(*out));
     CR_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
     while (ctx->ringCount > 0) {
-        cudaEvent_t* e = &ctx->ring[7 * ctx->ringHead];
-        CR_CUDA(cudaEventSynchronize(e[6]), "timing sync");
-        for (int i = 0; i < 6; i++) {
-            float ms = 0.0f;
-            CR_CUDA(cudaEventElapsedTime(&ms, e[i], e[i + 1]), "timing");
-            out->ms[i] += ms;
-        }
-        out->frames++;
-        ctx->ringHead = (ctx->ringHead + 1) % cr_context::kRing;
-        ctx->ringCount--;
+        cr_status s = fold_oldest(ctx);
+        if (s) return s;
     }
+    *out = ctx->folded;
+    ctx->folded = cr_stage_times{};
     return CR_OK;
 }
 

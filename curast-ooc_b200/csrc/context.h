@@ -1,0 +1,125 @@
+// context.h -- the library context and host helpers shared by api.cpp (the
+// single-view API) and batch.cpp (batched views, plans, autotuning).
+//
+// Translation units including this file are built with -ffp-contract=off:
+// world_view = view * world and the mirrored-instance determinant are formed
+// in glm's float order (libs/glm/glm/detail/type_mat4x4.inl:601-618,
+// func_geometric.inl:53-85), exactly as the reference's render host does
+// (src/CuRast_render.h:406-410) and its stage-1 kernel does
+// (src/kernels/triangles_visbuffer.cu:179-185).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <functional>
+#include <string>
+#include <vector>
+
+#include "cr_device.h"
+#include "curast_b200.h"
+
+namespace cr {
+
+cr_status fail(cr_status s, const char* fmt, ...);
+cr_status cuda_fail(cudaError_t e, const char* what);
+
+#define CR_CUDA(call, what)                                     \
+    do {                                                        \
+        cudaError_t _e = (call);                                \
+        if (_e != cudaSuccess) return ::cr::cuda_fail(_e, what); \
+    } while (0)
+
+struct MeshRec {
+    bool live = false;
+    bool owned = false;
+    float* positions = nullptr;
+    uint32_t* indices = nullptr;
+    uint32_t* colors = nullptr;
+    uint32_t numVertices = 0;
+    uint32_t numTriangles = 0;
+    size_t bytes = 0;
+};
+
+void mat4_mul(const float* a, const float* b, float* out);  // glm order
+float det3_glm(const float* m);                             // dot(cross(c0, c1), c2)
+void mat4_inverse(const float* m, float* out);              // glm::inverse order
+inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+struct Assembled {
+    std::vector<uint32_t> order;
+    std::vector<CrInstance> inst;
+    std::vector<float> worldView;   // 16 per instance
+    std::vector<float> world;       // 16 per instance
+    std::vector<CrSegment> seg;
+    uint64_t totalTriangles = 0;
+    uint64_t numItems = 0;
+    uint64_t outBytes = 0;     // vertex-pass record slots of all instances
+    uint64_t numVChunks = 0;   // vertex-pass chunks of all instances
+};
+
+}  // namespace cr
+
+struct cr_context {
+    cr_config cfg{};
+    int device = 0;
+    CrLaunchShape shape{};
+    CrBatchShape bshape{};              // occupancy maxima of the batched kernels
+    std::vector<cr::MeshRec> meshes;
+    size_t bytesInUse = 0;
+
+    // frame table: device copy + pinned staging
+    void* dFrame = nullptr;
+    size_t dFrameCap = 0;
+    void* hFrame = nullptr;
+    size_t hFrameCap = 0;
+    cudaEvent_t frameCopied = nullptr;
+    cudaEvent_t frameDone = nullptr;  // last kernel of the previous frame
+
+    // queues and per-vertex records
+    uint8_t* outcodes = nullptr;  // vertex-pass output (bytes, cells or view masks)
+    uint64_t outCap = 0;
+    uint64_t* ntList = nullptr;
+    uint64_t ntCap = 0;
+    CrTile* hugeList = nullptr;
+    uint64_t hugeCap = 0;
+    unsigned long long* counters = nullptr;
+    unsigned long long* hCounters = nullptr;  // pinned
+
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    // CR_RENDER_TIMING: a ring of event sets (7 per frame) drained on demand
+    static constexpr int kRing = 128;
+    std::vector<cudaEvent_t> ring;
+    int ringHead = 0, ringCount = 0;
+    cr_stage_times folded{};          // frames folded out of a full ring
+    cr_frame_stats last{};
+    bool pendingStats = false;
+    cudaStream_t lastStream = nullptr;
+
+    // autotuner results, one per scene class
+    std::vector<cr_tuning> tunings;
+
+    cr_status dev_alloc(void** p, size_t bytes, const char* what);
+    void dev_free(void* p, size_t bytes);
+};
+
+namespace cr {
+
+cr_status assemble(cr_context* ctx, const cr_instance* instances, uint32_t count, const float* view, uint32_t flags,
+                   Assembled& A);
+cr_status ensure_queues(cr_context* ctx, uint64_t ntWant, uint64_t hugeWant);
+// Grows the per-vertex record buffer to at least `bytes`.
+cr_status ensure_records(cr_context* ctx, uint64_t bytes);
+
+// Issues one frame.  issue(tev, rasterEnd) enqueues the stages on `stream`
+// with the context's current queues, recording tev[0..6] around them when
+// tev is non-null and rasterEnd after stage 3 when it is non-null.  This adds
+// the counter readback and statistics and, for CR_RENDER_SYNC, waits, reports
+// timeouts and overflow, and re-issues with grown queues (up to 3 attempts).
+using IssueFn = std::function<cr_status(cudaEvent_t* tev, cudaEvent_t rasterEnd)>;
+cr_status run_frame(cr_context* ctx, uint32_t flags, cudaStream_t stream, uint64_t instances, uint64_t triangles,
+                    const IssueFn& issue);
+
+const cr_tuning* find_tuning(const cr_context* ctx, uint32_t sceneClass);
+// Adds the oldest frame of the timing ring to ctx->folded (waits for it).
+cr_status fold_oldest(cr_context* ctx);
+
+}  // namespace cr

@@ -87,7 +87,7 @@ struct alignas(16) CrTile {     // HugeTriangle, HostDeviceInterface.h:254-259
 #define CR_ENTRY_INST_MASK 0x3ffffffull  // 26 bits of instance
 #define CR_MAX_VIEWS 64                  // views per batched frame (one bit each)
 
-// One view of a batched frame (single-view frames fill one).
+// One view of a batched frame.
 struct alignas(16) CrView {
     uint64_t* fb;               // visbuffer, W*H
     uint32_t* rgba;             // may be nullptr
@@ -98,13 +98,21 @@ struct alignas(16) CrView {
     float viewI[16];            // inverse(view), for the resolve
     float origin[3];
     float p00, p11;
-    uint32_t pad[3];
+    float fa;                   // f / aspect, rounded once in float
+    uint32_t resolveBlockBase;  // first block of this view in the resolve grid
+    uint32_t pad;
 };
+static_assert(sizeof(CrView) == 144, "CrView layout");
 
-// Multi-view vertex record: per frustum predicate one bit per view.
-struct alignas(8) CrViewMasks {
-    unsigned long long behind, right, left, top, bottom;
+// Multi-view vertex record (48 bytes, read as three 16-byte loads): per
+// frustum predicate of vertex_outcode one bit per view.  BEHIND bits are
+// exact; side bits may be a subset of the exact ones (a chunk classified as a
+// whole records only the side that proves it outside), which keeps every cull
+// derived from them sound.
+struct alignas(16) CrViewMasks {
+    unsigned long long behind, right, left, top, bottom, pad;
 };
+static_assert(sizeof(CrViewMasks) == 48, "CrViewMasks layout");
 
 struct CrFrameParams {
     const CrInstance* instances;
@@ -135,6 +143,7 @@ struct CrFrameParams {
     uint32_t numViews;
     uint32_t cellMode;          // 1: the vertex pass writes 8-byte cell records
     CrViewMasks* viewMasks;     // CrInstance::outBase + vertex
+    const uint32_t* flips;      // numViews * numInstances, view-major
 };
 
 struct CrResolveParams {
@@ -169,17 +178,27 @@ int cr_launch_stage2(const CrFrameParams& p, const CrLaunchShape& s, void* strea
 int cr_launch_stage3(const CrFrameParams& p, const CrLaunchShape& s, void* stream);
 int cr_launch_resolve(const CrResolveParams& p, void* stream);
 
-// Batched (multi-view) frame: one launch per stage over all views.
+// Batched (multi-view) frame: one launch per stage over all views.  Grid
+// sizes are chosen by the host (defaults from occupancy, or tuned).
 struct CrBatchShape {
-    int vertexBlocks, stage1Blocks, stage2Blocks, stage3Blocks;  // persistent grids
+    int numSMs;
+    int vertexBlocks;           // k_vertex_views, 256 threads each
+    int stage1Blocks;           // k_stage1_views, stage1Warps warps each
+    int stage2Blocks;           // k_stage2<MULTI>, stage2Warps warps each
+    int stage3Blocks;           // k_stage3<MULTI>, 8 warps each
+    int stage1Warps;            // 4 or 8
+    int stage2Warps;            // 4 or 8
 };
-int cr_launch_clear_views(const CrFrameParams& p, int maxPixels, void* stream);
+int cr_query_batch_shape(int device, CrBatchShape* out);  // occupancy maxima
+int cr_launch_clear_views(const CrFrameParams& p, uint64_t maxPixels, void* stream);
 int cr_launch_vertex_views(const CrFrameParams& p, const CrBatchShape& s, void* stream);
 int cr_launch_stage1_views(const CrFrameParams& p, const CrBatchShape& s, void* stream);
 int cr_launch_stage2_views(const CrFrameParams& p, const CrBatchShape& s, void* stream);
 int cr_launch_stage3_views(const CrFrameParams& p, const CrBatchShape& s, void* stream);
-int cr_launch_resolve_views(const CrFrameParams& p, int32_t display, int maxW, int maxH, void* stream);
-int cr_query_batch_shape(int device, CrBatchShape* out);
+// numBlocks: sum over views of ceil(W / 32) * ceil(H / 32); each view's
+// CrView::resolveBlockBase is the prefix sum of the preceding views' blocks.
+int cr_launch_resolve_views(const CrResolveParams& base, const CrView* views, uint32_t numViews, uint32_t numBlocks,
+                            void* stream);
 
 // Host helpers implemented in api.cpp.
 void cr_internal_set_error(const char* msg);

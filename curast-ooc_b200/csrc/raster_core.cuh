@@ -1,0 +1,858 @@
+// raster_core.cuh -- device code shared by the single-view kernels
+// (raster.cu) and the batched multi-view kernels (views.cu): glm-order
+// arithmetic, the reference's per-triangle stage-1 path, the stage-2 setup and
+// fragment loop, the stage-3 tile ray tracer and the bulk-copy primitives.
+//
+// Float semantics: every file including this one is compiled with
+// -fmad=false -prec-div=true -prec-sqrt=true -ftz=false, and every expression
+// keeps the reference's operation order (glm's for vector/matrix products).
+// The reference's fast-math reciprocals (__fdividef, tv.cu:206-211,249) are
+// IEEE divisions here.  With contraction off and IEEE division, each
+// triangle's coverage and depth are pure functions of the inputs, and the
+// visbuffer (an atomic 64-bit minimum over a fixed fragment set) is
+// independent of how the work is scheduled.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "cr_device.h"
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+struct V2 {
+    float x, y;
+};
+struct V3 {
+    float x, y, z;
+};
+
+// ---------------------------------------------------------------------------
+// glm-order arithmetic (libs/glm/glm/detail/type_mat4x4.inl:532-543,
+// func_geometric.inl:53-85) and the reference helpers
+// (src/kernels/rasterization_helpers.cuh)
+// ---------------------------------------------------------------------------
+struct Mat {
+    float4 c0, c1, c2, c3;
+};
+
+__device__ __forceinline__ Mat load_mat(const float4* m) {
+    Mat r;
+    r.c0 = __ldg(m + 0);
+    r.c1 = __ldg(m + 1);
+    r.c2 = __ldg(m + 2);
+    r.c3 = __ldg(m + 3);
+    return r;
+}
+
+// mat4 * vec4(p, 1) -> vec3: (m0*x + m1*y) + (m2*z + m3*1)
+__device__ __forceinline__ V3 xform(const Mat& m, const V3 p) {
+    V3 r;
+    r.x = (m.c0.x * p.x + m.c1.x * p.y) + (m.c2.x * p.z + m.c3.x * 1.0f);
+    r.y = (m.c0.y * p.x + m.c1.y * p.y) + (m.c2.y * p.z + m.c3.y * 1.0f);
+    r.z = (m.c0.z * p.x + m.c1.z * p.y) + (m.c2.z * p.z + m.c3.z * 1.0f);
+    return r;
+}
+
+__device__ __forceinline__ V3 sub3(V3 a, V3 b) { return V3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ float dot3(V3 a, V3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+__device__ __forceinline__ V3 cross3(V3 x, V3 y) {
+    return V3{x.y * y.z - y.y * x.z, x.z * y.x - y.z * x.x, x.x * y.y - y.x * x.y};
+}
+
+// helpers:95-101, with fa = f / aspect evaluated once
+__device__ __forceinline__ V3 to_ndc(V3 v, float fa, float f) {
+    float depth = -v.z;
+    return V3{(fa * v.x) / depth, (f * v.y) / depth, depth};
+}
+
+// helpers:103-108
+__device__ __forceinline__ V2 to_screen(V3 ndc, float w, float h) {
+    return V2{(ndc.x * 0.5f + 0.5f) * w, (ndc.y * 0.5f + 0.5f) * h};
+}
+
+// utils.cuh:205-213
+__device__ __forceinline__ float clamp_ref(float v, float lo, float hi) {
+    if (v < lo) return lo;
+    if (v > hi) return hi;
+    return v;
+}
+
+// helpers:35-52: 28-bit depth above a 36-bit triangle id
+__device__ __forceinline__ uint64_t pack_pixel(float depth, uint64_t id) {
+    uint32_t bits = __float_as_uint(depth);
+    uint32_t ud = ((bits & 0x7FFFFFFFu) == 0x7F800000u) ? 0x7FFFFFF8u : (bits & 0x7FFFFFF8u);
+    return ((uint64_t)ud << 33) | id;
+}
+
+__device__ __forceinline__ void fb_min(uint64_t* fb, uint32_t pid, uint64_t v) {
+    atomicMin(reinterpret_cast<unsigned long long*>(fb + pid), (unsigned long long)v);
+}
+
+// read-only load of a pointer field
+template <typename T>
+__device__ __forceinline__ T* ldg_ptr(T* const* p) {
+    return reinterpret_cast<T*>(__ldg(reinterpret_cast<const unsigned long long*>(p)));
+}
+
+__device__ __forceinline__ V3 load_pos(const float* pos, uint32_t idx) {
+    const float* q = pos + 3ull * idx;
+    return V3{__ldg(q), __ldg(q + 1), __ldg(q + 2)};
+}
+
+// ---------------------------------------------------------------------------
+// mbarrier / bulk-copy primitives (PTX ISA 8.x)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_barrier_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Waits for the given phase parity, giving up after timeout_ns.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint64_t timeout_ns) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = globaltimer_ns();
+    while (true) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (globaltimer_ns() - t0 > timeout_ns) return false;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Stage 1: one (triangle, instance) -- tv.cu:82-271
+// ---------------------------------------------------------------------------
+enum : int { S1_CULL = 0, S1_DONE = 1, S1_QUEUE = 2 };
+
+// fl(X / d) > 1 for d > 0 without the division.  With round-to-nearest-even,
+// fl(q) > 1 iff q > 1 + 2^-24, i.e. X - d > d * 2^-24.  Outside (d/2, 2d) the
+// answer is plain; inside, X - d is exact (Sterbenz) and d * 2^-24 is exact
+// for d >= 1e-30, so the comparison is exact.  Tiny, huge or NaN d divide.
+__device__ __forceinline__ bool ndc_beyond(float X, float d) {
+    if (!(d >= 1e-30f && d <= 1e30f)) return X / d > 1.0f;
+    if (X >= 2.0f * d) return true;
+    if (X <= 0.5f * d) return false;
+    return (X - d) > d * 5.9604644775390625e-8f;
+}
+
+// The render target of one view: visbuffer, size and projection.
+struct Target {
+    uint64_t* fb;
+    int32_t W, H;
+    float f, fa;  // proj[1][1] and f / aspect
+    uint32_t thrSmall;
+};
+
+__device__ __forceinline__ Target target_of(const CrFrameParams& p) {
+    return Target{p.fb, p.W, p.H, p.f, p.f / p.aspect, p.thrSmall};
+}
+
+__device__ __forceinline__ Target target_of(const CrFrameParams& p, uint32_t view) {
+    // fa is f / aspect rounded once in float on the host: the same value
+    // target_of(p) forms on the device
+    const CrView* v = p.views + view;
+    return Target{ldg_ptr(&v->fb), __ldg(&v->W), __ldg(&v->H), __ldg(&v->f), __ldg(&v->fa), p.thrSmall};
+}
+
+__device__ __forceinline__ int stage1_triangle(const Target& p, const float fa, const Mat& M,
+                                               const uint32_t flip, const V3 pa, const V3 pb, const V3 pc,
+                                               const uint64_t id) {
+    const float f = p.f;
+    const V3 av = xform(M, pa);
+    const V3 bv = xform(M, pb);
+    const V3 cv = xform(M, pc);
+    // The reference's culls (all behind, frustum sides, sample miss, back
+    // face) have no side effects, so any order gives the same outcome; the
+    // ones that need no division run first.
+    const float da = -av.z, db = -bv.z, dc = -cv.z;
+    if (da <= 0.0f && db <= 0.0f && dc <= 0.0f) return S1_CULL;  // tv.cu:119
+    {  // tv.cu:168-188
+        const V3 N = cross3(sub3(bv, av), sub3(cv, av));
+        float res = dot3(av, N);
+        if (flip) res = -res;
+        if (res >= 0.0f) return S1_CULL;
+    }
+    bool nontrivial = (da <= 0.0f || db <= 0.0f || dc <= 0.0f);
+    const float Xa = fa * av.x, Xb = fa * bv.x, Xc = fa * cv.x;
+    const float Ya = f * av.y, Yb = f * bv.y, Yc = f * cv.y;
+    if (!nontrivial) {  // tv.cu:113-118, on fl(X/d) without dividing
+        if (ndc_beyond(Xa, da) && ndc_beyond(Xb, db) && ndc_beyond(Xc, dc)) return S1_CULL;
+        if (ndc_beyond(-Xa, da) && ndc_beyond(-Xb, db) && ndc_beyond(-Xc, dc)) return S1_CULL;
+        if (ndc_beyond(Ya, da) && ndc_beyond(Yb, db) && ndc_beyond(Yc, dc)) return S1_CULL;
+        if (ndc_beyond(-Ya, da) && ndc_beyond(-Yb, db) && ndc_beyond(-Yc, dc)) return S1_CULL;
+    }
+    const V3 an = {Xa / da, Ya / da, da};  // viewToNDC, helpers:95-101
+    const V3 bn = {Xb / db, Yb / db, db};
+    const V3 cn = {Xc / dc, Yc / dc, dc};
+
+    const float Wf = (float)p.W, Hf = (float)p.H;
+    V2 as = to_screen(an, Wf, Hf);
+    V2 bs = to_screen(bn, Wf, Hf);
+    V2 cs = to_screen(cn, Wf, Hf);
+    as.x -= 0.5f; as.y -= 0.5f;
+    bs.x -= 0.5f; bs.y -= 0.5f;
+    cs.x -= 0.5f; cs.y -= 0.5f;
+
+    float min_x = fminf(as.x, fminf(bs.x, cs.x));
+    float max_x = fmaxf(as.x, fmaxf(bs.x, cs.x));
+    float min_y = fminf(as.y, fminf(bs.y, cs.y));
+    float max_y = fmaxf(as.y, fmaxf(bs.y, cs.y));
+    min_x = fmaxf(min_x, 0.0f);
+    max_x = fminf(max_x, (float)(p.W - 1));
+    min_y = fmaxf(min_y, 0.0f);
+    max_y = fminf(max_y, (float)(p.H - 1));
+
+    if (!nontrivial) {  // tv.cu:153-158, SAMPLE_OFFSET = 0
+        const float sx = floorf(min_x);
+        const float sy = floorf(min_y);
+        if (min_x > sx + 0.0f && max_x < sx + 1.0f + 0.0f) return S1_CULL;
+        if (min_y > sy + 0.0f && max_y < sy + 1.0f + 0.0f) return S1_CULL;
+    }
+
+    // tv.cu:162-166; the count is compared unsigned, as in the reference
+    const int size_x = (int)(ceilf(max_x) - ceilf(min_x));
+    const int size_y = (int)(ceilf(max_y) - ceilf(min_y));
+    const uint32_t numFragments = (uint32_t)size_x * (uint32_t)size_y;
+    if (numFragments > p.thrSmall) nontrivial = true;
+    if (nontrivial) return S1_QUEUE;
+
+    const V2 v_ab = {bs.x - as.x, bs.y - as.y};
+    const V2 v_ac = {cs.x - as.x, cs.y - as.y};
+    const float factor = 1.0f / (v_ab.x * v_ac.y - v_ab.y * v_ac.x);
+    const float iza = 1.0f / an.z;
+    const float izb = 1.0f / bn.z;
+    const float izc = 1.0f / cn.z;
+    const float ds_dx = v_ac.y * factor;
+    const float ds_dy = -v_ac.x * factor;
+    const float dt_dx = -v_ab.y * factor;
+    const float dt_dy = v_ab.x * factor;
+    const float start_x = ceilf(min_x);
+    const float start_y = ceilf(min_y);
+    const float s0x = start_x - as.x + 0.0f;
+    const float s0y = start_y - as.y + 0.0f;
+    float s_row = (s0x * v_ac.y - s0y * v_ac.x) * factor;
+    float t_row = (v_ab.x * s0y - v_ab.y * s0x) * factor;
+    int row_pid = (int)start_x + p.W * (int)start_y;
+    const uint32_t numPixels = (uint32_t)p.W * (uint32_t)p.H;
+    for (int fy = 0; fy < size_y; ++fy) {
+        float s = s_row;
+        float t = t_row;
+        int pid = row_pid;
+        for (int fx = 0; fx < size_x; ++fx) {
+            const float v = 1.0f - (s + t);
+            if (s > 0.0f && t > 0.0f && v > 0.0f && (uint32_t)pid < numPixels) {
+                const float inv_depth = v * iza + s * izb + t * izc;
+                const float depth = 1.0f / inv_depth;
+                fb_min(p.fb, (uint32_t)pid, pack_pixel(depth, id));
+            }
+            s += ds_dx;
+            t += dt_dx;
+            pid++;
+        }
+        s_row += ds_dy;
+        t_row += dt_dy;
+        row_pid += p.W;
+    }
+    return S1_DONE;
+}
+
+
+// ---------------------------------------------------------------------------
+// Vertex pass: one thread per (instance, vertex).  It evaluates the per-vertex
+// halves of stage 1's culls -- "behind the camera" and the four frustum sides
+// on fl(X / depth), the latter exactly without dividing -- into one byte, so
+// stage 1 can drop the (typically many) triangles all of whose vertices lie
+// behind one side from three gathered bytes, without fetching positions.
+// The transform is stage 1's own (same function, same M), so the predicates
+// are bit-identical to the ones the reference evaluates per triangle.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t vertex_outcode(const Mat& M, V3 p, float fa, float f) {
+    const V3 q = xform(M, p);
+    const float d = -q.z;
+    if (d <= 0.0f) return CR_OC_BEHIND;
+    const float X = fa * q.x, Y = f * q.y;
+    return (ndc_beyond(X, d) ? CR_OC_RIGHT : 0u) | (ndc_beyond(-X, d) ? CR_OC_LEFT : 0u) |
+           (ndc_beyond(Y, d) ? CR_OC_TOP : 0u) | (ndc_beyond(-Y, d) ? CR_OC_BOTTOM : 0u);
+}
+
+// Cell record of one vertex: the outcode plus stage 1's own screen position
+// (viewToNDC, ndcToScreen, -0.5: tv.cu:106-108,121-134, same operations in
+// the same order) reduced to its pixel cell.
+__device__ __forceinline__ uint64_t vertex_cell_record(const Mat& M, V3 p, float fa, float f, float Wf, float Hf,
+                                                       int W, int H) {
+    const V3 q = xform(M, p);
+    const float d = -q.z;
+    if (d <= 0.0f) return CR_OC_BEHIND;
+    const float X = fa * q.x, Y = f * q.y;
+    uint64_t rec = (ndc_beyond(X, d) ? CR_OC_RIGHT : 0u) | (ndc_beyond(-X, d) ? CR_OC_LEFT : 0u) |
+                   (ndc_beyond(Y, d) ? CR_OC_TOP : 0u) | (ndc_beyond(-Y, d) ? CR_OC_BOTTOM : 0u);
+    const V2 s = to_screen(V3{X / d, Y / d, d}, Wf, Hf);
+    const float sx = s.x - 0.5f, sy = s.y - 0.5f;
+    if (sx >= 0.0f && sx <= (float)(W - 1) && sy >= 0.0f && sy <= (float)(H - 1)) {
+        const float fx = floorf(sx), fy = floorf(sy);
+        rec |= CR_CELL_INSIDE | (sx > fx ? CR_CELL_FRACX : 0ull) | (sy > fy ? CR_CELL_FRACY : 0ull) |
+               ((uint64_t)(uint32_t)(int)fx << 16) | ((uint64_t)(uint32_t)(int)fy << 32);
+    }
+    return rec;
+}
+
+struct Item {
+    uint32_t seg;
+    uint32_t batch;
+    uint32_t chunk;
+};
+
+__device__ __forceinline__ Item decode_item(const CrFrameParams& p, uint64_t item) {
+    uint32_t lo = 0, hi = p.numSegments - 1;
+    while (lo < hi) {  // last segment whose itemBase <= item
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (__ldg(&p.segments[mid].itemBase) <= item) lo = mid;
+        else hi = mid - 1;
+    }
+    Item it;
+    it.seg = lo;
+    const uint64_t rem = item - __ldg(&p.segments[lo].itemBase);
+    const uint32_t nb = __ldg(&p.segments[lo].numBatches);
+    if (rem < nb) {  // first (often only) instance chunk: no division
+        it.chunk = 0;
+        it.batch = (uint32_t)rem;
+    } else if (rem <= 0xffffffffull) {
+        it.chunk = (uint32_t)rem / nb;
+        it.batch = (uint32_t)rem - it.chunk * nb;
+    } else {
+        it.chunk = (uint32_t)(rem / nb);
+        it.batch = (uint32_t)(rem - (uint64_t)it.chunk * nb);
+    }
+    return it;
+}
+
+// A full 32-triangle index tile of a 16-byte aligned index array is fetched by
+// TMA; tails and non-indexed meshes are read directly.
+__device__ __forceinline__ bool item_uses_tma(const CrSegment* sg, uint32_t batch) {
+    return (__ldg(&sg->flags) & 1u) && (uint64_t)(batch + 1) * CR_BATCH <= __ldg(&sg->numTriangles);
+}
+
+constexpr int S1_STAGES = 3;
+constexpr int S1_R = CR_BATCH / 32;  // triangles per lane per work item
+
+
+// ---------------------------------------------------------------------------
+// Stage 2 setup -- tv.cu:418-471 with computeScreenSpaceBoundingBox and
+// SutherlandHodgman::windowClipping (helpers:126-210, 350-460)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool sh_inside(V2 p, int e) {
+    // edges: x > -1, x < 1, y > -1, y < 1 written as sign*val >= sign*value
+    switch (e) {
+        case 0: return 1.0f * p.x >= 1.0f * -1.0f;
+        case 1: return -1.0f * p.x >= -1.0f * 1.0f;
+        case 2: return 1.0f * p.y >= 1.0f * -1.0f;
+        default: return -1.0f * p.y >= -1.0f * 1.0f;
+    }
+}
+
+__device__ __forceinline__ V2 sh_intersect(V2 p1, V2 p2, int e) {
+    const float value = (e == 0 || e == 2) ? -1.0f : 1.0f;
+    if (e < 2) {
+        const float t = (value - p1.x) / (p2.x - p1.x);
+        return V2{value, p1.y + t * (p2.y - p1.y)};
+    }
+    const float t = (value - p1.y) / (p2.y - p1.y);
+    return V2{p1.x + t * (p2.x - p1.x), value};
+}
+
+__device__ void window_clip(V2 a, V2 b, V2 c, V2& bmin, V2& bmax) {
+    V2 buf[2][8];
+    int cur = 0;
+    buf[0][0] = a;
+    buf[0][1] = b;
+    buf[0][2] = c;
+    int inCount = 3;
+    for (int e = 0; e < 4; e++) {
+        if (inCount == 0) break;
+        int outCount = 0;
+        V2 S = buf[cur][inCount - 1];
+        for (int i = 0; i < inCount; i++) {
+            const V2 E = buf[cur][i];
+            const bool Ein = sh_inside(E, e);
+            const bool Sin = sh_inside(S, e);
+            if (Ein) {
+                if (!Sin) buf[cur ^ 1][outCount++] = sh_intersect(S, E, e);
+                buf[cur ^ 1][outCount++] = E;
+            } else if (Sin) {
+                buf[cur ^ 1][outCount++] = sh_intersect(S, E, e);
+            }
+            S = E;
+        }
+        cur ^= 1;
+        inCount = outCount;
+    }
+    for (int i = 0; i < inCount; i++) {
+        const V2 q = buf[cur][i];
+        bmin.x = fminf(bmin.x, q.x);
+        bmin.y = fminf(bmin.y, q.y);
+        bmax.x = fmaxf(bmax.x, q.x);
+        bmax.y = fmaxf(bmax.y, q.y);
+    }
+}
+
+__device__ __forceinline__ V3 intersect_near(V3 p1, V3 p2) {
+    const float t = (-0.01f - p1.z) / (p2.z - p1.z);
+    const V3 d = sub3(p2, p1);
+    return V3{p1.x + t * d.x, p1.y + t * d.y, p1.z + t * d.z};
+}
+
+__device__ __forceinline__ V2 xy(V3 v) { return V2{v.x, v.y}; }
+
+// Returns false for all-behind triangles (unreachable: stage 1 culls them).
+__device__ bool screen_bbox(V3 an, V3 bn, V3 cn, V3 av, V3 bv, V3 cv, float fa, float f, float width,
+                            float height, float& min_x, float& max_x, float& min_y, float& max_y) {
+    V2 bmin = {1e10f, 1e10f};
+    V2 bmax = {-1e10f, -1e10f};
+    const int mask = (an.z <= 0.0f ? 1 : 0) | (bn.z <= 0.0f ? 2 : 0) | (cn.z <= 0.0f ? 4 : 0);
+    if (mask == 7) return false;
+    if (mask == 0) {
+        window_clip(xy(an), xy(bn), xy(cn), bmin, bmax);
+    } else {
+        V3 v0, v1, v2;
+        if (mask == 1 || mask == 6) { v0 = av; v1 = bv; v2 = cv; }
+        else if (mask == 2 || mask == 5) { v0 = bv; v1 = cv; v2 = av; }
+        else { v0 = cv; v1 = av; v2 = bv; }
+        const V3 I1 = intersect_near(v0, v1);
+        const V3 I2 = intersect_near(v0, v2);
+        if (mask == 1 || mask == 2 || mask == 4) {
+            const V2 p0 = xy(to_ndc(v1, fa, f));
+            const V2 p1 = xy(to_ndc(v2, fa, f));
+            const V2 pI1 = xy(to_ndc(I1, fa, f));
+            const V2 pI2 = xy(to_ndc(I2, fa, f));
+            window_clip(p0, p1, pI1, bmin, bmax);
+            window_clip(pI1, p1, pI2, bmin, bmax);
+        } else {
+            window_clip(xy(to_ndc(v0, fa, f)), xy(to_ndc(I1, fa, f)), xy(to_ndc(I2, fa, f)), bmin, bmax);
+        }
+    }
+    bmin.x = clamp_ref(bmin.x, -1.0f, 1.0f);
+    bmax.x = clamp_ref(bmax.x, -1.0f, 1.0f);
+    bmin.y = clamp_ref(bmin.y, -1.0f, 1.0f);
+    bmax.y = clamp_ref(bmax.y, -1.0f, 1.0f);
+    const float halfW = width * 0.5f;
+    const float halfH = height * 0.5f;
+    min_x = bmin.x * halfW + halfW;
+    min_y = bmin.y * halfH + halfH;
+    max_x = bmax.x * halfW + halfW;
+    max_y = bmax.y * halfH + halfH;
+    return true;
+}
+
+enum : int { S2_SKIP = 0, S2_RASTER = 1, S2_TILES = 2 };
+
+struct S2Setup {
+    float min_x, min_y, max_x, max_y;
+    float asx, asy, abx, aby, acx, acy;
+    float inv_det, iza, izb, izc;
+    int size_x, numFragments;
+    uint32_t id32;
+};
+
+__device__ __forceinline__ int stage2_setup(const CrFrameParams& p, const Target& t, uint64_t packed, S2Setup& o) {
+    const uint32_t view = (uint32_t)(packed >> CR_ENTRY_VIEW_SHIFT);
+    const uint32_t inst = (uint32_t)((packed >> 32) & CR_ENTRY_INST_MASK);
+    const uint32_t tri = (uint32_t)(packed & 0xffffffffu);
+    const CrInstance* I = p.instances + inst;
+    // tv.cu:414,424,519: the cumulative count is held in 32 bits
+    const uint32_t cum32 = (uint32_t)__ldg(&I->cum);
+    const Mat M = load_mat(p.world_view + 4ull * ((uint64_t)view * p.numInstances + inst));
+    const float fa = t.fa;
+    const uint32_t* ix = ldg_ptr(&I->indices);
+    const float* pos = ldg_ptr(&I->positions);
+    uint32_t i0, i1, i2;
+    if (ix) {
+        i0 = __ldg(ix + 3ull * tri + 0);
+        i1 = __ldg(ix + 3ull * tri + 1);
+        i2 = __ldg(ix + 3ull * tri + 2);
+    } else {
+        i0 = 3 * tri + 0;
+        i1 = 3 * tri + 1;
+        i2 = 3 * tri + 2;
+    }
+    const float f = t.f;
+    const V3 av = xform(M, load_pos(pos, i0));
+    const V3 bv = xform(M, load_pos(pos, i1));
+    const V3 cv = xform(M, load_pos(pos, i2));
+    const V3 an = to_ndc(av, fa, f);
+    const V3 bn = to_ndc(bv, fa, f);
+    const V3 cn = to_ndc(cv, fa, f);
+    const float Wf = (float)t.W, Hf = (float)t.H;
+    float min_x, max_x, min_y, max_y;
+    if (!screen_bbox(an, bn, cn, av, bv, cv, fa, f, Wf, Hf, min_x, max_x, min_y, max_y)) return S2_SKIP;
+    min_x -= 0.5f;
+    min_y -= 0.5f;
+    max_x += 0.5f;
+    max_y += 0.5f;
+    const V2 as = to_screen(an, Wf, Hf);
+    const V2 bs = to_screen(bn, Wf, Hf);
+    const V2 cs = to_screen(cn, Wf, Hf);
+    o.abx = bs.x - as.x;
+    o.aby = bs.y - as.y;
+    o.acx = cs.x - as.x;
+    o.acy = cs.y - as.y;
+    o.inv_det = 1.0f / (o.abx * o.acy - o.aby * o.acx);
+    o.size_x = (int)ceilf(max_x) - (int)floorf(min_x);
+    const int size_y = (int)ceilf(max_y) - (int)floorf(min_y);
+    o.numFragments = (int)((uint32_t)o.size_x * (uint32_t)size_y);
+    o.min_x = min_x;
+    o.min_y = min_y;
+    o.max_x = max_x;
+    o.max_y = max_y;
+    o.asx = as.x;
+    o.asy = as.y;
+    o.id32 = cum32 + tri;
+    if (min_x >= max_x || min_y >= max_y) return S2_SKIP;
+    if (o.numFragments >= (int)p.thrLarge || an.z <= 0.0f || bn.z <= 0.0f || cn.z <= 0.0f) return S2_TILES;
+    o.iza = 1.0f / an.z;
+    o.izb = 1.0f / bn.z;
+    o.izc = 1.0f / cn.z;
+    return S2_RASTER;
+}
+
+// Narrows one bounding-box row (pixel row py, columns start_x + [0, size_x))
+// to [xlo, xlo + len): every column outside it provably fails the float test
+// of tv.cu:539-547, so skipping it cannot change the visbuffer.
+//
+// With u = 2^-24 and the setup values taken as exact inputs, the float
+// results of
+//     s = (fl(fl(px - asx) + .5) * acy - fl(fl(py - asy) + .5) * acx) * inv_det
+// (and t, v = 1 - (s + t) likewise) differ from the real-valued affine
+// functions S, T, V = 1 - S - T by at most
+//     |s_f - S| <= u |inv_det| (|acy| (5.1|ax| + 2.4) + |acx| (5.1|ay| + 2.4)) * 1.001
+// (ax = px - asx, ay = py - asy; a standard first-order bound on the two
+// roundings of sx, the two products, the difference and the final product),
+// and |v_f - V| <= |s_f - S| + |t_f - T| + 2u (1 + |S| + |T|).  The margins
+// below over-cover these by 3x, in double precision, over the whole row; a
+// column whose S, T or V is below minus its margin cannot pass.  Non-finite
+// setups keep the whole row.
+__device__ __forceinline__ void row_span(float start_x, float py, int size_x, float asx, float asy, float abx,
+                                         float aby, float acx, float acy, float inv_det, int& xlo, int& len) {
+    xlo = 0;
+    len = size_x;
+    const double u = 5.9604644775390625e-08;
+    const double di = (double)inv_det;
+    const double px0 = (double)start_x, px1 = (double)start_x + (double)(size_x - 1);
+    const double c0 = 0.5 - (double)asx;  // sx = px + c0 (exactly, in reals)
+    const double ay = (double)py - (double)asy;
+    const double sy = ay + 0.5;
+    const double AX = fmax(fabs(px0 - (double)asx), fabs(px1 - (double)asx)) + 1.0;
+    const double AY = fabs(ay) + 1.0;
+    const double aS = (double)acy * di, bS = (c0 * (double)acy - sy * (double)acx) * di;
+    const double aT = -(double)aby * di, bT = ((double)abx * sy - (double)aby * c0) * di;
+    const double aV = -(aS + aT), bV = 1.0 - bS - bT;
+    const double Smax = fmax(fabs(aS * px0 + bS), fabs(aS * px1 + bS));
+    const double Tmax = fmax(fabs(aT * px0 + bT), fabs(aT * px1 + bT));
+    const double adi = fabs(di);
+    const double Es = 16.0 * u * adi * (fabs((double)acy) * AX + fabs((double)acx) * AY) + 4.0 * u * Smax + 1e-37;
+    const double Et = 16.0 * u * adi * (fabs((double)abx) * AY + fabs((double)aby) * AX) + 4.0 * u * Tmax + 1e-37;
+    const double Ev = 2.0 * (Es + Et) + 4.0 * u * (Smax + Tmax + 1.0) + 1e-37;
+    double lo = px0, hi = px1;
+    bool empty = false;
+    // keep px with a*px + b >= -E; NaN bounds leave lo/hi unchanged
+    auto keep = [&](double a, double b, double E) {
+        if (a > 0.0) lo = fmax(lo, (-E - b) / a);
+        else if (a < 0.0) hi = fmin(hi, (-E - b) / a);
+        else if (b < -E) empty = true;
+    };
+    keep(aS, bS, Es);
+    keep(aT, bT, Et);
+    keep(aV, bV, Ev);
+    if (empty) {
+        len = 0;
+        return;
+    }
+    double flo = floor(lo - px0) - 1.0;
+    double fhi = ceil(hi - px0) + 1.0;
+    flo = fmax(flo, 0.0);
+    fhi = fmin(fhi, (double)(size_x - 1));
+    if (!(flo <= fhi)) {
+        if (flo > fhi) len = 0;  // NaN keeps the whole row
+        return;
+    }
+    xlo = (int)flo;
+    len = (int)(fhi - flo) + 1;
+}
+
+// MULTI: entries carry their view (batched frames); otherwise view 0 is the
+// frame's single target.
+template <int WARPS, bool MULTI>
+__global__ void __launch_bounds__(WARPS * 32) k_stage2(const CrFrameParams p) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t gw = (uint64_t)blockIdx.x * WARPS + (threadIdx.x >> 5);
+    const uint64_t nw = (uint64_t)gridDim.x * WARPS;
+    const uint64_t count = min((uint64_t)p.counters[CR_CTR_NONTRIVIAL], p.ntCap);
+
+    // group size: 32 queued triangles per warp step when the queue is long,
+    // fewer when it is short so that every warp gets work
+    uint64_t G = (count + nw - 1) / nw;
+    G = G < 1 ? 1 : (G > 32 ? 32 : G);
+    for (uint64_t g = gw; g * G < count; g += nw) {
+        const uint64_t e = g * G + lane;
+        const bool mine = lane < (int)G && e < count;
+        const uint64_t packed = mine ? p.ntList[e] : 0ull;
+        const uint32_t view = MULTI ? (uint32_t)(packed >> CR_ENTRY_VIEW_SHIFT) : 0u;
+        const Target tg = MULTI ? target_of(p, view) : target_of(p);
+        S2Setup su;
+        int kind = S2_SKIP;
+        if (mine) kind = stage2_setup(p, tg, packed, su);
+
+        // ---- tiles: tv.cu:494-514, one atomic per warp --------------------
+        int tile_x = 0, tile_y = 0, tiles_x = 1;
+        uint32_t numTiles = 0;
+        if (kind == S2_TILES) {
+            tile_x = (int)su.min_x / CR_TILE_SIZE;
+            tile_y = (int)su.min_y / CR_TILE_SIZE;
+            tiles_x = ((int)su.max_x + CR_TILE_SIZE - 1) / CR_TILE_SIZE - tile_x;
+            const int tiles_y = ((int)su.max_y + CR_TILE_SIZE - 1) / CR_TILE_SIZE - tile_y;
+            numTiles = (uint32_t)tiles_x * (uint32_t)tiles_y;
+        }
+        uint32_t incl = numTiles;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t v = __shfl_up_sync(FULL, incl, d);
+            if (lane >= d) incl += v;
+        }
+        const uint32_t total = __shfl_sync(FULL, incl, 31);
+        if (total) {
+            unsigned long long base = 0;
+            if (lane == 0) base = atomicAdd(&p.counters[CR_CTR_HUGE], (unsigned long long)total);
+            base = __shfl_sync(FULL, base, 0);
+            const uint64_t mine = base + (incl - numTiles);
+            unsigned tmask = __ballot_sync(FULL, numTiles != 0);
+            while (tmask) {
+                const int j = __ffs(tmask) - 1;
+                tmask &= tmask - 1;
+                const uint32_t nT = __shfl_sync(FULL, numTiles, j);
+                const uint64_t b = __shfl_sync(FULL, mine, j);
+                const int tx = __shfl_sync(FULL, tile_x, j);
+                const int ty = __shfl_sync(FULL, tile_y, j);
+                const int tsx = __shfl_sync(FULL, tiles_x, j);
+                const uint64_t pk = __shfl_sync(FULL, packed, j);
+                for (uint32_t i = lane; i < nT; i += 32) {
+                    const uint64_t slot = b + i;
+                    if (slot < p.hugeCap) {
+                        CrTile t;
+                        t.instance = (int32_t)(((pk >> 32) & CR_ENTRY_INST_MASK) |
+                                               ((pk >> CR_ENTRY_VIEW_SHIFT) << 26));
+                        t.triangle = (int32_t)(pk & 0xffffffffu);
+                        t.tile_x = tx + (int)(i % (uint32_t)tsx);
+                        t.tile_y = ty + (int)(i / (uint32_t)tsx);
+                        p.hugeList[slot] = t;
+                    } else {
+                        atomicOr(&p.counters[CR_CTR_OVERFLOW], 2ull);
+                    }
+                }
+            }
+        }
+
+        // ---- fragments: tv.cu:516-561, lanes stride each triangle ---------
+        unsigned rmask = __ballot_sync(FULL, kind == S2_RASTER);
+        while (rmask) {
+            const int j = __ffs(rmask) - 1;
+            rmask &= rmask - 1;
+            const float min_x = __shfl_sync(FULL, su.min_x, j);
+            const float min_y = __shfl_sync(FULL, su.min_y, j);
+            const float asx = __shfl_sync(FULL, su.asx, j);
+            const float asy = __shfl_sync(FULL, su.asy, j);
+            const float abx = __shfl_sync(FULL, su.abx, j);
+            const float aby = __shfl_sync(FULL, su.aby, j);
+            const float acx = __shfl_sync(FULL, su.acx, j);
+            const float acy = __shfl_sync(FULL, su.acy, j);
+            const float inv_det = __shfl_sync(FULL, su.inv_det, j);
+            const float iza = __shfl_sync(FULL, su.iza, j);
+            const float izb = __shfl_sync(FULL, su.izb, j);
+            const float izc = __shfl_sync(FULL, su.izc, j);
+            const int size_x = __shfl_sync(FULL, su.size_x, j);
+            const int nf = __shfl_sync(FULL, su.numFragments, j);
+            const uint64_t id = (uint64_t)__shfl_sync(FULL, su.id32, j);
+            uint64_t* const fbj = MULTI ? (uint64_t*)__shfl_sync(FULL, (unsigned long long)tg.fb, j) : p.fb;
+            const int Wj = MULTI ? __shfl_sync(FULL, tg.W, j) : p.W;
+            const int numPixels = Wj * (MULTI ? __shfl_sync(FULL, tg.H, j) : p.H);
+            const float start_x = floorf(min_x);
+            const float start_y = floorf(min_y);
+            const int size_y = nf / size_x;
+            // The reference tests every fragment of the bounding box.  Here each
+            // row is first narrowed to the columns whose exact float test can
+            // still pass (row_span), the surviving spans of 32 rows are packed
+            // across the lanes, and each fragment then runs the reference's
+            // test unchanged -- so the same fragments are written.
+            for (int r0 = 0; r0 < size_y; r0 += 32) {
+                int xlo = 0, len = 0;
+                if (r0 + lane < size_y)
+                    row_span(start_x, start_y + (float)(r0 + lane), size_x, asx, asy, abx, aby, acx, acy, inv_det,
+                             xlo, len);
+                int incl = len;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const int v = __shfl_up_sync(FULL, incl, d);
+                    if (lane >= d) incl += v;
+                }
+                const int total = __shfl_sync(FULL, incl, 31);
+                for (int base = 0; base < total; base += 32) {
+                    const int k = base + lane;
+                    // first row of the group whose inclusive span sum exceeds k
+                    int r = 0;
+#pragma unroll
+                    for (int step = 16; step >= 1; step >>= 1) {
+                        const int c = __shfl_sync(FULL, incl, r + step - 1);
+                        if (c <= k) r += step;
+                    }
+                    const int rx = __shfl_sync(FULL, xlo, r);
+                    const int rend = __shfl_sync(FULL, incl, r);
+                    const int rlen = __shfl_sync(FULL, len, r);
+                    if (k >= total) continue;
+                    const int fx = rx + (k - (rend - rlen));
+                    const int fy = r0 + r;
+                    const float px = start_x + (float)fx;
+                    const float py = start_y + (float)fy;
+                    const float sx = px - asx + 0.5f;
+                    const float sy = py - asy + 0.5f;
+                    const float s = (sx * acy - sy * acx) * inv_det;
+                    const float t = (abx * sy - aby * sx) * inv_det;
+                    const float v = 1.0f - (s + t);
+                    if (s >= 0.0f && t >= 0.0f && v >= 0.0f) {
+                        // The reference only tests pid < W*H and writes negative
+                        // indices in front of the buffer; they are dropped here.
+                        const int pid = (int)px + Wj * (int)py;
+                        if (pid >= 0 && pid < numPixels) {
+                            const float inv_depth = v * iza + s * izb + t * izc;
+                            const float depth = 1.0f / inv_depth;
+                            fb_min(fbj, (uint32_t)pid, pack_pixel(depth, id));
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Stage 3 -- tv.cu:568-745 (RAYTRACE) with intersectTriangle_mt
+// (helpers:213-270, double-sided)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float intersect_mt(V3 dir, V3 v0, V3 e1, V3 e2) {
+    const V3 pvec = cross3(dir, e2);
+    const float det = dot3(e1, pvec);
+    if (det > -1e-7f && det < 1e-7f) return INFINITY;
+    const float inv_det = 1.0f / det;
+    const V3 tvec = {-v0.x, -v0.y, -v0.z};
+    const float u = dot3(tvec, pvec) * inv_det;
+    if (u < 0.0f || u > 1.0f) return INFINITY;
+    const V3 qvec = cross3(tvec, e1);
+    const float v = dot3(dir, qvec) * inv_det;
+    if (v < 0.0f || u + v > 1.0f) return INFINITY;
+    const float t = dot3(e2, qvec) * inv_det;
+    return t > 0.0f ? t : INFINITY;
+}
+
+template <int WARPS, bool MULTI>
+__global__ void __launch_bounds__(WARPS * 32) k_stage3(const CrFrameParams p) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t gw = (uint64_t)blockIdx.x * WARPS + (threadIdx.x >> 5);
+    const uint64_t nw = (uint64_t)gridDim.x * WARPS;
+    const uint64_t count = min((uint64_t)p.counters[CR_CTR_HUGE], p.hugeCap);
+
+    for (uint64_t ti = gw; ti < count; ti += nw) {
+        const CrTile tile = p.hugeList[ti];
+        const uint32_t inst = (uint32_t)tile.instance & (uint32_t)CR_ENTRY_INST_MASK;
+        const uint32_t view = MULTI ? ((uint32_t)tile.instance >> 26) : 0u;
+        const Target tg = MULTI ? target_of(p, view) : target_of(p);
+        const float f = tg.f;
+        const float fa = tg.fa;
+        const float Wf = (float)tg.W, Hf = (float)tg.H;
+        const int numPixels = tg.W * tg.H;
+        const CrInstance* I = p.instances + inst;
+        const Mat M = load_mat(p.world_view + 4ull * ((uint64_t)view * p.numInstances + inst));
+        const uint32_t tri = (uint32_t)tile.triangle;
+        const uint32_t* ix = ldg_ptr(&I->indices);
+        const float* pos = ldg_ptr(&I->positions);
+        uint32_t i0, i1, i2;
+        if (ix) {
+            i0 = __ldg(ix + 3ull * tri + 0);
+            i1 = __ldg(ix + 3ull * tri + 1);
+            i2 = __ldg(ix + 3ull * tri + 2);
+        } else {
+            i0 = 3 * tri + 0;
+            i1 = 3 * tri + 1;
+            i2 = 3 * tri + 2;
+        }
+        const V3 av = xform(M, load_pos(pos, i0));
+        const V3 bv = xform(M, load_pos(pos, i1));
+        const V3 cv = xform(M, load_pos(pos, i2));
+        const V3 e1 = sub3(bv, av);
+        const V3 e2 = sub3(cv, av);
+        const uint64_t id = __ldg(&I->cum) + (uint64_t)tri;
+
+        const float min_x = clamp_ref((float)(tile.tile_x * CR_TILE_SIZE), 0.0f, Wf);
+        const float min_y = clamp_ref((float)(tile.tile_y * CR_TILE_SIZE), 0.0f, Hf);
+        const float fx0 = floorf(min_x);
+        const float fy0 = floorf(min_y);
+        // each lane owns columns lane and lane + 32
+        int px[2];
+        float rx[2];
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            px[c] = (int)(fx0 + (float)(lane + 32 * c));
+            const float u = 2.0f * ((float)px[c] + 0.5f) / Wf - 1.0f;
+            rx[c] = (1.0f / fa) * u;
+        }
+        for (int y = 0; y < CR_TILE_SIZE; ++y) {
+            const int py = (int)(fy0 + (float)y);
+            const float v = 2.0f * ((float)py + 0.5f) / Hf - 1.0f;
+            const float ry = (1.0f / f) * v;
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const int pid = px[c] + tg.W * py;
+                const V3 d = {rx[c], ry, -1.0f};
+                const float inv = 1.0f / sqrtf(dot3(d, d));
+                const V3 dir = {d.x * inv, d.y * inv, d.z * inv};
+                const float t = intersect_mt(dir, av, e1, e2);
+                if (t == INFINITY || pid >= numPixels) continue;
+                const float depth = ((t * dir.x) * 0.0f + (t * dir.y) * 0.0f) + (t * dir.z) * -1.0f;
+                fb_min(tg.fb, (uint32_t)pid, pack_pixel(depth, id));
+            }
+        }
+    }
+}
+
+}  // namespace

@@ -59,10 +59,7 @@ __device__ __forceinline__ V3 load_pos(const float* pos, uint32_t idx) {
     return V3{__ldg(q), __ldg(q + 1), __ldg(q + 2)};
 }
 
-__global__ void __launch_bounds__(256) k_resolve(const CrResolveParams p) {
-    const int x = blockIdx.x * 32 + threadIdx.x;
-    const int y = blockIdx.y * 8 + threadIdx.y;
-    if (x >= p.W || y >= p.H) return;
+__device__ __forceinline__ void resolve_pixel(const CrResolveParams& p, const int x, const int y) {
     const int pid = x + p.W * y;
     const uint64_t pixel = __ldcs(reinterpret_cast<const unsigned long long*>(p.fb) + pid);
 
@@ -161,6 +158,56 @@ __global__ void __launch_bounds__(256) k_resolve(const CrResolveParams p) {
     if (p.rgba) __stcs(p.rgba + pid, isinf(depth) ? p.background : color);
 }
 
+__global__ void __launch_bounds__(256) k_resolve(const CrResolveParams p) {
+    const int x = blockIdx.x * 32 + threadIdx.x;
+    const int y = blockIdx.y * 8 + threadIdx.y;
+    if (x >= p.W || y >= p.H) return;
+    resolve_pixel(p, x, y);
+}
+
+// Batched frames: one flat grid of 32x32-pixel tiles over all views (view v
+// owns blocks [resolveBlockBase_v, resolveBlockBase_v+1), each thread four
+// rows of its tile, so the per-block view lookup is amortised over 1024
+// pixels); the view's target and inverse view matrix replace the
+// single-view fields of the shared parameters.
+__global__ void __launch_bounds__(256) k_resolve_views(const CrResolveParams base, const CrView* views,
+                                                       uint32_t numViews) {
+    __shared__ CrResolveParams s_p;
+    uint32_t lo = 0, hi = numViews - 1;  // view owning this block
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (__ldg(&views[mid].resolveBlockBase) <= blockIdx.x) lo = mid;
+        else hi = mid - 1;
+    }
+    const CrView* v = views + lo;
+    const int W = __ldg(&v->W), H = __ldg(&v->H);
+    const int t = threadIdx.y * 32 + threadIdx.x;
+    if (t == 0) {
+        s_p = base;
+        s_p.fb = ldg_ptr(&v->fb);
+        s_p.rgba = ldg_ptr(&v->rgba);
+        s_p.colorbuffer = ldg_ptr(&v->colorbuffer);
+        s_p.W = W;
+        s_p.H = H;
+        s_p.origin[0] = __ldg(&v->origin[0]);
+        s_p.origin[1] = __ldg(&v->origin[1]);
+        s_p.origin[2] = __ldg(&v->origin[2]);
+        s_p.p00 = __ldg(&v->p00);
+        s_p.p11 = __ldg(&v->p11);
+    }
+    if (t < 16) s_p.viewI[t] = __ldg(&v->viewI[t]);
+    __syncthreads();
+    const uint32_t b = blockIdx.x - __ldg(&v->resolveBlockBase);
+    const uint32_t bx = (uint32_t)(W + 31) / 32;
+    const int x = (int)(b % bx) * 32 + threadIdx.x;
+    if (x >= W) return;
+#pragma unroll 1
+    for (int k = 0; k < 4; ++k) {
+        const int y = (int)(b / bx) * 32 + threadIdx.y + 8 * k;
+        if (y < H) resolve_pixel(s_p, x, y);
+    }
+}
+
 }  // namespace
 
 int cr_launch_resolve(const CrResolveParams& p, void* stream) {
@@ -168,5 +215,12 @@ int cr_launch_resolve(const CrResolveParams& p, void* stream) {
     dim3 block(32, 8);
     dim3 grid((p.W + 31) / 32, (p.H + 7) / 8);
     k_resolve<<<grid, block, 0, (cudaStream_t)stream>>>(p);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int cr_launch_resolve_views(const CrResolveParams& base, const CrView* views, uint32_t numViews, uint32_t numBlocks,
+                            void* stream) {
+    if (numViews == 0 || numBlocks == 0 || base.numInstances == 0) return 0;
+    k_resolve_views<<<numBlocks, dim3(32, 8), 0, (cudaStream_t)stream>>>(base, views, numViews);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

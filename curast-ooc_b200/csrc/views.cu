@@ -1,0 +1,526 @@
+// views.cu -- batched multi-view kernels for sm_100a: up to 64 views of one
+// instance set rendered by one launch per stage.
+//
+// No counterpart in the reference, which renders one view per CuRast::draw
+// (src/CuRast_render.h:356-592).  Every (triangle, view) pair goes through
+// exactly the reference's per-view decisions -- the same stage-1 function,
+// the same stage-2 setup and fragment loop and the same stage-3 ray tracer as
+// the single-view kernels, on the same float values -- so each view's
+// visbuffer is bit-identical to a single-view render of that view.  What is
+// shared across views is everything that does not depend on the view:
+//
+//   vertex   positions are read once and one CrViewMasks record per vertex
+//            is written (behind / beyond each frustum side, one bit per
+//            view).  The bounding box of each warp's 128 consecutive vertices
+//            is first classified against each view's frustum with a rigorous
+//            float error bound (classify_chunk); only the views the box
+//            straddles are evaluated per vertex.
+//   stage 1  a work item's 1536-byte index tile is fetched once (bulk TMA
+//            copy into a per-warp ring, as the single-view stage 1) and its
+//            triangles' records are gathered once; three 64-bit AND/OR
+//            chains give each triangle the set of views in which it survives
+//            the all-behind / all-beyond-one-side culls.  The warp then
+//            visits, view by view, every view in which any of its triangles
+//            survives: that view's survivors are packed across the lanes (as
+//            the single-view stage 1 packs its survivors) and run the
+//            reference's full per-triangle path with the view's target and
+//            matrix, which are the same for the whole warp.  Queue entries
+//            carry their view (view << 58 | instance << 32 | triangle).
+//   stage 2/3  the single-view kernels instantiated with MULTI = true: each
+//            queued entry / tile reads its own view's target and matrix.
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "raster_core.cuh"
+
+namespace {
+
+constexpr int VV_THREADS = 256;
+constexpr int VV_PER_THREAD = CR_VCHUNK / VV_THREADS;  // 4 vertices per thread
+
+// Chunk classes (bit set) of one view; CH_INSIDE means no vertex is behind or
+// beyond any side, CH_BEHIND that every vertex is behind, CH_<side> that
+// every vertex is in front and beyond that side.
+enum : uint32_t {
+    CH_BEHIND = 1u,
+    CH_RIGHT = 2u,
+    CH_LEFT = 4u,
+    CH_TOP = 8u,
+    CH_BOTTOM = 16u,
+    CH_INSIDE = 32u,
+};
+
+__device__ __forceinline__ double lin_min(const double a[3], double b, const float lo[3], const float hi[3]) {
+    double s = b;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) s += a[j] >= 0.0 ? a[j] * (double)lo[j] : a[j] * (double)hi[j];
+    return s;
+}
+
+__device__ __forceinline__ double lin_max(const double a[3], double b, const float lo[3], const float hi[3]) {
+    double s = b;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) s += a[j] >= 0.0 ? a[j] * (double)hi[j] : a[j] * (double)lo[j];
+    return s;
+}
+
+// Classifies a box of object-space positions [lo, hi] for one view (rows of
+// world_view: rx, ry, rz; fa = f / aspect and f as the kernels use them).
+//
+// The device evaluates per vertex q = xform(M, p) in float (three products,
+// two levels of sums), d = -q.z, X = fl(fa * q.x), Y = fl(f * q.y), and the
+// predicates d <= 0 and fl(X / d) > 1 (ndc_beyond).  With S_x = sum_j
+// |M_xj| max|p_j| + |M_x3|, |q.x - Q_x| <= gamma_3 S_x < 2^-20 S_x where Q is
+// the exact affine value (likewise y, z), and fl(fa q.x) adds a relative
+// 2^-24.  So with delta = 2^-20 and the margin
+//     m = 2^-19 (fa S_x + S_z) + 1e-30,
+// min over the box of (fa Q_x + (1 + delta) Q_z) > m proves X >= (1 + delta) d
+// for every vertex, hence fl(X / d) >= 1 + 2^-20 > 1: every vertex is beyond
+// the right side; max over the box of (fa Q_x + (1 - delta) Q_z) < -m proves
+// fl(X / d) <= 1 - 2^-20: none is.  Min / max of an affine function over a
+// box are exact corner sums (double products of floats are exact; the
+// double sums' rounding is far inside the margin).  Non-finite bounds
+// classify nothing (comparisons with NaN fail).
+__device__ uint32_t classify_chunk(const float4 rx, const float4 ry, const float4 rz, float fa, float f,
+                                   const float lo[3], const float hi[3]) {
+    const double EPS = 9.5367431640625e-07;  // 2^-20
+    const double ABS = 1e-30;
+    const double ax[3] = {rx.x, rx.y, rx.z}, ay[3] = {ry.x, ry.y, ry.z}, az[3] = {rz.x, rz.y, rz.z};
+    double mabs[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) mabs[j] = fmax(fabs((double)lo[j]), fabs((double)hi[j]));
+    const double Sx = (fabs(ax[0]) * mabs[0] + fabs(ax[1]) * mabs[1]) + (fabs(ax[2]) * mabs[2] + fabs((double)rx.w));
+    const double Sy = (fabs(ay[0]) * mabs[0] + fabs(ay[1]) * mabs[1]) + (fabs(ay[2]) * mabs[2] + fabs((double)ry.w));
+    const double Sz = (fabs(az[0]) * mabs[0] + fabs(az[1]) * mabs[1]) + (fabs(az[2]) * mabs[2] + fabs((double)rz.w));
+    if (!(Sx < 1e30 && Sy < 1e30 && Sz < 1e30)) return 0u;
+    const double ez = EPS * Sz + ABS;
+    if (lin_min(az, rz.w, lo, hi) - ez >= 0.0) return CH_BEHIND;  // q.z >= 0 everywhere
+    if (!(lin_max(az, rz.w, lo, hi) + ez < 0.0)) return 0u;      // some vertex may be behind
+    const double F = (double)fa, G = (double)f;
+    const double mx = 2.0 * EPS * (F * Sx + Sz) + ABS;
+    const double my = 2.0 * EPS * (G * Sy + Sz) + ABS;
+    const double up = 1.0 + EPS, dn = 1.0 - EPS;
+    double a[3];
+    uint32_t c = 0u, inside = 0u;
+    // right: fa Q_x vs d = -Q_z
+#pragma unroll
+    for (int j = 0; j < 3; ++j) a[j] = F * ax[j] + up * az[j];
+    if (lin_min(a, F * rx.w + up * rz.w, lo, hi) > mx) c |= CH_RIGHT;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) a[j] = F * ax[j] + dn * az[j];
+    if (lin_max(a, F * rx.w + dn * rz.w, lo, hi) < -mx) inside |= 1u;
+    // left: -fa Q_x
+#pragma unroll
+    for (int j = 0; j < 3; ++j) a[j] = -F * ax[j] + up * az[j];
+    if (lin_min(a, -F * rx.w + up * rz.w, lo, hi) > mx) c |= CH_LEFT;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) a[j] = -F * ax[j] + dn * az[j];
+    if (lin_max(a, -F * rx.w + dn * rz.w, lo, hi) < -mx) inside |= 2u;
+    // top: f Q_y
+#pragma unroll
+    for (int j = 0; j < 3; ++j) a[j] = G * ay[j] + up * az[j];
+    if (lin_min(a, G * ry.w + up * rz.w, lo, hi) > my) c |= CH_TOP;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) a[j] = G * ay[j] + dn * az[j];
+    if (lin_max(a, G * ry.w + dn * rz.w, lo, hi) < -my) inside |= 4u;
+    // bottom: -f Q_y
+#pragma unroll
+    for (int j = 0; j < 3; ++j) a[j] = -G * ay[j] + up * az[j];
+    if (lin_min(a, -G * ry.w + up * rz.w, lo, hi) > my) c |= CH_BOTTOM;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) a[j] = -G * ay[j] + dn * az[j];
+    if (lin_max(a, -G * ry.w + dn * rz.w, lo, hi) < -my) inside |= 8u;
+    if (c) return c;
+    return inside == 15u ? CH_INSIDE : 0u;
+}
+
+// vertex_outcode with the matrix given as its x, y, z rows: the same float
+// operations in the same order as xform.
+__device__ __forceinline__ uint32_t outcode_rows(const float4 rx, const float4 ry, const float4 rz, V3 p, float fa,
+                                                 float f) {
+    const float qz = (rz.x * p.x + rz.y * p.y) + (rz.z * p.z + rz.w * 1.0f);
+    const float d = -qz;
+    if (d <= 0.0f) return CR_OC_BEHIND;
+    const float qx = (rx.x * p.x + rx.y * p.y) + (rx.z * p.z + rx.w * 1.0f);
+    const float qy = (ry.x * p.x + ry.y * p.y) + (ry.z * p.z + ry.w * 1.0f);
+    const float X = fa * qx, Y = f * qy;
+    return (ndc_beyond(X, d) ? CR_OC_RIGHT : 0u) | (ndc_beyond(-X, d) ? CR_OC_LEFT : 0u) |
+           (ndc_beyond(Y, d) ? CR_OC_TOP : 0u) | (ndc_beyond(-Y, d) ? CR_OC_BOTTOM : 0u);
+}
+
+__device__ __forceinline__ unsigned long long valid_views(uint32_t n) {
+    return n >= 64 ? ~0ull : ((1ull << n) - 1ull);
+}
+
+// One block per 1024-vertex chunk of one instance; each warp owns 128
+// consecutive vertices (lane + 32 k), classifies their bounding box against
+// every view (two views per lane) and evaluates per vertex only the views the
+// box straddles.  Consecutive vertices of a mesh are usually close (a grid
+// row, a patch), so a 128-vertex box is small and most views classify it as a
+// whole: entirely behind, entirely beyond one side, or entirely inside.
+__global__ void __launch_bounds__(VV_THREADS) k_vertex_views(const CrFrameParams p) {
+    __shared__ float4 s_rows[CR_MAX_VIEWS][3];
+    __shared__ float s_fa[CR_MAX_VIEWS], s_f[CR_MAX_VIEWS];
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const uint32_t nViews = p.numViews;
+    const unsigned long long valid = valid_views(nViews);
+
+    for (uint64_t c = blockIdx.x; c < p.numVChunks; c += gridDim.x) {
+        uint32_t lo = 0, hi = p.numInstances - 1;  // instance holding chunk c
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (__ldg(&p.instances[mid].vchunkBase) <= c) lo = mid;
+            else hi = mid - 1;
+        }
+        const uint32_t inst = lo;
+        const CrInstance* I = p.instances + inst;
+        const uint32_t nV = __ldg(&I->numVertices);
+        const uint32_t vw = (uint32_t)(c - __ldg(&I->vchunkBase)) * CR_VCHUNK + (uint32_t)warp * (32 * VV_PER_THREAD);
+        const float* pos = ldg_ptr(&I->positions);
+
+        // the views' matrix rows of this instance, once per chunk
+        if (tid < CR_MAX_VIEWS && (uint32_t)tid < nViews) {
+            const Mat M = load_mat(p.world_view + 4ull * ((uint64_t)tid * p.numInstances + inst));
+            s_rows[tid][0] = make_float4(M.c0.x, M.c1.x, M.c2.x, M.c3.x);
+            s_rows[tid][1] = make_float4(M.c0.y, M.c1.y, M.c2.y, M.c3.y);
+            s_rows[tid][2] = make_float4(M.c0.z, M.c1.z, M.c2.z, M.c3.z);
+            s_fa[tid] = __ldg(&p.views[tid].fa);
+            s_f[tid] = __ldg(&p.views[tid].f);
+        }
+        // this lane's vertices and the warp's bounding box
+        V3 pv[VV_PER_THREAD];
+        float bl[3] = {INFINITY, INFINITY, INFINITY}, bh[3] = {-INFINITY, -INFINITY, -INFINITY};
+        bool bad = false;
+#pragma unroll
+        for (int k = 0; k < VV_PER_THREAD; ++k) {
+            const uint32_t v = vw + lane + 32 * k;
+            pv[k] = v < nV ? load_pos(pos, v) : V3{0.0f, 0.0f, 0.0f};
+            if (v < nV) {
+                bad |= !(isfinite(pv[k].x) && isfinite(pv[k].y) && isfinite(pv[k].z));
+                bl[0] = fminf(bl[0], pv[k].x); bh[0] = fmaxf(bh[0], pv[k].x);
+                bl[1] = fminf(bl[1], pv[k].y); bh[1] = fmaxf(bh[1], pv[k].y);
+                bl[2] = fminf(bl[2], pv[k].z); bh[2] = fmaxf(bh[2], pv[k].z);
+            }
+        }
+#pragma unroll
+        for (int d = 16; d >= 1; d >>= 1) {
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                bl[j] = fminf(bl[j], __shfl_xor_sync(FULL, bl[j], d));
+                bh[j] = fmaxf(bh[j], __shfl_xor_sync(FULL, bh[j], d));
+            }
+        }
+        const bool anyBad = __any_sync(FULL, bad);
+        __syncthreads();  // s_rows ready
+
+        // classes of the warp's box: lane classifies views lane and lane + 32
+        uint32_t cls[2] = {0u, 0u};
+        const bool anyVertex = bl[0] <= bh[0];  // false only past the mesh's end
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const uint32_t v = (uint32_t)lane + 32u * h;
+            if (v < nViews && !anyBad && anyVertex)
+                cls[h] = classify_chunk(s_rows[v][0], s_rows[v][1], s_rows[v][2], s_fa[v], s_f[v], bl, bh);
+        }
+        auto cls64 = [&](uint32_t b) -> unsigned long long {
+            const unsigned lo32 = __ballot_sync(FULL, cls[0] & b), hi32 = __ballot_sync(FULL, cls[1] & b);
+            return (((unsigned long long)hi32 << 32) | lo32) & valid;
+        };
+        const unsigned long long cB = cls64(CH_BEHIND), cR = cls64(CH_RIGHT), cL = cls64(CH_LEFT),
+                                 cT = cls64(CH_TOP), cO = cls64(CH_BOTTOM), cI = cls64(CH_INSIDE);
+        unsigned long long mixed = anyVertex ? valid & ~(cB | cR | cL | cT | cO | cI) : 0ull;
+
+        unsigned long long mb[VV_PER_THREAD], mr[VV_PER_THREAD], ml[VV_PER_THREAD], mt[VV_PER_THREAD],
+            mo[VV_PER_THREAD];
+#pragma unroll
+        for (int k = 0; k < VV_PER_THREAD; ++k) {
+            mb[k] = cB;
+            mr[k] = cR;
+            ml[k] = cL;
+            mt[k] = cT;
+            mo[k] = cO;
+        }
+        while (mixed) {  // uniform across the warp
+            const int v = __ffsll((long long)mixed) - 1;
+            mixed &= mixed - 1;
+            const float4 rx = s_rows[v][0], ry = s_rows[v][1], rz = s_rows[v][2];
+            const float fa = s_fa[v], f = s_f[v];
+            const unsigned long long bit = 1ull << v;
+#pragma unroll
+            for (int k = 0; k < VV_PER_THREAD; ++k) {
+                const uint32_t o = outcode_rows(rx, ry, rz, pv[k], fa, f);
+                mb[k] |= (o & CR_OC_BEHIND) ? bit : 0ull;
+                mr[k] |= (o & CR_OC_RIGHT) ? bit : 0ull;
+                ml[k] |= (o & CR_OC_LEFT) ? bit : 0ull;
+                mt[k] |= (o & CR_OC_TOP) ? bit : 0ull;
+                mo[k] |= (o & CR_OC_BOTTOM) ? bit : 0ull;
+            }
+        }
+        CrViewMasks* out = p.viewMasks + __ldg(&I->outBase);
+#pragma unroll
+        for (int k = 0; k < VV_PER_THREAD; ++k) {
+            const uint32_t v = vw + lane + 32 * k;
+            if (v < nV) {
+                ulonglong2* r = reinterpret_cast<ulonglong2*>(out + v);
+                r[0] = make_ulonglong2(mb[k], mr[k]);
+                r[1] = make_ulonglong2(ml[k], mt[k]);
+                r[2] = make_ulonglong2(mo[k], 0ull);
+            }
+        }
+        __syncthreads();  // s_rows are rewritten for the next chunk
+    }
+}
+
+// Views of one triangle that survive the all-behind and all-beyond-one-side
+// culls (tv.cu:110-119) given its three vertex records.
+__device__ __forceinline__ unsigned long long surviving_views(const CrViewMasks* rec, uint32_t i0, uint32_t i1,
+                                                              uint32_t i2, unsigned long long valid) {
+    const ulonglong2* a = reinterpret_cast<const ulonglong2*>(rec + i0);
+    const ulonglong2* b = reinterpret_cast<const ulonglong2*>(rec + i1);
+    const ulonglong2* c = reinterpret_cast<const ulonglong2*>(rec + i2);
+    const ulonglong2 a0 = __ldg(a), a1 = __ldg(a + 1), a2 = __ldg(a + 2);
+    const ulonglong2 b0 = __ldg(b), b1 = __ldg(b + 1), b2 = __ldg(b + 2);
+    const ulonglong2 c0 = __ldg(c), c1 = __ldg(c + 1), c2 = __ldg(c + 2);
+    const unsigned long long allB = a0.x & b0.x & c0.x;
+    const unsigned long long anyB = a0.x | b0.x | c0.x;
+    const unsigned long long side =
+        (a0.y & b0.y & c0.y) | (a1.x & b1.x & c1.x) | (a1.y & b1.y & c1.y) | (a2.x & b2.x & c2.x);
+    return valid & ~(allB | (~anyB & side));
+}
+
+// MINB: resident blocks per SM the register allocation must allow (a tuning
+// knob: more warps to hide latency against fewer registers per thread).
+template <int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) k_stage1_views(const CrFrameParams p) {
+    __shared__ __align__(128) uint32_t s_idx[WARPS][S1_STAGES][CR_BATCH * 3];
+    __shared__ __align__(8) uint64_t s_bar[WARPS][S1_STAGES];
+    __shared__ uint8_t s_surv[WARPS][CR_BATCH];
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    const uint64_t gw = (uint64_t)blockIdx.x * WARPS + w;
+    const uint64_t nw = (uint64_t)gridDim.x * WARPS;
+    const unsigned long long valid = valid_views(p.numViews);
+
+    if (lane == 0) {
+        for (int s = 0; s < S1_STAGES; ++s) mbar_init(&s_bar[w][s], 1);
+        fence_barrier_init();
+    }
+    __syncwarp();
+    uint32_t pending = 0;  // ring slots with an issued, unconsumed copy
+    for (int s = 0; s < S1_STAGES; ++s) {
+        const uint64_t item = gw + (uint64_t)s * nw;
+        if (item >= p.numItems) break;
+        const Item it = decode_item(p, item);
+        const CrSegment* sg = p.segments + it.seg;
+        if (item_uses_tma(sg, it.batch)) {
+            pending |= 1u << s;
+            if (lane == 0)
+                bulk_load(s_idx[w][s], ldg_ptr(&sg->indices) + (uint64_t)it.batch * (CR_BATCH * 3), CR_BATCH * 12,
+                          &s_bar[w][s]);
+        }
+    }
+    __syncwarp();
+
+    uint32_t parity = 0;
+    uint32_t k = 0;
+    for (uint64_t item = gw; item < p.numItems; item += nw, ++k) {
+        const int slot = (int)(k % S1_STAGES);
+        const uint32_t bit = 1u << slot;
+        const Item it = decode_item(p, item);
+        const CrSegment* sg = p.segments + it.seg;
+        const uint32_t numTri = __ldg(&sg->numTriangles);
+        const uint32_t* gix = ldg_ptr(&sg->indices);
+        const bool tma = item_uses_tma(sg, it.batch);
+        const uint32_t tri0 = it.batch * CR_BATCH;
+        if (tma) {
+            const bool ok =
+                __all_sync(FULL, mbar_wait_bounded(&s_bar[w][slot], (parity & bit) ? 1u : 0u, p.waitTimeoutNs));
+            if (!ok) {
+                if (lane == 0) atomicOr(&p.counters[CR_CTR_TIMEOUT], 1ull);
+                break;
+            }
+            parity ^= bit;
+            pending &= ~bit;
+        }
+        auto index_of = [&](uint32_t pos, int c) -> uint32_t {
+            if (tma) return s_idx[w][slot][3 * pos + c];
+            const uint32_t t = tri0 + pos;
+            return gix ? __ldg(gix + 3ull * t + c) : 3 * t + c;
+        };
+
+        const uint32_t first = __ldg(&sg->firstInstance);
+        const uint32_t count = __ldg(&sg->instanceCount);
+        const uint32_t ib = first + it.chunk * CR_INST_CHUNK;
+        const uint32_t ie = min(ib + CR_INST_CHUNK, first + count);
+        const float* pos = ldg_ptr(&sg->positions);
+        for (uint32_t inst = ib; inst < ie; ++inst) {
+            const CrViewMasks* rec = p.viewMasks + __ldg(&p.instances[inst].outBase);
+            unsigned long long m[S1_R];
+#pragma unroll
+            for (int r = 0; r < S1_R; ++r) {
+                const uint32_t tp = r * 32 + lane;
+                m[r] = 0ull;
+                if (tri0 + tp < numTri)
+                    m[r] = surviving_views(rec, index_of(tp, 0), index_of(tp, 1), index_of(tp, 2), valid);
+            }
+            // views in which any of the warp's triangles survives, in order;
+            // per view the surviving triangles are packed across the lanes
+            // and run the reference's per-triangle path with that view's
+            // (warp-uniform) target and matrix
+            const unsigned long long any = m[0] | m[1] | m[2] | m[3];
+            unsigned long long todo = ((unsigned long long)__reduce_or_sync(FULL, (unsigned)(any >> 32)) << 32) |
+                                      __reduce_or_sync(FULL, (unsigned)any);
+            if (!todo) continue;
+            const uint64_t cum = __ldg(&p.instances[inst].cum);
+            while (todo) {
+                const uint32_t view = (uint32_t)(__ffsll((long long)todo) - 1);
+                todo &= todo - 1ull;
+                int nsurv = 0;
+#pragma unroll
+                for (int r = 0; r < S1_R; ++r) {
+                    const bool in = (m[r] >> view) & 1ull;
+                    const unsigned bm = __ballot_sync(FULL, in);
+                    if (in) s_surv[w][nsurv + __popc(bm & ((1u << lane) - 1u))] = (uint8_t)(r * 32 + lane);
+                    nsurv += __popc(bm);
+                }
+                __syncwarp();
+                const uint64_t vi = (uint64_t)view * p.numInstances + inst;
+                const Target tg = target_of(p, view);
+                const Mat M = load_mat(p.world_view + 4ull * vi);
+                const uint32_t flip = __ldg(p.flips + vi);
+                const uint64_t entryHi = ((uint64_t)view << CR_ENTRY_VIEW_SHIFT) | ((uint64_t)inst << 32);
+                for (int base = 0; base < nsurv; base += 32) {
+                    const int j = base + lane;
+                    int res = S1_CULL;
+                    uint32_t tri = 0;
+                    if (j < nsurv) {
+                        const uint32_t tp = s_surv[w][j];
+                        tri = tri0 + tp;
+                        const V3 pa = load_pos(pos, index_of(tp, 0));
+                        const V3 pb = load_pos(pos, index_of(tp, 1));
+                        const V3 pc = load_pos(pos, index_of(tp, 2));
+                        res = stage1_triangle(tg, tg.fa, M, flip, pa, pb, pc, cum + tri);
+                    }
+                    const unsigned qmask = __ballot_sync(FULL, res == S1_QUEUE);
+                    if (qmask) {  // warp-aggregated append, tv.cu:190-197, tagged with the view
+                        const int leader = __ffs(qmask) - 1;
+                        unsigned long long b = 0;
+                        if (lane == leader)
+                            b = atomicAdd(&p.counters[CR_CTR_NONTRIVIAL], (unsigned long long)__popc(qmask));
+                        b = __shfl_sync(FULL, b, leader);
+                        if (res == S1_QUEUE) {
+                            const uint64_t q = b + __popc(qmask & ((1u << lane) - 1u));
+                            if (q < p.ntCap) p.ntList[q] = entryHi | tri;
+                            else atomicOr(&p.counters[CR_CTR_OVERFLOW], 1ull);
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        }
+
+        __syncwarp();
+        {  // every read of this slot is done: refill it with the item S1_STAGES ahead
+            const uint64_t nxt = item + (uint64_t)S1_STAGES * nw;
+            if (nxt < p.numItems) {
+                const Item nt = decode_item(p, nxt);
+                const CrSegment* ns = p.segments + nt.seg;
+                if (item_uses_tma(ns, nt.batch)) {
+                    pending |= bit;
+                    if (lane == 0) {
+                        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                        bulk_load(s_idx[w][slot], ldg_ptr(&ns->indices) + (uint64_t)nt.batch * (CR_BATCH * 3),
+                                  CR_BATCH * 12, &s_bar[w][slot]);
+                    }
+                }
+            }
+        }
+    }
+    // only after a timeout can copies still be in flight: wait for them
+    // (bounded) so none lands in shared memory after the block has exited
+    for (int s = 0; s < S1_STAGES; ++s)
+        if (pending & (1u << s)) (void)mbar_wait_bounded(&s_bar[w][s], (parity >> s) & 1u, p.waitTimeoutNs);
+}
+
+// Clears every view's visbuffer (resolve.cu:213-232); blockIdx.y is the view.
+__global__ void __launch_bounds__(256) k_clear_views(const CrView* views, unsigned long long* counters) {
+    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x < CR_CTR_COUNT) counters[threadIdx.x] = 0ull;
+    const CrView* v = views + blockIdx.y;
+    uint64_t* fb = ldg_ptr(&v->fb);
+    const uint64_t n = (uint64_t)__ldg(&v->W) * (uint64_t)__ldg(&v->H);
+    const uint64_t clearv = 0xFFFFFFF000000000ull;
+    ulonglong2* q = reinterpret_cast<ulonglong2*>(fb);
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n / 2; i += stride)
+        q[i] = make_ulonglong2(clearv, clearv);
+    if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) fb[n - 1] = clearv;
+}
+
+}  // namespace
+
+constexpr int VS1_WARPS_MAX = 8;
+
+int cr_query_batch_shape(int device, CrBatchShape* out) {
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return -1;
+    int bv = 0, b1 = 0, b2 = 0, b3 = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bv, k_vertex_views, VV_THREADS, 0) != cudaSuccess) return -1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_stage1_views<8, 2>, 256, 0) != cudaSuccess) return -1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_stage2<8, true>, 256, 0) != cudaSuccess) return -1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b3, k_stage3<8, true>, 256, 0) != cudaSuccess) return -1;
+    out->numSMs = sms;
+    out->vertexBlocks = sms * (bv > 0 ? bv : 1);
+    out->stage1Blocks = sms * (b1 > 0 ? b1 : 1);
+    out->stage2Blocks = sms * (b2 > 0 ? b2 : 1);
+    out->stage3Blocks = sms * (b3 > 0 ? b3 : 1);
+    out->stage1Warps = 8;
+    out->stage2Warps = 8;
+    return 0;
+}
+
+int cr_launch_clear_views(const CrFrameParams& p, uint64_t maxPixels, void* stream) {
+    if (p.numViews == 0) return 0;
+    const uint64_t want = (maxPixels / 2 + 255) / 256;
+    const unsigned gx = (unsigned)(want < 1 ? 1 : (want > 148 * 4 ? 148 * 4 : want));
+    k_clear_views<<<dim3(gx, p.numViews), 256, 0, (cudaStream_t)stream>>>(p.views, p.counters);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int cr_launch_vertex_views(const CrFrameParams& p, const CrBatchShape& s, void* stream) {
+    if (p.numVChunks == 0 || p.numViews == 0) return 0;
+    uint64_t blocks = p.numVChunks;
+    if (blocks > (uint64_t)s.vertexBlocks) blocks = (uint64_t)s.vertexBlocks;
+    k_vertex_views<<<(unsigned)blocks, VV_THREADS, 0, (cudaStream_t)stream>>>(p);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int cr_launch_stage1_views(const CrFrameParams& p, const CrBatchShape& s, void* stream) {
+    if (p.numItems == 0 || p.numViews == 0) return 0;
+    const int warps = s.stage1Warps == 4 ? 4 : VS1_WARPS_MAX;
+    uint64_t blocks = (p.numItems + warps - 1) / warps;
+    if (blocks > (uint64_t)s.stage1Blocks) blocks = (uint64_t)s.stage1Blocks;
+    const unsigned b = (unsigned)blocks;
+    cudaStream_t st = (cudaStream_t)stream;
+    // the register-capped variants let more blocks share an SM
+    const bool capped = (uint64_t)s.stage1Blocks > (uint64_t)s.numSMs * (warps == 4 ? 4u : 2u);
+    if (warps == 4) {
+        if (capped) k_stage1_views<4, 6><<<b, 128, 0, st>>>(p);
+        else k_stage1_views<4, 4><<<b, 128, 0, st>>>(p);
+    } else {
+        if (capped) k_stage1_views<8, 3><<<b, 256, 0, st>>>(p);
+        else k_stage1_views<8, 2><<<b, 256, 0, st>>>(p);
+    }
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int cr_launch_stage2_views(const CrFrameParams& p, const CrBatchShape& s, void* stream) {
+    if (s.stage2Warps == 4) k_stage2<4, true><<<(unsigned)s.stage2Blocks, 128, 0, (cudaStream_t)stream>>>(p);
+    else k_stage2<8, true><<<(unsigned)s.stage2Blocks, 256, 0, (cudaStream_t)stream>>>(p);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int cr_launch_stage3_views(const CrFrameParams& p, const CrBatchShape& s, void* stream) {
+    k_stage3<8, true><<<(unsigned)s.stage3Blocks, 256, 0, (cudaStream_t)stream>>>(p);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}

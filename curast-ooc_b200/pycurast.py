@@ -121,6 +121,34 @@ class CrNoallocInstance(ctypes.Structure):
 CR_NOALLOC_MAX_INSTANCES = 16
 CR_NOALLOC_MAX_VERTICES = 4 << 20
 
+CR_MAX_BATCH_VIEWS = 64
+CR_TUNE_THRESHOLDS = 1
+
+
+class CrView(ctypes.Structure):
+    _fields_ = [("camera", CrCamera), ("d_visbuffer", _u64), ("d_rgba", _u64), ("d_colorbuffer", _u64)]
+
+
+class CrTuning(ctypes.Structure):
+    _fields_ = [
+        ("scene_class", _u32),
+        ("threshold_small", _u32),
+        ("threshold_large", _u32),
+        ("vertex_blocks", _u32),
+        ("stage1_blocks", _u32),
+        ("stage1_warps", _u32),
+        ("stage2_blocks", _u32),
+        ("stage2_warps", _u32),
+        ("stage3_blocks", _u32),
+        ("reserved0", _u32),
+        ("nontrivial_cap", _u64),
+        ("huge_cap", _u64),
+        ("ms_before", _f32),
+        ("ms_after", _f32),
+        ("candidates", _u32),
+        ("reserved", _u32 * 3),
+    ]
+
 
 EXPORTS = {
     "cr_drain_stage_times": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrStageTimes)]),
@@ -143,7 +171,70 @@ EXPORTS = {
     "cr_order_instances": (_i32, [ctypes.c_void_p, ctypes.c_void_p, _u32, _u32, ctypes.c_void_p, ctypes.c_void_p]),
     "cr_render_noalloc": (_i32, [_i32, ctypes.POINTER(CrNoallocInstance), _u32, ctypes.POINTER(CrCamera), _u64, _u64,
                                  _i32, ctypes.c_void_p]),
+    "cr_render_batch": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrInstance), _u32, ctypes.POINTER(CrView), _u32, _i32,
+                               _u32, ctypes.c_void_p]),
+    "cr_batch_plan_create": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrInstance), _u32, ctypes.POINTER(CrView), _u32,
+                                    _i32, _u32, ctypes.POINTER(ctypes.c_void_p)]),
+    "cr_batch_plan_set_cameras": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrCamera), _u32]),
+    "cr_batch_plan_launch": (_i32, [ctypes.c_void_p, ctypes.c_void_p]),
+    "cr_batch_plan_wait": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrFrameStats)]),
+    "cr_batch_plan_destroy": (_i32, [ctypes.c_void_p]),
+    "cr_autotune_batch": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrInstance), _u32, ctypes.POINTER(CrView), _u32, _u32,
+                                 ctypes.POINTER(CrTuning)]),
+    "cr_get_tuning": (_i32, [ctypes.c_void_p, _u32, ctypes.POINTER(CrTuning)]),
+    "cr_scene_class": (_u32, [_u64, _u64, _u32]),
 }
+
+
+def make_views(views):
+    """views: iterable of (camera, d_visbuffer, d_rgba, d_colorbuffer)."""
+    views = list(views)
+    arr = (CrView * max(len(views), 1))()
+    for i, (cam, vis, rgba, cb) in enumerate(views):
+        arr[i].camera = cam
+        arr[i].d_visbuffer = int(vis)
+        arr[i].d_rgba = int(rgba or 0)
+        arr[i].d_colorbuffer = int(cb or 0)
+    return arr, len(views)
+
+
+class BatchPlan:
+    """cr_batch_plan: a batched frame captured as a CUDA graph."""
+
+    def __init__(self, ctx, instances, views, display=CR_DISPLAY_VERTEX_COLORS, flags=0):
+        arr, n = make_instances(instances) if not isinstance(instances, tuple) else instances
+        varr, nv = make_views(views)
+        h = ctypes.c_void_p()
+        _check(load().cr_batch_plan_create(ctx.h, arr, n, varr, nv, int(display), int(flags), ctypes.byref(h)))
+        self.h = h
+        self.num_views = nv
+
+    def set_cameras(self, cameras):
+        arr = (CrCamera * len(cameras))(*cameras)
+        _check(load().cr_batch_plan_set_cameras(self.h, arr, len(cameras)))
+
+    def launch(self, stream=0):
+        _check(load().cr_batch_plan_launch(self.h, ctypes.c_void_p(int(stream))))
+
+    def wait(self):
+        s = CrFrameStats()
+        _check(load().cr_batch_plan_wait(self.h, ctypes.byref(s)))
+        return s
+
+    def close(self):
+        if self.h:
+            load().cr_batch_plan_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def scene_class(triangles, pixels, num_views):
+    return int(load().cr_scene_class(int(triangles), int(pixels), int(num_views)))
 
 
 def render_noalloc(device, instances, camera, d_visbuffer, d_rgba=0, display=CR_DISPLAY_VERTEX_COLORS, stream=0):
@@ -328,6 +419,25 @@ class Context:
         arr, n = make_instances(instances) if not isinstance(instances, tuple) else instances
         return load().cr_render(self.h, arr, n, ctypes.byref(camera), int(d_visbuffer), int(d_rgba),
                                 int(d_colorbuffer), int(display), int(flags), ctypes.c_void_p(int(stream)))
+
+    def render_batch(self, instances, views, display=CR_DISPLAY_VERTEX_COLORS, flags=CR_RENDER_SYNC, stream=0):
+        """views: iterable of (camera, d_visbuffer, d_rgba, d_colorbuffer)."""
+        arr, n = make_instances(instances) if not isinstance(instances, tuple) else instances
+        varr, nv = make_views(views)
+        _check(load().cr_render_batch(self.h, arr, n, varr, nv, int(display), int(flags),
+                                      ctypes.c_void_p(int(stream))))
+
+    def autotune_batch(self, instances, views, tune_flags=0):
+        arr, n = make_instances(instances) if not isinstance(instances, tuple) else instances
+        varr, nv = make_views(views)
+        t = CrTuning()
+        _check(load().cr_autotune_batch(self.h, arr, n, varr, nv, int(tune_flags), ctypes.byref(t)))
+        return t
+
+    def get_tuning(self, scene_class):
+        t = CrTuning()
+        st = load().cr_get_tuning(self.h, int(scene_class), ctypes.byref(t))
+        return st, t
 
     def stats(self):
         s = CrFrameStats()

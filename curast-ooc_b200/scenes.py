@@ -347,3 +347,99 @@ def instanced_camera(width=1920, height=1080, box=100.0):
     view = look_at((c, c + 0.35 * box, c + 2.1 * box), (c, c, c))
     proj = perspective(60.0, width / height, 0.1, 10.0 * box)
     return view, proj
+
+
+# ---------------------------------------------------------------------------
+# the batched-views scene: a fractal-displaced grid seen by 64 cameras
+# ---------------------------------------------------------------------------
+TERRAIN = dict(amp=0.06, octaves=7, f0=6.0)
+BATCH_RESOLUTIONS = ((512, 512), (1280, 720), (1920, 1080), (3840, 2160))
+
+
+def _terrain_waves(seed, octaves, f0):
+    rng = np.random.default_rng(seed + 1000)
+    waves = []
+    for k in range(octaves):
+        for _ in range(2):
+            th = rng.uniform(0.0, 2.0 * math.pi)
+            waves.append((math.cos(th), math.sin(th), f0 * 2.0 ** k * rng.uniform(0.8, 1.25),
+                          rng.uniform(0.0, 2.0 * math.pi), 0.5 ** k))
+    return waves
+
+
+def terrain_height(x, z, seed=31):
+    """Height of the terrain surface at (x, z) (numpy, float64)."""
+    x = np.asarray(x, np.float64)
+    z = np.asarray(z, np.float64)
+    h = np.zeros(np.broadcast(x, z).shape)
+    for c, s, fr, ph, a in _terrain_waves(seed, TERRAIN["octaves"], TERRAIN["f0"]):
+        h = h + a * np.sin(fr * (x * c + z * s) + ph)
+    return TERRAIN["amp"] * h
+
+
+def terrain(n=5477, seed=31, device="cuda"):
+    """Displaced grid of n x n quads (2 triangles each; n = 5477 gives 59.99M
+    triangles) over the unit square in x/z, heights a seeded sum of 14
+    sinusoids (7 octaves), RGBA8 colours uniform.  Triangles wind as
+    heightfield()'s (front faces up).  Built with torch on `device` in chunks;
+    returns (positions (V,3) f32, indices (T,3) i32, colours (V,) i32)."""
+    import torch
+
+    V = (n + 1) * (n + 1)
+    T = 2 * n * n
+    waves = _terrain_waves(seed, TERRAIN["octaves"], TERRAIN["f0"])
+    pos = torch.empty((V, 3), dtype=torch.float32, device=device)
+    idx = torch.empty((T, 3), dtype=torch.int32, device=device)
+    chunk = 1 << 24
+    for v0 in range(0, V, chunk):
+        g = torch.arange(v0, min(V, v0 + chunk), device=device, dtype=torch.int64)
+        x = (g % (n + 1)).double() / n
+        z = (g // (n + 1)).double() / n
+        h = torch.zeros_like(x)
+        for c, s, fr, ph, a in waves:
+            h += a * torch.sin(fr * (x * c + z * s) + ph)
+        pos[v0:v0 + g.shape[0], 0] = x.float()
+        pos[v0:v0 + g.shape[0], 1] = (TERRAIN["amp"] * h).float()
+        pos[v0:v0 + g.shape[0], 2] = z.float()
+    for t0 in range(0, T, chunk):
+        g = torch.arange(t0, min(T, t0 + chunk), device=device, dtype=torch.int64)
+        q = g // 2
+        j = q // n
+        i = q % n
+        v00 = j * (n + 1) + i
+        v10 = v00 + 1
+        v01 = v00 + (n + 1)
+        v11 = v01 + 1
+        second = (g % 2) == 1
+        a = torch.where(second, v10, v00)
+        b = v01
+        c = torch.where(second, v11, v10)
+        idx[t0:t0 + g.shape[0]] = torch.stack([a, b, c], 1).to(torch.int32)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    colors = torch.randint(-2**31, 2**31 - 1, (V,), dtype=torch.int32, device=device, generator=gen)
+    return pos, idx, colors
+
+
+def batch_cameras(num_views=64, seed=37, resolutions=BATCH_RESOLUTIONS, scale=1.0, terrain_seed=31):
+    """Seeded cameras over the terrain: resolution uniform among
+    `resolutions` (each side multiplied by `scale`), eye 0.03-0.3 above the
+    surface at a uniform point of [0.1, 0.9]^2, looking at the surface point
+    0.15-0.6 away in a uniform direction; fovy 60 degrees.  Returns a list of
+    (view, proj, width, height)."""
+    rng = np.random.default_rng(seed)
+    cams = []
+    for _ in range(num_views):
+        W, H = resolutions[int(rng.integers(len(resolutions)))]
+        W = max(1, int(round(W * scale)))
+        H = max(1, int(round(H * scale)))
+        ex, ez = rng.uniform(0.1, 0.9, 2)
+        ey = float(terrain_height(ex, ez, terrain_seed)) + rng.uniform(0.03, 0.3)
+        yaw = rng.uniform(0.0, 2.0 * math.pi)
+        dist = rng.uniform(0.15, 0.6)
+        tx, tz = ex + dist * math.cos(yaw), ez + dist * math.sin(yaw)
+        ty = float(terrain_height(tx, tz, terrain_seed))
+        view = look_at((ex, ey, ez), (tx, ty, tz))
+        proj = perspective(60.0, W / H, 0.001, 10.0)
+        cams.append((view, proj, W, H))
+    return cams

@@ -198,6 +198,92 @@ cr_status cr_drain_stage_times(cr_context* ctx, cr_stage_times* out);
 /* 4x4 helpers in glm's float operation order (host). */
 void cr_mat4_mul(const float* a, const float* b, float* out);
 
+/* ---- batched views -------------------------------------------------------
+ * No single counterpart in the reference, which renders one view per
+ * CuRast::draw (src/CuRast_render.h:356-592, drawTrianglesVisbuffer at
+ * :211-264).  cr_render_batch renders up to CR_MAX_BATCH_VIEWS views of one
+ * instance set, each at its own resolution into its own buffers, with one
+ * launch per stage: geometry is read once for all views and every view's
+ * culls come from one 48-byte record per vertex.  Each view's visbuffer and
+ * colour are bit-identical to cr_render of that view with the same
+ * instances, flags and context configuration.  Flags as cr_render
+ * (CR_RENDER_TIMING reports the batch's stages as one frame). */
+#define CR_MAX_BATCH_VIEWS 64u
+
+typedef struct cr_view {
+    cr_camera camera;
+    uint64_t d_visbuffer;      /* W*H uint64, 16-byte aligned                    */
+    uint64_t d_rgba;           /* W*H uint32, or 0                               */
+    uint64_t d_colorbuffer;    /* W*H uint64, or 0                               */
+} cr_view;
+
+cr_status cr_render_batch(cr_context* ctx, const cr_instance* instances, uint32_t count,
+                          const cr_view* views, uint32_t num_views, int32_t display,
+                          uint32_t flags, void* stream);
+
+/* A batched frame captured once as a CUDA graph: frame-table upload, clear,
+ * vertex pass, stages 1-3, resolve and counter readback replay with one
+ * cudaGraphLaunch.  The plan owns its queues, records and tables, so plans
+ * never share state with each other or with the context's eager renders.
+ * Instances, view count, resolutions and output buffers are fixed at
+ * creation; cameras may change between launches (cr_batch_plan_set_cameras).
+ * Queue capacities come from the context's tuning for the scene's class
+ * when cr_autotune_batch has run, else from an eager render of the creation
+ * views (grown until nothing overflows) plus headroom; a launch whose queues
+ * overflow anyway reports CR_ERR_QUEUE_OVERFLOW from cr_batch_plan_wait. */
+typedef struct cr_batch_plan cr_batch_plan;
+
+cr_status cr_batch_plan_create(cr_context* ctx, const cr_instance* instances, uint32_t count,
+                               const cr_view* views, uint32_t num_views, int32_t display,
+                               uint32_t flags, cr_batch_plan** out);
+/* cameras[i].width/height must equal the plan's; waits for the previous
+ * launch of the plan to finish reading its tables. */
+cr_status cr_batch_plan_set_cameras(cr_batch_plan* plan, const cr_camera* cameras, uint32_t num_views);
+cr_status cr_batch_plan_launch(cr_batch_plan* plan, void* stream);
+/* Waits for the last launch; stats may be NULL. */
+cr_status cr_batch_plan_wait(cr_batch_plan* plan, cr_frame_stats* stats);
+cr_status cr_batch_plan_destroy(cr_batch_plan* plan);
+
+/* ---- autotuning ----------------------------------------------------------
+ * cr_autotune_batch times candidate launch shapes (grid sizes and block
+ * shapes of the vertex pass and stages 1-3) of cr_render_batch on the given
+ * scene and views, keeps the fastest per stage and sizes the queues from the
+ * measured demand.  The result is stored in the context under the scene's
+ * class (triangle count, pixel count and view count, each rounded to a power
+ * of two) and used by every later batched render and plan of that class.
+ * Launch shapes never change the output.  With CR_TUNE_THRESHOLDS the tuner
+ * also tries stage thresholds (threshold_small in {64, 128, 256}) and, if
+ * one is faster, writes it into the context's configuration: thresholds
+ * decide which stage rasterises a triangle and so change the visbuffer, and
+ * keeping them in the context makes cr_render and cr_render_batch agree. */
+#define CR_TUNE_THRESHOLDS 1u
+
+typedef struct cr_tuning {
+    uint32_t scene_class;
+    uint32_t threshold_small;
+    uint32_t threshold_large;
+    uint32_t vertex_blocks;
+    uint32_t stage1_blocks;
+    uint32_t stage1_warps;
+    uint32_t stage2_blocks;
+    uint32_t stage2_warps;
+    uint32_t stage3_blocks;
+    uint32_t reserved0;
+    uint64_t nontrivial_cap;
+    uint64_t huge_cap;
+    float ms_before;           /* default shapes, device ms per batched frame  */
+    float ms_after;            /* tuned shapes                                 */
+    uint32_t candidates;       /* configurations timed                         */
+    uint32_t reserved[3];
+} cr_tuning;
+
+cr_status cr_autotune_batch(cr_context* ctx, const cr_instance* instances, uint32_t count,
+                            const cr_view* views, uint32_t num_views, uint32_t tune_flags,
+                            cr_tuning* out);
+/* Tuning stored for a scene class (CR_ERR_NOT_FOUND if none). */
+cr_status cr_get_tuning(cr_context* ctx, uint32_t scene_class, cr_tuning* out);
+uint32_t cr_scene_class(uint64_t triangles, uint64_t pixels, uint32_t num_views);
+
 /* ---- rendering without allocating ----------------------------------------
  * No counterpart in the reference (CuRast allocates its queues and buffers
  * itself).  For callers that must not allocate device memory while they
