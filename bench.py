@@ -93,6 +93,16 @@ def build_workload(name):
                     desc=f"seeded fractal-displaced grid of {quads}x{quads} quads ({idx.shape[0]:,} triangles) seen "
                          f"by {nv} seeded cameras, resolutions uniform among 512x512, 1280x720, 1920x1080, "
                          f"3840x2160")
+    if name.startswith("served_"):
+        # served_<R>rps: Poisson requests at R/s over three resident scenes,
+        # beside a 4e9-triangle out-of-core scene streamed from pinned host
+        # memory
+        return dict(name=name, rate=float(name.split("_")[1].rstrip("rps")), served=True, device=True,
+                    desc="Poisson-arriving requests over three resident scenes (1M-triangle heightfield, 60M-triangle "
+                         "terrain, 400M-triangle planet), resolutions uniform among 512x512, 1280x720, 1920x1080, "
+                         "3840x2160, under a 64 GiB framebuffer/queue budget; beside them a 3.997e9-triangle terrain "
+                         "of 61,009 nodes (<= 65,536 triangles each) in 72 GB of pinned host memory streamed under "
+                         "a 32 GiB geometry budget")
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -254,6 +264,8 @@ def run_ours(args, rank, world, local):
     wl = build_workload(args.workload)
     if wl.get("batched"):
         return run_batched(args, rank, world, local, wl)
+    if wl.get("served"):
+        return run_served(args, rank, world, local, wl)
     T, V, Tu = scene_counts(wl)
     W, H = wl["W"], wl["H"]
     ctx = pc.Context(device=local)
@@ -514,6 +526,168 @@ def run_batched(args, rank, world, local, wl):
     return line
 
 
+def served_requests(n, rate, seed=53):
+    """Seeded request stream: arrival times (Poisson), scene 0-2, camera."""
+    import math
+
+    import scenes
+
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n))
+    out = []
+    tcams = scenes.batch_cameras(256, seed=seed + 1)
+    for k in range(n):
+        W, H = scenes.BATCH_RESOLUTIONS[int(rng.integers(4))]
+        proj = scenes.perspective(60.0, W / H, 0.001, 10.0)
+        s = int(rng.integers(3))
+        if s == 0:  # heightfield: around the benchmark camera
+            eye = np.array([0.5, 0.6, 0.45]) + rng.uniform(-0.15, 0.15, 3)
+            view = scenes.look_at(eye, (0.5 + rng.uniform(-0.1, 0.1), 0.0, 0.24))
+        elif s == 1:  # terrain: the batched-views camera set
+            view = tcams[int(rng.integers(len(tcams)))][0]
+        else:  # planet: the benchmark camera turned by a few degrees
+            v0, _ = scenes.planet_camera(W, H)
+            a, b = rng.uniform(-0.05, 0.05, 2)
+            R = np.eye(4)
+            R[:3, :3] = (np.array([[math.cos(a), 0, math.sin(a)], [0, 1, 0], [-math.sin(a), 0, math.cos(a)]]) @
+                         np.array([[1, 0, 0], [0, math.cos(b), -math.sin(b)], [0, math.sin(b), math.cos(b)]]))
+            view = (R.T @ np.asarray(v0, np.float64).reshape(4, 4).T).T.reshape(16).astype(np.float32)
+        out.append((float(t[k]), s, view, proj, W, H))
+    return out
+
+
+def run_served(args, rank, world, local, wl):
+    """Continuous batching at the configured Poisson rate (latency), then the
+    same kind of requests submitted at once (capacity), then the plain loop:
+    one cr_render per request.  Beside them, frames of the out-of-core scene
+    run on the server's out-of-core lane."""
+    import torch
+
+    import pycurast as pc
+    import scenes
+
+    rate = wl["rate"]
+    ctx = pc.Context(device=local)
+    t0 = time.perf_counter()
+    hf = scenes.heightfield()
+    tp, ti, tc = scenes.terrain(n=5477, device="cuda")
+    pp, pi, pcol = scenes.planet(400_000_000, device="cuda")
+    h_hf = ctx.mesh_from_host(*hf)
+    h_tr = ctx.mesh_from_device(tp.data_ptr(), tp.shape[0], ti.data_ptr(), ti.shape[0], tc.data_ptr())
+    h_pl = ctx.mesh_from_device(pp.data_ptr(), pp.shape[0], pi.data_ptr(), pi.shape[0], pcol.data_ptr())
+    insts = [[(h_hf, scenes.identity())], [(h_tr, scenes.identity())], [(h_pl, scenes.identity())]]
+    tris = [hf[1].shape[0], ti.shape[0], pi.shape[0]]
+    nodes, okeep = scenes.ooc_terrain(nodes_x=args.ooc_nodes, nodes_z=args.ooc_nodes)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    ooc = pc.OocScene(ctx, nodes, geometry_budget=32 << 30)
+    ocams = [pc.make_camera(*c) for c in scenes.ooc_cameras(64)]
+    ooc_tris = sum(n[4] for n in nodes)
+
+    def serve(reqs, paced, with_ooc):
+        with pc.Server(ctx, memory_budget=64 << 30, slots=3) as srv:
+            ids = [srv.add_scene(s) for s in insts]
+            oid = srv.add_ooc_scene(ooc)
+            start = time.perf_counter()
+            pending = set()
+            k = 0
+            ook = 0
+            last_ooc = 0.0
+            while k < len(reqs) or pending:
+                now = time.perf_counter() - start
+                while k < len(reqs) and (not paced or reqs[k][0] <= now):
+                    _, s, view, proj, W, H = reqs[k]
+                    pending.add(srv.submit(ids[s], pc.make_camera(view, proj, W, H)))
+                    k += 1
+                if with_ooc and k < len(reqs) and now - last_ooc > 0.25:  # out-of-core frames beside them
+                    pending.add(srv.submit(oid, ocams[ook % len(ocams)]))
+                    ook += 1
+                    last_ooc = now
+                for r in srv.poll():
+                    if r.status != pc.CR_OK:
+                        raise RuntimeError(f"request {r.ticket} failed: {r.status}")
+                    srv.release(r.ticket)
+                    pending.discard(r.ticket)
+                if paced and k < len(reqs):
+                    time.sleep(max(0.0, min(0.0005, reqs[k][0] - (time.perf_counter() - start))))
+                else:
+                    time.sleep(0.0002)
+            st = srv.stats()
+            wall = time.perf_counter() - start
+        return st, wall, ook
+
+    n_req = max(200, int(rate * args.serve_seconds))
+    reqs = served_requests(n_req, rate)
+    serve(reqs[:64], False, False)  # warm-up (allocations, queue sizes)
+    st_paced, wall_paced, n_ooc = serve(reqs, True, True)
+    cap_reqs = served_requests(args.capacity_requests, rate, seed=61)
+    st_cap, wall_cap, _ = serve(cap_reqs, False, False)
+
+    # the plain loop: the capacity requests one cr_render at a time
+    vis = torch.empty(3840 * 2160, dtype=torch.int64, device="cuda")
+    rgba = torch.empty(3840 * 2160, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+    for _, s, view, proj, W, H in cap_reqs[:8]:
+        ctx.render(insts[s], pc.make_camera(view, proj, W, H), vis.data_ptr(), rgba.data_ptr(), flags=0,
+                   stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _, s, view, proj, W, H in cap_reqs:
+        ctx.render(insts[s], pc.make_camera(view, proj, W, H), vis.data_ptr(), rgba.data_ptr(), flags=0,
+                   stream=stream.cuda_stream)
+    b.record(stream)
+    torch.cuda.synchronize()
+    plain_s = a.elapsed_time(b) * 1e-3
+    plain_vps = len(cap_reqs) / plain_s
+    # one out-of-core frame alone, cold and warm cache
+    ooc_stats = []
+    for cam in ocams[:2] + ocams[:1]:
+        c0 = time.perf_counter()
+        st = ooc.render(cam, vis.data_ptr(), rgba.data_ptr(), flags=pc.CR_RENDER_SYNC) if cam.width * cam.height <= 3840 * 2160 else None
+        ooc_stats.append({"ms": (time.perf_counter() - c0) * 1e3, "visible_nodes": st.visible_nodes,
+                          "visible_triangles": st.visible_triangles, "uploaded_nodes": st.uploaded_nodes,
+                          "uploaded_GB": st.uploaded_bytes / 1e9, "resident_hits": st.resident_hits,
+                          "passes": st.passes})
+    ooc.close()
+    ctx.close()
+    if rank != 0:
+        return None
+    return {
+        "metric": "views/s served (continuous batching, mixed scenes and resolutions), p50/p99 latency vs plain loop",
+        "value": world * st_cap.views_per_s,
+        "unit": "views/s",
+        "n_gpus": world,
+        "steps": len(cap_reqs),
+        "warmup": 64,
+        "ms_per_step": 1e3 / st_cap.views_per_s,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": wl["name"], "desc": wl["desc"], "scene_triangles": tris,
+                   "ooc": {"nodes": len(nodes), "triangles": ooc_tris, "host_bytes": int(okeep[0].numel() * 4 +
+                                                                                     okeep[1].numel() * 4),
+                           "geometry_budget": 32 << 30, "frames_beside_paced_run": n_ooc, "alone": ooc_stats},
+                   "paced": {"rate_per_s": rate, "requests": len(reqs), "wall_s": wall_paced,
+                             "views_per_s": st_paced.views_per_s, "p50_ms": st_paced.p50_ms,
+                             "p99_ms": st_paced.p99_ms, "mean_ms": st_paced.mean_ms,
+                             "batches": int(st_paced.batches), "peak_GB": st_paced.peak_bytes / 1e9},
+                   "capacity": {"requests": len(cap_reqs), "views_per_s": st_cap.views_per_s,
+                                "p50_ms": st_cap.p50_ms, "p99_ms": st_cap.p99_ms, "batches": int(st_cap.batches),
+                                "mean_batch": st_cap.batched_views / max(1, st_cap.batches)},
+                   "plain_loop": {"views_per_s": plain_vps, "seconds": plain_s,
+                                  "note": "the capacity requests, one cr_render each, same GPU"},
+                   "speedup_vs_plain_loop": st_cap.views_per_s / plain_vps,
+                   "setup_s": setup_s, "parallelism": f"replicas x{world}"},
+        "e2e": {"value": world * st_cap.views_per_s, "unit": "views/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0, "note": "host submit to device completion, results left on the device"},
+        "gpu_launches": None,
+        "clocks": None,
+    }
+
+
 def scenes_identity():
     import scenes
 
@@ -650,6 +824,9 @@ def main(argv=None):
                          "instanced_<K>x<N>m_1080p, batched_<V>v_<N>m (V cameras over an N-million-triangle "
                          "terrain)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ooc-nodes", type=int, default=247, help="out-of-core scene: nodes per side (served_*)")
+    ap.add_argument("--serve-seconds", type=float, default=4.0, help="paced serving run length (served_*)")
+    ap.add_argument("--capacity-requests", type=int, default=512, help="requests of the capacity run (served_*)")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)
     rank, world, local = init_dist(args)

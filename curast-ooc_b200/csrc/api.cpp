@@ -95,6 +95,7 @@ void mat4_inverse(const float* m, float* out) {
 using namespace cr;
 
 cr_status cr_context::dev_alloc(void** p, size_t bytes, const char* what) {
+    std::lock_guard<std::mutex> lk(allocMu);
     if (cfg.memory_budget && bytesInUse + bytes > cfg.memory_budget)
         return fail(CR_ERR_OOM, "%s: %zu bytes would exceed the memory budget (%zu in use of %llu)", what, bytes,
                     bytesInUse, (unsigned long long)cfg.memory_budget);
@@ -108,6 +109,7 @@ cr_status cr_context::dev_alloc(void** p, size_t bytes, const char* what) {
 }
 void cr_context::dev_free(void* p, size_t bytes) {
     if (!p) return;
+    std::lock_guard<std::mutex> lk(allocMu);
     cudaFree(p);
     bytesInUse -= std::min(bytesInUse, bytes);
 }
@@ -129,13 +131,14 @@ void order_instances(uint32_t count, uint32_t flags, MeshOf meshOf, TrisOf trisO
 }
 
 cr_status assemble(cr_context* ctx, const cr_instance* instances, uint32_t count, const float* view, uint32_t flags,
-                   Assembled& A) {
+                   Assembled& A, const uint64_t* firstIds) {
     for (uint32_t i = 0; i < count; i++) {
         const uint32_t m = instances[i].mesh;
         if (m >= ctx->meshes.size() || !ctx->meshes[m].live) return fail(CR_ERR_NOT_FOUND, "instance %u: unknown mesh %u", i, m);
     }
+    // explicit first ids: the caller's order and ids (ranges may leave gaps)
     order_instances(
-        count, flags, [&](uint32_t i) { return instances[i].mesh; },
+        count, firstIds ? (flags | CR_RENDER_KEEP_ORDER) : flags, [&](uint32_t i) { return instances[i].mesh; },
         [&](uint32_t i) { return ctx->meshes[instances[i].mesh].numTriangles; }, A.order);
     A.inst.assign(count, CrInstance{});
     A.worldView.resize(16ull * count);
@@ -150,7 +153,7 @@ cr_status assemble(cr_context* ctx, const cr_instance* instances, uint32_t count
         ci.indices = m.indices;
         ci.positions = m.positions;
         ci.colors = m.colors;
-        ci.cum = sum;
+        ci.cum = firstIds ? firstIds[A.order[r]] : sum;
         ci.numTriangles = m.numTriangles;
         ci.numVertices = m.numVertices;
         ci.outBase = A.outBytes;
@@ -175,6 +178,9 @@ cr_status assemble(cr_context* ctx, const cr_instance* instances, uint32_t count
         }
         A.seg.back().instanceCount++;
         sum += m.numTriangles;
+        if (firstIds && (r > 0 && ci.cum < A.inst[r - 1].cum + A.inst[r - 1].numTriangles))
+            return fail(CR_ERR_INVALID, "explicit triangle ids must increase without overlap");
+        if (ci.cum + m.numTriangles > (1ull << 36)) return fail(CR_ERR_INVALID, "triangle ids hold 36 bits");
     }
     if (sum >= (1ull << 36)) return fail(CR_ERR_INVALID, "scene has %llu triangles; ids hold 36 bits", (unsigned long long)sum);
     for (CrSegment& s : A.seg) {
@@ -327,11 +333,13 @@ cr_status run_frame(cr_context* ctx, uint32_t flags, cudaStream_t stream, uint64
         ctx->last.overflow = ctx->hCounters[CR_CTR_OVERFLOW];
         if (ctx->hCounters[CR_CTR_TIMEOUT]) return fail(CR_ERR_TIMEOUT, "a device-side wait timed out");
         if (!ctx->last.overflow) return CR_OK;
-        if (!ctx->cfg.grow_on_overflow || (flags & CR_RENDER_NO_CLEAR))
+        if (!ctx->cfg.grow_on_overflow)
             return fail(CR_ERR_QUEUE_OVERFLOW, "queue overflow: nontrivial %llu/%llu, tiles %llu/%llu",
                         (unsigned long long)ctx->last.nontrivial, (unsigned long long)ctx->ntCap,
                         (unsigned long long)ctx->last.huge_tiles, (unsigned long long)ctx->hugeCap);
-        // the counters hold the exact demand of every queue that was fed in full
+        // the counters hold the exact demand of every queue that was fed in
+        // full; re-issuing the frame is safe even without a clear, since every
+        // fragment write is an atomic minimum (idempotent)
         const uint64_t ntWant = std::max<uint64_t>(ctx->ntCap, ctx->last.nontrivial + ctx->last.nontrivial / 8 + 1024);
         const uint64_t huWant = (ctx->last.overflow & 1)
                                     ? ctx->hugeCap
@@ -540,7 +548,7 @@ cr_status cr_frame_assemble(cr_context* ctx, const cr_instance* instances, uint3
                             uint32_t flags, uint32_t* order, uint64_t* first_id, float* world_view) {
     if (!ctx || (!instances && count) || !view) return fail(CR_ERR_INVALID, "cr_frame_assemble: NULL argument");
     Assembled A;
-    cr_status s = assemble(ctx, instances, count, view, flags, A);
+    cr_status s = assemble(ctx, instances, count, view, flags, A, nullptr);
     if (s) return s;
     for (uint32_t i = 0; i < count; i++) {
         if (order) order[i] = A.order[i];
@@ -568,6 +576,16 @@ cr_status cr_order_instances(const uint32_t* mesh, const uint32_t* triangles, ui
 cr_status cr_render(cr_context* ctx, const cr_instance* instances, uint32_t count, const cr_camera* cam,
                     uint64_t d_visbuffer, uint64_t d_rgba, uint64_t d_colorbuffer, int32_t display, uint32_t flags,
                     void* stream_) {
+    return render_impl(ctx, instances, count, nullptr, cam, d_visbuffer, d_rgba, d_colorbuffer, display, flags,
+                       stream_, 0, ~0ull);
+}
+
+}  // extern "C"
+
+cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_t count, const uint64_t* firstIds,
+                          const cr_camera* cam, uint64_t d_visbuffer, uint64_t d_rgba, uint64_t d_colorbuffer,
+                          int32_t display, uint32_t flags, void* stream_, uint64_t resolveIdLo,
+                          uint64_t resolveIdHi) {
     if (!ctx || !cam || (!instances && count)) return fail(CR_ERR_INVALID, "cr_render: NULL argument");
     if (cam->width <= 0 || cam->height <= 0 || (uint64_t)cam->width * cam->height >= (1ull << 31))
         return fail(CR_ERR_INVALID, "cr_render: bad resolution %dx%d", cam->width, cam->height);
@@ -578,7 +596,7 @@ cr_status cr_render(cr_context* ctx, const cr_instance* instances, uint32_t coun
     CR_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
 
     Assembled A;
-    cr_status s = assemble(ctx, instances, count, cam->view, flags, A);
+    cr_status s = assemble(ctx, instances, count, cam->view, flags, A, firstIds);
     if (s) return s;
     // frame tables, queues and counters are shared by consecutive frames,
     // which may be issued on different streams
@@ -624,6 +642,9 @@ cr_status cr_render(cr_context* ctx, const cr_instance* instances, uint32_t coun
     rp.p00 = cam->proj[0];
     rp.p11 = cam->proj[5];
     rp.background = 0xffffffffu;  // HostDeviceInterface.h:37 BACKGROUND_COLOR
+    rp.idLo = resolveIdLo;
+    rp.idHi = resolveIdHi;
+    rp.writeBackground = resolveIdLo == 0 ? 1u : 0u;
 
     auto issue = [&](cudaEvent_t* tev, cudaEvent_t rasterEnd) -> cr_status {
         fp.ntList = ctx->ntList;
@@ -632,22 +653,23 @@ cr_status cr_render(cr_context* ctx, const cr_instance* instances, uint32_t coun
         fp.hugeCap = ctx->hugeCap;
         auto mark = [&](int i) -> cudaError_t { return tev ? cudaEventRecord(tev[i], stream) : cudaSuccess; };
         CR_CUDA(mark(0), "event");
-        if (flags & CR_RENDER_NO_CLEAR) {
+        const bool raster = !(flags & kRenderResolveOnly);
+        if ((flags & CR_RENDER_NO_CLEAR) || !raster) {
             CR_CUDA(cudaMemsetAsync(ctx->counters, 0, CR_CTR_COUNT * sizeof(unsigned long long), stream), "counters");
         } else if (cr_launch_clear(fp.fb, numPixels, ctx->counters, stream)) {
             return fail(CR_ERR_CUDA, "clear launch: %s", cudaGetErrorString(cudaGetLastError()));
         }
         CR_CUDA(mark(1), "event");
-        if (count && cr_launch_vertex(fp, ctx->shape, stream))
+        if (raster && count && cr_launch_vertex(fp, ctx->shape, stream))
             return fail(CR_ERR_CUDA, "vertex-pass launch: %s", cudaGetErrorString(cudaGetLastError()));
         CR_CUDA(mark(2), "event");
-        if (count && cr_launch_stage1(fp, ctx->shape, stream))
+        if (raster && count && cr_launch_stage1(fp, ctx->shape, stream))
             return fail(CR_ERR_CUDA, "stage-1 launch: %s", cudaGetErrorString(cudaGetLastError()));
         CR_CUDA(mark(3), "event");
-        if (count && cr_launch_stage2(fp, ctx->shape, stream))
+        if (raster && count && cr_launch_stage2(fp, ctx->shape, stream))
             return fail(CR_ERR_CUDA, "stage-2 launch: %s", cudaGetErrorString(cudaGetLastError()));
         CR_CUDA(mark(4), "event");
-        if (count && cr_launch_stage3(fp, ctx->shape, stream))
+        if (raster && count && cr_launch_stage3(fp, ctx->shape, stream))
             return fail(CR_ERR_CUDA, "stage-3 launch: %s", cudaGetErrorString(cudaGetLastError()));
         CR_CUDA(mark(5), "event");
         if (rasterEnd) CR_CUDA(cudaEventRecord(rasterEnd, stream), "event");
@@ -658,6 +680,8 @@ cr_status cr_render(cr_context* ctx, const cr_instance* instances, uint32_t coun
     };
     return run_frame(ctx, flags, stream, count, A.totalTriangles, issue);
 }
+
+extern "C" {
 
 cr_status cr_sync(cr_context* ctx) {
     if (!ctx) return fail(CR_ERR_INVALID, "cr_sync: NULL context");

@@ -137,6 +137,9 @@ void base_params(const cr_context* ctx, int32_t display, CrFrameParams& fp, CrRe
     fp.debugFlags = ctx->cfg.debug_flags;
     rp.display = display;
     rp.background = 0xffffffffu;  // HostDeviceInterface.h:37 BACKGROUND_COLOR
+    rp.writeBackground = 1u;
+    rp.idLo = 0ull;
+    rp.idHi = ~0ull;
 }
 
 // The stages of one batched frame on `stream` (no host synchronisation, so
@@ -253,6 +256,106 @@ cr_status render_batch(cr_context* ctx, const cr_instance* instances, uint32_t c
 }
 
 }  // namespace
+
+// ---------------------------------------------------------------------------
+// Batches issued into caller-owned scratch (the server's slots)
+// ---------------------------------------------------------------------------
+cr_status cr::scratch_issue(cr_context* ctx, BatchScratch& S, const cr_instance* instances, uint32_t count,
+                            const cr_view* views, uint32_t nv, int32_t display, uint32_t flags, cudaStream_t stream) {
+    cr_status s = check_views(views, nv, flags);
+    if (s) return s;
+    Assembled A;
+    s = assemble(ctx, instances, count, views[0].camera.view, flags, A);
+    if (s) return s;
+    BatchTables B;
+    build_views(instances, A, views, nv, B);
+    const uint32_t sceneClass = cr_scene_class(A.totalTriangles, B.sumPixels, nv);
+    const CrBatchShape sh = shape_for(ctx, sceneClass);
+    const TableLayout L = layout_of(A.inst.size(), A.seg.size(), nv);
+    // the previous batch of this slot must have finished reading its tables
+    // (the slot's stream is in order; the host waits for the pinned copy)
+    if (S.tableCopied) CR_CUDA(cudaEventSynchronize(S.tableCopied), "slot staging");
+    auto grow = [&](void** d, size_t& cap, size_t want, const char* what) -> cr_status {
+        if (want <= cap) return CR_OK;
+        CR_CUDA(cudaStreamSynchronize(stream), "slot resize");
+        ctx->dev_free(*d, cap);
+        *d = nullptr;
+        cap = 0;
+        cr_status gs = ctx->dev_alloc(d, want, what);
+        if (gs) return gs;
+        cap = want;
+        return CR_OK;
+    };
+    if ((s = grow(&S.dTable, S.dTableCap, L.total * 2, "slot table")) ||
+        (s = grow(&S.records, S.recordCap, align_up(A.outBytes * sizeof(CrViewMasks), 256) + 256, "slot records")))
+        return s;
+    if (L.total > S.hTableCap) {
+        if (S.hTable) cudaFreeHost(S.hTable);
+        S.hTable = nullptr;
+        S.hTableCap = 0;
+        CR_CUDA(cudaMallocHost(&S.hTable, L.total * 2), "slot pinned table");
+        S.hTableCap = L.total * 2;
+    }
+    if (!S.counters) {
+        if ((s = ctx->dev_alloc((void**)&S.counters, CR_CTR_COUNT * 8, "slot counters"))) return s;
+        CR_CUDA(cudaMallocHost(&S.hCounters, CR_CTR_COUNT * 8), "slot pinned counters");
+        CR_CUDA(cudaEventCreateWithFlags(&S.tableCopied, cudaEventDisableTiming), "slot event");
+    }
+    pack_tables(A, B, L, (char*)S.hTable);
+    CR_CUDA(cudaMemcpyAsync(S.dTable, S.hTable, L.total, cudaMemcpyHostToDevice, stream), "slot table upload");
+    CR_CUDA(cudaEventRecord(S.tableCopied, stream), "slot event");
+    CrFrameParams fp{};
+    CrResolveParams rp{};
+    bind_tables(A, B, L, (char*)S.dTable, fp, rp);
+    base_params(ctx, display, fp, rp);
+    fp.viewMasks = (CrViewMasks*)S.records;
+    fp.counters = S.counters;
+    fp.ntList = S.ntList;
+    fp.ntCap = S.ntCap;
+    fp.hugeList = S.hugeList;
+    fp.hugeCap = S.hugeCap;
+    s = issue_batch(fp, rp, B, sh, count, flags, stream, nullptr, nullptr);
+    if (s) return s;
+    CR_CUDA(cudaMemcpyAsync(S.hCounters, S.counters, CR_CTR_COUNT * 8, cudaMemcpyDeviceToHost, stream),
+            "slot counters readback");
+    return CR_OK;
+}
+
+cr_status cr::scratch_grow_queues(cr_context* ctx, BatchScratch& S, uint64_t ntWant, uint64_t hugeWant) {
+    if (ntWant > S.ntCap) {
+        ctx->dev_free(S.ntList, S.ntCap * 8);
+        S.ntList = nullptr;
+        S.ntCap = 0;
+        cr_status s = ctx->dev_alloc((void**)&S.ntList, ntWant * 8, "slot stage-2 queue");
+        if (s) return s;
+        S.ntCap = ntWant;
+    }
+    if (hugeWant > S.hugeCap) {
+        ctx->dev_free(S.hugeList, S.hugeCap * sizeof(CrTile));
+        S.hugeList = nullptr;
+        S.hugeCap = 0;
+        cr_status s = ctx->dev_alloc((void**)&S.hugeList, hugeWant * sizeof(CrTile), "slot stage-3 queue");
+        if (s) return s;
+        S.hugeCap = hugeWant;
+    }
+    return CR_OK;
+}
+
+void cr::scratch_free(cr_context* ctx, BatchScratch& S) {
+    ctx->dev_free(S.dTable, S.dTableCap);
+    ctx->dev_free(S.records, S.recordCap);
+    ctx->dev_free(S.ntList, S.ntCap * 8);
+    ctx->dev_free(S.hugeList, S.hugeCap * sizeof(CrTile));
+    ctx->dev_free(S.counters, CR_CTR_COUNT * 8);
+    if (S.hTable) cudaFreeHost(S.hTable);
+    if (S.hCounters) cudaFreeHost(S.hCounters);
+    if (S.tableCopied) cudaEventDestroy(S.tableCopied);
+    S = BatchScratch{};
+}
+
+uint64_t cr::scratch_bytes(const BatchScratch& S) {
+    return S.dTableCap + S.recordCap + S.ntCap * 8 + S.hugeCap * sizeof(CrTile) + (S.counters ? CR_CTR_COUNT * 8 : 0);
+}
 
 struct cr_batch_plan {
     cr_context* ctx = nullptr;

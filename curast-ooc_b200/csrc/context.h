@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <functional>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -96,6 +97,7 @@ struct cr_context {
 
     // autotuner results, one per scene class
     std::vector<cr_tuning> tunings;
+    std::mutex allocMu;  // dev_alloc / dev_free (a server's threads share the context)
 
     cr_status dev_alloc(void** p, size_t bytes, const char* what);
     void dev_free(void* p, size_t bytes);
@@ -103,8 +105,21 @@ struct cr_context {
 
 namespace cr {
 
+// Frame assembly (CuRast_render.h:337-435).  firstIds, if not null, gives
+// instance i its first triangle id and keeps the given order (ids must
+// increase without overlap); else ids are the prefix sum in render order.
 cr_status assemble(cr_context* ctx, const cr_instance* instances, uint32_t count, const float* view, uint32_t flags,
-                   Assembled& A);
+                   Assembled& A, const uint64_t* firstIds = nullptr);
+
+// Internal render flag: resolve only (the frame's raster passes are done).
+constexpr uint32_t kRenderResolveOnly = 1u << 31;
+
+// cr_render with optional explicit first ids; the resolve writes only pixels
+// whose triangle id lies in [resolveIdLo, resolveIdHi) and the background
+// only when resolveIdLo == 0 (multi-pass frames resolve group by group).
+cr_status render_impl(cr_context* ctx, const cr_instance* instances, uint32_t count, const uint64_t* firstIds,
+                      const cr_camera* cam, uint64_t d_visbuffer, uint64_t d_rgba, uint64_t d_colorbuffer,
+                      int32_t display, uint32_t flags, void* stream, uint64_t resolveIdLo, uint64_t resolveIdHi);
 cr_status ensure_queues(cr_context* ctx, uint64_t ntWant, uint64_t hugeWant);
 // Grows the per-vertex record buffer to at least `bytes`.
 cr_status ensure_records(cr_context* ctx, uint64_t bytes);
@@ -119,6 +134,30 @@ cr_status run_frame(cr_context* ctx, uint32_t flags, cudaStream_t stream, uint64
                     const IssueFn& issue);
 
 const cr_tuning* find_tuning(const cr_context* ctx, uint32_t sceneClass);
+// Device and pinned buffers of one batched frame in flight (a server slot).
+struct BatchScratch {
+    void* dTable = nullptr;
+    size_t dTableCap = 0;
+    void* hTable = nullptr;  // pinned
+    size_t hTableCap = 0;
+    void* records = nullptr;
+    size_t recordCap = 0;
+    uint64_t* ntList = nullptr;
+    uint64_t ntCap = 0;
+    CrTile* hugeList = nullptr;
+    uint64_t hugeCap = 0;
+    unsigned long long* counters = nullptr;
+    unsigned long long* hCounters = nullptr;  // pinned; valid after the stream reaches the batch's end
+    cudaEvent_t tableCopied = nullptr;
+};
+// Issues a batched frame into S on `stream` (tables, stages, counter
+// readback); returns without waiting for it.
+cr_status scratch_issue(cr_context* ctx, BatchScratch& S, const cr_instance* instances, uint32_t count,
+                        const cr_view* views, uint32_t nv, int32_t display, uint32_t flags, cudaStream_t stream);
+cr_status scratch_grow_queues(cr_context* ctx, BatchScratch& S, uint64_t ntWant, uint64_t hugeWant);
+void scratch_free(cr_context* ctx, BatchScratch& S);
+uint64_t scratch_bytes(const BatchScratch& S);
+
 // Adds the oldest frame of the timing ring to ctx->folded (waits for it).
 cr_status fold_oldest(cr_context* ctx);
 

@@ -159,6 +159,8 @@ struct CrResolveParams {
     float origin[3];            // viewI * (0,0,0,1)
     float p00, p11;             // proj[0][0], proj[1][1]
     uint32_t background;
+    uint32_t writeBackground;   // 1: empty pixels get the background
+    uint64_t idLo, idHi;        // covered pixels are written only for ids in [idLo, idHi)
 };
 
 // Launch helpers implemented in raster.cu / resolve.cu.
@@ -199,6 +201,21 @@ int cr_launch_stage3_views(const CrFrameParams& p, const CrBatchShape& s, void* 
 // CrView::resolveBlockBase is the prefix sum of the preceding views' blocks.
 int cr_launch_resolve_views(const CrResolveParams& base, const CrView* views, uint32_t numViews, uint32_t numBlocks,
                             void* stream);
+
+// Per-node culling of out-of-core scenes (nodes.cu).
+struct CrNodeCullParams {
+    const float* boxes;         // 6 per node: object-space min xyz, max xyz
+    const float* worlds;        // 16 per node, or nullptr: `world` for every node
+    const float* worldViews;    // 16 per node, or nullptr: `worldView` for every node
+    float world[16];
+    float worldView[16];
+    float planes[16];           // left, right, bottom, top: normal xyz, d
+    float threshold;            // size test (0: off, as the reference's default)
+    uint32_t frustum;           // 1: frustum test on
+    uint32_t numNodes;
+    uint32_t* visible;          // out: 1 per visible node
+};
+int cr_launch_node_cull(const CrNodeCullParams& p, void* stream);
 
 // Host helpers implemented in api.cpp.
 void cr_internal_set_error(const char* msg);

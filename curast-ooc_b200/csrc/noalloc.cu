@@ -208,6 +208,9 @@ extern "C" cr_status cr_render_noalloc(int32_t device, const cr_noalloc_instance
     rp.p00 = cam->proj[0];
     rp.p11 = cam->proj[5];
     rp.background = 0xffffffffu;
+    rp.writeBackground = 1u;
+    rp.idLo = 0ull;
+    rp.idHi = ~0ull;
 
     const uint64_t numPixels = (uint64_t)cam->width * (uint64_t)cam->height;
     const CrLaunchShape& shape = g_shape[device];

@@ -549,9 +549,10 @@ __device__ __forceinline__ int stage2_setup(const CrFrameParams& p, const Target
     return S2_RASTER;
 }
 
-// Narrows one bounding-box row (pixel row py, columns start_x + [0, size_x))
-// to [xlo, xlo + len): every column outside it provably fails the float test
-// of tv.cu:539-547, so skipping it cannot change the visbuffer.
+// Narrows the rows of one stage-2 bounding box (rows start_y + [0, size_y),
+// columns start_x + [0, size_x)) to spans [xlo, xlo + len): every column
+// outside a row's span provably fails the float test of tv.cu:539-547, so
+// skipping it cannot change the visbuffer.
 //
 // With u = 2^-24 and the setup values taken as exact inputs, the float
 // results of
@@ -562,51 +563,90 @@ __device__ __forceinline__ int stage2_setup(const CrFrameParams& p, const Target
 // (ax = px - asx, ay = py - asy; a standard first-order bound on the two
 // roundings of sx, the two products, the difference and the final product),
 // and |v_f - V| <= |s_f - S| + |t_f - T| + 2u (1 + |S| + |T|).  The margins
-// below over-cover these by 3x, in double precision, over the whole row; a
-// column whose S, T or V is below minus its margin cannot pass.  Non-finite
-// setups keep the whole row.
-__device__ __forceinline__ void row_span(float start_x, float py, int size_x, float asx, float asy, float abx,
-                                         float aby, float acx, float acy, float inv_det, int& xlo, int& len) {
-    xlo = 0;
-    len = size_x;
+// below over-cover these by 3x, in double precision, over the whole box (|ax|,
+// |ay|, |S| and |T| at their maxima over it); a column whose S, T or V is
+// below minus its margin cannot pass.  S, T and V are affine, so per row each
+// condition bounds the column by an affine function of the row: the setup
+// folds everything per triangle into three (g0 + g1 sy) forms, and a row
+// costs a few double operations.  Non-finite setups keep every row whole.
+struct S2Span {
+    double g0[3], g1[3];  // per condition: bound (or emptiness test) = g0 + g1 * sy
+    int kind[3];          // 1: lower bound on px, -1: upper bound, 0: empty if g0 + g1 * sy < 0
+    double px0;
+    int size_x;
+    bool whole;
+};
+
+__device__ __forceinline__ S2Span s2_span_setup(float start_x, float start_y, int size_x, int size_y, float asx,
+                                                float asy, float abx, float aby, float acx, float acy, float inv_det) {
     const double u = 5.9604644775390625e-08;
+    S2Span P;
+    P.size_x = size_x;
+    P.px0 = (double)start_x;
     const double di = (double)inv_det;
     const double px0 = (double)start_x, px1 = (double)start_x + (double)(size_x - 1);
     const double c0 = 0.5 - (double)asx;  // sx = px + c0 (exactly, in reals)
-    const double ay = (double)py - (double)asy;
-    const double sy = ay + 0.5;
+    const double sy0 = ((double)start_y - (double)asy) + 0.5;
+    const double sy1 = sy0 + (double)(size_y - 1);
     const double AX = fmax(fabs(px0 - (double)asx), fabs(px1 - (double)asx)) + 1.0;
-    const double AY = fabs(ay) + 1.0;
-    const double aS = (double)acy * di, bS = (c0 * (double)acy - sy * (double)acx) * di;
-    const double aT = -(double)aby * di, bT = ((double)abx * sy - (double)aby * c0) * di;
-    const double aV = -(aS + aT), bV = 1.0 - bS - bT;
-    const double Smax = fmax(fabs(aS * px0 + bS), fabs(aS * px1 + bS));
-    const double Tmax = fmax(fabs(aT * px0 + bT), fabs(aT * px1 + bT));
+    const double AY = fmax(fabs(sy0 - 0.5), fabs(sy1 - 0.5)) + 1.0;
+    // S = aS px + cS0 + cS1 sy, T = aT px + cT0 + cT1 sy, V = 1 - S - T
+    const double aS = (double)acy * di, cS0 = c0 * (double)acy * di, cS1 = -(double)acx * di;
+    const double aT = -(double)aby * di, cT0 = -(double)aby * c0 * di, cT1 = (double)abx * di;
+    auto absmax = [&](double a, double b0, double b1) {
+        return fmax(fmax(fabs(a * px0 + b0 + b1 * sy0), fabs(a * px1 + b0 + b1 * sy0)),
+                    fmax(fabs(a * px0 + b0 + b1 * sy1), fabs(a * px1 + b0 + b1 * sy1)));
+    };
+    const double Smax = absmax(aS, cS0, cS1), Tmax = absmax(aT, cT0, cT1);
     const double adi = fabs(di);
     const double Es = 16.0 * u * adi * (fabs((double)acy) * AX + fabs((double)acx) * AY) + 4.0 * u * Smax + 1e-37;
     const double Et = 16.0 * u * adi * (fabs((double)abx) * AY + fabs((double)aby) * AX) + 4.0 * u * Tmax + 1e-37;
     const double Ev = 2.0 * (Es + Et) + 4.0 * u * (Smax + Tmax + 1.0) + 1e-37;
-    double lo = px0, hi = px1;
-    bool empty = false;
-    // keep px with a*px + b >= -E; NaN bounds leave lo/hi unchanged
-    auto keep = [&](double a, double b, double E) {
-        if (a > 0.0) lo = fmax(lo, (-E - b) / a);
-        else if (a < 0.0) hi = fmin(hi, (-E - b) / a);
-        else if (b < -E) empty = true;
-    };
-    keep(aS, bS, Es);
-    keep(aT, bT, Et);
-    keep(aV, bV, Ev);
-    if (empty) {
-        len = 0;
-        return;
+    const double A[3] = {aS, aT, -(aS + aT)};
+    const double B0[3] = {cS0, cT0, 1.0 - cS0 - cT0};
+    const double B1[3] = {cS1, cT1, -(cS1 + cT1)};
+    const double E[3] = {Es, Et, Ev};
+    bool fin = isfinite(Ev);
+    // keep px with A px + B0 + B1 sy >= -E
+    for (int k = 0; k < 3; ++k) {
+        if (A[k] != 0.0) {
+            const double ia = 1.0 / A[k];
+            P.kind[k] = A[k] > 0.0 ? 1 : -1;
+            P.g0[k] = (-E[k] - B0[k]) * ia;
+            P.g1[k] = -B1[k] * ia;
+        } else {
+            P.kind[k] = 0;
+            P.g0[k] = B0[k] + E[k];
+            P.g1[k] = B1[k];
+        }
+        fin = fin && isfinite(P.g0[k]) && isfinite(P.g1[k]);
     }
-    double flo = floor(lo - px0) - 1.0;
-    double fhi = ceil(hi - px0) + 1.0;
+    P.whole = !fin;
+    return P;
+}
+
+__device__ __forceinline__ void s2_row_span(const S2Span& P, float py, float asy, int& xlo, int& len) {
+    xlo = 0;
+    len = P.size_x;
+    if (P.whole) return;
+    const double sy = ((double)py - (double)asy) + 0.5;
+    double lo = P.px0, hi = P.px0 + (double)(P.size_x - 1);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const double g = P.g0[k] + P.g1[k] * sy;
+        if (P.kind[k] > 0) lo = fmax(lo, g);
+        else if (P.kind[k] < 0) hi = fmin(hi, g);
+        else if (g < 0.0) {
+            len = 0;
+            return;
+        }
+    }
+    double flo = floor(lo - P.px0) - 1.0;
+    double fhi = ceil(hi - P.px0) + 1.0;
     flo = fmax(flo, 0.0);
-    fhi = fmin(fhi, (double)(size_x - 1));
+    fhi = fmin(fhi, (double)(P.size_x - 1));
     if (!(flo <= fhi)) {
-        if (flo > fhi) len = 0;  // NaN keeps the whole row
+        if (flo > fhi) len = 0;
         return;
     }
     xlo = (int)flo;
@@ -713,14 +753,13 @@ __global__ void __launch_bounds__(WARPS * 32) k_stage2(const CrFrameParams p) {
             const int size_y = nf / size_x;
             // The reference tests every fragment of the bounding box.  Here each
             // row is first narrowed to the columns whose exact float test can
-            // still pass (row_span), the surviving spans of 32 rows are packed
+            // still pass (s2_row_span), the surviving spans of 32 rows are packed
             // across the lanes, and each fragment then runs the reference's
             // test unchanged -- so the same fragments are written.
+            const S2Span sp = s2_span_setup(start_x, start_y, size_x, size_y, asx, asy, abx, aby, acx, acy, inv_det);
             for (int r0 = 0; r0 < size_y; r0 += 32) {
                 int xlo = 0, len = 0;
-                if (r0 + lane < size_y)
-                    row_span(start_x, start_y + (float)(r0 + lane), size_x, asx, asy, abx, aby, acx, acy, inv_det,
-                             xlo, len);
+                if (r0 + lane < size_y) s2_row_span(sp, start_y + (float)(r0 + lane), asy, xlo, len);
                 int incl = len;
 #pragma unroll
                 for (int d = 1; d < 32; d <<= 1) {
@@ -785,8 +824,108 @@ __device__ __forceinline__ float intersect_mt(V3 dir, V3 v0, V3 e1, V3 e2) {
     return t > 0.0f ? t : INFINITY;
 }
 
+// Which pixels of a stage-3 tile can pass intersect_mt.  With the float
+// ray direction dir = normalize(d), d = (rx, ry, -1), and tvec = -a:
+//     det = dir . N1,  U = dir . N2,  V = dir . Q,  T = e2 . Q
+// (N1 = e2 x e1, N2 = e2 x tvec, Q = tvec x e1), u = U / det, v = V / det,
+// t = T / det.  A hit needs t > 0, so det has the sign s of T, and then
+// s U >= 0, s V >= 0 and s (U + V - det) <= 0 -- all linear in d, hence in
+// the column for a fixed row.  The float test differs from these exact
+// values by the rounding of the cross and dot products (<= 8u products of
+// the 1-norms of the factors), of the normalisation and of rx, ry (absorbed
+// as perturbations of d), and of the division and sum (<= 6u |det|); the
+// margins below over-cover all of them by 2x, in double precision, so a
+// column outside the span cannot pass the float test.  A triangle whose T is
+// within its error bound of 0, or with non-finite values, is not pruned.
+struct S3Prune {
+    bool on;
+    int s;
+    double n1[3], n2[3], q[3], k[3];  // k = N2 + Q - N1
+    double mD, mU, mV, mK;            // margins as multiples of |d| (unnormalised)
+    double ex, ey;                    // absolute error of rx, ry
+};
+
+__device__ __forceinline__ void cross_d(const double* a, const double* b, double* c) {
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+__device__ __forceinline__ S3Prune s3_prune_setup(V3 av, V3 e1f, V3 e2f, float fa, float f) {
+    const double u = 5.9604644775390625e-08;
+    S3Prune P;
+    const double t[3] = {-(double)av.x, -(double)av.y, -(double)av.z};
+    const double e1[3] = {e1f.x, e1f.y, e1f.z}, e2[3] = {e2f.x, e2f.y, e2f.z};
+    cross_d(e2, e1, P.n1);
+    cross_d(e2, t, P.n2);
+    cross_d(t, e1, P.q);
+    for (int i = 0; i < 3; ++i) P.k[i] = P.n2[i] + P.q[i] - P.n1[i];
+    const double T = e2[0] * P.q[0] + e2[1] * P.q[1] + e2[2] * P.q[2];
+    auto n1s = [](const double* v) { return fabs(v[0]) + fabs(v[1]) + fabs(v[2]); };
+    const double St = n1s(t), S1 = n1s(e1), S2 = n1s(e2);
+    const double eD = 8.0 * u * 1.001 * S1 * S2, eU = 8.0 * u * 1.001 * St * S2, eV = 8.0 * u * 1.001 * St * S1;
+    const double eT = 8.0 * u * S2 * St * S1;
+    P.mD = eD;
+    P.mU = eU;
+    P.mV = eV;
+    P.mK = 6.0 * u * 1.001 * n1s(P.n1) + 1.01 * eD + eU + eV;
+    P.ex = 8.0 * u * (1.0 / (double)fa);
+    P.ey = 8.0 * u * (1.0 / (double)f);
+    P.on = isfinite(T) && isfinite(eT) && fabs(T) > 2.0 * eT && isfinite(P.mK);
+    P.s = T > 0.0 ? 1 : -1;
+    return P;
+}
+
+// Columns [xlo, xlo + len) of tile row py (columns fx0 + [0, 64)) that can
+// pass; the whole row when pruning is off or anything is not finite.
+__device__ __forceinline__ void s3_row_span(const S3Prune& P, float fx0, float py, float Wf, float Hf, float fa,
+                                           float f, int& xlo, int& len) {
+    xlo = 0;
+    len = CR_TILE_SIZE;
+    if (!P.on) return;
+    const double u = 5.9604644775390625e-08;
+    const double ia = 1.0 / (double)fa, ib = 1.0 / (double)f;
+    // rx(c) = A c + B for c = 0..63 (exact affine model of the float rx)
+    const double A = 2.0 * ia / (double)Wf;
+    const double B = ia * (2.0 * ((double)fx0 + 0.5) / (double)Wf - 1.0);
+    const double ry = ib * (2.0 * ((double)py + 0.5) / (double)Hf - 1.0);
+    const double dxm = fmax(fabs(B), fabs(A * 63.0 + B)) + P.ex, dym = fabs(ry) + P.ey;
+    const double dn = sqrt(dxm * dxm + dym * dym + 1.0) * (1.0 + 16.0 * u);
+    const double ex = P.ex + 2.0 * u * dxm, ey = P.ey + 2.0 * u * dym;
+    double lo = 0.0, hi = 63.0;
+    bool empty = false;
+    // keep columns with sg * (N . d) >= -margin, d = (A c + B, ry, -1)
+    auto keep = [&](const double* N, double sg, double eps) {
+        const double m = 2.0 * (eps * dn + fabs(N[0]) * ex + fabs(N[1]) * ey +
+                                8.0 * u * (fabs(N[0]) * dxm + fabs(N[1]) * dym + fabs(N[2])));
+        const double a = sg * N[0] * A;
+        const double b = sg * (N[0] * B + N[1] * ry - N[2]);
+        if (a > 0.0) lo = fmax(lo, (-m - b) / a);
+        else if (a < 0.0) hi = fmin(hi, (-m - b) / a);
+        else if (b < -m) empty = true;
+    };
+    const double s = (double)P.s;
+    keep(P.n1, s, P.mD);
+    keep(P.n2, s, P.mU);
+    keep(P.q, s, P.mV);
+    keep(P.k, -s, P.mK);
+    if (empty) {
+        len = 0;
+        return;
+    }
+    double flo = floor(lo) - 1.0, fhi = ceil(hi) + 1.0;
+    flo = fmax(flo, 0.0);
+    fhi = fmin(fhi, 63.0);
+    if (!(flo <= fhi)) {
+        if (flo > fhi) len = 0;  // NaN keeps the whole row
+        return;
+    }
+    xlo = (int)flo;
+    len = (int)(fhi - flo) + 1;
+}
+
 template <int WARPS, bool MULTI>
-__global__ void __launch_bounds__(WARPS * 32) k_stage3(const CrFrameParams p) {
+__global__ void __launch_bounds__(WARPS * 32, 3) k_stage3(const CrFrameParams p) {
     const int lane = threadIdx.x & 31;
     const uint64_t gw = (uint64_t)blockIdx.x * WARPS + (threadIdx.x >> 5);
     const uint64_t nw = (uint64_t)gridDim.x * WARPS;
@@ -827,23 +966,46 @@ __global__ void __launch_bounds__(WARPS * 32) k_stage3(const CrFrameParams p) {
         const float min_y = clamp_ref((float)(tile.tile_y * CR_TILE_SIZE), 0.0f, Hf);
         const float fx0 = floorf(min_x);
         const float fy0 = floorf(min_y);
-        // each lane owns columns lane and lane + 32
-        int px[2];
-        float rx[2];
+        // rows in two groups of 32: each lane finds the passing columns of
+        // rows lane and lane + 32, then each group's spans are packed across
+        // the lanes
+        int spanLo[2], spanLen[2];
+        {
+            const S3Prune P = s3_prune_setup(av, e1, e2, fa, f);
 #pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            px[c] = (int)(fx0 + (float)(lane + 32 * c));
-            const float u = 2.0f * ((float)px[c] + 0.5f) / Wf - 1.0f;
-            rx[c] = (1.0f / fa) * u;
+            for (int g = 0; g < 2; ++g)
+                s3_row_span(P, fx0, (float)(int)(fy0 + (float)(32 * g + lane)), Wf, Hf, fa, f, spanLo[g], spanLen[g]);
         }
-        for (int y = 0; y < CR_TILE_SIZE; ++y) {
-            const int py = (int)(fy0 + (float)y);
-            const float v = 2.0f * ((float)py + 0.5f) / Hf - 1.0f;
-            const float ry = (1.0f / f) * v;
 #pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                const int pid = px[c] + tg.W * py;
-                const V3 d = {rx[c], ry, -1.0f};
+        for (int g = 0; g < 2; ++g) {
+            const int r0 = 32 * g;
+            const int xlo = spanLo[g], len = spanLen[g];
+            int incl = len;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int v = __shfl_up_sync(FULL, incl, d);
+                if (lane >= d) incl += v;
+            }
+            const int total = __shfl_sync(FULL, incl, 31);
+            for (int base = 0; base < total; base += 32) {
+                const int k = base + lane;
+                int r = 0;
+#pragma unroll
+                for (int step = 16; step >= 1; step >>= 1) {
+                    const int c = __shfl_sync(FULL, incl, r + step - 1);
+                    if (c <= k) r += step;
+                }
+                const int rx0 = __shfl_sync(FULL, xlo, r);
+                const int rend = __shfl_sync(FULL, incl, r);
+                const int rlen = __shfl_sync(FULL, len, r);
+                if (k >= total) continue;
+                // the reference's per-pixel ray (tv.cu:690-705), unchanged
+                const int px = (int)(fx0 + (float)(rx0 + (k - (rend - rlen))));
+                const int py = (int)(fy0 + (float)(r0 + r));
+                const float uu = 2.0f * ((float)px + 0.5f) / Wf - 1.0f;
+                const float vv = 2.0f * ((float)py + 0.5f) / Hf - 1.0f;
+                const V3 d = {(1.0f / fa) * uu, (1.0f / f) * vv, -1.0f};
+                const int pid = px + tg.W * py;
                 const float inv = 1.0f / sqrtf(dot3(d, d));
                 const V3 dir = {d.x * inv, d.y * inv, d.z * inv};
                 const float t = intersect_mt(dir, av, e1, e2);

@@ -68,6 +68,7 @@ __device__ __forceinline__ void resolve_pixel(const CrResolveParams& p, const in
     const float depth = (ud == 0x7FFFFFF8u) ? INFINITY : __uint_as_float(ud);
     const uint64_t tid = pixel & 0xFFFFFFFFFull;
 
+    if (isinf(depth) ? !p.writeBackground : (tid < p.idLo || tid >= p.idHi)) return;  // another pass owns it
     uint32_t color = 0;
     if (!isinf(depth)) {
         // instance whose [cum, next cum) holds tid (resolve.cu:697-721)

@@ -129,6 +129,80 @@ class CrView(ctypes.Structure):
     _fields_ = [("camera", CrCamera), ("d_visbuffer", _u64), ("d_rgba", _u64), ("d_colorbuffer", _u64)]
 
 
+class CrOocNode(ctypes.Structure):
+    _fields_ = [
+        ("positions", ctypes.c_void_p),
+        ("indices", ctypes.c_void_p),
+        ("colors", ctypes.c_void_p),
+        ("num_vertices", _u32),
+        ("num_triangles", _u32),
+        ("aabb_min", _f32 * 3),
+        ("aabb_max", _f32 * 3),
+        ("world", _f32 * 16),
+    ]
+
+
+class CrOocConfig(ctypes.Structure):
+    _fields_ = [("geometry_budget", _u64), ("size_threshold", _f32), ("frustum_culling", _u32), ("reserved", _u32 * 4)]
+
+
+class CrOocStats(ctypes.Structure):
+    _fields_ = [
+        ("visible_nodes", _u32),
+        ("resident_hits", _u32),
+        ("uploaded_nodes", _u32),
+        ("evicted_nodes", _u32),
+        ("passes", _u32),
+        ("cache_slots", _u32),
+        ("uploaded_bytes", _u64),
+        ("visible_triangles", _u64),
+    ]
+
+
+CR_OOC_MAX_NODE_TRIANGLES = 65536
+
+
+class CrServerConfig(ctypes.Structure):
+    _fields_ = [("memory_budget", _u64), ("slots", _u32), ("max_batch_views", _u32), ("display", _i32),
+                ("reserved", _u32 * 5)]
+
+
+class CrServerRequest(ctypes.Structure):
+    _fields_ = [("scene", _u32), ("reserved", _u32), ("camera", CrCamera)]
+
+
+class CrServerResult(ctypes.Structure):
+    _fields_ = [
+        ("ticket", _u64),
+        ("status", _i32),
+        ("scene", _u32),
+        ("width", _i32),
+        ("height", _i32),
+        ("d_visbuffer", _u64),
+        ("d_rgba", _u64),
+        ("submit_us", ctypes.c_double),
+        ("start_us", ctypes.c_double),
+        ("done_us", ctypes.c_double),
+        ("batch_views", _u32),
+        ("reserved", _u32),
+    ]
+
+
+class CrServerStats(ctypes.Structure):
+    _fields_ = [
+        ("submitted", _u64),
+        ("completed", _u64),
+        ("batches", _u64),
+        ("batched_views", _u64),
+        ("budget_bytes", _u64),
+        ("peak_bytes", _u64),
+        ("p50_ms", ctypes.c_double),
+        ("p99_ms", ctypes.c_double),
+        ("mean_ms", ctypes.c_double),
+        ("views_per_s", ctypes.c_double),
+    ]
+
+
 class CrTuning(ctypes.Structure):
     _fields_ = [
         ("scene_class", _u32),
@@ -183,7 +257,127 @@ EXPORTS = {
                                  ctypes.POINTER(CrTuning)]),
     "cr_get_tuning": (_i32, [ctypes.c_void_p, _u32, ctypes.POINTER(CrTuning)]),
     "cr_scene_class": (_u32, [_u64, _u64, _u32]),
+    "cr_ooc_create": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrOocNode), _u32, ctypes.POINTER(CrOocConfig),
+                             ctypes.POINTER(ctypes.c_void_p)]),
+    "cr_ooc_render": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrCamera), _u64, _u64, _i32, _u32, ctypes.c_void_p,
+                             ctypes.POINTER(CrOocStats)]),
+    "cr_ooc_select": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrCamera), ctypes.c_void_p]),
+    "cr_ooc_destroy": (_i32, [ctypes.c_void_p]),
+    "cr_server_create": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrServerConfig), ctypes.POINTER(ctypes.c_void_p)]),
+    "cr_server_add_scene": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrInstance), _u32, ctypes.POINTER(_u32)]),
+    "cr_server_add_ooc_scene": (_i32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(_u32)]),
+    "cr_server_submit": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrServerRequest), ctypes.POINTER(_u64)]),
+    "cr_server_poll": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrServerResult), _u32, ctypes.POINTER(_u32)]),
+    "cr_server_wait": (_i32, [ctypes.c_void_p, _u64, _u32, ctypes.POINTER(CrServerResult)]),
+    "cr_server_release": (_i32, [ctypes.c_void_p, _u64]),
+    "cr_server_get_stats": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrServerStats)]),
+    "cr_server_destroy": (_i32, [ctypes.c_void_p]),
 }
+
+
+class Server:
+    """cr_server: continuous batching over resident scenes."""
+
+    def __init__(self, ctx, memory_budget=0, slots=0, max_batch_views=0, display=CR_DISPLAY_VERTEX_COLORS):
+        cfg = CrServerConfig(int(memory_budget), int(slots), int(max_batch_views), int(display))
+        h = ctypes.c_void_p()
+        _check(load().cr_server_create(ctx.h, ctypes.byref(cfg), ctypes.byref(h)))
+        self.h = h
+
+    def add_scene(self, instances):
+        arr, n = make_instances(instances) if not isinstance(instances, tuple) else instances
+        out = _u32()
+        _check(load().cr_server_add_scene(self.h, arr, n, ctypes.byref(out)))
+        return out.value
+
+    def add_ooc_scene(self, ooc):
+        out = _u32()
+        _check(load().cr_server_add_ooc_scene(self.h, ooc.h, ctypes.byref(out)))
+        return out.value
+
+    def submit(self, scene, camera):
+        r = CrServerRequest(int(scene), 0, camera)
+        t = _u64()
+        _check(load().cr_server_submit(self.h, ctypes.byref(r), ctypes.byref(t)))
+        return t.value
+
+    def poll(self, max_results=256):
+        arr = (CrServerResult * max_results)()
+        n = _u32()
+        _check(load().cr_server_poll(self.h, arr, max_results, ctypes.byref(n)))
+        return [arr[k] for k in range(n.value)]
+
+    def wait(self, ticket, timeout_ms=60000):
+        r = CrServerResult()
+        _check(load().cr_server_wait(self.h, int(ticket), int(timeout_ms), ctypes.byref(r)))
+        return r
+
+    def release(self, ticket):
+        _check(load().cr_server_release(self.h, int(ticket)))
+
+    def stats(self):
+        s = CrServerStats()
+        _check(load().cr_server_get_stats(self.h, ctypes.byref(s)))
+        return s
+
+    def close(self):
+        if self.h:
+            load().cr_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class OocScene:
+    """cr_ooc: nodes whose geometry stays in pinned host memory.
+
+    nodes: iterable of (positions_addr, indices_addr, colors_addr or 0,
+    num_vertices, num_triangles, aabb_min, aabb_max, world) -- host addresses
+    of pinned buffers (e.g. tensor.data_ptr() of pin_memory tensors)."""
+
+    def __init__(self, ctx, nodes, geometry_budget, size_threshold=0.0, frustum_culling=1):
+        nodes = list(nodes)
+        arr = (CrOocNode * len(nodes))()
+        for k, (pp, ip, cp, nv, nt, lo, hi, world) in enumerate(nodes):
+            arr[k].positions = int(pp)
+            arr[k].indices = int(ip)
+            arr[k].colors = int(cp) if cp else None
+            arr[k].num_vertices = int(nv)
+            arr[k].num_triangles = int(nt)
+            arr[k].aabb_min = (_f32 * 3)(*[float(x) for x in lo])
+            arr[k].aabb_max = (_f32 * 3)(*[float(x) for x in hi])
+            arr[k].world = _f16(world)
+        cfg = CrOocConfig(int(geometry_budget), float(size_threshold), int(frustum_culling))
+        h = ctypes.c_void_p()
+        _check(load().cr_ooc_create(ctx.h, arr, len(nodes), ctypes.byref(cfg), ctypes.byref(h)))
+        self.h = h
+        self.count = len(nodes)
+
+    def render(self, camera, d_visbuffer, d_rgba=0, display=CR_DISPLAY_VERTEX_COLORS, flags=CR_RENDER_SYNC, stream=0):
+        st = CrOocStats()
+        _check(load().cr_ooc_render(self.h, ctypes.byref(camera), int(d_visbuffer), int(d_rgba), int(display),
+                                    int(flags), ctypes.c_void_p(int(stream)), ctypes.byref(st)))
+        return st
+
+    def select(self, camera):
+        out = np.zeros(self.count, np.uint8)
+        _check(load().cr_ooc_select(self.h, ctypes.byref(camera), out.ctypes.data))
+        return out
+
+    def close(self):
+        if self.h:
+            load().cr_ooc_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def make_views(views):

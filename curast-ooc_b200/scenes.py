@@ -443,3 +443,92 @@ def batch_cameras(num_views=64, seed=37, resolutions=BATCH_RESOLUTIONS, scale=1.
         proj = perspective(60.0, W / H, 0.001, 10.0)
         cams.append((view, proj, W, H))
     return cams
+
+
+# ---------------------------------------------------------------------------
+# the out-of-core scene: a large terrain cut into nodes of <= 64K triangles
+# ---------------------------------------------------------------------------
+def ooc_terrain(nodes_x=247, nodes_z=247, quads=181, seed=41, extent=8.0, with_colors=False, device="cuda"):
+    """Nodes of a seeded fractal terrain over [0, extent]^2 (x/z): node (i, j)
+    is a quads x quads grid (2 triangles per quad; 181 -> 65,522 triangles)
+    over its square of a nodes_x x nodes_z tiling, stored node after node in
+    pinned host memory (247 x 247 nodes: 3.997e9 triangles, 72 GB without
+    colours).  Built on `device` a batch of nodes at a time.
+
+    Returns (nodes, keep): nodes as pycurast.OocScene expects them
+    (host addresses of the pinned tensors, identity world) and the tensors
+    that own the memory."""
+    import torch
+
+    n = quads
+    nv, nt = (n + 1) * (n + 1), 2 * n * n
+    count = nodes_x * nodes_z
+    pos = torch.empty((count, nv, 3), dtype=torch.float32, pin_memory=True)
+    idx = torch.empty((count, nt, 3), dtype=torch.int32, pin_memory=True)
+    col = torch.empty((count, nv), dtype=torch.int32, pin_memory=True) if with_colors else None
+    waves = _terrain_waves(seed, TERRAIN["octaves"], TERRAIN["f0"])
+    # one node's index pattern (the same for every node)
+    g = torch.arange(nt, device=device, dtype=torch.int64)
+    q = g // 2
+    j = q // n
+    i = q % n
+    v00 = j * (n + 1) + i
+    second = (g % 2) == 1
+    local = torch.stack([torch.where(second, v00 + 1, v00), v00 + (n + 1),
+                         torch.where(second, v00 + n + 2, v00 + 1)], 1).to(torch.int32)
+    lv = torch.arange(nv, device=device, dtype=torch.int64)
+    lx = (lv % (n + 1)).double()
+    lz = (lv // (n + 1)).double()
+    batch = 256
+    boxes = np.empty((count, 6), np.float32)
+    amp = TERRAIN["amp"] * extent
+    for b0 in range(0, count, batch):
+        ks = torch.arange(b0, min(count, b0 + batch), device=device, dtype=torch.int64)
+        ni = (ks % nodes_x).double()
+        nj = (ks // nodes_x).double()
+        x = (ni[:, None] * n + lx[None, :]) / (nodes_x * n) * extent
+        z = (nj[:, None] * n + lz[None, :]) / (nodes_z * n) * extent
+        h = torch.zeros_like(x)
+        for c, s, fr, ph, a in waves:
+            h += a * torch.sin(fr * (x * c + z * s) / extent + ph)
+        p = torch.stack([x.float(), (amp * h).float(), z.float()], 2)
+        pos[b0:b0 + ks.shape[0]].copy_(p)
+        idx[b0:b0 + ks.shape[0]].copy_(local[None].expand(ks.shape[0], -1, -1))
+        boxes[b0:b0 + ks.shape[0], :3] = p.amin(1).cpu().numpy()
+        boxes[b0:b0 + ks.shape[0], 3:] = p.amax(1).cpu().numpy()
+        if col is not None:
+            gen = torch.Generator(device=device)
+            gen.manual_seed(seed * 1000003 + b0)
+            col[b0:b0 + ks.shape[0]].copy_(torch.randint(-2**31, 2**31 - 1, (ks.shape[0], nv), dtype=torch.int32,
+                                                         device=device, generator=gen))
+    world = identity()
+    pb, ib = pos.data_ptr(), idx.data_ptr()
+    cb = col.data_ptr() if col is not None else 0
+    nodes = [(pb + k * nv * 12, ib + k * nt * 12, (cb + k * nv * 4) if cb else 0, nv, nt, boxes[k, :3], boxes[k, 3:],
+              world) for k in range(count)]
+    return nodes, (pos, idx, col, boxes)
+
+
+def ooc_cameras(num_views, seed=43, extent=8.0, terrain_seed=41, resolutions=BATCH_RESOLUTIONS, scale=1.0):
+    """Cameras over the out-of-core terrain: eye 0.05-0.4 x extent/8 above
+    the surface, looking 0.3-1.2 x extent/8 ahead (as batch_cameras)."""
+    rng = np.random.default_rng(seed)
+    cams = []
+    u = extent / 8.0
+    amp = TERRAIN["amp"] * extent
+
+    def height(x, z):
+        return float(amp * terrain_height(x / extent, z / extent, terrain_seed) / TERRAIN["amp"])
+
+    for _ in range(num_views):
+        W, H = resolutions[int(rng.integers(len(resolutions)))]
+        W = max(1, int(round(W * scale)))
+        H = max(1, int(round(H * scale)))
+        ex, ez = rng.uniform(0.1 * extent, 0.9 * extent, 2)
+        ey = height(ex, ez) + rng.uniform(0.05, 0.4) * u
+        yaw = rng.uniform(0.0, 2.0 * math.pi)
+        dist = rng.uniform(0.3, 1.2) * u
+        tx, tz = ex + dist * math.cos(yaw), ez + dist * math.sin(yaw)
+        view = look_at((ex, ey, ez), (tx, height(tx, tz), tz))
+        cams.append((view, perspective(60.0, W / H, 0.001, 100.0), W, H))
+    return cams

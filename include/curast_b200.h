@@ -284,6 +284,133 @@ cr_status cr_autotune_batch(cr_context* ctx, const cr_instance* instances, uint3
 cr_status cr_get_tuning(cr_context* ctx, uint32_t scene_class, cr_tuning* out);
 uint32_t cr_scene_class(uint64_t triangles, uint64_t pixels, uint32_t num_views);
 
+/* ---- out-of-core scenes ------------------------------------------------------
+ * A scene of many nodes whose geometry stays in the caller's pinned host
+ * memory.  Per view, the nodes the reference would draw are selected on the
+ * GPU by the reference's own node culling (SNTriangles::update,
+ * src/scene/SNTriangles.h:29-105: world AABB against the four side planes of
+ * proj * view, and the size test, in the same float operations); the
+ * selected nodes are made resident in a device cache of at most
+ * geometry_budget bytes -- missing ones copied with cudaMemcpyAsync on the
+ * scene's own copy stream, least recently used ones evicted -- and drawn as
+ * one frame in the reference's order (triangle count descending, then node
+ * index; src/CuRast_render.h:316-345), ids being the prefix sum over the
+ * selected nodes.  A selection larger than the cache is drawn in several
+ * passes into the same visbuffer with the same ids, then resolved group by
+ * group, so the output does not depend on the budget. */
+#define CR_OOC_MAX_NODE_TRIANGLES 65536u
+
+typedef struct cr_ooc_node {
+    const float* positions;     /* host, pinned (cudaHostAlloc / cudaHostRegister) */
+    const uint32_t* indices;    /* host, pinned; 3 per triangle                    */
+    const uint32_t* colors;     /* host, pinned; RGBA8 per vertex, or NULL          */
+    uint32_t num_vertices;
+    uint32_t num_triangles;     /* at most CR_OOC_MAX_NODE_TRIANGLES               */
+    float aabb_min[3];          /* object space                                    */
+    float aabb_max[3];
+    float world[16];            /* object -> world                                 */
+} cr_ooc_node;
+
+typedef struct cr_ooc_config {
+    uint64_t geometry_budget;   /* device bytes for resident node geometry         */
+    float size_threshold;       /* CuRastSettings::threshold (0: off, its default) */
+    uint32_t frustum_culling;   /* CuRastSettings::enableFrustumCulling (1)        */
+    uint32_t reserved[4];
+} cr_ooc_config;
+
+typedef struct cr_ooc_stats {
+    uint32_t visible_nodes;
+    uint32_t resident_hits;     /* selected nodes already on the device            */
+    uint32_t uploaded_nodes;
+    uint32_t evicted_nodes;
+    uint32_t passes;            /* raster passes (> 1: selection exceeded the cache) */
+    uint32_t cache_slots;
+    uint64_t uploaded_bytes;
+    uint64_t visible_triangles;
+} cr_ooc_stats;
+
+typedef struct cr_ooc cr_ooc;
+
+cr_status cr_ooc_create(cr_context* ctx, const cr_ooc_node* nodes, uint32_t count,
+                        const cr_ooc_config* cfg, cr_ooc** out);
+/* Renders one view (flags and buffers as cr_render; CR_RENDER_KEEP_ORDER
+ * and CR_RENDER_NO_CLEAR are not accepted).  Waits for the node selection
+ * (a small device-to-host copy); waits for the frame only with
+ * CR_RENDER_SYNC.  stats may be NULL. */
+cr_status cr_ooc_render(cr_ooc* ooc, const cr_camera* camera, uint64_t d_visbuffer, uint64_t d_rgba,
+                        int32_t display, uint32_t flags, void* stream, cr_ooc_stats* stats);
+/* The node selection alone: visible[i] = 1 if node i would be drawn. */
+cr_status cr_ooc_select(cr_ooc* ooc, const cr_camera* camera, uint8_t* visible);
+cr_status cr_ooc_destroy(cr_ooc* ooc);
+
+/* ---- serving ------------------------------------------------------------------
+ * No counterpart in the reference (one interactive view).  A server owns
+ * resident scenes (instance sets of the context's meshes, or out-of-core
+ * scenes) and renders requests of mixed resolution and scene as they arrive,
+ * with continuous batching: a dispatcher thread admits each request as soon
+ * as its visbuffer and RGBA8 image fit in the memory budget, and whenever one
+ * of `slots` device streams is free launches the requests waiting for the
+ * scene of the oldest one as one batched frame (cr_render_batch's kernels,
+ * up to max_batch_views views), so batches of different scenes overlap on
+ * the device.  Requests of out-of-core scenes run one at a time on their own
+ * lane (cr_ooc_render), beside the batches.  Each result is bit-identical
+ * to cr_render of the same view alone.  While a server exists, its context
+ * is used only through the server. */
+typedef struct cr_server cr_server;
+
+typedef struct cr_server_config {
+    uint64_t memory_budget;    /* bytes for framebuffers + slot queues (0: 64 GiB) */
+    uint32_t slots;            /* batches in flight (device streams; 0: 3)          */
+    uint32_t max_batch_views;  /* views per batch (1..64; 0: 64)                    */
+    int32_t display;           /* resolve mode of every request                    */
+    uint32_t reserved[5];
+} cr_server_config;
+
+typedef struct cr_server_request {
+    uint32_t scene;            /* from cr_server_add_scene / _add_ooc_scene         */
+    uint32_t reserved;
+    cr_camera camera;
+} cr_server_request;
+
+typedef struct cr_server_result {
+    uint64_t ticket;
+    int32_t status;            /* CR_OK or the error of its frame                 */
+    uint32_t scene;
+    int32_t width, height;
+    uint64_t d_visbuffer;      /* server-owned; valid until cr_server_release     */
+    uint64_t d_rgba;
+    double submit_us;          /* host steady clock, microseconds                  */
+    double start_us;           /* its batch was issued                             */
+    double done_us;            /* its batch finished on the device                 */
+    uint32_t batch_views;      /* views in the batch it rode in                    */
+    uint32_t reserved;
+} cr_server_result;
+
+typedef struct cr_server_stats {
+    uint64_t submitted, completed, batches, batched_views;
+    uint64_t budget_bytes, peak_bytes;  /* framebuffer + slot bytes               */
+    double p50_ms, p99_ms, mean_ms;     /* submit -> done of completed requests     */
+    double views_per_s;                 /* completed / (last done - first submit)   */
+} cr_server_stats;
+
+cr_status cr_server_create(cr_context* ctx, const cr_server_config* cfg, cr_server** out);
+cr_status cr_server_add_scene(cr_server* server, const cr_instance* instances, uint32_t count,
+                              uint32_t* scene_out);
+cr_status cr_server_add_ooc_scene(cr_server* server, cr_ooc* ooc, uint32_t* scene_out);
+/* Never blocks; the request waits for memory and a slot inside the server.
+ * CR_ERR_INVALID for an unknown scene, a bad camera or a request larger than
+ * the whole budget. */
+cr_status cr_server_submit(cr_server* server, const cr_server_request* request, uint64_t* ticket);
+/* Completed results not yet returned, in completion order. */
+cr_status cr_server_poll(cr_server* server, cr_server_result* results, uint32_t max, uint32_t* count);
+/* Waits (up to timeout_ms) for one request; CR_ERR_TIMEOUT if it is not done. */
+cr_status cr_server_wait(cr_server* server, uint64_t ticket, uint32_t timeout_ms, cr_server_result* result);
+/* Returns a completed request's buffers to the budget. */
+cr_status cr_server_release(cr_server* server, uint64_t ticket);
+cr_status cr_server_get_stats(cr_server* server, cr_server_stats* stats);
+/* Waits for every submitted request, then stops the threads. */
+cr_status cr_server_destroy(cr_server* server);
+
 /* ---- rendering without allocating ----------------------------------------
  * No counterpart in the reference (CuRast allocates its queues and buffers
  * itself).  For callers that must not allocate device memory while they
