@@ -158,6 +158,7 @@ cr_status assemble(cr_context* ctx, const cr_instance* instances, uint32_t count
         ci.numVertices = m.numVertices;
         ci.outBase = A.outBytes;
         ci.vchunkBase = A.numVChunks;
+        ci.chunkBoxes = m.chunkBoxes;
         A.outBytes += align_up(m.numVertices, 16);
         A.numVChunks += (m.numVertices + CR_VCHUNK - 1) / CR_VCHUNK;
         float* wv = &A.worldView[16ull * r];
@@ -174,6 +175,7 @@ cr_status assemble(cr_context* ctx, const cr_instance* instances, uint32_t count
             s.firstInstance = r;
             s.instanceCount = 0;
             s.flags = (m.indices && ((uintptr_t)m.indices & 15u) == 0) ? 1u : 0u;
+            s.itemBoxes = m.itemBoxes;
             A.seg.push_back(s);
         }
         A.seg.back().instanceCount++;
@@ -211,6 +213,21 @@ cr_status ensure_queues(cr_context* ctx, uint64_t ntWant, uint64_t hugeWant) {
         if (s) return s;
         ctx->hugeCap = hugeWant;
     }
+    return CR_OK;
+}
+
+cr_status build_mesh_boxes(cr_context* ctx, MeshRec& m) {
+    const size_t ib = align_up((size_t)((m.numTriangles + CR_BATCH - 1) / CR_BATCH) * 24, 256);
+    const size_t cb = align_up((size_t)((m.numVertices + CR_VCHUNK - 1) / CR_VCHUNK) * 24, 256);
+    if (!m.itemBoxes) {
+        cr_status s = ctx->dev_alloc((void**)&m.itemBoxes, ib + cb, "mesh boxes");
+        if (s) return s;
+        m.chunkBoxes = (float*)((char*)m.itemBoxes + ib);
+        m.boxBytes = ib + cb;
+    }
+    if (cr_launch_mesh_boxes(m.indices, m.positions, m.numTriangles, m.numVertices, m.itemBoxes, m.chunkBoxes, 0))
+        return fail(CR_ERR_CUDA, "mesh box launch: %s", cudaGetErrorString(cudaGetLastError()));
+    CR_CUDA(cudaDeviceSynchronize(), "mesh boxes");
     return CR_OK;
 }
 
@@ -292,8 +309,17 @@ cr_status fold_oldest(cr_context* ctx) {
     return CR_OK;
 }
 
+void read_counters(cr_context* ctx) {
+    const unsigned long long* c = ctx->hCounters;
+    ctx->last.nontrivial = c[CR_CTR_NONTRIVIAL];
+    ctx->last.huge_tiles = c[CR_CTR_HUGE];
+    ctx->last.overflow = c[CR_CTR_OVERFLOW];
+    ctx->last.work_items_drawn = ctx->last.work_items ? c[CR_CTR_ITEMS] : 0;
+    ctx->last.vertex_chunks_evaluated = ctx->last.vertex_chunks ? c[CR_CTR_CHUNKS] : 0;
+}
+
 cr_status run_frame(cr_context* ctx, uint32_t flags, cudaStream_t stream, uint64_t instances, uint64_t triangles,
-                    const IssueFn& issue) {
+                    const IssueFn& issue, uint64_t items, uint64_t chunks) {
     const bool sync = (flags & CR_RENDER_SYNC) != 0;
     for (int attempt = 0; attempt < 3; ++attempt) {
         cudaEvent_t* tev = nullptr;  // 7 timing events of this frame, or none
@@ -318,6 +344,8 @@ cr_status run_frame(cr_context* ctx, uint32_t flags, cudaStream_t stream, uint64
         ctx->last = cr_frame_stats{};
         ctx->last.instances = instances;
         ctx->last.triangles = triangles;
+        ctx->last.work_items = items;
+        ctx->last.vertex_chunks = chunks;
         ctx->pendingStats = true;
         ctx->lastStream = stream;
         CR_CUDA(cudaEventRecord(ctx->frameDone, stream), "frame event");
@@ -328,9 +356,7 @@ cr_status run_frame(cr_context* ctx, uint32_t flags, cudaStream_t stream, uint64
         cudaEventElapsedTime(&ctx->last.ms_raster, ctx->ev[0], ctx->ev[1]);
         cudaEventElapsedTime(&ctx->last.ms_resolve, ctx->ev[1], ctx->ev[2]);
         ctx->pendingStats = false;
-        ctx->last.nontrivial = ctx->hCounters[CR_CTR_NONTRIVIAL];
-        ctx->last.huge_tiles = ctx->hCounters[CR_CTR_HUGE];
-        ctx->last.overflow = ctx->hCounters[CR_CTR_OVERFLOW];
+        read_counters(ctx);
         if (ctx->hCounters[CR_CTR_TIMEOUT]) return fail(CR_ERR_TIMEOUT, "a device-side wait timed out");
         if (!ctx->last.overflow) return CR_OK;
         if (!ctx->cfg.grow_on_overflow)
@@ -440,12 +466,15 @@ cr_status cr_destroy(cr_context* ctx) {
     if (!ctx) return CR_OK;
     cudaSetDevice(ctx->device);
     cudaDeviceSynchronize();
-    for (MeshRec& m : ctx->meshes)
+    for (MeshRec& m : ctx->meshes) {
         if (m.live && m.owned) {
             cudaFree(m.positions);
             cudaFree(m.indices);
             cudaFree(m.colors);
         }
+        if (m.itemBoxes) cudaFree(m.itemBoxes);
+    }
+    if (ctx->itemList) cudaFree(ctx->itemList);
     if (ctx->outcodes) cudaFree(ctx->outcodes);
     if (ctx->ntList) cudaFree(ctx->ntList);
     if (ctx->hugeList) cudaFree(ctx->hugeList);
@@ -514,6 +543,16 @@ cr_status cr_mesh_create(cr_context* ctx, const cr_mesh_desc* d, uint32_t* mesh_
     } else {
         return fail(CR_ERR_INVALID, "cr_mesh_create: unknown memory kind %d", d->memory);
     }
+    cr_status bs = build_mesh_boxes(ctx, m);
+    if (bs) {
+        if (m.owned) {
+            ctx->dev_free(m.positions, 0);
+            ctx->dev_free(m.indices, 0);
+            ctx->dev_free(m.colors, 0);
+            ctx->bytesInUse -= std::min(ctx->bytesInUse, m.bytes);
+        }
+        return bs;
+    }
     ctx->meshes.push_back(m);
     *mesh_out = (uint32_t)(ctx->meshes.size() - 1);
     return CR_OK;
@@ -530,8 +569,16 @@ cr_status cr_mesh_destroy(cr_context* ctx, uint32_t mesh) {
         cudaFree(m.colors);
         ctx->bytesInUse -= std::min(ctx->bytesInUse, m.bytes);
     }
+    ctx->dev_free(m.itemBoxes, m.boxBytes);
     m = MeshRec{};
     return CR_OK;
+}
+
+cr_status cr_mesh_refresh(cr_context* ctx, uint32_t mesh) {
+    if (!ctx || mesh >= ctx->meshes.size() || !ctx->meshes[mesh].live) return fail(CR_ERR_NOT_FOUND, "unknown mesh %u", mesh);
+    CR_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    CR_CUDA(cudaDeviceSynchronize(), "mesh refresh");
+    return build_mesh_boxes(ctx, ctx->meshes[mesh]);
 }
 
 cr_status cr_mesh_device_arrays(cr_context* ctx, uint32_t mesh, uint64_t* d_positions, uint64_t* d_indices,
@@ -611,6 +658,22 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
     if (cam->width > 65535 || cam->height > 65535) cellMode = 0;  // cells hold 16-bit coordinates
     s = ensure_records(ctx, A.outBytes * (cellMode ? 8 : 1));
     if (s) return s;
+    if (A.numItems > ctx->itemCap || A.numVChunks > ctx->chunkCap) {
+        // item-cull survivors (at most every item) and one class per chunk
+        CR_CUDA(cudaDeviceSynchronize(), "cull buffer resize");
+        ctx->dev_free(ctx->itemList, ctx->itemBytes);
+        ctx->itemList = nullptr;
+        ctx->itemCap = ctx->chunkCap = ctx->itemBytes = 0;
+        const uint64_t items = A.numItems + A.numItems / 8 + 1024;
+        const uint64_t chunks = A.numVChunks + A.numVChunks / 8 + 1024;
+        const size_t bytes = align_up(items * 8, 256) + align_up(chunks * 4, 256);
+        s = ctx->dev_alloc((void**)&ctx->itemList, bytes, "cull buffers");
+        if (s) return s;
+        ctx->itemCap = items;
+        ctx->chunkCap = chunks;
+        ctx->itemBytes = bytes;
+        ctx->chunkList = (uint32_t*)((char*)ctx->itemList + align_up(items * 8, 256));
+    }
     CrFrameParams fp{};
     CrResolveParams rp{};
     if (count) {
@@ -619,6 +682,9 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
     }
     fp.outcodes = ctx->outcodes;
     fp.cellMode = cellMode;
+    fp.itemList = ctx->itemList;
+    fp.itemCap = ctx->itemCap;
+    fp.chunkList = ctx->chunkList;
     fp.fb = (uint64_t*)d_visbuffer;
     fp.W = cam->width;
     fp.H = cam->height;
@@ -660,7 +726,7 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
             return fail(CR_ERR_CUDA, "clear launch: %s", cudaGetErrorString(cudaGetLastError()));
         }
         CR_CUDA(mark(1), "event");
-        if (raster && count && cr_launch_vertex(fp, ctx->shape, stream))
+        if (raster && count && (cr_launch_cull(fp, ctx->shape, stream) || cr_launch_vertex(fp, ctx->shape, stream)))
             return fail(CR_ERR_CUDA, "vertex-pass launch: %s", cudaGetErrorString(cudaGetLastError()));
         CR_CUDA(mark(2), "event");
         if (raster && count && cr_launch_stage1(fp, ctx->shape, stream))
@@ -678,7 +744,9 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
         CR_CUDA(mark(6), "event");
         return CR_OK;
     };
-    return run_frame(ctx, flags, stream, count, A.totalTriangles, issue);
+    const bool culled = fp.itemList && !(flags & kRenderResolveOnly);
+    return run_frame(ctx, flags, stream, count, A.totalTriangles, issue, culled ? A.numItems : 0,
+                     culled ? A.numVChunks : 0);
 }
 
 extern "C" {
@@ -688,9 +756,7 @@ cr_status cr_sync(cr_context* ctx) {
     CR_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
     if (ctx->pendingStats) {
         CR_CUDA(cudaStreamSynchronize(ctx->lastStream), "sync");
-        ctx->last.nontrivial = ctx->hCounters[CR_CTR_NONTRIVIAL];
-        ctx->last.huge_tiles = ctx->hCounters[CR_CTR_HUGE];
-        ctx->last.overflow = ctx->hCounters[CR_CTR_OVERFLOW];
+        read_counters(ctx);
         ctx->pendingStats = false;
         if (ctx->hCounters[CR_CTR_TIMEOUT]) return fail(CR_ERR_TIMEOUT, "a device-side wait timed out");
         if (ctx->last.overflow)

@@ -38,6 +38,10 @@ struct MeshRec {
     uint32_t numVertices = 0;
     uint32_t numTriangles = 0;
     size_t bytes = 0;
+    // hierarchical-cull boxes (library-owned, also for borrowed meshes)
+    float* itemBoxes = nullptr;   // per CR_BATCH triangles
+    float* chunkBoxes = nullptr;  // per CR_VCHUNK vertices
+    size_t boxBytes = 0;
 };
 
 void mat4_mul(const float* a, const float* b, float* out);  // glm order
@@ -80,6 +84,11 @@ struct cr_context {
     uint64_t outCap = 0;
     uint64_t* ntList = nullptr;
     uint64_t ntCap = 0;
+    uint2* itemList = nullptr;    // item-cull survivors, then the chunk list
+    uint64_t itemCap = 0;
+    uint32_t* chunkList = nullptr;
+    uint64_t chunkCap = 0;
+    size_t itemBytes = 0;
     CrTile* hugeList = nullptr;
     uint64_t hugeCap = 0;
     unsigned long long* counters = nullptr;
@@ -121,6 +130,8 @@ cr_status render_impl(cr_context* ctx, const cr_instance* instances, uint32_t co
                       const cr_camera* cam, uint64_t d_visbuffer, uint64_t d_rgba, uint64_t d_colorbuffer,
                       int32_t display, uint32_t flags, void* stream, uint64_t resolveIdLo, uint64_t resolveIdHi);
 cr_status ensure_queues(cr_context* ctx, uint64_t ntWant, uint64_t hugeWant);
+// (Re)builds a mesh's hierarchical-cull boxes from its current contents.
+cr_status build_mesh_boxes(cr_context* ctx, MeshRec& m);
 // Grows the per-vertex record buffer to at least `bytes`.
 cr_status ensure_records(cr_context* ctx, uint64_t bytes);
 
@@ -131,7 +142,9 @@ cr_status ensure_records(cr_context* ctx, uint64_t bytes);
 // timeouts and overflow, and re-issues with grown queues (up to 3 attempts).
 using IssueFn = std::function<cr_status(cudaEvent_t* tev, cudaEvent_t rasterEnd)>;
 cr_status run_frame(cr_context* ctx, uint32_t flags, cudaStream_t stream, uint64_t instances, uint64_t triangles,
-                    const IssueFn& issue);
+                    const IssueFn& issue, uint64_t items = 0, uint64_t chunks = 0);
+// Copies the pinned counters of the last frame into ctx->last.
+void read_counters(cr_context* ctx);
 
 const cr_tuning* find_tuning(const cr_context* ctx, uint32_t sceneClass);
 // Device and pinned buffers of one batched frame in flight (a server slot).
@@ -144,6 +157,11 @@ struct BatchScratch {
     size_t recordCap = 0;
     uint64_t* ntList = nullptr;
     uint64_t ntCap = 0;
+    uint2* itemList = nullptr;    // item-cull survivors, then the chunk list
+    uint64_t itemCap = 0;
+    uint32_t* chunkList = nullptr;
+    uint64_t chunkCap = 0;
+    size_t itemBytes = 0;
     CrTile* hugeList = nullptr;
     uint64_t hugeCap = 0;
     unsigned long long* counters = nullptr;

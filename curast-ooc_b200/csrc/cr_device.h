@@ -22,6 +22,8 @@
 #define CR_CTR_HUGE 1           // tiles appended to the stage-3 queue
 #define CR_CTR_OVERFLOW 2       // bit 0: stage-2 queue, bit 1: stage-3 queue
 #define CR_CTR_TIMEOUT 3        // nonzero if a bounded device wait gave up
+#define CR_CTR_ITEMS 4          // stage-1 work items that survive the item cull
+#define CR_CTR_CHUNKS 5         // vertex-pass chunks that need per-vertex records
 #define CR_CTR_COUNT 8
 
 struct alignas(16) CrInstance {
@@ -35,6 +37,8 @@ struct alignas(16) CrInstance {
     uint32_t pad0;
     uint64_t outBase;           // first outcode byte of this instance
     uint64_t vchunkBase;        // first vertex-pass chunk of this instance
+    const float* chunkBoxes;    // per CR_VCHUNK vertices: min xyz, max xyz (or nullptr)
+    uint64_t pad1;
 };
 
 // Per-(instance, vertex) outcode bits written by the vertex pass.  They are
@@ -59,7 +63,7 @@ struct alignas(16) CrInstance {
 #define CR_CELL_INSIDE (1ull << 8)
 #define CR_CELL_FRACX (1ull << 9)
 #define CR_CELL_FRACY (1ull << 10)
-static_assert(sizeof(CrInstance) == 64, "CrInstance layout");
+static_assert(sizeof(CrInstance) == 80, "CrInstance layout");
 
 struct alignas(16) CrSegment {
     const uint32_t* indices;
@@ -71,8 +75,10 @@ struct alignas(16) CrSegment {
     uint32_t numChunks;         // ceil(instanceCount / CR_INST_CHUNK)
     uint32_t flags;             // bit 0: index array 16-byte aligned (TMA tiles)
     uint64_t itemBase;          // first stage-1 work item of this segment
+    const float* itemBoxes;     // per CR_BATCH triangles: box of their vertices (or nullptr)
+    uint64_t pad;
 };
-static_assert(sizeof(CrSegment) == 48, "CrSegment layout");
+static_assert(sizeof(CrSegment) == 64, "CrSegment layout");
 
 struct alignas(16) CrTile {     // HugeTriangle, HostDeviceInterface.h:254-259
     int32_t instance;           // instance | view << 26 (view 0 in single-view frames)
@@ -144,6 +150,14 @@ struct CrFrameParams {
     uint32_t cellMode;          // 1: the vertex pass writes 8-byte cell records
     CrViewMasks* viewMasks;     // CrInstance::outBase + vertex
     const uint32_t* flips;      // numViews * numInstances, view-major
+    // item cull: surviving work items {item, instance mask within its
+    // instance chunk}, counted in counters[CR_CTR_ITEMS]; nullptr: every item
+    uint2* itemList;
+    uint64_t itemCap;
+    // vertex-pass chunks that need per-vertex records (the frame cull writes
+    // the others' records from their boxes), counted in
+    // counters[CR_CTR_CHUNKS]; nullptr: every chunk
+    uint32_t* chunkList;
 };
 
 struct CrResolveParams {
@@ -178,7 +192,16 @@ int cr_launch_vertex(const CrFrameParams& p, const CrLaunchShape& s, void* strea
 int cr_launch_stage1(const CrFrameParams& p, const CrLaunchShape& s, void* stream);
 int cr_launch_stage2(const CrFrameParams& p, const CrLaunchShape& s, void* stream);
 int cr_launch_stage3(const CrFrameParams& p, const CrLaunchShape& s, void* stream);
+// Classifies every vertex-pass chunk and every stage-1 item of the frame
+// (runs before the vertex pass).
+int cr_launch_cull(const CrFrameParams& p, const CrLaunchShape& s, void* stream);
 int cr_launch_resolve(const CrResolveParams& p, void* stream);
+
+// Mesh preparation (meshprep.cu): the box of the vertices of every CR_BATCH
+// consecutive triangles and of every CR_VCHUNK consecutive vertices (a box
+// with a non-finite position is NaN and culls nothing).
+int cr_launch_mesh_boxes(const uint32_t* indices, const float* positions, uint32_t numTriangles,
+                         uint32_t numVertices, float* itemBoxes, float* chunkBoxes, void* stream);
 
 // Batched (multi-view) frame: one launch per stage over all views.  Grid
 // sizes are chosen by the host (defaults from occupancy, or tuned).

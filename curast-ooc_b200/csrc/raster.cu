@@ -21,6 +21,7 @@
 //   stage 3  one warp per 64x64 tile (the reference: one 64-thread block),
 //            each lane ray-traces two columns.        reference: tv.cu:568-745
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cstdint>
 
 #include "raster_core.cuh"
@@ -31,7 +32,10 @@ template <int THREADS>
 __global__ void __launch_bounds__(THREADS) k_vertex(const CrFrameParams p) {
     const float fa = p.f / p.aspect;
     const float Wf = (float)p.W, Hf = (float)p.H;
-    for (uint64_t c = blockIdx.x; c < p.numVChunks; c += gridDim.x) {
+    // the chunks the frame cull left for per-vertex records (or every chunk)
+    const uint64_t nChunks = p.chunkList ? min((uint64_t)p.counters[CR_CTR_CHUNKS], p.numVChunks) : p.numVChunks;
+    for (uint64_t k = blockIdx.x; k < nChunks; k += gridDim.x) {
+        const uint64_t c = p.chunkList ? (uint64_t)__ldg(p.chunkList + k) : k;
         uint32_t lo = 0, hi = p.numInstances - 1;  // instance holding chunk c
         while (lo < hi) {
             const uint32_t mid = (lo + hi + 1) >> 1;
@@ -52,6 +56,125 @@ __global__ void __launch_bounds__(THREADS) k_vertex(const CrFrameParams p) {
             uint8_t* out = p.outcodes + __ldg(&I->outBase);
             for (uint32_t v = v0 + threadIdx.x; v < v1; v += THREADS)
                 out[v] = (uint8_t)vertex_outcode(M, load_pos(pos, v), fa, p.f);
+        }
+    }
+}
+
+// Frame cull, before the vertex pass; one thread per vertex-pass chunk, then
+// one per stage-1 work item.
+//   chunks  a chunk whose box proves CR_OC_* bits for every vertex
+//           (classify_chunk: exact "behind", a sound subset of the sides) gets
+//           those bits as its records here, without its positions being read;
+//           the others are listed for the vertex pass.
+//   items   the item's box is classified for each instance of its chunk; an
+//           instance whose box is wholly behind or beyond one side has every
+//           triangle of the item culled by the reference's own tests
+//           (tv.cu:110-119).  Items with a surviving instance are appended
+//           (warp-aggregated) with the mask of those instances.
+// Skipping what the boxes prove cannot change the visbuffer.
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) k_cull(const CrFrameParams p) {
+    const int lane = threadIdx.x & 31;
+    const float fa = p.f / p.aspect;
+    const uint64_t stride = (uint64_t)gridDim.x * THREADS;
+    const uint64_t nChunks = p.chunkList ? p.numVChunks : 0;
+    for (uint64_t base = (uint64_t)blockIdx.x * THREADS; base < nChunks; base += stride) {
+        const uint64_t g = base + threadIdx.x;
+        uint32_t cls = 0;
+        if (g < nChunks) {
+            uint32_t lo = 0, hi = p.numInstances - 1;  // instance holding chunk g
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi + 1) >> 1;
+                if (__ldg(&p.instances[mid].vchunkBase) <= g) lo = mid;
+                else hi = mid - 1;
+            }
+            const CrInstance* I = p.instances + lo;
+            const uint64_t cIdx = g - __ldg(&I->vchunkBase);
+            const float* cb = ldg_ptr(&I->chunkBoxes);
+            if (cb) {
+                const float* bx = cb + 6ull * cIdx;
+                const float blo[3] = {__ldg(bx), __ldg(bx + 1), __ldg(bx + 2)};
+                const float bhi[3] = {__ldg(bx + 3), __ldg(bx + 4), __ldg(bx + 5)};
+                cls = classify_box(load_mat(p.world_view + 4ull * lo), fa, p.f, blo, bhi) & CR_OC_MASK;
+            }
+        }
+        // classified chunks' records, written here by the whole warp (one
+        // chunk at a time, coalesced): their positions are never read
+        unsigned fillMask = __ballot_sync(FULL, cls != 0);
+        while (fillMask) {
+            const int j = __ffs(fillMask) - 1;
+            fillMask &= fillMask - 1;
+            const uint64_t gj = __shfl_sync(FULL, g, j);
+            const uint32_t cj = __shfl_sync(FULL, cls, j);
+            uint32_t lo = 0, hi = p.numInstances - 1;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi + 1) >> 1;
+                if (__ldg(&p.instances[mid].vchunkBase) <= gj) lo = mid;
+                else hi = mid - 1;
+            }
+            const CrInstance* I = p.instances + lo;
+            const uint64_t cIdx = gj - __ldg(&I->vchunkBase);
+            const uint32_t nv = min((uint32_t)CR_VCHUNK, __ldg(&I->numVertices) - (uint32_t)cIdx * CR_VCHUNK);
+            const uint64_t v0 = __ldg(&I->outBase) + cIdx * CR_VCHUNK;
+            if (p.cellMode) {  // 16-byte aligned: (outBase + k CR_VCHUNK) * 8
+                uint64_t* out = reinterpret_cast<uint64_t*>(p.outcodes) + v0;
+                for (uint32_t v = 2 * lane; v < nv; v += 64) {
+                    if (v + 1 < nv) *reinterpret_cast<ulonglong2*>(out + v) = make_ulonglong2(cj, cj);
+                    else out[v] = cj;
+                }
+            } else {  // 16-byte aligned: outBase and CR_VCHUNK are multiples of 16
+                uint8_t* out = p.outcodes + v0;
+                const uint32_t word = cj * 0x01010101u;
+                for (uint32_t v = 16 * lane; v < nv; v += 512) {
+                    if (v + 16 <= nv) *reinterpret_cast<uint4*>(out + v) = make_uint4(word, word, word, word);
+                    else
+                        for (uint32_t u = v; u < nv; ++u) out[u] = (uint8_t)cj;
+                }
+            }
+        }
+        // chunks that need per-vertex records, listed for the vertex pass
+        const bool eval = g < nChunks && cls == 0;
+        const unsigned m = __ballot_sync(FULL, eval);
+        if (m) {
+            const int leader = __ffs(m) - 1;
+            unsigned long long b = 0;
+            if (lane == leader) b = atomicAdd(&p.counters[CR_CTR_CHUNKS], (unsigned long long)__popc(m));
+            b = __shfl_sync(FULL, b, leader);
+            if (eval) p.chunkList[b + __popc(m & ((1u << lane) - 1u))] = (uint32_t)g;
+        }
+    }
+    if (!p.itemList) return;
+    for (uint64_t base = (uint64_t)blockIdx.x * THREADS; base < p.numItems; base += stride) {
+        const uint64_t item = base + threadIdx.x;
+        uint32_t mask = 0;
+        if (item < p.numItems) {
+            const Item it = decode_item(p, item);
+            const CrSegment* sg = p.segments + it.seg;
+            const uint32_t first = __ldg(&sg->firstInstance);
+            const uint32_t ib = first + it.chunk * CR_INST_CHUNK;
+            const uint32_t ie = min(ib + CR_INST_CHUNK, first + __ldg(&sg->instanceCount));
+            const float* boxes = ldg_ptr(&sg->itemBoxes);
+            if (!boxes) {
+                mask = (1u << (ie - ib)) - 1u;
+            } else {
+                const float* bx = boxes + 6ull * it.batch;
+                const float blo[3] = {__ldg(bx), __ldg(bx + 1), __ldg(bx + 2)};
+                const float bhi[3] = {__ldg(bx + 3), __ldg(bx + 4), __ldg(bx + 5)};
+                for (uint32_t inst = ib; inst < ie; ++inst)
+                    if (!(classify_box(load_mat(p.world_view + 4ull * inst), fa, p.f, blo, bhi) & CR_OC_MASK))
+                        mask |= 1u << (inst - ib);
+            }
+        }
+        const unsigned m = __ballot_sync(FULL, mask != 0);
+        if (m) {
+            const int leader = __ffs(m) - 1;
+            unsigned long long b = 0;
+            if (lane == leader) b = atomicAdd(&p.counters[CR_CTR_ITEMS], (unsigned long long)__popc(m));
+            b = __shfl_sync(FULL, b, leader);
+            if (mask) {
+                const uint64_t q = b + __popc(m & ((1u << lane) - 1u));
+                if (q < p.itemCap) p.itemList[q] = make_uint2((uint32_t)item, mask);
+            }
         }
     }
 }
@@ -80,11 +203,15 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_stage1(const CrFrameParams p)
     __syncwarp();
     // `pending` marks ring slots holding an issued, not yet consumed tile copy.
     // Every lane tracks it identically; lane 0 issues the copies.
+    // work items: the item cull's survivors (with their instance masks) or,
+    // without an item list, every item
+    const uint64_t nItems = p.itemList ? min((uint64_t)p.counters[CR_CTR_ITEMS], p.itemCap) : p.numItems;
+    auto item_at = [&](uint64_t k) -> uint64_t { return p.itemList ? (uint64_t)__ldg(&p.itemList[k].x) : k; };
     uint32_t pending = 0;
     for (int s = 0; s < S1_STAGES; ++s) {
-        const uint64_t item = gw + (uint64_t)s * nw;
-        if (item >= p.numItems) break;
-        const Item it = decode_item(p, item);
+        const uint64_t pk = gw + (uint64_t)s * nw;
+        if (pk >= nItems) break;
+        const Item it = decode_item(p, item_at(pk));
         const CrSegment* sg = p.segments + it.seg;
         if (item_uses_tma(sg, it.batch)) {
             pending |= 1u << s;
@@ -101,9 +228,11 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_stage1(const CrFrameParams p)
     const float fa = p.f / p.aspect;
     uint32_t parity = 0;
     uint32_t k = 0;
-    for (uint64_t item = gw; item < p.numItems; item += nw, ++k) {
+    for (uint64_t pk = gw; pk < nItems; pk += nw, ++k) {
         const int slot = (int)(k % S1_STAGES);
         const uint32_t bit = 1u << slot;
+        const uint64_t item = item_at(pk);
+        const uint32_t imask = p.itemList ? __ldg(&p.itemList[pk].y) : 0xffffffffu;
         const Item it = decode_item(p, item);
         const CrSegment* sg = p.segments + it.seg;
         const uint32_t numTri = __ldg(&sg->numTriangles);
@@ -142,6 +271,7 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_stage1(const CrFrameParams p)
         const uint32_t ib = first + it.chunk * CR_INST_CHUNK;
         const uint32_t ie = min(ib + CR_INST_CHUNK, first + count);
         for (uint32_t inst = ib; inst < ie; ++inst) {
+            if (!((imask >> (inst - ib)) & 1u)) continue;  // its box proved every triangle culled
             const uint64_t ob = __ldg(&p.instances[inst].outBase);
             bool culledR[S1_R];
             if (p.cellMode) {
@@ -232,9 +362,9 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_stage1(const CrFrameParams p)
 
         __syncwarp();
         {  // every read of this slot is done: refill it with the item S1_STAGES ahead
-            const uint64_t nxt = item + (uint64_t)S1_STAGES * nw;
-            if (nxt < p.numItems) {
-                const Item nt = decode_item(p, nxt);
+            const uint64_t npk = pk + (uint64_t)S1_STAGES * nw;
+            if (npk < nItems) {
+                const Item nt = decode_item(p, item_at(npk));
                 const CrSegment* ns = p.segments + nt.seg;
                 if (item_uses_tma(ns, nt.batch)) {
                     pending |= bit;
@@ -305,6 +435,16 @@ int cr_launch_vertex(const CrFrameParams& p, const CrLaunchShape& s, void* strea
     uint64_t blocks = p.numVChunks;
     if (blocks > (uint64_t)s.vertexBlocks) blocks = (uint64_t)s.vertexBlocks;
     k_vertex<VX_THREADS><<<(unsigned)blocks, VX_THREADS, 0, (cudaStream_t)stream>>>(p);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int cr_launch_cull(const CrFrameParams& p, const CrLaunchShape& s, void* stream) {
+    if (!p.itemList && !p.chunkList) return 0;
+    const uint64_t work = std::max<uint64_t>(p.numItems, p.chunkList ? p.numVChunks : 0);
+    if (work == 0) return 0;
+    uint64_t blocks = (work + 255) / 256;
+    if (blocks > (uint64_t)s.numSMs * 8) blocks = (uint64_t)s.numSMs * 8;
+    k_cull<256><<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(p);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

@@ -38,102 +38,6 @@ namespace {
 constexpr int VV_THREADS = 256;
 constexpr int VV_PER_THREAD = CR_VCHUNK / VV_THREADS;  // 4 vertices per thread
 
-// Chunk classes (bit set) of one view; CH_INSIDE means no vertex is behind or
-// beyond any side, CH_BEHIND that every vertex is behind, CH_<side> that
-// every vertex is in front and beyond that side.
-enum : uint32_t {
-    CH_BEHIND = 1u,
-    CH_RIGHT = 2u,
-    CH_LEFT = 4u,
-    CH_TOP = 8u,
-    CH_BOTTOM = 16u,
-    CH_INSIDE = 32u,
-};
-
-__device__ __forceinline__ double lin_min(const double a[3], double b, const float lo[3], const float hi[3]) {
-    double s = b;
-#pragma unroll
-    for (int j = 0; j < 3; ++j) s += a[j] >= 0.0 ? a[j] * (double)lo[j] : a[j] * (double)hi[j];
-    return s;
-}
-
-__device__ __forceinline__ double lin_max(const double a[3], double b, const float lo[3], const float hi[3]) {
-    double s = b;
-#pragma unroll
-    for (int j = 0; j < 3; ++j) s += a[j] >= 0.0 ? a[j] * (double)hi[j] : a[j] * (double)lo[j];
-    return s;
-}
-
-// Classifies a box of object-space positions [lo, hi] for one view (rows of
-// world_view: rx, ry, rz; fa = f / aspect and f as the kernels use them).
-//
-// The device evaluates per vertex q = xform(M, p) in float (three products,
-// two levels of sums), d = -q.z, X = fl(fa * q.x), Y = fl(f * q.y), and the
-// predicates d <= 0 and fl(X / d) > 1 (ndc_beyond).  With S_x = sum_j
-// |M_xj| max|p_j| + |M_x3|, |q.x - Q_x| <= gamma_3 S_x < 2^-20 S_x where Q is
-// the exact affine value (likewise y, z), and fl(fa q.x) adds a relative
-// 2^-24.  So with delta = 2^-20 and the margin
-//     m = 2^-19 (fa S_x + S_z) + 1e-30,
-// min over the box of (fa Q_x + (1 + delta) Q_z) > m proves X >= (1 + delta) d
-// for every vertex, hence fl(X / d) >= 1 + 2^-20 > 1: every vertex is beyond
-// the right side; max over the box of (fa Q_x + (1 - delta) Q_z) < -m proves
-// fl(X / d) <= 1 - 2^-20: none is.  Min / max of an affine function over a
-// box are exact corner sums (double products of floats are exact; the
-// double sums' rounding is far inside the margin).  Non-finite bounds
-// classify nothing (comparisons with NaN fail).
-__device__ uint32_t classify_chunk(const float4 rx, const float4 ry, const float4 rz, float fa, float f,
-                                   const float lo[3], const float hi[3]) {
-    const double EPS = 9.5367431640625e-07;  // 2^-20
-    const double ABS = 1e-30;
-    const double ax[3] = {rx.x, rx.y, rx.z}, ay[3] = {ry.x, ry.y, ry.z}, az[3] = {rz.x, rz.y, rz.z};
-    double mabs[3];
-#pragma unroll
-    for (int j = 0; j < 3; ++j) mabs[j] = fmax(fabs((double)lo[j]), fabs((double)hi[j]));
-    const double Sx = (fabs(ax[0]) * mabs[0] + fabs(ax[1]) * mabs[1]) + (fabs(ax[2]) * mabs[2] + fabs((double)rx.w));
-    const double Sy = (fabs(ay[0]) * mabs[0] + fabs(ay[1]) * mabs[1]) + (fabs(ay[2]) * mabs[2] + fabs((double)ry.w));
-    const double Sz = (fabs(az[0]) * mabs[0] + fabs(az[1]) * mabs[1]) + (fabs(az[2]) * mabs[2] + fabs((double)rz.w));
-    if (!(Sx < 1e30 && Sy < 1e30 && Sz < 1e30)) return 0u;
-    const double ez = EPS * Sz + ABS;
-    if (lin_min(az, rz.w, lo, hi) - ez >= 0.0) return CH_BEHIND;  // q.z >= 0 everywhere
-    if (!(lin_max(az, rz.w, lo, hi) + ez < 0.0)) return 0u;      // some vertex may be behind
-    const double F = (double)fa, G = (double)f;
-    const double mx = 2.0 * EPS * (F * Sx + Sz) + ABS;
-    const double my = 2.0 * EPS * (G * Sy + Sz) + ABS;
-    const double up = 1.0 + EPS, dn = 1.0 - EPS;
-    double a[3];
-    uint32_t c = 0u, inside = 0u;
-    // right: fa Q_x vs d = -Q_z
-#pragma unroll
-    for (int j = 0; j < 3; ++j) a[j] = F * ax[j] + up * az[j];
-    if (lin_min(a, F * rx.w + up * rz.w, lo, hi) > mx) c |= CH_RIGHT;
-#pragma unroll
-    for (int j = 0; j < 3; ++j) a[j] = F * ax[j] + dn * az[j];
-    if (lin_max(a, F * rx.w + dn * rz.w, lo, hi) < -mx) inside |= 1u;
-    // left: -fa Q_x
-#pragma unroll
-    for (int j = 0; j < 3; ++j) a[j] = -F * ax[j] + up * az[j];
-    if (lin_min(a, -F * rx.w + up * rz.w, lo, hi) > mx) c |= CH_LEFT;
-#pragma unroll
-    for (int j = 0; j < 3; ++j) a[j] = -F * ax[j] + dn * az[j];
-    if (lin_max(a, -F * rx.w + dn * rz.w, lo, hi) < -mx) inside |= 2u;
-    // top: f Q_y
-#pragma unroll
-    for (int j = 0; j < 3; ++j) a[j] = G * ay[j] + up * az[j];
-    if (lin_min(a, G * ry.w + up * rz.w, lo, hi) > my) c |= CH_TOP;
-#pragma unroll
-    for (int j = 0; j < 3; ++j) a[j] = G * ay[j] + dn * az[j];
-    if (lin_max(a, G * ry.w + dn * rz.w, lo, hi) < -my) inside |= 4u;
-    // bottom: -f Q_y
-#pragma unroll
-    for (int j = 0; j < 3; ++j) a[j] = -G * ay[j] + up * az[j];
-    if (lin_min(a, -G * ry.w + up * rz.w, lo, hi) > my) c |= CH_BOTTOM;
-#pragma unroll
-    for (int j = 0; j < 3; ++j) a[j] = -G * ay[j] + dn * az[j];
-    if (lin_max(a, -G * ry.w + dn * rz.w, lo, hi) < -my) inside |= 8u;
-    if (c) return c;
-    return inside == 15u ? CH_INSIDE : 0u;
-}
-
 // vertex_outcode with the matrix given as its x, y, z rows: the same float
 // operations in the same order as xform.
 __device__ __forceinline__ uint32_t outcode_rows(const float4 rx, const float4 ry, const float4 rz, V3 p, float fa,

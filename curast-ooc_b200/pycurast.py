@@ -100,6 +100,10 @@ class CrFrameStats(ctypes.Structure):
         ("ms_raster", _f32),
         ("ms_resolve", _f32),
         ("reserved", _f32),
+        ("work_items", _u64),
+        ("work_items_drawn", _u64),
+        ("vertex_chunks", _u64),
+        ("vertex_chunks_evaluated", _u64),
     ]
 
 
@@ -233,6 +237,7 @@ EXPORTS = {
     "cr_abi_version": (_i32, []),
     "cr_mesh_create": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrMeshDesc), ctypes.POINTER(_u32)]),
     "cr_mesh_destroy": (_i32, [ctypes.c_void_p, _u32]),
+    "cr_mesh_refresh": (_i32, [ctypes.c_void_p, _u32]),
     "cr_mesh_device_arrays": (_i32, [ctypes.c_void_p, _u32, ctypes.POINTER(_u64), ctypes.POINTER(_u64),
                                      ctypes.POINTER(_u64)]),
     "cr_frame_assemble": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrInstance), _u32, ctypes.c_void_p, _u32,

@@ -149,6 +149,13 @@ typedef struct cr_frame_stats {
     float ms_raster;
     float ms_resolve;
     float reserved;
+    /* hierarchical culling: stage-1 work items (128 triangles x an instance
+     * chunk) and vertex-pass chunks (1024 vertices of an instance), in all
+     * and after the per-view box tests */
+    uint64_t work_items;
+    uint64_t work_items_drawn;
+    uint64_t vertex_chunks;
+    uint64_t vertex_chunks_evaluated;
 } cr_frame_stats;
 
 /* ---- context ---------------------------------------------------------- */
@@ -161,6 +168,11 @@ int cr_abi_version(void);
 /* ---- geometry ----------------------------------------------------------- */
 cr_status cr_mesh_create(cr_context* ctx, const cr_mesh_desc* desc, uint32_t* mesh_out);
 cr_status cr_mesh_destroy(cr_context* ctx, uint32_t mesh);
+/* Per-view culling of whole groups of triangles uses bounding boxes computed
+ * from the mesh's contents when it is created.  A caller that changes the
+ * contents of a borrowed (CR_MEM_DEVICE) mesh afterwards calls
+ * cr_mesh_refresh before rendering it again. */
+cr_status cr_mesh_refresh(cr_context* ctx, uint32_t mesh);
 /* Device pointers of a mesh's arrays (for callers that share them). */
 cr_status cr_mesh_device_arrays(cr_context* ctx, uint32_t mesh, uint64_t* d_positions,
                                 uint64_t* d_indices, uint64_t* d_colors);
