@@ -360,11 +360,23 @@ def run_ours(args, rank, world, local):
     # figure keeps the reference's 12T + 12V + 16P (+ 12P resolve), counting
     # the geometry a full scan reads: culled groups are not read, so it can
     # exceed the bandwidth peak.
-    rec = 8 if (len(wl["instances"]) > 1) else 1
+    # frames that draw a mesh more than once cull from box proofs and per-item
+    # vertex lists (no per-vertex records in device memory)
+    mids = [m for m, _ in wl["instances"]]
+    direct = len(set(mids)) < len(mids)
+    rec = 0 if direct else 1
     items, items_drawn = int(fstats.work_items), int(fstats.work_items_drawn)
     chunks, chunks_eval = int(fstats.vertex_chunks), int(fstats.vertex_chunks_evaluated)
     nV_inst = sum(wl["meshes"][m][0].shape[0] for m, _ in wl["instances"])
-    if chunks:
+    if direct:
+        # frame cull: one 24-byte item box per item (the instance matrices
+        # stay in L1) and 8 B per listed item; stage 1: the 1408-byte vertex
+        # list block of each listed item and the positions of its distinct
+        # vertices (at most 128 x 12 B for these meshes)
+        v_eval, tri_drawn = 0, min(T, items_drawn * 128)
+        algo = {"vertex": 24 * items + 8 * items_drawn,
+                "stage1": (1408 + 12 * 128) * items_drawn}
+    elif chunks:
         v_eval = min(nV_inst, chunks_eval * 1024)
         tri_drawn = min(T, items_drawn * 128)
         algo = {"vertex": 24 * (chunks + items) + (12 + rec) * v_eval + 8 * items_drawn,

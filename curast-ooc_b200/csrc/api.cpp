@@ -130,6 +130,63 @@ void order_instances(uint32_t count, uint32_t flags, MeshOf meshOf, TrisOf trisO
     });
 }
 
+// The device's classify_chunk (raster_core.cuh) for one mesh box, in double
+// on the host: the same rigorous bounds on the float transform of every
+// vertex in the box.  Returns CR_OC_BEHIND, a union of side bits, or
+// CR_MESH_INSIDE; 0 when nothing is proven (also for non-finite boxes).
+static uint32_t classify_mesh_box(const float* wv, float fa, float f, const float* box) {
+    const double EPS = 9.5367431640625e-07;  // 2^-20
+    const double ABS = 1e-30;
+    const float* lo = box;
+    const float* hi = box + 3;
+    double ax[3], ay[3], az[3], mabs[3];
+    for (int j = 0; j < 3; ++j) {  // column-major: element (row r, column j) at 4 j + r
+        ax[j] = wv[4 * j + 0];
+        ay[j] = wv[4 * j + 1];
+        az[j] = wv[4 * j + 2];
+        mabs[j] = std::fmax(std::fabs((double)lo[j]), std::fabs((double)hi[j]));
+    }
+    const double tx = wv[12], ty = wv[13], tz = wv[14];
+    const double Sx = (std::fabs(ax[0]) * mabs[0] + std::fabs(ax[1]) * mabs[1]) + (std::fabs(ax[2]) * mabs[2] + std::fabs(tx));
+    const double Sy = (std::fabs(ay[0]) * mabs[0] + std::fabs(ay[1]) * mabs[1]) + (std::fabs(ay[2]) * mabs[2] + std::fabs(ty));
+    const double Sz = (std::fabs(az[0]) * mabs[0] + std::fabs(az[1]) * mabs[1]) + (std::fabs(az[2]) * mabs[2] + std::fabs(tz));
+    if (!(Sx < 1e30 && Sy < 1e30 && Sz < 1e30)) return 0u;
+    auto lin_min = [&](const double* a, double b) {
+        double s = b;
+        for (int j = 0; j < 3; ++j) s += a[j] >= 0.0 ? a[j] * (double)lo[j] : a[j] * (double)hi[j];
+        return s;
+    };
+    auto lin_max = [&](const double* a, double b) {
+        double s = b;
+        for (int j = 0; j < 3; ++j) s += a[j] >= 0.0 ? a[j] * (double)hi[j] : a[j] * (double)lo[j];
+        return s;
+    };
+    const double ez = EPS * Sz + ABS;
+    if (lin_min(az, tz) - ez >= 0.0) return CR_OC_BEHIND;
+    if (!(lin_max(az, tz) + ez < 0.0)) return 0u;
+    const double F = fa, G = f;
+    const double mx = 2.0 * EPS * (F * Sx + Sz) + ABS;
+    const double my = 2.0 * EPS * (G * Sy + Sz) + ABS;
+    const double up = 1.0 + EPS, dn = 1.0 - EPS;
+    double a[3];
+    uint32_t c = 0u, inside = 0u;
+    const double* rows[2] = {ax, ay};
+    const double tr[2] = {tx, ty};
+    const double sc[2] = {F, G};
+    const double mm[2] = {mx, my};
+    const uint32_t bitPos[2] = {CR_OC_RIGHT, CR_OC_TOP}, bitNeg[2] = {CR_OC_LEFT, CR_OC_BOTTOM};
+    for (int r = 0; r < 2; ++r)
+        for (int sg = 0; sg < 2; ++sg) {
+            const double k = sg == 0 ? sc[r] : -sc[r];
+            for (int j = 0; j < 3; ++j) a[j] = k * rows[r][j] + up * az[j];
+            if (lin_min(a, k * tr[r] + up * tz) > mm[r]) c |= sg == 0 ? bitPos[r] : bitNeg[r];
+            for (int j = 0; j < 3; ++j) a[j] = k * rows[r][j] + dn * az[j];
+            if (lin_max(a, k * tr[r] + dn * tz) < -mm[r]) inside |= 1u << (2 * r + sg);
+        }
+    if (c) return c;
+    return inside == 15u ? CR_MESH_INSIDE : 0u;
+}
+
 cr_status assemble(cr_context* ctx, const cr_instance* instances, uint32_t count, const float* view, uint32_t flags,
                    Assembled& A, const uint64_t* firstIds) {
     for (uint32_t i = 0; i < count; i++) {
@@ -176,6 +233,9 @@ cr_status assemble(cr_context* ctx, const cr_instance* instances, uint32_t count
             s.instanceCount = 0;
             s.flags = (m.indices && ((uintptr_t)m.indices & 15u) == 0) ? 1u : 0u;
             s.itemBoxes = m.itemBoxes;
+            s.subBoxes = m.subBoxes;
+            s.localLists = m.localLists;
+            s.localCounts = m.localCounts;
             A.seg.push_back(s);
         }
         A.seg.back().instanceCount++;
@@ -219,16 +279,46 @@ cr_status ensure_queues(cr_context* ctx, uint64_t ntWant, uint64_t hugeWant) {
 cr_status build_mesh_boxes(cr_context* ctx, MeshRec& m) {
     const size_t ib = align_up((size_t)((m.numTriangles + CR_BATCH - 1) / CR_BATCH) * 24, 256);
     const size_t cb = align_up((size_t)((m.numVertices + CR_VCHUNK - 1) / CR_VCHUNK) * 24, 256);
+    const size_t sb = align_up((size_t)((m.numTriangles + CR_SUB - 1) / CR_SUB) * 24, 256);
     if (!m.itemBoxes) {
-        cr_status s = ctx->dev_alloc((void**)&m.itemBoxes, ib + cb, "mesh boxes");
+        cr_status s = ctx->dev_alloc((void**)&m.itemBoxes, ib + cb + sb + 256, "mesh boxes");
         if (s) return s;
         m.chunkBoxes = (float*)((char*)m.itemBoxes + ib);
-        m.boxBytes = ib + cb;
+        m.subBoxes = (float*)((char*)m.itemBoxes + ib + cb);
+        m.boxBytes = ib + cb + sb + 256;
     }
-    if (cr_launch_mesh_boxes(m.indices, m.positions, m.numTriangles, m.numVertices, m.itemBoxes, m.chunkBoxes, 0))
+    float* meshBox = (float*)((char*)m.itemBoxes + ib + cb + sb);
+    if (cr_launch_mesh_boxes(m.indices, m.positions, m.numTriangles, m.numVertices, m.itemBoxes, m.chunkBoxes,
+                             m.subBoxes, meshBox, 0))
         return fail(CR_ERR_CUDA, "mesh box launch: %s", cudaGetErrorString(cudaGetLastError()));
     CR_CUDA(cudaDeviceSynchronize(), "mesh boxes");
+    CR_CUDA(cudaMemcpy(m.box, meshBox, sizeof(m.box), cudaMemcpyDeviceToHost), "mesh box readback");
     return CR_OK;
+}
+
+// Per-item vertex lists of an indexed mesh, built once on first use (a
+// budget or allocation failure leaves them absent: the frame then draws
+// without them, with the same output).
+void ensure_local_lists(cr_context* ctx, MeshRec& m) {
+    if (m.localTried || !m.indices || m.numTriangles == 0) return;
+    m.localTried = true;
+    const size_t nItems = (m.numTriangles + CR_BATCH - 1) / CR_BATCH;
+    const size_t lb = align_up(nItems * CR_LOCAL_BYTES, 256);
+    const size_t bytes = lb + align_up(nItems * 4, 256);
+    if (ctx->dev_alloc((void**)&m.localLists, bytes, "vertex lists") != CR_OK) {
+        cr_internal_set_error("");
+        m.localLists = nullptr;
+        return;
+    }
+    m.localCounts = (uint32_t*)(m.localLists + lb);
+    m.localBytes = bytes;
+    if (cr_launch_local_lists(m.indices, m.numTriangles, m.localLists, m.localCounts, 0) ||
+        cudaDeviceSynchronize() != cudaSuccess) {
+        ctx->dev_free(m.localLists, m.localBytes);
+        m.localLists = nullptr;
+        m.localCounts = nullptr;
+        m.localBytes = 0;
+    }
 }
 
 // Packs the assembled frame into pinned memory and copies it to the device.
@@ -473,6 +563,7 @@ cr_status cr_destroy(cr_context* ctx) {
             cudaFree(m.colors);
         }
         if (m.itemBoxes) cudaFree(m.itemBoxes);
+        if (m.localLists) cudaFree(m.localLists);
     }
     if (ctx->itemList) cudaFree(ctx->itemList);
     if (ctx->outcodes) cudaFree(ctx->outcodes);
@@ -570,6 +661,7 @@ cr_status cr_mesh_destroy(cr_context* ctx, uint32_t mesh) {
         ctx->bytesInUse -= std::min(ctx->bytesInUse, m.bytes);
     }
     ctx->dev_free(m.itemBoxes, m.boxBytes);
+    ctx->dev_free(m.localLists, m.localBytes);
     m = MeshRec{};
     return CR_OK;
 }
@@ -578,7 +670,13 @@ cr_status cr_mesh_refresh(cr_context* ctx, uint32_t mesh) {
     if (!ctx || mesh >= ctx->meshes.size() || !ctx->meshes[mesh].live) return fail(CR_ERR_NOT_FOUND, "unknown mesh %u", mesh);
     CR_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
     CR_CUDA(cudaDeviceSynchronize(), "mesh refresh");
-    return build_mesh_boxes(ctx, ctx->meshes[mesh]);
+    MeshRec& m = ctx->meshes[mesh];
+    ctx->dev_free(m.localLists, m.localBytes);  // rebuilt on next use
+    m.localLists = nullptr;
+    m.localCounts = nullptr;
+    m.localBytes = 0;
+    m.localTried = false;
+    return build_mesh_boxes(ctx, m);
 }
 
 cr_status cr_mesh_device_arrays(cr_context* ctx, uint32_t mesh, uint64_t* d_positions, uint64_t* d_indices,
@@ -642,21 +740,48 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
     cudaStream_t stream = (cudaStream_t)stream_;
     CR_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
 
+    // what stage 1 culls from: one outcode byte or one 8-byte cell record per
+    // (instance, vertex), or (no records) box proofs of the sample-miss cull
+    // and per-item vertex lists; the choice changes speed only, never the output
+    const uint32_t rec = ctx->cfg.cull_records;
+    bool instanced = false;  // some mesh drawn more than once
+    if (rec == CR_CULL_AUTO && count > 1) {
+        std::vector<uint32_t> ms(count);
+        for (uint32_t i = 0; i < count; i++) ms[i] = instances[i].mesh;
+        std::sort(ms.begin(), ms.end());
+        instanced = std::adjacent_find(ms.begin(), ms.end()) != ms.end();
+    }
+    uint32_t cellMode = rec == CR_CULL_CELLS      ? CR_REC_CELLS
+                        : rec == CR_CULL_OUTCODES ? CR_REC_OUTCODES
+                        : rec == CR_CULL_BOXES    ? CR_REC_BOXES
+                        : instanced               ? CR_REC_BOXES
+                        : count > 1               ? CR_REC_CELLS
+                                                  : CR_REC_OUTCODES;
+    if (cellMode == CR_REC_CELLS && (cam->width > 65535 || cam->height > 65535))
+        cellMode = CR_REC_OUTCODES;  // cells hold 16-bit coordinates
+    const bool direct = cellMode == CR_REC_BOXES;
+    if (direct && !(flags & kRenderResolveOnly))
+        for (uint32_t i = 0; i < count; i++) {
+            const uint32_t m = instances[i].mesh;
+            if (m < ctx->meshes.size() && ctx->meshes[m].live) ensure_local_lists(ctx, ctx->meshes[m]);
+        }
+
     Assembled A;
     cr_status s = assemble(ctx, instances, count, cam->view, flags, A, firstIds);
     if (s) return s;
+    {  // whole-mesh classes: fa as the kernels form it (f / aspect in float)
+        const float f = cam->proj[5];
+        const float fa = f / ((float)cam->width / (float)cam->height);
+        for (uint32_t r = 0; r < count; r++)
+            A.inst[r].meshClass =
+                classify_mesh_box(&A.worldView[16ull * r], fa, f, ctx->meshes[instances[A.order[r]].mesh].box);
+    }
     // frame tables, queues and counters are shared by consecutive frames,
     // which may be issued on different streams
     CR_CUDA(cudaStreamWaitEvent(stream, ctx->frameDone, 0), "stream wait");
     const uint64_t numPixels = (uint64_t)cam->width * (uint64_t)cam->height;
 
-    // vertex-pass records: one outcode byte, or one 8-byte cell record, per
-    // (instance, vertex); the choice changes speed only, never the output
-    uint32_t cellMode = ctx->cfg.cull_records == CR_CULL_CELLS ? 1u
-                        : ctx->cfg.cull_records == CR_CULL_OUTCODES ? 0u
-                                                                    : (count > 1 ? 1u : 0u);
-    if (cam->width > 65535 || cam->height > 65535) cellMode = 0;  // cells hold 16-bit coordinates
-    s = ensure_records(ctx, A.outBytes * (cellMode ? 8 : 1));
+    s = ensure_records(ctx, direct ? 0 : A.outBytes * (cellMode == CR_REC_CELLS ? 8 : 1));
     if (s) return s;
     if (A.numItems > ctx->itemCap || A.numVChunks > ctx->chunkCap) {
         // item-cull survivors (at most every item) and one class per chunk
@@ -685,6 +810,10 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
     fp.itemList = ctx->itemList;
     fp.itemCap = ctx->itemCap;
     fp.chunkList = ctx->chunkList;
+    if (direct) {  // no vertex pass: no chunks to classify or evaluate
+        fp.chunkList = nullptr;
+        fp.numVChunks = 0;
+    }
     fp.fb = (uint64_t*)d_visbuffer;
     fp.W = cam->width;
     fp.H = cam->height;
@@ -746,7 +875,7 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
     };
     const bool culled = fp.itemList && !(flags & kRenderResolveOnly);
     return run_frame(ctx, flags, stream, count, A.totalTriangles, issue, culled ? A.numItems : 0,
-                     culled ? A.numVChunks : 0);
+                     culled ? fp.numVChunks : 0);
 }
 
 extern "C" {

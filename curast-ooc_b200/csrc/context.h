@@ -13,6 +13,7 @@
 #include <functional>
 #include <mutex>
 #include <string>
+#include <cmath>
 #include <vector>
 
 #include "cr_device.h"
@@ -41,7 +42,14 @@ struct MeshRec {
     // hierarchical-cull boxes (library-owned, also for borrowed meshes)
     float* itemBoxes = nullptr;   // per CR_BATCH triangles
     float* chunkBoxes = nullptr;  // per CR_VCHUNK vertices
+    float* subBoxes = nullptr;    // per CR_SUB triangles
     size_t boxBytes = 0;
+    float box[6] = {NAN, NAN, NAN, NAN, NAN, NAN};  // host copy of the mesh box
+    // per-item vertex lists, built on first use in a box-culled frame
+    uint8_t* localLists = nullptr;
+    uint32_t* localCounts = nullptr;
+    size_t localBytes = 0;
+    bool localTried = false;
 };
 
 void mat4_mul(const float* a, const float* b, float* out);  // glm order

@@ -16,6 +16,17 @@
 #define CR_TILE_SIZE 64         // HostDeviceInterface.h:261
 #define CR_BATCH 128            // triangles per stage-1 warp item (4 per lane)
 #define CR_INST_CHUNK 16        // instances per stage-1 warp item
+#define CR_SUB 16               // triangles per sub-box (CR_BATCH / CR_SUB per item)
+// Per-item vertex lists (CR_REC_BOXES frames): for each item, the sorted
+// distinct vertices its triangles reference (at most CR_LOCAL_MAX) and each
+// triangle's three positions in that list, in one CR_LOCAL_BYTES block:
+//   uint32_t vertex[CR_LOCAL_MAX]    bytes    0 .. 1023
+//   uint8_t  corner[3 * CR_BATCH]    bytes 1024 .. 1407
+// and, per item, the number of distinct vertices (CR_LOCAL_NONE: more than
+// CR_LOCAL_MAX, or a non-indexed mesh; the item is drawn without a list).
+#define CR_LOCAL_MAX 256
+#define CR_LOCAL_BYTES 1408
+#define CR_LOCAL_NONE 0xffffffffu
 
 // counters[] slots
 #define CR_CTR_NONTRIVIAL 0     // entries appended to the stage-2 queue
@@ -34,7 +45,7 @@ struct alignas(16) CrInstance {
     uint32_t numTriangles;
     uint32_t flip;              // det(world_view 3x3) < 0, tv.cu:179-185
     uint32_t numVertices;
-    uint32_t pad0;
+    uint32_t meshClass;         // the whole mesh box classified for this view (CR_MESH_*)
     uint64_t outBase;           // first outcode byte of this instance
     uint64_t vchunkBase;        // first vertex-pass chunk of this instance
     const float* chunkBoxes;    // per CR_VCHUNK vertices: min xyz, max xyz (or nullptr)
@@ -50,6 +61,12 @@ struct alignas(16) CrInstance {
 #define CR_OC_TOP 8u            // ndc.y > +1                      (tv.cu:116)
 #define CR_OC_BOTTOM 16u        // ndc.y < -1                      (tv.cu:117)
 #define CR_OC_SIDES 30u
+// CrInstance::meshClass: the bounding box of every vertex of the mesh,
+// classified for the frame's view on the host with the same rigorous bounds
+// as the device's item boxes.  Any CR_OC_* bit: every triangle of the
+// instance is culled; CR_MESH_INSIDE: no vertex is behind the camera or
+// beyond a frustum side, so no item box needs classifying; 0: unknown.
+#define CR_MESH_INSIDE 32u
 #define CR_VCHUNK 1024          // vertices per vertex-pass chunk
 
 // Cell records (8 bytes per (instance, vertex), CrFrameParams::cellMode):
@@ -76,9 +93,11 @@ struct alignas(16) CrSegment {
     uint32_t flags;             // bit 0: index array 16-byte aligned (TMA tiles)
     uint64_t itemBase;          // first stage-1 work item of this segment
     const float* itemBoxes;     // per CR_BATCH triangles: box of their vertices (or nullptr)
-    uint64_t pad;
+    const float* subBoxes;      // per CR_SUB triangles: box of their vertices (or nullptr)
+    const uint8_t* localLists;  // per item, CR_LOCAL_BYTES (or nullptr)
+    const uint32_t* localCounts;  // per item, distinct vertices or CR_LOCAL_NONE
 };
-static_assert(sizeof(CrSegment) == 64, "CrSegment layout");
+static_assert(sizeof(CrSegment) == 80, "CrSegment layout");
 
 struct alignas(16) CrTile {     // HugeTriangle, HostDeviceInterface.h:254-259
     int32_t instance;           // instance | view << 26 (view 0 in single-view frames)
@@ -147,7 +166,7 @@ struct CrFrameParams {
     // view-major; the vertex pass writes CrViewMasks records instead of bytes
     const CrView* views;
     uint32_t numViews;
-    uint32_t cellMode;          // 1: the vertex pass writes 8-byte cell records
+    uint32_t cellMode;          // CR_REC_* below: what stage 1 culls from
     CrViewMasks* viewMasks;     // CrInstance::outBase + vertex
     const uint32_t* flips;      // numViews * numInstances, view-major
     // item cull: surviving work items {item, instance mask within its
@@ -159,6 +178,12 @@ struct CrFrameParams {
     // counters[CR_CTR_CHUNKS]; nullptr: every chunk
     uint32_t* chunkList;
 };
+
+// CrFrameParams::cellMode
+#define CR_REC_OUTCODES 0u      // the vertex pass writes 1-byte outcodes
+#define CR_REC_CELLS 1u         // the vertex pass writes 8-byte cell records
+#define CR_REC_BOXES 2u         // no vertex pass: item and sub-box proofs of the
+                                // sample-miss cull, survivors evaluated directly
 
 struct CrResolveParams {
     const CrInstance* instances;
@@ -198,10 +223,15 @@ int cr_launch_cull(const CrFrameParams& p, const CrLaunchShape& s, void* stream)
 int cr_launch_resolve(const CrResolveParams& p, void* stream);
 
 // Mesh preparation (meshprep.cu): the box of the vertices of every CR_BATCH
-// consecutive triangles and of every CR_VCHUNK consecutive vertices (a box
+// and every CR_SUB consecutive triangles and of every CR_VCHUNK consecutive
+// vertices (a box
 // with a non-finite position is NaN and culls nothing).
 int cr_launch_mesh_boxes(const uint32_t* indices, const float* positions, uint32_t numTriangles,
-                         uint32_t numVertices, float* itemBoxes, float* chunkBoxes, void* stream);
+                         uint32_t numVertices, float* itemBoxes, float* chunkBoxes, float* subBoxes,
+                         float* meshBox, void* stream);
+// Per-item vertex lists of an indexed mesh (see CR_LOCAL_BYTES).
+int cr_launch_local_lists(const uint32_t* indices, uint32_t numTriangles, uint8_t* lists, uint32_t* counts,
+                          void* stream);
 
 // Batched (multi-view) frame: one launch per stage over all views.  Grid
 // sizes are chosen by the host (defaults from occupancy, or tuned).

@@ -3,8 +3,12 @@
 //
 //   item boxes   one per CR_BATCH (128) consecutive triangles: the box of
 //                every vertex those triangles reference (a stage-1 work item)
+//   sub-boxes    one per CR_SUB (16) consecutive triangles, for the sample-miss
+//                proof of box_misses_samples
 //   chunk boxes  one per CR_VCHUNK (1024) consecutive vertices (a vertex-pass
 //                chunk)
+//   mesh box     the union of the item boxes, classified per instance on the
+//                host
 // Per view, a box classified by classify_chunk as wholly behind the camera
 // or wholly beyond one frustum side proves that every triangle of the item
 // (every vertex of the chunk) meets the reference's own cull for it, so the
@@ -60,6 +64,37 @@ __global__ void __launch_bounds__(256) k_item_boxes(const uint32_t* idx, const f
     }
 }
 
+// Half a warp per sub-box: lane t of the half is its triangle t.
+__global__ void __launch_bounds__(256) k_sub_boxes(const uint32_t* idx, const float* pos, uint32_t nT, float* boxes) {
+    const int lane = threadIdx.x & 31;
+    const int half = lane >> 4, hl = lane & 15;
+    static_assert(CR_SUB == 16, "half-warp per sub-box");
+    const uint32_t nSub = (nT + CR_SUB - 1) / CR_SUB;
+    const uint32_t nPairs = (nSub + 1) / 2;
+    for (uint32_t b = blockIdx.x * 8 + (threadIdx.x >> 5); b < nPairs; b += gridDim.x * 8) {
+        const uint32_t sb = 2 * b + half;
+        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        bool bad = false;
+        const uint32_t t = sb * CR_SUB + hl;
+        if (sb < nSub && t < nT)
+            for (int k = 0; k < 3; ++k) {
+                const uint32_t v = idx ? __ldg(idx + 3ull * t + k) : 3 * t + k;
+                extend(lo, hi, bad, pos + 3ull * v);
+            }
+#pragma unroll
+        for (int d = 8; d >= 1; d >>= 1)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                lo[j] = fminf(lo[j], __shfl_xor_sync(FULL, lo[j], d));
+                hi[j] = fmaxf(hi[j], __shfl_xor_sync(FULL, hi[j], d));
+            }
+        const unsigned anyBad = __ballot_sync(FULL, bad);
+        bad = (anyBad >> (16 * half)) & 0xffffu;
+        if (sb < nSub && hl < 6)
+            boxes[6ull * sb + hl] = bad ? __int_as_float(0x7fffffff) : (hl < 3 ? lo[hl] : hi[hl - 3]);
+    }
+}
+
 // One warp per chunk of CR_VCHUNK vertices.
 __global__ void __launch_bounds__(256) k_chunk_boxes(const float* pos, uint32_t nV, float* boxes) {
     const int lane = threadIdx.x & 31;
@@ -73,16 +108,151 @@ __global__ void __launch_bounds__(256) k_chunk_boxes(const float* pos, uint32_t 
     }
 }
 
+// One block: the union of the item boxes (a NaN box makes it NaN).
+__global__ void __launch_bounds__(256) k_mesh_box(const float* itemBoxes, uint32_t nItems, float* out) {
+    __shared__ float s_lo[3][8], s_hi[3][8];
+    __shared__ int s_bad[8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    bool bad = false;
+    for (uint32_t b = threadIdx.x; b < nItems; b += 256) {
+        const float* q = itemBoxes + 6ull * b;
+        for (int j = 0; j < 3; ++j) {
+            const float l = __ldg(q + j), h = __ldg(q + 3 + j);
+            bad |= !(l <= h);  // NaN boxes
+            lo[j] = fminf(lo[j], l);
+            hi[j] = fmaxf(hi[j], h);
+        }
+    }
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            lo[j] = fminf(lo[j], __shfl_xor_sync(FULL, lo[j], d));
+            hi[j] = fmaxf(hi[j], __shfl_xor_sync(FULL, hi[j], d));
+        }
+    bad = __any_sync(FULL, bad);
+    if (lane == 0) {
+        for (int j = 0; j < 3; ++j) {
+            s_lo[j][w] = lo[j];
+            s_hi[j][w] = hi[j];
+        }
+        s_bad[w] = bad;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        const int j = threadIdx.x % 3;
+        float v = threadIdx.x < 3 ? INFINITY : -INFINITY;
+        int anyBad = 0;
+        for (int k = 0; k < 8; ++k) {
+            v = threadIdx.x < 3 ? fminf(v, s_lo[j][k]) : fmaxf(v, s_hi[j][k]);
+            anyBad |= s_bad[k];
+        }
+        out[threadIdx.x] = (anyBad || nItems == 0) ? __int_as_float(0x7fffffff) : v;
+    }
+}
+
+// One warp per item: the item's 3 CR_BATCH indices are sorted in shared
+// memory (bitonic network over 512 slots, padded with ~0u), the distinct
+// values compacted into the list, and each index replaced by its position in
+// the list (binary search).  Items with more than CR_LOCAL_MAX distinct
+// vertices get CR_LOCAL_NONE.
+constexpr int LL_WARPS = 4;
+__global__ void __launch_bounds__(LL_WARPS * 32) k_local_lists(const uint32_t* idx, uint32_t nT, uint8_t* lists,
+                                                                uint32_t* counts) {
+    __shared__ uint32_t s_key[LL_WARPS][512];
+    __shared__ uint32_t s_uni[LL_WARPS][512];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t* key = s_key[w];
+    uint32_t* uni = s_uni[w];
+    const uint32_t nItems = (nT + CR_BATCH - 1) / CR_BATCH;
+    for (uint32_t b = blockIdx.x * LL_WARPS + w; b < nItems; b += gridDim.x * LL_WARPS) {
+        const uint32_t t0 = b * CR_BATCH;
+        const uint32_t nt = min((uint32_t)CR_BATCH, nT - t0);
+        for (int i = lane; i < 512; i += 32) key[i] = i < 3 * (int)nt ? __ldg(idx + 3ull * t0 + i) : ~0u;
+        __syncwarp();
+        for (int k = 2; k <= 512; k <<= 1)
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = lane; i < 512; i += 32) {
+                    const int l = i ^ j;
+                    if (l > i) {
+                        const uint32_t a = key[i], c = key[l];
+                        const bool up = (i & k) == 0;
+                        if ((a > c) == up) {
+                            key[i] = c;
+                            key[l] = a;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        // distinct values: lane owns slots 16 lane .. 16 lane + 15
+        uint32_t flags = 0;
+        for (int q = 0; q < 16; ++q) {
+            const int i = 16 * lane + q;
+            const uint32_t v = key[i];
+            if (v != ~0u && (i == 0 || key[i - 1] != v)) flags |= 1u << q;
+        }
+        const int mine = __popc(flags);
+        int incl = mine;
+        for (int d = 1; d < 32; d <<= 1) {
+            const int o = __shfl_up_sync(FULL, incl, d);
+            if (lane >= d) incl += o;
+        }
+        const int total = __shfl_sync(FULL, incl, 31);
+        int pos = incl - mine;
+        for (int q = 0; q < 16; ++q)
+            if ((flags >> q) & 1u) uni[pos++] = key[16 * lane + q];
+        __syncwarp();
+        if (lane == 0) counts[b] = total <= CR_LOCAL_MAX ? (uint32_t)total : CR_LOCAL_NONE;
+        if (total > CR_LOCAL_MAX) continue;  // warp-uniform
+        uint8_t* L = lists + (uint64_t)b * CR_LOCAL_BYTES;
+        uint32_t* vl = reinterpret_cast<uint32_t*>(L);
+        for (int i = lane; i < CR_LOCAL_MAX; i += 32) vl[i] = i < total ? uni[i] : 0u;
+        for (int i = lane; i < 3 * CR_BATCH; i += 32) {
+            uint8_t loc = 0;
+            if (i < 3 * (int)nt) {
+                const uint32_t v = __ldg(idx + 3ull * t0 + i);
+                int lo = 0, hi = total - 1;  // uni[lo] == v
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (uni[mid] < v) lo = mid + 1;
+                    else hi = mid;
+                }
+                loc = (uint8_t)lo;
+            }
+            L[1024 + i] = loc;
+        }
+        __syncwarp();
+    }
+}
+
 }  // namespace
 
+int cr_launch_local_lists(const uint32_t* indices, uint32_t numTriangles, uint8_t* lists, uint32_t* counts,
+                          void* stream) {
+    const uint32_t nItems = (numTriangles + CR_BATCH - 1) / CR_BATCH;
+    if (!nItems) return 0;
+    const uint32_t want = (nItems + LL_WARPS - 1) / LL_WARPS;
+    k_local_lists<<<want < 148 * 16 ? want : 148 * 16, LL_WARPS * 32, 0, (cudaStream_t)stream>>>(
+        indices, numTriangles, lists, counts);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
 int cr_launch_mesh_boxes(const uint32_t* indices, const float* positions, uint32_t numTriangles,
-                         uint32_t numVertices, float* itemBoxes, float* chunkBoxes, void* stream) {
+                         uint32_t numVertices, float* itemBoxes, float* chunkBoxes, float* subBoxes,
+                         float* meshBox, void* stream) {
     cudaStream_t st = (cudaStream_t)stream;
     const uint32_t nItems = (numTriangles + CR_BATCH - 1) / CR_BATCH;
     const uint32_t nChunks = (numVertices + CR_VCHUNK - 1) / CR_VCHUNK;
     if (nItems) k_item_boxes<<<(nItems + 7) / 8 < 148 * 16 ? (nItems + 7) / 8 : 148 * 16, 256, 0, st>>>(
         indices, positions, numTriangles, itemBoxes);
+    const uint32_t nPairs = ((numTriangles + CR_SUB - 1) / CR_SUB + 1) / 2;
+    if (nPairs && subBoxes)
+        k_sub_boxes<<<(nPairs + 7) / 8 < 148 * 16 ? (nPairs + 7) / 8 : 148 * 16, 256, 0, st>>>(
+            indices, positions, numTriangles, subBoxes);
     if (nChunks) k_chunk_boxes<<<(nChunks + 7) / 8 < 148 * 16 ? (nChunks + 7) / 8 : 148 * 16, 256, 0, st>>>(
         positions, numVertices, chunkBoxes);
+    if (meshBox) k_mesh_box<<<1, 256, 0, st>>>(itemBoxes, nItems, meshBox);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

@@ -48,7 +48,7 @@ __global__ void __launch_bounds__(THREADS) k_vertex(const CrFrameParams p) {
         const uint32_t v1 = min(v0 + (uint32_t)CR_VCHUNK, nV);
         const float* pos = ldg_ptr(&I->positions);
         const Mat M = load_mat(p.world_view + 4ull * lo);
-        if (p.cellMode) {
+        if (p.cellMode == CR_REC_CELLS) {
             uint64_t* out = reinterpret_cast<uint64_t*>(p.outcodes) + __ldg(&I->outBase);
             for (uint32_t v = v0 + threadIdx.x; v < v1; v += THREADS)
                 out[v] = vertex_cell_record(M, load_pos(pos, v), fa, p.f, Wf, Hf, p.W, p.H);
@@ -69,7 +69,9 @@ __global__ void __launch_bounds__(THREADS) k_vertex(const CrFrameParams p) {
 //   items   the item's box is classified for each instance of its chunk; an
 //           instance whose box is wholly behind or beyond one side has every
 //           triangle of the item culled by the reference's own tests
-//           (tv.cu:110-119).  Items with a surviving instance are appended
+//           (tv.cu:110-119); without vertex records (CR_REC_BOXES) so has one
+//           whose box provably misses every sample (box_misses_samples,
+//           tv.cu:153-158).  Items with a surviving instance are appended
 //           (warp-aggregated) with the mask of those instances.
 // Skipping what the boxes prove cannot change the visbuffer.
 template <int THREADS>
@@ -116,7 +118,7 @@ __global__ void __launch_bounds__(THREADS) k_cull(const CrFrameParams p) {
             const uint64_t cIdx = gj - __ldg(&I->vchunkBase);
             const uint32_t nv = min((uint32_t)CR_VCHUNK, __ldg(&I->numVertices) - (uint32_t)cIdx * CR_VCHUNK);
             const uint64_t v0 = __ldg(&I->outBase) + cIdx * CR_VCHUNK;
-            if (p.cellMode) {  // 16-byte aligned: (outBase + k CR_VCHUNK) * 8
+            if (p.cellMode == CR_REC_CELLS) {  // 16-byte aligned: (outBase + k CR_VCHUNK) * 8
                 uint64_t* out = reinterpret_cast<uint64_t*>(p.outcodes) + v0;
                 for (uint32_t v = 2 * lane; v < nv; v += 64) {
                     if (v + 1 < nv) *reinterpret_cast<ulonglong2*>(out + v) = make_ulonglong2(cj, cj);
@@ -144,6 +146,7 @@ __global__ void __launch_bounds__(THREADS) k_cull(const CrFrameParams p) {
         }
     }
     if (!p.itemList) return;
+    const double invW = 1.0 / (double)p.W, invH = 1.0 / (double)p.H;
     for (uint64_t base = (uint64_t)blockIdx.x * THREADS; base < p.numItems; base += stride) {
         const uint64_t item = base + threadIdx.x;
         uint32_t mask = 0;
@@ -160,9 +163,16 @@ __global__ void __launch_bounds__(THREADS) k_cull(const CrFrameParams p) {
                 const float* bx = boxes + 6ull * it.batch;
                 const float blo[3] = {__ldg(bx), __ldg(bx + 1), __ldg(bx + 2)};
                 const float bhi[3] = {__ldg(bx + 3), __ldg(bx + 4), __ldg(bx + 5)};
-                for (uint32_t inst = ib; inst < ie; ++inst)
-                    if (!(classify_box(load_mat(p.world_view + 4ull * inst), fa, p.f, blo, bhi) & CR_OC_MASK))
-                        mask |= 1u << (inst - ib);
+                const bool samples = p.cellMode == CR_REC_BOXES;
+                for (uint32_t inst = ib; inst < ie; ++inst) {
+                    // the instance's whole-mesh class, from the host, first
+                    const uint32_t mc = __ldg(&p.instances[inst].meshClass);
+                    if (mc & CR_OC_MASK) continue;
+                    const Mat M = load_mat(p.world_view + 4ull * inst);
+                    if (!(mc & CR_MESH_INSIDE) && (classify_box(M, fa, p.f, blo, bhi) & CR_OC_MASK)) continue;
+                    if (samples && box_misses_samples(M, fa, p.f, p.W, p.H, invW, invH, blo, bhi)) continue;
+                    mask |= 1u << (inst - ib);
+                }
             }
         }
         const unsigned m = __ballot_sync(FULL, mask != 0);
@@ -179,25 +189,93 @@ __global__ void __launch_bounds__(THREADS) k_cull(const CrFrameParams p) {
     }
 }
 
+// Culls from the vertex pass's records (outcode bytes or cell records),
+// gathered per triangle corner.
+__device__ __forceinline__ void gather_culls(const CrFrameParams& p, uint32_t inst, const uint32_t (&ix)[S1_R][3],
+                                             const bool (&act)[S1_R], bool (&culledR)[S1_R]) {
+    if (p.cellMode == CR_REC_CELLS) {
+        const uint64_t* rec = reinterpret_cast<const uint64_t*>(p.outcodes) + __ldg(&p.instances[inst].outBase);
+        uint64_t o[S1_R][3];
+#pragma unroll
+        for (int r = 0; r < S1_R; ++r) {
+            o[r][0] = act[r] ? __ldg(rec + ix[r][0]) : 0ull;
+            o[r][1] = act[r] ? __ldg(rec + ix[r][1]) : 0ull;
+            o[r][2] = act[r] ? __ldg(rec + ix[r][2]) : 0ull;
+        }
+#pragma unroll
+        for (int r = 0; r < S1_R; ++r) culledR[r] = cell_culled(o[r][0], o[r][1], o[r][2]);
+    } else {
+        const uint8_t* oc = p.outcodes + __ldg(&p.instances[inst].outBase);
+        uint32_t o[S1_R][3];
+#pragma unroll
+        for (int r = 0; r < S1_R; ++r) {
+            o[r][0] = act[r] ? __ldg(oc + ix[r][0]) : 0u;
+            o[r][1] = act[r] ? __ldg(oc + ix[r][1]) : 0u;
+            o[r][2] = act[r] ? __ldg(oc + ix[r][2]) : 0u;
+        }
+        // all behind (tv.cu:119) or all beyond one side with none behind
+        // (tv.cu:110-118)
+#pragma unroll
+        for (int r = 0; r < S1_R; ++r) {
+            const uint32_t all = o[r][0] & o[r][1] & o[r][2];
+            const uint32_t any = o[r][0] | o[r][1] | o[r][2];
+            culledR[r] = (all & CR_OC_BEHIND) || (!(any & CR_OC_BEHIND) && (all & CR_OC_SIDES));
+        }
+    }
+}
+
+// What the ring slot of an item holds: its index tile (a full 128-triangle
+// tile of a 16-byte aligned index array), in box-culled frames its vertex-list
+// block when it has one, or nothing (tails and non-indexed meshes, read
+// directly).
+struct TileSrc {
+    const void* src;
+    uint32_t bytes;
+    bool local;
+};
+
+template <bool BOXES>
+__device__ __forceinline__ TileSrc tile_source(const CrSegment* sg, uint32_t batch) {
+    if (BOXES) {
+        const uint32_t* lc = ldg_ptr(&sg->localCounts);
+        if (lc && __ldg(lc + batch) <= CR_LOCAL_MAX)
+            return TileSrc{ldg_ptr(&sg->localLists) + (uint64_t)batch * CR_LOCAL_BYTES, CR_LOCAL_BYTES, true};
+    }
+    if (item_uses_tma(sg, batch))
+        return TileSrc{ldg_ptr(&sg->indices) + (uint64_t)batch * (CR_BATCH * 3), CR_BATCH * 12, false};
+    return TileSrc{nullptr, 0, false};
+}
+
 // A work item is CR_BATCH (128) consecutive triangles of one mesh x up to
-// CR_INST_CHUNK of its instances.  Per item a warp: waits for the item's
-// 1536-byte index tile (TMA ring), gathers the 3 x 4 vertex outcodes of its
-// four triangles per lane at once, culls all-behind / all-beyond-one-side
-// triangles from them, packs the survivors across the lanes and runs the
-// reference's full per-triangle path (stage1_triangle) on those, then hands
-// the ring slot to the item S1_STAGES ahead.
-template <int WARPS>
+// CR_INST_CHUNK of its instances.  Per item a warp waits for the item's tile
+// (TMA ring, one 1D bulk copy per item issued STAGES items ahead), then per
+// instance decides which of its triangles can be culled without positions,
+// packs the others across the lanes and runs the reference's full
+// per-triangle path (stage1_triangle) on those.
+//   records (BOXES false)  the 1-byte outcodes or 8-byte cell records of the
+//                          vertex pass, gathered per triangle corner
+//   BOXES, vertex list     the item's distinct vertices (at most 256) get
+//                          cell records in shared memory per instance, the
+//                          same records the vertex pass would write; each
+//                          triangle reads its three from there
+//   BOXES, no list         sub-box proofs of the sample-miss cull, one per
+//                          (instance, 16 triangles), spread over the lanes
+// Nontrivial triangles are appended with one atomic per warp (ballot / popc).
+template <int WARPS, bool BOXES>
 __global__ void __launch_bounds__(WARPS * 32, 3) k_stage1(const CrFrameParams p) {
-    __shared__ __align__(128) uint32_t s_idx[WARPS][S1_STAGES][CR_BATCH * 3];
-    __shared__ __align__(8) uint64_t s_bar[WARPS][S1_STAGES];
+    constexpr int STAGES = BOXES ? 2 : S1_STAGES;
+    static_assert(CR_LOCAL_BYTES <= CR_BATCH * 12, "a vertex-list block fits a ring slot");
+    __shared__ __align__(128) uint32_t s_idx[WARPS][STAGES][CR_BATCH * 3];
+    __shared__ __align__(8) uint64_t s_bar[WARPS][STAGES];
     __shared__ uint8_t s_surv[WARPS][CR_BATCH];
+    __shared__ __align__(16) uint64_t s_rec[BOXES ? WARPS : 1][BOXES ? CR_LOCAL_MAX : 1];
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
     const uint64_t gw = (uint64_t)blockIdx.x * WARPS + w;
     const uint64_t nw = (uint64_t)gridDim.x * WARPS;
 
     if (lane == 0) {
-        for (int s = 0; s < S1_STAGES; ++s) mbar_init(&s_bar[w][s], 1);
+        for (int s = 0; s < STAGES; ++s) mbar_init(&s_bar[w][s], 1);
         fence_barrier_init();
     }
     __syncwarp();
@@ -208,28 +286,27 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_stage1(const CrFrameParams p)
     const uint64_t nItems = p.itemList ? min((uint64_t)p.counters[CR_CTR_ITEMS], p.itemCap) : p.numItems;
     auto item_at = [&](uint64_t k) -> uint64_t { return p.itemList ? (uint64_t)__ldg(&p.itemList[k].x) : k; };
     uint32_t pending = 0;
-    for (int s = 0; s < S1_STAGES; ++s) {
+    for (int s = 0; s < STAGES; ++s) {
         const uint64_t pk = gw + (uint64_t)s * nw;
         if (pk >= nItems) break;
         const Item it = decode_item(p, item_at(pk));
-        const CrSegment* sg = p.segments + it.seg;
-        if (item_uses_tma(sg, it.batch)) {
+        const TileSrc ts = tile_source<BOXES>(p.segments + it.seg, it.batch);
+        if (ts.src) {
             pending |= 1u << s;
             // failure-detection test hook: the first copy is never issued, so
             // its bounded wait must run out and report a timeout
             const bool drop = (p.debugFlags & 1u) && gw == 0 && s == 0;
-            if (lane == 0 && !drop)
-                bulk_load(s_idx[w][s], ldg_ptr(&sg->indices) + (uint64_t)it.batch * (CR_BATCH * 3),
-                          CR_BATCH * 12, &s_bar[w][s]);
+            if (lane == 0 && !drop) bulk_load(s_idx[w][s], ts.src, ts.bytes, &s_bar[w][s]);
         }
     }
     __syncwarp();
 
     const float fa = p.f / p.aspect;
+    const float Wf = (float)p.W, Hf = (float)p.H;
     uint32_t parity = 0;
     uint32_t k = 0;
     for (uint64_t pk = gw; pk < nItems; pk += nw, ++k) {
-        const int slot = (int)(k % S1_STAGES);
+        const int slot = (int)(k % STAGES);
         const uint32_t bit = 1u << slot;
         const uint64_t item = item_at(pk);
         const uint32_t imask = p.itemList ? __ldg(&p.itemList[pk].y) : 0xffffffffu;
@@ -237,7 +314,9 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_stage1(const CrFrameParams p)
         const CrSegment* sg = p.segments + it.seg;
         const uint32_t numTri = __ldg(&sg->numTriangles);
         const uint32_t* gix = ldg_ptr(&sg->indices);
-        const bool tma = item_uses_tma(sg, it.batch);
+        const TileSrc ts = tile_source<BOXES>(sg, it.batch);
+        const bool tma = ts.src != nullptr;
+        const bool local = BOXES && ts.local;
         const uint32_t tri0 = it.batch * CR_BATCH;
         if (tma) {
             const bool ok =
@@ -249,9 +328,12 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_stage1(const CrFrameParams p)
             parity ^= bit;
             pending &= ~bit;
         }
-        // vertex indices of this lane's triangles (tile position r*32 + lane)
+        const uint32_t* tile = s_idx[w][slot];
+        const uint8_t* corner = reinterpret_cast<const uint8_t*>(tile) + 1024;  // vertex-list blocks
+        // vertex index of corner c of the triangle at tile position pos
         auto index_of = [&](uint32_t pos, int c) -> uint32_t {
-            if (tma) return s_idx[w][slot][3 * pos + c];
+            if (local) return tile[corner[3 * pos + c]];
+            if (tma) return tile[3 * pos + c];
             const uint32_t t = tri0 + pos;
             return gix ? __ldg(gix + 3ull * t + c) : 3 * t + c;
         };
@@ -261,6 +343,7 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_stage1(const CrFrameParams p)
         for (int r = 0; r < S1_R; ++r) {
             const uint32_t pos = r * 32 + lane;
             act[r] = tri0 + pos < numTri;
+            if (BOXES) continue;  // box-culled frames gather no records by index
             ix[r][0] = act[r] ? index_of(pos, 0) : 0;
             ix[r][1] = act[r] ? index_of(pos, 1) : 0;
             ix[r][2] = act[r] ? index_of(pos, 2) : 0;
@@ -270,54 +353,70 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_stage1(const CrFrameParams p)
         const uint32_t count = __ldg(&sg->instanceCount);
         const uint32_t ib = first + it.chunk * CR_INST_CHUNK;
         const uint32_t ie = min(ib + CR_INST_CHUNK, first + count);
-        for (uint32_t inst = ib; inst < ie; ++inst) {
-            if (!((imask >> (inst - ib)) & 1u)) continue;  // its box proved every triangle culled
-            const uint64_t ob = __ldg(&p.instances[inst].outBase);
-            bool culledR[S1_R];
-            if (p.cellMode) {
-                const uint64_t* rec = reinterpret_cast<const uint64_t*>(p.outcodes) + ob;
-                uint64_t o[S1_R][3];
-#pragma unroll
-                for (int r = 0; r < S1_R; ++r) {
-                    o[r][0] = act[r] ? __ldg(rec + ix[r][0]) : 0ull;
-                    o[r][1] = act[r] ? __ldg(rec + ix[r][1]) : 0ull;
-                    o[r][2] = act[r] ? __ldg(rec + ix[r][2]) : 0ull;
-                }
-#pragma unroll
-                for (int r = 0; r < S1_R; ++r) {
-                    const uint64_t all = o[r][0] & o[r][1] & o[r][2];
-                    const uint64_t any = o[r][0] | o[r][1] | o[r][2];
-                    bool c = (all & CR_OC_BEHIND) || (!(any & CR_OC_BEHIND) && (all & CR_OC_SIDES));
-                    // sample miss (tv.cu:153-158): with every vertex on screen
-                    // (so the bbox clamps change nothing), the box misses all
-                    // samples in x (y) iff all three x (y) lie strictly inside
-                    // one pixel cell
-                    if (!c && !(any & CR_OC_BEHIND) && (all & CR_CELL_INSIDE)) {
-                        const uint64_t diff = (o[r][0] ^ o[r][1]) | (o[r][0] ^ o[r][2]);
-                        const bool missX = (all & CR_CELL_FRACX) && !(diff & 0x00000000ffff0000ull);
-                        const bool missY = (all & CR_CELL_FRACY) && !(diff & 0x0000ffff00000000ull);
-                        c = missX || missY;
+        const uint32_t alive = imask & ((1u << (ie - ib)) - 1u);
+        // items without a vertex list: sub-box proofs of the sample-miss cull
+        // for every (surviving instance, sub-box) pair, spread over the lanes;
+        // bit 8 k + b of subw[k / 4] is set unless sub-box b of the k-th
+        // surviving instance is proven to miss every sample
+        uint32_t subw[4] = {~0u, ~0u, ~0u, ~0u};
+        if (BOXES && !local) {
+            const float* sbx = ldg_ptr(&sg->subBoxes);
+            const int nsub = (int)min((uint32_t)(CR_BATCH / CR_SUB), (numTri - tri0 + CR_SUB - 1) / CR_SUB);
+            const int pairs = __popc(alive) * (CR_BATCH / CR_SUB);
+            if (sbx) {
+#pragma unroll 1
+                for (int t = 0; t < 4; ++t) {
+                    if (t * 32 >= pairs) break;
+                    const int j = t * 32 + lane;
+                    bool keep = true;
+                    if (j < pairs && (j & 7) < nsub) {
+                        const uint32_t islot = __fns(alive, 0, (j >> 3) + 1);
+                        const float* bx = sbx + 6ull * ((uint64_t)it.batch * (CR_BATCH / CR_SUB) + (j & 7));
+                        const float blo[3] = {__ldg(bx), __ldg(bx + 1), __ldg(bx + 2)};
+                        const float bhi[3] = {__ldg(bx + 3), __ldg(bx + 4), __ldg(bx + 5)};
+                        keep = !box_misses_samples(load_mat(p.world_view + 4ull * (ib + islot)), fa, p.f, p.W, p.H,
+                                                   1.0 / (double)p.W, 1.0 / (double)p.H, blo, bhi);
                     }
-                    culledR[r] = c;
-                }
-            } else {
-                const uint8_t* oc = p.outcodes + ob;
-                uint32_t o[S1_R][3];
-#pragma unroll
-                for (int r = 0; r < S1_R; ++r) {
-                    o[r][0] = act[r] ? __ldg(oc + ix[r][0]) : 0u;
-                    o[r][1] = act[r] ? __ldg(oc + ix[r][1]) : 0u;
-                    o[r][2] = act[r] ? __ldg(oc + ix[r][2]) : 0u;
-                }
-#pragma unroll
-                for (int r = 0; r < S1_R; ++r) {
-                    const uint32_t all = o[r][0] & o[r][1] & o[r][2];
-                    const uint32_t any = o[r][0] | o[r][1] | o[r][2];
-                    culledR[r] = (all & CR_OC_BEHIND) || (!(any & CR_OC_BEHIND) && (all & CR_OC_SIDES));
+                    subw[t] = __ballot_sync(FULL, keep);
                 }
             }
-            // all behind (tv.cu:119) or all beyond one side with none behind
-            // (tv.cu:110-118): culled from the outcodes alone
+        }
+        static_assert(CR_BATCH / CR_SUB == 8 && CR_INST_CHUNK <= 16, "8 sub-boxes x 16 instances in 4 ballots");
+        const uint32_t nLocal = local ? __ldg(ldg_ptr(&sg->localCounts) + it.batch) : 0u;
+        const float* pos = ldg_ptr(&sg->positions);
+        int rank = 0;
+        for (uint32_t inst = ib; inst < ie; ++inst) {
+            if (!((alive >> (inst - ib)) & 1u)) continue;  // its box proved every triangle culled
+            const int kk = rank++;
+            const Mat M = load_mat(p.world_view + 4ull * inst);
+            bool culledR[S1_R];
+            if constexpr (!BOXES) {
+                gather_culls(p, inst, ix, act, culledR);
+            } else if (local) {
+                // cell records of the item's distinct vertices for this
+                // instance; an instance whose mesh box is inside the frustum
+                // has the outcode 0 at every vertex
+                const bool inside = (__ldg(&p.instances[inst].meshClass) & CR_MESH_INSIDE) != 0u;
+                uint64_t* rec = s_rec[w];
+                for (uint32_t v = lane; v < nLocal; v += 32)
+                    rec[v] = inside ? vertex_cell_record_inside(M, load_pos(pos, tile[v]), fa, p.f, Wf, Hf, p.W, p.H)
+                                    : vertex_cell_record(M, load_pos(pos, tile[v]), fa, p.f, Wf, Hf, p.W, p.H);
+                __syncwarp();
+#pragma unroll
+                for (int r = 0; r < S1_R; ++r) {
+                    const uint32_t tp = r * 32 + lane;
+                    const uint64_t o0 = act[r] ? rec[corner[3 * tp + 0]] : 0ull;
+                    const uint64_t o1 = act[r] ? rec[corner[3 * tp + 1]] : 0ull;
+                    const uint64_t o2 = act[r] ? rec[corner[3 * tp + 2]] : 0ull;
+                    culledR[r] = cell_culled(o0, o1, o2);
+                }
+            } else {
+                const uint32_t w4 = (kk >> 2) == 0 ? subw[0] : (kk >> 2) == 1 ? subw[1] : (kk >> 2) == 2 ? subw[2] : subw[3];
+                const uint32_t sm = (w4 >> (8 * (kk & 3))) & 0xffu;
+#pragma unroll
+                for (int r = 0; r < S1_R; ++r) culledR[r] = !((sm >> (2 * r + (lane >> 4))) & 1u);
+            }
+            // culled from the records or proofs alone: pack the others
             int nsurv = 0;
 #pragma unroll
             for (int r = 0; r < S1_R; ++r) {
@@ -328,10 +427,8 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_stage1(const CrFrameParams p)
             }
             __syncwarp();
             if (nsurv == 0) continue;
-            const Mat M = load_mat(p.world_view + 4ull * inst);
             const uint32_t flip = __ldg(&p.instances[inst].flip);
             const uint64_t cum = __ldg(&p.instances[inst].cum);
-            const float* pos = ldg_ptr(&sg->positions);
             for (int base = 0; base < nsurv; base += 32) {
                 const int j = base + lane;
                 int res = S1_CULL;
@@ -361,17 +458,16 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_stage1(const CrFrameParams p)
         }
 
         __syncwarp();
-        {  // every read of this slot is done: refill it with the item S1_STAGES ahead
-            const uint64_t npk = pk + (uint64_t)S1_STAGES * nw;
+        {  // every read of this slot is done: refill it with the item STAGES ahead
+            const uint64_t npk = pk + (uint64_t)STAGES * nw;
             if (npk < nItems) {
                 const Item nt = decode_item(p, item_at(npk));
-                const CrSegment* ns = p.segments + nt.seg;
-                if (item_uses_tma(ns, nt.batch)) {
+                const TileSrc ns = tile_source<BOXES>(p.segments + nt.seg, nt.batch);
+                if (ns.src) {
                     pending |= bit;
                     if (lane == 0) {
                         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                        bulk_load(s_idx[w][slot], ldg_ptr(&ns->indices) + (uint64_t)nt.batch * (CR_BATCH * 3),
-                                  CR_BATCH * 12, &s_bar[w][slot]);
+                        bulk_load(s_idx[w][slot], ns.src, ns.bytes, &s_bar[w][slot]);
                     }
                 }
             }
@@ -379,7 +475,7 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_stage1(const CrFrameParams p)
     }
     // only after a timeout can copies still be in flight: wait for them
     // (bounded) so none lands in shared memory after the block has exited
-    for (int s = 0; s < S1_STAGES; ++s)
+    for (int s = 0; s < STAGES; ++s)
         if (pending & (1u << s)) (void)mbar_wait_bounded(&s_bar[w][s], (parity >> s) & 1u, p.waitTimeoutNs);
 }
 
@@ -407,7 +503,7 @@ int cr_query_launch_shape(int device, CrLaunchShape* out) {
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return -1;
     int b1 = 0, b2 = 0, b3 = 0, bv = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_stage1<S1_WARPS>, S1_WARPS * 32, 0) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_stage1<S1_WARPS, false>, S1_WARPS * 32, 0) != cudaSuccess)
         return -1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bv, k_vertex<VX_THREADS>, VX_THREADS, 0) != cudaSuccess)
         return -1;
@@ -453,7 +549,10 @@ int cr_launch_stage1(const CrFrameParams& p, const CrLaunchShape& s, void* strea
     uint64_t warps = p.numItems;
     uint64_t blocks = (warps + S1_WARPS - 1) / S1_WARPS;
     if (blocks > (uint64_t)s.stage1Blocks) blocks = (uint64_t)s.stage1Blocks;
-    k_stage1<S1_WARPS><<<(unsigned)blocks, S1_WARPS * 32, 0, (cudaStream_t)stream>>>(p);
+    if (p.cellMode == CR_REC_BOXES)
+        k_stage1<S1_WARPS, true><<<(unsigned)blocks, S1_WARPS * 32, 0, (cudaStream_t)stream>>>(p);
+    else
+        k_stage1<S1_WARPS, false><<<(unsigned)blocks, S1_WARPS * 32, 0, (cudaStream_t)stream>>>(p);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

@@ -418,6 +418,119 @@ __device__ __forceinline__ uint32_t classify_box(const Mat& M, float fa, float f
                           make_float4(M.c0.z, M.c1.z, M.c2.z, M.c3.z), fa, f, lo, hi);
 }
 
+// Corner c (bit j: hi on axis j) of an affine form: base + the steps of set bits.
+__device__ __forceinline__ double corner_of(double base, const double st[3], int c) {
+    double q = base;
+    if (c & 1) q += st[0];
+    if (c & 2) q += st[1];
+    if (c & 4) q += st[2];
+    return q;
+}
+
+// One screen axis of box_misses_samples: true if every vertex of the box has
+// a float screen coordinate strictly inside (k, k + 1) for one integer k >= 0.
+// The corner numerators are F (bn + st_n) (F = fa, or f) and the depths
+// -(bz + st_z), summed in double; SX = |F| S_x (or S_y) and SZ = S_z scale the
+// rounding: EX = 2^-19 SX and ED bound the float evaluation error of X and d
+// at any vertex of the box; Dmin > 4 ED is the smallest depth.
+//
+// The exact coordinate s(p) = W ((X / D) / 2 + 1/2) - 1/2 is an increasing
+// function of X / D, a linear-fractional function with D > 0 on the box, so
+// its extremes over the box are at corners.  Stage 1 evaluates it as
+// fl(fl(fl(fl(X^ / d^) * 0.5 + 0.5) * W) - 0.5); with |X / D| <= R its error is
+// below Es = W/2 En + 3 2^-24 W (R/2 + 1/2) + 2^-25, En = (EX + R ED) /
+// (Dmin - ED) + 2^-24 (R + En); invD >= 1 / (Dmin - ED).  Each corner is checked against the bounds
+// k + Es, k + 1 - Es by cross-multiplication (D > 0), with a tolerance above
+// the double rounding of the corner sums and of the check.  k >= 0: for
+// k = -1 the bounding box's clamp to 0 makes floor(min_x) = 0 and the cull
+// fails; for k >= W - 1 the clamp of max_x to W - 1 keeps max_x < k + 1 and
+// the cull holds.
+__device__ __forceinline__ bool axis_misses_samples(double F, double bn, const double stn[3], double bz,
+                                                    const double stz[3], double invD, double ED, double SX, double SZ,
+                                                    double Wd, double invW) {
+    const double EX = SX * 1.9073486328125e-06;  // 2^-19
+    // k from corner 0 (any estimate will do: the corner checks prove the rest)
+    const float s0 = (float)Wd * ((float)(F * bn) * __frcp_rn((float)-bz) * 0.5f + 0.5f) - 0.5f;
+    if (!(s0 >= 0.0f && s0 < 1e9f)) return false;  // also NaN
+    const double k = (double)floorf(s0);
+    // |X / D| <= R on the interval the checks below allow; invW is within
+    // 2^-52 of 1 / W, far inside the slack of Es
+    const double R = fmax(fabs(2.0 * ((k + 0.5) * invW) - 1.0), fabs(2.0 * ((k + 1.5) * invW) - 1.0));
+    const double En = (EX + R * ED) * invD + 1.1920928955078125e-07 * (R + 1.0);                  // 2^-23
+    const double Es = 0.5 * Wd * En + 2.384185791015625e-07 * (Wd * (0.5 * R + 0.5) + 1.0) + 1e-6;  // 2^-22
+    if (!(Es < 0.25)) return false;
+    const double alo = 2.0 * ((k + Es + 0.5) * invW) - 1.0;
+    const double ahi = 2.0 * ((k + 1.0 - Es + 0.5) * invW) - 1.0;
+    const double tol0 = SX + R * SZ;
+#pragma unroll 1
+    for (int c = 0; c < 8; ++c) {
+        const double X = F * corner_of(bn, stn, c);
+        const double D = -corner_of(bz, stz, c);
+        const double tol = 2.842170943040401e-14 * ((fabs(X) + R * D) + tol0);  // 2^-45
+        if (!(X - alo * D > tol && ahi * D - X > tol)) return false;
+    }
+    return true;
+}
+
+// True if every vertex p in the object-space box [lo, hi] is, in stage 1's
+// float arithmetic (xform, viewToNDC, ndcToScreen, -0.5: tv.cu:103-134), in
+// front of the camera (depth > 0) and strictly inside one pixel column or one
+// pixel row of samples.  Then every triangle whose vertices lie in the box has
+// isNontrivial false and meets the reference's sample-miss cull (tv.cu:153-158),
+// so it writes nothing.  The float transform of a vertex is within 3 2^-24 S
+// of the exact affine value (S = sum_j |M_j| max|p_j| + |M_3| per row; the
+// bound uses 2^-19 S, which also covers fl(fa q.x)).  Corner values are exact
+// products of floats summed in double.  Non-finite boxes prove nothing.
+// invW, invH: 1 / W and 1 / H in double (any rounding: they only place the
+// bounds the corners are checked against).
+__device__ bool box_misses_samples(const Mat& M, float fa, float f, int W, int H, double invW, double invH,
+                                   const float lo[3], const float hi[3]) {
+    const double E19 = 1.9073486328125e-06;  // 2^-19
+    const double ax[3] = {M.c0.x, M.c1.x, M.c2.x}, ay[3] = {M.c0.y, M.c1.y, M.c2.y};
+    const double az[3] = {M.c0.z, M.c1.z, M.c2.z};
+    double mabs[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) mabs[j] = fmax(fabs((double)lo[j]), fabs((double)hi[j]));
+    const double Sz = (fabs(az[0]) * mabs[0] + fabs(az[1]) * mabs[1]) + (fabs(az[2]) * mabs[2] + fabs((double)M.c3.z));
+    if (!(Sz < 1e30)) return false;
+    double bz = M.c3.z, stz[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        bz += az[j] * (double)lo[j];
+        stz[j] = az[j] * (double)hi[j] - az[j] * (double)lo[j];
+    }
+    double Dmin = 1e300;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) Dmin = fmin(Dmin, -corner_of(bz, stz, c));
+    const double ED = E19 * Sz + 1e-30;
+    if (!(Dmin > 4.0 * ED && Dmin < 1e30)) return false;  // every vertex in front, with room
+    // an upper bound of 1 / (Dmin - ED): the float reciprocal of the rounded
+    // value is within 2^-22.9 of it; (1 + 2^-20) covers that
+    const double invD = (double)__frcp_rn((float)(Dmin - ED)) * 1.00000095367431640625;
+    {
+        const double Sx =
+            (fabs(ax[0]) * mabs[0] + fabs(ax[1]) * mabs[1]) + (fabs(ax[2]) * mabs[2] + fabs((double)M.c3.x));
+        double bx = M.c3.x, stx[3];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            bx += ax[j] * (double)lo[j];
+            stx[j] = ax[j] * (double)hi[j] - ax[j] * (double)lo[j];
+        }
+        if (Sx < 1e30 &&
+            axis_misses_samples(fa, bx, stx, bz, stz, invD, ED, fabs((double)fa) * Sx, Sz, (double)W, invW))
+            return true;
+    }
+    const double Sy = (fabs(ay[0]) * mabs[0] + fabs(ay[1]) * mabs[1]) + (fabs(ay[2]) * mabs[2] + fabs((double)M.c3.y));
+    double by = M.c3.y, sty[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        by += ay[j] * (double)lo[j];
+        sty[j] = ay[j] * (double)hi[j] - ay[j] * (double)lo[j];
+    }
+    return Sy < 1e30 &&
+           axis_misses_samples(f, by, sty, bz, stz, invD, ED, fabs((double)f) * Sy, Sz, (double)H, invH);
+}
+
 // Cell record of one vertex: the outcode plus stage 1's own screen position
 // (viewToNDC, ndcToScreen, -0.5: tv.cu:106-108,121-134, same operations in
 // the same order) reduced to its pixel cell.
@@ -437,6 +550,42 @@ __device__ __forceinline__ uint64_t vertex_cell_record(const Mat& M, V3 p, float
                ((uint64_t)(uint32_t)(int)fx << 16) | ((uint64_t)(uint32_t)(int)fy << 32);
     }
     return rec;
+}
+
+// vertex_cell_record for a vertex known to be in front of the camera and
+// inside every frustum side (its instance's mesh box classified inside): the
+// outcode is 0, so only the cell is formed (same operations, same values).
+__device__ __forceinline__ uint64_t vertex_cell_record_inside(const Mat& M, V3 p, float fa, float f, float Wf,
+                                                              float Hf, int W, int H) {
+    const V3 q = xform(M, p);
+    const float d = -q.z;
+    const float X = fa * q.x, Y = f * q.y;
+    const V2 s = to_screen(V3{X / d, Y / d, d}, Wf, Hf);
+    const float sx = s.x - 0.5f, sy = s.y - 0.5f;
+    uint64_t rec = 0;
+    if (sx >= 0.0f && sx <= (float)(W - 1) && sy >= 0.0f && sy <= (float)(H - 1)) {
+        const float fx = floorf(sx), fy = floorf(sy);
+        rec = CR_CELL_INSIDE | (sx > fx ? CR_CELL_FRACX : 0ull) | (sy > fy ? CR_CELL_FRACY : 0ull) |
+              ((uint64_t)(uint32_t)(int)fx << 16) | ((uint64_t)(uint32_t)(int)fy << 32);
+    }
+    return rec;
+}
+
+// Stage 1's culls decided from three cell records: all behind (tv.cu:119),
+// all beyond one side with none behind (tv.cu:110-118), or -- with every
+// vertex on screen, so the bounding box's clamps change nothing -- all three
+// x (or y) strictly inside one pixel cell, the sample miss (tv.cu:153-158).
+__device__ __forceinline__ bool cell_culled(uint64_t o0, uint64_t o1, uint64_t o2) {
+    const uint64_t all = o0 & o1 & o2;
+    const uint64_t any = o0 | o1 | o2;
+    if ((all & CR_OC_BEHIND) || (!(any & CR_OC_BEHIND) && (all & CR_OC_SIDES))) return true;
+    if (!(any & CR_OC_BEHIND) && (all & CR_CELL_INSIDE)) {
+        const uint64_t diff = (o0 ^ o1) | (o0 ^ o2);
+        const bool missX = (all & CR_CELL_FRACX) && !(diff & 0x00000000ffff0000ull);
+        const bool missY = (all & CR_CELL_FRACY) && !(diff & 0x0000ffff00000000ull);
+        return missX || missY;
+    }
+    return false;
 }
 
 struct Item {

@@ -64,6 +64,7 @@ class CrConfig(ctypes.Structure):
 CR_CULL_AUTO = 0
 CR_CULL_OUTCODES = 1
 CR_CULL_CELLS = 2
+CR_CULL_BOXES = 3
 
 
 CR_DEBUG_DROP_FIRST_TILE_COPY = 1

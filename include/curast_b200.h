@@ -76,15 +76,22 @@ typedef struct cr_config {
     uint32_t reserved[4];
 } cr_config;
 
-/* Per-vertex records written before stage 1.  Both give bit-identical
- * output; they differ in what stage 1 can cull without fetching positions:
- * OUTCODES (1 byte: behind / beyond a frustum side) suits scenes whose
- * triangles are mostly off-screen, CELLS (8 bytes: also the exact pixel cell)
- * additionally culls sub-pixel triangles that miss every sample.  AUTO picks
- * CELLS for frames with more than one instance. */
+/* What stage 1 culls from.  All give bit-identical output; they differ in
+ * what stage 1 can cull without fetching positions.  OUTCODES and CELLS are
+ * per-(instance, vertex) records written before stage 1: OUTCODES (1 byte:
+ * behind / beyond a frustum side) suits scenes whose triangles are mostly
+ * off-screen, CELLS (8 bytes: also the exact pixel cell) additionally culls
+ * sub-pixel triangles that miss every sample.  BOXES writes no records to
+ * device memory: per instance it proves from the mesh's precomputed boxes
+ * that whole 128-triangle groups miss every sample, and culls the rest from
+ * cell records of each group's distinct vertices kept in shared memory
+ * (per-group vertex lists, built on first use) -- suited to many instances that are small on screen.  AUTO picks
+ * BOXES for frames that draw some mesh more than once, CELLS for other frames
+ * with more than one instance, else OUTCODES. */
 #define CR_CULL_AUTO 0u
 #define CR_CULL_OUTCODES 1u
 #define CR_CULL_CELLS 2u
+#define CR_CULL_BOXES 3u
 
 /* Failure-detection test hook: stage 1 never issues its first index-tile
  * copy, so the bounded wait for it runs out; the frame then reports

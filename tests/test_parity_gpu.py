@@ -210,11 +210,12 @@ def test_instanced_field(ctx):
     assert_same_vis(vis, rvis, "ours vs reference (instanced stage 1)")
 
 
-@pytest.mark.parametrize("records", [pc.CR_CULL_OUTCODES, pc.CR_CULL_CELLS])
+@pytest.mark.parametrize("records", [pc.CR_CULL_OUTCODES, pc.CR_CULL_CELLS, pc.CR_CULL_BOXES])
 def test_cull_records_do_not_change_output(gpu, records):
-    """Both kinds of per-vertex records (outcode bytes, cell records that
-    also decide the sample-miss cull) give the oracle's visbuffer, on a
-    sub-pixel-heavy instanced scene and on a planet."""
+    """Every cull source (outcode bytes, cell records that also decide the
+    sample-miss cull, box proofs of the sample-miss cull without records)
+    gives the oracle's visbuffer, on a sub-pixel-heavy instanced scene and on
+    a planet."""
     torch = _torch()
     with pc.Context(cull_records=records) as c:
         pos, idx, col = scenes.asteroid(20_000, device="cuda")
@@ -233,6 +234,64 @@ def test_cull_records_do_not_change_output(gpu, records):
         vis = render_ours(c, None, [(0, scenes.identity())], view, proj, W, H, handles=[h])[0]
         m = (pos.cpu().numpy(), idx.cpu().numpy().view(np.uint32), col.cpu().numpy().view(np.uint32))
         assert_same_vis(vis, render_oracle([m], [(0, scenes.identity())], view, proj, W, H)[0], "planet")
+
+
+def test_boxes_camera_inside_instance_field(gpu):
+    """Box-culled frames (CR_CULL_BOXES) with the camera inside the instance
+    field: instances behind the camera, across the near plane and frustum
+    sides, large on screen (stages 2 and 3) and far and sub-pixel, so both the
+    frame cull's classes and the shared-memory cell records with outcodes are
+    exercised, against the oracle."""
+    pos, idx, col = scenes.asteroid(20_000, device="cuda")
+    worlds = scenes.instanced_field(400, seed=5, box=30.0)
+    W, H = 480, 320
+    view = scenes.look_at((15.0, 15.0, 15.0), (25.0, 12.0, 3.0))
+    proj = scenes.perspective(70.0, W / H)
+    m = (pos.cpu().numpy(), idx.cpu().numpy().view(np.uint32), col.cpu().numpy().view(np.uint32))
+    inst = [(0, w) for w in worlds]
+    with pc.Context(cull_records=pc.CR_CULL_BOXES) as c:
+        h = c.mesh_from_device(pos.data_ptr(), pos.shape[0], idx.data_ptr(), idx.shape[0], col.data_ptr())
+        vis, rgba, _, stats = render_ours(c, None, inst, view, proj, W, H, handles=[h])
+    ovis, orgba, _, ost = render_oracle([m], inst, view, proj, W, H)
+    assert ost.nontrivial > 0 and (ovis != CLEAR).mean() > 0.05
+    assert_same_vis(vis, ovis, "camera inside the field")
+    assert channel_diff(rgba, orgba) <= COLOR_TOL
+
+
+def test_box_proofs_at_pixel_edges(gpu):
+    """Clusters of tiny triangles placed a hair inside, on and across pixel
+    sample lines (offsets from 1e-6 to 0.3 pixel, both signs), many instances
+    of one mesh: the box proofs of the sample-miss cull (CR_CULL_BOXES) must
+    keep every triangle the oracle draws."""
+    rng = np.random.default_rng(321)
+    W, H = 640, 480
+    depth = 6.0
+    proj = scenes.perspective(60.0, W / H)
+    f = float(proj[5])
+    fa = np.float32(f) / np.float32(W / H)
+    px = 2.0 * depth / (f * H)  # object units per pixel at this depth
+    # one mesh: 2048 triangles in a ball of radius 0.02 pixel
+    n = 2048
+    c = rng.normal(size=(n, 1, 3)) * (0.01 * px)
+    tri = (c + rng.normal(size=(n, 3, 3)) * (0.004 * px)).astype(np.float32)
+    pos = tri.reshape(-1, 3)
+    idx = np.arange(pos.shape[0], dtype=np.uint32).reshape(-1, 3)
+    col = rng.integers(0, 2**32, pos.shape[0], dtype=np.uint64).astype(np.uint32)
+    offs = np.array([1e-6, 1e-5, 1e-4, 1e-3, 0.01, 0.02, 0.05, 0.3])
+    inst = []
+    for k in range(600):
+        sx = rng.integers(8, W - 8) + rng.choice(offs) * rng.choice([-1.0, 1.0])
+        sy = rng.integers(8, H - 8) + rng.choice(offs) * rng.choice([-1.0, 1.0])
+        # invert the screen mapping of stage 1 (sample k at screen x = k + 0.5)
+        d = depth * (1.0 + 0.01 * rng.uniform())
+        x = (2.0 * (sx + 0.5) / W - 1.0) * d / float(fa)
+        y = (2.0 * (sy + 0.5) / H - 1.0) * d / f
+        inst.append((0, scenes.translate_scale(x, y, -d)))
+    with pc.Context(cull_records=pc.CR_CULL_BOXES) as cx:
+        vis, _, _, _ = render_ours(cx, [(pos, idx, col)], inst, scenes.identity(), proj, W, H)
+    ovis = render_oracle([(pos, idx, col)], inst, scenes.identity(), proj, W, H)[0]
+    assert (ovis != CLEAR).sum() > 100
+    assert_same_vis(vis, ovis, "box proofs at pixel edges")
 
 
 def test_stage2_span_narrowing_on_slivers(ctx):
