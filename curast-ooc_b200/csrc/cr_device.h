@@ -21,11 +21,12 @@
 // distinct vertices its triangles reference (at most CR_LOCAL_MAX) and each
 // triangle's three positions in that list, in one CR_LOCAL_BYTES block:
 //   uint32_t vertex[CR_LOCAL_MAX]    bytes    0 .. 1023
-//   uint8_t  corner[3 * CR_BATCH]    bytes 1024 .. 1407
+//   uint32_t corners[CR_BATCH]       bytes 1024 .. 1535, list positions of
+//                                    corners 0, 1, 2 in bytes 0, 1, 2
 // and, per item, the number of distinct vertices (CR_LOCAL_NONE: more than
 // CR_LOCAL_MAX, or a non-indexed mesh; the item is drawn without a list).
 #define CR_LOCAL_MAX 256
-#define CR_LOCAL_BYTES 1408
+#define CR_LOCAL_BYTES 1536
 #define CR_LOCAL_NONE 0xffffffffu
 
 // counters[] slots

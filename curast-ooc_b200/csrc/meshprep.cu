@@ -209,19 +209,20 @@ __global__ void __launch_bounds__(LL_WARPS * 32) k_local_lists(const uint32_t* i
         uint8_t* L = lists + (uint64_t)b * CR_LOCAL_BYTES;
         uint32_t* vl = reinterpret_cast<uint32_t*>(L);
         for (int i = lane; i < CR_LOCAL_MAX; i += 32) vl[i] = i < total ? uni[i] : 0u;
-        for (int i = lane; i < 3 * CR_BATCH; i += 32) {
-            uint8_t loc = 0;
-            if (i < 3 * (int)nt) {
-                const uint32_t v = __ldg(idx + 3ull * t0 + i);
+        uint32_t* corners = reinterpret_cast<uint32_t*>(L + 1024);
+        for (int t = lane; t < CR_BATCH; t += 32) {
+            uint32_t word = 0;
+            for (int c = 0; c < 3 && t < (int)nt; ++c) {
+                const uint32_t v = __ldg(idx + 3ull * (t0 + t) + c);
                 int lo = 0, hi = total - 1;  // uni[lo] == v
                 while (lo < hi) {
                     const int mid = (lo + hi) >> 1;
                     if (uni[mid] < v) lo = mid + 1;
                     else hi = mid;
                 }
-                loc = (uint8_t)lo;
+                word |= (uint32_t)lo << (8 * c);
             }
-            L[1024 + i] = loc;
+            corners[t] = word;
         }
         __syncwarp();
     }

@@ -235,8 +235,8 @@ struct TileSrc {
 };
 
 template <bool BOXES>
-__device__ __forceinline__ TileSrc tile_source(const CrSegment* sg, uint32_t batch) {
-    if (BOXES) {
+__device__ __forceinline__ TileSrc tile_source(const CrSegment* sg, uint32_t batch, bool allowLocal) {
+    if (BOXES && allowLocal) {
         const uint32_t* lc = ldg_ptr(&sg->localCounts);
         if (lc && __ldg(lc + batch) <= CR_LOCAL_MAX)
             return TileSrc{ldg_ptr(&sg->localLists) + (uint64_t)batch * CR_LOCAL_BYTES, CR_LOCAL_BYTES, true};
@@ -261,18 +261,23 @@ __device__ __forceinline__ TileSrc tile_source(const CrSegment* sg, uint32_t bat
 //   BOXES, no list         sub-box proofs of the sample-miss cull, one per
 //                          (instance, 16 triangles), spread over the lanes
 // Nontrivial triangles are appended with one atomic per warp (ballot / popc).
+#ifndef CR_S1_BOXES_MIN_BLOCKS
+#define CR_S1_BOXES_MIN_BLOCKS 3
+#endif
 template <int WARPS, bool BOXES>
-__global__ void __launch_bounds__(WARPS * 32, 3) k_stage1(const CrFrameParams p) {
+__global__ void __launch_bounds__(WARPS * 32, BOXES ? CR_S1_BOXES_MIN_BLOCKS : 3) k_stage1(const CrFrameParams p) {
     constexpr int STAGES = BOXES ? 2 : S1_STAGES;
     static_assert(CR_LOCAL_BYTES <= CR_BATCH * 12, "a vertex-list block fits a ring slot");
     __shared__ __align__(128) uint32_t s_idx[WARPS][STAGES][CR_BATCH * 3];
     __shared__ __align__(8) uint64_t s_bar[WARPS][STAGES];
-    __shared__ uint8_t s_surv[WARPS][CR_BATCH];
-    __shared__ __align__(16) uint64_t s_rec[BOXES ? WARPS : 1][BOXES ? CR_LOCAL_MAX : 1];
+    __shared__ uint16_t s_ring[WARPS][S1_RING];
+    __shared__ __align__(16) uint32_t s_rec[BOXES ? WARPS : 1][BOXES ? CR_LOCAL_MAX : 1];
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
     const uint64_t gw = (uint64_t)blockIdx.x * WARPS + w;
     const uint64_t nw = (uint64_t)gridDim.x * WARPS;
+    // shared-memory cell records hold 12-bit pixel cells
+    const bool lists = BOXES && p.W <= 4096 && p.H <= 4096;
 
     if (lane == 0) {
         for (int s = 0; s < STAGES; ++s) mbar_init(&s_bar[w][s], 1);
@@ -290,7 +295,7 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_stage1(const CrFrameParams p)
         const uint64_t pk = gw + (uint64_t)s * nw;
         if (pk >= nItems) break;
         const Item it = decode_item(p, item_at(pk));
-        const TileSrc ts = tile_source<BOXES>(p.segments + it.seg, it.batch);
+        const TileSrc ts = tile_source<BOXES>(p.segments + it.seg, it.batch, lists);
         if (ts.src) {
             pending |= 1u << s;
             // failure-detection test hook: the first copy is never issued, so
@@ -303,6 +308,7 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_stage1(const CrFrameParams p)
 
     const float fa = p.f / p.aspect;
     const float Wf = (float)p.W, Hf = (float)p.H;
+    const float Wm1 = (float)(p.W - 1), Hm1 = (float)(p.H - 1);
     uint32_t parity = 0;
     uint32_t k = 0;
     for (uint64_t pk = gw; pk < nItems; pk += nw, ++k) {
@@ -314,7 +320,7 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_stage1(const CrFrameParams p)
         const CrSegment* sg = p.segments + it.seg;
         const uint32_t numTri = __ldg(&sg->numTriangles);
         const uint32_t* gix = ldg_ptr(&sg->indices);
-        const TileSrc ts = tile_source<BOXES>(sg, it.batch);
+        const TileSrc ts = tile_source<BOXES>(sg, it.batch, lists);
         const bool tma = ts.src != nullptr;
         const bool local = BOXES && ts.local;
         const uint32_t tri0 = it.batch * CR_BATCH;
@@ -329,10 +335,9 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_stage1(const CrFrameParams p)
             pending &= ~bit;
         }
         const uint32_t* tile = s_idx[w][slot];
-        const uint8_t* corner = reinterpret_cast<const uint8_t*>(tile) + 1024;  // vertex-list blocks
         // vertex index of corner c of the triangle at tile position pos
         auto index_of = [&](uint32_t pos, int c) -> uint32_t {
-            if (local) return tile[corner[3 * pos + c]];
+            if (local) return tile[(tile[CR_LOCAL_MAX + pos] >> (8 * c)) & 0xffu];
             if (tma) return tile[3 * pos + c];
             const uint32_t t = tri0 + pos;
             return gix ? __ldg(gix + 3ull * t + c) : 3 * t + c;
@@ -384,63 +389,35 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_stage1(const CrFrameParams p)
         static_assert(CR_BATCH / CR_SUB == 8 && CR_INST_CHUNK <= 16, "8 sub-boxes x 16 instances in 4 ballots");
         const uint32_t nLocal = local ? __ldg(ldg_ptr(&sg->localCounts) + it.batch) : 0u;
         const float* pos = ldg_ptr(&sg->positions);
-        int rank = 0;
-        for (uint32_t inst = ib; inst < ie; ++inst) {
-            if (!((alive >> (inst - ib)) & 1u)) continue;  // its box proved every triangle culled
-            const int kk = rank++;
-            const Mat M = load_mat(p.world_view + 4ull * inst);
-            bool culledR[S1_R];
-            if constexpr (!BOXES) {
-                gather_culls(p, inst, ix, act, culledR);
-            } else if (local) {
-                // cell records of the item's distinct vertices for this
-                // instance; an instance whose mesh box is inside the frustum
-                // has the outcode 0 at every vertex
-                const bool inside = (__ldg(&p.instances[inst].meshClass) & CR_MESH_INSIDE) != 0u;
-                uint64_t* rec = s_rec[w];
-                for (uint32_t v = lane; v < nLocal; v += 32)
-                    rec[v] = inside ? vertex_cell_record_inside(M, load_pos(pos, tile[v]), fa, p.f, Wf, Hf, p.W, p.H)
-                                    : vertex_cell_record(M, load_pos(pos, tile[v]), fa, p.f, Wf, Hf, p.W, p.H);
-                __syncwarp();
-#pragma unroll
-                for (int r = 0; r < S1_R; ++r) {
-                    const uint32_t tp = r * 32 + lane;
-                    const uint64_t o0 = act[r] ? rec[corner[3 * tp + 0]] : 0ull;
-                    const uint64_t o1 = act[r] ? rec[corner[3 * tp + 1]] : 0ull;
-                    const uint64_t o2 = act[r] ? rec[corner[3 * tp + 2]] : 0ull;
-                    culledR[r] = cell_culled(o0, o1, o2);
-                }
-            } else {
-                const uint32_t w4 = (kk >> 2) == 0 ? subw[0] : (kk >> 2) == 1 ? subw[1] : (kk >> 2) == 2 ? subw[2] : subw[3];
-                const uint32_t sm = (w4 >> (8 * (kk & 3))) & 0xffu;
-#pragma unroll
-                for (int r = 0; r < S1_R; ++r) culledR[r] = !((sm >> (2 * r + (lane >> 4))) & 1u);
-            }
-            // culled from the records or proofs alone: pack the others
-            int nsurv = 0;
-#pragma unroll
-            for (int r = 0; r < S1_R; ++r) {
-                const bool culled = culledR[r];
-                const unsigned m = __ballot_sync(FULL, act[r] && !culled);
-                if (act[r] && !culled) s_surv[w][nsurv + __popc(m & ((1u << lane) - 1u))] = (uint8_t)(r * 32 + lane);
-                nsurv += __popc(m);
-            }
-            __syncwarp();
-            if (nsurv == 0) continue;
-            const uint32_t flip = __ldg(&p.instances[inst].flip);
-            const uint64_t cum = __ldg(&p.instances[inst].cum);
-            for (int base = 0; base < nsurv; base += 32) {
-                const int j = base + lane;
+        // Triangles no record or proof culls, queued across the item's
+        // instances as (instance slot << 8 | tile position) in a per-warp ring
+        // and run through the reference's full path 32 at a time.
+        uint16_t* ring = s_ring[w];
+        uint32_t qh = 0, qt = 0;  // ring head / tail (warp-uniform)
+        // evaluates queued triangles 32 at a time (all: down to an empty
+        // ring); in record-culled frames the ring holds one instance's
+        // triangles, whose matrix, flip and first id the warp passes in
+        auto drain = [&](bool all, const Mat* Mu, uint32_t flipu, uint64_t cumu) {
+            while (qt - qh >= 32u || (all && qt > qh)) {
+                const uint32_t j = qh + lane;
                 int res = S1_CULL;
-                uint32_t tri = 0;
-                if (j < nsurv) {
-                    const uint32_t tp = s_surv[w][j];
+                uint32_t tri = 0, inst = 0;
+                if (j < qt) {
+                    const uint32_t e = ring[j & (S1_RING - 1)];
+                    const uint32_t tp = e & 0xffu;
+                    inst = ib + (e >> 8);
                     tri = tri0 + tp;
                     const V3 pa = load_pos(pos, index_of(tp, 0));
                     const V3 pb = load_pos(pos, index_of(tp, 1));
                     const V3 pc = load_pos(pos, index_of(tp, 2));
-                    res = stage1_triangle(target_of(p), fa, M, flip, pa, pb, pc, cum + tri);
+                    if (!BOXES)
+                        res = stage1_triangle(target_of(p), fa, *Mu, flipu, pa, pb, pc, cumu + tri);
+                    else
+                        res = stage1_triangle(target_of(p), fa, load_mat(p.world_view + 4ull * inst),
+                                              __ldg(&p.instances[inst].flip), pa, pb, pc,
+                                              __ldg(&p.instances[inst].cum) + tri);
                 }
+                qh = min(qh + 32u, qt);
                 const unsigned qmask = __ballot_sync(FULL, res == S1_QUEUE);
                 if (qmask) {  // warp-aggregated append, tv.cu:190-197
                     const int leader = __ffs(qmask) - 1;
@@ -453,16 +430,75 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_stage1(const CrFrameParams p)
                         else atomicOr(&p.counters[CR_CTR_OVERFLOW], 1ull);
                     }
                 }
+                __syncwarp();
+            }
+        };
+        int rank = 0;
+        for (uint32_t inst = ib; inst < ie; ++inst) {
+            if (!((alive >> (inst - ib)) & 1u)) continue;  // its box proved every triangle culled
+            const int kk = rank++;
+            bool culledR[S1_R];
+            if constexpr (!BOXES) {
+                gather_culls(p, inst, ix, act, culledR);
+            } else if (local) {
+                // cell records of the item's distinct vertices for this
+                // instance; an instance whose mesh box is inside the frustum
+                // has the outcode 0 at every vertex
+                const Mat M = load_mat(p.world_view + 4ull * inst);
+                const bool inside = (__ldg(&p.instances[inst].meshClass) & CR_MESH_INSIDE) != 0u;
+                uint32_t* rec = s_rec[w];
+                if (inside) {
+                    for (uint32_t v = lane; v < nLocal; v += 64) {
+                        const uint32_t v2 = v + 32;
+                        const uint32_t r0 = vertex_cell32<false>(M, load_pos(pos, tile[v]), fa, p.f, Wf, Hf, Wm1, Hm1);
+                        const uint32_t r1 = v2 < nLocal ? vertex_cell32<false>(M, load_pos(pos, tile[v2]), fa, p.f, Wf,
+                                                                               Hf, Wm1, Hm1)
+                                                        : 0u;
+                        rec[v] = r0;
+                        if (v2 < nLocal) rec[v2] = r1;
+                    }
+                } else {
+                    for (uint32_t v = lane; v < nLocal; v += 32)
+                        rec[v] = vertex_cell32<true>(M, load_pos(pos, tile[v]), fa, p.f, Wf, Hf, Wm1, Hm1);
+                }
+                __syncwarp();
+                const uint32_t* cw = tile + CR_LOCAL_MAX;  // corner words
+#pragma unroll
+                for (int r = 0; r < S1_R; ++r) {
+                    const uint32_t c = cw[r * 32 + lane];
+                    culledR[r] = !act[r] || cell32_culled(rec[c & 0xffu], rec[(c >> 8) & 0xffu], rec[(c >> 16) & 0xffu]);
+                }
+            } else {
+                const uint32_t w4 = (kk >> 2) == 0 ? subw[0] : (kk >> 2) == 1 ? subw[1] : (kk >> 2) == 2 ? subw[2] : subw[3];
+                const uint32_t sm = (w4 >> (8 * (kk & 3))) & 0xffu;
+#pragma unroll
+                for (int r = 0; r < S1_R; ++r) culledR[r] = !((sm >> (2 * r + (lane >> 4))) & 1u);
+            }
+            // queue the others
+#pragma unroll
+            for (int r = 0; r < S1_R; ++r) {
+                const bool keep = act[r] && !culledR[r];
+                const unsigned m = __ballot_sync(FULL, keep);
+                if (keep) ring[(qt + __popc(m & ((1u << lane) - 1u))) & (S1_RING - 1)] =
+                    (uint16_t)(((inst - ib) << 8) | (uint32_t)(r * 32 + lane));
+                qt += __popc(m);
             }
             __syncwarp();
+            if constexpr (BOXES) {
+                drain(false, nullptr, 0u, 0ull);
+            } else {
+                if (qt == qh) continue;
+                const Mat M = load_mat(p.world_view + 4ull * inst);
+                drain(true, &M, __ldg(&p.instances[inst].flip), __ldg(&p.instances[inst].cum));
+            }
         }
-
+        if constexpr (BOXES) drain(true, nullptr, 0u, 0ull);
         __syncwarp();
         {  // every read of this slot is done: refill it with the item STAGES ahead
             const uint64_t npk = pk + (uint64_t)STAGES * nw;
             if (npk < nItems) {
                 const Item nt = decode_item(p, item_at(npk));
-                const TileSrc ns = tile_source<BOXES>(p.segments + nt.seg, nt.batch);
+                const TileSrc ns = tile_source<BOXES>(p.segments + nt.seg, nt.batch, lists);
                 if (ns.src) {
                     pending |= bit;
                     if (lane == 0) {

@@ -552,23 +552,46 @@ __device__ __forceinline__ uint64_t vertex_cell_record(const Mat& M, V3 p, float
     return rec;
 }
 
-// vertex_cell_record for a vertex known to be in front of the camera and
-// inside every frustum side (its instance's mesh box classified inside): the
-// outcode is 0, so only the cell is formed (same operations, same values).
-__device__ __forceinline__ uint64_t vertex_cell_record_inside(const Mat& M, V3 p, float fa, float f, float Wf,
-                                                              float Hf, int W, int H) {
+// 32-bit cell record (shared-memory records of box-culled frames, W and H at
+// most 4096): bits 0..4 the outcode, bit 5 on screen, bit 6 x not an
+// integer, bit 7 y not an integer, bits 8..19 floor(x), bits 20..31 floor(y).
+// `sides`: false when the vertex is known to be in front of the camera and
+// inside every frustum side (outcode 0, no predicates evaluated).
+#define CR_C32_INSIDE 0x20u
+#define CR_C32_FRACX 0x40u
+#define CR_C32_FRACY 0x80u
+template <bool SIDES>
+__device__ __forceinline__ uint32_t vertex_cell32(const Mat& M, V3 p, float fa, float f, float Wf, float Hf,
+                                                  float Wm1, float Hm1) {
     const V3 q = xform(M, p);
     const float d = -q.z;
+    uint32_t rec = 0;
     const float X = fa * q.x, Y = f * q.y;
+    if (SIDES) {
+        if (d <= 0.0f) return CR_OC_BEHIND;
+        rec = (ndc_beyond(X, d) ? CR_OC_RIGHT : 0u) | (ndc_beyond(-X, d) ? CR_OC_LEFT : 0u) |
+              (ndc_beyond(Y, d) ? CR_OC_TOP : 0u) | (ndc_beyond(-Y, d) ? CR_OC_BOTTOM : 0u);
+    }
     const V2 s = to_screen(V3{X / d, Y / d, d}, Wf, Hf);
     const float sx = s.x - 0.5f, sy = s.y - 0.5f;
-    uint64_t rec = 0;
-    if (sx >= 0.0f && sx <= (float)(W - 1) && sy >= 0.0f && sy <= (float)(H - 1)) {
+    if (sx >= 0.0f && sx <= Wm1 && sy >= 0.0f && sy <= Hm1) {
         const float fx = floorf(sx), fy = floorf(sy);
-        rec = CR_CELL_INSIDE | (sx > fx ? CR_CELL_FRACX : 0ull) | (sy > fy ? CR_CELL_FRACY : 0ull) |
-              ((uint64_t)(uint32_t)(int)fx << 16) | ((uint64_t)(uint32_t)(int)fy << 32);
+        rec |= CR_C32_INSIDE | (sx > fx ? CR_C32_FRACX : 0u) | (sy > fy ? CR_C32_FRACY : 0u) |
+               ((uint32_t)(int)fx << 8) | ((uint32_t)(int)fy << 20);
     }
     return rec;
+}
+
+// cell_culled on 32-bit records.
+__device__ __forceinline__ bool cell32_culled(uint32_t o0, uint32_t o1, uint32_t o2) {
+    const uint32_t all = o0 & o1 & o2;
+    const uint32_t any = o0 | o1 | o2;
+    if ((all & CR_OC_BEHIND) || (!(any & CR_OC_BEHIND) && (all & CR_OC_SIDES))) return true;
+    if (!(any & CR_OC_BEHIND) && (all & CR_C32_INSIDE)) {
+        const uint32_t diff = (o0 ^ o1) | (o0 ^ o2);
+        return ((all & CR_C32_FRACX) && !(diff & 0x000fff00u)) || ((all & CR_C32_FRACY) && !(diff & 0xfff00000u));
+    }
+    return false;
 }
 
 // Stage 1's culls decided from three cell records: all behind (tv.cu:119),
@@ -626,6 +649,7 @@ __device__ __forceinline__ bool item_uses_tma(const CrSegment* sg, uint32_t batc
 
 constexpr int S1_STAGES = 3;
 constexpr int S1_R = CR_BATCH / 32;  // triangles per lane per work item
+constexpr int S1_RING = 256;         // stage-1 survivor ring entries per warp
 
 
 // ---------------------------------------------------------------------------
