@@ -45,6 +45,32 @@ TableLayout layout_of(size_t n, size_t m, size_t V) {
     return L;
 }
 
+// One device allocation per batched frame holds the vertex pass's records
+// and the frame cull's outputs.
+struct CullLayout {
+    size_t oChunkMasks, oUniform, oChunkList, oItems, total;
+};
+
+CullLayout cull_layout(const Assembled& A) {
+    CullLayout L;
+    L.oChunkMasks = align_up(A.outBytes * sizeof(CrViewMasks), 256);
+    L.oUniform = align_up(L.oChunkMasks + A.numVChunks * sizeof(CrViewMasks), 256);
+    L.oChunkList = align_up(L.oUniform + A.numVChunks, 256);
+    L.oItems = align_up(L.oChunkList + A.numVChunks * 4, 256);
+    L.total = align_up(L.oItems + A.numItems * sizeof(CrItemViews), 256) + 256;
+    return L;
+}
+
+void bind_cull(const Assembled& A, const CullLayout& L, void* base, CrFrameParams& fp) {
+    char* b = (char*)base;
+    fp.viewMasks = (CrViewMasks*)b;
+    fp.chunkMasks = (CrViewMasks*)(b + L.oChunkMasks);
+    fp.chunkUniform = (uint8_t*)(b + L.oUniform);
+    fp.chunkList = (uint32_t*)(b + L.oChunkList);
+    fp.itemViews = (CrItemViews*)(b + L.oItems);
+    fp.itemCap = A.numItems;
+}
+
 cr_status check_views(const cr_view* views, uint32_t nv, uint32_t flags) {
     if (!views || nv == 0) return fail(CR_ERR_INVALID, "batched render: no views");
     if (nv > CR_MAX_BATCH_VIEWS) return fail(CR_ERR_INVALID, "batched render: %u views (at most %u)", nv, CR_MAX_BATCH_VIEWS);
@@ -154,6 +180,8 @@ cr_status issue_batch(const CrFrameParams& fp, const CrResolveParams& rp, const 
         return fail(CR_ERR_CUDA, "batched clear launch: %s", cudaGetErrorString(cudaGetLastError()));
     }
     CR_CUDA(mark(1), "event");
+    if (count && cr_launch_cull_views(fp, sh, stream))
+        return fail(CR_ERR_CUDA, "batched frame-cull launch: %s", cudaGetErrorString(cudaGetLastError()));
     if (count && cr_launch_vertex_views(fp, sh, stream))
         return fail(CR_ERR_CUDA, "batched vertex-pass launch: %s", cudaGetErrorString(cudaGetLastError()));
     CR_CUDA(mark(2), "event");
@@ -213,7 +241,8 @@ cr_status render_batch(cr_context* ctx, const cr_instance* instances, uint32_t c
         if (s) return s;
     }
     CR_CUDA(cudaStreamWaitEvent(stream, ctx->frameDone, 0), "stream wait");
-    s = ensure_records(ctx, A.outBytes * sizeof(CrViewMasks));
+    const CullLayout CL = cull_layout(A);
+    s = ensure_records(ctx, CL.total);
     if (s) return s;
 
     // frame table through the context's pinned staging buffer
@@ -243,7 +272,7 @@ cr_status render_batch(cr_context* ctx, const cr_instance* instances, uint32_t c
     CrResolveParams rp{};
     bind_tables(A, B, L, (char*)ctx->dFrame, fp, rp);
     base_params(ctx, display, fp, rp);
-    fp.viewMasks = (CrViewMasks*)ctx->outcodes;
+    bind_cull(A, CL, ctx->outcodes, fp);
     fp.counters = ctx->counters;
     auto issue = [&](cudaEvent_t* tev, cudaEvent_t rasterEnd) -> cr_status {
         fp.ntList = ctx->ntList;
@@ -252,7 +281,7 @@ cr_status render_batch(cr_context* ctx, const cr_instance* instances, uint32_t c
         fp.hugeCap = ctx->hugeCap;
         return issue_batch(fp, rp, B, sh, count, flags, stream, tev, rasterEnd);
     };
-    return run_frame(ctx, flags, stream, count, A.totalTriangles * nv, issue);
+    return run_frame(ctx, flags, stream, count, A.totalTriangles * nv, issue, A.numItems, A.numVChunks);
 }
 
 }  // namespace
@@ -286,8 +315,9 @@ cr_status cr::scratch_issue(cr_context* ctx, BatchScratch& S, const cr_instance*
         cap = want;
         return CR_OK;
     };
+    const CullLayout CL = cull_layout(A);
     if ((s = grow(&S.dTable, S.dTableCap, L.total * 2, "slot table")) ||
-        (s = grow(&S.records, S.recordCap, align_up(A.outBytes * sizeof(CrViewMasks), 256) + 256, "slot records")))
+        (s = grow(&S.records, S.recordCap, CL.total, "slot records")))
         return s;
     if (L.total > S.hTableCap) {
         if (S.hTable) cudaFreeHost(S.hTable);
@@ -308,7 +338,7 @@ cr_status cr::scratch_issue(cr_context* ctx, BatchScratch& S, const cr_instance*
     CrResolveParams rp{};
     bind_tables(A, B, L, (char*)S.dTable, fp, rp);
     base_params(ctx, display, fp, rp);
-    fp.viewMasks = (CrViewMasks*)S.records;
+    bind_cull(A, CL, S.records, fp);
     fp.counters = S.counters;
     fp.ntList = S.ntList;
     fp.ntCap = S.ntCap;
@@ -457,7 +487,7 @@ cr_status cr_batch_plan_create(cr_context* ctx, const cr_instance* instances, ui
         huNeed = ctx->last.huge_tiles + ctx->last.huge_tiles / 2 + 65536;
     }
     p->L = layout_of(p->A.inst.size(), p->A.seg.size(), num_views);
-    p->recordBytes = align_up(p->A.outBytes * sizeof(CrViewMasks), 256) + 256;
+    p->recordBytes = cull_layout(p->A).total;
     if ((s = ctx->dev_alloc(&p->dTable, p->L.total, "plan table")) ||
         (s = ctx->dev_alloc(&p->records, p->recordBytes, "plan records"))) {
         plan_free(p);
@@ -492,7 +522,7 @@ cr_status cr_batch_plan_create(cr_context* ctx, const cr_instance* instances, ui
     CrResolveParams rp{};
     bind_tables(p->A, p->B, p->L, (char*)p->dTable, fp, rp);
     base_params(ctx, display, fp, rp);
-    fp.viewMasks = (CrViewMasks*)p->records;
+    bind_cull(p->A, cull_layout(p->A), p->records, fp);
     fp.counters = p->counters;
     fp.ntList = p->ntList;
     fp.ntCap = p->ntCap;

@@ -140,6 +140,18 @@ struct alignas(16) CrViewMasks {
 };
 static_assert(sizeof(CrViewMasks) == 48, "CrViewMasks layout");
 
+// Batched frame cull output: a work item with a view in which its box is not
+// proven culled, the set of those views, and the subset in which the box
+// straddles a frustum plane (in the others it is wholly inside: no triangle
+// of the item is culled by the per-vertex predicates there).
+struct alignas(8) CrItemViews {
+    unsigned long long views;
+    unsigned long long straddle;
+    uint32_t item;
+    uint32_t pad;
+};
+static_assert(sizeof(CrItemViews) == 24, "CrItemViews layout");
+
 struct CrFrameParams {
     const CrInstance* instances;
     const float4* world_view;   // 4 per instance
@@ -178,6 +190,14 @@ struct CrFrameParams {
     // the others' records from their boxes), counted in
     // counters[CR_CTR_CHUNKS]; nullptr: every chunk
     uint32_t* chunkList;
+    // batched frames: the frame cull's surviving items with their views
+    // (counted in counters[CR_CTR_ITEMS], at most itemCap; nullptr: every
+    // item in every view), and per vertex chunk one CrViewMasks record valid
+    // for all its vertices where chunkUniform is 1 (no view straddles the
+    // chunk's box); the vertex pass writes per-vertex records of the others
+    CrItemViews* itemViews;
+    CrViewMasks* chunkMasks;
+    uint8_t* chunkUniform;
 };
 
 // CrFrameParams::cellMode
@@ -251,6 +271,9 @@ int cr_launch_vertex_views(const CrFrameParams& p, const CrBatchShape& s, void* 
 int cr_launch_stage1_views(const CrFrameParams& p, const CrBatchShape& s, void* stream);
 int cr_launch_stage2_views(const CrFrameParams& p, const CrBatchShape& s, void* stream);
 int cr_launch_stage3_views(const CrFrameParams& p, const CrBatchShape& s, void* stream);
+// Batched frame cull (before the vertex pass): classifies every vertex chunk
+// and work item against every view.
+int cr_launch_cull_views(const CrFrameParams& p, const CrBatchShape& s, void* stream);
 // numBlocks: sum over views of ceil(W / 32) * ceil(H / 32); each view's
 // CrView::resolveBlockBase is the prefix sum of the preceding views' blocks.
 int cr_launch_resolve_views(const CrResolveParams& base, const CrView* views, uint32_t numViews, uint32_t numBlocks,

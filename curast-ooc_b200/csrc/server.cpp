@@ -553,6 +553,17 @@ cr_status cr_server_get_stats(cr_server* sv, cr_server_stats* st) {
     return CR_OK;
 }
 
+cr_status cr_server_reset_stats(cr_server* sv) {
+    if (!sv) return fail(CR_ERR_INVALID, "cr_server_reset_stats: NULL argument");
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->nSubmitted = sv->nCompleted = sv->nBatches = sv->nBatchedViews = 0;
+    sv->latencies.clear();
+    sv->firstSubmit = 0;
+    sv->lastDone = 0;
+    sv->peak = 0;
+    return CR_OK;
+}
+
 cr_status cr_server_destroy(cr_server* sv) {
     if (!sv) return CR_OK;
     {

@@ -29,6 +29,7 @@
 //   stage 2/3  the single-view kernels instantiated with MULTI = true: each
 //            queued entry / tile reads its own view's target and matrix.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cstdint>
 
 #include "raster_core.cuh"
@@ -70,7 +71,10 @@ __global__ void __launch_bounds__(VV_THREADS) k_vertex_views(const CrFrameParams
     const uint32_t nViews = p.numViews;
     const unsigned long long valid = valid_views(nViews);
 
-    for (uint64_t c = blockIdx.x; c < p.numVChunks; c += gridDim.x) {
+    // the chunks the frame cull left for per-vertex records (or every chunk)
+    const uint64_t nChunks = p.chunkList ? min((uint64_t)p.counters[CR_CTR_CHUNKS], p.numVChunks) : p.numVChunks;
+    for (uint64_t k = blockIdx.x; k < nChunks; k += gridDim.x) {
+        const uint64_t c = p.chunkList ? (uint64_t)__ldg(p.chunkList + k) : k;
         uint32_t lo = 0, hi = p.numInstances - 1;  // instance holding chunk c
         while (lo < hi) {
             const uint32_t mid = (lo + hi + 1) >> 1;
@@ -176,13 +180,25 @@ __global__ void __launch_bounds__(VV_THREADS) k_vertex_views(const CrFrameParams
     }
 }
 
+// The record of vertex v of an instance: its chunk's record where the frame
+// cull proved the chunk uniform in every view, else the vertex pass's.
+__device__ __forceinline__ const ulonglong2* record_of(const CrFrameParams& p, const CrViewMasks* rec,
+                                                       uint64_t vchunkBase, uint32_t v) {
+    if (p.chunkUniform) {
+        const uint64_t c = vchunkBase + v / CR_VCHUNK;
+        if (__ldg(p.chunkUniform + c)) return reinterpret_cast<const ulonglong2*>(p.chunkMasks + c);
+    }
+    return reinterpret_cast<const ulonglong2*>(rec + v);
+}
+
 // Views of one triangle that survive the all-behind and all-beyond-one-side
 // culls (tv.cu:110-119) given its three vertex records.
-__device__ __forceinline__ unsigned long long surviving_views(const CrViewMasks* rec, uint32_t i0, uint32_t i1,
+__device__ __forceinline__ unsigned long long surviving_views(const CrFrameParams& p, const CrViewMasks* rec,
+                                                              uint64_t vchunkBase, uint32_t i0, uint32_t i1,
                                                               uint32_t i2, unsigned long long valid) {
-    const ulonglong2* a = reinterpret_cast<const ulonglong2*>(rec + i0);
-    const ulonglong2* b = reinterpret_cast<const ulonglong2*>(rec + i1);
-    const ulonglong2* c = reinterpret_cast<const ulonglong2*>(rec + i2);
+    const ulonglong2* a = record_of(p, rec, vchunkBase, i0);
+    const ulonglong2* b = record_of(p, rec, vchunkBase, i1);
+    const ulonglong2* c = record_of(p, rec, vchunkBase, i2);
     const ulonglong2 a0 = __ldg(a), a1 = __ldg(a + 1), a2 = __ldg(a + 2);
     const ulonglong2 b0 = __ldg(b), b1 = __ldg(b + 1), b2 = __ldg(b + 2);
     const ulonglong2 c0 = __ldg(c), c1 = __ldg(c + 1), c2 = __ldg(c + 2);
@@ -211,11 +227,14 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_stage1_views(const CrFrame
         fence_barrier_init();
     }
     __syncwarp();
+    // work items: the frame cull's survivors with their views, or every item
+    const uint64_t nItems = p.itemViews ? min((uint64_t)p.counters[CR_CTR_ITEMS], p.itemCap) : p.numItems;
+    auto item_at = [&](uint64_t k) -> uint64_t { return p.itemViews ? (uint64_t)__ldg(&p.itemViews[k].item) : k; };
     uint32_t pending = 0;  // ring slots with an issued, unconsumed copy
     for (int s = 0; s < S1_STAGES; ++s) {
-        const uint64_t item = gw + (uint64_t)s * nw;
-        if (item >= p.numItems) break;
-        const Item it = decode_item(p, item);
+        const uint64_t pk = gw + (uint64_t)s * nw;
+        if (pk >= nItems) break;
+        const Item it = decode_item(p, item_at(pk));
         const CrSegment* sg = p.segments + it.seg;
         if (item_uses_tma(sg, it.batch)) {
             pending |= 1u << s;
@@ -228,10 +247,15 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_stage1_views(const CrFrame
 
     uint32_t parity = 0;
     uint32_t k = 0;
-    for (uint64_t item = gw; item < p.numItems; item += nw, ++k) {
+    for (uint64_t pk = gw; pk < nItems; pk += nw, ++k) {
         const int slot = (int)(k % S1_STAGES);
         const uint32_t bit = 1u << slot;
-        const Item it = decode_item(p, item);
+        const Item it = decode_item(p, item_at(pk));
+        // views of the item; records are gathered only for those its box
+        // straddles (in the others every vertex is inside the frustum)
+        const unsigned long long itemViews = p.itemViews ? __ldg(&p.itemViews[pk].views) & valid : valid;
+        const unsigned long long itemStraddle = p.itemViews ? __ldg(&p.itemViews[pk].straddle) & itemViews : valid;
+        const unsigned long long itemInside = itemViews & ~itemStraddle;
         const CrSegment* sg = p.segments + it.seg;
         const uint32_t numTri = __ldg(&sg->numTriangles);
         const uint32_t* gix = ldg_ptr(&sg->indices);
@@ -260,13 +284,16 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_stage1_views(const CrFrame
         const float* pos = ldg_ptr(&sg->positions);
         for (uint32_t inst = ib; inst < ie; ++inst) {
             const CrViewMasks* rec = p.viewMasks + __ldg(&p.instances[inst].outBase);
+            const uint64_t vcb = __ldg(&p.instances[inst].vchunkBase);
             unsigned long long m[S1_R];
 #pragma unroll
             for (int r = 0; r < S1_R; ++r) {
                 const uint32_t tp = r * 32 + lane;
                 m[r] = 0ull;
                 if (tri0 + tp < numTri)
-                    m[r] = surviving_views(rec, index_of(tp, 0), index_of(tp, 1), index_of(tp, 2), valid);
+                    m[r] = itemInside | (itemStraddle ? surviving_views(p, rec, vcb, index_of(tp, 0), index_of(tp, 1),
+                                                                        index_of(tp, 2), itemStraddle)
+                                                      : 0ull);
             }
             // views in which any of the warp's triangles survives, in order;
             // per view the surviving triangles are packed across the lanes
@@ -326,9 +353,9 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_stage1_views(const CrFrame
 
         __syncwarp();
         {  // every read of this slot is done: refill it with the item S1_STAGES ahead
-            const uint64_t nxt = item + (uint64_t)S1_STAGES * nw;
-            if (nxt < p.numItems) {
-                const Item nt = decode_item(p, nxt);
+            const uint64_t nxt = pk + (uint64_t)S1_STAGES * nw;
+            if (nxt < nItems) {
+                const Item nt = decode_item(p, item_at(nxt));
                 const CrSegment* ns = p.segments + nt.seg;
                 if (item_uses_tma(ns, nt.batch)) {
                     pending |= bit;
@@ -345,6 +372,221 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_stage1_views(const CrFrame
     // (bounded) so none lands in shared memory after the block has exited
     for (int s = 0; s < S1_STAGES; ++s)
         if (pending & (1u << s)) (void)mbar_wait_bounded(&s_bar[w][s], (parity >> s) & 1u, p.waitTimeoutNs);
+}
+
+// Classes of one box (warp-uniform) in every view of `which` for one
+// instance: lane classifies views lane and lane + 32; the six 64-bit masks
+// (behind, right, left, top, bottom, inside) come from ballots.
+struct ViewClasses {
+    unsigned long long B, R, L, T, O, I;
+};
+
+__device__ __forceinline__ ViewClasses classify_views(const CrFrameParams& p, uint32_t inst, const float lo[3],
+                                                      const float hi[3], unsigned long long which, int lane) {
+    uint32_t cls[2] = {0u, 0u};
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const uint32_t v = (uint32_t)lane + 32u * h;
+        if (v < p.numViews && ((which >> v) & 1ull)) {
+            const Mat M = load_mat(p.world_view + 4ull * ((uint64_t)v * p.numInstances + inst));
+            cls[h] = classify_box(M, __ldg(&p.views[v].fa), __ldg(&p.views[v].f), lo, hi);
+        }
+    }
+    auto m64 = [&](uint32_t b) -> unsigned long long {
+        const unsigned lo32 = __ballot_sync(FULL, cls[0] & b), hi32 = __ballot_sync(FULL, cls[1] & b);
+        return ((unsigned long long)hi32 << 32) | lo32;
+    };
+    return ViewClasses{m64(CH_BEHIND), m64(CH_RIGHT), m64(CH_LEFT), m64(CH_TOP), m64(CH_BOTTOM), m64(CH_INSIDE)};
+}
+
+// The box of 32 lanes' boxes (lanes without one pass +inf / -inf).
+__device__ __forceinline__ void warp_box(float lo[3], float hi[3]) {
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            lo[j] = fminf(lo[j], __shfl_xor_sync(FULL, lo[j], d));
+            hi[j] = fmaxf(hi[j], __shfl_xor_sync(FULL, hi[j], d));
+        }
+}
+
+__device__ __forceinline__ bool load_box(const float* b, float lo[3], float hi[3]) {
+    for (int j = 0; j < 3; ++j) {
+        lo[j] = __ldg(b + j);
+        hi[j] = __ldg(b + 3 + j);
+    }
+    return lo[0] <= hi[0] && lo[1] <= hi[1] && lo[2] <= hi[2];  // false for NaN boxes
+}
+
+// Batched frame cull, before the vertex pass.  A warp takes 32 consecutive
+// vertex chunks (then 32 consecutive work items): it classifies their common
+// box against every view first (rigorous float bounds, classify_chunk), and
+// each lane then classifies its own box only in the views the common box
+// straddles.
+//   chunks  a chunk no view straddles gets one record for all its vertices
+//           (exact behind bits; side bits of the sides that prove it
+//           outside) and no per-vertex pass; the others are listed for the
+//           vertex pass.
+//   items   an item whose box is wholly behind or beyond one side in a view
+//           has every triangle culled there by the reference's own tests
+//           (tv.cu:110-119); items are listed with the views left, and items
+//           left with none are not visited by stage 1.
+__global__ void __launch_bounds__(256) k_cull_views(const CrFrameParams p) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t gwarp = (uint64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    const uint64_t nwarps = (uint64_t)gridDim.x * 8;
+    const unsigned long long valid = valid_views(p.numViews);
+    const float INF = __int_as_float(0x7f800000);
+
+    if (p.chunkList)
+        for (uint64_t base = gwarp * 32; base < p.numVChunks; base += nwarps * 32) {
+            const uint64_t g = base + lane;
+            const bool has = g < p.numVChunks;
+            uint32_t inst = 0;
+            float lo[3] = {INF, INF, INF}, hi[3] = {-INF, -INF, -INF};
+            bool boxOk = false;
+            if (has) {
+                uint32_t a = 0, b = p.numInstances - 1;  // instance holding chunk g
+                while (a < b) {
+                    const uint32_t mid = (a + b + 1) >> 1;
+                    if (__ldg(&p.instances[mid].vchunkBase) <= g) a = mid;
+                    else b = mid - 1;
+                }
+                inst = a;
+                const float* cb = ldg_ptr(&p.instances[inst].chunkBoxes);
+                if (cb) boxOk = load_box(cb + 6ull * (g - __ldg(&p.instances[inst].vchunkBase)), lo, hi);
+                if (!boxOk) lo[0] = lo[1] = lo[2] = INF, hi[0] = hi[1] = hi[2] = -INF;
+            }
+            const uint32_t inst0 = __shfl_sync(FULL, inst, 0);
+            const bool same = __all_sync(FULL, !has || (boxOk && inst == inst0));
+            ViewClasses c{0ull, 0ull, 0ull, 0ull, 0ull, 0ull};
+            unsigned long long todo = valid;  // views this lane classifies alone
+            if (same) {
+                float glo[3] = {lo[0], lo[1], lo[2]}, ghi[3] = {hi[0], hi[1], hi[2]};
+                warp_box(glo, ghi);
+                c = classify_views(p, inst0, glo, ghi, valid, lane);
+                todo = valid & ~(c.B | c.R | c.L | c.T | c.O | c.I);
+            }
+            if (has && boxOk) {
+                while (todo) {
+                    const uint32_t v = (uint32_t)(__ffsll((long long)todo) - 1);
+                    todo &= todo - 1ull;
+                    const Mat M = load_mat(p.world_view + 4ull * ((uint64_t)v * p.numInstances + inst));
+                    const uint32_t k = classify_box(M, __ldg(&p.views[v].fa), __ldg(&p.views[v].f), lo, hi);
+                    const unsigned long long bit = 1ull << v;
+                    if (k & CH_BEHIND) c.B |= bit;
+                    if (k & CH_RIGHT) c.R |= bit;
+                    if (k & CH_LEFT) c.L |= bit;
+                    if (k & CH_TOP) c.T |= bit;
+                    if (k & CH_BOTTOM) c.O |= bit;
+                    if (k & CH_INSIDE) c.I |= bit;
+                }
+            }
+            const bool uniform = has && boxOk && !(valid & ~(c.B | c.R | c.L | c.T | c.O | c.I));
+            if (has) {
+                p.chunkUniform[g] = uniform ? 1 : 0;
+                if (uniform) {
+                    ulonglong2* r = reinterpret_cast<ulonglong2*>(p.chunkMasks + g);
+                    r[0] = make_ulonglong2(c.B, c.R);
+                    r[1] = make_ulonglong2(c.L, c.T);
+                    r[2] = make_ulonglong2(c.O, 0ull);
+                }
+            }
+            const unsigned m = __ballot_sync(FULL, has && !uniform);
+            if (m) {
+                const int leader = __ffs(m) - 1;
+                unsigned long long b = 0;
+                if (lane == leader) b = atomicAdd(&p.counters[CR_CTR_CHUNKS], (unsigned long long)__popc(m));
+                b = __shfl_sync(FULL, b, leader);
+                if (has && !uniform) p.chunkList[b + __popc(m & ((1u << lane) - 1u))] = (uint32_t)g;
+            }
+        }
+
+    if (!p.itemViews) return;
+    for (uint64_t base = gwarp * 32; base < p.numItems; base += nwarps * 32) {
+        const uint64_t item = base + lane;
+        const bool has = item < p.numItems;
+        uint32_t seg = 0, chunk = 0, ib = 0, ie = 0;
+        float lo[3] = {INF, INF, INF}, hi[3] = {-INF, -INF, -INF};
+        bool boxOk = false;
+        if (has) {
+            const Item it = decode_item(p, item);
+            seg = it.seg;
+            chunk = it.chunk;
+            const CrSegment* sg = p.segments + it.seg;
+            const uint32_t first = __ldg(&sg->firstInstance);
+            ib = first + it.chunk * CR_INST_CHUNK;
+            ie = min(ib + CR_INST_CHUNK, first + __ldg(&sg->instanceCount));
+            const float* boxes = ldg_ptr(&sg->itemBoxes);
+            if (boxes) boxOk = load_box(boxes + 6ull * it.batch, lo, hi);
+            if (!boxOk) lo[0] = lo[1] = lo[2] = INF, hi[0] = hi[1] = hi[2] = -INF;
+        }
+        const uint32_t seg0 = __shfl_sync(FULL, seg, 0), chunk0 = __shfl_sync(FULL, chunk, 0);
+        const bool same = __all_sync(FULL, !has || (boxOk && seg == seg0 && chunk == chunk0));
+        unsigned long long views = 0ull, straddle = 0ull;
+        // the item alone in view v: culled, wholly inside, or straddling
+        auto classify_item = [&](uint32_t inst, uint32_t v) {
+            const unsigned long long bit = 1ull << v;
+            if (!boxOk) {
+                views |= bit;
+                straddle |= bit;
+                return;
+            }
+            const Mat M = load_mat(p.world_view + 4ull * ((uint64_t)v * p.numInstances + inst));
+            const uint32_t k = classify_box(M, __ldg(&p.views[v].fa), __ldg(&p.views[v].f), lo, hi);
+            if (k & CR_OC_MASK) return;
+            views |= bit;
+            if (!(k & CH_INSIDE)) straddle |= bit;
+        };
+        if (same) {
+            float glo[3] = {lo[0], lo[1], lo[2]}, ghi[3] = {hi[0], hi[1], hi[2]};
+            warp_box(glo, ghi);
+            const uint32_t gib = __shfl_sync(FULL, ib, 0), gie = __shfl_sync(FULL, ie, 0);
+            for (uint32_t inst = gib; inst < gie; ++inst) {
+                const ViewClasses c = classify_views(p, inst, glo, ghi, valid, lane);
+                // views where the common box is culled cull every item, where
+                // it is inside every item is inside; the items are classified
+                // alone in the others
+                const unsigned long long culled = c.B | c.R | c.L | c.T | c.O;
+                views |= c.I;
+                unsigned long long todo = valid & ~culled & ~c.I;
+                if (has)
+                    while (todo) {
+                        const uint32_t v = (uint32_t)(__ffsll((long long)todo) - 1);
+                        todo &= todo - 1ull;
+                        classify_item(inst, v);
+                    }
+            }
+        } else if (has) {
+            for (uint32_t inst = ib; inst < ie; ++inst) {
+                unsigned long long todo = valid;
+                while (todo) {
+                    const uint32_t v = (uint32_t)(__ffsll((long long)todo) - 1);
+                    todo &= todo - 1ull;
+                    classify_item(inst, v);
+                }
+            }
+        }
+        const bool keep = has && views != 0ull;
+        const unsigned m = __ballot_sync(FULL, keep);
+        if (m) {
+            const int leader = __ffs(m) - 1;
+            unsigned long long b = 0;
+            if (lane == leader) b = atomicAdd(&p.counters[CR_CTR_ITEMS], (unsigned long long)__popc(m));
+            b = __shfl_sync(FULL, b, leader);
+            if (keep) {
+                const uint64_t q = b + __popc(m & ((1u << lane) - 1u));
+                if (q < p.itemCap) {
+                    CrItemViews e;
+                    e.views = views;
+                    e.straddle = straddle;
+                    e.item = (uint32_t)item;
+                    e.pad = 0;
+                    p.itemViews[q] = e;
+                }
+            }
+        }
+    }
 }
 
 // Clears every view's visbuffer (resolve.cu:213-232); blockIdx.y is the view.
@@ -396,6 +638,16 @@ int cr_launch_vertex_views(const CrFrameParams& p, const CrBatchShape& s, void* 
     uint64_t blocks = p.numVChunks;
     if (blocks > (uint64_t)s.vertexBlocks) blocks = (uint64_t)s.vertexBlocks;
     k_vertex_views<<<(unsigned)blocks, VV_THREADS, 0, (cudaStream_t)stream>>>(p);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int cr_launch_cull_views(const CrFrameParams& p, const CrBatchShape& s, void* stream) {
+    if (p.numViews == 0 || (!p.itemViews && !p.chunkList)) return 0;
+    const uint64_t work = std::max<uint64_t>(p.numItems, p.chunkList ? p.numVChunks : 0);
+    if (work == 0) return 0;
+    uint64_t blocks = (work + 255) / 256;
+    if (blocks > (uint64_t)s.numSMs * 8) blocks = (uint64_t)s.numSMs * 8;
+    k_cull_views<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(p);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

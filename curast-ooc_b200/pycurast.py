@@ -277,6 +277,7 @@ EXPORTS = {
     "cr_server_wait": (_i32, [ctypes.c_void_p, _u64, _u32, ctypes.POINTER(CrServerResult)]),
     "cr_server_release": (_i32, [ctypes.c_void_p, _u64]),
     "cr_server_get_stats": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrServerStats)]),
+    "cr_server_reset_stats": (_i32, [ctypes.c_void_p]),
     "cr_server_destroy": (_i32, [ctypes.c_void_p]),
 }
 
@@ -325,6 +326,9 @@ class Server:
         s = CrServerStats()
         _check(load().cr_server_get_stats(self.h, ctypes.byref(s)))
         return s
+
+    def reset_stats(self):
+        _check(load().cr_server_reset_stats(self.h))
 
     def close(self):
         if self.h:

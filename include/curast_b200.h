@@ -427,6 +427,9 @@ cr_status cr_server_wait(cr_server* server, uint64_t ticket, uint32_t timeout_ms
 /* Returns a completed request's buffers to the budget. */
 cr_status cr_server_release(cr_server* server, uint64_t ticket);
 cr_status cr_server_get_stats(cr_server* server, cr_server_stats* stats);
+/* Starts a new statistics window (counts, latencies, throughput span) on a
+ * running server; requests in flight are counted in the new window. */
+cr_status cr_server_reset_stats(cr_server* server);
 /* Waits for every submitted request, then stops the threads. */
 cr_status cr_server_destroy(cr_server* server);
 
