@@ -49,8 +49,29 @@ def load_peaks():
 # ---------------------------------------------------------------------------
 def build_workload(name):
     """Seeded synthetic stand-ins for the reference's benchmark scenes.
-    Host workloads hold numpy arrays, device workloads torch CUDA tensors."""
+    Host workloads hold numpy arrays, device workloads torch CUDA tensors.
+    A "_c" suffix renders the same scene's meshes in the reference's
+    compressed format (bit-packed indices, 16-bit positions)."""
     import scenes
+
+    if name.endswith("_c"):
+        import pycurast as pc
+
+        import oracle_lib as ol
+
+        wl = build_workload(name[:-2])
+        comps, decoded = [], []
+        for mesh in wl["meshes"]:
+            p, i, c = host_mesh(mesh)
+            comp = pc.compress_mesh(p, i)
+            comps.append(comp)
+            dp, di = ol.decode_compressed(comp.packed, i.size, comp.index_min, comp.index_max, comp.positions,
+                                          comp.aabb_min, comp.aabb_max)
+            decoded.append((dp, di, c))
+        wl.update(name=name, compressed=comps, decoded=decoded,
+                  desc=wl["desc"] + "; meshes in the reference's compressed format (IX_PU16: bit-packed indices, "
+                                    "16-bit quantised positions)")
+        return wl
 
     if name == "heightfield_1m_1080p":
         W, H = 1920, 1080
@@ -282,7 +303,9 @@ def run_ours(args, rank, world, local):
     T, V, Tu = scene_counts(wl)
     W, H = wl["W"], wl["H"]
     ctx = pc.Context(device=local)
-    if wl["device"]:
+    if wl.get("compressed"):
+        handles = [ctx.mesh_compressed(comp, dec[2]) for comp, dec in zip(wl["compressed"], wl["decoded"])]
+    elif wl["device"]:
         handles = [ctx.mesh_from_device(p.data_ptr(), p.shape[0], i.data_ptr(), i.shape[0], c.data_ptr())
                    for (p, i, c) in wl["meshes"]]
     else:
@@ -384,11 +407,18 @@ def run_ours(args, rank, world, local):
     else:
         v_eval, tri_drawn = nV_inst, T
         algo = {"vertex": (12 + rec) * nV_inst, "stage1": 12 * T + rec * nV_inst}
+    if wl.get("compressed"):
+        # compressed meshes: 6-byte positions, 3 x bits / 8 bytes of indices per triangle
+        ib = 3 * wl["compressed"][0].bits / 8.0
+        algo = {"vertex": 24 * (chunks + items) + (6 + rec) * v_eval + 8 * items_drawn,
+                "stage1": ib * tri_drawn + rec * v_eval}
     dominant = max(("vertex", "stage1", "stage2", "stage3", "resolve", "clear"), key=lambda s: stage_ms[s])
     rk = "stage1" if dominant not in algo else dominant
     t_k = stage_ms[rk]
     achieved = algo[rk] / (t_k * 1e-3) / 1e9
     frame_bytes = 12 * T + 12 * V + 16 * W * H + 12 * W * H
+    if wl.get("compressed"):
+        frame_bytes = int(3 * wl["compressed"][0].bits / 8.0 * T) + 6 * V + 16 * W * H + 12 * W * H
     frame_gbs = frame_bytes / (ms * 1e-3) / 1e9
     line = {
         "metric": "Gtris/s @1080p (plain 3-stage visbuffer + resolve, one frame per step)",
@@ -758,7 +788,10 @@ def run_reference(args, rank, world, local):
         ref = ol.Reference("native", device=local)
     except Exception as e:  # noqa: BLE001
         return {"impl": "reference", "unavailable": f"reference kernels not loadable: {e}"}
-    if wl["device"]:
+    if wl.get("compressed"):  # the reference's *_compressed kernels
+        ids = [ref.mesh_compressed_host(cp.packed, cp.positions, cp.num_triangles, dec[2], cp.aabb_min, cp.aabb_max,
+                                        cp.index_min, cp.index_max) for cp, dec in zip(wl["compressed"], wl["decoded"])]
+    elif wl["device"]:
         ids = [ref.mesh_device(p.data_ptr(), p.shape[0], i.data_ptr(), i.shape[0], c.data_ptr())
                for (p, i, c) in wl["meshes"]]
     else:
@@ -770,7 +803,7 @@ def run_reference(args, rank, world, local):
     # build decides a handful of edge triangles differently).
     items = []
     for m, w in wl["instances"]:
-        p, i, c = host_mesh(wl["meshes"][m])
+        p, i, c = wl["decoded"][m] if wl.get("compressed") else host_mesh(wl["meshes"][m])
         items.append((p, i, c, w))
     _, ost = ol.raster(ol.Frame(items, wl["view"]), W, H, wl["proj"][5], nthreads=os.cpu_count() or 1)
     del items

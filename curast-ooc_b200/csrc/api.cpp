@@ -216,6 +216,7 @@ cr_status assemble(cr_context* ctx, const cr_instance* instances, uint32_t count
         ci.outBase = A.outBytes;
         ci.vchunkBase = A.numVChunks;
         ci.chunkBoxes = m.chunkBoxes;
+        if (m.compressed) ci.codec = m.codec;
         A.outBytes += align_up(m.numVertices, 16);
         A.numVChunks += (m.numVertices + CR_VCHUNK - 1) / CR_VCHUNK;
         float* wv = &A.worldView[16ull * r];
@@ -231,7 +232,9 @@ cr_status assemble(cr_context* ctx, const cr_instance* instances, uint32_t count
             s.numTriangles = m.numTriangles;
             s.firstInstance = r;
             s.instanceCount = 0;
-            s.flags = (m.indices && ((uintptr_t)m.indices & 15u) == 0) ? 1u : 0u;
+            // plain 16-byte aligned index arrays are fetched as TMA tiles
+            s.flags = (!m.compressed && m.indices && ((uintptr_t)m.indices & 15u) == 0) ? 1u : 0u;
+            if (m.compressed) s.codec = m.codec;
             s.itemBoxes = m.itemBoxes;
             s.subBoxes = m.subBoxes;
             s.localLists = m.localLists;
@@ -288,8 +291,10 @@ cr_status build_mesh_boxes(cr_context* ctx, MeshRec& m) {
         m.boxBytes = ib + cb + sb + 256;
     }
     float* meshBox = (float*)((char*)m.itemBoxes + ib + cb + sb);
-    if (cr_launch_mesh_boxes(m.indices, m.positions, m.numTriangles, m.numVertices, m.itemBoxes, m.chunkBoxes,
-                             m.subBoxes, meshBox, 0))
+    m.dCodec = (CrCodec*)((char*)meshBox + 64);
+    CR_CUDA(cudaMemcpy(m.dCodec, &m.codec, sizeof(CrCodec), cudaMemcpyHostToDevice), "mesh codec");
+    if (cr_launch_mesh_boxes(m.indices, m.positions, m.compressed ? m.dCodec : nullptr, m.numTriangles,
+                             m.numVertices, m.itemBoxes, m.chunkBoxes, m.subBoxes, meshBox, 0))
         return fail(CR_ERR_CUDA, "mesh box launch: %s", cudaGetErrorString(cudaGetLastError()));
     CR_CUDA(cudaDeviceSynchronize(), "mesh boxes");
     CR_CUDA(cudaMemcpy(m.box, meshBox, sizeof(m.box), cudaMemcpyDeviceToHost), "mesh box readback");
@@ -312,7 +317,8 @@ void ensure_local_lists(cr_context* ctx, MeshRec& m) {
     }
     m.localCounts = (uint32_t*)(m.localLists + lb);
     m.localBytes = bytes;
-    if (cr_launch_local_lists(m.indices, m.numTriangles, m.localLists, m.localCounts, 0) ||
+    if (cr_launch_local_lists(m.indices, m.compressed ? m.dCodec : nullptr, m.numTriangles, m.localLists,
+                              m.localCounts, 0) ||
         cudaDeviceSynchronize() != cudaSuccess) {
         ctx->dev_free(m.localLists, m.localBytes);
         m.localLists = nullptr;
@@ -649,6 +655,152 @@ cr_status cr_mesh_create(cr_context* ctx, const cr_mesh_desc* d, uint32_t* mesh_
     return CR_OK;
 }
 
+uint32_t cr_compressed_index_bits(uint32_t index_min, uint32_t index_max) {
+    // src/CuRast_render.h:358-359 (and src/LargeGlbLoader.h:494): in float
+    const uint32_t range = index_max - index_min;
+    return (uint32_t)std::ceil(std::log2((float)(range + 1u)));
+}
+
+uint64_t cr_compressed_index_words(uint64_t num_indices, uint32_t bits) {
+    return (num_indices * bits + 31) / 32 + 1;
+}
+
+cr_status cr_compress_mesh(const float* positions, uint32_t num_vertices, const uint32_t* indices,
+                           uint32_t num_triangles, uint16_t* positions_out, uint32_t* packed_out,
+                           uint64_t packed_words, float* aabb_min, float* aabb_max, uint32_t* index_min,
+                           uint32_t* index_max) {
+    if (!positions || !indices || !positions_out || !packed_out || !aabb_min || !aabb_max || !index_min || !index_max)
+        return fail(CR_ERR_INVALID, "cr_compress_mesh: NULL argument");
+    if (num_vertices == 0) return fail(CR_ERR_INVALID, "cr_compress_mesh: no vertices");
+    const uint64_t n = 3ull * num_triangles;
+    uint32_t lo = 0xffffffffu, hi = 0;
+    for (uint64_t k = 0; k < n; k++) {
+        lo = std::min(lo, indices[k]);
+        hi = std::max(hi, indices[k]);
+    }
+    if (n == 0) lo = hi = 0;
+    const uint32_t bits = cr_compressed_index_bits(lo, hi);
+    if (bits > 32) return fail(CR_ERR_INVALID, "cr_compress_mesh: index range needs %u bits", bits);
+    if (packed_words < cr_compressed_index_words(n, bits))
+        return fail(CR_ERR_INVALID, "cr_compress_mesh: packed_out holds %llu words, %llu needed",
+                    (unsigned long long)packed_words, (unsigned long long)cr_compressed_index_words(n, bits));
+    memset(packed_out, 0, packed_words * 4);
+    // BitEdit::writeU32 (src/BitEdit.h:29-): the value's bits at bit offset
+    // bits * k, spilling into the next word
+    for (uint64_t k = 0; k < n && bits; k++) {
+        const uint64_t off = bits * k;
+        const uint64_t w = off / 32;
+        const uint32_t sh = (uint32_t)(off % 32);
+        const uint64_t v = (uint64_t)(indices[k] - lo) << sh;
+        packed_out[w] |= (uint32_t)v;
+        if (sh + bits > 32) packed_out[w + 1] |= (uint32_t)(v >> 32);
+    }
+    float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (uint32_t v = 0; v < num_vertices; v++)
+        for (int j = 0; j < 3; j++) {
+            mn[j] = std::min(mn[j], positions[3ull * v + j]);
+            mx[j] = std::max(mx[j], positions[3ull * v + j]);
+        }
+    float size[3];
+    for (int j = 0; j < 3; j++) size[j] = mx[j] - mn[j];  // vec3 aabbSize = max - min (float)
+    for (uint32_t v = 0; v < num_vertices; v++)
+        for (int j = 0; j < 3; j++) {
+            uint16_t q = 0;
+            if (size[j] > 0.0f) {  // src/LargeGlbLoader.h:666-668
+                const double x = 65536.0 * (double)(positions[3ull * v + j] - mn[j]) / (double)size[j];
+                q = (uint16_t)std::min(std::max(x, 0.0), 65535.0);
+            }
+            positions_out[3ull * v + j] = q;
+        }
+    for (int j = 0; j < 3; j++) {
+        aabb_min[j] = mn[j];
+        aabb_max[j] = mx[j];
+    }
+    *index_min = lo;
+    *index_max = hi;
+    return CR_OK;
+}
+
+cr_status cr_mesh_create_compressed(cr_context* ctx, const cr_compressed_mesh_desc* d, uint32_t* mesh_out) {
+    if (!ctx || !d || !mesh_out) return fail(CR_ERR_INVALID, "cr_mesh_create_compressed: NULL argument");
+    if (!d->positions || d->num_vertices == 0) return fail(CR_ERR_INVALID, "cr_mesh_create_compressed: no positions");
+    if (!d->packed_indices && d->num_triangles)
+        return fail(CR_ERR_INVALID, "cr_mesh_create_compressed: compressed meshes are indexed");
+    if (d->index_max < d->index_min) return fail(CR_ERR_INVALID, "cr_mesh_create_compressed: index_max < index_min");
+    const uint32_t bits = cr_compressed_index_bits(d->index_min, d->index_max);
+    if (bits > 32) return fail(CR_ERR_INVALID, "cr_mesh_create_compressed: index range needs %u bits", bits);
+    if (d->num_triangles && (uint64_t)d->index_max >= d->num_vertices)
+        return fail(CR_ERR_INVALID, "cr_mesh_create_compressed: index_max %u beyond %u vertices", d->index_max,
+                    d->num_vertices);
+    cudaSetDevice(ctx->device);
+    MeshRec m;
+    m.live = true;
+    m.compressed = true;
+    m.numVertices = d->num_vertices;
+    m.numTriangles = d->num_triangles;
+    // CuRast_render.h:378: compressionFactor = (aabb.max - aabb.min) / 65536 (float)
+    for (int j = 0; j < 3; j++) {
+        const float size = d->aabb_max[j] - d->aabb_min[j];
+        m.codec.cf[j] = size / 65536.0f;
+        m.codec.mn[j] = d->aabb_min[j];
+    }
+    m.codec.indexMin = d->index_min;
+    m.codec.bits = bits | CR_CODEC_IX_PU16;
+    const uint64_t words = cr_compressed_index_words(3ull * d->num_triangles, bits);
+    if (d->memory == CR_MEM_DEVICE) {
+        m.owned = false;
+        m.positions = (float*)const_cast<uint16_t*>(d->positions);
+        m.indices = const_cast<uint32_t*>(d->packed_indices);
+        m.colors = const_cast<uint32_t*>(d->colors);
+    } else if (d->memory == CR_MEM_HOST) {
+        m.owned = true;
+        const size_t pb = align_up((size_t)d->num_vertices * 6, 256) + 256;
+        const size_t ib = d->num_triangles ? align_up(words * 4, 256) + 256 : 0;
+        const size_t cb = d->colors ? align_up((size_t)d->num_vertices * 4, 256) : 0;
+        cr_status s = ctx->dev_alloc((void**)&m.positions, pb, "mesh positions");
+        if (s) return s;
+        m.bytes += pb;
+        CR_CUDA(cudaMemcpy(m.positions, d->positions, (size_t)d->num_vertices * 6, cudaMemcpyHostToDevice),
+                "mesh positions upload");
+        if (ib) {
+            if ((s = ctx->dev_alloc((void**)&m.indices, ib, "mesh indices"))) {
+                ctx->dev_free(m.positions, pb);
+                return s;
+            }
+            m.bytes += ib;
+            CR_CUDA(cudaMemset(m.indices, 0, ib), "mesh index padding");
+            // the last word past the packed bits may be absent on the host
+            CR_CUDA(cudaMemcpy(m.indices, d->packed_indices, (words - 1) * 4, cudaMemcpyHostToDevice),
+                    "mesh indices upload");
+        }
+        if (cb) {
+            if ((s = ctx->dev_alloc((void**)&m.colors, cb, "mesh colours"))) {
+                ctx->dev_free(m.positions, pb);
+                ctx->dev_free(m.indices, ib);
+                return s;
+            }
+            m.bytes += cb;
+            CR_CUDA(cudaMemcpy(m.colors, d->colors, (size_t)d->num_vertices * 4, cudaMemcpyHostToDevice),
+                    "mesh colours upload");
+        }
+    } else {
+        return fail(CR_ERR_INVALID, "cr_mesh_create_compressed: unknown memory kind %d", d->memory);
+    }
+    cr_status bs = build_mesh_boxes(ctx, m);
+    if (bs) {
+        if (m.owned) {
+            ctx->dev_free(m.positions, 0);
+            ctx->dev_free(m.indices, 0);
+            ctx->dev_free(m.colors, 0);
+            ctx->bytesInUse -= std::min(ctx->bytesInUse, m.bytes);
+        }
+        return bs;
+    }
+    ctx->meshes.push_back(m);
+    *mesh_out = (uint32_t)(ctx->meshes.size() - 1);
+    return CR_OK;
+}
+
 cr_status cr_mesh_destroy(cr_context* ctx, uint32_t mesh) {
     if (!ctx || mesh >= ctx->meshes.size() || !ctx->meshes[mesh].live) return fail(CR_ERR_NOT_FOUND, "unknown mesh %u", mesh);
     MeshRec& m = ctx->meshes[mesh];
@@ -824,6 +976,8 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
     fp.counters = ctx->counters;
     fp.waitTimeoutNs = (uint64_t)ctx->cfg.wait_timeout_ms * 1000000ull;
     fp.debugFlags = ctx->cfg.debug_flags;
+    for (const CrSegment& sg : A.seg)
+        if (sg.codec.bits & CR_CODEC_IX_PU16) fp.anyPacked = 1u;
 
     rp.display = display;
     rp.fb = (const uint64_t*)d_visbuffer;

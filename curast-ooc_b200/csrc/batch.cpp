@@ -140,6 +140,8 @@ void pack_tables(const Assembled& A, const BatchTables& B, const TableLayout& L,
 // Device pointers of a packed table at d.
 void bind_tables(const Assembled& A, const BatchTables& B, const TableLayout& L, char* d, CrFrameParams& fp,
                  CrResolveParams& rp) {
+    for (const CrSegment& sg : A.seg)
+        if (sg.codec.bits & CR_CODEC_IX_PU16) fp.anyPacked = 1u;
     fp.instances = (const CrInstance*)(d + L.oInst);
     fp.world_view = (const float4*)(d + L.oWV);
     fp.world = (const float4*)(d + L.oW);

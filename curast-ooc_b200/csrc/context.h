@@ -45,6 +45,10 @@ struct MeshRec {
     float* subBoxes = nullptr;    // per CR_SUB triangles
     size_t boxBytes = 0;
     float box[6] = {NAN, NAN, NAN, NAN, NAN, NAN};  // host copy of the mesh box
+    // compressed meshes (positions are uint16 xyz, indices bit-packed)
+    bool compressed = false;
+    CrCodec codec{};
+    CrCodec* dCodec = nullptr;    // device copy, inside the box allocation
     // per-item vertex lists, built on first use in a box-culled frame
     uint8_t* localLists = nullptr;
     uint32_t* localCounts = nullptr;

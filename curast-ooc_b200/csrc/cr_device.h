@@ -38,6 +38,18 @@
 #define CR_CTR_CHUNKS 5         // vertex-pass chunks that need per-vertex records
 #define CR_CTR_COUNT 8
 
+// Compressed geometry (the reference's IX_PU16 meshes, CMesh fields
+// compressionFactor / index_min / aabb.min / bitsPerIndex / compressed,
+// src/kernels/HostDeviceInterface.h:196-234); all zero for plain meshes.
+struct alignas(16) CrCodec {
+    float cf[3];                // (aabb.max - aabb.min) / 65536 per axis
+    uint32_t indexMin;          // added to every packed index
+    float mn[3];                // aabb.min
+    uint32_t bits;              // bits per packed index (0..32) | CR_CODEC_IX_PU16
+};
+#define CR_CODEC_IX_PU16 0x100u
+static_assert(sizeof(CrCodec) == 32, "CrCodec layout");
+
 struct alignas(16) CrInstance {
     const uint32_t* indices;    // nullptr -> vertex index 3*t+k
     const float* positions;     // xyz, 12-byte stride
@@ -51,6 +63,7 @@ struct alignas(16) CrInstance {
     uint64_t vchunkBase;        // first vertex-pass chunk of this instance
     const float* chunkBoxes;    // per CR_VCHUNK vertices: min xyz, max xyz (or nullptr)
     uint64_t pad1;
+    CrCodec codec;              // compressed meshes: positions are uint16 xyz
 };
 
 // Per-(instance, vertex) outcode bits written by the vertex pass.  They are
@@ -81,7 +94,7 @@ struct alignas(16) CrInstance {
 #define CR_CELL_INSIDE (1ull << 8)
 #define CR_CELL_FRACX (1ull << 9)
 #define CR_CELL_FRACY (1ull << 10)
-static_assert(sizeof(CrInstance) == 80, "CrInstance layout");
+static_assert(sizeof(CrInstance) == 112, "CrInstance layout");
 
 struct alignas(16) CrSegment {
     const uint32_t* indices;
@@ -97,8 +110,9 @@ struct alignas(16) CrSegment {
     const float* subBoxes;      // per CR_SUB triangles: box of their vertices (or nullptr)
     const uint8_t* localLists;  // per item, CR_LOCAL_BYTES (or nullptr)
     const uint32_t* localCounts;  // per item, distinct vertices or CR_LOCAL_NONE
+    CrCodec codec;              // compressed meshes (flags bit 0 is then clear)
 };
-static_assert(sizeof(CrSegment) == 80, "CrSegment layout");
+static_assert(sizeof(CrSegment) == 112, "CrSegment layout");
 
 struct alignas(16) CrTile {     // HugeTriangle, HostDeviceInterface.h:254-259
     int32_t instance;           // instance | view << 26 (view 0 in single-view frames)
@@ -172,7 +186,7 @@ struct CrFrameParams {
     unsigned long long* counters;
     uint64_t waitTimeoutNs;     // bound of every device-side wait
     uint32_t debugFlags;        // CR_DEBUG_* (failure-detection tests)
-    uint32_t pad;
+    uint32_t anyPacked;         // 1: some mesh of the frame is compressed
     uint8_t* outcodes;          // vertex-pass output, CrInstance::outBase + vertex
     uint64_t numVChunks;        // vertex-pass chunks of all instances
     // batched frames: world_view holds numViews * numInstances matrices,
@@ -247,12 +261,13 @@ int cr_launch_resolve(const CrResolveParams& p, void* stream);
 // and every CR_SUB consecutive triangles and of every CR_VCHUNK consecutive
 // vertices (a box
 // with a non-finite position is NaN and culls nothing).
-int cr_launch_mesh_boxes(const uint32_t* indices, const float* positions, uint32_t numTriangles,
-                         uint32_t numVertices, float* itemBoxes, float* chunkBoxes, float* subBoxes,
-                         float* meshBox, void* stream);
+// `codec`: device copy of a compressed mesh's codec, or nullptr.
+int cr_launch_mesh_boxes(const uint32_t* indices, const float* positions, const CrCodec* codec,
+                         uint32_t numTriangles, uint32_t numVertices, float* itemBoxes, float* chunkBoxes,
+                         float* subBoxes, float* meshBox, void* stream);
 // Per-item vertex lists of an indexed mesh (see CR_LOCAL_BYTES).
-int cr_launch_local_lists(const uint32_t* indices, uint32_t numTriangles, uint8_t* lists, uint32_t* counts,
-                          void* stream);
+int cr_launch_local_lists(const uint32_t* indices, const CrCodec* codec, uint32_t numTriangles, uint8_t* lists,
+                          uint32_t* counts, void* stream);
 
 // Batched (multi-view) frame: one launch per stage over all views.  Grid
 // sizes are chosen by the host (defaults from occupancy, or tuned).

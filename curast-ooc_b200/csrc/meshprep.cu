@@ -19,17 +19,19 @@
 #include <cstdint>
 
 #include "cr_device.h"
+#include "geom.cuh"
 
 namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
 
-__device__ __forceinline__ void extend(float* lo, float* hi, bool& bad, const float* q) {
+__device__ __forceinline__ void extend(float* lo, float* hi, bool& bad, const GeomRef& g, uint32_t v) {
+    float q[3];
+    geom_pos(g, v, q[0], q[1], q[2]);
     for (int j = 0; j < 3; ++j) {
-        const float v = __ldg(q + j);
-        bad |= !isfinite(v);
-        lo[j] = fminf(lo[j], v);
-        hi[j] = fmaxf(hi[j], v);
+        bad |= !isfinite(q[j]);
+        lo[j] = fminf(lo[j], q[j]);
+        hi[j] = fmaxf(hi[j], q[j]);
     }
 }
 
@@ -46,8 +48,10 @@ __device__ __forceinline__ void warp_write_box(float* lo, float* hi, bool bad, f
 }
 
 // One warp per item: lane + 32 r, r < 4, are its triangles.
-__global__ void __launch_bounds__(256) k_item_boxes(const uint32_t* idx, const float* pos, uint32_t nT, float* boxes) {
+__global__ void __launch_bounds__(256) k_item_boxes(const uint32_t* idx, const float* pos, const CrCodec* codec,
+                                                    uint32_t nT, float* boxes) {
     const int lane = threadIdx.x & 31;
+    const GeomRef g = geom_from(pos, idx, codec);
     const uint32_t nItems = (nT + CR_BATCH - 1) / CR_BATCH;
     for (uint32_t b = blockIdx.x * 8 + (threadIdx.x >> 5); b < nItems; b += gridDim.x * 8) {
         float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
@@ -56,8 +60,7 @@ __global__ void __launch_bounds__(256) k_item_boxes(const uint32_t* idx, const f
             const uint32_t t = b * CR_BATCH + r * 32 + lane;
             if (t >= nT) continue;
             for (int k = 0; k < 3; ++k) {
-                const uint32_t v = idx ? __ldg(idx + 3ull * t + k) : 3 * t + k;
-                extend(lo, hi, bad, pos + 3ull * v);
+                extend(lo, hi, bad, g, geom_index(g, 3ull * t + k));
             }
         }
         warp_write_box(lo, hi, bad, boxes + 6ull * b, lane);
@@ -65,8 +68,10 @@ __global__ void __launch_bounds__(256) k_item_boxes(const uint32_t* idx, const f
 }
 
 // Half a warp per sub-box: lane t of the half is its triangle t.
-__global__ void __launch_bounds__(256) k_sub_boxes(const uint32_t* idx, const float* pos, uint32_t nT, float* boxes) {
+__global__ void __launch_bounds__(256) k_sub_boxes(const uint32_t* idx, const float* pos, const CrCodec* codec,
+                                                   uint32_t nT, float* boxes) {
     const int lane = threadIdx.x & 31;
+    const GeomRef g = geom_from(pos, idx, codec);
     const int half = lane >> 4, hl = lane & 15;
     static_assert(CR_SUB == 16, "half-warp per sub-box");
     const uint32_t nSub = (nT + CR_SUB - 1) / CR_SUB;
@@ -78,8 +83,7 @@ __global__ void __launch_bounds__(256) k_sub_boxes(const uint32_t* idx, const fl
         const uint32_t t = sb * CR_SUB + hl;
         if (sb < nSub && t < nT)
             for (int k = 0; k < 3; ++k) {
-                const uint32_t v = idx ? __ldg(idx + 3ull * t + k) : 3 * t + k;
-                extend(lo, hi, bad, pos + 3ull * v);
+                extend(lo, hi, bad, g, geom_index(g, 3ull * t + k));
             }
 #pragma unroll
         for (int d = 8; d >= 1; d >>= 1)
@@ -96,14 +100,16 @@ __global__ void __launch_bounds__(256) k_sub_boxes(const uint32_t* idx, const fl
 }
 
 // One warp per chunk of CR_VCHUNK vertices.
-__global__ void __launch_bounds__(256) k_chunk_boxes(const float* pos, uint32_t nV, float* boxes) {
+__global__ void __launch_bounds__(256) k_chunk_boxes(const float* pos, const CrCodec* codec, uint32_t nV,
+                                                     float* boxes) {
     const int lane = threadIdx.x & 31;
+    const GeomRef g = geom_from(pos, nullptr, codec);
     const uint32_t nChunks = (nV + CR_VCHUNK - 1) / CR_VCHUNK;
     for (uint32_t c = blockIdx.x * 8 + (threadIdx.x >> 5); c < nChunks; c += gridDim.x * 8) {
         float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
         bool bad = false;
         for (uint32_t v = c * CR_VCHUNK + lane; v < min(nV, (c + 1) * CR_VCHUNK); v += 32)
-            extend(lo, hi, bad, pos + 3ull * v);
+            extend(lo, hi, bad, g, v);
         warp_write_box(lo, hi, bad, boxes + 6ull * c, lane);
     }
 }
@@ -158,8 +164,9 @@ __global__ void __launch_bounds__(256) k_mesh_box(const float* itemBoxes, uint32
 // the list (binary search).  Items with more than CR_LOCAL_MAX distinct
 // vertices get CR_LOCAL_NONE.
 constexpr int LL_WARPS = 4;
-__global__ void __launch_bounds__(LL_WARPS * 32) k_local_lists(const uint32_t* idx, uint32_t nT, uint8_t* lists,
-                                                                uint32_t* counts) {
+__global__ void __launch_bounds__(LL_WARPS * 32) k_local_lists(const uint32_t* idx, const CrCodec* codec, uint32_t nT,
+                                                                uint8_t* lists, uint32_t* counts) {
+    const GeomRef g = geom_from(nullptr, idx, codec);
     __shared__ uint32_t s_key[LL_WARPS][512];
     __shared__ uint32_t s_uni[LL_WARPS][512];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -169,7 +176,7 @@ __global__ void __launch_bounds__(LL_WARPS * 32) k_local_lists(const uint32_t* i
     for (uint32_t b = blockIdx.x * LL_WARPS + w; b < nItems; b += gridDim.x * LL_WARPS) {
         const uint32_t t0 = b * CR_BATCH;
         const uint32_t nt = min((uint32_t)CR_BATCH, nT - t0);
-        for (int i = lane; i < 512; i += 32) key[i] = i < 3 * (int)nt ? __ldg(idx + 3ull * t0 + i) : ~0u;
+        for (int i = lane; i < 512; i += 32) key[i] = i < 3 * (int)nt ? geom_index(g, 3ull * t0 + i) : ~0u;
         __syncwarp();
         for (int k = 2; k <= 512; k <<= 1)
             for (int j = k >> 1; j > 0; j >>= 1) {
@@ -213,7 +220,7 @@ __global__ void __launch_bounds__(LL_WARPS * 32) k_local_lists(const uint32_t* i
         for (int t = lane; t < CR_BATCH; t += 32) {
             uint32_t word = 0;
             for (int c = 0; c < 3 && t < (int)nt; ++c) {
-                const uint32_t v = __ldg(idx + 3ull * (t0 + t) + c);
+                const uint32_t v = geom_index(g, 3ull * (t0 + t) + c);
                 int lo = 0, hi = total - 1;  // uni[lo] == v
                 while (lo < hi) {
                     const int mid = (lo + hi) >> 1;
@@ -230,30 +237,30 @@ __global__ void __launch_bounds__(LL_WARPS * 32) k_local_lists(const uint32_t* i
 
 }  // namespace
 
-int cr_launch_local_lists(const uint32_t* indices, uint32_t numTriangles, uint8_t* lists, uint32_t* counts,
-                          void* stream) {
+int cr_launch_local_lists(const uint32_t* indices, const CrCodec* codec, uint32_t numTriangles, uint8_t* lists,
+                          uint32_t* counts, void* stream) {
     const uint32_t nItems = (numTriangles + CR_BATCH - 1) / CR_BATCH;
     if (!nItems) return 0;
     const uint32_t want = (nItems + LL_WARPS - 1) / LL_WARPS;
     k_local_lists<<<want < 148 * 16 ? want : 148 * 16, LL_WARPS * 32, 0, (cudaStream_t)stream>>>(
-        indices, numTriangles, lists, counts);
+        indices, codec, numTriangles, lists, counts);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
-int cr_launch_mesh_boxes(const uint32_t* indices, const float* positions, uint32_t numTriangles,
-                         uint32_t numVertices, float* itemBoxes, float* chunkBoxes, float* subBoxes,
-                         float* meshBox, void* stream) {
+int cr_launch_mesh_boxes(const uint32_t* indices, const float* positions, const CrCodec* codec,
+                         uint32_t numTriangles, uint32_t numVertices, float* itemBoxes, float* chunkBoxes,
+                         float* subBoxes, float* meshBox, void* stream) {
     cudaStream_t st = (cudaStream_t)stream;
     const uint32_t nItems = (numTriangles + CR_BATCH - 1) / CR_BATCH;
     const uint32_t nChunks = (numVertices + CR_VCHUNK - 1) / CR_VCHUNK;
     if (nItems) k_item_boxes<<<(nItems + 7) / 8 < 148 * 16 ? (nItems + 7) / 8 : 148 * 16, 256, 0, st>>>(
-        indices, positions, numTriangles, itemBoxes);
+        indices, positions, codec, numTriangles, itemBoxes);
     const uint32_t nPairs = ((numTriangles + CR_SUB - 1) / CR_SUB + 1) / 2;
     if (nPairs && subBoxes)
         k_sub_boxes<<<(nPairs + 7) / 8 < 148 * 16 ? (nPairs + 7) / 8 : 148 * 16, 256, 0, st>>>(
-            indices, positions, numTriangles, subBoxes);
+            indices, positions, codec, numTriangles, subBoxes);
     if (nChunks) k_chunk_boxes<<<(nChunks + 7) / 8 < 148 * 16 ? (nChunks + 7) / 8 : 148 * 16, 256, 0, st>>>(
-        positions, numVertices, chunkBoxes);
+        positions, codec, numVertices, chunkBoxes);
     if (meshBox) k_mesh_box<<<1, 256, 0, st>>>(itemBoxes, nItems, meshBox);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

@@ -46,16 +46,16 @@ __global__ void __launch_bounds__(THREADS) k_vertex(const CrFrameParams p) {
         const uint32_t v0 = (uint32_t)(c - __ldg(&I->vchunkBase)) * CR_VCHUNK;
         const uint32_t nV = __ldg(&I->numVertices);
         const uint32_t v1 = min(v0 + (uint32_t)CR_VCHUNK, nV);
-        const float* pos = ldg_ptr(&I->positions);
+        const GeomRef g = geom_of(I);
         const Mat M = load_mat(p.world_view + 4ull * lo);
         if (p.cellMode == CR_REC_CELLS) {
             uint64_t* out = reinterpret_cast<uint64_t*>(p.outcodes) + __ldg(&I->outBase);
             for (uint32_t v = v0 + threadIdx.x; v < v1; v += THREADS)
-                out[v] = vertex_cell_record(M, load_pos(pos, v), fa, p.f, Wf, Hf, p.W, p.H);
+                out[v] = vertex_cell_record(M, pos_of(g, v), fa, p.f, Wf, Hf, p.W, p.H);
         } else {
             uint8_t* out = p.outcodes + __ldg(&I->outBase);
             for (uint32_t v = v0 + threadIdx.x; v < v1; v += THREADS)
-                out[v] = (uint8_t)vertex_outcode(M, load_pos(pos, v), fa, p.f);
+                out[v] = (uint8_t)vertex_outcode(M, pos_of(g, v), fa, p.f);
         }
     }
 }
@@ -264,7 +264,9 @@ __device__ __forceinline__ TileSrc tile_source(const CrSegment* sg, uint32_t bat
 #ifndef CR_S1_BOXES_MIN_BLOCKS
 #define CR_S1_BOXES_MIN_BLOCKS 3
 #endif
-template <int WARPS, bool BOXES>
+// PACKED: compiled for frames with compressed meshes (plain frames carry no
+// decoding code).
+template <int WARPS, bool BOXES, bool PACKED>
 __global__ void __launch_bounds__(WARPS * 32, BOXES ? CR_S1_BOXES_MIN_BLOCKS : 3) k_stage1(const CrFrameParams p) {
     constexpr int STAGES = BOXES ? 2 : S1_STAGES;
     static_assert(CR_LOCAL_BYTES <= CR_BATCH * 12, "a vertex-list block fits a ring slot");
@@ -319,7 +321,7 @@ __global__ void __launch_bounds__(WARPS * 32, BOXES ? CR_S1_BOXES_MIN_BLOCKS : 3
         const Item it = decode_item(p, item);
         const CrSegment* sg = p.segments + it.seg;
         const uint32_t numTri = __ldg(&sg->numTriangles);
-        const uint32_t* gix = ldg_ptr(&sg->indices);
+        const GeomRef geo = geom_of_t<PACKED>(sg);
         const TileSrc ts = tile_source<BOXES>(sg, it.batch, lists);
         const bool tma = ts.src != nullptr;
         const bool local = BOXES && ts.local;
@@ -339,8 +341,7 @@ __global__ void __launch_bounds__(WARPS * 32, BOXES ? CR_S1_BOXES_MIN_BLOCKS : 3
         auto index_of = [&](uint32_t pos, int c) -> uint32_t {
             if (local) return tile[(tile[CR_LOCAL_MAX + pos] >> (8 * c)) & 0xffu];
             if (tma) return tile[3 * pos + c];
-            const uint32_t t = tri0 + pos;
-            return gix ? __ldg(gix + 3ull * t + c) : 3 * t + c;
+            return geom_index(geo, 3ull * (tri0 + pos) + c);
         };
         uint32_t ix[S1_R][3];
         bool act[S1_R];
@@ -388,7 +389,6 @@ __global__ void __launch_bounds__(WARPS * 32, BOXES ? CR_S1_BOXES_MIN_BLOCKS : 3
         }
         static_assert(CR_BATCH / CR_SUB == 8 && CR_INST_CHUNK <= 16, "8 sub-boxes x 16 instances in 4 ballots");
         const uint32_t nLocal = local ? __ldg(ldg_ptr(&sg->localCounts) + it.batch) : 0u;
-        const float* pos = ldg_ptr(&sg->positions);
         // Triangles no record or proof culls, queued across the item's
         // instances as (instance slot << 8 | tile position) in a per-warp ring
         // and run through the reference's full path 32 at a time.
@@ -407,9 +407,9 @@ __global__ void __launch_bounds__(WARPS * 32, BOXES ? CR_S1_BOXES_MIN_BLOCKS : 3
                     const uint32_t tp = e & 0xffu;
                     inst = ib + (e >> 8);
                     tri = tri0 + tp;
-                    const V3 pa = load_pos(pos, index_of(tp, 0));
-                    const V3 pb = load_pos(pos, index_of(tp, 1));
-                    const V3 pc = load_pos(pos, index_of(tp, 2));
+                    const V3 pa = pos_of(geo, index_of(tp, 0));
+                    const V3 pb = pos_of(geo, index_of(tp, 1));
+                    const V3 pc = pos_of(geo, index_of(tp, 2));
                     if (!BOXES)
                         res = stage1_triangle(target_of(p), fa, *Mu, flipu, pa, pb, pc, cumu + tri);
                     else
@@ -450,8 +450,8 @@ __global__ void __launch_bounds__(WARPS * 32, BOXES ? CR_S1_BOXES_MIN_BLOCKS : 3
                 if (inside) {
                     for (uint32_t v = lane; v < nLocal; v += 64) {
                         const uint32_t v2 = v + 32;
-                        const uint32_t r0 = vertex_cell32<false>(M, load_pos(pos, tile[v]), fa, p.f, Wf, Hf, Wm1, Hm1);
-                        const uint32_t r1 = v2 < nLocal ? vertex_cell32<false>(M, load_pos(pos, tile[v2]), fa, p.f, Wf,
+                        const uint32_t r0 = vertex_cell32<false>(M, pos_of(geo, tile[v]), fa, p.f, Wf, Hf, Wm1, Hm1);
+                        const uint32_t r1 = v2 < nLocal ? vertex_cell32<false>(M, pos_of(geo, tile[v2]), fa, p.f, Wf,
                                                                                Hf, Wm1, Hm1)
                                                         : 0u;
                         rec[v] = r0;
@@ -459,7 +459,7 @@ __global__ void __launch_bounds__(WARPS * 32, BOXES ? CR_S1_BOXES_MIN_BLOCKS : 3
                     }
                 } else {
                     for (uint32_t v = lane; v < nLocal; v += 32)
-                        rec[v] = vertex_cell32<true>(M, load_pos(pos, tile[v]), fa, p.f, Wf, Hf, Wm1, Hm1);
+                        rec[v] = vertex_cell32<true>(M, pos_of(geo, tile[v]), fa, p.f, Wf, Hf, Wm1, Hm1);
                 }
                 __syncwarp();
                 const uint32_t* cw = tile + CR_LOCAL_MAX;  // corner words
@@ -539,7 +539,8 @@ int cr_query_launch_shape(int device, CrLaunchShape* out) {
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return -1;
     int b1 = 0, b2 = 0, b3 = 0, bv = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_stage1<S1_WARPS, false>, S1_WARPS * 32, 0) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_stage1<S1_WARPS, false, false>, S1_WARPS * 32, 0) !=
+        cudaSuccess)
         return -1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bv, k_vertex<VX_THREADS>, VX_THREADS, 0) != cudaSuccess)
         return -1;
@@ -585,10 +586,15 @@ int cr_launch_stage1(const CrFrameParams& p, const CrLaunchShape& s, void* strea
     uint64_t warps = p.numItems;
     uint64_t blocks = (warps + S1_WARPS - 1) / S1_WARPS;
     if (blocks > (uint64_t)s.stage1Blocks) blocks = (uint64_t)s.stage1Blocks;
-    if (p.cellMode == CR_REC_BOXES)
-        k_stage1<S1_WARPS, true><<<(unsigned)blocks, S1_WARPS * 32, 0, (cudaStream_t)stream>>>(p);
-    else
-        k_stage1<S1_WARPS, false><<<(unsigned)blocks, S1_WARPS * 32, 0, (cudaStream_t)stream>>>(p);
+    const unsigned b = (unsigned)blocks;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (p.cellMode == CR_REC_BOXES) {
+        if (p.anyPacked) k_stage1<S1_WARPS, true, true><<<b, S1_WARPS * 32, 0, st>>>(p);
+        else k_stage1<S1_WARPS, true, false><<<b, S1_WARPS * 32, 0, st>>>(p);
+    } else {
+        if (p.anyPacked) k_stage1<S1_WARPS, false, true><<<b, S1_WARPS * 32, 0, st>>>(p);
+        else k_stage1<S1_WARPS, false, false><<<b, S1_WARPS * 32, 0, st>>>(p);
+    }
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

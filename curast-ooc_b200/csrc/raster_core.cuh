@@ -16,6 +16,7 @@
 #include <cstdint>
 
 #include "cr_device.h"
+#include "geom.cuh"
 namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
@@ -98,6 +99,13 @@ __device__ __forceinline__ T* ldg_ptr(T* const* p) {
 __device__ __forceinline__ V3 load_pos(const float* pos, uint32_t idx) {
     const float* q = pos + 3ull * idx;
     return V3{__ldg(q), __ldg(q + 1), __ldg(q + 2)};
+}
+
+// Position of vertex v of a plain or compressed mesh (geom.cuh).
+__device__ __forceinline__ V3 pos_of(const GeomRef& g, uint32_t v) {
+    V3 r;
+    geom_pos(g, v, r.x, r.y, r.z);
+    return r;
 }
 
 // ---------------------------------------------------------------------------
@@ -778,22 +786,14 @@ __device__ __forceinline__ int stage2_setup(const CrFrameParams& p, const Target
     const uint32_t cum32 = (uint32_t)__ldg(&I->cum);
     const Mat M = load_mat(p.world_view + 4ull * ((uint64_t)view * p.numInstances + inst));
     const float fa = t.fa;
-    const uint32_t* ix = ldg_ptr(&I->indices);
-    const float* pos = ldg_ptr(&I->positions);
-    uint32_t i0, i1, i2;
-    if (ix) {
-        i0 = __ldg(ix + 3ull * tri + 0);
-        i1 = __ldg(ix + 3ull * tri + 1);
-        i2 = __ldg(ix + 3ull * tri + 2);
-    } else {
-        i0 = 3 * tri + 0;
-        i1 = 3 * tri + 1;
-        i2 = 3 * tri + 2;
-    }
+    const GeomRef g = geom_of(I);
+    const uint32_t i0 = geom_index(g, 3ull * tri + 0);
+    const uint32_t i1 = geom_index(g, 3ull * tri + 1);
+    const uint32_t i2 = geom_index(g, 3ull * tri + 2);
     const float f = t.f;
-    const V3 av = xform(M, load_pos(pos, i0));
-    const V3 bv = xform(M, load_pos(pos, i1));
-    const V3 cv = xform(M, load_pos(pos, i2));
+    const V3 av = xform(M, pos_of(g, i0));
+    const V3 bv = xform(M, pos_of(g, i1));
+    const V3 cv = xform(M, pos_of(g, i2));
     const V3 an = to_ndc(av, fa, f);
     const V3 bn = to_ndc(bv, fa, f);
     const V3 cn = to_ndc(cv, fa, f);
@@ -1224,21 +1224,13 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_stage3(const CrFrameParams p)
         const CrInstance* I = p.instances + inst;
         const Mat M = load_mat(p.world_view + 4ull * ((uint64_t)view * p.numInstances + inst));
         const uint32_t tri = (uint32_t)tile.triangle;
-        const uint32_t* ix = ldg_ptr(&I->indices);
-        const float* pos = ldg_ptr(&I->positions);
-        uint32_t i0, i1, i2;
-        if (ix) {
-            i0 = __ldg(ix + 3ull * tri + 0);
-            i1 = __ldg(ix + 3ull * tri + 1);
-            i2 = __ldg(ix + 3ull * tri + 2);
-        } else {
-            i0 = 3 * tri + 0;
-            i1 = 3 * tri + 1;
-            i2 = 3 * tri + 2;
-        }
-        const V3 av = xform(M, load_pos(pos, i0));
-        const V3 bv = xform(M, load_pos(pos, i1));
-        const V3 cv = xform(M, load_pos(pos, i2));
+        const GeomRef g = geom_of(I);
+        const uint32_t i0 = geom_index(g, 3ull * tri + 0);
+        const uint32_t i1 = geom_index(g, 3ull * tri + 1);
+        const uint32_t i2 = geom_index(g, 3ull * tri + 2);
+        const V3 av = xform(M, pos_of(g, i0));
+        const V3 bv = xform(M, pos_of(g, i1));
+        const V3 cv = xform(M, pos_of(g, i2));
         const V3 e1 = sub3(bv, av);
         const V3 e2 = sub3(cv, av);
         const uint64_t id = __ldg(&I->cum) + (uint64_t)tri;

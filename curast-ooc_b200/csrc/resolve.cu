@@ -12,6 +12,7 @@
 #include <cstdint>
 
 #include "cr_device.h"
+#include "geom.cuh"
 
 namespace {
 
@@ -54,9 +55,10 @@ __device__ __forceinline__ T* ldg_ptr(T* const* p) {
     return reinterpret_cast<T*>(__ldg(reinterpret_cast<const unsigned long long*>(p)));
 }
 
-__device__ __forceinline__ V3 load_pos(const float* pos, uint32_t idx) {
-    const float* q = pos + 3ull * idx;
-    return V3{__ldg(q), __ldg(q + 1), __ldg(q + 2)};
+__device__ __forceinline__ V3 pos_of(const GeomRef& g, uint32_t v) {
+    V3 r;
+    geom_pos(g, v, r.x, r.y, r.z);
+    return r;
 }
 
 __device__ __forceinline__ void resolve_pixel(const CrResolveParams& p, const int x, const int y) {
@@ -88,22 +90,15 @@ __device__ __forceinline__ void resolve_pixel(const CrResolveParams& p, const in
         } else if (p.display == 5) {  // DisplayAttribute::TRIANGLE_ID
             color = tri * 12345678u;
         } else if (p.display == 4 && colors) {  // DisplayAttribute::VERTEX_COLORS
-            const uint32_t* ix = ldg_ptr(&I->indices);
-            uint32_t i0, i1, i2;
-            if (ix) {
-                i0 = __ldg(ix + 3ull * tri + 0);
-                i1 = __ldg(ix + 3ull * tri + 1);
-                i2 = __ldg(ix + 3ull * tri + 2);
-            } else {
-                i0 = 3 * tri + 0;
-                i1 = 3 * tri + 1;
-                i2 = 3 * tri + 2;
-            }
-            const float* pos = ldg_ptr(&I->positions);
+            // resolve.cu:742-764: plain or compressed refetch (geom.cuh)
+            const GeomRef g = geom_of(I);
+            const uint32_t i0 = geom_index(g, 3ull * tri + 0);
+            const uint32_t i1 = geom_index(g, 3ull * tri + 1);
+            const uint32_t i2 = geom_index(g, 3ull * tri + 2);
             const float4* W4 = p.world + 4ull * lo;
-            const V3 aw = xform_f4(W4, load_pos(pos, i0));
-            const V3 bw = xform_f4(W4, load_pos(pos, i1));
-            const V3 cw = xform_f4(W4, load_pos(pos, i2));
+            const V3 aw = xform_f4(W4, pos_of(g, i0));
+            const V3 bw = xform_f4(W4, pos_of(g, i1));
+            const V3 cw = xform_f4(W4, pos_of(g, i2));
 
             // computeRayDir, resolve.cu:662-676
             const V3 origin = {p.origin[0], p.origin[1], p.origin[2]};

@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(VV_THREADS) k_vertex_views(const CrFrameParams
         const CrInstance* I = p.instances + inst;
         const uint32_t nV = __ldg(&I->numVertices);
         const uint32_t vw = (uint32_t)(c - __ldg(&I->vchunkBase)) * CR_VCHUNK + (uint32_t)warp * (32 * VV_PER_THREAD);
-        const float* pos = ldg_ptr(&I->positions);
+        const GeomRef g = geom_of(I);
 
         // the views' matrix rows of this instance, once per chunk
         if (tid < CR_MAX_VIEWS && (uint32_t)tid < nViews) {
@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(VV_THREADS) k_vertex_views(const CrFrameParams
 #pragma unroll
         for (int k = 0; k < VV_PER_THREAD; ++k) {
             const uint32_t v = vw + lane + 32 * k;
-            pv[k] = v < nV ? load_pos(pos, v) : V3{0.0f, 0.0f, 0.0f};
+            pv[k] = v < nV ? pos_of(g, v) : V3{0.0f, 0.0f, 0.0f};
             if (v < nV) {
                 bad |= !(isfinite(pv[k].x) && isfinite(pv[k].y) && isfinite(pv[k].z));
                 bl[0] = fminf(bl[0], pv[k].x); bh[0] = fmaxf(bh[0], pv[k].x);
@@ -211,7 +211,8 @@ __device__ __forceinline__ unsigned long long surviving_views(const CrFrameParam
 
 // MINB: resident blocks per SM the register allocation must allow (a tuning
 // knob: more warps to hide latency against fewer registers per thread).
-template <int WARPS, int MINB>
+// PACKED: compiled for frames with compressed meshes.
+template <int WARPS, int MINB, bool PACKED>
 __global__ void __launch_bounds__(WARPS * 32, MINB) k_stage1_views(const CrFrameParams p) {
     __shared__ __align__(128) uint32_t s_idx[WARPS][S1_STAGES][CR_BATCH * 3];
     __shared__ __align__(8) uint64_t s_bar[WARPS][S1_STAGES];
@@ -258,7 +259,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_stage1_views(const CrFrame
         const unsigned long long itemInside = itemViews & ~itemStraddle;
         const CrSegment* sg = p.segments + it.seg;
         const uint32_t numTri = __ldg(&sg->numTriangles);
-        const uint32_t* gix = ldg_ptr(&sg->indices);
+        const GeomRef geo = geom_of_t<PACKED>(sg);
         const bool tma = item_uses_tma(sg, it.batch);
         const uint32_t tri0 = it.batch * CR_BATCH;
         if (tma) {
@@ -273,15 +274,13 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_stage1_views(const CrFrame
         }
         auto index_of = [&](uint32_t pos, int c) -> uint32_t {
             if (tma) return s_idx[w][slot][3 * pos + c];
-            const uint32_t t = tri0 + pos;
-            return gix ? __ldg(gix + 3ull * t + c) : 3 * t + c;
+            return geom_index(geo, 3ull * (tri0 + pos) + c);
         };
 
         const uint32_t first = __ldg(&sg->firstInstance);
         const uint32_t count = __ldg(&sg->instanceCount);
         const uint32_t ib = first + it.chunk * CR_INST_CHUNK;
         const uint32_t ie = min(ib + CR_INST_CHUNK, first + count);
-        const float* pos = ldg_ptr(&sg->positions);
         for (uint32_t inst = ib; inst < ie; ++inst) {
             const CrViewMasks* rec = p.viewMasks + __ldg(&p.instances[inst].outBase);
             const uint64_t vcb = __ldg(&p.instances[inst].vchunkBase);
@@ -328,9 +327,9 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_stage1_views(const CrFrame
                     if (j < nsurv) {
                         const uint32_t tp = s_surv[w][j];
                         tri = tri0 + tp;
-                        const V3 pa = load_pos(pos, index_of(tp, 0));
-                        const V3 pb = load_pos(pos, index_of(tp, 1));
-                        const V3 pc = load_pos(pos, index_of(tp, 2));
+                        const V3 pa = pos_of(geo, index_of(tp, 0));
+                        const V3 pb = pos_of(geo, index_of(tp, 1));
+                        const V3 pc = pos_of(geo, index_of(tp, 2));
                         res = stage1_triangle(tg, tg.fa, M, flip, pa, pb, pc, cum + tri);
                     }
                     const unsigned qmask = __ballot_sync(FULL, res == S1_QUEUE);
@@ -612,7 +611,7 @@ int cr_query_batch_shape(int device, CrBatchShape* out) {
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return -1;
     int bv = 0, b1 = 0, b2 = 0, b3 = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bv, k_vertex_views, VV_THREADS, 0) != cudaSuccess) return -1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_stage1_views<8, 2>, 256, 0) != cudaSuccess) return -1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_stage1_views<8, 2, false>, 256, 0) != cudaSuccess) return -1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_stage2<8, true>, 256, 0) != cudaSuccess) return -1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b3, k_stage3<8, true>, 256, 0) != cudaSuccess) return -1;
     out->numSMs = sms;
@@ -660,12 +659,20 @@ int cr_launch_stage1_views(const CrFrameParams& p, const CrBatchShape& s, void* 
     cudaStream_t st = (cudaStream_t)stream;
     // the register-capped variants let more blocks share an SM
     const bool capped = (uint64_t)s.stage1Blocks > (uint64_t)s.numSMs * (warps == 4 ? 4u : 2u);
-    if (warps == 4) {
-        if (capped) k_stage1_views<4, 6><<<b, 128, 0, st>>>(p);
-        else k_stage1_views<4, 4><<<b, 128, 0, st>>>(p);
+    if (p.anyPacked) {
+        if (warps == 4) {
+            if (capped) k_stage1_views<4, 6, true><<<b, 128, 0, st>>>(p);
+            else k_stage1_views<4, 4, true><<<b, 128, 0, st>>>(p);
+        } else {
+            if (capped) k_stage1_views<8, 3, true><<<b, 256, 0, st>>>(p);
+            else k_stage1_views<8, 2, true><<<b, 256, 0, st>>>(p);
+        }
+    } else if (warps == 4) {
+        if (capped) k_stage1_views<4, 6, false><<<b, 128, 0, st>>>(p);
+        else k_stage1_views<4, 4, false><<<b, 128, 0, st>>>(p);
     } else {
-        if (capped) k_stage1_views<8, 3><<<b, 256, 0, st>>>(p);
-        else k_stage1_views<8, 2><<<b, 256, 0, st>>>(p);
+        if (capped) k_stage1_views<8, 3, false><<<b, 256, 0, st>>>(p);
+        else k_stage1_views<8, 2, false><<<b, 256, 0, st>>>(p);
     }
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

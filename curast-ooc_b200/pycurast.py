@@ -82,6 +82,22 @@ class CrMeshDesc(ctypes.Structure):
     ]
 
 
+class CrCompressedMeshDesc(ctypes.Structure):
+    _fields_ = [
+        ("packed_indices", ctypes.c_void_p),
+        ("positions", ctypes.c_void_p),
+        ("colors", ctypes.c_void_p),
+        ("aabb_min", _f32 * 3),
+        ("aabb_max", _f32 * 3),
+        ("index_min", _u32),
+        ("index_max", _u32),
+        ("num_vertices", _u32),
+        ("num_triangles", _u32),
+        ("memory", _i32),
+        ("reserved", _u32),
+    ]
+
+
 class CrInstance(ctypes.Structure):
     _fields_ = [("mesh", _u32), ("reserved", _u32), ("world", _f32 * 16)]
 
@@ -238,6 +254,11 @@ EXPORTS = {
     "cr_abi_version": (_i32, []),
     "cr_mesh_create": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrMeshDesc), ctypes.POINTER(_u32)]),
     "cr_mesh_destroy": (_i32, [ctypes.c_void_p, _u32]),
+    "cr_mesh_create_compressed": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrCompressedMeshDesc), ctypes.POINTER(_u32)]),
+    "cr_compressed_index_bits": (_u32, [_u32, _u32]),
+    "cr_compressed_index_words": (_u64, [_u64, _u32]),
+    "cr_compress_mesh": (_i32, [ctypes.c_void_p, _u32, ctypes.c_void_p, _u32, ctypes.c_void_p, ctypes.c_void_p, _u64,
+                                ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(_u32), ctypes.POINTER(_u32)]),
     "cr_mesh_refresh": (_i32, [ctypes.c_void_p, _u32]),
     "cr_mesh_device_arrays": (_i32, [ctypes.c_void_p, _u32, ctypes.POINTER(_u64), ctypes.POINTER(_u64),
                                      ctypes.POINTER(_u64)]),
@@ -280,6 +301,41 @@ EXPORTS = {
     "cr_server_reset_stats": (_i32, [ctypes.c_void_p]),
     "cr_server_destroy": (_i32, [ctypes.c_void_p]),
 }
+
+
+class Compressed:
+    """A mesh in the reference's compressed format (cr_compress_mesh)."""
+
+    def __init__(self, positions, packed, aabb_min, aabb_max, index_min, index_max, num_triangles):
+        self.positions = positions      # (V, 3) uint16
+        self.packed = packed            # uint32 words
+        self.aabb_min = aabb_min
+        self.aabb_max = aabb_max
+        self.index_min = index_min
+        self.index_max = index_max
+        self.num_triangles = num_triangles
+
+    @property
+    def bits(self):
+        return int(load().cr_compressed_index_bits(self.index_min, self.index_max))
+
+
+def compress_mesh(positions, indices):
+    """Packs a float mesh as the reference's loader does (cr_compress_mesh)."""
+    pos = np.ascontiguousarray(positions, dtype=np.float32)
+    idx = np.ascontiguousarray(indices, dtype=np.uint32)
+    n = idx.size
+    lo, hi = (int(idx.min()), int(idx.max())) if n else (0, 0)
+    bits = int(load().cr_compressed_index_bits(lo, hi))
+    words = int(load().cr_compressed_index_words(n, bits))
+    packed = np.zeros(words, np.uint32)
+    q = np.zeros((pos.shape[0], 3), np.uint16)
+    mn, mx = (_f32 * 3)(), (_f32 * 3)()
+    imin, imax = _u32(), _u32()
+    _check(load().cr_compress_mesh(pos.ctypes.data, pos.shape[0], idx.ctypes.data, n // 3, q.ctypes.data,
+                                   packed.ctypes.data, words, mn, mx, ctypes.byref(imin), ctypes.byref(imax)))
+    return Compressed(q, packed, np.array(mn[:], np.float32), np.array(mx[:], np.float32), imin.value, imax.value,
+                      n // 3)
 
 
 class Server:
@@ -595,6 +651,24 @@ class Context:
         d.memory = CR_MEM_DEVICE
         out = _u32()
         _check(load().cr_mesh_create(self.h, ctypes.byref(d), ctypes.byref(out)))
+        return out.value
+
+    def mesh_compressed(self, comp, colors=None):
+        """Uploads a compressed mesh (a Compressed from compress_mesh)."""
+        col = None if colors is None else np.ascontiguousarray(colors, dtype=np.uint32)
+        d = CrCompressedMeshDesc()
+        d.packed_indices = comp.packed.ctypes.data
+        d.positions = comp.positions.ctypes.data
+        d.colors = col.ctypes.data if col is not None else None
+        d.aabb_min = (_f32 * 3)(*[float(x) for x in comp.aabb_min])
+        d.aabb_max = (_f32 * 3)(*[float(x) for x in comp.aabb_max])
+        d.index_min = comp.index_min
+        d.index_max = comp.index_max
+        d.num_vertices = comp.positions.shape[0]
+        d.num_triangles = comp.num_triangles
+        d.memory = CR_MEM_HOST
+        out = _u32()
+        _check(load().cr_mesh_create_compressed(self.h, ctypes.byref(d), ctypes.byref(out)))
         return out.value
 
     def mesh_device_arrays(self, mesh):

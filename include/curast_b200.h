@@ -110,6 +110,31 @@ typedef struct cr_mesh_desc {
     uint32_t reserved;
 } cr_mesh_desc;
 
+/* Compressed geometry: the reference's IX_PU16 meshes (CMesh fields
+ * compressed / bitsPerIndex / index_min / index_max / aabb /
+ * compressionFactor, src/kernels/HostDeviceInterface.h:196-234; packed by
+ * src/LargeGlbLoader.h:480-500,660-672).  Index k of the mesh is the
+ * bits_per_index-bit field at bit offset bits_per_index * k of
+ * packed_indices (little-endian 32-bit words, src/BitEdit.h:8-26) plus
+ * index_min, with bits_per_index = ceil(log2f(float(index_max - index_min +
+ * 1))) (src/CuRast_render.h:358-359); the position of vertex v is, per axis,
+ * float(X) * ((aabb_max - aabb_min) / 65536) + aabb_min with X the axis's
+ * uint16 in positions[3 v .. 3 v + 2] (tv.cu:48-58).  Rendered exactly as the
+ * reference's *_compressed kernels render it. */
+typedef struct cr_compressed_mesh_desc {
+    const uint32_t* packed_indices; /* (3 * num_triangles * bits + 31) / 32 words  */
+    const uint16_t* positions;      /* X, Y, Z per vertex (6-byte stride)           */
+    const uint32_t* colors;         /* RGBA8 per vertex; may be NULL                */
+    float aabb_min[3];
+    float aabb_max[3];
+    uint32_t index_min;
+    uint32_t index_max;
+    uint32_t num_vertices;          /* entries of positions (and colors)            */
+    uint32_t num_triangles;
+    int32_t memory;                 /* CR_MEM_HOST: copied; CR_MEM_DEVICE: borrowed */
+    uint32_t reserved;
+} cr_compressed_mesh_desc;
+
 typedef struct cr_instance {
     uint32_t mesh;             /* handle from cr_mesh_create                       */
     uint32_t reserved;
@@ -175,6 +200,26 @@ int cr_abi_version(void);
 /* ---- geometry ----------------------------------------------------------- */
 cr_status cr_mesh_create(cr_context* ctx, const cr_mesh_desc* desc, uint32_t* mesh_out);
 cr_status cr_mesh_destroy(cr_context* ctx, uint32_t mesh);
+/* A compressed mesh (the reference's compressed CMesh, CuRast_render.h:356-379).
+ * As BitEdit::readU32, the reader loads a second word only for a field that
+ * spans two, so the packed array needs no padding. */
+cr_status cr_mesh_create_compressed(cr_context* ctx, const cr_compressed_mesh_desc* desc, uint32_t* mesh_out);
+/* bits per packed index for an index range (src/CuRast_render.h:358-359). */
+uint32_t cr_compressed_index_bits(uint32_t index_min, uint32_t index_max);
+/* 32-bit words cr_compress_mesh writes for num_indices indices: the packed
+ * bits rounded up to whole words, plus one zero word. */
+uint64_t cr_compressed_index_words(uint64_t num_indices, uint32_t bits);
+/* Host-side packing of a plain mesh into the compressed format, as the
+ * reference's loader packs glTF accessors (src/LargeGlbLoader.h:480-500,
+ * 660-672): index_min / index_max over all indices, values minus index_min
+ * bit-packed; aabb = min / max of the positions, X = clamp(65536 * (x -
+ * min) / (max - min), 0, 65535) in double, truncated (0 on a flat axis).
+ * packed_out holds cr_compressed_index_words(3 * num_triangles, bits) words;
+ * positions_out 3 * num_vertices values. */
+cr_status cr_compress_mesh(const float* positions, uint32_t num_vertices, const uint32_t* indices,
+                           uint32_t num_triangles, uint16_t* positions_out, uint32_t* packed_out,
+                           uint64_t packed_words, float* aabb_min, float* aabb_max, uint32_t* index_min,
+                           uint32_t* index_max);
 /* Per-view culling of whole groups of triangles uses bounding boxes computed
  * from the mesh's contents when it is created.  A caller that changes the
  * contents of a borrowed (CR_MEM_DEVICE) mesh afterwards calls

@@ -150,6 +150,8 @@ def harness():
         lib.refh_mesh_host.argtypes = [_vp, _u32, _vp, _u32, _vp]
         lib.refh_mesh_device.restype = _i32
         lib.refh_mesh_device.argtypes = [_u64, _u32, _u64, _u32, _u64]
+        lib.refh_mesh_compressed_host.restype = _i32
+        lib.refh_mesh_compressed_host.argtypes = [_vp, _u64, _vp, _u32, _u32, _vp, _vp, _vp, _u32, _u32]
         lib.refh_reset_meshes.restype = _i32
         lib.refh_frame.restype = _i32
         lib.refh_frame.argtypes = [_vp, _vp, _u32, _vp, _vp, _i32, _i32, _i32, _i32, _u64, _u64, _i32, _vp, _vp,
@@ -198,6 +200,19 @@ class Reference:
             raise RuntimeError(f"refh_mesh_host: {h} {self.lib.refh_last_error().decode()}")
         return h
 
+    def mesh_compressed_host(self, packed, qpos, nT, col, aabb_min, aabb_max, index_min, index_max):
+        packed = np.ascontiguousarray(packed, np.uint32)
+        qpos = np.ascontiguousarray(qpos, np.uint16)
+        col = None if col is None else np.ascontiguousarray(col, np.uint32)
+        mn = np.ascontiguousarray(aabb_min, np.float32)
+        mx = np.ascontiguousarray(aabb_max, np.float32)
+        h = self.lib.refh_mesh_compressed_host(packed.ctypes.data, packed.size, qpos.ctypes.data, qpos.shape[0], nT,
+                                               col.ctypes.data if col is not None else None, mn.ctypes.data,
+                                               mx.ctypes.data, int(index_min), int(index_max))
+        if h < 0:
+            raise RuntimeError(f"refh_mesh_compressed_host: {h} {self.lib.refh_last_error().decode()}")
+        return h
+
     def mesh_device(self, d_pos, nV, d_idx, nT, d_col=0):
         return self.lib.refh_mesh_device(int(d_pos), int(nV), int(d_idx), int(nT), int(d_col))
 
@@ -223,3 +238,62 @@ class Reference:
         if rc != 0:
             raise RuntimeError(f"refh_frame: {rc} {self.lib.refh_last_error().decode()}")
         return vis, cb, rgba, ms, counts
+
+
+# ---------------------------------------------------------------------------
+# compressed geometry (IX_PU16) -- CPU restatement of the reference's packing
+# (src/LargeGlbLoader.h:480-500, 660-672) and decoding (src/BitEdit.h:8-26,
+# triangles_visbuffer.cu:48-58)
+# ---------------------------------------------------------------------------
+def compressed_index_bits(index_min, index_max):
+    """src/CuRast_render.h:358-359: ceil(log2f(float(range + 1)))."""
+    return int(np.ceil(np.log2(np.float32(index_max - index_min + 1))))
+
+
+def pack_compressed(positions, indices):
+    """The reference loader's packing: index_min/max over all indices, values
+    minus index_min written bits-wide LSB-first into 32-bit words; positions
+    quantised per axis as clamp(65536 * (x - min) / (max - min), 0, 65535) in
+    double (float differences), truncated.  A flat axis gives 0."""
+    pos = np.asarray(positions, np.float32)
+    idx = np.asarray(indices, np.uint32).reshape(-1)
+    lo, hi = (int(idx.min()), int(idx.max())) if idx.size else (0, 0)
+    bits = compressed_index_bits(lo, hi)
+    words = (idx.size * bits + 31) // 32 + 1
+    acc = np.zeros(words + 1, np.uint64)
+    if bits:
+        off = np.arange(idx.size, dtype=np.uint64) * np.uint64(bits)
+        w = off >> np.uint64(5)
+        sh = off & np.uint64(31)
+        v = (idx.astype(np.uint64) - np.uint64(lo)) << sh
+        np.add.at(acc, w, v & np.uint64(0xFFFFFFFF))
+        np.add.at(acc, w + np.uint64(1), v >> np.uint64(32))
+    packed = acc[:words].astype(np.uint32)
+    mn, mx = pos.min(0), pos.max(0)
+    size = (mx - mn).astype(np.float32)
+    diff = (pos - mn).astype(np.float32)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        q = 65536.0 * diff.astype(np.float64) / size.astype(np.float64)
+    q = np.where(size > 0, np.clip(q, 0.0, 65535.0), 0.0).astype(np.uint16)
+    return packed, q, mn, mx, lo, hi
+
+
+def decode_compressed(packed, num_indices, index_min, index_max, qpos, aabb_min, aabb_max):
+    """Plain (float32 positions, uint32 indices) of a compressed mesh, with the
+    reference's float operations: BitEdit::readU32 + index_min, and
+    float(X) * ((max - min) / 65536) + min per axis, each operation rounded
+    to float32."""
+    bits = compressed_index_bits(index_min, index_max)
+    words = np.concatenate([np.asarray(packed, np.uint32), np.zeros(2, np.uint32)]).astype(np.uint64)
+    if bits == 0 or bits > 32:
+        idx = np.full(num_indices, index_min, np.uint64)
+    else:
+        off = np.arange(num_indices, dtype=np.uint64) * np.uint64(bits)
+        w = off >> np.uint64(5)
+        sh = off & np.uint64(31)
+        comb = words[w] | (words[w + np.uint64(1)] << np.uint64(32))
+        idx = ((comb >> sh) & np.uint64((1 << bits) - 1)) + np.uint64(index_min)
+    mn = np.asarray(aabb_min, np.float32)
+    cf = (np.asarray(aabb_max, np.float32) - mn) / np.float32(65536.0)
+    pos = np.asarray(qpos, np.uint16).astype(np.float32) * cf + mn
+    return pos.astype(np.float32), idx.astype(np.uint32).reshape(-1, 3)

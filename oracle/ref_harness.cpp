@@ -84,6 +84,7 @@ CUcontext g_ctx = nullptr;
 CUdevice g_dev = 0;
 CUmodule g_mod_tv = nullptr, g_mod_resolve = nullptr;
 CUfunction g_stage1 = nullptr, g_stage1_inst = nullptr, g_stage2 = nullptr, g_stage3 = nullptr;
+CUfunction g_stage1c = nullptr, g_stage1c_inst = nullptr, g_stage2c = nullptr, g_stage3c = nullptr;
 CUfunction g_clear = nullptr, g_resolve = nullptr, g_screenshot = nullptr;
 int g_numSMs = 0;
 char g_err[1024] = {0};
@@ -92,6 +93,10 @@ struct RefMesh {
     CUdeviceptr pos = 0, idx = 0, col = 0;
     uint32_t nV = 0, nT = 0;
     bool owned = false;
+    // compressed (IX_PU16) meshes: CMesh fields of CuRast_render.h:356-379
+    bool compressed = false;
+    float aabbMin[3] = {0, 0, 0}, aabbMax[3] = {0, 0, 0};
+    uint32_t indexMin = 0, indexMax = 0;
 };
 std::vector<RefMesh> g_meshes;
 
@@ -172,6 +177,11 @@ int refh_init(const char* dir, const char* mode, int device) {
                                    "kernel_stage1_drawSmallTriangles_indexbuffer_uncompressed_instanced"));
     CK(g_drv.p_cuModuleGetFunction(&g_stage2, g_mod_tv, "kernel_stage2_drawMediumTriangles_indexbuffer_uncompressed"));
     CK(g_drv.p_cuModuleGetFunction(&g_stage3, g_mod_tv, "kernel_stage3_drawHugeTriangles_indexbuffer_uncompressed"));
+    CK(g_drv.p_cuModuleGetFunction(&g_stage1c, g_mod_tv, "kernel_stage1_drawSmallTriangles_indexbuffer_compressed"));
+    CK(g_drv.p_cuModuleGetFunction(&g_stage1c_inst, g_mod_tv,
+                                   "kernel_stage1_drawSmallTriangles_indexbuffer_compressed_instanced"));
+    CK(g_drv.p_cuModuleGetFunction(&g_stage2c, g_mod_tv, "kernel_stage2_drawMediumTriangles_indexbuffer_compressed"));
+    CK(g_drv.p_cuModuleGetFunction(&g_stage3c, g_mod_tv, "kernel_stage3_drawHugeTriangles_indexbuffer_compressed"));
     CK(g_drv.p_cuModuleGetFunction(&g_clear, g_mod_resolve, "kernel_clearFramebuffer"));
     CK(g_drv.p_cuModuleGetFunction(&g_resolve, g_mod_resolve, "kernel_resolve_visbuffer_to_colorbuffer2D"));
     CK(g_drv.p_cuModuleGetFunction(&g_screenshot, g_mod_resolve, "kernel_resolve_colorbuffer_to_screenshot"));
@@ -196,6 +206,29 @@ int refh_mesh_host(const float* pos, uint32_t nV, const uint32_t* idx, uint32_t 
     CK(g_drv.p_cuMemcpyHtoD(m.pos, pos, (size_t)nV * 12));
     CK(g_drv.p_cuMemAlloc(&m.idx, (size_t)nT * 12 + 16));
     CK(g_drv.p_cuMemcpyHtoD(m.idx, idx, (size_t)nT * 12));
+    if (col) {
+        CK(g_drv.p_cuMemAlloc(&m.col, (size_t)nV * 4 + 16));
+        CK(g_drv.p_cuMemcpyHtoD(m.col, col, (size_t)nV * 4));
+    }
+    g_meshes.push_back(m);
+    return (int)g_meshes.size() - 1;
+}
+
+// Uploads a compressed mesh: packed index words (`words` of them), uint16
+// xyz positions, its aabb and index range.
+int refh_mesh_compressed_host(const uint32_t* packed, uint64_t words, const uint16_t* pos, uint32_t nV, uint32_t nT,
+                              const uint32_t* col, const float* aabbMin, const float* aabbMax, uint32_t indexMin,
+                              uint32_t indexMax) {
+    RefMesh m;
+    m.nV = nV; m.nT = nT; m.owned = true; m.compressed = true;
+    for (int j = 0; j < 3; j++) { m.aabbMin[j] = aabbMin[j]; m.aabbMax[j] = aabbMax[j]; }
+    m.indexMin = indexMin; m.indexMax = indexMax;
+    CK(g_drv.p_cuCtxSetCurrent(g_ctx));
+    CK(g_drv.p_cuMemAlloc(&m.pos, (size_t)nV * 6 + 16));
+    CK(g_drv.p_cuMemcpyHtoD(m.pos, pos, (size_t)nV * 6));
+    CK(g_drv.p_cuMemAlloc(&m.idx, words * 4 + 16));
+    CK(g_drv.p_cuMemsetD8(m.idx, 0, words * 4 + 16));
+    CK(g_drv.p_cuMemcpyHtoD(m.idx, packed, words * 4));
     if (col) {
         CK(g_drv.p_cuMemAlloc(&m.col, (size_t)nV * 4 + 16));
         CK(g_drv.p_cuMemcpyHtoD(m.col, col, (size_t)nV * 4));
@@ -255,6 +288,15 @@ int refh_frame(const int32_t* meshIds, const float* worlds, uint32_t nInst, cons
         c.numVertices = rm.nV;
         c.isLoaded = true;
         c.compressed = false;
+        if (rm.compressed) {  // CuRast_render.h:358-378
+            c.compressed = true;
+            c.index_min = rm.indexMin;
+            c.index_max = rm.indexMax;
+            c.bitsPerIndex = (uint32_t)ceil(log2f(float(rm.indexMax - rm.indexMin + 1)));
+            c.aabb.min = glm::vec3(rm.aabbMin[0], rm.aabbMin[1], rm.aabbMin[2]);
+            c.aabb.max = glm::vec3(rm.aabbMax[0], rm.aabbMax[1], rm.aabbMax[2]);
+            c.compressionFactor = (c.aabb.max - c.aabb.min) / 65536.0f;
+        }
         c.id = (int)i;
         c.address = (uint64_t)meshIds[i] + 1;
         glm::vec3 c0 = c.world[0], c1 = c.world[1], c2 = c.world[2];
@@ -377,9 +419,12 @@ int refh_frame(const int32_t* meshIds, const float* worlds, uint32_t nInst, cons
         CKC(g_drv.p_cuLaunchKernel(g_clear, gridClear, 1, 1, 256, 1, 1, 0, 0, clearArgsFb, nullptr));
         CKC(g_drv.p_cuLaunchKernel(g_clear, gridClear, 1, 1, 256, 1, 1, 0, 0, clearArgsCb, nullptr));
         void* rargs[] = {&args};
-        int lc = launch_cooperative(instanced ? g_stage1_inst : g_stage1, TRIANGLES_PER_SWEEP, rargs, 0);
-        if (!lc) lc = launch_cooperative(g_stage2, 128, rargs, 0);
-        if (!lc) lc = launch_cooperative(g_stage3, 64, rargs, 0);
+        // CuRast_render.h:234-243: the kernel variant follows meshes[0].compressed
+        const bool comp = unique[0].compressed;
+        int lc = launch_cooperative(comp ? (instanced ? g_stage1c_inst : g_stage1c) : (instanced ? g_stage1_inst : g_stage1),
+                                    TRIANGLES_PER_SWEEP, rargs, 0);
+        if (!lc) lc = launch_cooperative(comp ? g_stage2c : g_stage2, 128, rargs, 0);
+        if (!lc) lc = launch_cooperative(comp ? g_stage3c : g_stage3, 64, rargs, 0);
         if (lc) { cleanup(); return lc; }
         CKC(g_drv.p_cuEventRecord(e1, 0));
         void* resolveArgs[] = {&d_all, &nInst, &d_prefix, &mouse, &mouse, &d_state, &rs, &jpp};
