@@ -327,6 +327,13 @@ void ensure_local_lists(cr_context* ctx, MeshRec& m) {
     }
 }
 
+void ensure_local_lists_for(cr_context* ctx, const cr_instance* instances, uint32_t count) {
+    for (uint32_t i = 0; i < count; i++) {
+        const uint32_t m = instances[i].mesh;
+        if (m < ctx->meshes.size() && ctx->meshes[m].live) ensure_local_lists(ctx, ctx->meshes[m]);
+    }
+}
+
 // Packs the assembled frame into pinned memory and copies it to the device.
 cr_status upload_frame(cr_context* ctx, const Assembled& A, cudaStream_t stream, CrFrameParams& fp,
                        CrResolveParams& rp) {

@@ -71,6 +71,15 @@ void bind_cull(const Assembled& A, const CullLayout& L, void* base, CrFrameParam
     fp.itemCap = A.numItems;
 }
 
+// Vertex-list stage 1 (k_stage1_views_lists; no vertex pass) for views whose
+// pixel cells fit the 12-bit cell records.
+void use_lists(const BatchTables& B, CrFrameParams& fp) {
+    if (B.maxW > 4096 || B.maxH > 4096) return;
+    fp.cellMode = CR_REC_BOXES;
+    fp.chunkList = nullptr;
+    fp.chunkUniform = nullptr;
+}
+
 cr_status check_views(const cr_view* views, uint32_t nv, uint32_t flags) {
     if (!views || nv == 0) return fail(CR_ERR_INVALID, "batched render: no views");
     if (nv > CR_MAX_BATCH_VIEWS) return fail(CR_ERR_INVALID, "batched render: %u views (at most %u)", nv, CR_MAX_BATCH_VIEWS);
@@ -231,6 +240,7 @@ cr_status render_batch(cr_context* ctx, const cr_instance* instances, uint32_t c
     cr_status s = check_views(views, nv, flags);
     if (s) return s;
     CR_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    ensure_local_lists_for(ctx, instances, count);
     Assembled A;
     s = assemble(ctx, instances, count, views[0].camera.view, flags, A);
     if (s) return s;
@@ -275,6 +285,7 @@ cr_status render_batch(cr_context* ctx, const cr_instance* instances, uint32_t c
     bind_tables(A, B, L, (char*)ctx->dFrame, fp, rp);
     base_params(ctx, display, fp, rp);
     bind_cull(A, CL, ctx->outcodes, fp);
+    use_lists(B, fp);
     fp.counters = ctx->counters;
     auto issue = [&](cudaEvent_t* tev, cudaEvent_t rasterEnd) -> cr_status {
         fp.ntList = ctx->ntList;
@@ -295,6 +306,7 @@ cr_status cr::scratch_issue(cr_context* ctx, BatchScratch& S, const cr_instance*
                             const cr_view* views, uint32_t nv, int32_t display, uint32_t flags, cudaStream_t stream) {
     cr_status s = check_views(views, nv, flags);
     if (s) return s;
+    ensure_local_lists_for(ctx, instances, count);
     Assembled A;
     s = assemble(ctx, instances, count, views[0].camera.view, flags, A);
     if (s) return s;
@@ -341,6 +353,7 @@ cr_status cr::scratch_issue(cr_context* ctx, BatchScratch& S, const cr_instance*
     bind_tables(A, B, L, (char*)S.dTable, fp, rp);
     base_params(ctx, display, fp, rp);
     bind_cull(A, CL, S.records, fp);
+    use_lists(B, fp);
     fp.counters = S.counters;
     fp.ntList = S.ntList;
     fp.ntCap = S.ntCap;
@@ -464,6 +477,7 @@ cr_status cr_batch_plan_create(cr_context* ctx, const cr_instance* instances, ui
     p->flags = flags;
     p->instances.assign(instances, instances + count);
     p->views.assign(views, views + num_views);
+    ensure_local_lists_for(ctx, instances, count);
     s = assemble(ctx, instances, count, views[0].camera.view, flags, p->A);
     if (s) {
         delete p;
@@ -525,6 +539,7 @@ cr_status cr_batch_plan_create(cr_context* ctx, const cr_instance* instances, ui
     bind_tables(p->A, p->B, p->L, (char*)p->dTable, fp, rp);
     base_params(ctx, display, fp, rp);
     bind_cull(p->A, cull_layout(p->A), p->records, fp);
+    use_lists(p->B, fp);
     fp.counters = p->counters;
     fp.ntList = p->ntList;
     fp.ntCap = p->ntCap;

@@ -146,6 +146,10 @@ cr_status ensure_queues(cr_context* ctx, uint64_t ntWant, uint64_t hugeWant);
 cr_status build_mesh_boxes(cr_context* ctx, MeshRec& m);
 // Grows the per-vertex record buffer to at least `bytes`.
 cr_status ensure_records(cr_context* ctx, uint64_t bytes);
+// Builds a mesh's per-item vertex lists on first use (absent on failure).
+void ensure_local_lists(cr_context* ctx, MeshRec& m);
+// Vertex lists for every mesh of an instance list (batched frames).
+void ensure_local_lists_for(cr_context* ctx, const cr_instance* instances, uint32_t count);
 
 // Issues one frame.  issue(tev, rasterEnd) enqueues the stages on `stream`
 // with the context's current queues, recording tev[0..6] around them when

@@ -191,6 +191,12 @@ __device__ __forceinline__ const ulonglong2* record_of(const CrFrameParams& p, c
     return reinterpret_cast<const ulonglong2*>(rec + v);
 }
 
+struct TileSrc {
+    const void* src;
+    uint32_t bytes;
+    bool local;
+};
+
 // Views of one triangle that survive the all-behind and all-beyond-one-side
 // culls (tv.cu:110-119) given its three vertex records.
 __device__ __forceinline__ unsigned long long surviving_views(const CrFrameParams& p, const CrViewMasks* rec,
@@ -588,6 +594,265 @@ __global__ void __launch_bounds__(256) k_cull_views(const CrFrameParams p) {
     }
 }
 
+#ifndef CR_RECORD_SPAN_PX
+#define CR_RECORD_SPAN_PX 12.0f
+#endif
+// Whether cell records of an item's vertices are likely to cull most of its
+// triangles in one view: the item box's projected extent, bounded from its
+// bounding sphere, is small enough for its 128 triangles to be about a pixel
+// or less.  Only the speed depends on the answer.
+__device__ __forceinline__ bool records_pay(const Mat& M, const Target& tg, const float box[6], bool hasBox) {
+    if (!hasBox) return true;
+    const float cx = 0.5f * (box[0] + box[3]), cy = 0.5f * (box[1] + box[4]), cz = 0.5f * (box[2] + box[5]);
+    const float ex = box[3] - box[0], ey = box[4] - box[1], ez = box[5] - box[2];
+    const float r = 0.5f * sqrtf(ex * ex + ey * ey + ez * ez);
+    // largest column norm of the 3x3 part: the view-space radius bound
+    const float s0 = M.c0.x * M.c0.x + M.c0.y * M.c0.y + M.c0.z * M.c0.z;
+    const float s1 = M.c1.x * M.c1.x + M.c1.y * M.c1.y + M.c1.z * M.c1.z;
+    const float s2 = M.c2.x * M.c2.x + M.c2.y * M.c2.y + M.c2.z * M.c2.z;
+    const float rv = r * sqrtf(fmaxf(s0, fmaxf(s1, s2))) * 1.01f;
+    const float d = -((M.c0.z * cx + M.c1.z * cy) + (M.c2.z * cz + M.c3.z));
+    if (!(d - rv > 0.0f)) return false;  // near or behind the camera: large on screen
+    const float spanPx = rv * fmaxf(tg.f, tg.fa) * (float)max(tg.W, tg.H) / (d - rv);
+    return spanPx < CR_RECORD_SPAN_PX;
+}
+
+// Stage 1 of batched frames whose meshes have per-item vertex lists (the
+// frame cull's item list is required; no vertex pass runs).  Per item the
+// warp's TMA ring carries the item's 1536-byte vertex-list block.  Per
+// (instance, view) of the item: where the item is small on screen, the warp
+// computes the 32-bit cell records of the item's distinct vertices in shared
+// memory -- without the frustum predicates in views whose frustum holds the
+// item's box -- culls each triangle from its three records and queues the
+// rest (view, instance, triangle) in a per-warp ring that runs the
+// reference's full path 32 at a time; where it is large, every triangle runs
+// the full path at once with the view's target and matrix for the warp.
+// Items without a list run every triangle in every view of the item.
+template <int WARPS, int MINB, bool PACKED>
+__global__ void __launch_bounds__(WARPS * 32, MINB) k_stage1_views_lists(const CrFrameParams p) {
+    constexpr int STAGES = 2;
+    __shared__ __align__(128) uint32_t s_idx[WARPS][STAGES][CR_BATCH * 3];
+    __shared__ __align__(8) uint64_t s_bar[WARPS][STAGES];
+    __shared__ uint32_t s_rec[WARPS][CR_LOCAL_MAX];
+    __shared__ uint32_t s_ring[WARPS][S1_RING];
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    const uint64_t gw = (uint64_t)blockIdx.x * WARPS + w;
+    const uint64_t nw = (uint64_t)gridDim.x * WARPS;
+    const unsigned long long valid = valid_views(p.numViews);
+
+    if (lane == 0) {
+        for (int s = 0; s < STAGES; ++s) mbar_init(&s_bar[w][s], 1);
+        fence_barrier_init();
+    }
+    __syncwarp();
+    const uint64_t nItems = min((uint64_t)p.counters[CR_CTR_ITEMS], p.itemCap);
+    // the ring slot's source: vertex-list block, index tile, or nothing
+    auto source = [&](uint64_t k) -> TileSrc {
+        const Item it = decode_item(p, (uint64_t)__ldg(&p.itemViews[k].item));
+        const CrSegment* sg = p.segments + it.seg;
+        const uint32_t* lc = ldg_ptr(&sg->localCounts);
+        if (lc && __ldg(lc + it.batch) <= CR_LOCAL_MAX)
+            return TileSrc{ldg_ptr(&sg->localLists) + (uint64_t)it.batch * CR_LOCAL_BYTES, CR_LOCAL_BYTES, true};
+        if (item_uses_tma(sg, it.batch))
+            return TileSrc{ldg_ptr(&sg->indices) + (uint64_t)it.batch * (CR_BATCH * 3), CR_BATCH * 12, false};
+        return TileSrc{nullptr, 0, false};
+    };
+    uint32_t pending = 0;
+    for (int s = 0; s < STAGES; ++s) {
+        const uint64_t pk = gw + (uint64_t)s * nw;
+        if (pk >= nItems) break;
+        const TileSrc ts = source(pk);
+        if (ts.src) {
+            pending |= 1u << s;
+            if (lane == 0) bulk_load(s_idx[w][s], ts.src, ts.bytes, &s_bar[w][s]);
+        }
+    }
+    __syncwarp();
+
+    uint32_t parity = 0;
+    uint32_t k = 0;
+    for (uint64_t pk = gw; pk < nItems; pk += nw, ++k) {
+        const int slot = (int)(k % STAGES);
+        const uint32_t bit = 1u << slot;
+        const Item it = decode_item(p, (uint64_t)__ldg(&p.itemViews[pk].item));
+        const unsigned long long itemViews = __ldg(&p.itemViews[pk].views) & valid;
+        const unsigned long long itemStraddle = __ldg(&p.itemViews[pk].straddle) & itemViews;
+        const CrSegment* sg = p.segments + it.seg;
+        const uint32_t numTri = __ldg(&sg->numTriangles);
+        const GeomRef geo = geom_of_t<PACKED>(sg);
+        const TileSrc ts = source(pk);
+        const bool tma = ts.src != nullptr;
+        const bool local = ts.local;
+        const uint32_t tri0 = it.batch * CR_BATCH;
+        if (tma) {
+            const bool ok =
+                __all_sync(FULL, mbar_wait_bounded(&s_bar[w][slot], (parity & bit) ? 1u : 0u, p.waitTimeoutNs));
+            if (!ok) {
+                if (lane == 0) atomicOr(&p.counters[CR_CTR_TIMEOUT], 1ull);
+                break;
+            }
+            parity ^= bit;
+            pending &= ~bit;
+        }
+        const uint32_t* tile = s_idx[w][slot];
+        auto index_of = [&](uint32_t pos, int c) -> uint32_t {
+            if (local) return tile[(tile[CR_LOCAL_MAX + pos] >> (8 * c)) & 0xffu];
+            if (tma) return tile[3 * pos + c];
+            return geom_index(geo, 3ull * (tri0 + pos) + c);
+        };
+        bool act[S1_R];
+#pragma unroll
+        for (int r = 0; r < S1_R; ++r) act[r] = tri0 + r * 32 + lane < numTri;
+        const uint32_t first = __ldg(&sg->firstInstance);
+        const uint32_t ib = first + it.chunk * CR_INST_CHUNK;
+        const uint32_t ie = min(ib + CR_INST_CHUNK, first + __ldg(&sg->instanceCount));
+        const uint32_t nLocal = local ? __ldg(ldg_ptr(&sg->localCounts) + it.batch) : 0u;
+        float itemBox[6] = {0, 0, 0, 0, 0, 0};
+        const float* boxes = ldg_ptr(&sg->itemBoxes);
+        const bool hasBox = boxes != nullptr;
+        if (hasBox)
+            for (int j = 0; j < 6; ++j) itemBox[j] = __ldg(boxes + 6ull * it.batch + j);
+
+        // survivors: view << 12 | instance slot << 8 | tile position
+        uint32_t* ring = s_ring[w];
+        uint32_t qh = 0, qt = 0;
+        auto drain = [&](bool all) {
+            while (qt - qh >= 32u || (all && qt > qh)) {
+                const uint32_t j = qh + lane;
+                int res = S1_CULL;
+                uint32_t tri = 0, inst = 0, view = 0;
+                if (j < qt) {
+                    const uint32_t e = ring[j & (S1_RING - 1)];
+                    const uint32_t tp = e & 0xffu;
+                    inst = ib + ((e >> 8) & 0xfu);
+                    view = e >> 12;
+                    tri = tri0 + tp;
+                    const uint64_t vi = (uint64_t)view * p.numInstances + inst;
+                    const Target tg = target_of(p, view);
+                    const V3 pa = pos_of(geo, index_of(tp, 0));
+                    const V3 pb = pos_of(geo, index_of(tp, 1));
+                    const V3 pc = pos_of(geo, index_of(tp, 2));
+                    res = stage1_triangle(tg, tg.fa, load_mat(p.world_view + 4ull * vi), __ldg(p.flips + vi), pa, pb,
+                                          pc, __ldg(&p.instances[inst].cum) + tri);
+                }
+                qh = min(qh + 32u, qt);
+                const unsigned qmask = __ballot_sync(FULL, res == S1_QUEUE);
+                if (qmask) {  // warp-aggregated append, tv.cu:190-197, tagged with the view
+                    const int leader = __ffs(qmask) - 1;
+                    unsigned long long b = 0;
+                    if (lane == leader) b = atomicAdd(&p.counters[CR_CTR_NONTRIVIAL], (unsigned long long)__popc(qmask));
+                    b = __shfl_sync(FULL, b, leader);
+                    if (res == S1_QUEUE) {
+                        const uint64_t q = b + __popc(qmask & ((1u << lane) - 1u));
+                        if (q < p.ntCap)
+                            p.ntList[q] = ((uint64_t)view << CR_ENTRY_VIEW_SHIFT) | ((uint64_t)inst << 32) | tri;
+                        else atomicOr(&p.counters[CR_CTR_OVERFLOW], 1ull);
+                    }
+                }
+                __syncwarp();
+            }
+        };
+        for (uint32_t inst = ib; inst < ie; ++inst) {
+            unsigned long long todo = itemViews;
+            while (todo) {
+                const uint32_t view = (uint32_t)(__ffsll((long long)todo) - 1);
+                todo &= todo - 1ull;
+                bool culledR[S1_R];
+                const Target tg = target_of(p, view);
+                const Mat M = load_mat(p.world_view + 4ull * ((uint64_t)view * p.numInstances + inst));
+                if (local && records_pay(M, tg, itemBox, hasBox)) {
+                    const float Wf = (float)tg.W, Hf = (float)tg.H;
+                    const float Wm1 = (float)(tg.W - 1), Hm1 = (float)(tg.H - 1);
+                    uint32_t* rec = s_rec[w];
+                    if ((itemStraddle >> view) & 1ull) {
+                        for (uint32_t v = lane; v < nLocal; v += 32)
+                            rec[v] = vertex_cell32<true>(M, pos_of(geo, tile[v]), tg.fa, tg.f, Wf, Hf, Wm1, Hm1);
+                    } else {  // the item's box is inside this view's frustum
+                        for (uint32_t v = lane; v < nLocal; v += 64) {
+                            const uint32_t v2 = v + 32;
+                            const uint32_t r0 = vertex_cell32<false>(M, pos_of(geo, tile[v]), tg.fa, tg.f, Wf, Hf, Wm1, Hm1);
+                            const uint32_t r1 =
+                                v2 < nLocal ? vertex_cell32<false>(M, pos_of(geo, tile[v2]), tg.fa, tg.f, Wf, Hf, Wm1, Hm1)
+                                            : 0u;
+                            rec[v] = r0;
+                            if (v2 < nLocal) rec[v2] = r1;
+                        }
+                    }
+                    __syncwarp();
+                    const uint32_t* cw = tile + CR_LOCAL_MAX;
+#pragma unroll
+                    for (int r = 0; r < S1_R; ++r) {
+                        const uint32_t c = cw[r * 32 + lane];
+                        culledR[r] = !act[r] || cell32_culled(rec[c & 0xffu], rec[(c >> 8) & 0xffu], rec[(c >> 16) & 0xffu]);
+                    }
+                } else {
+                    // large on screen: every triangle through the full path
+                    // now, with this view's target and matrix for the warp
+                    const uint64_t vi = (uint64_t)view * p.numInstances + inst;
+                    const uint32_t flip = __ldg(p.flips + vi);
+                    const uint64_t cum = __ldg(&p.instances[inst].cum);
+                    const uint64_t entryHi = ((uint64_t)view << CR_ENTRY_VIEW_SHIFT) | ((uint64_t)inst << 32);
+#pragma unroll 1
+                    for (int r = 0; r < S1_R; ++r) {
+                        const uint32_t tp = r * 32 + lane;
+                        int res = S1_CULL;
+                        if (act[r]) {
+                            const V3 pa = pos_of(geo, index_of(tp, 0));
+                            const V3 pb = pos_of(geo, index_of(tp, 1));
+                            const V3 pc = pos_of(geo, index_of(tp, 2));
+                            res = stage1_triangle(tg, tg.fa, M, flip, pa, pb, pc, cum + tri0 + tp);
+                        }
+                        const unsigned qmask = __ballot_sync(FULL, res == S1_QUEUE);
+                        if (qmask) {
+                            const int leader = __ffs(qmask) - 1;
+                            unsigned long long b = 0;
+                            if (lane == leader)
+                                b = atomicAdd(&p.counters[CR_CTR_NONTRIVIAL], (unsigned long long)__popc(qmask));
+                            b = __shfl_sync(FULL, b, leader);
+                            if (res == S1_QUEUE) {
+                                const uint64_t q = b + __popc(qmask & ((1u << lane) - 1u));
+                                if (q < p.ntCap) p.ntList[q] = entryHi | (tri0 + tp);
+                                else atomicOr(&p.counters[CR_CTR_OVERFLOW], 1ull);
+                            }
+                        }
+                    }
+                    continue;
+                }
+#pragma unroll
+                for (int r = 0; r < S1_R; ++r) {
+                    const bool keep = !culledR[r];
+                    const unsigned m = __ballot_sync(FULL, keep);
+                    if (keep)
+                        ring[(qt + __popc(m & ((1u << lane) - 1u))) & (S1_RING - 1)] =
+                            (view << 12) | ((inst - ib) << 8) | (uint32_t)(r * 32 + lane);
+                    qt += __popc(m);
+                }
+                __syncwarp();
+                drain(false);
+            }
+        }
+        drain(true);
+
+        __syncwarp();
+        {  // refill this slot with the item STAGES ahead
+            const uint64_t nxt = pk + (uint64_t)STAGES * nw;
+            if (nxt < nItems) {
+                const TileSrc ns = source(nxt);
+                if (ns.src) {
+                    pending |= bit;
+                    if (lane == 0) {
+                        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                        bulk_load(s_idx[w][slot], ns.src, ns.bytes, &s_bar[w][slot]);
+                    }
+                }
+            }
+        }
+    }
+    for (int s = 0; s < STAGES; ++s)
+        if (pending & (1u << s)) (void)mbar_wait_bounded(&s_bar[w][s], (parity >> s) & 1u, p.waitTimeoutNs);
+}
+
 // Clears every view's visbuffer (resolve.cu:213-232); blockIdx.y is the view.
 __global__ void __launch_bounds__(256) k_clear_views(const CrView* views, unsigned long long* counters) {
     if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x < CR_CTR_COUNT) counters[threadIdx.x] = 0ull;
@@ -633,7 +898,7 @@ int cr_launch_clear_views(const CrFrameParams& p, uint64_t maxPixels, void* stre
 }
 
 int cr_launch_vertex_views(const CrFrameParams& p, const CrBatchShape& s, void* stream) {
-    if (p.numVChunks == 0 || p.numViews == 0) return 0;
+    if (p.numVChunks == 0 || p.numViews == 0 || p.cellMode == CR_REC_BOXES) return 0;
     uint64_t blocks = p.numVChunks;
     if (blocks > (uint64_t)s.vertexBlocks) blocks = (uint64_t)s.vertexBlocks;
     k_vertex_views<<<(unsigned)blocks, VV_THREADS, 0, (cudaStream_t)stream>>>(p);
@@ -657,6 +922,13 @@ int cr_launch_stage1_views(const CrFrameParams& p, const CrBatchShape& s, void* 
     if (blocks > (uint64_t)s.stage1Blocks) blocks = (uint64_t)s.stage1Blocks;
     const unsigned b = (unsigned)blocks;
     cudaStream_t st = (cudaStream_t)stream;
+    if (p.cellMode == CR_REC_BOXES && p.itemViews) {  // vertex lists (no vertex pass)
+        uint64_t lb = (p.numItems + 7) / 8;
+        if (lb > (uint64_t)s.numSMs * 3) lb = (uint64_t)s.numSMs * 3;
+        if (p.anyPacked) k_stage1_views_lists<8, 3, true><<<(unsigned)lb, 256, 0, st>>>(p);
+        else k_stage1_views_lists<8, 3, false><<<(unsigned)lb, 256, 0, st>>>(p);
+        return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    }
     // the register-capped variants let more blocks share an SM
     const bool capped = (uint64_t)s.stage1Blocks > (uint64_t)s.numSMs * (warps == 4 ? 4u : 2u);
     if (p.anyPacked) {
