@@ -65,7 +65,9 @@ __global__ void __launch_bounds__(THREADS) k_vertex(const CrFrameParams p) {
 //   chunks  a chunk whose box proves CR_OC_* bits for every vertex
 //           (classify_chunk: exact "behind", a sound subset of the sides) gets
 //           those bits as its records here, without its positions being read;
-//           the others are listed for the vertex pass.
+//           so does (with outcode records) a chunk wholly inside the frustum,
+//           whose every outcode is 0; the others are listed for the vertex
+//           pass.
 //   items   the item's box is classified for each instance of its chunk; an
 //           instance whose box is wholly behind or beyond one side has every
 //           triangle of the item culled by the reference's own tests
@@ -74,6 +76,9 @@ __global__ void __launch_bounds__(THREADS) k_vertex(const CrFrameParams p) {
 //           tv.cu:153-158).  Items with a surviving instance are appended
 //           (warp-aggregated) with the mask of those instances.
 // Skipping what the boxes prove cannot change the visbuffer.
+// A chunk class meaning "fill its records with 0" (wholly inside).
+constexpr uint32_t CR_FILL_ZERO = 0x100u;
+
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS) k_cull(const CrFrameParams p) {
     const int lane = threadIdx.x & 31;
@@ -97,7 +102,12 @@ __global__ void __launch_bounds__(THREADS) k_cull(const CrFrameParams p) {
                 const float* bx = cb + 6ull * cIdx;
                 const float blo[3] = {__ldg(bx), __ldg(bx + 1), __ldg(bx + 2)};
                 const float bhi[3] = {__ldg(bx + 3), __ldg(bx + 4), __ldg(bx + 5)};
-                cls = classify_box(load_mat(p.world_view + 4ull * lo), fa, p.f, blo, bhi) & CR_OC_MASK;
+                const uint32_t c = classify_box(load_mat(p.world_view + 4ull * lo), fa, p.f, blo, bhi);
+                // wholly behind / beyond a side: those outcode bits at every
+                // vertex; wholly inside: outcode 0 at every vertex (1-byte
+                // records only: cell records also need each vertex's cell)
+                if (c & CR_OC_MASK) cls = c & CR_OC_MASK;
+                else if ((c & CH_INSIDE) && p.cellMode == CR_REC_OUTCODES) cls = CR_FILL_ZERO;
             }
         }
         // classified chunks' records, written here by the whole warp (one
@@ -107,7 +117,7 @@ __global__ void __launch_bounds__(THREADS) k_cull(const CrFrameParams p) {
             const int j = __ffs(fillMask) - 1;
             fillMask &= fillMask - 1;
             const uint64_t gj = __shfl_sync(FULL, g, j);
-            const uint32_t cj = __shfl_sync(FULL, cls, j);
+            const uint32_t cj = __shfl_sync(FULL, cls, j) & CR_OC_MASK;  // CR_FILL_ZERO fills 0
             uint32_t lo = 0, hi = p.numInstances - 1;
             while (lo < hi) {
                 const uint32_t mid = (lo + hi + 1) >> 1;
