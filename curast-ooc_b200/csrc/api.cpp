@@ -588,6 +588,8 @@ cr_status cr_destroy(cr_context* ctx) {
     if (ctx->hCounters) cudaFreeHost(ctx->hCounters);
     if (ctx->frameCopied) cudaEventDestroy(ctx->frameCopied);
     if (ctx->frameDone) cudaEventDestroy(ctx->frameDone);
+    if (ctx->postDone) cudaEventDestroy(ctx->postDone);
+    if (ctx->postScratch) cudaFree(ctx->postScratch);
     for (cudaEvent_t& e : ctx->ev)
         if (e) cudaEventDestroy(e);
     for (cudaEvent_t& e : ctx->ring)
@@ -1064,6 +1066,67 @@ cr_status cr_drain_stage_times(cr_context* ctx, cr_stage_times* out) {
     }
     *out = ctx->folded;
     ctx->folded = cr_stage_times{};
+    return CR_OK;
+}
+
+cr_status cr_postprocess(cr_context* ctx, const cr_post_desc* d, void* stream_) {
+    if (!ctx || !d) return fail(CR_ERR_INVALID, "cr_postprocess: NULL argument");
+    if (!d->d_colorbuffer || !d->d_rgba) return fail(CR_ERR_INVALID, "cr_postprocess: NULL buffer");
+    if (d->width <= 0 || d->height <= 0 || (uint64_t)d->width * d->height >= (1ull << 31))
+        return fail(CR_ERR_INVALID, "cr_postprocess: bad size %dx%d", d->width, d->height);
+    CrPostParams p{};
+    p.colorbuffer = (const uint64_t*)d->d_colorbuffer;
+    p.W = d->width;
+    p.H = d->height;
+    p.p00 = d->proj00;
+    p.p11 = d->proj11;
+    p.edl = (d->flags & CR_POST_EDL) ? 1 : 0;
+    p.ssao = (d->flags & CR_POST_SSAO) ? 1 : 0;
+    p.background = d->background;
+    p.out = (uint32_t*)d->d_rgba;
+    if (d->mode == CR_POST_SCREENSHOT) {
+        if (d->window_width <= 0) return fail(CR_ERR_INVALID, "cr_postprocess: window_width must be positive");
+        p.mode = CR_POST_MODE_SCREENSHOT;
+        p.windowW = d->window_width;
+        p.outW = d->width;
+        p.outH = d->height;
+    } else if (d->mode == CR_POST_DISPLAY) {
+        if (d->out_width <= 0 || d->out_height <= 0 || d->width % d->out_width || d->height % d->out_height ||
+            d->width / d->out_width != d->height / d->out_height)
+            return fail(CR_ERR_INVALID, "cr_postprocess: the colorbuffer (%dx%d) must be an integer multiple of the "
+                        "display", d->width, d->height);
+        p.mode = CR_POST_MODE_DISPLAY;
+        p.windowW = d->out_width;
+        p.outW = d->out_width;
+        p.outH = d->out_height;
+    } else {
+        return fail(CR_ERR_INVALID, "cr_postprocess: unknown mode %d", d->mode);
+    }
+    cudaStream_t stream = (cudaStream_t)stream_;
+    CR_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    if (!ctx->postDone) {
+        CR_CUDA(cudaEventCreateWithFlags(&ctx->postDone, cudaEventDisableTiming), "post event");
+        CR_CUDA(cudaEventRecord(ctx->postDone, stream), "post event");
+    }
+    if (p.ssao) {
+        const size_t need = align_up((size_t)p.W * p.H * 8, 256) + (size_t)p.W * p.H * 4;
+        if (need > ctx->postCap) {
+            CR_CUDA(cudaDeviceSynchronize(), "post scratch resize");
+            ctx->dev_free(ctx->postScratch, ctx->postCap);
+            ctx->postScratch = nullptr;
+            ctx->postCap = 0;
+            cr_status s = ctx->dev_alloc(&ctx->postScratch, need, "post-processing scratch");
+            if (s) return s;
+            ctx->postCap = need;
+        }
+        p.occlusion = (uint64_t*)ctx->postScratch;
+        p.shade = (float*)((char*)ctx->postScratch + align_up((size_t)p.W * p.H * 8, 256));
+    }
+    // the scratch is shared: the previous post (any stream) must be done
+    CR_CUDA(cudaStreamWaitEvent(stream, ctx->postDone, 0), "post wait");
+    if (cr_launch_post(p, stream))
+        return fail(CR_ERR_CUDA, "post-processing launch: %s", cudaGetErrorString(cudaGetLastError()));
+    CR_CUDA(cudaEventRecord(ctx->postDone, stream), "post event");
     return CR_OK;
 }
 

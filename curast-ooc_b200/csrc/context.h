@@ -90,6 +90,10 @@ struct cr_context {
     size_t hFrameCap = 0;
     cudaEvent_t frameCopied = nullptr;
     cudaEvent_t frameDone = nullptr;  // last kernel of the previous frame
+    // post-processing scratch (SSAO occlusion + shade) and its last user
+    void* postScratch = nullptr;
+    size_t postCap = 0;
+    cudaEvent_t postDone = nullptr;
 
     // queues and per-vertex records
     uint8_t* outcodes = nullptr;  // vertex-pass output (bytes, cells or view masks)

@@ -237,6 +237,26 @@ struct CrResolveParams {
     uint64_t idLo, idHi;        // covered pixels are written only for ids in [idLo, idHi)
 };
 
+// Post-processing of the colorbuffer (post.cu): the reference's EDL, SSAO and
+// final resolves.
+#define CR_POST_MODE_SCREENSHOT 0   // kernel_resolve_colorbuffer_to_screenshot
+#define CR_POST_MODE_DISPLAY 1      // kernel_resolve_colorbuffer_to_opengl_2D
+#define CR_BACKGROUND_COLOR 0xffffffffu  // BACKGROUND_COLOR, HostDeviceInterface.h:37
+struct CrPostParams {
+    const uint64_t* colorbuffer;  // W*H: depth bits << 32 | RGBA8
+    int32_t W, H;
+    float p00, p11;               // proj[0][0], proj[1][1]
+    int32_t edl, ssao;            // 1: apply
+    int32_t mode;                 // CR_POST_MODE_*
+    int32_t windowW;              // screenshot: EDL distance = W / windowW
+    int32_t outW, outH;           // output size (display: W / outW = supersampling factor)
+    uint32_t background;
+    uint64_t* occlusion;          // W*H scratch (SSAO)
+    float* shade;                 // W*H scratch (SSAO)
+    uint32_t* out;                // outW*outH RGBA8
+};
+int cr_launch_post(const CrPostParams& p, void* stream);
+
 // Launch helpers implemented in raster.cu / resolve.cu.
 struct CrLaunchShape {
     int numSMs;

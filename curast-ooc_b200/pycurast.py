@@ -98,6 +98,29 @@ class CrCompressedMeshDesc(ctypes.Structure):
     ]
 
 
+class CrPostDesc(ctypes.Structure):
+    _fields_ = [
+        ("d_colorbuffer", _u64),
+        ("width", _i32),
+        ("height", _i32),
+        ("proj00", _f32),
+        ("proj11", _f32),
+        ("flags", _u32),
+        ("mode", _i32),
+        ("window_width", _i32),
+        ("out_width", _i32),
+        ("out_height", _i32),
+        ("background", _u32),
+        ("d_rgba", _u64),
+    ]
+
+
+CR_POST_EDL = 1
+CR_POST_SSAO = 2
+CR_POST_SCREENSHOT = 0
+CR_POST_DISPLAY = 1
+
+
 class CrInstance(ctypes.Structure):
     _fields_ = [("mesh", _u32), ("reserved", _u32), ("world", _f32 * 16)]
 
@@ -267,6 +290,7 @@ EXPORTS = {
     "cr_render": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrInstance), _u32, ctypes.POINTER(CrCamera), _u64, _u64,
                          _u64, _i32, _u32, ctypes.c_void_p]),
     "cr_last_frame_stats": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrFrameStats)]),
+    "cr_postprocess": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrPostDesc), ctypes.c_void_p]),
     "cr_sync": (_i32, [ctypes.c_void_p]),
     "cr_mat4_mul": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "cr_order_instances": (_i32, [ctypes.c_void_p, ctypes.c_void_p, _u32, _u32, ctypes.c_void_p, ctypes.c_void_p]),
@@ -652,6 +676,22 @@ class Context:
         out = _u32()
         _check(load().cr_mesh_create(self.h, ctypes.byref(d), ctypes.byref(out)))
         return out.value
+
+    def postprocess(self, d_colorbuffer, width, height, proj, d_rgba, flags, mode=CR_POST_SCREENSHOT,
+                    window_width=None, out_size=None, background=0xFFFFFFFF, stream=0):
+        """cr_postprocess: EDL / SSAO and the screenshot or display resolve."""
+        d = CrPostDesc()
+        d.d_colorbuffer = int(d_colorbuffer)
+        d.width, d.height = int(width), int(height)
+        d.proj00, d.proj11 = float(proj[0]), float(proj[5])
+        d.flags = int(flags)
+        d.mode = int(mode)
+        d.window_width = int(window_width if window_width else width)
+        ow, oh = out_size if out_size else (width, height)
+        d.out_width, d.out_height = int(ow), int(oh)
+        d.background = int(background)
+        d.d_rgba = int(d_rgba)
+        _check(load().cr_postprocess(self.h, ctypes.byref(d), ctypes.c_void_p(int(stream))))
 
     def mesh_compressed(self, comp, colors=None):
         """Uploads a compressed mesh (a Compressed from compress_mesh)."""

@@ -253,6 +253,40 @@ cr_status cr_render(cr_context* ctx, const cr_instance* instances, uint32_t coun
                     const cr_camera* camera, uint64_t d_visbuffer, uint64_t d_rgba,
                     uint64_t d_colorbuffer, int32_t display, uint32_t flags, void* stream);
 
+/* ---- post-processing ----------------------------------------------------
+ * The reference's image pass after the colour resolve, on the colorbuffer
+ * cr_render writes (d_colorbuffer): eye-dome lighting (getEdlShadingFactor,
+ * src/kernels/resolve.cu:234-268), screen-space ambient occlusion
+ * (kernel_ssaoOcclusion / kernel_ssaoBlur, resolve.cu:549-640) and one of its
+ * two final resolves:
+ *   CR_POST_SCREENSHOT  kernel_resolve_colorbuffer_to_screenshot
+ *                       (resolve.cu:1264-1313): out = width x height, EDL
+ *                       distance width / window_width
+ *   CR_POST_DISPLAY     kernel_resolve_colorbuffer_to_opengl_2D
+ *                       (resolve.cu:1143-1260) with a device RGBA8 buffer in
+ *                       place of the OpenGL surface: out_width x out_height,
+ *                       the colorbuffer an integer multiple of it (>1:
+ *                       supersampling, factor x factor blocks averaged).
+ * SSAO scratch (12 bytes per colorbuffer pixel) is owned by the context;
+ * posts issued on different streams are ordered by the library. */
+#define CR_POST_EDL 1u
+#define CR_POST_SSAO 2u
+#define CR_POST_SCREENSHOT 0
+#define CR_POST_DISPLAY 1
+typedef struct cr_post_desc {
+    uint64_t d_colorbuffer;    /* width*height uint64: depth bits << 32 | RGBA8  */
+    int32_t width, height;     /* of the colorbuffer                             */
+    float proj00, proj11;      /* the camera's proj[0] and proj[5]               */
+    uint32_t flags;            /* CR_POST_EDL | CR_POST_SSAO                     */
+    int32_t mode;              /* CR_POST_SCREENSHOT or CR_POST_DISPLAY          */
+    int32_t window_width;      /* SCREENSHOT: the window width (EDL distance)    */
+    int32_t out_width;         /* DISPLAY: the display size                      */
+    int32_t out_height;
+    uint32_t background;       /* colour of pixels with no triangle              */
+    uint64_t d_rgba;           /* output RGBA8                                   */
+} cr_post_desc;
+cr_status cr_postprocess(cr_context* ctx, const cr_post_desc* desc, void* stream);
+
 /* Statistics of the last frame rendered with CR_RENDER_SYNC (or after
  * cr_sync). */
 cr_status cr_last_frame_stats(cr_context* ctx, cr_frame_stats* out);

@@ -66,6 +66,8 @@ def oracle():
         lib.orc_clear.argtypes = [_vp, _u64]
         lib.orc_mat4_mul.restype = None
         lib.orc_mat4_mul.argtypes = [_vp, _vp, _vp]
+        lib.orc_post.restype = _i32
+        lib.orc_post.argtypes = [_vp, _i32, _i32, _f32, _f32, _i32, _i32, _i32, _i32, _i32, _i32, _u32, _vp, _i32]
         _orc = lib
     return _orc
 
@@ -156,6 +158,8 @@ def harness():
         lib.refh_frame.restype = _i32
         lib.refh_frame.argtypes = [_vp, _vp, _u32, _vp, _vp, _i32, _i32, _i32, _i32, _u64, _u64, _i32, _vp, _vp,
                                    _vp, _vp, _vp]
+        lib.refh_post.restype = _i32
+        lib.refh_post.argtypes = [_vp, _i32, _i32, _vp, _i32, _i32, _i32, _i32, _i32, _i32, _u32, _vp]
         lib.refh_mat4_mul.restype = None
         lib.refh_mat4_mul.argtypes = [_vp, _vp, _vp]
         lib.refh_sizeof_cmesh.restype = _i32
@@ -199,6 +203,19 @@ class Reference:
         if h < 0:
             raise RuntimeError(f"refh_mesh_host: {h} {self.lib.refh_last_error().decode()}")
         return h
+
+    def post(self, colorbuffer, W, H, proj, edl, ssao, mode=0, window_width=None, out_size=None,
+             background=0xFFFFFFFF):
+        """The reference's post-processing kernels on a host colorbuffer."""
+        cb = np.ascontiguousarray(colorbuffer, np.uint64)
+        pr = np.ascontiguousarray(np.asarray(proj, np.float32).reshape(16))
+        ow, oh = out_size if out_size else (W, H)
+        out = np.empty((W * H) if mode == 0 else (ow * oh), np.uint32)
+        rc = self.lib.refh_post(cb.ctypes.data, W, H, pr.ctypes.data, int(edl), int(ssao), int(mode),
+                                int(window_width or W), int(ow), int(oh), int(background), out.ctypes.data)
+        if rc != 0:
+            raise RuntimeError(f"refh_post: {rc} {self.lib.refh_last_error().decode()}")
+        return out
 
     def mesh_compressed_host(self, packed, qpos, nT, col, aabb_min, aabb_max, index_min, index_max):
         packed = np.ascontiguousarray(packed, np.uint32)
@@ -297,3 +314,17 @@ def decode_compressed(packed, num_indices, index_min, index_max, qpos, aabb_min,
     cf = (np.asarray(aabb_max, np.float32) - mn) / np.float32(65536.0)
     pos = np.asarray(qpos, np.uint16).astype(np.float32) * cf + mn
     return pos.astype(np.float32), idx.astype(np.uint32).reshape(-1, 3)
+
+
+def post(colorbuffer, W, H, proj, edl, ssao, mode=0, window_width=None, out_size=None, background=0xFFFFFFFF,
+         nthreads=0):
+    """CPU restatement of the reference's EDL / SSAO post-processing and its
+    screenshot (mode 0) or display (mode 1) resolve; returns RGBA8."""
+    cb = np.ascontiguousarray(colorbuffer, np.uint64)
+    ow, oh = out_size if out_size else (W, H)
+    out = np.empty((W * H) if mode == 0 else (ow * oh), np.uint32)
+    rc = oracle().orc_post(cb.ctypes.data, W, H, float(proj[0]), float(proj[5]), int(edl), int(ssao), int(mode),
+                           int(window_width or W), int(ow), int(oh), int(background), out.ctypes.data, nthreads)
+    if rc != 0:
+        raise RuntimeError(f"orc_post: {rc}")
+    return out

@@ -880,3 +880,255 @@ int orc_resolve(const orc_instance* inst, uint32_t nInst, const uint64_t* prefix
     }
     return 0;
 }
+
+/* ------------------------------------------------------------------------
+ * Post-processing of the colorbuffer -- CPU restatement of the reference's
+ * getEdlShadingFactor (resolve.cu:234-268), ssao_viewPos / ssao_normal /
+ * getSSAOShadingFactor (resolve.cu:276-470), kernel_ssaoOcclusion /
+ * kernel_ssaoBlur (resolve.cu:549-640), kernel_resolve_colorbuffer_to_screenshot
+ * (resolve.cu:1264-1313) and kernel_resolve_colorbuffer_to_opengl_2D
+ * (resolve.cu:1143-1260, its surface a plain RGBA8 array).  Float operations
+ * in the reference's order; transcendental functions from libm.
+ * ------------------------------------------------------------------------ */
+typedef struct { float x, y, z; } p3;
+static inline p3 p3add(p3 a, p3 b) { p3 r = {a.x + b.x, a.y + b.y, a.z + b.z}; return r; }
+static inline p3 p3sub(p3 a, p3 b) { p3 r = {a.x - b.x, a.y - b.y, a.z - b.z}; return r; }
+static inline p3 p3mul(p3 a, float s) { p3 r = {a.x * s, a.y * s, a.z * s}; return r; }
+static inline float p3dot(p3 a, p3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+static inline p3 p3cross(p3 x, p3 y) {
+    p3 r = {x.y * y.z - y.y * x.z, x.z * y.x - y.z * x.x, x.x * y.y - y.x * x.y};
+    return r;
+}
+static inline p3 p3norm(p3 v) { return p3mul(v, 1.0f / sqrtf(p3dot(v, v))); }
+static inline int iclampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+/* the GPU's float -> int conversion: truncation, saturating, NaN -> 0 */
+static inline int f2i_rz(float v) {
+    if (v != v) return 0;
+    if (v >= 2147483647.0f) return 2147483647;
+    if (v <= -2147483648.0f) return (int)0x80000000u;
+    return (int)v;
+}
+
+typedef struct {
+    const uint64_t* cb;
+    int W, H;
+    float p00, p11;
+} orc_post_src;
+
+static inline float post_depth(const orc_post_src* s, int pid) {
+    union { uint32_t u; float f; } c;
+    c.u = (uint32_t)(s->cb[pid] >> 32);
+    return c.f;
+}
+
+static float post_edl(const orc_post_src* s, float depth, int x, int y, int distance) {
+    float sum = 0.0f;
+    const int numSamples = 8;
+    for (int i = 0; i < numSamples; i++) {
+        const float u = 2.0f * 3.1415f * (float)i / (float)numSamples;
+        const float dx = (float)distance * cosf(u);
+        const float dy = (float)distance * sinf(u);
+        const int nx = f2i_rz((float)x + dx), ny = f2i_rz((float)y + dy);
+        float nd = INFINITY;
+        if (nx >= 0 && nx < s->W && ny >= 0 && ny < s->H) nd = post_depth(s, nx + s->W * ny);
+        sum += fmaxf(log2f(depth) - log2f(nd), 0.0f);
+    }
+    const float response = sum / (float)numSamples;
+    const float edlStrength = 0.9f;
+    float shade = expf(-response * 300.0f * edlStrength);
+    shade = clampf_ref(shade, 0.3f, 1.0f);
+    return shade * 0.8f + 0.2f;
+}
+
+static inline p3 post_view_pos(const orc_post_src* s, float px, float py, float depth) {
+    const float ndc_x = (2.0f * (px + 0.5f) / (float)s->W) - 1.0f;
+    const float ndc_y = (2.0f * (py + 0.5f) / (float)s->H) - 1.0f;
+    p3 r = {ndc_x * depth / s->p00, ndc_y * depth / s->p11, depth};
+    return r;
+}
+
+static inline float post_dep(const orc_post_src* s, int nx, int ny) {
+    return post_depth(s, iclampi(ny, 0, s->H - 1) * s->W + iclampi(nx, 0, s->W - 1));
+}
+
+static p3 post_normal(const orc_post_src* s, int x, int y, float d0) {
+    const float dr = post_dep(s, x + 1, y), dl = post_dep(s, x - 1, y);
+    const float dd = post_dep(s, x, y + 1), du = post_dep(s, x, y - 1);
+    const int use_right = fabsf(dr - d0) < fabsf(d0 - dl);
+    const int use_down = fabsf(dd - d0) < fabsf(d0 - du);
+    const int sx = use_right ? +1 : -1, sy = use_down ? +1 : -1;
+    const float dh = use_right ? dr : dl, dv = use_down ? dd : du;
+    if (isinf(dh) || isinf(dv)) { p3 r = {0.0f, 0.0f, -1.0f}; return r; }
+    const p3 P = post_view_pos(s, (float)x, (float)y, d0);
+    const p3 Ph = post_view_pos(s, (float)(x + sx), (float)y, dh);
+    const p3 Pv = post_view_pos(s, (float)x, (float)(y + sy), dv);
+    const p3 dPh = (sx > 0) ? p3sub(Ph, P) : p3sub(P, Ph);
+    const p3 dPv = (sy > 0) ? p3sub(Pv, P) : p3sub(P, Pv);
+    p3 N = p3norm(p3cross(dPh, dPv));
+    if (N.z > 0.0f) { N.x = -N.x; N.y = -N.y; N.z = -N.z; }
+    return N;
+}
+
+static float post_ssao(const orc_post_src* s, float center_depth, int x, int y) {
+    if (isinf(center_depth) || center_depth <= 0.0f) return 1.0f;
+    const int NUM_SAMPLES = 32;
+    const float RADIUS_FRACTION = 0.2025f, INTENSITY = 1.1f, RANGE_MUL = 2.5f, BIAS_FRACTION = 0.05f;
+    const float world_radius = center_depth * RADIUS_FRACTION;
+    const float bias = BIAS_FRACTION * world_radius;
+    const p3 P = post_view_pos(s, (float)x, (float)y, center_depth);
+    const p3 N = post_normal(s, x, y, center_depth);
+    const float dz_left = center_depth - post_dep(s, x - 1, y);
+    const float dz_right = post_dep(s, x + 1, y) - center_depth;
+    const float dz_up = center_depth - post_dep(s, x, y - 1);
+    const float dz_down = post_dep(s, x, y + 1) - center_depth;
+    const float dz_dx = (fabsf(dz_left) < fabsf(dz_right)) ? dz_left : dz_right;
+    const float dz_dy = (fabsf(dz_up) < fabsf(dz_down)) ? dz_up : dz_down;
+    p3 up;
+    if (fabsf(N.z) < 0.95f) { up.x = 0.0f; up.y = 0.0f; up.z = 1.0f; }
+    else { up.x = 1.0f; up.y = 0.0f; up.z = 0.0f; }
+    const p3 T = p3norm(p3cross(up, N));
+    const p3 B = p3cross(N, T);
+    uint32_t h = (uint32_t)x * 2246822519u ^ (uint32_t)y * 3266489917u;
+    h ^= h >> 13;
+    h *= 0xbf58476du;
+    h ^= h >> 31;
+    const float rand_angle = (float)(h >> 8) * (6.28318530f / (float)(1 << 24));
+    float occlusion = 0.0f;
+    const float INV_N = 1.0f / (float)NUM_SAMPLES;
+    const float GOLDEN_ANGLE = 2.39996323f;
+    for (int i = 0; i < NUM_SAMPLES; ++i) {
+        const float fi = ((float)i + 0.5f) * INV_N;
+        const float sin_theta = sqrtf(fi);
+        const float cos_theta = sqrtf(1.0f - fi);
+        const float phi = (float)i * GOLDEN_ANGLE + rand_angle;
+        const p3 dir = p3add(p3add(p3mul(T, sin_theta * cosf(phi)), p3mul(B, sin_theta * sinf(phi))), p3mul(N, cos_theta));
+        const float r = world_radius * sqrtf((float)(i + 1) * INV_N);
+        const p3 S = p3add(P, p3mul(dir, r));
+        if (S.z <= 0.001f) continue;
+        const float inv_z = 1.0f / S.z;
+        const float spx = ((s->p00 * S.x * inv_z) + 1.0f) * 0.5f * (float)s->W - 0.5f;
+        const float spy = ((s->p11 * S.y * inv_z) + 1.0f) * 0.5f * (float)s->H - 0.5f;
+        const int sx = iclampi(f2i_rz(spx), 0, s->W - 1);
+        const int sy = iclampi(f2i_rz(spy), 0, s->H - 1);
+        const float actual_depth = post_depth(s, sy * s->W + sx);
+        if (isinf(actual_depth)) continue;
+        const float dx = spx - (float)x, dy = spy - (float)y;
+        const float expected_z = center_depth + dz_dx * dx + dz_dy * dy;
+        const float dz = expected_z - actual_depth;
+        if (dz > bias && dz < world_radius * RANGE_MUL) {
+            const float range_falloff = 1.0f - dz / (world_radius * RANGE_MUL);
+            occlusion += range_falloff * cos_theta;
+        }
+    }
+    return clampf_ref(1.0f - occlusion * INV_N * INTENSITY, 0.0f, 1.0f);
+}
+
+static uint32_t post_shade_pixel(const orc_post_src* s, const float* shadeBuf, int edl, int ssao, int x, int y,
+                                 int edlDistance, uint32_t background) {
+    const int pid = x + s->W * y;
+    const uint64_t pixel = s->cb[pid];
+    const float depth = post_depth(s, pid);
+    uint32_t color = (uint32_t)(pixel & 0xffffffffu);
+    float e = 1.0f, a = 1.0f;
+    if (edl) e = post_edl(s, depth, x, y, edlDistance);
+    if (ssao) a = shadeBuf[pid] * 0.4f + 0.6f;
+    if (isinf(depth)) color = background;
+    const float shade = e * a;
+    uint32_t out = color & 0xff000000u;
+    for (int k = 0; k < 3; ++k) {
+        const float c = shade * (float)((color >> (8 * k)) & 0xffu);
+        out |= ((uint32_t)(uint8_t)c) << (8 * k);
+    }
+    return out;
+}
+
+/* mode 0: screenshot (out W x H, EDL distance W / windowW); mode 1: display
+ * (out outW x outH, W / outW supersampling).  Returns 0. */
+int orc_post(const uint64_t* cb, int W, int H, float p00, float p11, int edl, int ssao, int mode, int windowW, int outW,
+             int outH, uint32_t background, uint32_t* out, int nthreads) {
+    set_threads(nthreads);
+    orc_post_src s = {cb, W, H, p00, p11};
+    float* shadeBuf = NULL;
+    if (ssao) {
+        uint64_t* occ = (uint64_t*)malloc((size_t)W * H * 8);
+        shadeBuf = (float*)malloc((size_t)W * H * 4);
+        if (!occ || !shadeBuf) { free(occ); free(shadeBuf); return -1; }
+#pragma omp parallel for schedule(dynamic, 16)
+        for (int y = 0; y < H; y++)
+            for (int x = 0; x < W; x++) {
+                const int pid = x + W * y;
+                const float depth = post_depth(&s, pid);
+                const float a = post_ssao(&s, depth, x, y);
+                union { float f; uint32_t u; } dz, az;
+                dz.f = depth;
+                az.f = a;
+                occ[pid] = ((uint64_t)dz.u << 32) | az.u;
+            }
+        static const float gaussian[7] = {0.015625f, 0.09375f, 0.234375f, 0.3125f, 0.234375f, 0.09375f, 0.015625f};
+#pragma omp parallel for schedule(static)
+        for (int y = 0; y < H; y++)
+            for (int x = 0; x < W; x++) {
+                const int c = y * W + x;
+                union { uint32_t u; float f; } cd;
+                cd.u = (uint32_t)(occ[c] >> 32);
+                if (isinf(cd.f)) { shadeBuf[c] = 1.0f; continue; }
+                float sum = 0.0f, tw = 0.0f;
+                for (int dy = -3; dy <= 3; dy++)
+                    for (int dx = -3; dx <= 3; dx++) {
+                        const int nx = iclampi(x + dx, 0, W - 1), ny = iclampi(y + dy, 0, H - 1);
+                        union { uint32_t u; float f; } so;
+                        so.u = (uint32_t)(occ[ny * W + nx] & 0xffffffffu);
+                        const float w = gaussian[dx + 3] * gaussian[dy + 3] * 1.0f;
+                        sum += w * so.f;
+                        tw += w;
+                    }
+                shadeBuf[c] = tw > 0.0f ? sum / tw : 1.0f;
+            }
+        free(occ);
+    }
+    if (mode == 0) {
+#pragma omp parallel for schedule(static)
+        for (int y = 0; y < H; y++)
+            for (int x = 0; x < W; x++) out[x + W * y] = post_shade_pixel(&s, shadeBuf, edl, ssao, x, y, W / windowW, background);
+    } else if (outW == W && outH == H) {
+#pragma omp parallel for schedule(static)
+        for (int y = 0; y < H; y++)
+            for (int x = 0; x < W; x++) out[x + W * y] = post_shade_pixel(&s, shadeBuf, edl, ssao, x, y, 1, background);
+    } else {
+        const int f = W / outW;
+#pragma omp parallel for schedule(static)
+        for (int ty = 0; ty < outH; ty++)
+            for (int tx = 0; tx < outW; tx++) {
+                float cr = 0.0f, cg = 0.0f, cbl = 0.0f, e = 0.0f, a = 0.0f;
+                int n = 0;
+                for (int dx = 0; dx < f; dx++)
+                    for (int dy = 0; dy < f; dy++) {
+                        const int sx = f * tx + dx, sy = f * ty + dy, sp = sx + W * sy;
+                        const float depth = post_depth(&s, sp);
+                        const uint32_t C = (uint32_t)(cb[sp] & 0xffffffffu);
+                        cr += (float)((C >> 0) & 0xff);
+                        cg += (float)((C >> 8) & 0xff);
+                        cbl += (float)((C >> 16) & 0xff);
+                        if (isinf(depth)) {
+                            cr += (float)((0xffffffffu >> 0) & 0xff);
+                            cg += (float)((0xffffffffu >> 8) & 0xff);
+                            cbl += (float)((0xffffffffu >> 16) & 0xff);
+                        }
+                        if (edl) e += post_edl(&s, depth, sx, sy, f);
+                        if (ssao) a += shadeBuf[sp];
+                        n++;
+                    }
+                e = edl ? e / (float)n : 1.0f;
+                a = ssao ? a / (float)n : 1.0f;
+                const float shade = e * a;
+                cr = shade * cr / (float)n;
+                cg = shade * cg / (float)n;
+                cbl = shade * cbl / (float)n;
+                out[tx + outW * ty] = (uint32_t)(uint8_t)clampf_ref(cr, 0.0f, 255.0f) |
+                                      ((uint32_t)(uint8_t)clampf_ref(cg, 0.0f, 255.0f) << 8) |
+                                      ((uint32_t)(uint8_t)clampf_ref(cbl, 0.0f, 255.0f) << 16) | 0xff000000u;
+            }
+    }
+    free(shadeBuf);
+    return 0;
+}

@@ -60,6 +60,7 @@ struct Driver {
     FN(cuOccupancyMaxActiveBlocksPerMultiprocessor) FN(cuDeviceGetAttribute) FN(cuEventCreate)
     FN(cuEventRecord) FN(cuEventSynchronize) FN(cuEventElapsedTime) FN(cuEventDestroy)
     FN(cuGetErrorString) FN(cuMemcpyHtoDAsync) FN(cuMemsetD8Async)
+    FN(cuArray3DCreate) FN(cuArrayDestroy) FN(cuSurfObjectCreate) FN(cuSurfObjectDestroy) FN(cuMemcpy2D)
 #undef FN
     bool load() {
         if (h) return true;
@@ -74,6 +75,7 @@ struct Driver {
         LD(cuOccupancyMaxActiveBlocksPerMultiprocessor) LD(cuDeviceGetAttribute) LD(cuEventCreate)
         LD(cuEventRecord) LD(cuEventSynchronize) LD(cuEventElapsedTime) LD(cuEventDestroy)
         LD(cuGetErrorString) LD(cuMemcpyHtoDAsync) LD(cuMemsetD8Async)
+        LD(cuArray3DCreate) LD(cuArrayDestroy) LD(cuSurfObjectCreate) LD(cuSurfObjectDestroy) LD(cuMemcpy2D)
 #undef LD
         return true;
     }
@@ -86,6 +88,7 @@ CUmodule g_mod_tv = nullptr, g_mod_resolve = nullptr;
 CUfunction g_stage1 = nullptr, g_stage1_inst = nullptr, g_stage2 = nullptr, g_stage3 = nullptr;
 CUfunction g_stage1c = nullptr, g_stage1c_inst = nullptr, g_stage2c = nullptr, g_stage3c = nullptr;
 CUfunction g_clear = nullptr, g_resolve = nullptr, g_screenshot = nullptr;
+CUfunction g_ssaoOcc = nullptr, g_ssaoBlur = nullptr, g_display = nullptr;
 int g_numSMs = 0;
 char g_err[1024] = {0};
 
@@ -185,6 +188,9 @@ int refh_init(const char* dir, const char* mode, int device) {
     CK(g_drv.p_cuModuleGetFunction(&g_clear, g_mod_resolve, "kernel_clearFramebuffer"));
     CK(g_drv.p_cuModuleGetFunction(&g_resolve, g_mod_resolve, "kernel_resolve_visbuffer_to_colorbuffer2D"));
     CK(g_drv.p_cuModuleGetFunction(&g_screenshot, g_mod_resolve, "kernel_resolve_colorbuffer_to_screenshot"));
+    CK(g_drv.p_cuModuleGetFunction(&g_ssaoOcc, g_mod_resolve, "kernel_ssaoOcclusion"));
+    CK(g_drv.p_cuModuleGetFunction(&g_ssaoBlur, g_mod_resolve, "kernel_ssaoBlur"));
+    CK(g_drv.p_cuModuleGetFunction(&g_display, g_mod_resolve, "kernel_resolve_colorbuffer_to_opengl_2D"));
     return 0;
 }
 
@@ -465,6 +471,95 @@ int refh_frame(const int32_t* meshIds, const float* worlds, uint32_t nInst, cons
     }
     return 0;
 #undef CKC
+}
+
+// The reference's post-processing of a colorbuffer (host array, W*H): SSAO
+// (kernel_ssaoOcclusion + kernel_ssaoBlur) when `ssao`, then the screenshot
+// resolve (mode 0, out W*H) or the display resolve (mode 1) written to a CUDA
+// array through a surface object, as the OpenGL surface it normally writes
+// (out outW*outH).  proj: the camera's 16 floats.
+int refh_post(const uint64_t* colorbuffer, int W, int H, const float* proj, int edl, int ssao, int mode, int windowW,
+              int outW, int outH, uint32_t background, uint32_t* out) {
+    if (W <= 0 || H <= 0) return -3;
+    CK(g_drv.p_cuCtxSetCurrent(g_ctx));
+    const uint64_t P = (uint64_t)W * H;
+    CUdeviceptr d_cb = 0, d_occ = 0, d_shade = 0, d_shot = 0, d_state = 0;
+    CUarray arr = nullptr;
+    CUsurfObject surf = 0;
+    auto cleanup = [&]() {
+        CUdeviceptr ps[] = {d_cb, d_occ, d_shade, d_shot, d_state};
+        for (CUdeviceptr q : ps)
+            if (q) g_drv.p_cuMemFree(q);
+        if (surf) g_drv.p_cuSurfObjectDestroy(surf);
+        if (arr) g_drv.p_cuArrayDestroy(arr);
+    };
+#define CKP(call)                   \
+    do {                            \
+        int _q = [&]() -> int { CK(call); return 0; }(); \
+        if (_q) { cleanup(); return _q; } \
+    } while (0)
+    CKP(g_drv.p_cuMemAlloc(&d_cb, P * 8));
+    CKP(g_drv.p_cuMemcpyHtoD(d_cb, colorbuffer, P * 8));
+    CKP(g_drv.p_cuMemAlloc(&d_occ, P * 8));
+    CKP(g_drv.p_cuMemAlloc(&d_shade, P * 4));
+    CKP(g_drv.p_cuMemAlloc(&d_state, sizeof(DeviceState)));
+    CKP(g_drv.p_cuMemsetD8(d_state, 0, sizeof(DeviceState)));
+    RenderTarget target;
+    memset(&target, 0, sizeof(target));
+    target.colorbuffer = (uint64_t*)d_cb;
+    target.width = W;
+    target.height = H;
+    memcpy(&target.proj, proj, 64);
+    CUdeviceptr d_ctarget = 0;
+    size_t ctsz = 0;
+    CKP(g_drv.p_cuModuleGetGlobal(&d_ctarget, &ctsz, g_mod_resolve, "c_target"));
+    CKP(g_drv.p_cuMemcpyHtoD(d_ctarget, &target, sizeof(target)));
+    if (ssao) {
+        void* a[] = {&d_occ, &d_shade};
+        CKP(g_drv.p_cuLaunchKernel(g_ssaoOcc, (W + 15) / 16, (H + 15) / 16, 1, 16, 16, 1, 0, 0, a, nullptr));
+        CKP(g_drv.p_cuLaunchKernel(g_ssaoBlur, (W + 15) / 16, (H + 15) / 16, 1, 16, 16, 1, 0, 0, a, nullptr));
+    }
+    bool bEdl = edl != 0, bSsao = ssao != 0;
+    if (mode == 0) {
+        CKP(g_drv.p_cuMemAlloc(&d_shot, P * 4));
+        int wh = (int)((int64_t)windowW * H / W);
+        void* a[] = {&d_shot, &d_shade, &bEdl, &bSsao, &windowW, &wh, &background};
+        CKP(g_drv.p_cuLaunchKernel(g_screenshot, (W + 15) / 16, (H + 15) / 16, 1, 16, 16, 1, 0, 0, a, nullptr));
+        CKP(g_drv.p_cuCtxSynchronize());
+        CKP(g_drv.p_cuMemcpyDtoH(out, d_shot, P * 4));
+    } else {
+        CUDA_ARRAY3D_DESCRIPTOR ad;
+        memset(&ad, 0, sizeof(ad));
+        ad.Width = (size_t)outW;
+        ad.Height = (size_t)outH;
+        ad.Depth = 0;
+        ad.Format = CU_AD_FORMAT_UNSIGNED_INT8;
+        ad.NumChannels = 4;
+        ad.Flags = CUDA_ARRAY3D_SURFACE_LDST;
+        CKP(g_drv.p_cuArray3DCreate(&arr, &ad));
+        CUDA_RESOURCE_DESC rd;
+        memset(&rd, 0, sizeof(rd));
+        rd.resType = CU_RESOURCE_TYPE_ARRAY;
+        rd.res.array.hArray = arr;
+        CKP(g_drv.p_cuSurfObjectCreate(&surf, &rd));
+        int mouse = -1;
+        void* a[] = {&surf, &d_shade, &outW, &outH, &mouse, &mouse, &d_state, &bEdl, &bSsao, &background};
+        CKP(g_drv.p_cuLaunchKernel(g_display, (outW + 15) / 16, (outH + 15) / 16, 1, 16, 16, 1, 0, 0, a, nullptr));
+        CKP(g_drv.p_cuCtxSynchronize());
+        CUDA_MEMCPY2D cp;
+        memset(&cp, 0, sizeof(cp));
+        cp.srcMemoryType = CU_MEMORYTYPE_ARRAY;
+        cp.srcArray = arr;
+        cp.dstMemoryType = CU_MEMORYTYPE_HOST;
+        cp.dstHost = out;
+        cp.dstPitch = (size_t)outW * 4;
+        cp.WidthInBytes = (size_t)outW * 4;
+        cp.Height = (size_t)outH;
+        CKP(g_drv.p_cuMemcpy2D(&cp));
+    }
+    cleanup();
+    return 0;
+#undef CKP
 }
 
 }  // extern "C"
