@@ -487,6 +487,23 @@ const cr_tuning* find_tuning(const cr_context* ctx, uint32_t sceneClass) {
 
 }  // namespace cr
 
+namespace cr {
+void quantize_positions(const float* positions, uint32_t num_vertices, const float* mn, const float* mx,
+                        uint16_t* out) {
+    float size[3];
+    for (int j = 0; j < 3; j++) size[j] = mx[j] - mn[j];  // vec3 aabbSize = max - min (float)
+    for (uint32_t v = 0; v < num_vertices; v++)
+        for (int j = 0; j < 3; j++) {
+            uint16_t q = 0;
+            if (size[j] > 0.0f) {  // src/LargeGlbLoader.h:666-668
+                const double x = 65536.0 * (double)(positions[3ull * v + j] - mn[j]) / (double)size[j];
+                q = (uint16_t)std::min(std::max(x, 0.0), 65535.0);
+            }
+            out[3ull * v + j] = q;
+        }
+}
+}  // namespace cr
+
 // Internal helpers shared with noalloc.cu (declared in cr_device.h).
 void cr_internal_set_error(const char* msg) { g_error = msg; }
 void cr_internal_mat4_inverse(const float* m, float* out) { mat4_inverse(m, out); }
@@ -710,17 +727,7 @@ cr_status cr_compress_mesh(const float* positions, uint32_t num_vertices, const 
             mn[j] = std::min(mn[j], positions[3ull * v + j]);
             mx[j] = std::max(mx[j], positions[3ull * v + j]);
         }
-    float size[3];
-    for (int j = 0; j < 3; j++) size[j] = mx[j] - mn[j];  // vec3 aabbSize = max - min (float)
-    for (uint32_t v = 0; v < num_vertices; v++)
-        for (int j = 0; j < 3; j++) {
-            uint16_t q = 0;
-            if (size[j] > 0.0f) {  // src/LargeGlbLoader.h:666-668
-                const double x = 65536.0 * (double)(positions[3ull * v + j] - mn[j]) / (double)size[j];
-                q = (uint16_t)std::min(std::max(x, 0.0), 65535.0);
-            }
-            positions_out[3ull * v + j] = q;
-        }
+    cr::quantize_positions(positions, num_vertices, mn, mx, positions_out);
     for (int j = 0; j < 3; j++) {
         aabb_min[j] = mn[j];
         aabb_max[j] = mx[j];

@@ -59,6 +59,10 @@ struct MeshRec {
 void mat4_mul(const float* a, const float* b, float* out);  // glm order
 float det3_glm(const float* m);                             // dot(cross(c0, c1), c2)
 void mat4_inverse(const float* m, float* out);              // glm::inverse order
+// u16 quantisation of positions against the box [mn, mx]
+// (src/LargeGlbLoader.h:650-668); 0 on a flat axis
+void quantize_positions(const float* positions, uint32_t num_vertices, const float* mn, const float* mx,
+                        uint16_t* out);
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 struct Assembled {

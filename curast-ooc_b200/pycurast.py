@@ -186,6 +186,22 @@ class CrOocNode(ctypes.Structure):
     ]
 
 
+class CrGlbMesh(ctypes.Structure):
+    _fields_ = [
+        ("positions", ctypes.c_void_p),
+        ("indices", ctypes.c_void_p),
+        ("colors", ctypes.c_void_p),
+        ("num_vertices", _u32),
+        ("num_triangles", _u32),
+        ("aabb_min", _f32 * 3),
+        ("aabb_max", _f32 * 3),
+    ]
+
+
+CR_GLB_COMPRESS = 1
+CR_GLB_PIN_HOST = 2
+
+
 class CrOocConfig(ctypes.Structure):
     _fields_ = [("geometry_budget", _u64), ("size_threshold", _f32), ("frustum_culling", _u32), ("reserved", _u32 * 4)]
 
@@ -314,6 +330,15 @@ EXPORTS = {
                              ctypes.POINTER(CrOocStats)]),
     "cr_ooc_select": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrCamera), ctypes.c_void_p]),
     "cr_ooc_destroy": (_i32, [ctypes.c_void_p]),
+    "cr_glb_open": (_i32, [ctypes.c_void_p, _u64, ctypes.POINTER(ctypes.c_void_p)]),
+    "cr_glb_open_file": (_i32, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "cr_glb_counts": (_i32, [ctypes.c_void_p, ctypes.POINTER(_u32), ctypes.POINTER(_u32)]),
+    "cr_glb_mesh_arrays": (_i32, [ctypes.c_void_p, _u32, ctypes.POINTER(CrGlbMesh)]),
+    "cr_glb_instances": (_i32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(CrInstance)]),
+    "cr_glb_create_meshes": (_i32, [ctypes.c_void_p, ctypes.c_void_p, _u32, ctypes.c_void_p]),
+    "cr_glb_ooc_nodes": (_i32, [ctypes.c_void_p, _u32, _u32, ctypes.c_void_p, ctypes.POINTER(CrOocNode),
+                                ctypes.POINTER(_u32)]),
+    "cr_glb_close": (_i32, [ctypes.c_void_p]),
     "cr_server_create": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrServerConfig), ctypes.POINTER(ctypes.c_void_p)]),
     "cr_server_add_scene": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrInstance), _u32, ctypes.POINTER(_u32)]),
     "cr_server_add_ooc_scene": (_i32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(_u32)]),
@@ -430,22 +455,25 @@ class OocScene:
     of pinned buffers (e.g. tensor.data_ptr() of pin_memory tensors)."""
 
     def __init__(self, ctx, nodes, geometry_budget, size_threshold=0.0, frustum_culling=1):
-        nodes = list(nodes)
-        arr = (CrOocNode * len(nodes))()
-        for k, (pp, ip, cp, nv, nt, lo, hi, world) in enumerate(nodes):
-            arr[k].positions = int(pp)
-            arr[k].indices = int(ip)
-            arr[k].colors = int(cp) if cp else None
-            arr[k].num_vertices = int(nv)
-            arr[k].num_triangles = int(nt)
-            arr[k].aabb_min = (_f32 * 3)(*[float(x) for x in lo])
-            arr[k].aabb_max = (_f32 * 3)(*[float(x) for x in hi])
-            arr[k].world = _f16(world)
+        if isinstance(nodes, ctypes.Array) and nodes._type_ is CrOocNode:
+            arr = nodes  # e.g. Glb.ooc_nodes()
+        else:
+            nodes = list(nodes)
+            arr = (CrOocNode * len(nodes))()
+            for k, (pp, ip, cp, nv, nt, lo, hi, world) in enumerate(nodes):
+                arr[k].positions = int(pp)
+                arr[k].indices = int(ip)
+                arr[k].colors = int(cp) if cp else None
+                arr[k].num_vertices = int(nv)
+                arr[k].num_triangles = int(nt)
+                arr[k].aabb_min = (_f32 * 3)(*[float(x) for x in lo])
+                arr[k].aabb_max = (_f32 * 3)(*[float(x) for x in hi])
+                arr[k].world = _f16(world)
         cfg = CrOocConfig(int(geometry_budget), float(size_threshold), int(frustum_culling))
         h = ctypes.c_void_p()
-        _check(load().cr_ooc_create(ctx.h, arr, len(nodes), ctypes.byref(cfg), ctypes.byref(h)))
+        _check(load().cr_ooc_create(ctx.h, arr, len(arr), ctypes.byref(cfg), ctypes.byref(h)))
         self.h = h
-        self.count = len(nodes)
+        self.count = len(arr)
 
     def render(self, camera, d_visbuffer, d_rgba=0, display=CR_DISPLAY_VERTEX_COLORS, flags=CR_RENDER_SYNC, stream=0):
         st = CrOocStats()
@@ -468,6 +496,91 @@ class OocScene:
 
     def __exit__(self, *exc):
         self.close()
+
+
+class Glb:
+    """cr_glb: a binary glTF file read as the reference's loader reads it.
+
+    Glb(data=bytes) or Glb(path=...).  mesh(k) returns numpy copies of glb mesh
+    k; instances(handles) the draw list; create_meshes(ctx) uploads every mesh;
+    ooc_nodes() the out-of-core node array (valid while this object lives)."""
+
+    def __init__(self, data=None, path=None):
+        h = ctypes.c_void_p()
+        if path is not None:
+            _check(load().cr_glb_open_file(os.fsencode(path), ctypes.byref(h)))
+        else:
+            buf = np.frombuffer(bytes(data), np.uint8)
+            _check(load().cr_glb_open(buf.ctypes.data if buf.size else None, buf.size, ctypes.byref(h)))
+        self.h = h
+        nm, ni = _u32(), _u32()
+        _check(load().cr_glb_counts(self.h, ctypes.byref(nm), ctypes.byref(ni)))
+        self.num_meshes, self.num_instances = nm.value, ni.value
+
+    def mesh(self, k):
+        m = CrGlbMesh()
+        _check(load().cr_glb_mesh_arrays(self.h, int(k), ctypes.byref(m)))
+        nv, nt = m.num_vertices, m.num_triangles
+
+        def arr(addr, n, dt):
+            if not addr:
+                return None
+            return np.ctypeslib.as_array((dt * n).from_address(addr)).copy()
+
+        pos = arr(m.positions, 3 * nv, _f32).reshape(nv, 3)
+        idx = arr(m.indices, 3 * nt, _u32)
+        col = arr(m.colors, nv, _u32)
+        return {"positions": pos, "indices": None if idx is None else idx.reshape(nt, 3), "colors": col,
+                "num_triangles": nt, "aabb_min": np.array(m.aabb_min[:], np.float32),
+                "aabb_max": np.array(m.aabb_max[:], np.float32)}
+
+    @staticmethod
+    def _root(root):
+        if root is None:
+            return None, None
+        r = np.ascontiguousarray(np.asarray(root, np.float32).reshape(16))
+        return r, r.ctypes.data
+
+    def instances(self, handles=None, root=None):
+        """(CrInstance array, count); root: world of the file's root nodes' parent."""
+        arr = (CrInstance * max(self.num_instances, 1))()
+        hv = None
+        if handles is not None:
+            hv = np.ascontiguousarray(handles, dtype=np.uint32)
+        r, rp = self._root(root)
+        _check(load().cr_glb_instances(self.h, hv.ctypes.data if hv is not None else None, rp, arr))
+        return arr, self.num_instances
+
+    def create_meshes(self, ctx, compress=False):
+        out = np.zeros(max(self.num_meshes, 1), np.uint32)
+        _check(load().cr_glb_create_meshes(ctx.h, self.h, CR_GLB_COMPRESS if compress else 0, out.ctypes.data))
+        return out[: self.num_meshes]
+
+    def ooc_nodes(self, max_node_triangles=0, pin=False, root=None):
+        flags = CR_GLB_PIN_HOST if pin else 0
+        n = _u32()
+        r, rp = self._root(root)
+        _check(load().cr_glb_ooc_nodes(self.h, int(max_node_triangles), flags, rp, None, ctypes.byref(n)))
+        arr = (CrOocNode * max(n.value, 1))()
+        _check(load().cr_glb_ooc_nodes(self.h, int(max_node_triangles), flags, rp, arr, ctypes.byref(n)))
+        return (CrOocNode * n.value).from_buffer(arr)
+
+    def close(self):
+        if self.h:
+            load().cr_glb_close(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def make_views(views):

@@ -441,6 +441,71 @@ cr_status cr_ooc_render(cr_ooc* ooc, const cr_camera* camera, uint64_t d_visbuff
 cr_status cr_ooc_select(cr_ooc* ooc, const cr_camera* camera, uint8_t* visible);
 cr_status cr_ooc_destroy(cr_ooc* ooc);
 
+/* ---- glb ingest ---------------------------------------------------------------
+ * A self-contained binary glTF 2.0 file (.glb: JSON chunk + BIN chunks, no
+ * external uris) read as the reference's loader reads it
+ * (src/LargeGlbLoader.h:434-1330, src/GLTFLoader.h:230-400):
+ *   - one mesh per primitive, in (glTF mesh, primitive) order; POSITION a
+ *     float VEC3 accessor; indices u8 / u16 / u32 widened to u32, none =
+ *     non-indexed (num_triangles = num_vertices / 3); COLOR_0 VEC4 u8 or
+ *     VEC3 u8 with a 4-byte stride taken as stored RGBA8, VEC3 float with each
+ *     channel divided by 256 while above 1 and truncated to a byte, alpha 255;
+ *     a mesh's box is its POSITION accessor's min / max;
+ *   - a node's transform is its "matrix" or the identity (translation /
+ *     rotation / scale are ignored, as the reference ignores them); world =
+ *     parent world * matrix in glm order, the file's root nodes under
+ *     root_world (the world of the loader's glb node, which an application
+ *     may set, src/main.cpp:78; NULL = identity);
+ *   - one instance per (node, primitive of its mesh), in the order the
+ *     reference's scene walk collects them: pre-order, a node's children
+ *     after its first primitive and before its other primitives (the
+ *     reference hangs them below the first primitive's scene node).
+ *     cr_render then orders them as the reference's draw does; with
+ *     CR_RENDER_KEEP_ORDER the walk order is kept.
+ * Every index is checked against its primitive's vertices. */
+typedef struct cr_glb cr_glb;
+
+#define CR_GLB_COMPRESS 1u  /* cr_glb_create_meshes: indexed primitives as IX_PU16
+                             * meshes, quantised against the accessor box
+                             * (the loader's `compress` option)                 */
+#define CR_GLB_PIN_HOST 2u  /* cr_glb_ooc_nodes: node arrays in page-locked host
+                             * memory (needs a CUDA device)                      */
+
+typedef struct cr_glb_mesh {
+    const float* positions;    /* xyz per vertex                                   */
+    const uint32_t* indices;   /* 3 per triangle; NULL for a non-indexed primitive */
+    const uint32_t* colors;    /* RGBA8 per vertex; NULL without COLOR_0            */
+    uint32_t num_vertices;
+    uint32_t num_triangles;
+    float aabb_min[3];
+    float aabb_max[3];
+} cr_glb_mesh;
+
+/* Parses a copy of the file's bytes; CR_ERR_INVALID (message in
+ * cr_last_error) for anything malformed or outside the subset above. */
+cr_status cr_glb_open(const void* bytes, uint64_t size, cr_glb** out);
+cr_status cr_glb_open_file(const char* path, cr_glb** out);
+cr_status cr_glb_counts(const cr_glb* glb, uint32_t* num_meshes, uint32_t* num_instances);
+/* Host arrays of mesh k, owned by glb (valid until cr_glb_close). */
+cr_status cr_glb_mesh_arrays(const cr_glb* glb, uint32_t mesh, cr_glb_mesh* out);
+/* num_instances instances; mesh = mesh_handles[k] for glb mesh k (mesh_handles
+ * NULL: k itself); root_world 16 floats column-major or NULL. */
+cr_status cr_glb_instances(const cr_glb* glb, const uint32_t* mesh_handles, const float* root_world,
+                           cr_instance* out);
+/* Creates every mesh in ctx (host copies); mesh_handles gets num_meshes handles. */
+cr_status cr_glb_create_meshes(cr_context* ctx, const cr_glb* glb, uint32_t flags, uint32_t* mesh_handles);
+/* Out-of-core nodes for cr_ooc_create: one per (instance, piece), a piece
+ * being a primitive of at most max_node_triangles triangles (0:
+ * CR_OOC_MAX_NODE_TRIANGLES), or a run of that many consecutive triangles of
+ * a larger one with its vertices compacted in first-use order.  Pieces are
+ * indexed, shared between the instances of a mesh, and boxed by the
+ * primitive's box (whole) or their own vertices (split).  With nodes NULL
+ * only *count is written.  The arrays live in glb until cr_glb_close or a
+ * call with other parameters. */
+cr_status cr_glb_ooc_nodes(cr_glb* glb, uint32_t max_node_triangles, uint32_t flags, const float* root_world,
+                           cr_ooc_node* nodes, uint32_t* count);
+cr_status cr_glb_close(cr_glb* glb);
+
 /* ---- serving ------------------------------------------------------------------
  * No counterpart in the reference (one interactive view).  A server owns
  * resident scenes (instance sets of the context's meshes, or out-of-core
