@@ -114,6 +114,24 @@ def build_workload(name):
                     desc=f"seeded fractal-displaced grid of {quads}x{quads} quads ({idx.shape[0]:,} triangles) seen "
                          f"by {nv} seeded cameras, resolutions uniform among 512x512, 1280x720, 1920x1080, "
                          f"3840x2160")
+    if name.startswith("post_"):
+        # post_2160p_ss2: EDL + SSAO + the 2x supersampled display resolve of a
+        # 3840x2160 colorbuffer (the 1M-triangle heightfield) to 1920x1080
+        W, H, oW, oH = 3840, 2160, 1920, 1080
+        pos, idx, col = scenes.heightfield()
+        view, proj = scenes.heightfield_camera(W, H)
+        return dict(name=name, W=W, H=H, outW=oW, outH=oH, meshes=[(pos, idx, col)],
+                    instances=[(0, scenes.identity())], view=view, proj=proj, device=False, post=True,
+                    desc="eye-dome lighting + ambient occlusion (32 samples, 7x7 blur) + 2x2 supersampled display "
+                         "resolve of the 3840x2160 colorbuffer of the 1M-triangle heightfield, to 1920x1080")
+    if name.startswith("glb_"):
+        # glb_<N>m: a binary glTF file of N one-million-triangle primitives
+        # (u32 indices, RGBA8 colours, one node each), in host memory
+        n = int(name.split("_")[1].rstrip("m"))
+        return dict(name=name, glb=True, primitives=n,
+                    desc=f"binary glTF file of {n} primitives of 1,048,576 triangles (1024x512-quad heightfield "
+                         f"patches: float VEC3 positions, u32 indices, VEC4 u8 colours), one node with a matrix "
+                         f"each, read from host memory into resident meshes and an instance list")
     if name.startswith("served_"):
         # served_<R>rps: Poisson requests at R/s over three resident scenes,
         # beside a 4e9-triangle out-of-core scene streamed from pinned host
@@ -300,6 +318,10 @@ def run_ours(args, rank, world, local):
         return run_batched(args, rank, world, local, wl)
     if wl.get("served"):
         return run_served(args, rank, world, local, wl)
+    if wl.get("post"):
+        return run_post(args, rank, world, local, wl)
+    if wl.get("glb"):
+        return run_glb(args, rank, world, local, wl)
     T, V, Tu = scene_counts(wl)
     W, H = wl["W"], wl["H"]
     ctx = pc.Context(device=local)
@@ -459,6 +481,259 @@ def run_ours(args, rank, world, local):
         line["cpu_baseline"] = cpu_baseline(wl)
     ctx.close()
     return line
+
+
+POST_METRIC = "Mpx/s (EDL + SSAO + 2x supersampled display resolve of a 3840x2160 colorbuffer, per pass)"
+
+
+def post_colorbuffer_oracle(wl):
+    """The workload's colorbuffer from the CPU oracle (host uint64 array)."""
+    import oracle_lib as ol
+
+    p, i, c = host_mesh(wl["meshes"][0])
+    fr = ol.Frame([(p, i, c, wl["instances"][0][1])], wl["view"])
+    fb, _ = ol.raster(fr, wl["W"], wl["H"], wl["proj"][5], nthreads=os.cpu_count() or 1)
+    cb, _ = ol.resolve(fr, wl["view"], wl["proj"], wl["W"], wl["H"], fb, nthreads=os.cpu_count() or 1)
+    return cb
+
+
+def post_bytes(wl):
+    """Algorithmic bytes of one post pass: occlusion reads the colorbuffer
+    (8 B) and writes depth + occlusion (8 B) per source pixel, the blur reads
+    those 8 B and writes the 4-byte shade, the display resolve reads the
+    colorbuffer and the shade of every source pixel and writes one RGBA8 per
+    output pixel (neighbour reads hit in cache)."""
+    P = wl["W"] * wl["H"]
+    return 16 * P + 12 * P + 12 * P + 4 * wl["outW"] * wl["outH"]
+
+
+def run_post(args, rank, world, local, wl):
+    """One step = one cr_postprocess pass (EDL + SSAO + display resolve) on a
+    colorbuffer resident in HBM; the pass's working set (66 MB colorbuffer,
+    66 MB occlusion, 33 MB shade) exceeds L2."""
+    import torch
+
+    import pycurast as pc
+
+    W, H, oW, oH = wl["W"], wl["H"], wl["outW"], wl["outH"]
+    ctx = pc.Context(device=local)
+    h = ctx.mesh_from_host(*wl["meshes"][0])
+    cam = pc.make_camera(wl["view"], wl["proj"], W, H)
+    vis = torch.empty(W * H, dtype=torch.int64, device="cuda")
+    rgba = torch.empty(W * H, dtype=torch.int32, device="cuda")
+    cb = torch.empty(W * H, dtype=torch.int64, device="cuda")
+    ctx.render([(h, wl["instances"][0][1])], cam, vis.data_ptr(), rgba.data_ptr(), cb.data_ptr(),
+               flags=pc.CR_RENDER_SYNC)
+    out = torch.empty(oW * oH, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    flags = pc.CR_POST_EDL | pc.CR_POST_SSAO
+
+    def post(d_cb):
+        ctx.postprocess(d_cb, W, H, wl["proj"], out.data_ptr(), flags, mode=pc.CR_POST_DISPLAY, window_width=oW,
+                        out_size=(oW, oH), stream=sh)
+
+    for _ in range(args.warmup):
+        post(cb.data_ptr())
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local) if rank == 0 else None
+    if clocks:
+        clocks.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        evs[k][0].record(stream)
+        post(cb.data_ptr())
+        evs[k][1].record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop() if clocks else None
+    ms = max_over_ranks(float(np.mean([a.elapsed_time(b) for a, b in evs])), world)
+
+    # end to end: the colorbuffer from pinned host memory, the image back
+    host_cb = torch.empty(W * H, dtype=torch.int64, pin_memory=True)
+    host_cb.copy_(cb)
+    host_out = torch.empty(oW * oH, dtype=torch.int32, pin_memory=True)
+    cb2 = torch.empty_like(cb)
+    e2e_ms = []
+    for k in range(args.steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        cb2.copy_(host_cb, non_blocking=True)
+        post(cb2.data_ptr())
+        host_out.copy_(out, non_blocking=True)
+        b.record(stream)
+        b.synchronize()
+        e2e_ms.append(a.elapsed_time(b))
+    e2e = max_over_ranks(float(np.mean(e2e_ms)), world)
+    if rank != 0:
+        ctx.close()
+        return None
+    peak, peak_kind = load_peaks()
+    algo = post_bytes(wl)
+    achieved = algo / (ms * 1e-3) / 1e9
+    line = {
+        "metric": POST_METRIC,
+        "value": world * W * H / (ms * 1e-3) / 1e6,
+        "unit": "Mpx/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": wl["name"], "desc": wl["desc"], "width": W, "height": H, "out_width": oW,
+                   "out_height": oH, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (165 MB working set per pass)"},
+        "e2e": {"value": world * W * H / (e2e * 1e-3) / 1e6, "unit": "Mpx/s", "ms_per_step": e2e,
+                "h2d_bytes_per_step": 8 * W * H, "d2h_bytes_per_step": 4 * oW * oH},
+        "roofline": {"kernel": "k_ssao_occlusion + k_ssao_blur + k_post_resolve (one pass)", "bound": "hbm",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "algorithmic_bytes": algo, "kernel_ms": ms, "traffic": None,
+                     "note": "issue-bound: 32 hemisphere samples with trigonometry per pixel"},
+        "gpu_launches": 3 * args.steps,
+        "clocks": clk,
+    }
+    if not args.no_cpu_baseline:
+        import oracle_lib as ol
+
+        hcb = host_cb.numpy().view(np.uint64)
+        ncores = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        ol.post(hcb, W, H, wl["proj"], 1, 1, mode=1, window_width=oW, out_size=(oW, oH), nthreads=ncores)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": W * H / dt / 1e6, "unit": "Mpx/s", "cores": ncores, "kind": "port",
+                                "sample": f"the oracle's post pass over the whole colorbuffer, all {ncores} host "
+                                          f"threads (OpenMP), {dt:.2f} s"}
+    ctx.close()
+    return line
+
+
+def glb_file(wl):
+    import glb_writer
+    import scenes
+
+    pos, idx, col = scenes.heightfield()
+    rgba = col.view(np.uint8).reshape(-1, 4)
+    prim = dict(positions=pos, indices=idx, index_type="u32", colors=rgba, color_format="vec4u8")
+    n = wl["primitives"]
+    nodes = [dict(mesh=k, matrix=scenes.translate_scale(1.1 * (k % 8), 0.0, 0.6 * (k // 8))) for k in range(n)]
+    return glb_writer.build_glb([[prim] for _ in range(n)], nodes), idx.shape[0] * n
+
+
+def h2d_peak_gbs():
+    """Pinned host -> device copy rate of this box (1 GiB), the bound of any
+    ingest that ends on the device."""
+    import torch
+
+    src = torch.empty(1 << 30, dtype=torch.uint8, pin_memory=True)
+    dst = torch.empty(1 << 30, dtype=torch.uint8, device="cuda")
+    dst.copy_(src, non_blocking=True)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(3):
+        dst.copy_(src, non_blocking=True)
+    b.record()
+    b.synchronize()
+    return 3 * (1 << 30) / (a.elapsed_time(b) * 1e-3) / 1e9
+
+
+GLB_METRIC = "Mtris/s (binary glTF in host memory -> resident meshes + instance list)"
+
+
+def run_glb(args, rank, world, local, wl):
+    """One step = cr_glb_open of the file's bytes, cr_glb_create_meshes (host
+    copies uploaded) and cr_glb_instances, ended by a device synchronize.  A
+    host-driven path: timed by the host clock with the device synchronized on
+    both sides."""
+    import torch
+
+    import pycurast as pc
+
+    data, T = glb_file(wl)
+    ctx = pc.Context(device=local)
+
+    def step():
+        with pc.Glb(data=data) as g:
+            handles = g.create_meshes(ctx)
+            g.instances(handles)
+        torch.cuda.synchronize()
+        return handles
+
+    for _ in range(args.warmup):
+        for hm in step():
+            ctx.mesh_destroy(hm)
+    barrier(world)
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        hs = step()
+        times.append(time.perf_counter() - t0)
+        for hm in hs:
+            ctx.mesh_destroy(hm)
+    barrier(world)
+    ms = max_over_ranks(float(np.mean(times)) * 1e3, world)
+    if rank != 0:
+        ctx.close()
+        return None
+    peak = h2d_peak_gbs()
+    achieved = len(data) / (ms * 1e-3) / 1e9
+    value = world * T / (ms * 1e-3) / 1e6
+    line = {
+        "metric": GLB_METRIC,
+        "value": value,
+        "unit": "Mtris/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": wl["name"], "desc": wl["desc"], "triangles": T, "file_bytes": len(data),
+                   "parallelism": f"replicas x{world}", "l2": "not applicable (host path; file > L2)"},
+        "e2e": {"value": value, "unit": "Mtris/s", "ms_per_step": ms, "h2d_bytes_per_step": len(data),
+                "d2h_bytes_per_step": 0},
+        "roofline": {"kernel": "host parse + upload (cr_glb_open, cr_glb_create_meshes)", "bound": "pcie",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": "measured here: pinned host-to-device copy of 1 GiB",
+                     "algorithmic_bytes": len(data), "kernel_ms": ms, "traffic": None},
+        "gpu_launches": None,
+        "note": "the step is host code plus one upload and one mesh-preparation pass per primitive",
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = glb_oracle_baseline(wl)
+    ctx.close()
+    return line
+
+
+def glb_oracle_baseline(wl):
+    """The oracle's restatement of the reference loader (Python, one thread)
+    on one primitive of the same form."""
+    import glb_writer
+    import scenes
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import glb_oracle
+
+    pos, idx, col = scenes.heightfield()
+    prim = dict(positions=pos, indices=idx, index_type="u32", colors=col.view(np.uint8).reshape(-1, 4),
+                color_format="vec4u8")
+    sample = glb_writer.build_glb([[prim]], [dict(mesh=0, matrix=scenes.identity())])
+    t0 = time.perf_counter()
+    glb_oracle.load(sample)
+    dt = time.perf_counter() - t0
+    return {"value": idx.shape[0] / dt / 1e6, "unit": "Mtris/s", "cores": 1, "kind": "port",
+            "sample": f"the oracle's loader restatement on a one-primitive file of the same form "
+                      f"({idx.shape[0]:,} triangles), one thread, {dt:.2f} s"}
 
 
 def run_batched(args, rank, world, local, wl):
@@ -782,6 +1057,19 @@ def run_reference(args, rank, world, local):
     wl = build_workload(args.workload)
     if wl.get("batched"):
         return run_reference_batched(args, wl, local)
+    if wl.get("post"):
+        return run_reference_post(args, wl, local)
+    if wl.get("glb"):
+        # the reference loader does not build here (C++23 <print>/<stacktrace>,
+        # its mapped-file layer, scene graph and CUDA driver): its restatement
+        # is the reference arm
+        base = glb_oracle_baseline(wl)
+        return {"impl": "reference", "metric": GLB_METRIC, "value": base["value"], "unit": "Mtris/s", "n_gpus": 1,
+                "steps": 1, "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded)",
+                "config": {"workload": wl["name"], "desc": wl["desc"], "parallelism": "single host thread"},
+                "cpu_baseline": base,
+                "e2e": {"value": base["value"], "unit": "Mtris/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     T, V, Tu = scene_counts(wl)
     W, H = wl["W"], wl["H"]
     try:
@@ -893,6 +1181,43 @@ def run_reference_batched(args, wl, local):
     }
 
 
+def run_reference_post(args, wl, local):
+    """The reference's own post kernels (NVRTC fast-math build) on the same
+    colorbuffer, repeated back to back."""
+    import oracle_lib as ol
+
+    try:
+        ref = ol.Reference("native", device=local)
+    except Exception as e:  # noqa: BLE001
+        return {"impl": "reference", "unavailable": f"reference kernels not loadable: {e}"}
+    W, H, oW, oH = wl["W"], wl["H"], wl["outW"], wl["outH"]
+    cb = post_colorbuffer_oracle(wl)
+    ref.post_timed(cb, W, H, wl["proj"], 1, 1, max(args.warmup, 1), mode=1, window_width=oW, out_size=(oW, oH))
+    ms, _ = ref.post_timed(cb, W, H, wl["proj"], 1, 1, args.steps, mode=1, window_width=oW, out_size=(oW, oH))
+    v = W * H / (ms * 1e-3) / 1e6
+    return {
+        "impl": "reference",
+        "metric": POST_METRIC,
+        "value": v,
+        "unit": "Mpx/s",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": wl["name"], "desc": wl["desc"], "width": W, "height": H, "out_width": oW,
+                   "out_height": oH, "parallelism": "single GPU",
+                   "build": "CuRast NVRTC recipe (--use_fast_math, LTO) for sm_100a"},
+        "cpu_baseline": {"kind": "reference", "value": v, "unit": "Mpx/s", "cores": 0,
+                         "sample": "not a CPU run: the reference's own CUDA post kernels on this B200"},
+        "e2e": {"value": v, "unit": "Mpx/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -902,7 +1227,8 @@ def main(argv=None):
     ap.add_argument("--workload", default="planet_400m_1080p",
                     help="planet_400m_1080p (the 400M-triangle dense mesh), planet_<N>m_1080p, heightfield_1m_1080p, "
                          "instanced_<K>x<N>m_1080p, batched_<V>v_<N>m (V cameras over an N-million-triangle "
-                         "terrain)")
+                         "terrain), served_<R>rps, post_2160p_ss2 (EDL + SSAO + supersampled resolve), glb_<N>m "
+                         "(binary glTF ingest of N one-million-triangle primitives)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ooc-nodes", type=int, default=247, help="out-of-core scene: nodes per side (served_*)")
     ap.add_argument("--serve-seconds", type=float, default=4.0, help="paced serving run length (served_*)")

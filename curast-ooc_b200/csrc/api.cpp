@@ -7,12 +7,15 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "context.h"
@@ -611,61 +614,56 @@ cr_status cr_destroy(cr_context* ctx) {
         if (e) cudaEventDestroy(e);
     for (cudaEvent_t& e : ctx->ring)
         if (e) cudaEventDestroy(e);
+    for (cr_context::Stager& st : ctx->stagers) {
+        cudaFreeHost(st.host);
+        cudaStreamDestroy(st.stream);
+        cudaEventDestroy(st.done[0]);
+        cudaEventDestroy(st.done[1]);
+    }
     delete ctx;
     return CR_OK;
 }
 
-cr_status cr_mesh_create(cr_context* ctx, const cr_mesh_desc* d, uint32_t* mesh_out) {
-    if (!ctx || !d || !mesh_out) return fail(CR_ERR_INVALID, "cr_mesh_create: NULL argument");
-    if (!d->positions || d->num_vertices == 0) return fail(CR_ERR_INVALID, "cr_mesh_create: no positions");
-    if (!d->indices && (uint64_t)d->num_triangles * 3 > d->num_vertices)
-        return fail(CR_ERR_INVALID, "cr_mesh_create: non-indexed mesh needs 3 vertices per triangle");
-    cudaSetDevice(ctx->device);
-    MeshRec m;
+}  // extern "C"
+
+namespace cr {
+
+cr_status alloc_owned_mesh(cr_context* ctx, uint32_t nV, uint32_t nT, bool indexed, bool colored, MeshRec& m) {
+    m = MeshRec{};
     m.live = true;
-    m.numVertices = d->num_vertices;
-    m.numTriangles = d->num_triangles;
-    if (d->memory == CR_MEM_DEVICE) {
-        m.owned = false;
-        m.positions = const_cast<float*>(d->positions);
-        m.indices = const_cast<uint32_t*>(d->indices);
-        m.colors = const_cast<uint32_t*>(d->colors);
-    } else if (d->memory == CR_MEM_HOST) {
-        m.owned = true;
-        const size_t pb = align_up((size_t)d->num_vertices * 12, 256) + 256;
-        // index tiles are fetched in 384-byte bursts; pad to whole tiles
-        const size_t ib = d->indices ? align_up((size_t)d->num_triangles * 12, 384) + 256 : 0;
-        const size_t cb = d->colors ? align_up((size_t)d->num_vertices * 4, 256) : 0;
-        cr_status s = ctx->dev_alloc((void**)&m.positions, pb, "mesh positions");
-        if (s) return s;
-        m.bytes += pb;
-        CR_CUDA(cudaMemcpy(m.positions, d->positions, (size_t)d->num_vertices * 12, cudaMemcpyHostToDevice),
-                "mesh positions upload");
-        if (ib) {
-            s = ctx->dev_alloc((void**)&m.indices, ib, "mesh indices");
-            if (s) {
-                ctx->dev_free(m.positions, pb);
-                return s;
-            }
-            m.bytes += ib;
-            CR_CUDA(cudaMemset(m.indices, 0, ib), "mesh index padding");
-            CR_CUDA(cudaMemcpy(m.indices, d->indices, (size_t)d->num_triangles * 12, cudaMemcpyHostToDevice),
-                    "mesh indices upload");
-        }
-        if (cb) {
-            s = ctx->dev_alloc((void**)&m.colors, cb, "mesh colours");
-            if (s) {
-                ctx->dev_free(m.positions, pb);
-                ctx->dev_free(m.indices, ib);
-                return s;
-            }
-            m.bytes += cb;
-            CR_CUDA(cudaMemcpy(m.colors, d->colors, (size_t)d->num_vertices * 4, cudaMemcpyHostToDevice),
-                    "mesh colours upload");
-        }
-    } else {
-        return fail(CR_ERR_INVALID, "cr_mesh_create: unknown memory kind %d", d->memory);
+    m.owned = true;
+    m.numVertices = nV;
+    m.numTriangles = nT;
+    const size_t pb = align_up((size_t)nV * 12, 256) + 256;
+    // index tiles are fetched in 384-byte bursts; pad to whole tiles
+    const size_t ib = indexed ? align_up((size_t)nT * 12, 384) + 256 : 0;
+    const size_t cb = colored ? align_up((size_t)nV * 4, 256) : 0;
+    cr_status s = ctx->dev_alloc((void**)&m.positions, pb, "mesh positions");
+    if (s) return s;
+    if (ib && (s = ctx->dev_alloc((void**)&m.indices, ib, "mesh indices")) != CR_OK) {
+        ctx->dev_free(m.positions, pb);
+        return s;
     }
+    if (cb && (s = ctx->dev_alloc((void**)&m.colors, cb, "mesh colours")) != CR_OK) {
+        ctx->dev_free(m.positions, pb);
+        ctx->dev_free(m.indices, ib);
+        return s;
+    }
+    m.bytes = pb + ib + cb;
+    if (ib) {
+        const size_t used = (size_t)nT * 12;
+        const cudaError_t e = cudaMemset((char*)m.indices + used, 0, ib - used);
+        if (e != cudaSuccess) {
+            ctx->dev_free(m.positions, pb);
+            ctx->dev_free(m.indices, ib);
+            ctx->dev_free(m.colors, cb);
+            return cuda_fail(e, "mesh index padding");
+        }
+    }
+    return CR_OK;
+}
+
+cr_status register_mesh(cr_context* ctx, MeshRec& m, uint32_t* handle) {
     cr_status bs = build_mesh_boxes(ctx, m);
     if (bs) {
         if (m.owned) {
@@ -674,11 +672,109 @@ cr_status cr_mesh_create(cr_context* ctx, const cr_mesh_desc* d, uint32_t* mesh_
             ctx->dev_free(m.colors, 0);
             ctx->bytesInUse -= std::min(ctx->bytesInUse, m.bytes);
         }
+        ctx->dev_free(m.itemBoxes, m.boxBytes);
         return bs;
     }
     ctx->meshes.push_back(m);
-    *mesh_out = (uint32_t)(ctx->meshes.size() - 1);
+    *handle = (uint32_t)(ctx->meshes.size() - 1);
     return CR_OK;
+}
+
+cr_status upload_parallel(cr_context* ctx, const std::vector<CopyJob>& jobs) {
+    constexpr size_t kHalf = 8u << 20;
+    if (ctx->stagers.empty()) {
+        const unsigned n = std::min(8u, std::max(1u, std::thread::hardware_concurrency()));
+        for (unsigned i = 0; i < n; i++) {
+            cr_context::Stager st;
+            cudaError_t e = cudaHostAlloc((void**)&st.host, 2 * kHalf, cudaHostAllocDefault);
+            if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st.stream, cudaStreamNonBlocking);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&st.done[0], cudaEventDisableTiming);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&st.done[1], cudaEventDisableTiming);
+            if (e != cudaSuccess) {
+                if (st.host) cudaFreeHost(st.host);
+                if (st.stream) cudaStreamDestroy(st.stream);
+                if (st.done[0]) cudaEventDestroy(st.done[0]);
+                if (ctx->stagers.empty()) return cuda_fail(e, "upload staging");
+                cudaGetLastError();
+                break;  // fewer workers
+            }
+            ctx->stagers.push_back(st);
+        }
+    }
+    struct Piece {
+        char* dst;
+        const char* src;
+        size_t n;
+    };
+    std::vector<Piece> pieces;
+    for (const CopyJob& j : jobs)
+        for (size_t o = 0; o < j.bytes; o += kHalf)
+            pieces.push_back({(char*)j.dst + o, (const char*)j.src + o, std::min(kHalf, j.bytes - o)});
+    std::atomic<size_t> next{0};
+    std::atomic<int> failed{0};
+    auto worker = [&](cr_context::Stager& st) {
+        if (cudaSetDevice(ctx->device) != cudaSuccess) failed = 1;
+        bool used[2] = {false, false};
+        int half = 0;
+        for (size_t k; !failed && (k = next.fetch_add(1)) < pieces.size(); half ^= 1) {
+            uint8_t* buf = st.host + half * kHalf;
+            if (used[half] && cudaEventSynchronize(st.done[half]) != cudaSuccess) failed = 1;
+            memcpy(buf, pieces[k].src, pieces[k].n);
+            if (cudaMemcpyAsync(pieces[k].dst, buf, pieces[k].n, cudaMemcpyHostToDevice, st.stream) != cudaSuccess ||
+                cudaEventRecord(st.done[half], st.stream) != cudaSuccess)
+                failed = 1;
+            used[half] = true;
+        }
+        if (cudaStreamSynchronize(st.stream) != cudaSuccess) failed = 1;
+    };
+    const size_t nw = std::min(ctx->stagers.size(), std::max<size_t>(1, pieces.size()));
+    std::vector<std::thread> pool;
+    for (size_t i = 1; i < nw; i++) pool.emplace_back(worker, std::ref(ctx->stagers[i]));
+    worker(ctx->stagers[0]);
+    for (auto& t : pool) t.join();
+    if (failed) return fail(CR_ERR_CUDA, "bulk upload: %s", cudaGetErrorString(cudaGetLastError()));
+    return CR_OK;
+}
+
+}  // namespace cr
+
+extern "C" {
+
+cr_status cr_mesh_create(cr_context* ctx, const cr_mesh_desc* d, uint32_t* mesh_out) {
+    if (!ctx || !d || !mesh_out) return fail(CR_ERR_INVALID, "cr_mesh_create: NULL argument");
+    if (!d->positions || d->num_vertices == 0) return fail(CR_ERR_INVALID, "cr_mesh_create: no positions");
+    if (!d->indices && (uint64_t)d->num_triangles * 3 > d->num_vertices)
+        return fail(CR_ERR_INVALID, "cr_mesh_create: non-indexed mesh needs 3 vertices per triangle");
+    cudaSetDevice(ctx->device);
+    MeshRec m;
+    if (d->memory == CR_MEM_DEVICE) {
+        m.live = true;
+        m.owned = false;
+        m.numVertices = d->num_vertices;
+        m.numTriangles = d->num_triangles;
+        m.positions = const_cast<float*>(d->positions);
+        m.indices = const_cast<uint32_t*>(d->indices);
+        m.colors = const_cast<uint32_t*>(d->colors);
+    } else if (d->memory == CR_MEM_HOST) {
+        cr_status s = alloc_owned_mesh(ctx, d->num_vertices, d->num_triangles, d->indices != nullptr,
+                                       d->colors != nullptr, m);
+        if (s) return s;
+        cudaError_t e = cudaMemcpy(m.positions, d->positions, (size_t)d->num_vertices * 12, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && d->indices)
+            e = cudaMemcpy(m.indices, d->indices, (size_t)d->num_triangles * 12, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && d->colors)
+            e = cudaMemcpy(m.colors, d->colors, (size_t)d->num_vertices * 4, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            ctx->dev_free(m.positions, 0);
+            ctx->dev_free(m.indices, 0);
+            ctx->dev_free(m.colors, 0);
+            ctx->bytesInUse -= std::min(ctx->bytesInUse, m.bytes);
+            return cuda_fail(e, "mesh upload");
+        }
+    } else {
+        return fail(CR_ERR_INVALID, "cr_mesh_create: unknown memory kind %d", d->memory);
+    }
+    return register_mesh(ctx, m, mesh_out);
 }
 
 uint32_t cr_compressed_index_bits(uint32_t index_min, uint32_t index_max) {

@@ -65,6 +65,23 @@ void quantize_positions(const float* positions, uint32_t num_vertices, const flo
                         uint16_t* out);
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// A host -> device copy of a bulk upload.
+struct CopyJob {
+    void* dst;
+    const void* src;
+    size_t bytes;
+};
+// Device buffers of an owned mesh of nV vertices and nT triangles (positions,
+// indices padded to whole 384-byte tiles with the padding zeroed, colours),
+// not yet filled; on failure nothing stays allocated.
+cr_status alloc_owned_mesh(cr_context* ctx, uint32_t nV, uint32_t nT, bool indexed, bool colored, MeshRec& m);
+// Builds the mesh's boxes and registers it; frees it on failure.
+cr_status register_mesh(cr_context* ctx, MeshRec& m, uint32_t* handle);
+// The copies, split into 8 MiB pieces, on up to 8 host threads, each staging
+// through its own page-locked buffer on its own stream; returns when all
+// have landed.
+cr_status upload_parallel(cr_context* ctx, const std::vector<CopyJob>& jobs);
+
 struct Assembled {
     std::vector<uint32_t> order;
     std::vector<CrInstance> inst;
@@ -123,6 +140,16 @@ struct cr_context {
     cr_frame_stats last{};
     bool pendingStats = false;
     cudaStream_t lastStream = nullptr;
+
+    // bulk host uploads (glb ingest): per worker thread a page-locked
+    // staging buffer in two halves, a stream and the halves' copy events,
+    // created on first use
+    struct Stager {
+        uint8_t* host = nullptr;
+        cudaStream_t stream = nullptr;
+        cudaEvent_t done[2] = {nullptr, nullptr};
+    };
+    std::vector<Stager> stagers;
 
     // autotuner results, one per scene class
     std::vector<cr_tuning> tunings;

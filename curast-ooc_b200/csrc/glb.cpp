@@ -32,6 +32,7 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -39,6 +40,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "context.h"
@@ -275,7 +277,6 @@ cr_status glb_fail(const char* msg) { return fail(CR_ERR_INVALID, "glb: %s", msg
 }  // namespace
 
 struct cr_glb {
-    std::vector<uint8_t> bytes;  // owned copy of the file
     struct Mesh {
         std::vector<float> positions;
         std::vector<uint32_t> indices;  // empty: non-indexed
@@ -330,9 +331,7 @@ struct cr_glb {
 
 namespace {
 
-cr_status parse(cr_glb& g) {
-    const uint8_t* d = g.bytes.data();
-    const uint64_t size = g.bytes.size();
+cr_status parse(cr_glb& g, const uint8_t* d, uint64_t size) {
     if (size < 20 || rd<uint32_t>(d) != 0x46546C67u) return glb_fail("not a binary glTF (magic)");
     if (rd<uint32_t>(d + 4) != 2) return glb_fail("glTF version is not 2");
     const uint64_t total = std::min<uint64_t>(rd<uint32_t>(d + 8), size);
@@ -374,6 +373,14 @@ cr_status parse(cr_glb& g) {
         }
 
     // ---- meshes: one per primitive --------------------------------------------
+    // validated here, converted below in parallel (one primitive per task)
+    struct Task {
+        Acc pos, idx, col;
+        bool hasIdx = false;
+        int colMode = 0;  // 0 none, 1 stored RGBA8 bytes, 2 VEC3 float
+        bool hasBox = false;
+    };
+    std::vector<Task> tasks;
     std::vector<std::pair<uint32_t, uint32_t>> meshRange;  // glTF mesh -> [first, end)
     if (const JVal* ms = root.arrOf("meshes"))
         for (const JVal& jm : ms->arr) {
@@ -384,76 +391,123 @@ cr_status parse(cr_glb& g) {
                     const JVal* jpos = attrs ? attrs->get("POSITION") : nullptr;
                     if (!jpos || jpos->kind != JVal::NUM) return glb_fail("primitive without POSITION");
                     if (pr.numOr("mode", 4) != 4) return glb_fail("only triangle primitives (mode 4) are supported");
-                    Acc a;
-                    if (!accessor_of(root, views, jpos->num, a) || a.type != "VEC3" || a.ct != CT_F32)
-                        return glb_fail("POSITION must be a float VEC3 accessor inside its bufferView");
-                    if (a.count == 0 || a.count > 0xffffffffull) return glb_fail("POSITION count out of range");
+                    Task t;
                     cr_glb::Mesh m;
-                    m.numVertices = (uint32_t)a.count;
-                    m.positions.resize(3ull * a.count);
-                    for (uint64_t k = 0; k < a.count; k++) memcpy(&m.positions[3 * k], a.base + k * a.stride, 12);
-                    if (!vec3_of(a.j->get("min"), m.box) || !vec3_of(a.j->get("max"), m.box + 3)) {
-                        // accessor bounds are required by glTF for POSITION;
-                        // without them the box is the vertices' own
-                        for (int k = 0; k < 3; k++) {
-                            m.box[k] = INFINITY;
-                            m.box[3 + k] = -INFINITY;
-                        }
-                        for (uint32_t v = 0; v < m.numVertices; v++)
-                            for (int k = 0; k < 3; k++) {
-                                m.box[k] = std::min(m.box[k], m.positions[3ull * v + k]);
-                                m.box[3 + k] = std::max(m.box[3 + k], m.positions[3ull * v + k]);
-                            }
-                    }
+                    if (!accessor_of(root, views, jpos->num, t.pos) || t.pos.type != "VEC3" || t.pos.ct != CT_F32)
+                        return glb_fail("POSITION must be a float VEC3 accessor inside its bufferView");
+                    if (t.pos.count == 0 || t.pos.count > 0xffffffffull) return glb_fail("POSITION count out of range");
+                    m.numVertices = (uint32_t)t.pos.count;
+                    // accessor bounds are required by glTF for POSITION;
+                    // without them the box is the vertices' own
+                    t.hasBox = vec3_of(t.pos.j->get("min"), m.box) && vec3_of(t.pos.j->get("max"), m.box + 3);
                     if (const JVal* ji = pr.get("indices"); ji && ji->kind == JVal::NUM) {
-                        Acc ia;
+                        Acc& ia = t.idx;
                         if (!accessor_of(root, views, ji->num, ia) || ia.type != "SCALAR" ||
                             (ia.ct != CT_U8 && ia.ct != CT_U16 && ia.ct != CT_U32))
                             return glb_fail("indices must be an unsigned SCALAR accessor");
-                        const uint64_t es = (uint64_t)comp_size(ia.ct);
-                        if (ia.count * es > ia.room) return glb_fail("indices outside their bufferView");
+                        if (ia.count * (uint64_t)comp_size(ia.ct) > ia.room)
+                            return glb_fail("indices outside their bufferView");
                         if (ia.count / 3 > 0xffffffffull) return glb_fail("too many triangles");
+                        t.hasIdx = true;
                         m.numTriangles = (uint32_t)(ia.count / 3);
-                        m.indices.resize(3ull * m.numTriangles);
-                        for (uint64_t k = 0; k < m.indices.size(); k++) {
-                            const uint8_t* q = ia.base + k * es;
-                            const uint32_t v = ia.ct == CT_U8 ? q[0] : ia.ct == CT_U16 ? rd<uint16_t>(q) : rd<uint32_t>(q);
-                            if (v >= m.numVertices) return glb_fail("index beyond its primitive's vertices");
-                            m.indices[k] = v;
-                        }
                     } else {
                         m.numTriangles = m.numVertices / 3;
                     }
                     if (const JVal* jc = attrs->get("COLOR_0"); jc && jc->kind == JVal::NUM) {
-                        Acc ca;
+                        Acc& ca = t.col;
                         if (!accessor_of(root, views, jc->num, ca)) return glb_fail("bad COLOR_0 accessor");
                         if (ca.count < m.numVertices) return glb_fail("COLOR_0 has fewer entries than POSITION");
-                        m.colors.resize(m.numVertices);
-                        const bool asStored = (ca.type == "VEC4" && ca.ct == CT_U8) ||
-                                              (ca.type == "VEC3" && ca.ct == CT_U8 && ca.stride == 4);
-                        if (asStored) {
+                        if ((ca.type == "VEC4" && ca.ct == CT_U8) || (ca.type == "VEC3" && ca.ct == CT_U8 && ca.stride == 4)) {
                             if (4ull * m.numVertices > ca.room) return glb_fail("COLOR_0 outside its bufferView");
-                            memcpy(m.colors.data(), ca.base, 4ull * m.numVertices);
+                            t.colMode = 1;
                         } else if (ca.type == "VEC3" && ca.ct == CT_F32) {
-                            for (uint32_t k = 0; k < m.numVertices; k++) {
-                                float c[3];
-                                memcpy(c, ca.base + k * ca.stride, 12);
-                                uint32_t rgba = 0xff000000u;
-                                for (int ch = 0; ch < 3; ch++) {
-                                    float x = c[ch];
-                                    while (x > 1.0f) x = x / 256.0f;
-                                    rgba |= (uint32_t)byte_of(x) << (8 * ch);
-                                }
-                                m.colors[k] = rgba;
-                            }
+                            t.colMode = 2;
                         } else {
                             return glb_fail("COLOR_0 must be VEC4 u8, VEC3 u8 with stride 4, or VEC3 float");
                         }
                     }
                     g.meshes.push_back(std::move(m));
+                    tasks.push_back(t);
                 }
             meshRange.emplace_back(first, (uint32_t)g.meshes.size());
         }
+    // conversion: independent per primitive
+    auto convert = [&](size_t k) -> bool {
+        const Task& t = tasks[k];
+        cr_glb::Mesh& m = g.meshes[k];
+        const uint64_t nv = m.numVertices;
+        m.positions.resize(3 * nv);
+        if (t.pos.stride == 12) {
+            memcpy(m.positions.data(), t.pos.base, 12 * nv);
+        } else {
+            for (uint64_t v = 0; v < nv; v++) memcpy(&m.positions[3 * v], t.pos.base + v * t.pos.stride, 12);
+        }
+        if (!t.hasBox) {
+            for (int j = 0; j < 3; j++) {
+                m.box[j] = INFINITY;
+                m.box[3 + j] = -INFINITY;
+            }
+            for (uint64_t v = 0; v < nv; v++)
+                for (int j = 0; j < 3; j++) {
+                    m.box[j] = std::min(m.box[j], m.positions[3 * v + j]);
+                    m.box[3 + j] = std::max(m.box[3 + j], m.positions[3 * v + j]);
+                }
+        }
+        if (t.hasIdx) {
+            const uint64_t n = 3ull * m.numTriangles;
+            m.indices.resize(n);
+            uint32_t* out = m.indices.data();
+            const uint8_t* q = t.idx.base;
+            uint32_t hi = 0;
+            if (t.idx.ct == CT_U32) {
+                memcpy(out, q, 4 * n);
+                for (uint64_t i = 0; i < n; i++) hi = std::max(hi, out[i]);
+            } else if (t.idx.ct == CT_U16) {
+                for (uint64_t i = 0; i < n; i++) {
+                    out[i] = rd<uint16_t>(q + 2 * i);
+                    hi = std::max(hi, out[i]);
+                }
+            } else {
+                for (uint64_t i = 0; i < n; i++) {
+                    out[i] = q[i];
+                    hi = std::max(hi, out[i]);
+                }
+            }
+            if (n && hi >= m.numVertices) return false;  // an index beyond the primitive's vertices
+        }
+        if (t.colMode == 1) {
+            m.colors.resize(nv);
+            memcpy(m.colors.data(), t.col.base, 4 * nv);
+        } else if (t.colMode == 2) {
+            m.colors.resize(nv);
+            for (uint64_t v = 0; v < nv; v++) {
+                float c[3];
+                memcpy(c, t.col.base + v * t.col.stride, 12);
+                uint32_t rgba = 0xff000000u;
+                for (int ch = 0; ch < 3; ch++) {
+                    float x = c[ch];
+                    while (x > 1.0f) x = x / 256.0f;
+                    rgba |= (uint32_t)byte_of(x) << (8 * ch);
+                }
+                m.colors[v] = rgba;
+            }
+        }
+        return true;
+    };
+    {
+        const size_t nthreads = std::min<size_t>({tasks.size(), 16, std::max(1u, std::thread::hardware_concurrency())});
+        std::atomic<size_t> next{0};
+        std::atomic<bool> bad{false};
+        auto worker = [&]() {
+            for (size_t k; (k = next.fetch_add(1)) < tasks.size();)
+                if (!convert(k)) bad = true;
+        };
+        std::vector<std::thread> pool;
+        for (size_t i = 1; i < nthreads; i++) pool.emplace_back(worker);
+        worker();
+        for (auto& th : pool) th.join();
+        if (bad) return glb_fail("index beyond its primitive's vertices");
+    }
 
     // ---- nodes -----------------------------------------------------------------
     const JVal* ns = root.arrOf("nodes");
@@ -634,8 +688,7 @@ cr_status cr_glb_open(const void* bytes, uint64_t size, cr_glb** out) {
     if (!bytes || !out) return fail(CR_ERR_INVALID, "cr_glb_open: NULL argument");
     *out = nullptr;
     std::unique_ptr<cr_glb> g(new cr_glb());
-    g->bytes.assign((const uint8_t*)bytes, (const uint8_t*)bytes + size);
-    if (cr_status s = parse(*g)) return s;
+    if (cr_status s = parse(*g, (const uint8_t*)bytes, size)) return s;
     *out = g.release();
     return CR_OK;
 }
@@ -645,17 +698,18 @@ cr_status cr_glb_open_file(const char* path, cr_glb** out) {
     *out = nullptr;
     FILE* f = fopen(path, "rb");
     if (!f) return fail(CR_ERR_NOT_FOUND, "glb: cannot open %s", path);
-    std::unique_ptr<cr_glb> g(new cr_glb());
+    std::vector<uint8_t> bytes;
     if (fseek(f, 0, SEEK_END) == 0) {
         const long n = ftell(f);
         if (n > 0 && fseek(f, 0, SEEK_SET) == 0) {
-            g->bytes.resize((size_t)n);
-            if (fread(g->bytes.data(), 1, (size_t)n, f) != (size_t)n) g->bytes.clear();
+            bytes.resize((size_t)n);
+            if (fread(bytes.data(), 1, (size_t)n, f) != (size_t)n) bytes.clear();
         }
     }
     fclose(f);
-    if (g->bytes.empty()) return fail(CR_ERR_INVALID, "glb: cannot read %s", path);
-    if (cr_status s = parse(*g)) return s;
+    if (bytes.empty()) return fail(CR_ERR_INVALID, "glb: cannot read %s", path);
+    std::unique_ptr<cr_glb> g(new cr_glb());
+    if (cr_status s = parse(*g, bytes.data(), bytes.size())) return s;
     *out = g.release();
     return CR_OK;
 }
@@ -697,49 +751,82 @@ cr_status cr_glb_create_meshes(cr_context* ctx, const cr_glb* g, uint32_t flags,
     if (!ctx || !g || (!mesh_handles && !g->meshes.empty()))
         return fail(CR_ERR_INVALID, "cr_glb_create_meshes: NULL argument");
     if (flags & ~(uint32_t)CR_GLB_COMPRESS) return fail(CR_ERR_INVALID, "cr_glb_create_meshes: unknown flags");
-    size_t made = 0;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(CR_ERR_CUDA, "cr_glb_create_meshes: cudaSetDevice");
+    // plain meshes: every buffer allocated first, then one parallel staged
+    // upload of all of them, then their boxes
+    std::vector<size_t> plain;
+    for (size_t k = 0; k < g->meshes.size(); k++)
+        if (!(flags & CR_GLB_COMPRESS) || g->meshes[k].indices.empty()) plain.push_back(k);
+    std::vector<MeshRec> recs(plain.size());
+    std::vector<CopyJob> jobs;
     cr_status s = CR_OK;
-    for (; made < g->meshes.size(); made++) {
-        const cr_glb::Mesh& m = g->meshes[made];
-        if ((flags & CR_GLB_COMPRESS) && !m.indices.empty()) {
-            const uint64_t n = 3ull * m.numTriangles;
-            uint32_t lo = 0, hi = 0;
-            if (n) {
-                lo = *std::min_element(m.indices.begin(), m.indices.end());
-                hi = *std::max_element(m.indices.begin(), m.indices.end());
-            }
-            std::vector<uint32_t> packed(cr_compressed_index_words(n, cr_compressed_index_bits(lo, hi)));
-            std::vector<uint16_t> q(3ull * m.numVertices);
-            cr_compressed_mesh_desc d{};
-            s = cr_compress_mesh(m.positions.data(), m.numVertices, m.indices.data(), m.numTriangles, q.data(),
-                                 packed.data(), packed.size(), d.aabb_min, d.aabb_max, &d.index_min, &d.index_max);
-            if (s) break;
-            // the loader quantises against the accessor's bounds
-            quantize_positions(m.positions.data(), m.numVertices, m.box, m.box + 3, q.data());
-            memcpy(d.aabb_min, m.box, 12);
-            memcpy(d.aabb_max, m.box + 3, 12);
-            d.packed_indices = packed.data();
-            d.positions = q.data();
-            d.colors = m.colors.empty() ? nullptr : m.colors.data();
-            d.num_vertices = m.numVertices;
-            d.num_triangles = m.numTriangles;
-            d.memory = CR_MEM_HOST;
-            s = cr_mesh_create_compressed(ctx, &d, &mesh_handles[made]);
-        } else {
-            cr_mesh_desc d{};
-            d.positions = m.positions.data();
-            d.indices = m.indices.empty() ? nullptr : m.indices.data();
-            d.colors = m.colors.empty() ? nullptr : m.colors.data();
-            d.num_vertices = m.numVertices;
-            d.num_triangles = m.numTriangles;
-            d.memory = CR_MEM_HOST;
-            s = cr_mesh_create(ctx, &d, &mesh_handles[made]);
-        }
+    size_t allocated = 0;
+    for (; allocated < plain.size(); allocated++) {
+        const cr_glb::Mesh& m = g->meshes[plain[allocated]];
+        MeshRec& r = recs[allocated];
+        s = alloc_owned_mesh(ctx, m.numVertices, m.numTriangles, !m.indices.empty(), !m.colors.empty(), r);
         if (s) break;
+        jobs.push_back({r.positions, m.positions.data(), 12ull * m.numVertices});
+        if (!m.indices.empty()) jobs.push_back({r.indices, m.indices.data(), 12ull * m.numTriangles});
+        if (!m.colors.empty()) jobs.push_back({r.colors, m.colors.data(), 4ull * m.numVertices});
+    }
+    if (s == CR_OK) s = upload_parallel(ctx, jobs);
+    if (s != CR_OK) {
+        const std::string msg = cr_last_error();
+        for (size_t k = 0; k < allocated; k++) {
+            ctx->dev_free(recs[k].positions, 0);
+            ctx->dev_free(recs[k].indices, 0);
+            ctx->dev_free(recs[k].colors, 0);
+            ctx->bytesInUse -= std::min(ctx->bytesInUse, recs[k].bytes);
+        }
+        return fail(s, "%s", msg.c_str());
+    }
+    std::vector<char> done(g->meshes.size(), 0);
+    for (size_t k = 0; k < plain.size() && s == CR_OK; k++) {
+        s = register_mesh(ctx, recs[k], &mesh_handles[plain[k]]);
+        if (s == CR_OK) {
+            done[plain[k]] = 1;
+        } else {  // the later ones were never registered
+            for (size_t j = k + 1; j < plain.size(); j++) {
+                ctx->dev_free(recs[j].positions, 0);
+                ctx->dev_free(recs[j].indices, 0);
+                ctx->dev_free(recs[j].colors, 0);
+                ctx->bytesInUse -= std::min(ctx->bytesInUse, recs[j].bytes);
+            }
+        }
+    }
+    for (size_t made = 0; made < g->meshes.size() && s == CR_OK; made++) {
+        const cr_glb::Mesh& m = g->meshes[made];
+        if (done[made]) continue;  // compressed: packed on the host, as the loader packs
+        const uint64_t n = 3ull * m.numTriangles;
+        uint32_t lo = 0, hi = 0;
+        if (n) {
+            lo = *std::min_element(m.indices.begin(), m.indices.end());
+            hi = *std::max_element(m.indices.begin(), m.indices.end());
+        }
+        std::vector<uint32_t> packed(cr_compressed_index_words(n, cr_compressed_index_bits(lo, hi)));
+        std::vector<uint16_t> q(3ull * m.numVertices);
+        cr_compressed_mesh_desc d{};
+        s = cr_compress_mesh(m.positions.data(), m.numVertices, m.indices.data(), m.numTriangles, q.data(),
+                             packed.data(), packed.size(), d.aabb_min, d.aabb_max, &d.index_min, &d.index_max);
+        if (s) break;
+        // the loader quantises against the accessor's bounds
+        quantize_positions(m.positions.data(), m.numVertices, m.box, m.box + 3, q.data());
+        memcpy(d.aabb_min, m.box, 12);
+        memcpy(d.aabb_max, m.box + 3, 12);
+        d.packed_indices = packed.data();
+        d.positions = q.data();
+        d.colors = m.colors.empty() ? nullptr : m.colors.data();
+        d.num_vertices = m.numVertices;
+        d.num_triangles = m.numTriangles;
+        d.memory = CR_MEM_HOST;
+        s = cr_mesh_create_compressed(ctx, &d, &mesh_handles[made]);
+        if (s == CR_OK) done[made] = 1;
     }
     if (s != CR_OK) {  // leave no half-made scene behind
         const std::string msg = cr_last_error();
-        for (size_t k = 0; k < made; k++) cr_mesh_destroy(ctx, mesh_handles[k]);
+        for (size_t k = 0; k < done.size(); k++)
+            if (done[k]) cr_mesh_destroy(ctx, mesh_handles[k]);
         return fail(s, "%s", msg.c_str());
     }
     return CR_OK;

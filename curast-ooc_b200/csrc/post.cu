@@ -13,7 +13,8 @@
 // Float semantics as the rest of the library (-fmad=false, IEEE division and
 // square root): every expression keeps the reference's operation order, so
 // the image matches the reference's IEEE-mode build up to the last-place
-// differences of the transcendental functions (cosf, sinf, log2f, expf).
+// differences of the transcendental functions (cosf, sinf, log2f, expf;
+// sincosf for the per-sample angle).
 // One thread per pixel; SSAO is the only stage that reads far neighbours
 // (32 samples within a depth-proportional radius).
 #include <cuda_runtime.h>
@@ -52,20 +53,43 @@ __device__ __forceinline__ float depth_at(const CrPostParams& p, int pid) {
     return __uint_as_float((uint32_t)(__ldg(reinterpret_cast<const unsigned long long*>(p.colorbuffer) + pid) >> 32));
 }
 
+// The angle-only terms of both effects, the same for every pixel: computed
+// once per block into shared memory by the same device functions the
+// per-pixel expressions would call, so the values are bit-identical.
+struct PostTables {
+    float edlCos[8], edlSin[8];                 // cosf / sinf(2 * 3.1415 * i / 8)
+    float sinTheta[32], cosTheta[32], rad[32];  // sqrtf(fi), sqrtf(1 - fi), sqrtf((i + 1) / 32)
+};
+
+__device__ __forceinline__ void post_tables(PostTables& t, int tid) {
+    if (tid < 8) {
+        const float u = 2.0f * 3.1415f * float(tid) / float(8);
+        t.edlCos[tid] = cosf(u);
+        t.edlSin[tid] = sinf(u);
+    }
+    if (tid < 32) {
+        const float INV_N = 1.0f / float(32);
+        const float fi = (float(tid) + 0.5f) * INV_N;
+        t.sinTheta[tid] = sqrtf(fi);
+        t.cosTheta[tid] = sqrtf(1.0f - fi);
+        t.rad[tid] = sqrtf(float(tid + 1) * INV_N);
+    }
+}
+
 // getEdlShadingFactor (resolve.cu:234-268): eight neighbours on a circle of
 // `distance` pixels, positions truncated to integers as the reference's
 // int-parameter lambda truncates them.
-__device__ float edl_factor(const CrPostParams& p, float depth, int x, int y, int distance) {
+__device__ float edl_factor(const CrPostParams& p, const PostTables& t, float depth, int x, int y, int distance) {
     float sum = 0.0f;
     const int numSamples = 8;
+    const float ld = log2f(depth);
     for (int i = 0; i < numSamples; i++) {
-        const float u = 2.0f * 3.1415f * float(i) / float(numSamples);
-        const float dx = float(distance) * cosf(u);
-        const float dy = float(distance) * sinf(u);
+        const float dx = float(distance) * t.edlCos[i];
+        const float dy = float(distance) * t.edlSin[i];
         const int nx = (int)((float)x + dx), ny = (int)((float)y + dy);
         float nd = INFINITY;
         if (nx >= 0 && nx < p.W && ny >= 0 && ny < p.H) nd = depth_at(p, nx + p.W * ny);
-        sum += fmaxf(log2f(depth) - log2f(nd), 0.0f);
+        sum += fmaxf(ld - log2f(nd), 0.0f);
     }
     const float response = sum / float(numSamples);
     const float edlStrength = 0.9f;
@@ -106,7 +130,7 @@ __device__ P3 view_normal(const CrPostParams& p, int x, int y, float d0) {
 __device__ __forceinline__ int to_int(float v) { return __float2int_rz(v); }
 
 // getSSAOShadingFactor (resolve.cu:350-470)
-__device__ float ssao_factor(const CrPostParams& p, float center_depth, int x, int y) {
+__device__ float ssao_factor(const CrPostParams& p, const PostTables& t, float center_depth, int x, int y) {
     if (isinf(center_depth) || center_depth <= 0.0f) return 1.0f;
     const int NUM_SAMPLES = 32;
     const float RADIUS_FRACTION = 0.2025f;
@@ -136,12 +160,13 @@ __device__ float ssao_factor(const CrPostParams& p, float center_depth, int x, i
     const float INV_N = 1.0f / float(NUM_SAMPLES);
     const float GOLDEN_ANGLE = 2.39996323f;
     for (int i = 0; i < NUM_SAMPLES; ++i) {
-        const float fi = (float(i) + 0.5f) * INV_N;
-        const float sin_theta = sqrtf(fi);
-        const float cos_theta = sqrtf(1.0f - fi);
+        const float sin_theta = t.sinTheta[i];
+        const float cos_theta = t.cosTheta[i];
         const float phi = float(i) * GOLDEN_ANGLE + rand_angle;
-        const P3 dir = padd(padd(pmul(T, sin_theta * cosf(phi)), pmul(B, sin_theta * sinf(phi))), pmul(N, cos_theta));
-        const float r = world_radius * sqrtf(float(i + 1) * INV_N);
+        float sphi, cphi;
+        sincosf(phi, &sphi, &cphi);
+        const P3 dir = padd(padd(pmul(T, sin_theta * cphi), pmul(B, sin_theta * sphi)), pmul(N, cos_theta));
+        const float r = world_radius * t.rad[i];
         const P3 S = padd(P, pmul(dir, r));
         if (S.z <= 0.001f) continue;
         // ssao_screenPos (resolve.cu:289-296)
@@ -166,11 +191,14 @@ __device__ float ssao_factor(const CrPostParams& p, float center_depth, int x, i
 
 // kernel_ssaoOcclusion (resolve.cu:549-568)
 __global__ void __launch_bounds__(256) k_ssao_occlusion(const CrPostParams p) {
+    __shared__ PostTables t;
+    post_tables(t, threadIdx.y * 32 + threadIdx.x);
+    __syncthreads();
     const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y;
     if (x >= p.W || y >= p.H) return;
     const int pid = x + p.W * y;
     const float depth = depth_at(p, pid);
-    const float ssao = ssao_factor(p, depth, x, y);
+    const float ssao = ssao_factor(p, t, depth, x, y);
     p.occlusion[pid] = ((uint64_t)__float_as_uint(depth) << 32) | (uint64_t)__float_as_uint(ssao);
 }
 
@@ -205,14 +233,14 @@ __global__ void __launch_bounds__(256) k_ssao_blur(const CrPostParams p) {
 
 // One output pixel of the screenshot / same-size display resolve
 // (resolve.cu:1161-1191, 1264-1313).
-__device__ __forceinline__ uint32_t shade_pixel(const CrPostParams& p, int x, int y, int edlDistance,
-                                                uint32_t background) {
+__device__ __forceinline__ uint32_t shade_pixel(const CrPostParams& p, const PostTables& t, int x, int y,
+                                                int edlDistance, uint32_t background) {
     const int pid = x + p.W * y;
     const uint64_t pixel = __ldg(reinterpret_cast<const unsigned long long*>(p.colorbuffer) + pid);
     const float depth = __uint_as_float((uint32_t)(pixel >> 32));
     uint32_t color = (uint32_t)(pixel & 0xffffffffu);
     float edl = 1.0f, ssao = 1.0f;
-    if (p.edl) edl = edl_factor(p, depth, x, y, edlDistance);
+    if (p.edl) edl = edl_factor(p, t, depth, x, y, edlDistance);
     if (p.ssao) ssao = p.shade[pid] * 0.4f + 0.6f;
     if (isinf(depth)) color = background;
     const float shade = edl * ssao;
@@ -225,15 +253,18 @@ __device__ __forceinline__ uint32_t shade_pixel(const CrPostParams& p, int x, in
 }
 
 __global__ void __launch_bounds__(256) k_post_resolve(const CrPostParams p) {
+    __shared__ PostTables t;
+    post_tables(t, threadIdx.y * 32 + threadIdx.x);
+    __syncthreads();
     const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y;
     if (x >= p.outW || y >= p.outH) return;
     if (p.mode == CR_POST_MODE_SCREENSHOT) {
         // supersamplingFactor = source.width / windowWidth (resolve.cu:1290)
-        p.out[x + p.outW * y] = shade_pixel(p, x, y, p.W / p.windowW, p.background);
+        p.out[x + p.outW * y] = shade_pixel(p, t, x, y, p.W / p.windowW, p.background);
         return;
     }
     if (p.outW == p.W && p.outH == p.H) {
-        p.out[x + p.outW * y] = shade_pixel(p, x, y, 1, p.background);
+        p.out[x + p.outW * y] = shade_pixel(p, t, x, y, 1, p.background);
         return;
     }
     // supersampled display (resolve.cu:1193-1257)
@@ -256,7 +287,7 @@ __global__ void __launch_bounds__(256) k_post_resolve(const CrPostParams p) {
                 cg += (CR_BACKGROUND_COLOR >> 8) & 0xff;
                 cbl += (CR_BACKGROUND_COLOR >> 16) & 0xff;
             }
-            if (p.edl) edl += edl_factor(p, depth, sx, sy, f);
+            if (p.edl) edl += edl_factor(p, t, depth, sx, sy, f);
             if (p.ssao) ssao += p.shade[spid];
             numSamples++;
         }

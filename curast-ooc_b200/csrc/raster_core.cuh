@@ -573,21 +573,21 @@ __device__ __forceinline__ uint32_t vertex_cell32(const Mat& M, V3 p, float fa, 
                                                   float Wm1, float Hm1) {
     const V3 q = xform(M, p);
     const float d = -q.z;
-    uint32_t rec = 0;
     const float X = fa * q.x, Y = f * q.y;
-    if (SIDES) {
-        if (d <= 0.0f) return CR_OC_BEHIND;
-        rec = (ndc_beyond(X, d) ? CR_OC_RIGHT : 0u) | (ndc_beyond(-X, d) ? CR_OC_LEFT : 0u) |
-              (ndc_beyond(Y, d) ? CR_OC_TOP : 0u) | (ndc_beyond(-Y, d) ? CR_OC_BOTTOM : 0u);
-    }
+    if (SIDES && d <= 0.0f) return CR_OC_BEHIND;
     const V2 s = to_screen(V3{X / d, Y / d, d}, Wf, Hf);
     const float sx = s.x - 0.5f, sy = s.y - 0.5f;
     if (sx >= 0.0f && sx <= Wm1 && sy >= 0.0f && sy <= Hm1) {
+        // on screen, so beyond no side: ndc_beyond(X, d) is fl(X / d) > 1,
+        // and fl(X / d) > 1 gives sx >= W - 0.5 > W - 1 (fl(X / d) < -1
+        // gives sx <= -0.5), each rounding step being monotone
         const float fx = floorf(sx), fy = floorf(sy);
-        rec |= CR_C32_INSIDE | (sx > fx ? CR_C32_FRACX : 0u) | (sy > fy ? CR_C32_FRACY : 0u) |
+        return CR_C32_INSIDE | (sx > fx ? CR_C32_FRACX : 0u) | (sy > fy ? CR_C32_FRACY : 0u) |
                ((uint32_t)(int)fx << 8) | ((uint32_t)(int)fy << 20);
     }
-    return rec;
+    if (!SIDES) return 0u;
+    return (ndc_beyond(X, d) ? CR_OC_RIGHT : 0u) | (ndc_beyond(-X, d) ? CR_OC_LEFT : 0u) |
+           (ndc_beyond(Y, d) ? CR_OC_TOP : 0u) | (ndc_beyond(-Y, d) ? CR_OC_BOTTOM : 0u);
 }
 
 // cell_culled on 32-bit records.

@@ -824,6 +824,9 @@ class Context:
         _check(load().cr_mesh_create_compressed(self.h, ctypes.byref(d), ctypes.byref(out)))
         return out.value
 
+    def mesh_destroy(self, mesh):
+        _check(load().cr_mesh_destroy(self.h, int(mesh)))
+
     def mesh_device_arrays(self, mesh):
         p, i, c = _u64(), _u64(), _u64()
         _check(load().cr_mesh_device_arrays(self.h, mesh, ctypes.byref(p), ctypes.byref(i), ctypes.byref(c)))

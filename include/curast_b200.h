@@ -481,7 +481,8 @@ typedef struct cr_glb_mesh {
     float aabb_max[3];
 } cr_glb_mesh;
 
-/* Parses a copy of the file's bytes; CR_ERR_INVALID (message in
+/* Reads the file's bytes during the call (they are not kept; primitives are
+ * converted on up to 16 host threads); CR_ERR_INVALID (message in
  * cr_last_error) for anything malformed or outside the subset above. */
 cr_status cr_glb_open(const void* bytes, uint64_t size, cr_glb** out);
 cr_status cr_glb_open_file(const char* path, cr_glb** out);

@@ -160,6 +160,9 @@ def harness():
                                    _vp, _vp, _vp]
         lib.refh_post.restype = _i32
         lib.refh_post.argtypes = [_vp, _i32, _i32, _vp, _i32, _i32, _i32, _i32, _i32, _i32, _u32, _vp]
+        lib.refh_post_timed.restype = _i32
+        lib.refh_post_timed.argtypes = [_vp, _i32, _i32, _vp, _i32, _i32, _i32, _i32, _i32, _i32, _u32, _vp, _i32,
+                                        ctypes.POINTER(_f32)]
         lib.refh_mat4_mul.restype = None
         lib.refh_mat4_mul.argtypes = [_vp, _vp, _vp]
         lib.refh_sizeof_cmesh.restype = _i32
@@ -216,6 +219,22 @@ class Reference:
         if rc != 0:
             raise RuntimeError(f"refh_post: {rc} {self.lib.refh_last_error().decode()}")
         return out
+
+    def post_timed(self, colorbuffer, W, H, proj, edl, ssao, reps, mode=0, window_width=None, out_size=None,
+                   background=0xFFFFFFFF):
+        """The reference's post kernels run `reps` times back to back; returns
+        (mean ms of one pass, output of the last)."""
+        cb = np.ascontiguousarray(colorbuffer, np.uint64)
+        pr = np.ascontiguousarray(np.asarray(proj, np.float32).reshape(16))
+        ow, oh = out_size if out_size else (W, H)
+        out = np.empty((W * H) if mode == 0 else (ow * oh), np.uint32)
+        ms = _f32()
+        rc = self.lib.refh_post_timed(cb.ctypes.data, W, H, pr.ctypes.data, int(edl), int(ssao), int(mode),
+                                      int(window_width or W), int(ow), int(oh), int(background), out.ctypes.data,
+                                      int(reps), ctypes.byref(ms))
+        if rc != 0:
+            raise RuntimeError(f"refh_post_timed: {rc} {self.lib.refh_last_error().decode()}")
+        return float(ms.value), out
 
     def mesh_compressed_host(self, packed, qpos, nT, col, aabb_min, aabb_max, index_min, index_max):
         packed = np.ascontiguousarray(packed, np.uint32)

@@ -477,10 +477,13 @@ int refh_frame(const int32_t* meshIds, const float* worlds, uint32_t nInst, cons
 // (kernel_ssaoOcclusion + kernel_ssaoBlur) when `ssao`, then the screenshot
 // resolve (mode 0, out W*H) or the display resolve (mode 1) written to a CUDA
 // array through a surface object, as the OpenGL surface it normally writes
-// (out outW*outH).  proj: the camera's 16 floats.
-int refh_post(const uint64_t* colorbuffer, int W, int H, const float* proj, int edl, int ssao, int mode, int windowW,
-              int outW, int outH, uint32_t background, uint32_t* out) {
-    if (W <= 0 || H <= 0) return -3;
+// (out outW*outH).  proj: the camera's 16 floats.  refh_post_timed repeats
+// the kernel sequence `reps` times between two events and writes the mean
+// milliseconds of one sequence to *ms (the output is that of the last).
+int refh_post_timed(const uint64_t* colorbuffer, int W, int H, const float* proj, int edl, int ssao, int mode,
+                    int windowW, int outW, int outH, uint32_t background, uint32_t* out, int reps, float* ms) {
+    if (W <= 0 || H <= 0 || reps < 1) return -3;
+    CUevent e0 = nullptr, e1 = nullptr;
     CK(g_drv.p_cuCtxSetCurrent(g_ctx));
     const uint64_t P = (uint64_t)W * H;
     CUdeviceptr d_cb = 0, d_occ = 0, d_shade = 0, d_shot = 0, d_state = 0;
@@ -492,6 +495,8 @@ int refh_post(const uint64_t* colorbuffer, int W, int H, const float* proj, int 
             if (q) g_drv.p_cuMemFree(q);
         if (surf) g_drv.p_cuSurfObjectDestroy(surf);
         if (arr) g_drv.p_cuArrayDestroy(arr);
+        if (e0) g_drv.p_cuEventDestroy(e0);
+        if (e1) g_drv.p_cuEventDestroy(e1);
     };
 #define CKP(call)                   \
     do {                            \
@@ -514,19 +519,11 @@ int refh_post(const uint64_t* colorbuffer, int W, int H, const float* proj, int 
     size_t ctsz = 0;
     CKP(g_drv.p_cuModuleGetGlobal(&d_ctarget, &ctsz, g_mod_resolve, "c_target"));
     CKP(g_drv.p_cuMemcpyHtoD(d_ctarget, &target, sizeof(target)));
-    if (ssao) {
-        void* a[] = {&d_occ, &d_shade};
-        CKP(g_drv.p_cuLaunchKernel(g_ssaoOcc, (W + 15) / 16, (H + 15) / 16, 1, 16, 16, 1, 0, 0, a, nullptr));
-        CKP(g_drv.p_cuLaunchKernel(g_ssaoBlur, (W + 15) / 16, (H + 15) / 16, 1, 16, 16, 1, 0, 0, a, nullptr));
-    }
     bool bEdl = edl != 0, bSsao = ssao != 0;
+    int wh = (int)((int64_t)windowW * H / W);
+    int mouse = -1;
     if (mode == 0) {
         CKP(g_drv.p_cuMemAlloc(&d_shot, P * 4));
-        int wh = (int)((int64_t)windowW * H / W);
-        void* a[] = {&d_shot, &d_shade, &bEdl, &bSsao, &windowW, &wh, &background};
-        CKP(g_drv.p_cuLaunchKernel(g_screenshot, (W + 15) / 16, (H + 15) / 16, 1, 16, 16, 1, 0, 0, a, nullptr));
-        CKP(g_drv.p_cuCtxSynchronize());
-        CKP(g_drv.p_cuMemcpyDtoH(out, d_shot, P * 4));
     } else {
         CUDA_ARRAY3D_DESCRIPTOR ad;
         memset(&ad, 0, sizeof(ad));
@@ -542,10 +539,38 @@ int refh_post(const uint64_t* colorbuffer, int W, int H, const float* proj, int 
         rd.resType = CU_RESOURCE_TYPE_ARRAY;
         rd.res.array.hArray = arr;
         CKP(g_drv.p_cuSurfObjectCreate(&surf, &rd));
-        int mouse = -1;
-        void* a[] = {&surf, &d_shade, &outW, &outH, &mouse, &mouse, &d_state, &bEdl, &bSsao, &background};
-        CKP(g_drv.p_cuLaunchKernel(g_display, (outW + 15) / 16, (outH + 15) / 16, 1, 16, 16, 1, 0, 0, a, nullptr));
-        CKP(g_drv.p_cuCtxSynchronize());
+    }
+    if (ms) {
+        CKP(g_drv.p_cuEventCreate(&e0, CU_EVENT_DEFAULT));
+        CKP(g_drv.p_cuEventCreate(&e1, CU_EVENT_DEFAULT));
+        CKP(g_drv.p_cuEventRecord(e0, 0));
+    }
+    for (int r = 0; r < reps; r++) {
+        if (ssao) {
+            void* a[] = {&d_occ, &d_shade};
+            CKP(g_drv.p_cuLaunchKernel(g_ssaoOcc, (W + 15) / 16, (H + 15) / 16, 1, 16, 16, 1, 0, 0, a, nullptr));
+            CKP(g_drv.p_cuLaunchKernel(g_ssaoBlur, (W + 15) / 16, (H + 15) / 16, 1, 16, 16, 1, 0, 0, a, nullptr));
+        }
+        if (mode == 0) {
+            void* a[] = {&d_shot, &d_shade, &bEdl, &bSsao, &windowW, &wh, &background};
+            CKP(g_drv.p_cuLaunchKernel(g_screenshot, (W + 15) / 16, (H + 15) / 16, 1, 16, 16, 1, 0, 0, a, nullptr));
+        } else {
+            void* a[] = {&surf, &d_shade, &outW, &outH, &mouse, &mouse, &d_state, &bEdl, &bSsao, &background};
+            CKP(g_drv.p_cuLaunchKernel(g_display, (outW + 15) / 16, (outH + 15) / 16, 1, 16, 16, 1, 0, 0, a,
+                                       nullptr));
+        }
+    }
+    if (ms) {
+        CKP(g_drv.p_cuEventRecord(e1, 0));
+        CKP(g_drv.p_cuEventSynchronize(e1));
+        float t = 0.0f;
+        CKP(g_drv.p_cuEventElapsedTime(&t, e0, e1));
+        *ms = t / (float)reps;
+    }
+    CKP(g_drv.p_cuCtxSynchronize());
+    if (mode == 0) {
+        CKP(g_drv.p_cuMemcpyDtoH(out, d_shot, P * 4));
+    } else {
         CUDA_MEMCPY2D cp;
         memset(&cp, 0, sizeof(cp));
         cp.srcMemoryType = CU_MEMORYTYPE_ARRAY;
@@ -560,6 +585,12 @@ int refh_post(const uint64_t* colorbuffer, int W, int H, const float* proj, int 
     cleanup();
     return 0;
 #undef CKP
+}
+
+int refh_post(const uint64_t* colorbuffer, int W, int H, const float* proj, int edl, int ssao, int mode, int windowW,
+              int outW, int outH, uint32_t background, uint32_t* out) {
+    return refh_post_timed(colorbuffer, W, H, proj, edl, ssao, mode, windowW, outW, outH, background, out, 1,
+                           nullptr);
 }
 
 }  // extern "C"
