@@ -222,6 +222,12 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # distributed plumbing (replicas)
 # ---------------------------------------------------------------------------
+def step_spread(ms_steps):
+    """Median and 99th percentile of the per-step device times (this rank)."""
+    a = np.asarray(ms_steps, np.float64)
+    return {"p50": float(np.percentile(a, 50)), "p99": float(np.percentile(a, 99)), "steps": int(a.size)}
+
+
 def init_dist(args, backend=None):
     """One process per GPU (RANK / LOCAL_RANK / WORLD_SIZE / MASTER_* from the
     launcher).  NCCL on GPUs; gloo when there is no GPU (the CPU tests)."""
@@ -458,7 +464,7 @@ def run_ours(args, rank, world, local):
         "config": {"workload": wl["name"], "desc": wl["desc"], "triangles": T, "vertices": V,
                    "width": W, "height": H, "parallelism": f"replicas x{world}",
                    "l2": "flushed between steps" if flush is not None else "inputs larger than L2",
-                   "stage_ms": stage_ms, "dominant_stage": dominant,
+                   "stage_ms": stage_ms, "dominant_stage": dominant, "step_ms": step_spread(ms_steps),
                    "nontrivial": int(fstats.nontrivial), "huge_tiles": int(fstats.huge_tiles),
                    "hierarchical_cull": {"work_items": items, "work_items_drawn": items_drawn,
                                          "vertex_chunks": chunks, "vertex_chunks_evaluated": chunks_eval,
@@ -549,7 +555,8 @@ def run_post(args, rank, world, local, wl):
     torch.cuda.synchronize()
     barrier(world)
     clk = clocks.stop() if clocks else None
-    ms = max_over_ranks(float(np.mean([a.elapsed_time(b) for a, b in evs])), world)
+    post_steps = [a.elapsed_time(b) for a, b in evs]
+    ms = max_over_ranks(float(np.mean(post_steps)), world)
 
     # end to end: the colorbuffer from pinned host memory, the image back
     host_cb = torch.empty(W * H, dtype=torch.int64, pin_memory=True)
@@ -588,7 +595,7 @@ def run_post(args, rank, world, local, wl):
         "data": "synthetic (seeded)",
         "config": {"workload": wl["name"], "desc": wl["desc"], "width": W, "height": H, "out_width": oW,
                    "out_height": oH, "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (165 MB working set per pass)"},
+                   "l2": "inputs larger than L2 (165 MB working set per pass)", "step_ms": step_spread(post_steps)},
         "e2e": {"value": world * W * H / (e2e * 1e-3) / 1e6, "unit": "Mpx/s", "ms_per_step": e2e,
                 "h2d_bytes_per_step": 8 * W * H, "d2h_bytes_per_step": 4 * oW * oH},
         "roofline": {"kernel": "k_ssao_occlusion + k_ssao_blur + k_post_resolve (one pass)", "bound": "hbm",
@@ -851,7 +858,7 @@ def run_batched(args, rank, world, local, wl):
         "config": {"workload": wl["name"], "desc": wl["desc"], "triangles": T, "vertices": V, "views": nv,
                    "pixels": P, "parallelism": f"replicas x{world}",
                    "l2": "per-step visbuffers and images ({:.1f} GB) exceed L2".format(28 * P / 1e9),
-                   "stage_ms": stage_ms, "dominant_stage": dominant,
+                   "stage_ms": stage_ms, "dominant_stage": dominant, "step_ms": step_spread(ms_steps),
                    "nontrivial": int(fstats.nontrivial), "huge_tiles": int(fstats.huge_tiles),
                    "plain_loop": {"ms_per_step": plain_ms, "views_per_s": world * nv / (plain_ms * 1e-3),
                                   "note": f"{nv} cr_render calls per step, same GPU, same outputs"},

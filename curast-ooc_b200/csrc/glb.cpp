@@ -29,6 +29,10 @@
 //     pre-order walk visits primitive 0, the children's subtrees, then the
 //     node's other primitives.
 #include <cuda_runtime.h>
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <array>
@@ -696,20 +700,24 @@ cr_status cr_glb_open(const void* bytes, uint64_t size, cr_glb** out) {
 cr_status cr_glb_open_file(const char* path, cr_glb** out) {
     if (!path || !out) return fail(CR_ERR_INVALID, "cr_glb_open_file: NULL argument");
     *out = nullptr;
-    FILE* f = fopen(path, "rb");
-    if (!f) return fail(CR_ERR_NOT_FOUND, "glb: cannot open %s", path);
-    std::vector<uint8_t> bytes;
-    if (fseek(f, 0, SEEK_END) == 0) {
-        const long n = ftell(f);
-        if (n > 0 && fseek(f, 0, SEEK_SET) == 0) {
-            bytes.resize((size_t)n);
-            if (fread(bytes.data(), 1, (size_t)n, f) != (size_t)n) bytes.clear();
-        }
+    // mapped read-only: the parse copies what it keeps, so the file's pages
+    // are only read once, straight from the page cache
+    const int fd = open(path, O_RDONLY);
+    if (fd < 0) return fail(CR_ERR_NOT_FOUND, "glb: cannot open %s", path);
+    struct stat st;
+    if (fstat(fd, &st) != 0 || st.st_size <= 0) {
+        close(fd);
+        return fail(CR_ERR_INVALID, "glb: cannot read %s", path);
     }
-    fclose(f);
-    if (bytes.empty()) return fail(CR_ERR_INVALID, "glb: cannot read %s", path);
+    const size_t n = (size_t)st.st_size;
+    void* map = mmap(nullptr, n, PROT_READ, MAP_PRIVATE, fd, 0);
+    close(fd);
+    if (map == MAP_FAILED) return fail(CR_ERR_INVALID, "glb: cannot map %s", path);
+    madvise(map, n, MADV_SEQUENTIAL);
     std::unique_ptr<cr_glb> g(new cr_glb());
-    if (cr_status s = parse(*g, bytes.data(), bytes.size())) return s;
+    const cr_status s = parse(*g, (const uint8_t*)map, n);
+    munmap(map, n);
+    if (s) return s;
     *out = g.release();
     return CR_OK;
 }
