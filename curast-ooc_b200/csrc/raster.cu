@@ -28,6 +28,9 @@
 
 namespace {
 
+#ifndef VX_UNROLL
+#define VX_UNROLL 4
+#endif
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS) k_vertex(const CrFrameParams p) {
     const float fa = p.f / p.aspect;
@@ -48,14 +51,26 @@ __global__ void __launch_bounds__(THREADS) k_vertex(const CrFrameParams p) {
         const uint32_t v1 = min(v0 + (uint32_t)CR_VCHUNK, nV);
         const GeomRef g = geom_of(I);
         const Mat M = load_mat(p.world_view + 4ull * lo);
-        if (p.cellMode == CR_REC_CELLS) {
-            uint64_t* out = reinterpret_cast<uint64_t*>(p.outcodes) + __ldg(&I->outBase);
-            for (uint32_t v = v0 + threadIdx.x; v < v1; v += THREADS)
-                out[v] = vertex_cell_record(M, pos_of(g, v), fa, p.f, Wf, Hf, p.W, p.H);
-        } else {
-            uint8_t* out = p.outcodes + __ldg(&I->outBase);
-            for (uint32_t v = v0 + threadIdx.x; v < v1; v += THREADS)
-                out[v] = (uint8_t)vertex_outcode(M, pos_of(g, v), fa, p.f);
+        // each thread loads VX_UNROLL positions before transforming any:
+        // the pass is latency-bound on these gathers
+        constexpr int U = VX_UNROLL;
+        for (uint32_t v = v0 + threadIdx.x; v < v1; v += U * THREADS) {
+            V3 q[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (v + u * THREADS < v1) q[u] = pos_of(g, v + u * THREADS);
+            if (p.cellMode == CR_REC_CELLS) {
+                uint64_t* out = reinterpret_cast<uint64_t*>(p.outcodes) + __ldg(&I->outBase);
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                    if (v + u * THREADS < v1)
+                        out[v + u * THREADS] = vertex_cell_record(M, q[u], fa, p.f, Wf, Hf, p.W, p.H);
+            } else {
+                uint8_t* out = p.outcodes + __ldg(&I->outBase);
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                    if (v + u * THREADS < v1) out[v + u * THREADS] = (uint8_t)vertex_outcode(M, q[u], fa, p.f);
+            }
         }
     }
 }
