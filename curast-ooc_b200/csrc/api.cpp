@@ -1185,6 +1185,9 @@ cr_status cr_postprocess(cr_context* ctx, const cr_post_desc* d, void* stream_) 
     p.p11 = d->proj11;
     p.edl = (d->flags & CR_POST_EDL) ? 1 : 0;
     p.ssao = (d->flags & CR_POST_SSAO) ? 1 : 0;
+    p.fast = (d->flags & CR_POST_FAST_MATH) ? 1 : 0;
+    if (d->flags & ~(uint32_t)(CR_POST_EDL | CR_POST_SSAO | CR_POST_FAST_MATH))
+        return fail(CR_ERR_INVALID, "cr_postprocess: unknown flags 0x%x", d->flags);
     p.background = d->background;
     p.out = (uint32_t*)d->d_rgba;
     if (d->mode == CR_POST_SCREENSHOT) {

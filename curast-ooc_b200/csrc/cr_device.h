@@ -247,6 +247,7 @@ struct CrPostParams {
     int32_t W, H;
     float p00, p11;               // proj[0][0], proj[1][1]
     int32_t edl, ssao;            // 1: apply
+    int32_t fast;                 // 1: the reference build's fast-math approximations
     int32_t mode;                 // CR_POST_MODE_*
     int32_t windowW;              // screenshot: EDL distance = W / windowW
     int32_t outW, outH;           // output size (display: W / outW = supersampling factor)

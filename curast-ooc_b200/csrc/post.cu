@@ -1,319 +1,11 @@
-// post.cu -- the reference's image post-processing after the colour resolve,
-// on the 64-bit colorbuffer (depth bits << 32 | RGBA8) that cr_render writes:
-//
-//   eye-dome lighting   getEdlShadingFactor            resolve.cu:234-268
-//   ambient occlusion   kernel_ssaoOcclusion,          resolve.cu:276-472,549-568
-//                       kernel_ssaoBlur                resolve.cu:570-640
-//   final resolves      kernel_resolve_colorbuffer_to_screenshot   resolve.cu:1264-1313
-//                       kernel_resolve_colorbuffer_to_opengl_2D    resolve.cu:1143-1260
-//                       (its display surface is a device RGBA8 buffer here;
-//                       when the display is smaller than the colorbuffer it
-//                       averages factor x factor blocks: supersampling)
-//
-// Float semantics as the rest of the library (-fmad=false, IEEE division and
-// square root): every expression keeps the reference's operation order, so
-// the image matches the reference's IEEE-mode build up to the last-place
-// differences of the transcendental functions (cosf, sinf, log2f, expf;
-// sincosf for the per-sample angle).
-// One thread per pixel; SSAO is the only stage that reads far neighbours
-// (32 samples within a depth-proportional radius).
-#include <cuda_runtime.h>
-#include <cstdint>
+// post.cu -- the IEEE post-processing kernels (post_kernels.cuh) and the
+// launch entry, which hands CR_POST_FAST_MATH passes to post_fast.cu.
+#include "post_kernels.cuh"
 
-#include "cr_device.h"
-
-namespace {
-
-struct P3 {
-    float x, y, z;
-};
-
-__device__ __forceinline__ P3 padd(P3 a, P3 b) { return P3{a.x + b.x, a.y + b.y, a.z + b.z}; }
-__device__ __forceinline__ P3 psub(P3 a, P3 b) { return P3{a.x - b.x, a.y - b.y, a.z - b.z}; }
-__device__ __forceinline__ P3 pmul(P3 a, float s) { return P3{a.x * s, a.y * s, a.z * s}; }
-__device__ __forceinline__ float pdot(P3 a, P3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
-__device__ __forceinline__ P3 pcross(P3 x, P3 y) {
-    return P3{x.y * y.z - y.y * x.z, x.z * y.x - y.z * x.x, x.x * y.y - y.x * x.y};
-}
-// glm::normalize: v * inversesqrt(dot(v, v)), inversesqrt(x) = 1 / sqrt(x)
-__device__ __forceinline__ P3 pnormalize(P3 v) { return pmul(v, 1.0f / sqrtf(pdot(v, v))); }
-
-__device__ __forceinline__ float fclamp(float v, float lo, float hi) {  // utils.cuh:205-213
-    if (v < lo) return lo;
-    if (v > hi) return hi;
-    return v;
-}
-__device__ __forceinline__ int iclamp(int v, int lo, int hi) {
-    if (v < lo) return lo;
-    if (v > hi) return hi;
-    return v;
-}
-
-__device__ __forceinline__ float depth_at(const CrPostParams& p, int pid) {
-    return __uint_as_float((uint32_t)(__ldg(reinterpret_cast<const unsigned long long*>(p.colorbuffer) + pid) >> 32));
-}
-
-// The angle-only terms of both effects, the same for every pixel: computed
-// once per block into shared memory by the same device functions the
-// per-pixel expressions would call, so the values are bit-identical.
-struct PostTables {
-    float edlCos[8], edlSin[8];                 // cosf / sinf(2 * 3.1415 * i / 8)
-    float sinTheta[32], cosTheta[32], rad[32];  // sqrtf(fi), sqrtf(1 - fi), sqrtf((i + 1) / 32)
-};
-
-__device__ __forceinline__ void post_tables(PostTables& t, int tid) {
-    if (tid < 8) {
-        const float u = 2.0f * 3.1415f * float(tid) / float(8);
-        t.edlCos[tid] = cosf(u);
-        t.edlSin[tid] = sinf(u);
-    }
-    if (tid < 32) {
-        const float INV_N = 1.0f / float(32);
-        const float fi = (float(tid) + 0.5f) * INV_N;
-        t.sinTheta[tid] = sqrtf(fi);
-        t.cosTheta[tid] = sqrtf(1.0f - fi);
-        t.rad[tid] = sqrtf(float(tid + 1) * INV_N);
-    }
-}
-
-// getEdlShadingFactor (resolve.cu:234-268): eight neighbours on a circle of
-// `distance` pixels, positions truncated to integers as the reference's
-// int-parameter lambda truncates them.
-__device__ float edl_factor(const CrPostParams& p, const PostTables& t, float depth, int x, int y, int distance) {
-    float sum = 0.0f;
-    const int numSamples = 8;
-    const float ld = log2f(depth);
-    for (int i = 0; i < numSamples; i++) {
-        const float dx = float(distance) * t.edlCos[i];
-        const float dy = float(distance) * t.edlSin[i];
-        const int nx = (int)((float)x + dx), ny = (int)((float)y + dy);
-        float nd = INFINITY;
-        if (nx >= 0 && nx < p.W && ny >= 0 && ny < p.H) nd = depth_at(p, nx + p.W * ny);
-        sum += fmaxf(ld - log2f(nd), 0.0f);
-    }
-    const float response = sum / float(numSamples);
-    const float edlStrength = 0.9f;
-    float shade = expf(-response * 300.0f * edlStrength);
-    shade = fclamp(shade, 0.3f, 1.0f);
-    return shade * 0.8f + 0.2f;
-}
-
-// ssao_viewPos (resolve.cu:279-287)
-__device__ __forceinline__ P3 view_pos(const CrPostParams& p, float px, float py, float depth) {
-    const float ndc_x = (2.0f * (px + 0.5f) / float(p.W)) - 1.0f;
-    const float ndc_y = (2.0f * (py + 0.5f) / float(p.H)) - 1.0f;
-    return P3{ndc_x * depth / p.p00, ndc_y * depth / p.p11, depth};
-}
-
-// ssao_normal (resolve.cu:299-336)
-__device__ P3 view_normal(const CrPostParams& p, int x, int y, float d0) {
-    auto dep = [&](int nx, int ny) { return depth_at(p, iclamp(ny, 0, p.H - 1) * p.W + iclamp(nx, 0, p.W - 1)); };
-    const float dr = dep(x + 1, y), dl = dep(x - 1, y);
-    const float dd = dep(x, y + 1), du = dep(x, y - 1);
-    const bool use_right = fabsf(dr - d0) < fabsf(d0 - dl);
-    const bool use_down = fabsf(dd - d0) < fabsf(d0 - du);
-    const int sx = use_right ? +1 : -1;
-    const int sy = use_down ? +1 : -1;
-    const float dh = use_right ? dr : dl;
-    const float dv = use_down ? dd : du;
-    if (isinf(dh) || isinf(dv)) return P3{0.0f, 0.0f, -1.0f};
-    const P3 P = view_pos(p, float(x), float(y), d0);
-    const P3 Ph = view_pos(p, float(x + sx), float(y), dh);
-    const P3 Pv = view_pos(p, float(x), float(y + sy), dv);
-    const P3 dPh = (sx > 0) ? psub(Ph, P) : psub(P, Ph);
-    const P3 dPv = (sy > 0) ? psub(Pv, P) : psub(P, Pv);
-    const P3 N = pnormalize(pcross(dPh, dPv));
-    return (N.z > 0.0f) ? P3{-N.x, -N.y, -N.z} : N;
-}
-
-// float -> int as the GPU converts (truncation, saturating, NaN -> 0)
-__device__ __forceinline__ int to_int(float v) { return __float2int_rz(v); }
-
-// getSSAOShadingFactor (resolve.cu:350-470)
-__device__ float ssao_factor(const CrPostParams& p, const PostTables& t, float center_depth, int x, int y) {
-    if (isinf(center_depth) || center_depth <= 0.0f) return 1.0f;
-    const int NUM_SAMPLES = 32;
-    const float RADIUS_FRACTION = 0.2025f;
-    const float INTENSITY = 1.1f;
-    const float RANGE_MUL = 2.5f;
-    const float BIAS_FRACTION = 0.05f;
-    const float world_radius = center_depth * RADIUS_FRACTION;
-    const float bias = BIAS_FRACTION * world_radius;
-    const P3 P = view_pos(p, float(x), float(y), center_depth);
-    const P3 N = view_normal(p, x, y, center_depth);
-    auto dep = [&](int nx, int ny) { return depth_at(p, iclamp(ny, 0, p.H - 1) * p.W + iclamp(nx, 0, p.W - 1)); };
-    const float dz_left = center_depth - dep(x - 1, y);
-    const float dz_right = dep(x + 1, y) - center_depth;
-    const float dz_up = center_depth - dep(x, y - 1);
-    const float dz_down = dep(x, y + 1) - center_depth;
-    const float dz_dx = (fabsf(dz_left) < fabsf(dz_right)) ? dz_left : dz_right;
-    const float dz_dy = (fabsf(dz_up) < fabsf(dz_down)) ? dz_up : dz_down;
-    const P3 up = (fabsf(N.z) < 0.95f) ? P3{0.0f, 0.0f, 1.0f} : P3{1.0f, 0.0f, 0.0f};
-    const P3 T = pnormalize(pcross(up, N));
-    const P3 B = pcross(N, T);
-    uint32_t h = uint32_t(x) * 2246822519u ^ uint32_t(y) * 3266489917u;
-    h ^= h >> 13;
-    h *= 0xbf58476du;
-    h ^= h >> 31;
-    const float rand_angle = float(h >> 8) * (6.28318530f / float(1 << 24));
-    float occlusion = 0.0f;
-    const float INV_N = 1.0f / float(NUM_SAMPLES);
-    const float GOLDEN_ANGLE = 2.39996323f;
-    for (int i = 0; i < NUM_SAMPLES; ++i) {
-        const float sin_theta = t.sinTheta[i];
-        const float cos_theta = t.cosTheta[i];
-        const float phi = float(i) * GOLDEN_ANGLE + rand_angle;
-        float sphi, cphi;
-        sincosf(phi, &sphi, &cphi);
-        const P3 dir = padd(padd(pmul(T, sin_theta * cphi), pmul(B, sin_theta * sphi)), pmul(N, cos_theta));
-        const float r = world_radius * t.rad[i];
-        const P3 S = padd(P, pmul(dir, r));
-        if (S.z <= 0.001f) continue;
-        // ssao_screenPos (resolve.cu:289-296)
-        const float inv_z = 1.0f / S.z;
-        const float spx = ((p.p00 * S.x * inv_z) + 1.0f) * 0.5f * float(p.W) - 0.5f;
-        const float spy = ((p.p11 * S.y * inv_z) + 1.0f) * 0.5f * float(p.H) - 0.5f;
-        const int sx = iclamp(to_int(spx), 0, p.W - 1);
-        const int sy = iclamp(to_int(spy), 0, p.H - 1);
-        const float actual_depth = depth_at(p, sy * p.W + sx);
-        if (isinf(actual_depth)) continue;
-        const float dx = spx - float(x);
-        const float dy = spy - float(y);
-        const float expected_z = center_depth + dz_dx * dx + dz_dy * dy;
-        const float dz = expected_z - actual_depth;
-        if (dz > bias && dz < world_radius * RANGE_MUL) {
-            const float range_falloff = 1.0f - dz / (world_radius * RANGE_MUL);
-            occlusion += range_falloff * cos_theta;
-        }
-    }
-    return fclamp(1.0f - occlusion * INV_N * INTENSITY, 0.0f, 1.0f);
-}
-
-// kernel_ssaoOcclusion (resolve.cu:549-568)
-__global__ void __launch_bounds__(256) k_ssao_occlusion(const CrPostParams p) {
-    __shared__ PostTables t;
-    post_tables(t, threadIdx.y * 32 + threadIdx.x);
-    __syncthreads();
-    const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y;
-    if (x >= p.W || y >= p.H) return;
-    const int pid = x + p.W * y;
-    const float depth = depth_at(p, pid);
-    const float ssao = ssao_factor(p, t, depth, x, y);
-    p.occlusion[pid] = ((uint64_t)__float_as_uint(depth) << 32) | (uint64_t)__float_as_uint(ssao);
-}
-
-// kernel_ssaoBlur (resolve.cu:570-640): 7x7 Gaussian (the reference computes
-// a bilateral weight and then sets it to 1)
-__global__ void __launch_bounds__(256) k_ssao_blur(const CrPostParams p) {
-    const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y;
-    if (x >= p.W || y >= p.H) return;
-    const int centerIdx = y * p.W + x;
-    const float center_depth = __uint_as_float((uint32_t)(p.occlusion[centerIdx] >> 32));
-    if (isinf(center_depth)) {
-        p.shade[centerIdx] = 1.0f;
-        return;
-    }
-    const int RADIUS = 3;
-    const float gaussian[7] = {0.015625f, 0.09375f, 0.234375f, 0.3125f, 0.234375f, 0.09375f, 0.015625f};
-    float sum = 0.0f, totalWeight = 0.0f;
-    for (int dy = -RADIUS; dy <= RADIUS; dy++)
-        for (int dx = -RADIUS; dx <= RADIUS; dx++) {
-            const int nx = iclamp(x + dx, 0, p.W - 1);
-            const int ny = iclamp(y + dy, 0, p.H - 1);
-            const uint64_t occ = p.occlusion[ny * p.W + nx];
-            const float sample_occlusion = __uint_as_float((uint32_t)(occ & 0xffffffffu));
-            const float w = gaussian[dx + RADIUS] * gaussian[dy + RADIUS] * 1.0f;
-            sum += w * sample_occlusion;
-            totalWeight += w;
-        }
-    float shade = 1.0f;
-    if (totalWeight > 0.0f) shade = sum / totalWeight;
-    p.shade[centerIdx] = shade;
-}
-
-// One output pixel of the screenshot / same-size display resolve
-// (resolve.cu:1161-1191, 1264-1313).
-__device__ __forceinline__ uint32_t shade_pixel(const CrPostParams& p, const PostTables& t, int x, int y,
-                                                int edlDistance, uint32_t background) {
-    const int pid = x + p.W * y;
-    const uint64_t pixel = __ldg(reinterpret_cast<const unsigned long long*>(p.colorbuffer) + pid);
-    const float depth = __uint_as_float((uint32_t)(pixel >> 32));
-    uint32_t color = (uint32_t)(pixel & 0xffffffffu);
-    float edl = 1.0f, ssao = 1.0f;
-    if (p.edl) edl = edl_factor(p, t, depth, x, y, edlDistance);
-    if (p.ssao) ssao = p.shade[pid] * 0.4f + 0.6f;
-    if (isinf(depth)) color = background;
-    const float shade = edl * ssao;
-    uint32_t out = color & 0xff000000u;
-    for (int k = 0; k < 3; ++k) {
-        const float c = shade * float((color >> (8 * k)) & 0xffu);
-        out |= ((uint32_t)(unsigned char)__float2uint_rz(c)) << (8 * k);
-    }
-    return out;
-}
-
-__global__ void __launch_bounds__(256) k_post_resolve(const CrPostParams p) {
-    __shared__ PostTables t;
-    post_tables(t, threadIdx.y * 32 + threadIdx.x);
-    __syncthreads();
-    const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y;
-    if (x >= p.outW || y >= p.outH) return;
-    if (p.mode == CR_POST_MODE_SCREENSHOT) {
-        // supersamplingFactor = source.width / windowWidth (resolve.cu:1290)
-        p.out[x + p.outW * y] = shade_pixel(p, t, x, y, p.W / p.windowW, p.background);
-        return;
-    }
-    if (p.outW == p.W && p.outH == p.H) {
-        p.out[x + p.outW * y] = shade_pixel(p, t, x, y, 1, p.background);
-        return;
-    }
-    // supersampled display (resolve.cu:1193-1257)
-    const int f = p.W / p.outW;
-    float cr = 0.0f, cg = 0.0f, cbl = 0.0f;
-    float edl = 0.0f, ssao = 0.0f;
-    int numSamples = 0;
-    for (int dx = 0; dx < f; dx++)
-        for (int dy = 0; dy < f; dy++) {
-            const int sx = f * x + dx, sy = f * y + dy;
-            const int spid = sx + p.W * sy;
-            const uint64_t pixel = __ldg(reinterpret_cast<const unsigned long long*>(p.colorbuffer) + spid);
-            const float depth = __uint_as_float((uint32_t)(pixel >> 32));
-            const uint32_t C = (uint32_t)(pixel & 0xffffffffu);
-            cr += (C >> 0) & 0xff;
-            cg += (C >> 8) & 0xff;
-            cbl += (C >> 16) & 0xff;
-            if (isinf(depth)) {  // BACKGROUND_COLOR, HostDeviceInterface.h:37
-                cr += (CR_BACKGROUND_COLOR >> 0) & 0xff;
-                cg += (CR_BACKGROUND_COLOR >> 8) & 0xff;
-                cbl += (CR_BACKGROUND_COLOR >> 16) & 0xff;
-            }
-            if (p.edl) edl += edl_factor(p, t, depth, sx, sy, f);
-            if (p.ssao) ssao += p.shade[spid];
-            numSamples++;
-        }
-    edl = p.edl ? edl / float(numSamples) : 1.0f;
-    ssao = p.ssao ? ssao / float(numSamples) : 1.0f;
-    const float shade = edl * ssao;
-    const float n = float(numSamples);
-    cr = shade * cr / n;
-    cg = shade * cg / n;
-    cbl = shade * cbl / n;
-    const uint32_t r8 = (unsigned char)__float2uint_rz(fclamp(cr, 0.0f, 255.0f));
-    const uint32_t g8 = (unsigned char)__float2uint_rz(fclamp(cg, 0.0f, 255.0f));
-    const uint32_t b8 = (unsigned char)__float2uint_rz(fclamp(cbl, 0.0f, 255.0f));
-    p.out[x + p.outW * y] = r8 | (g8 << 8) | (b8 << 16) | 0xff000000u;
-}
-
-}  // namespace
+int cr_launch_post_fast(const CrPostParams& p, void* stream);
 
 int cr_launch_post(const CrPostParams& p, void* stream) {
-    cudaStream_t st = (cudaStream_t)stream;
-    if (p.ssao) {
-        const dim3 g((p.W + 31) / 32, (p.H + 7) / 8);
-        k_ssao_occlusion<<<g, dim3(32, 8), 0, st>>>(p);
-        k_ssao_blur<<<g, dim3(32, 8), 0, st>>>(p);
-    }
-    const dim3 g((p.outW + 31) / 32, (p.outH + 7) / 8);
-    k_post_resolve<<<g, dim3(32, 8), 0, st>>>(p);
+    if (p.fast) return cr_launch_post_fast(p, stream);
+    launch_post<false>(p, (cudaStream_t)stream);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

@@ -117,6 +117,7 @@ class CrPostDesc(ctypes.Structure):
 
 CR_POST_EDL = 1
 CR_POST_SSAO = 2
+CR_POST_FAST_MATH = 4
 CR_POST_SCREENSHOT = 0
 CR_POST_DISPLAY = 1
 

@@ -271,13 +271,19 @@ cr_status cr_render(cr_context* ctx, const cr_instance* instances, uint32_t coun
  * posts issued on different streams are ordered by the library. */
 #define CR_POST_EDL 1u
 #define CR_POST_SSAO 2u
+/* The transcendental functions, divisions and square roots of both effects
+ * as the reference's own build computes them (it compiles with
+ * --use_fast_math): hardware approximations.  Without the flag they are IEEE
+ * and the image follows the IEEE-mode restatement; either way colours stay
+ * within a few units of the reference's image of the same build mode. */
+#define CR_POST_FAST_MATH 4u
 #define CR_POST_SCREENSHOT 0
 #define CR_POST_DISPLAY 1
 typedef struct cr_post_desc {
     uint64_t d_colorbuffer;    /* width*height uint64: depth bits << 32 | RGBA8  */
     int32_t width, height;     /* of the colorbuffer                             */
     float proj00, proj11;      /* the camera's proj[0] and proj[5]               */
-    uint32_t flags;            /* CR_POST_EDL | CR_POST_SSAO                     */
+    uint32_t flags;            /* CR_POST_EDL | CR_POST_SSAO | CR_POST_FAST_MATH */
     int32_t mode;              /* CR_POST_SCREENSHOT or CR_POST_DISPLAY          */
     int32_t window_width;      /* SCREENSHOT: the window width (EDL distance)    */
     int32_t out_width;         /* DISPLAY: the display size                      */

@@ -5,6 +5,11 @@ restatement and against the reference's own post kernels (IEEE-mode build).
 Colours within 1 per 8-bit channel for all but a few pixels whose ambient
 occlusion sits on a sampling decision that the last bit of a transcendental
 function can flip."""
+import json
+import os
+import subprocess
+import sys
+
 import numpy as np
 import pytest
 
@@ -92,3 +97,44 @@ def test_post_rejects_bad_sizes(gpu):
         with pytest.raises(pc.CurastError):
             ctx.postprocess(t.data_ptr(), 100, 60, scenes.perspective(60.0, 1.6), o.data_ptr(), 0, pc.CR_POST_DISPLAY,
                             out_size=(33, 20))
+
+
+def test_fast_math_post_close_to_ieee(gpu):
+    """CR_POST_FAST_MATH (the reference build's approximations) differs from
+    the IEEE pass on a few pixels by a few units, as the reference's own
+    fast-math build differs from its IEEE build (at most 4 on this scene)."""
+    import torch
+
+    W, H = 480, 288
+    ow, oh = W // 2, H // 2
+    mesh, view, proj = _scene(W, H)
+    flags = pc.CR_POST_EDL | pc.CR_POST_SSAO
+    with pc.Context() as ctx:
+        _, _, cb, _ = render_ours(ctx, [mesh], [(0, scenes.identity())], view, proj, W, H)
+        dcb = torch.from_numpy(cb.view(np.int64)).cuda()
+        outs = []
+        for fl in (flags, flags | pc.CR_POST_FAST_MATH):
+            out = torch.empty(ow * oh, dtype=torch.int32, device="cuda")
+            ctx.postprocess(dcb.data_ptr(), W, H, proj, out.data_ptr(), fl, pc.CR_POST_DISPLAY, out_size=(ow, oh))
+            torch.cuda.synchronize()
+            outs.append(out.cpu().numpy().view(np.uint32))
+    ieee, fast = outs
+    for other, what in ((ieee, "IEEE pass"), (ol.post(cb, W, H, proj, True, True, mode=1, out_size=(ow, oh)), "oracle")):
+        d = _diffs(fast, other)
+        assert d.max() <= 6, f"fast vs {what}: max channel difference {d.max()}"
+        assert (d > 1).mean() <= 1e-3, f"fast vs {what}: {(d > 1).sum()} pixels differ by more than 1"
+
+
+def test_fast_math_post_matches_reference_fast_build(gpu):
+    """Against the reference's own post kernels in their native
+    --use_fast_math build (a separate process: the harness holds one build
+    mode per process)."""
+    if not os.path.exists(ol.HARNESS_SO):
+        pytest.skip("reference harness not built")
+    script = os.path.join(os.path.dirname(os.path.abspath(__file__)), "post_fast_build_check.py")
+    res = subprocess.run([sys.executable, script], capture_output=True, text=True, timeout=600)
+    assert res.returncode == 0, res.stderr[-2000:]
+    cases = [json.loads(line) for line in res.stdout.splitlines() if line.startswith("{")]
+    assert len(cases) == 2
+    for c in cases:
+        assert c["max"] <= 3 and c["over1"] <= 1e-3, c
