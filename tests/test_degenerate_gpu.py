@@ -82,3 +82,25 @@ def test_hostile_soup_instanced_every_cull_path(gpu, records):
     assert (ovis != pc.CLEAR_PIXEL).mean() > 0.05
     assert_same_vis(vis, ovis, f"hostile instanced soup (records {records}) vs oracle")
     assert channel_diff(rgba, orgba) <= COLOR_TOL
+
+
+def test_hostile_soup_batched_views_equal_single_views(gpu):
+    """Batched frames (frame cull over views, vertex lists or view masks)
+    on the hostile soup: every view equals cr_render of that view alone."""
+    from test_batch_gpu import assert_views_equal, batched, plain_loop
+
+    m = hostile_soup(8000, seed=227)
+    rng = np.random.default_rng(229)
+    cams = []
+    for k in range(8):
+        W, H = [(256, 160), (200, 200), (96, 160), (320, 180)][k % 4]
+        view = scenes.identity() if k % 2 == 0 else scenes.look_at(rng.uniform(-2, 2, 3), rng.uniform(-1, 1, 3) +
+                                                                     np.array([0.0, 0.0, -4.0]))
+        cams.append((view, scenes.perspective(60.0, W / H), W, H))
+    with pc.Context() as c:
+        h = c.mesh_from_host(*m)
+        for inst in ([(h, scenes.identity())],
+                     [(h, scenes.identity()), (h, scenes.translate_scale(0.5, 0.0, -2.0, 0.7))]):
+            a = batched(c, inst, cams, colorbuffer=True)
+            b = plain_loop(c, inst, cams, colorbuffer=True)
+            assert_views_equal(a, b, f"hostile batched vs plain ({len(inst)} instances)")
