@@ -369,7 +369,7 @@ def run_ours(args, rank, world, local):
         if flush is not None:
             flush.fill_(k)
         evs[k][0].record(stream)
-        ctx.render(inst, cam, vis.data_ptr(), rgba.data_ptr(), flags=pc.CR_RENDER_TIMING, stream=sh)
+        ctx.render(inst, cam, vis.data_ptr(), rgba.data_ptr(), flags=0, stream=sh)
         evs[k][1].record(stream)
     torch.cuda.synchronize()
     barrier(world)
@@ -377,6 +377,16 @@ def run_ours(args, rank, world, local):
     ctx.sync()
     ms_steps = [a.elapsed_time(b) for a, b in evs]
     ms = max_over_ranks(float(np.mean(ms_steps)), world)
+    # per-stage times from as many frames again, with events between the
+    # stages (they keep consecutive kernels from overlapping, so the frame
+    # times above are taken without them)
+    ctx.drain_stage_times()
+    for k in range(args.steps):
+        if flush is not None:
+            flush.fill_(k)
+        ctx.render(inst, cam, vis.data_ptr(), rgba.data_ptr(), flags=pc.CR_RENDER_TIMING, stream=sh)
+    torch.cuda.synchronize()
+    ctx.sync()
     stage_ms, nframes = ctx.drain_stage_times()
     stage_ms = {k: v / max(nframes, 1) for k, v in stage_ms.items()}
 

@@ -33,6 +33,7 @@ namespace {
 #endif
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS) k_vertex(const CrFrameParams p) {
+    pdl_enter();
     const float fa = p.f / p.aspect;
     const float Wf = (float)p.W, Hf = (float)p.H;
     // the chunks the frame cull left for per-vertex records (or every chunk)
@@ -96,6 +97,7 @@ constexpr uint32_t CR_FILL_ZERO = 0x100u;
 
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS) k_cull(const CrFrameParams p) {
+    pdl_enter();
     const int lane = threadIdx.x & 31;
     const float fa = p.f / p.aspect;
     const uint64_t stride = (uint64_t)gridDim.x * THREADS;
@@ -293,6 +295,7 @@ __device__ __forceinline__ TileSrc tile_source(const CrSegment* sg, uint32_t bat
 // decoding code).
 template <int WARPS, bool BOXES, bool PACKED>
 __global__ void __launch_bounds__(WARPS * 32, BOXES ? CR_S1_BOXES_MIN_BLOCKS : 3) k_stage1(const CrFrameParams p) {
+    pdl_enter();
     constexpr int STAGES = BOXES ? 2 : S1_STAGES;
     static_assert(CR_LOCAL_BYTES <= CR_BATCH * 12, "a vertex-list block fits a ring slot");
     __shared__ __align__(128) uint32_t s_idx[WARPS][STAGES][CR_BATCH * 3];
@@ -543,6 +546,9 @@ __global__ void __launch_bounds__(WARPS * 32, BOXES ? CR_S1_BOXES_MIN_BLOCKS : 3
 // resolve.cu:213-232 (0xFFFFFFF0'00000000 per pixel), 16-byte stores; block 0
 // also resets the frame's counters.
 __global__ void __launch_bounds__(256) k_clear(uint64_t* fb, uint64_t n, unsigned long long* counters) {
+    // launched the ordinary way (it overwrites what the previous frame's
+    // resolve reads); lets the frame cull be scheduled early
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     if (blockIdx.x == 0 && threadIdx.x < CR_CTR_COUNT) counters[threadIdx.x] = 0ull;
     const uint64_t clearv = 0xFFFFFFF000000000ull;
     const uint64_t n2 = n / 2;
@@ -581,6 +587,25 @@ int cr_query_launch_shape(int device, CrLaunchShape* out) {
     return 0;
 }
 
+namespace {
+// Launches kernel(p) on stream, allowed to be scheduled while the stream's
+// previous kernel finishes (it waits in pdl_enter).
+template <typename Kernel, typename... Args>
+int launch_pdl(Kernel kernel, unsigned grid, unsigned block, void* stream, const Args&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = (cudaStream_t)stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...) == cudaSuccess ? 0 : -1;
+}
+}  // namespace
+
 int cr_launch_clear(uint64_t* fb, uint64_t numPixels, unsigned long long* counters, void* stream) {
     const uint64_t want = (numPixels / 2 + 255) / 256;
     const unsigned grid = (unsigned)(want < 1 ? 1 : (want > 148 * 16 ? 148 * 16 : want));
@@ -592,8 +617,7 @@ int cr_launch_vertex(const CrFrameParams& p, const CrLaunchShape& s, void* strea
     if (p.numVChunks == 0) return 0;
     uint64_t blocks = p.numVChunks;
     if (blocks > (uint64_t)s.vertexBlocks) blocks = (uint64_t)s.vertexBlocks;
-    k_vertex<VX_THREADS><<<(unsigned)blocks, VX_THREADS, 0, (cudaStream_t)stream>>>(p);
-    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    return launch_pdl(k_vertex<VX_THREADS>, (unsigned)blocks, VX_THREADS, stream, p);
 }
 
 int cr_launch_cull(const CrFrameParams& p, const CrLaunchShape& s, void* stream) {
@@ -602,8 +626,7 @@ int cr_launch_cull(const CrFrameParams& p, const CrLaunchShape& s, void* stream)
     if (work == 0) return 0;
     uint64_t blocks = (work + 255) / 256;
     if (blocks > (uint64_t)s.numSMs * 8) blocks = (uint64_t)s.numSMs * 8;
-    k_cull<256><<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(p);
-    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    return launch_pdl(k_cull<256>, (unsigned)blocks, 256, stream, p);
 }
 
 int cr_launch_stage1(const CrFrameParams& p, const CrLaunchShape& s, void* stream) {
@@ -612,23 +635,17 @@ int cr_launch_stage1(const CrFrameParams& p, const CrLaunchShape& s, void* strea
     uint64_t blocks = (warps + S1_WARPS - 1) / S1_WARPS;
     if (blocks > (uint64_t)s.stage1Blocks) blocks = (uint64_t)s.stage1Blocks;
     const unsigned b = (unsigned)blocks;
-    cudaStream_t st = (cudaStream_t)stream;
-    if (p.cellMode == CR_REC_BOXES) {
-        if (p.anyPacked) k_stage1<S1_WARPS, true, true><<<b, S1_WARPS * 32, 0, st>>>(p);
-        else k_stage1<S1_WARPS, true, false><<<b, S1_WARPS * 32, 0, st>>>(p);
-    } else {
-        if (p.anyPacked) k_stage1<S1_WARPS, false, true><<<b, S1_WARPS * 32, 0, st>>>(p);
-        else k_stage1<S1_WARPS, false, false><<<b, S1_WARPS * 32, 0, st>>>(p);
-    }
-    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    if (p.cellMode == CR_REC_BOXES)
+        return p.anyPacked ? launch_pdl(k_stage1<S1_WARPS, true, true>, b, S1_WARPS * 32, stream, p)
+                           : launch_pdl(k_stage1<S1_WARPS, true, false>, b, S1_WARPS * 32, stream, p);
+    return p.anyPacked ? launch_pdl(k_stage1<S1_WARPS, false, true>, b, S1_WARPS * 32, stream, p)
+                       : launch_pdl(k_stage1<S1_WARPS, false, false>, b, S1_WARPS * 32, stream, p);
 }
 
 int cr_launch_stage2(const CrFrameParams& p, const CrLaunchShape& s, void* stream) {
-    k_stage2<S2_WARPS, false><<<(unsigned)s.stage2Blocks, S2_WARPS * 32, 0, (cudaStream_t)stream>>>(p);
-    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    return launch_pdl(k_stage2<S2_WARPS, false>, (unsigned)s.stage2Blocks, S2_WARPS * 32, stream, p);
 }
 
 int cr_launch_stage3(const CrFrameParams& p, const CrLaunchShape& s, void* stream) {
-    k_stage3<S3_WARPS, false><<<(unsigned)s.stage3Blocks, S3_WARPS * 32, 0, (cudaStream_t)stream>>>(p);
-    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    return launch_pdl(k_stage3<S3_WARPS, false>, (unsigned)s.stage3Blocks, S3_WARPS * 32, stream, p);
 }

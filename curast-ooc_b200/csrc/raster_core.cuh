@@ -21,6 +21,17 @@ namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
 
+// Programmatic dependent launch.  The plain frame's kernels after the clear
+// are launched with cudaLaunchAttributeProgrammaticStreamSerialization: each
+// may be scheduled while its predecessor finishes, waits here until the
+// predecessor has completed (and its writes are visible) before touching any
+// memory, and lets its own successor be scheduled.  Launched the ordinary
+// way, both instructions are no-ops.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 struct V2 {
     float x, y;
 };
@@ -938,6 +949,7 @@ __device__ __forceinline__ void s2_row_span(const S2Span& P, float py, float asy
 // frame's single target.
 template <int WARPS, bool MULTI>
 __global__ void __launch_bounds__(WARPS * 32) k_stage2(const CrFrameParams p) {
+    pdl_enter();
     const int lane = threadIdx.x & 31;
     const uint64_t gw = (uint64_t)blockIdx.x * WARPS + (threadIdx.x >> 5);
     const uint64_t nw = (uint64_t)gridDim.x * WARPS;
@@ -1207,6 +1219,7 @@ __device__ __forceinline__ void s3_row_span(const S3Prune& P, float fx0, float p
 
 template <int WARPS, bool MULTI>
 __global__ void __launch_bounds__(WARPS * 32, 3) k_stage3(const CrFrameParams p) {
+    pdl_enter();
     const int lane = threadIdx.x & 31;
     const uint64_t gw = (uint64_t)blockIdx.x * WARPS + (threadIdx.x >> 5);
     const uint64_t nw = (uint64_t)gridDim.x * WARPS;

@@ -155,6 +155,9 @@ __device__ __forceinline__ void resolve_pixel(const CrResolveParams& p, const in
 }
 
 __global__ void __launch_bounds__(256) k_resolve(const CrResolveParams p) {
+    // launched after the raster stages with programmatic stream
+    // serialization: wait for them before reading the visbuffer
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     const int x = blockIdx.x * 32 + threadIdx.x;
     const int y = blockIdx.y * 8 + threadIdx.y;
     if (x >= p.W || y >= p.H) return;
@@ -208,10 +211,16 @@ __global__ void __launch_bounds__(256) k_resolve_views(const CrResolveParams bas
 
 int cr_launch_resolve(const CrResolveParams& p, void* stream) {
     if (p.W <= 0 || p.H <= 0 || p.numInstances == 0) return 0;
-    dim3 block(32, 8);
-    dim3 grid((p.W + 31) / 32, (p.H + 7) / 8);
-    k_resolve<<<grid, block, 0, (cudaStream_t)stream>>>(p);
-    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((p.W + 31) / 32, (p.H + 7) / 8);
+    cfg.blockDim = dim3(32, 8);
+    cfg.stream = (cudaStream_t)stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_resolve, p) == cudaSuccess ? 0 : -1;
 }
 
 int cr_launch_resolve_views(const CrResolveParams& base, const CrView* views, uint32_t numViews, uint32_t numBlocks,
