@@ -137,6 +137,24 @@ void order_instances(uint32_t count, uint32_t flags, MeshOf meshOf, TrisOf trisO
 // on the host: the same rigorous bounds on the float transform of every
 // vertex in the box.  Returns CR_OC_BEHIND, a union of side bits, or
 // CR_MESH_INSIDE; 0 when nothing is proven (also for non-finite boxes).
+// Pixels of the screen covered by the projected box (the whole screen when
+// a corner is not in front of the camera); an estimate that only steers
+// speed choices.
+static double screen_box_area(const float* wv, float fa, float f, int W, int H, const float* box) {
+    double x0 = 1e300, x1 = -1e300, y0 = 1e300, y1 = -1e300;
+    for (int c = 0; c < 8; ++c) {
+        const double p[3] = {box[(c & 1) ? 3 : 0], box[(c & 2) ? 4 : 1], box[(c & 4) ? 5 : 2]};
+        double q[3];
+        for (int r = 0; r < 3; ++r) q[r] = wv[r] * p[0] + wv[4 + r] * p[1] + wv[8 + r] * p[2] + wv[12 + r];
+        const double d = -q[2];
+        if (!(d > 1e-6)) return (double)W * H;  // also NaN boxes
+        const double sx = (fa * q[0] / d * 0.5 + 0.5) * W, sy = (f * q[1] / d * 0.5 + 0.5) * H;
+        x0 = std::min(x0, sx), x1 = std::max(x1, sx), y0 = std::min(y0, sy), y1 = std::max(y1, sy);
+    }
+    const double w = std::min(x1, (double)W) - std::max(x0, 0.0), h = std::min(y1, (double)H) - std::max(y0, 0.0);
+    return (w > 0.0 && h > 0.0) ? w * h : 0.0;
+}
+
 static uint32_t classify_mesh_box(const float* wv, float fa, float f, const float* box) {
     const double EPS = 9.5367431640625e-07;  // 2^-20
     const double ABS = 1e-30;
@@ -1033,12 +1051,18 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
     Assembled A;
     cr_status s = assemble(ctx, instances, count, cam->view, flags, A, firstIds);
     if (s) return s;
+    float pxPerTriangle = 0.0f;  // screen area the instances' boxes cover per triangle (an estimate)
     {  // whole-mesh classes: fa as the kernels form it (f / aspect in float)
         const float f = cam->proj[5];
         const float fa = f / ((float)cam->width / (float)cam->height);
-        for (uint32_t r = 0; r < count; r++)
-            A.inst[r].meshClass =
-                classify_mesh_box(&A.worldView[16ull * r], fa, f, ctx->meshes[instances[A.order[r]].mesh].box);
+        double area = 0.0, tris = 0.0;
+        for (uint32_t r = 0; r < count; r++) {
+            const MeshRec& m = ctx->meshes[instances[A.order[r]].mesh];
+            A.inst[r].meshClass = classify_mesh_box(&A.worldView[16ull * r], fa, f, m.box);
+            area += screen_box_area(&A.worldView[16ull * r], fa, f, cam->width, cam->height, m.box);
+            tris += (double)m.numTriangles;
+        }
+        if (tris > 0.0) pxPerTriangle = (float)(area / tris);
     }
     // frame tables, queues and counters are shared by consecutive frames,
     // which may be issued on different streams
@@ -1071,6 +1095,9 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
     }
     fp.outcodes = ctx->outcodes;
     fp.cellMode = cellMode;
+    // frames whose triangles cover pixels (not mostly sub-pixel ones) keep
+    // many lanes rasterizing in stage 1: spread those rasters over the warp
+    fp.coopRaster = pxPerTriangle >= 0.5f ? 1u : 0u;
     fp.itemList = ctx->itemList;
     fp.itemCap = ctx->itemCap;
     fp.chunkList = ctx->chunkList;

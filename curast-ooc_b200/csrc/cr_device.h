@@ -187,6 +187,7 @@ struct CrFrameParams {
     uint64_t waitTimeoutNs;     // bound of every device-side wait
     uint32_t debugFlags;        // CR_DEBUG_* (failure-detection tests)
     uint32_t anyPacked;         // 1: some mesh of the frame is compressed
+    uint32_t coopRaster;        // 1: stage 1 spreads its tiny rasters over the warp
     uint8_t* outcodes;          // vertex-pass output, CrInstance::outBase + vertex
     uint64_t numVChunks;        // vertex-pass chunks of all instances
     // batched frames: world_view holds numViews * numInstances matrices,

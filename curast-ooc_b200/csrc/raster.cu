@@ -288,12 +288,17 @@ __device__ __forceinline__ TileSrc tile_source(const CrSegment* sg, uint32_t bat
 //   BOXES, no list         sub-box proofs of the sample-miss cull, one per
 //                          (instance, 16 triangles), spread over the lanes
 // Nontrivial triangles are appended with one atomic per warp (ballot / popc).
+// a drain batch whose largest tiny raster has more fragments than this is
+// rasterized across the warp (stage1_coop_raster)
+#ifndef CR_COOP_MIN_FRAGMENTS
+#define CR_COOP_MIN_FRAGMENTS 8
+#endif
 #ifndef CR_S1_BOXES_MIN_BLOCKS
 #define CR_S1_BOXES_MIN_BLOCKS 3
 #endif
 // PACKED: compiled for frames with compressed meshes (plain frames carry no
 // decoding code).
-template <int WARPS, bool BOXES, bool PACKED>
+template <int WARPS, bool BOXES, bool PACKED, bool COOP = false>
 __global__ void __launch_bounds__(WARPS * 32, BOXES ? CR_S1_BOXES_MIN_BLOCKS : 3) k_stage1(const CrFrameParams p) {
     pdl_enter();
     constexpr int STAGES = BOXES ? 2 : S1_STAGES;
@@ -430,6 +435,8 @@ __global__ void __launch_bounds__(WARPS * 32, BOXES ? CR_S1_BOXES_MIN_BLOCKS : 3
                 const uint32_t j = qh + lane;
                 int res = S1_CULL;
                 uint32_t tri = 0, inst = 0;
+                S1Raster ras;
+                uint64_t rid = 0;
                 if (j < qt) {
                     const uint32_t e = ring[j & (S1_RING - 1)];
                     const uint32_t tp = e & 0xffu;
@@ -438,12 +445,24 @@ __global__ void __launch_bounds__(WARPS * 32, BOXES ? CR_S1_BOXES_MIN_BLOCKS : 3
                     const V3 pa = pos_of(geo, index_of(tp, 0));
                     const V3 pb = pos_of(geo, index_of(tp, 1));
                     const V3 pc = pos_of(geo, index_of(tp, 2));
-                    if (!BOXES)
-                        res = stage1_triangle(target_of(p), fa, *Mu, flipu, pa, pb, pc, cumu + tri);
-                    else
+                    if (!BOXES) {
+                        rid = cumu + tri;
+                        res = stage1_triangle<COOP>(target_of(p), fa, *Mu, flipu, pa, pb, pc, rid, &ras);
+                    } else {
                         res = stage1_triangle(target_of(p), fa, load_mat(p.world_view + 4ull * inst),
                                               __ldg(&p.instances[inst].flip), pa, pb, pc,
                                               __ldg(&p.instances[inst].cum) + tri);
+                    }
+                }
+                if constexpr (!BOXES && COOP) {
+                    // the lanes' tiny rasters: spread over the warp when one of
+                    // them would hold the others up, else each lane its own
+                    const bool mine = res == S1_RASTER;
+                    const int frags = mine ? max(ras.size_x, 0) * max(ras.size_y, 0) : 0;
+                    if (__reduce_max_sync(FULL, (unsigned)frags) > CR_COOP_MIN_FRAGMENTS)
+                        stage1_coop_raster(target_of(p), mine, ras, rid);
+                    else if (mine)
+                        stage1_own_raster(target_of(p), ras, rid);
                 }
                 qh = min(qh + 32u, qt);
                 const unsigned qmask = __ballot_sync(FULL, res == S1_QUEUE);
@@ -638,6 +657,9 @@ int cr_launch_stage1(const CrFrameParams& p, const CrLaunchShape& s, void* strea
     if (p.cellMode == CR_REC_BOXES)
         return p.anyPacked ? launch_pdl(k_stage1<S1_WARPS, true, true>, b, S1_WARPS * 32, stream, p)
                            : launch_pdl(k_stage1<S1_WARPS, true, false>, b, S1_WARPS * 32, stream, p);
+    if (p.coopRaster)
+        return p.anyPacked ? launch_pdl(k_stage1<S1_WARPS, false, true, true>, b, S1_WARPS * 32, stream, p)
+                           : launch_pdl(k_stage1<S1_WARPS, false, false, true>, b, S1_WARPS * 32, stream, p);
     return p.anyPacked ? launch_pdl(k_stage1<S1_WARPS, false, true>, b, S1_WARPS * 32, stream, p)
                        : launch_pdl(k_stage1<S1_WARPS, false, false>, b, S1_WARPS * 32, stream, p);
 }

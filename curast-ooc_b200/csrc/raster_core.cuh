@@ -176,7 +176,15 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 // ---------------------------------------------------------------------------
 // Stage 1: one (triangle, instance) -- tv.cu:82-271
 // ---------------------------------------------------------------------------
-enum : int { S1_CULL = 0, S1_DONE = 1, S1_QUEUE = 2 };
+enum : int { S1_CULL = 0, S1_DONE = 1, S1_QUEUE = 2, S1_RASTER = 3 };
+
+// The tiny raster of one stage-1 triangle, as stage1_triangle sets it up
+// (tv.cu:200-270): row starts advance by (ds_dy, dt_dy) per row, fragments
+// by (ds_dx, dt_dx) per column.
+struct S1Raster {
+    float s_row, t_row, ds_dx, dt_dx, ds_dy, dt_dy, iza, izb, izc;
+    int row_pid, size_x, size_y;
+};
 
 // fl(X / d) > 1 for d > 0 without the division.  With round-to-nearest-even,
 // fl(q) > 1 iff q > 1 + 2^-24, i.e. X - d > d * 2^-24.  Outside (d/2, 2d) the
@@ -208,9 +216,12 @@ __device__ __forceinline__ Target target_of(const CrFrameParams& p, uint32_t vie
     return Target{ldg_ptr(&v->fb), __ldg(&v->W), __ldg(&v->H), __ldg(&v->f), __ldg(&v->fa), p.thrSmall};
 }
 
+// With COOP the tiny raster is not run here: its setup goes to *coop and
+// S1_RASTER is returned, for stage1_coop_raster to run across the warp.
+template <bool COOP = false>
 __device__ __forceinline__ int stage1_triangle(const Target& p, const float fa, const Mat& M,
                                                const uint32_t flip, const V3 pa, const V3 pb, const V3 pc,
-                                               const uint64_t id) {
+                                               const uint64_t id, S1Raster* coop = nullptr) {
     const float f = p.f;
     const V3 av = xform(M, pa);
     const V3 bv = xform(M, pb);
@@ -287,6 +298,10 @@ __device__ __forceinline__ int stage1_triangle(const Target& p, const float fa, 
     float s_row = (s0x * v_ac.y - s0y * v_ac.x) * factor;
     float t_row = (v_ab.x * s0y - v_ab.y * s0x) * factor;
     int row_pid = (int)start_x + p.W * (int)start_y;
+    if constexpr (COOP) {
+        *coop = S1Raster{s_row, t_row, ds_dx, dt_dx, ds_dy, dt_dy, iza, izb, izc, row_pid, size_x, size_y};
+        return S1_RASTER;
+    }
     const uint32_t numPixels = (uint32_t)p.W * (uint32_t)p.H;
     for (int fy = 0; fy < size_y; ++fy) {
         float s = s_row;
@@ -310,6 +325,97 @@ __device__ __forceinline__ int stage1_triangle(const Target& p, const float fa, 
     return S1_DONE;
 }
 
+
+// The tiny raster of one lane's S1_RASTER triangle by that lane alone: the
+// loop of stage1_triangle.
+__device__ __forceinline__ void stage1_own_raster(const Target& p, const S1Raster& r, const uint64_t id) {
+    const uint32_t numPixels = (uint32_t)p.W * (uint32_t)p.H;
+    float s_row = r.s_row, t_row = r.t_row;
+    int row_pid = r.row_pid;
+    for (int fy = 0; fy < r.size_y; ++fy) {
+        float s = s_row;
+        float t = t_row;
+        int pid = row_pid;
+        for (int fx = 0; fx < r.size_x; ++fx) {
+            const float v = 1.0f - (s + t);
+            if (s > 0.0f && t > 0.0f && v > 0.0f && (uint32_t)pid < numPixels) {
+                const float inv_depth = v * r.iza + s * r.izb + t * r.izc;
+                const float depth = 1.0f / inv_depth;
+                fb_min(p.fb, (uint32_t)pid, pack_pixel(depth, id));
+            }
+            s += r.ds_dx;
+            t += r.dt_dx;
+            pid++;
+        }
+        s_row += r.ds_dy;
+        t_row += r.dt_dy;
+        row_pid += p.W;
+    }
+}
+
+// The tiny rasters of the lanes that returned S1_RASTER, run by the whole
+// warp: each (triangle, row) is one task, 32 at a time.  A task replays the
+// row-start additions of the rows above it and then walks its row in
+// order, so every fragment sees the same float values as in the one-thread
+// loop of stage1_triangle (the sums are formed in the same sequence) and
+// the same fragments are written; the warp no longer waits on its largest
+// triangle.  Rows of a triangle without columns are skipped (they write
+// nothing).  All lanes of the warp must call it.
+__device__ __forceinline__ void stage1_coop_raster(const Target& p, const bool mine, const S1Raster& r,
+                                                   const uint64_t id) {
+    const int lane = threadIdx.x & 31;
+    const int rows = (mine && r.size_x > 0 && r.size_y > 0) ? r.size_y : 0;
+    int incl = rows;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int v = __shfl_up_sync(FULL, incl, d);
+        if (lane >= d) incl += v;
+    }
+    const int total = __shfl_sync(FULL, incl, 31);
+    const uint32_t numPixels = (uint32_t)p.W * (uint32_t)p.H;
+    for (int base = 0; base < total; base += 32) {
+        const int k = base + lane;
+        int j = 0;  // the lane whose rows hold task k: first with incl > k
+#pragma unroll
+        for (int step = 16; step >= 1; step >>= 1) {
+            const int c = __shfl_sync(FULL, incl, j + step - 1);
+            if (c <= k) j += step;
+        }
+        const int first = __shfl_sync(FULL, incl, j) - __shfl_sync(FULL, rows, j);
+        float s_row = __shfl_sync(FULL, r.s_row, j);
+        float t_row = __shfl_sync(FULL, r.t_row, j);
+        const float ds_dx = __shfl_sync(FULL, r.ds_dx, j);
+        const float dt_dx = __shfl_sync(FULL, r.dt_dx, j);
+        const float ds_dy = __shfl_sync(FULL, r.ds_dy, j);
+        const float dt_dy = __shfl_sync(FULL, r.dt_dy, j);
+        const float iza = __shfl_sync(FULL, r.iza, j);
+        const float izb = __shfl_sync(FULL, r.izb, j);
+        const float izc = __shfl_sync(FULL, r.izc, j);
+        const int row_pid = __shfl_sync(FULL, r.row_pid, j);
+        const int size_x = __shfl_sync(FULL, r.size_x, j);
+        const uint64_t tid = __shfl_sync(FULL, (unsigned long long)id, j);
+        if (k >= total) continue;
+        const int fy = k - first;
+        for (int i = 0; i < fy; ++i) {
+            s_row += ds_dy;
+            t_row += dt_dy;
+        }
+        float s = s_row;
+        float t = t_row;
+        int pid = row_pid + fy * p.W;
+        for (int fx = 0; fx < size_x; ++fx) {
+            const float v = 1.0f - (s + t);
+            if (s > 0.0f && t > 0.0f && v > 0.0f && (uint32_t)pid < numPixels) {
+                const float inv_depth = v * iza + s * izb + t * izc;
+                const float depth = 1.0f / inv_depth;
+                fb_min(p.fb, (uint32_t)pid, pack_pixel(depth, tid));
+            }
+            s += ds_dx;
+            t += dt_dx;
+            pid++;
+        }
+    }
+}
 
 // ---------------------------------------------------------------------------
 // Vertex pass: one thread per (instance, vertex).  It evaluates the per-vertex
