@@ -1242,7 +1242,7 @@ cr_status cr_postprocess(cr_context* ctx, const cr_post_desc* d, void* stream_) 
         CR_CUDA(cudaEventRecord(ctx->postDone, stream), "post event");
     }
     if (p.ssao) {
-        const size_t need = align_up((size_t)p.W * p.H * 8, 256) + (size_t)p.W * p.H * 4;
+        const size_t need = align_up((size_t)p.W * p.H * 4, 256) + (size_t)p.W * p.H * 4;
         if (need > ctx->postCap) {
             CR_CUDA(cudaDeviceSynchronize(), "post scratch resize");
             ctx->dev_free(ctx->postScratch, ctx->postCap);
@@ -1252,8 +1252,8 @@ cr_status cr_postprocess(cr_context* ctx, const cr_post_desc* d, void* stream_) 
             if (s) return s;
             ctx->postCap = need;
         }
-        p.occlusion = (uint64_t*)ctx->postScratch;
-        p.shade = (float*)((char*)ctx->postScratch + align_up((size_t)p.W * p.H * 8, 256));
+        p.ao = (float*)ctx->postScratch;
+        p.shade = (float*)((char*)ctx->postScratch + align_up((size_t)p.W * p.H * 4, 256));
     }
     // the scratch is shared: the previous post (any stream) must be done
     CR_CUDA(cudaStreamWaitEvent(stream, ctx->postDone, 0), "post wait");

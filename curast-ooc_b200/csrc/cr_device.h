@@ -253,7 +253,7 @@ struct CrPostParams {
     int32_t windowW;              // screenshot: EDL distance = W / windowW
     int32_t outW, outH;           // output size (display: W / outW = supersampling factor)
     uint32_t background;
-    uint64_t* occlusion;          // W*H scratch (SSAO)
+    float* ao;                    // W*H scratch: occlusion before the blur
     float* shade;                 // W*H scratch (SSAO)
     uint32_t* out;                // outW*outH RGBA8
 };

@@ -53,10 +53,16 @@ template <bool FAST>
 __device__ __forceinline__ float mcos(float x) { return FAST ? __cosf(x) : cosf(x); }
 template <bool FAST>
 __device__ __forceinline__ float msin(float x) { return FAST ? __sinf(x) : sinf(x); }
+// The fast pair is the two hardware approximations __sincosf is made of,
+// taken as values: through __sincosf's pointers the pair went to the stack.
 template <bool FAST>
 __device__ __forceinline__ void msincos(float x, float* s, float* c) {
-    if (FAST) __sincosf(x, s, c);
-    else sincosf(x, s, c);
+    if (FAST) {
+        *s = __sinf(x);
+        *c = __cosf(x);
+    } else {
+        sincosf(x, s, c);
+    }
 }
 template <bool FAST>
 __device__ __forceinline__ float mlog2(float x) { return FAST ? __log2f(x) : log2f(x); }
@@ -89,8 +95,9 @@ __device__ __forceinline__ int iclamp(int v, int lo, int hi) {
     return v;
 }
 
+// The depth half of a colorbuffer word: a 32-bit load of its high word.
 __device__ __forceinline__ float depth_at(const CrPostParams& p, int pid) {
-    return __uint_as_float((uint32_t)(__ldg(reinterpret_cast<const unsigned long long*>(p.colorbuffer) + pid) >> 32));
+    return __uint_as_float(__ldg(reinterpret_cast<const unsigned int*>(p.colorbuffer) + 2 * (size_t)pid + 1));
 }
 
 // The angle-only terms of both effects, the same for every pixel: computed
@@ -132,6 +139,30 @@ __device__ float edl_factor(const CrPostParams& p, const PostTables& t, float de
         float nd = INFINITY;
         if (nx >= 0 && nx < p.W && ny >= 0 && ny < p.H) nd = depth_at(p, nx + p.W * ny);
         sum += fmaxf(ld - mlog2<FAST>(nd), 0.0f);
+    }
+    const float response = mdiv<FAST>(sum, float(numSamples));
+    const float edlStrength = 0.9f;
+    float shade = mexp<FAST>(-response * 300.0f * edlStrength);
+    shade = fclamp(shade, 0.3f, 1.0f);
+    return shade * 0.8f + 0.2f;
+}
+
+// getEdlShadingFactor on a shared-memory tile of log2(depth) -- the same
+// function of the same depths, each logarithm taken once per tile pixel
+// instead of once per tap.  (x, y) are image coordinates, so the tap
+// positions truncate exactly as above; (tx0, ty0) is the tile's image origin
+// and taps outside the image read the tile's log2(INFINITY).
+template <bool FAST>
+__device__ float edl_factor_tile(const PostTables& t, const float* lt, int tw, int tx0, int ty0, int x, int y,
+                                 int distance) {
+    float sum = 0.0f;
+    const int numSamples = 8;
+    const float ld = lt[(y - ty0) * tw + (x - tx0)];
+    for (int i = 0; i < numSamples; i++) {
+        const float dx = float(distance) * t.edlCos[i];
+        const float dy = float(distance) * t.edlSin[i];
+        const int nx = (int)((float)x + dx), ny = (int)((float)y + dy);
+        sum += fmaxf(ld - lt[(ny - ty0) * tw + (nx - tx0)], 0.0f);
     }
     const float response = mdiv<FAST>(sum, float(numSamples));
     const float edlStrength = 0.9f;
@@ -236,7 +267,7 @@ __device__ float ssao_factor(const CrPostParams& p, const PostTables& t, float c
 
 // kernel_ssaoOcclusion (resolve.cu:549-568)
 template <bool FAST>
-__global__ void __launch_bounds__(256) k_ssao_occlusion(const CrPostParams p) {
+__global__ void __launch_bounds__(256, 4) k_ssao_occlusion(const CrPostParams p) {
     __shared__ PostTables t;
     post_tables<FAST>(t, threadIdx.y * PB_X + threadIdx.x);
     __syncthreads();
@@ -244,38 +275,72 @@ __global__ void __launch_bounds__(256) k_ssao_occlusion(const CrPostParams p) {
     if (x >= p.W || y >= p.H) return;
     const int pid = x + p.W * y;
     const float depth = depth_at(p, pid);
-    const float ssao = ssao_factor<FAST>(p, t, depth, x, y);
-    p.occlusion[pid] = ((uint64_t)__float_as_uint(depth) << 32) | (uint64_t)__float_as_uint(ssao);
+    // The reference packs depth << 32 | occlusion into its blur input, where
+    // only the occlusion and isinf(depth) are read.  Occlusion is +0..1 (or
+    // NaN), so a pixel without geometry is written as -1: its taps read
+    // |-1| = 1, the value the reference computes there, and the sign marks
+    // it as a background centre.
+    p.ao[pid] = isinf(depth) ? -1.0f : ssao_factor<FAST>(p, t, depth, x, y);
 }
 
 // kernel_ssaoBlur (resolve.cu:570-640): 7x7 Gaussian (the reference computes
-// a bilateral weight and then sets it to 1)
+// a bilateral weight and then sets it to 1).  A block blurs 32 x 32 pixels
+// from its occlusion tile with a 3-pixel apron, staged in shared memory
+// edge-clamped as the reference clamps each tap; each thread blurs a 2 x 2
+// quad from the 8 x 8 window of taps it shares, held in registers, and sums
+// each pixel's 49 taps in the reference's order.
+constexpr int BLUR_PX = 2;
+
 template <bool FAST>
 __global__ void __launch_bounds__(256) k_ssao_blur(const CrPostParams p) {
-    const int x = blockIdx.x * PB_X + threadIdx.x, y = blockIdx.y * PB_Y + threadIdx.y;
-    if (x >= p.W || y >= p.H) return;
-    const int centerIdx = y * p.W + x;
-    const float center_depth = __uint_as_float((uint32_t)(p.occlusion[centerIdx] >> 32));
-    if (isinf(center_depth)) {
-        p.shade[centerIdx] = 1.0f;
-        return;
-    }
-    const int RADIUS = 3;
-    const float gaussian[7] = {0.015625f, 0.09375f, 0.234375f, 0.3125f, 0.234375f, 0.09375f, 0.015625f};
-    float sum = 0.0f, totalWeight = 0.0f;
-    for (int dy = -RADIUS; dy <= RADIUS; dy++)
-        for (int dx = -RADIUS; dx <= RADIUS; dx++) {
-            const int nx = iclamp(x + dx, 0, p.W - 1);
-            const int ny = iclamp(y + dy, 0, p.H - 1);
-            const uint64_t occ = p.occlusion[ny * p.W + nx];
-            const float sample_occlusion = __uint_as_float((uint32_t)(occ & 0xffffffffu));
-            const float w = gaussian[dx + RADIUS] * gaussian[dy + RADIUS] * 1.0f;
-            sum += w * sample_occlusion;
-            totalWeight += w;
+    constexpr int RADIUS = 3, BX = PB_X * BLUR_PX, BY = PB_Y * BLUR_PX, WIN = 2 * RADIUS + BLUR_PX;
+    constexpr int TX = BX + 2 * RADIUS, TY = BY + 2 * RADIUS, N = TX * TY, NT = PB_X * PB_Y;
+    static_assert(TX % 2 == 0 && WIN % 2 == 0, "float2 rows");
+    __shared__ __align__(16) float tile[TY][TX];
+    const int tid = threadIdx.y * PB_X + threadIdx.x;
+    const int x0 = blockIdx.x * BX - RADIUS, y0 = blockIdx.y * BY - RADIUS;
+#pragma unroll
+    for (int k = 0; k < (N + NT - 1) / NT; k++) {
+        const int i = tid + NT * k;
+        if (i < N) {
+            const int ty = i / TX, tx = i - ty * TX;
+            tile[ty][tx] = p.ao[iclamp(y0 + ty, 0, p.H - 1) * p.W + iclamp(x0 + tx, 0, p.W - 1)];
         }
-    float shade = 1.0f;
-    if (totalWeight > 0.0f) shade = mdiv<FAST>(sum, totalWeight);
-    p.shade[centerIdx] = shade;
+    }
+    __syncthreads();
+    const int lx = BLUR_PX * threadIdx.x, ly = BLUR_PX * threadIdx.y;
+    float v[WIN][WIN];
+#pragma unroll
+    for (int r = 0; r < WIN; r++)
+#pragma unroll
+        for (int c = 0; c < WIN; c += 2) {
+            const float2 q = *reinterpret_cast<const float2*>(&tile[ly + r][lx + c]);
+            v[r][c] = q.x;
+            v[r][c + 1] = q.y;
+        }
+    const float gaussian[7] = {0.015625f, 0.09375f, 0.234375f, 0.3125f, 0.234375f, 0.09375f, 0.015625f};
+#pragma unroll
+    for (int j = 0; j < BLUR_PX; j++)
+#pragma unroll
+        for (int i = 0; i < BLUR_PX; i++) {
+            const int x = blockIdx.x * BX + lx + i, y = blockIdx.y * BY + ly + j;
+            if (x >= p.W || y >= p.H) continue;
+            float shade = 1.0f;
+            if (!(v[j + RADIUS][i + RADIUS] < 0.0f)) {  // centre depth finite (or NaN)
+                float sum = 0.0f, totalWeight = 0.0f;
+#pragma unroll
+                for (int dy = -RADIUS; dy <= RADIUS; dy++)
+#pragma unroll
+                    for (int dx = -RADIUS; dx <= RADIUS; dx++) {
+                        const float sample_occlusion = fabsf(v[j + RADIUS + dy][i + RADIUS + dx]);
+                        const float w = gaussian[dx + RADIUS] * gaussian[dy + RADIUS] * 1.0f;
+                        sum += w * sample_occlusion;
+                        totalWeight += w;
+                    }
+                if (totalWeight > 0.0f) shade = mdiv<FAST>(sum, totalWeight);
+            }
+            p.shade[y * p.W + x] = shade;
+        }
 }
 
 // One output pixel of the screenshot / same-size display resolve
@@ -353,15 +418,105 @@ __global__ void __launch_bounds__(256) k_post_resolve(const CrPostParams p) {
     p.out[x + p.outW * y] = r8 | (g8 << 8) | (b8 << 16) | 0xff000000u;
 }
 
+// The supersampled display resolve (resolve.cu:1193-1257) for factors F of 2
+// to 4: the EDL taps read a shared-memory tile of log2(depth) over the
+// block's source pixels with an apron of F + 1 (a tap lies within
+// F * |cos| < F + 1 of its pixel and truncates toward zero), and every
+// thread issues its F x F colour and shade loads together.
+template <bool FAST, int F>
+__global__ void __launch_bounds__(256) k_post_display_ss(const CrPostParams p) {
+    constexpr int TW = PB_X * F + 2 * (F + 1), TH = PB_Y * F + 2 * (F + 1), N = TW * TH, NT = PB_X * PB_Y;
+    __shared__ PostTables t;
+    __shared__ float lt[N];
+    const int tid = threadIdx.y * PB_X + threadIdx.x;
+    post_tables<FAST>(t, tid);
+    const int tx0 = blockIdx.x * PB_X * F - (F + 1), ty0 = blockIdx.y * PB_Y * F - (F + 1);
+    if (p.edl) {
+#pragma unroll
+        for (int k = 0; k < (N + NT - 1) / NT; k++) {
+            const int i = tid + NT * k;
+            if (i < N) {
+                const int iy = i / TW, gx = tx0 + (i - iy * TW), gy = ty0 + iy;
+                float nd = INFINITY;
+                if (gx >= 0 && gx < p.W && gy >= 0 && gy < p.H) nd = depth_at(p, gx + p.W * gy);
+                lt[i] = mlog2<FAST>(nd);
+            }
+        }
+    }
+    __syncthreads();
+    const int x = blockIdx.x * PB_X + threadIdx.x, y = blockIdx.y * PB_Y + threadIdx.y;
+    if (x >= p.outW || y >= p.outH) return;
+    uint64_t px[F][F];
+    float sh[F][F];
+#pragma unroll
+    for (int dx = 0; dx < F; dx++)
+#pragma unroll
+        for (int dy = 0; dy < F; dy++) {
+            const int spid = (F * x + dx) + p.W * (F * y + dy);
+            px[dx][dy] = __ldg(reinterpret_cast<const unsigned long long*>(p.colorbuffer) + spid);
+            sh[dx][dy] = p.ssao ? p.shade[spid] : 0.0f;
+        }
+    float cr = 0.0f, cg = 0.0f, cbl = 0.0f;
+    float edl = 0.0f, ssao = 0.0f;
+    int numSamples = 0;
+#pragma unroll
+    for (int dx = 0; dx < F; dx++)
+#pragma unroll
+        for (int dy = 0; dy < F; dy++) {
+            const uint64_t pixel = px[dx][dy];
+            const float depth = __uint_as_float((uint32_t)(pixel >> 32));
+            const uint32_t C = (uint32_t)(pixel & 0xffffffffu);
+            cr += (C >> 0) & 0xff;
+            cg += (C >> 8) & 0xff;
+            cbl += (C >> 16) & 0xff;
+            if (isinf(depth)) {  // BACKGROUND_COLOR, HostDeviceInterface.h:37
+                cr += (CR_BACKGROUND_COLOR >> 0) & 0xff;
+                cg += (CR_BACKGROUND_COLOR >> 8) & 0xff;
+                cbl += (CR_BACKGROUND_COLOR >> 16) & 0xff;
+            }
+            if (p.edl) edl += edl_factor_tile<FAST>(t, lt, TW, tx0, ty0, F * x + dx, F * y + dy, F);
+            if (p.ssao) ssao += sh[dx][dy];
+            numSamples++;
+        }
+    edl = p.edl ? mdiv<FAST>(edl, float(numSamples)) : 1.0f;
+    ssao = p.ssao ? mdiv<FAST>(ssao, float(numSamples)) : 1.0f;
+    const float shade = edl * ssao;
+    const float n = float(numSamples);
+    cr = mdiv<FAST>(shade * cr, n);
+    cg = mdiv<FAST>(shade * cg, n);
+    cbl = mdiv<FAST>(shade * cbl, n);
+    const uint32_t r8 = (unsigned char)__float2uint_rz(fclamp(cr, 0.0f, 255.0f));
+    const uint32_t g8 = (unsigned char)__float2uint_rz(fclamp(cg, 0.0f, 255.0f));
+    const uint32_t b8 = (unsigned char)__float2uint_rz(fclamp(cbl, 0.0f, 255.0f));
+    p.out[x + p.outW * y] = r8 | (g8 << 8) | (b8 << 16) | 0xff000000u;
+}
+
 template <bool FAST>
 void launch_post(const CrPostParams& p, cudaStream_t st) {
     if (p.ssao) {
+        // the occlusion taps scatter over hundreds of pixels: as much L1 as
+        // the SM offers
+        static bool carveout = false;
+        if (!carveout) {
+            cudaFuncSetAttribute(k_ssao_occlusion<FAST>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxL1);
+            carveout = true;
+        }
         const dim3 g((p.W + PB_X - 1) / PB_X, (p.H + PB_Y - 1) / PB_Y);
         k_ssao_occlusion<FAST><<<g, dim3(PB_X, PB_Y), 0, st>>>(p);
-        k_ssao_blur<FAST><<<g, dim3(PB_X, PB_Y), 0, st>>>(p);
+        const dim3 gb((p.W + PB_X * BLUR_PX - 1) / (PB_X * BLUR_PX), (p.H + PB_Y * BLUR_PX - 1) / (PB_Y * BLUR_PX));
+        k_ssao_blur<FAST><<<gb, dim3(PB_X, PB_Y), 0, st>>>(p);
     }
     const dim3 g((p.outW + PB_X - 1) / PB_X, (p.outH + PB_Y - 1) / PB_Y);
-    k_post_resolve<FAST><<<g, dim3(PB_X, PB_Y), 0, st>>>(p);
+    const int f = p.W / p.outW;
+    if (p.mode == CR_POST_MODE_SCREENSHOT || f < 2 || f > 4)
+        k_post_resolve<FAST><<<g, dim3(PB_X, PB_Y), 0, st>>>(p);
+    else if (f == 2)
+        k_post_display_ss<FAST, 2><<<g, dim3(PB_X, PB_Y), 0, st>>>(p);
+    else if (f == 3)
+        k_post_display_ss<FAST, 3><<<g, dim3(PB_X, PB_Y), 0, st>>>(p);
+    else
+        k_post_display_ss<FAST, 4><<<g, dim3(PB_X, PB_Y), 0, st>>>(p);
 }
 
 }  // namespace
