@@ -708,6 +708,19 @@ def run_glb(args, rank, world, local, wl):
             ctx.mesh_destroy(hm)
     barrier(world)
     ms = max_over_ranks(float(np.mean(times)) * 1e3, world)
+    # one more step, split into its phases (host clock, device synchronized)
+    t0 = time.perf_counter()
+    g = pc.Glb(data=data)
+    t1 = time.perf_counter()
+    hs = g.create_meshes(ctx)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    g.instances(hs)
+    g.close()
+    t3 = time.perf_counter()
+    for hm in hs:
+        ctx.mesh_destroy(hm)
+    phases = {"open": (t1 - t0) * 1e3, "create_meshes": (t2 - t1) * 1e3, "instances_close": (t3 - t2) * 1e3}
     if rank != 0:
         ctx.close()
         return None
@@ -728,7 +741,8 @@ def run_glb(args, rank, world, local, wl):
         "dtype": "u32",
         "data": "synthetic (seeded)",
         "config": {"workload": wl["name"], "desc": wl["desc"], "triangles": T, "file_bytes": len(data),
-                   "parallelism": f"replicas x{world}", "l2": "not applicable (host path; file > L2)"},
+                   "parallelism": f"replicas x{world}", "l2": "not applicable (host path; file > L2)",
+                   "phases_ms": phases},
         "e2e": {"value": value, "unit": "Mtris/s", "ms_per_step": ms, "h2d_bytes_per_step": len(data),
                 "d2h_bytes_per_step": 0},
         "roofline": {"kernel": "host parse + upload (cr_glb_open, cr_glb_create_meshes)", "bound": "pcie",

@@ -45,6 +45,7 @@
 #include <memory>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "context.h"
@@ -280,11 +281,35 @@ cr_status glb_fail(const char* msg) { return fail(CR_ERR_INVALID, "glb: %s", msg
 
 }  // namespace
 
+// A vector whose resize leaves new elements uninitialised: every mesh array
+// is written in full by the conversion, so zero-filling it first would be a
+// second pass over hundreds of megabytes.
+template <class T>
+struct DefaultInit : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = DefaultInit<U>;
+    };
+    DefaultInit() = default;
+    template <class U>
+    DefaultInit(const DefaultInit<U>&) noexcept {}
+    template <class U>
+    void construct(U* p) noexcept(std::is_nothrow_default_constructible<U>::value) {
+        ::new ((void*)p) U;
+    }
+    template <class U, class... A>
+    void construct(U* p, A&&... a) {
+        ::new ((void*)p) U(std::forward<A>(a)...);
+    }
+};
+template <class T>
+using raw_vector = std::vector<T, DefaultInit<T>>;
+
 struct cr_glb {
     struct Mesh {
-        std::vector<float> positions;
-        std::vector<uint32_t> indices;  // empty: non-indexed
-        std::vector<uint32_t> colors;   // empty: none
+        raw_vector<float> positions;
+        raw_vector<uint32_t> indices;  // empty: non-indexed
+        raw_vector<uint32_t> colors;   // empty: none
         uint32_t numVertices = 0, numTriangles = 0;
         float box[6] = {0, 0, 0, 0, 0, 0};
     };
@@ -463,9 +488,20 @@ cr_status parse(cr_glb& g, const uint8_t* d, uint64_t size) {
             uint32_t* out = m.indices.data();
             const uint8_t* q = t.idx.base;
             uint32_t hi = 0;
-            if (t.idx.ct == CT_U32) {
-                memcpy(out, q, 4 * n);
-                for (uint64_t i = 0; i < n; i++) hi = std::max(hi, out[i]);
+            if (t.idx.ct == CT_U32) {  // copied and range-checked in one pass
+                const uint64_t n8 = n & ~7ull;
+                uint32_t h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                for (uint64_t i = 0; i < n8; i += 8)
+                    for (int l = 0; l < 8; l++) {
+                        const uint32_t v = rd<uint32_t>(q + 4 * (i + l));
+                        out[i + l] = v;
+                        h[l] = std::max(h[l], v);
+                    }
+                for (uint64_t i = n8; i < n; i++) {
+                    out[i] = rd<uint32_t>(q + 4 * i);
+                    hi = std::max(hi, out[i]);
+                }
+                for (int l = 0; l < 8; l++) hi = std::max(hi, h[l]);
             } else if (t.idx.ct == CT_U16) {
                 for (uint64_t i = 0; i < n; i++) {
                     out[i] = rd<uint16_t>(q + 2 * i);
