@@ -300,7 +300,8 @@ cr_status ensure_queues(cr_context* ctx, uint64_t ntWant, uint64_t hugeWant) {
     return CR_OK;
 }
 
-cr_status build_mesh_boxes(cr_context* ctx, MeshRec& m) {
+// Allocates (once) and launches the mesh's box pass on the legacy stream.
+cr_status launch_mesh_boxes(cr_context* ctx, MeshRec& m) {
     const size_t ib = align_up((size_t)((m.numTriangles + CR_BATCH - 1) / CR_BATCH) * 24, 256);
     const size_t cb = align_up((size_t)((m.numVertices + CR_VCHUNK - 1) / CR_VCHUNK) * 24, 256);
     const size_t sb = align_up((size_t)((m.numTriangles + CR_SUB - 1) / CR_SUB) * 24, 256);
@@ -311,15 +312,24 @@ cr_status build_mesh_boxes(cr_context* ctx, MeshRec& m) {
         m.subBoxes = (float*)((char*)m.itemBoxes + ib + cb);
         m.boxBytes = ib + cb + sb + 256;
     }
-    float* meshBox = (float*)((char*)m.itemBoxes + ib + cb + sb);
-    m.dCodec = (CrCodec*)((char*)meshBox + 64);
+    m.meshBox = (float*)((char*)m.itemBoxes + ib + cb + sb);
+    m.dCodec = (CrCodec*)((char*)m.meshBox + 64);
     CR_CUDA(cudaMemcpy(m.dCodec, &m.codec, sizeof(CrCodec), cudaMemcpyHostToDevice), "mesh codec");
     if (cr_launch_mesh_boxes(m.indices, m.positions, m.compressed ? m.dCodec : nullptr, m.numTriangles,
-                             m.numVertices, m.itemBoxes, m.chunkBoxes, m.subBoxes, meshBox, 0))
+                             m.numVertices, m.itemBoxes, m.chunkBoxes, m.subBoxes, m.meshBox, 0))
         return fail(CR_ERR_CUDA, "mesh box launch: %s", cudaGetErrorString(cudaGetLastError()));
-    CR_CUDA(cudaDeviceSynchronize(), "mesh boxes");
-    CR_CUDA(cudaMemcpy(m.box, meshBox, sizeof(m.box), cudaMemcpyDeviceToHost), "mesh box readback");
     return CR_OK;
+}
+
+cr_status read_mesh_box(MeshRec& m) {
+    CR_CUDA(cudaMemcpy(m.box, m.meshBox, sizeof(m.box), cudaMemcpyDeviceToHost), "mesh box readback");
+    return CR_OK;
+}
+
+cr_status build_mesh_boxes(cr_context* ctx, MeshRec& m) {
+    if (cr_status s = launch_mesh_boxes(ctx, m)) return s;
+    CR_CUDA(cudaDeviceSynchronize(), "mesh boxes");
+    return read_mesh_box(m);
 }
 
 // Per-item vertex lists of an indexed mesh, built once on first use (a
@@ -610,8 +620,10 @@ cr_status cr_destroy(cr_context* ctx) {
     for (MeshRec& m : ctx->meshes) {
         if (m.live && m.owned) {
             cudaFree(m.positions);
-            cudaFree(m.indices);
-            cudaFree(m.colors);
+            if (!m.oneBlock) {
+                cudaFree(m.indices);
+                cudaFree(m.colors);
+            }
         }
         if (m.itemBoxes) cudaFree(m.itemBoxes);
         if (m.localLists) cudaFree(m.localLists);
@@ -656,45 +668,69 @@ cr_status alloc_owned_mesh(cr_context* ctx, uint32_t nV, uint32_t nT, bool index
     // index tiles are fetched in 384-byte bursts; pad to whole tiles
     const size_t ib = indexed ? align_up((size_t)nT * 12, 384) + 256 : 0;
     const size_t cb = colored ? align_up((size_t)nV * 4, 256) : 0;
-    cr_status s = ctx->dev_alloc((void**)&m.positions, pb, "mesh positions");
+    // one allocation for the three arrays: device allocations cost about
+    // as much as uploading megabytes
+    char* base = nullptr;
+    cr_status s = ctx->dev_alloc((void**)&base, pb + ib + cb, "mesh arrays");
     if (s) return s;
-    if (ib && (s = ctx->dev_alloc((void**)&m.indices, ib, "mesh indices")) != CR_OK) {
-        ctx->dev_free(m.positions, pb);
-        return s;
-    }
-    if (cb && (s = ctx->dev_alloc((void**)&m.colors, cb, "mesh colours")) != CR_OK) {
-        ctx->dev_free(m.positions, pb);
-        ctx->dev_free(m.indices, ib);
-        return s;
-    }
+    m.oneBlock = true;
+    m.positions = (float*)base;
+    m.indices = ib ? (uint32_t*)(base + pb) : nullptr;
+    m.colors = cb ? (uint32_t*)(base + pb + ib) : nullptr;
     m.bytes = pb + ib + cb;
     if (ib) {
         const size_t used = (size_t)nT * 12;
         const cudaError_t e = cudaMemset((char*)m.indices + used, 0, ib - used);
         if (e != cudaSuccess) {
-            ctx->dev_free(m.positions, pb);
-            ctx->dev_free(m.indices, ib);
-            ctx->dev_free(m.colors, cb);
+            ctx->dev_free(base, m.bytes);
             return cuda_fail(e, "mesh index padding");
         }
     }
     return CR_OK;
 }
 
+void free_mesh_arrays(cr_context* ctx, MeshRec& m) {
+    ctx->dev_free(m.positions, 0);
+    if (!m.oneBlock) {
+        ctx->dev_free(m.indices, 0);
+        ctx->dev_free(m.colors, 0);
+    }
+    ctx->bytesInUse -= std::min(ctx->bytesInUse, m.bytes);
+}
+
 cr_status register_mesh(cr_context* ctx, MeshRec& m, uint32_t* handle) {
     cr_status bs = build_mesh_boxes(ctx, m);
     if (bs) {
-        if (m.owned) {
-            ctx->dev_free(m.positions, 0);
-            ctx->dev_free(m.indices, 0);
-            ctx->dev_free(m.colors, 0);
-            ctx->bytesInUse -= std::min(ctx->bytesInUse, m.bytes);
-        }
+        if (m.owned) free_mesh_arrays(ctx, m);
         ctx->dev_free(m.itemBoxes, m.boxBytes);
         return bs;
     }
     ctx->meshes.push_back(m);
     *handle = (uint32_t)(ctx->meshes.size() - 1);
+    return CR_OK;
+}
+
+cr_status register_meshes(cr_context* ctx, std::vector<MeshRec>& recs, std::vector<uint32_t>& handles) {
+    cr_status s = CR_OK;
+    for (size_t k = 0; k < recs.size() && s == CR_OK; k++) s = launch_mesh_boxes(ctx, recs[k]);
+    if (s == CR_OK) {
+        const cudaError_t e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) s = cuda_fail(e, "mesh boxes");
+    }
+    for (size_t k = 0; k < recs.size() && s == CR_OK; k++) s = read_mesh_box(recs[k]);
+    if (s != CR_OK) {
+        for (MeshRec& m : recs) {
+            if (m.owned) free_mesh_arrays(ctx, m);
+            ctx->dev_free(m.itemBoxes, m.boxBytes);
+            m = MeshRec{};
+        }
+        return s;
+    }
+    handles.clear();
+    for (MeshRec& m : recs) {
+        ctx->meshes.push_back(m);
+        handles.push_back((uint32_t)(ctx->meshes.size() - 1));
+    }
     return CR_OK;
 }
 
@@ -783,10 +819,7 @@ cr_status cr_mesh_create(cr_context* ctx, const cr_mesh_desc* d, uint32_t* mesh_
         if (e == cudaSuccess && d->colors)
             e = cudaMemcpy(m.colors, d->colors, (size_t)d->num_vertices * 4, cudaMemcpyHostToDevice);
         if (e != cudaSuccess) {
-            ctx->dev_free(m.positions, 0);
-            ctx->dev_free(m.indices, 0);
-            ctx->dev_free(m.colors, 0);
-            ctx->bytesInUse -= std::min(ctx->bytesInUse, m.bytes);
+            free_mesh_arrays(ctx, m);
             return cuda_fail(e, "mesh upload");
         }
     } else {
@@ -918,12 +951,7 @@ cr_status cr_mesh_create_compressed(cr_context* ctx, const cr_compressed_mesh_de
     }
     cr_status bs = build_mesh_boxes(ctx, m);
     if (bs) {
-        if (m.owned) {
-            ctx->dev_free(m.positions, 0);
-            ctx->dev_free(m.indices, 0);
-            ctx->dev_free(m.colors, 0);
-            ctx->bytesInUse -= std::min(ctx->bytesInUse, m.bytes);
-        }
+        if (m.owned) free_mesh_arrays(ctx, m);
         return bs;
     }
     ctx->meshes.push_back(m);
@@ -936,12 +964,7 @@ cr_status cr_mesh_destroy(cr_context* ctx, uint32_t mesh) {
     MeshRec& m = ctx->meshes[mesh];
     cudaSetDevice(ctx->device);
     cudaDeviceSynchronize();
-    if (m.owned) {
-        cudaFree(m.positions);
-        cudaFree(m.indices);
-        cudaFree(m.colors);
-        ctx->bytesInUse -= std::min(ctx->bytesInUse, m.bytes);
-    }
+    if (m.owned) free_mesh_arrays(ctx, m);
     ctx->dev_free(m.itemBoxes, m.boxBytes);
     ctx->dev_free(m.localLists, m.localBytes);
     m = MeshRec{};

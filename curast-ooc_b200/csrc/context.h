@@ -33,6 +33,7 @@ cr_status cuda_fail(cudaError_t e, const char* what);
 struct MeshRec {
     bool live = false;
     bool owned = false;
+    bool oneBlock = false;  // owned arrays share the allocation at `positions`
     float* positions = nullptr;
     uint32_t* indices = nullptr;
     uint32_t* colors = nullptr;
@@ -43,6 +44,7 @@ struct MeshRec {
     float* itemBoxes = nullptr;   // per CR_BATCH triangles
     float* chunkBoxes = nullptr;  // per CR_VCHUNK vertices
     float* subBoxes = nullptr;    // per CR_SUB triangles
+    float* meshBox = nullptr;     // the whole mesh's box (6 floats)
     size_t boxBytes = 0;
     float box[6] = {NAN, NAN, NAN, NAN, NAN, NAN};  // host copy of the mesh box
     // compressed meshes (positions are uint16 xyz, indices bit-packed)
@@ -77,6 +79,9 @@ struct CopyJob {
 cr_status alloc_owned_mesh(cr_context* ctx, uint32_t nV, uint32_t nT, bool indexed, bool colored, MeshRec& m);
 // Builds the mesh's boxes and registers it; frees it on failure.
 cr_status register_mesh(cr_context* ctx, MeshRec& m, uint32_t* handle);
+// register_mesh for many meshes with one synchronize; handles in order.  On
+// failure none is registered and every buffer of `recs` is freed.
+cr_status register_meshes(cr_context* ctx, std::vector<MeshRec>& recs, std::vector<uint32_t>& handles);
 // The copies, split into 8 MiB pieces, on up to 8 host threads, each staging
 // through its own page-locked buffer on its own stream; returns when all
 // have landed.
@@ -179,6 +184,12 @@ cr_status render_impl(cr_context* ctx, const cr_instance* instances, uint32_t co
 cr_status ensure_queues(cr_context* ctx, uint64_t ntWant, uint64_t hugeWant);
 // (Re)builds a mesh's hierarchical-cull boxes from its current contents.
 cr_status build_mesh_boxes(cr_context* ctx, MeshRec& m);
+// build_mesh_boxes in two halves: the launch, and the box read back after a
+// synchronize (for many meshes: all launches, one synchronize).
+cr_status launch_mesh_boxes(cr_context* ctx, MeshRec& m);
+cr_status read_mesh_box(MeshRec& m);
+// Frees an owned mesh's arrays and returns their bytes to the budget.
+void free_mesh_arrays(cr_context* ctx, MeshRec& m);
 // Grows the per-vertex record buffer to at least `bytes`.
 cr_status ensure_records(cr_context* ctx, uint64_t bytes);
 // Builds a mesh's per-item vertex lists on first use (absent on failure).

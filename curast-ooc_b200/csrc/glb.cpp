@@ -818,25 +818,17 @@ cr_status cr_glb_create_meshes(cr_context* ctx, const cr_glb* g, uint32_t flags,
     if (s != CR_OK) {
         const std::string msg = cr_last_error();
         for (size_t k = 0; k < allocated; k++) {
-            ctx->dev_free(recs[k].positions, 0);
-            ctx->dev_free(recs[k].indices, 0);
-            ctx->dev_free(recs[k].colors, 0);
-            ctx->bytesInUse -= std::min(ctx->bytesInUse, recs[k].bytes);
+            free_mesh_arrays(ctx, recs[k]);
         }
         return fail(s, "%s", msg.c_str());
     }
     std::vector<char> done(g->meshes.size(), 0);
-    for (size_t k = 0; k < plain.size() && s == CR_OK; k++) {
-        s = register_mesh(ctx, recs[k], &mesh_handles[plain[k]]);
-        if (s == CR_OK) {
+    {
+        std::vector<uint32_t> hs;
+        s = register_meshes(ctx, recs, hs);
+        for (size_t k = 0; s == CR_OK && k < plain.size(); k++) {
+            mesh_handles[plain[k]] = hs[k];
             done[plain[k]] = 1;
-        } else {  // the later ones were never registered
-            for (size_t j = k + 1; j < plain.size(); j++) {
-                ctx->dev_free(recs[j].positions, 0);
-                ctx->dev_free(recs[j].indices, 0);
-                ctx->dev_free(recs[j].colors, 0);
-                ctx->bytesInUse -= std::min(ctx->bytesInUse, recs[j].bytes);
-            }
         }
     }
     for (size_t made = 0; made < g->meshes.size() && s == CR_OK; made++) {
