@@ -65,16 +65,21 @@ def test_screenshot_post(gpu, flags):
                                  (cb & np.uint64(0xFFFFFFFF)).astype(np.uint32))).mean() > 0.05
 
 
-@pytest.mark.parametrize("factor", [1, 2, 3])
-def test_display_post_supersampled(gpu, factor):
+@pytest.mark.parametrize("factor,edl,ssao", [(1, True, True), (2, True, True), (3, True, True), (4, True, True),
+                                             (2, True, False), (2, False, True), (5, True, True)])
+def test_display_post_supersampled(gpu, factor, edl, ssao):
     """The display resolve, at the colorbuffer's size (factor 1) and
-    averaging factor x factor blocks of a supersampled render."""
+    averaging factor x factor blocks of a supersampled render: factors 2 to 4
+    take the EDL taps from a shared-memory tile, larger ones read them
+    directly; each effect alone and both together."""
     import torch
 
     W, H = 240 * factor, 144 * factor
+    if factor == 5:  # output rows and columns that fill no whole block
+        W, H = 5 * 203, 5 * 117
     ow, oh = W // factor, H // factor
     mesh, view, proj = _scene(W, H)
-    flags = pc.CR_POST_EDL | pc.CR_POST_SSAO
+    flags = (pc.CR_POST_EDL if edl else 0) | (pc.CR_POST_SSAO if ssao else 0)
     with pc.Context() as ctx:
         _, _, cb, _ = render_ours(ctx, [mesh], [(0, scenes.identity())], view, proj, W, H)
         dcb = torch.from_numpy(cb.view(np.int64)).cuda()
@@ -82,9 +87,9 @@ def test_display_post_supersampled(gpu, factor):
         ctx.postprocess(dcb.data_ptr(), W, H, proj, out.data_ptr(), flags, pc.CR_POST_DISPLAY, out_size=(ow, oh))
         torch.cuda.synchronize()
         ours = out.cpu().numpy().view(np.uint32)
-    orc = ol.post(cb, W, H, proj, True, True, mode=1, out_size=(ow, oh))
+    orc = ol.post(cb, W, H, proj, edl, ssao, mode=1, out_size=(ow, oh))
     _assert_close(ours, orc, "ours vs oracle")
-    ref = reference().post(cb, W, H, proj, True, True, mode=1, out_size=(ow, oh))
+    ref = reference().post(cb, W, H, proj, edl, ssao, mode=1, out_size=(ow, oh))
     _assert_close(ours, ref, "ours vs reference")
 
 
