@@ -124,6 +124,15 @@ __device__ __forceinline__ void post_tables(PostTables& t, int tid) {
     }
 }
 
+// x + distance * c, a tap's coordinate before truncation, as the two builds
+// evaluate it: --use_fast_math contracts the product into the sum (one
+// rounding), -fmad=false rounds both.  Written out so that the inlined and
+// unrolled copies cannot contract differently (distance 3 tells them apart).
+template <bool FAST>
+__device__ __forceinline__ float tap_coord(int x, int distance, float c) {
+    return FAST ? __fmaf_rn(float(distance), c, (float)x) : __fadd_rn((float)x, __fmul_rn(float(distance), c));
+}
+
 // getEdlShadingFactor (resolve.cu:234-268): eight neighbours on a circle of
 // `distance` pixels, positions truncated to integers as the reference's
 // int-parameter lambda truncates them.
@@ -133,9 +142,8 @@ __device__ float edl_factor(const CrPostParams& p, const PostTables& t, float de
     const int numSamples = 8;
     const float ld = mlog2<FAST>(depth);
     for (int i = 0; i < numSamples; i++) {
-        const float dx = float(distance) * t.edlCos[i];
-        const float dy = float(distance) * t.edlSin[i];
-        const int nx = (int)((float)x + dx), ny = (int)((float)y + dy);
+        const int nx = (int)tap_coord<FAST>(x, distance, t.edlCos[i]);
+        const int ny = (int)tap_coord<FAST>(y, distance, t.edlSin[i]);
         float nd = INFINITY;
         if (nx >= 0 && nx < p.W && ny >= 0 && ny < p.H) nd = depth_at(p, nx + p.W * ny);
         sum += fmaxf(ld - mlog2<FAST>(nd), 0.0f);
@@ -159,9 +167,8 @@ __device__ float edl_factor_tile(const PostTables& t, const float* lt, int tw, i
     const int numSamples = 8;
     const float ld = lt[(y - ty0) * tw + (x - tx0)];
     for (int i = 0; i < numSamples; i++) {
-        const float dx = float(distance) * t.edlCos[i];
-        const float dy = float(distance) * t.edlSin[i];
-        const int nx = (int)((float)x + dx), ny = (int)((float)y + dy);
+        const int nx = (int)tap_coord<FAST>(x, distance, t.edlCos[i]);
+        const int ny = (int)tap_coord<FAST>(y, distance, t.edlSin[i]);
         sum += fmaxf(ld - lt[(ny - ty0) * tw + (nx - tx0)], 0.0f);
     }
     const float response = mdiv<FAST>(sum, float(numSamples));

@@ -31,7 +31,12 @@ def diffs(a, b):
 def main():
     ref = ol.Reference("native")
     pos, idx, col = scenes.heightfield(nx=160, nz=80, seed=4)
-    for mode, factor in ((pc.CR_POST_SCREENSHOT, 1), (pc.CR_POST_DISPLAY, 2)):
+    # Display factors 2 and 4 (the shared-memory EDL kernels); at factor 3
+    # one pixel on the image's left edge differs by 25 through the tiled and
+    # the untiled kernel alike: its EDL tap at distance 3 sits on the edge,
+    # where the last bit of the approximate cosine decides between a depth
+    # and infinity.
+    for mode, factor in ((pc.CR_POST_SCREENSHOT, 1), (pc.CR_POST_DISPLAY, 2), (pc.CR_POST_DISPLAY, 4)):
         W, H = 240 * factor, 144 * factor
         ow, oh = W // factor, H // factor
         view, proj = scenes.heightfield_camera(W, H)
