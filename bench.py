@@ -223,7 +223,7 @@ class ClockSampler:
 # distributed plumbing (replicas)
 # ---------------------------------------------------------------------------
 def step_spread(ms_steps):
-    """Median and 99th percentile of the per-step device times (this rank)."""
+    """Median and 99th percentile of the per-step times (this rank)."""
     a = np.asarray(ms_steps, np.float64)
     return {"p50": float(np.percentile(a, 50)), "p99": float(np.percentile(a, 99)), "steps": int(a.size)}
 
@@ -708,19 +708,24 @@ def run_glb(args, rank, world, local, wl):
             ctx.mesh_destroy(hm)
     barrier(world)
     ms = max_over_ranks(float(np.mean(times)) * 1e3, world)
-    # one more step, split into its phases (host clock, device synchronized)
-    t0 = time.perf_counter()
-    g = pc.Glb(data=data)
-    t1 = time.perf_counter()
-    hs = g.create_meshes(ctx)
-    torch.cuda.synchronize()
-    t2 = time.perf_counter()
-    g.instances(hs)
-    g.close()
-    t3 = time.perf_counter()
-    for hm in hs:
-        ctx.mesh_destroy(hm)
-    phases = {"open": (t1 - t0) * 1e3, "create_meshes": (t2 - t1) * 1e3, "instances_close": (t3 - t2) * 1e3}
+    # three more steps, each split into its phases (host clock, device
+    # synchronized); the median of each phase
+    split = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        g = pc.Glb(data=data)
+        t1 = time.perf_counter()
+        hs = g.create_meshes(ctx)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        g.instances(hs)
+        g.close()
+        t3 = time.perf_counter()
+        for hm in hs:
+            ctx.mesh_destroy(hm)
+        split.append(((t1 - t0) * 1e3, (t2 - t1) * 1e3, (t3 - t2) * 1e3))
+    med = np.median(np.array(split), axis=0)
+    phases = {"open": float(med[0]), "create_meshes": float(med[1]), "instances_close": float(med[2])}
     if rank != 0:
         ctx.close()
         return None
@@ -742,7 +747,7 @@ def run_glb(args, rank, world, local, wl):
         "data": "synthetic (seeded)",
         "config": {"workload": wl["name"], "desc": wl["desc"], "triangles": T, "file_bytes": len(data),
                    "parallelism": f"replicas x{world}", "l2": "not applicable (host path; file > L2)",
-                   "phases_ms": phases},
+                   "phases_ms": phases, "step_ms": step_spread([t * 1e3 for t in times])},
         "e2e": {"value": value, "unit": "Mtris/s", "ms_per_step": ms, "h2d_bytes_per_step": len(data),
                 "d2h_bytes_per_step": 0},
         "roofline": {"kernel": "host parse + upload (cr_glb_open, cr_glb_create_meshes)", "bound": "pcie",
