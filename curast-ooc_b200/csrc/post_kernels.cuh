@@ -438,6 +438,19 @@ __global__ void __launch_bounds__(256) k_post_display_ss(const CrPostParams p) {
     const int tid = threadIdx.y * PB_X + threadIdx.x;
     post_tables<FAST>(t, tid);
     const int tx0 = blockIdx.x * PB_X * F - (F + 1), ty0 = blockIdx.y * PB_Y * F - (F + 1);
+    const int x = blockIdx.x * PB_X + threadIdx.x, y = blockIdx.y * PB_Y + threadIdx.y;
+    const bool inside = x < p.outW && y < p.outH;
+    // this thread's colour and shade loads first: in flight while the tile fills
+    uint64_t px[F][F];
+    float sh[F][F];
+#pragma unroll
+    for (int dx = 0; dx < F; dx++)
+#pragma unroll
+        for (int dy = 0; dy < F; dy++) {
+            const int spid = (F * x + dx) + p.W * (F * y + dy);
+            px[dx][dy] = inside ? __ldg(reinterpret_cast<const unsigned long long*>(p.colorbuffer) + spid) : 0ull;
+            sh[dx][dy] = inside && p.ssao ? p.shade[spid] : 0.0f;
+        }
     if (p.edl) {
 #pragma unroll
         for (int k = 0; k < (N + NT - 1) / NT; k++) {
@@ -451,18 +464,7 @@ __global__ void __launch_bounds__(256) k_post_display_ss(const CrPostParams p) {
         }
     }
     __syncthreads();
-    const int x = blockIdx.x * PB_X + threadIdx.x, y = blockIdx.y * PB_Y + threadIdx.y;
-    if (x >= p.outW || y >= p.outH) return;
-    uint64_t px[F][F];
-    float sh[F][F];
-#pragma unroll
-    for (int dx = 0; dx < F; dx++)
-#pragma unroll
-        for (int dy = 0; dy < F; dy++) {
-            const int spid = (F * x + dx) + p.W * (F * y + dy);
-            px[dx][dy] = __ldg(reinterpret_cast<const unsigned long long*>(p.colorbuffer) + spid);
-            sh[dx][dy] = p.ssao ? p.shade[spid] : 0.0f;
-        }
+    if (!inside) return;
     float cr = 0.0f, cg = 0.0f, cbl = 0.0f;
     float edl = 0.0f, ssao = 0.0f;
     int numSamples = 0;
