@@ -92,15 +92,21 @@ def build_workload(name):
                     desc=f"one seeded {tris:,}-triangle displaced icosphere drawn as {count} instances (uniform "
                          f"rotation, scale 0.5-2, positions uniform in a 100^3 box), 1920x1080")
     if name.startswith("planet_"):
-        # planet_<N>m_1080p: the dense subdivided-sphere scene with N million triangles
-        count = int(name.split("_")[1].rstrip("m")) * 1_000_000
+        # planet_<N>m_1080p: the dense subdivided-sphere scene with N million
+        # triangles, camera just above the surface; planet_orbit_<N>m_1080p:
+        # the same mesh seen whole from outside (its geometry must be read)
+        parts = name.split("_")
+        orbit = parts[1] == "orbit"
+        count = int(parts[2 if orbit else 1].rstrip("m")) * 1_000_000
         W, H = 1920, 1080
         pos, idx, col = scenes.planet(count, device="cuda", width=W, height=H)
-        view, proj = scenes.planet_camera(W, H)
+        view, proj = scenes.planet_orbit_camera(W, H) if orbit else scenes.planet_camera(W, H)
+        where = ("seen whole from 2.6 radii (about half of the triangles face the camera, all of them in the frustum)"
+                 if orbit else "camera 0.035 radii above the surface")
         return dict(name=name, W=W, H=H, meshes=[(pos, idx, col)], instances=[(0, scenes.identity())],
                     view=view, proj=proj, device=True,
                     desc=f"seeded displaced icosphere, {count:,} triangles, per-patch subdivision levels giving a "
-                         f"lognormal pre-clip projected-area histogram, 1920x1080")
+                         f"lognormal pre-clip projected-area histogram, {where}, 1920x1080")
     if name.startswith("batched_"):
         # batched_<V>v_<N>m: N-million-triangle terrain seen by V seeded cameras
         nv_s, n_s = name.split("_")[1:3]
@@ -303,6 +309,35 @@ def cpu_baseline(wl, budget_s=20.0):
                       f"all {ncores} host threads (OpenMP), {dt:.2f} s"}
 
 
+def frame_parity(wl, ctx, inst, vis, rgba, nthreads=None):
+    """The bench's last frame against the CPU oracle's rendering of the same
+    frame (instances in the order cr_render draws them): visbuffer bit for
+    bit, RGBA8 within 1 per 8-bit channel.  Returns the parity record and the
+    oracle's raster time of the whole frame (seconds)."""
+    import oracle_lib as ol
+
+    nthreads = nthreads or os.cpu_count() or 1
+    W, H = wl["W"], wl["H"]
+    order, _, _ = ctx.frame_assemble(inst, wl["view"])
+    meshes = wl["decoded"] if wl.get("compressed") else [host_mesh(m) for m in wl["meshes"]]
+    items = [(*meshes[wl["instances"][k][0]], wl["instances"][k][1]) for k in order]
+    fr = ol.Frame(items, wl["view"])
+    t0 = time.perf_counter()
+    fb, ost = ol.raster(fr, W, H, wl["proj"][5], nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    _, orgba = ol.resolve(fr, wl["view"], wl["proj"], W, H, fb, nthreads=nthreads)
+    got = vis.cpu().numpy().view(np.uint64)
+    img = rgba.cpu().numpy().view(np.uint32)
+    bad = int((got != fb).sum())
+    ch = int(np.abs(img.view(np.uint8).astype(np.int16) - orgba.view(np.uint8).astype(np.int16)).max())
+    rec = {"visbuffer": "bit-exact" if bad == 0 else f"{bad} of {W * H} pixels differ",
+           "rgba_max_channel_diff": ch, "pixels": W * H, "covered": int((fb != np.uint64(0xFFFFFFF000000000)).sum()),
+           "oracle_nontrivial": int(ost.nontrivial), "oracle_huge_tiles": int(ost.huge_tiles),
+           "checked": "the last timed frame against the CPU oracle (IEEE restatement of the reference kernels)"}
+    del fr, items, meshes
+    return rec, dt, bad == 0 and ch <= 1
+
+
 def read_traffic(kernel, workload):
     path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.txt")
     try:
@@ -410,7 +445,11 @@ def run_ours(args, rank, world, local):
     h2d = 3 * ((n * 64 + 255) // 256 * 256) + (48 + 255) // 256 * 256
 
     if rank != 0:
+        ctx.close()
         return None
+    parity, oracle_s, parity_ok = (None, None, None)
+    if not args.no_parity:
+        parity, oracle_s, parity_ok = frame_parity(wl, ctx, inst, vis, rgba)
     peak, peak_kind = load_peaks()
     # Algorithmic bytes per launch, per unit processed.  The frame cull (timed
     # with the vertex pass) reads a 24-byte box per vertex chunk and per work
@@ -493,8 +532,18 @@ def run_ours(args, rank, world, local):
         "gpu_launches": 6 * args.steps,
         "clocks": clk,
     }
+    if parity is not None:
+        line["parity"] = "bit-exact" if parity_ok else "MISMATCH"
+        line["parity_detail"] = parity
     if not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(wl)
+        if oracle_s is not None and len(wl["instances"]) == 1 and oracle_s < 30.0:
+            # the parity check's oracle raster of the whole frame is the baseline
+            ncores = os.cpu_count() or 1
+            line["cpu_baseline"] = {"value": T / oracle_s / 1e9, "unit": "Gtris/s", "cores": ncores, "kind": "port",
+                                    "sample": f"oracle raster of the whole frame (all {T:,} triangles), all {ncores} "
+                                              f"host threads (OpenMP), {oracle_s:.2f} s"}
+        else:
+            line["cpu_baseline"] = cpu_baseline(wl)
     ctx.close()
     return line
 
@@ -642,8 +691,18 @@ def run_post(args, rank, world, local, wl):
     return line
 
 
-def glb_file(wl):
+def glb_writer_module():
+    """The binary glTF writer the glb tests build their files with."""
+    tests = os.path.join(ROOT, "tests")
+    if tests not in sys.path:
+        sys.path.insert(0, tests)
     import glb_writer
+
+    return glb_writer
+
+
+def glb_file(wl):
+    glb_writer = glb_writer_module()
     import scenes
 
     pos, idx, col = scenes.heightfield()
@@ -766,7 +825,7 @@ def run_glb(args, rank, world, local, wl):
 def glb_oracle_baseline(wl):
     """The oracle's restatement of the reference loader (Python, one thread)
     on one primitive of the same form."""
-    import glb_writer
+    glb_writer = glb_writer_module()
     import scenes
 
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -1278,6 +1337,7 @@ def main(argv=None):
                          "terrain), served_<R>rps, post_2160p_ss2 (EDL + SSAO + supersampled resolve), glb_<N>m "
                          "(binary glTF ingest of N one-million-triangle primitives)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the oracle check of the last frame")
     ap.add_argument("--ooc-nodes", type=int, default=247, help="out-of-core scene: nodes per side (served_*)")
     ap.add_argument("--serve-seconds", type=float, default=4.0, help="paced serving run length (served_*)")
     ap.add_argument("--capacity-requests", type=int, default=512, help="requests of the capacity run (served_*)")

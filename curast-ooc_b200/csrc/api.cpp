@@ -1184,7 +1184,8 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
             return fail(CR_ERR_CUDA, "stage-3 launch: %s", cudaGetErrorString(cudaGetLastError()));
         CR_CUDA(mark(5), "event");
         if (rasterEnd) CR_CUDA(cudaEventRecord(rasterEnd, stream), "event");
-        if (!(flags & CR_RENDER_NO_RESOLVE) && count && cr_launch_resolve(rp, stream))
+        // an empty frame still resolves: its image is all background
+        if (!(flags & CR_RENDER_NO_RESOLVE) && cr_launch_resolve(rp, stream))
             return fail(CR_ERR_CUDA, "resolve launch: %s", cudaGetErrorString(cudaGetLastError()));
         CR_CUDA(mark(6), "event");
         return CR_OK;

@@ -206,7 +206,7 @@ cr_status issue_batch(const CrFrameParams& fp, const CrResolveParams& rp, const 
         return fail(CR_ERR_CUDA, "batched stage-3 launch: %s", cudaGetErrorString(cudaGetLastError()));
     CR_CUDA(mark(5), "event");
     if (rasterEnd) CR_CUDA(cudaEventRecord(rasterEnd, stream), "event");
-    if (!(flags & CR_RENDER_NO_RESOLVE) && count &&
+    if (!(flags & CR_RENDER_NO_RESOLVE) &&
         cr_launch_resolve_views(rp, fp.views, fp.numViews, B.resolveBlocks, stream))
         return fail(CR_ERR_CUDA, "batched resolve launch: %s", cudaGetErrorString(cudaGetLastError()));
     CR_CUDA(mark(6), "event");

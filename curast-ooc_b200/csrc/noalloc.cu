@@ -79,6 +79,9 @@ cr_status setup(int device) {
     return CR_OK;
 }
 
+cr_status render_on_device(int32_t device, const cr_noalloc_instance* instances, uint32_t count, const cr_camera* cam,
+                           uint64_t d_visbuffer, uint64_t d_rgba, int32_t display, void* stream_);
+
 }  // namespace
 
 extern "C" cr_status cr_render_noalloc(int32_t device, const cr_noalloc_instance* instances, uint32_t count,
@@ -92,6 +95,7 @@ extern "C" cr_status cr_render_noalloc(int32_t device, const cr_noalloc_instance
         return fail(CR_ERR_INVALID, "cr_render_noalloc: bad resolution%s");
     if (!d_visbuffer || (d_visbuffer & 15))
         return fail(CR_ERR_INVALID, "cr_render_noalloc: visbuffer must be a 16-byte aligned device pointer%s");
+    if (d_rgba & 3) return fail(CR_ERR_INVALID, "cr_render_noalloc: the RGBA8 image must be 4-byte aligned%s");
     if (device < 0 || device >= kMaxDevices) return fail(CR_ERR_INVALID, "cr_render_noalloc: bad device%s");
     uint64_t vsum = 0, tsum = 0;
     for (uint32_t i = 0; i < count; i++) {
@@ -109,8 +113,22 @@ extern "C" cr_status cr_render_noalloc(int32_t device, const cr_noalloc_instance
                     (long long)vsum, (long long)CR_NOALLOC_MAX_VERTICES);
     if (tsum >= (1ull << 36)) return fail(CR_ERR_INVALID, "cr_render_noalloc: too many triangles%s");
 
-    cudaError_t e = cudaSetDevice(device);
+    // the caller's current device is put back on every return
+    int callerDevice = -1;
+    cudaError_t e = cudaGetDevice(&callerDevice);
+    if (e != cudaSuccess) return fail(CR_ERR_CUDA, "cr_render_noalloc: cudaGetDevice: %s", cudaGetErrorString(e));
+    e = cudaSetDevice(device);
     if (e != cudaSuccess) return fail(CR_ERR_CUDA, "cr_render_noalloc: cudaSetDevice: %s", cudaGetErrorString(e));
+    const cr_status s = render_on_device(device, instances, count, cam, d_visbuffer, d_rgba, display, stream_);
+    if (callerDevice != device) cudaSetDevice(callerDevice);
+    return s;
+}
+
+namespace {
+
+cr_status render_on_device(int32_t device, const cr_noalloc_instance* instances, uint32_t count, const cr_camera* cam,
+                           uint64_t d_visbuffer, uint64_t d_rgba, int32_t display, void* stream_) {
+    cudaError_t e;
     cr_status s = setup(device);
     if (s) return s;
     unsigned char* scratch = g_scratch[device];
@@ -218,7 +236,7 @@ extern "C" cr_status cr_render_noalloc(int32_t device, const cr_noalloc_instance
     if (cr_launch_clear(fp.fb, numPixels, fp.counters, stream) ||
         (count && (cr_launch_vertex(fp, shape, stream) || cr_launch_stage1(fp, shape, stream) ||
                    cr_launch_stage2(fp, shape, stream) || cr_launch_stage3(fp, shape, stream))) ||
-        (count && d_rgba && cr_launch_resolve(rp, stream)))
+        (d_rgba && cr_launch_resolve(rp, stream)))
         return fail(CR_ERR_CUDA, "cr_render_noalloc: launch failed: %s", cudaGetErrorString(cudaGetLastError()));
 
     unsigned long long counters[CR_CTR_COUNT];
@@ -231,3 +249,5 @@ extern "C" cr_status cr_render_noalloc(int32_t device, const cr_noalloc_instance
                     "", (long long)counters[CR_CTR_NONTRIVIAL], (long long)counters[CR_CTR_HUGE]);
     return CR_OK;
 }
+
+}  // namespace

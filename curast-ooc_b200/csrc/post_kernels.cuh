@@ -504,13 +504,10 @@ template <bool FAST>
 void launch_post(const CrPostParams& p, cudaStream_t st) {
     if (p.ssao) {
         // the occlusion taps scatter over hundreds of pixels: as much L1 as
-        // the SM offers
-        static bool carveout = false;
-        if (!carveout) {
-            cudaFuncSetAttribute(k_ssao_occlusion<FAST>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 cudaSharedmemCarveoutMaxL1);
-            carveout = true;
-        }
+        // the SM offers.  The attribute belongs to the current device, and
+        // setting it is a cheap host call, so every pass sets it.
+        cudaFuncSetAttribute(k_ssao_occlusion<FAST>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxL1);
         const dim3 g((p.W + PB_X - 1) / PB_X, (p.H + PB_Y - 1) / PB_Y);
         k_ssao_occlusion<FAST><<<g, dim3(PB_X, PB_Y), 0, st>>>(p);
         const dim3 gb((p.W + PB_X * BLUR_PX - 1) / (PB_X * BLUR_PX), (p.H + PB_Y * BLUR_PX - 1) / (PB_Y * BLUR_PX));

@@ -65,9 +65,11 @@ __device__ __forceinline__ void resolve_pixel(const CrResolveParams& p, const in
     const int pid = x + p.W * y;
     const uint64_t pixel = __ldcs(reinterpret_cast<const unsigned long long*>(p.fb) + pid);
 
-    // unpack_pixel, helpers:54-66
+    // unpack_pixel, helpers:54-66; a frame without instances has drawn
+    // nothing, so every pixel is background (the reference resolves the
+    // cleared buffer unconditionally, resolve.cu:1134-1140)
     const uint32_t ud = (uint32_t)(pixel >> 33) & 0x7FFFFFF8u;
-    const float depth = (ud == 0x7FFFFFF8u) ? INFINITY : __uint_as_float(ud);
+    const float depth = (ud == 0x7FFFFFF8u || p.numInstances == 0) ? INFINITY : __uint_as_float(ud);
     const uint64_t tid = pixel & 0xFFFFFFFFFull;
 
     if (isinf(depth) ? !p.writeBackground : (tid < p.idLo || tid >= p.idHi)) return;  // another pass owns it
@@ -210,7 +212,7 @@ __global__ void __launch_bounds__(256) k_resolve_views(const CrResolveParams bas
 }  // namespace
 
 int cr_launch_resolve(const CrResolveParams& p, void* stream) {
-    if (p.W <= 0 || p.H <= 0 || p.numInstances == 0) return 0;
+    if (p.W <= 0 || p.H <= 0) return 0;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((p.W + 31) / 32, (p.H + 7) / 8);
     cfg.blockDim = dim3(32, 8);
@@ -225,7 +227,7 @@ int cr_launch_resolve(const CrResolveParams& p, void* stream) {
 
 int cr_launch_resolve_views(const CrResolveParams& base, const CrView* views, uint32_t numViews, uint32_t numBlocks,
                             void* stream) {
-    if (numViews == 0 || numBlocks == 0 || base.numInstances == 0) return 0;
+    if (numViews == 0 || numBlocks == 0) return 0;
     k_resolve_views<<<numBlocks, dim3(32, 8), 0, (cudaStream_t)stream>>>(base, views, numViews);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

@@ -164,6 +164,24 @@ def planet_camera(width=1920, height=1080):
     return view, proj
 
 
+# direction from the planet's centre to the orbit camera: the triangle-weighted
+# mean direction of the seed-17 planet's patches, so that about half of its
+# triangles face the camera
+PLANET_ORBIT_DIR = (0.0756, -0.0559, 0.2443)
+
+
+def planet_orbit_camera(width=1920, height=1080, distance=2.6):
+    """The planet seen whole from outside: the eye `distance` radii from the
+    centre (the whole sphere inside the 60-degree field of view), looking at
+    the centre, so most triangles are in the frustum and about half face the
+    camera -- a frame whose geometry must be read."""
+    d = np.asarray(PLANET_ORBIT_DIR, np.float64)
+    eye = d / np.linalg.norm(d) * distance
+    view = look_at(eye, (0.0, 0.0, 0.0))
+    proj = perspective(PLANET["fovy"], width / height, 0.01, 10.0)
+    return view, proj
+
+
 def _planet_levels(num_triangles, seed, width, height):
     """Per-patch subdivision levels: each patch's triangles get a projected
     area drawn from a lognormal around a common median, so the triangle-

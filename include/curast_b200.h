@@ -601,12 +601,19 @@ cr_status cr_server_destroy(cr_server* server);
  *     summed over them, else CR_ERR_INVALID.  A frame needing more than
  *     CR_NOALLOC_MAX_NONTRIVIAL stage-2 or CR_NOALLOC_MAX_TILES stage-3
  *     entries returns CR_ERR_QUEUE_OVERFLOW (output incomplete).
- *   - The call is synchronous on `stream` (it reads back the queue counters).
- *   - The first call on a device looks up the array's device address (once
- *     per device); make that first call before any stream capture.
+ *   - The call is synchronous on `stream`: it uploads the frame table from
+ *     host memory and reads back the queue counters, then synchronises the
+ *     stream.  So it must never be called on a stream that is being captured
+ *     into a CUDA graph.  The first call on a device also looks up the
+ *     array's device address (once per device).
  *   - Every call shares the one array: calls that overlap on the GPU (other
  *     streams, other host threads) race and must be serialised by the caller.
- *     Each call resets the counters it needs; nothing else carries over. */
+ *     Each call resets the counters it needs; nothing else carries over.
+ *   - d_visbuffer is 16-byte aligned, d_rgba (NULL: no image) 4-byte aligned.
+ *     With count == 0 the visbuffer is cleared and the image is all
+ *     background.
+ *   - The calling thread's current device is the same after the call as
+ *     before it. */
 #define CR_NOALLOC_MAX_INSTANCES 16u
 #define CR_NOALLOC_MAX_VERTICES (4u << 20)
 #define CR_NOALLOC_MAX_NONTRIVIAL (512u << 10)

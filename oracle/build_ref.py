@@ -22,7 +22,8 @@ The source text is read at build time only; nothing from the reference is
 copied into this repository.  Outputs go to oracle/_ref/ (git-ignored, but
 shipped with the working tree so the GPU tests can load them).
 
-Usage:  python oracle/build_ref.py [--reference /root/reference] [--force]
+Usage:  python oracle/build_ref.py [--reference DIR] [--force]
+        (DIR defaults to $CURAST_REFERENCE, else /root/reference)
 """
 import argparse
 import os
@@ -164,7 +165,7 @@ def build(ref: str, force: bool = False) -> None:
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("CURAST_REFERENCE", "/root/reference"))
     ap.add_argument("--force", action="store_true")
     a = ap.parse_args(argv)
     if not os.path.isdir(a.reference):

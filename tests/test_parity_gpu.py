@@ -371,9 +371,13 @@ def test_empty_frame_clears(ctx):
     vis = torch.zeros(W * H, dtype=torch.int64, device="cuda")
     rgba = torch.zeros(W * H, dtype=torch.int32, device="cuda")
     cam = pc.make_camera(scenes.identity(), scenes.perspective(60.0, W / H), W, H)
-    ctx.render(pc.make_instances([]), cam, vis.data_ptr(), rgba.data_ptr())
+    cb = torch.zeros(W * H, dtype=torch.int64, device="cuda")
+    ctx.render(pc.make_instances([]), cam, vis.data_ptr(), rgba.data_ptr(), cb.data_ptr())
     torch.cuda.synchronize()
     assert (vis.cpu().numpy().view(np.uint64) == CLEAR).all()
+    # the reference resolves unconditionally: background colour, infinite depth
+    assert (rgba.cpu().numpy().view(np.uint32) == 0xFFFFFFFF).all()
+    assert (cb.cpu().numpy().view(np.uint64) == np.uint64(0x7F800000 << 32)).all()
 
 
 def test_bounded_wait_timeout_is_reported_and_context_survives(gpu):

@@ -4,9 +4,10 @@ It exists for callers that may not allocate device memory while they render
 (a plug-in whose host owns all device memory or caps it, a frame loop that
 cannot take cudaMalloc/cudaFree's device-wide synchronisation mid-frame).  It
 runs the same kernels as cr_render with all scratch in one static device
-array, so its output must equal cr_render's: visbuffer bit for bit, colours
-within 1 per 8-bit channel -- here on two calls in a row with different
-cameras, which also shows that nothing from one call leaks into the next.
+array, so its output must equal cr_render's: visbuffer and RGBA8 image bit
+for bit (both paths run the same resolve kernel on the same frame table) --
+here on two calls in a row with different cameras, which also shows that
+nothing from one call leaks into the next.
 
 This file is named to be collected last, so a run that stops at the first
 failure has run every other test before it.
@@ -18,7 +19,6 @@ import pycurast as pc
 import scenes
 
 pytestmark = pytest.mark.gpu
-COLOR_TOL = 1
 
 
 def _scene(torch):
@@ -67,9 +67,25 @@ def test_noalloc_matches_cr_render_on_two_calls(gpu):
             b = vis_b.cpu().numpy().view(np.uint64)
             assert (a != pc.CLEAR_PIXEL).sum() > 1000
             assert np.array_equal(a, b), f"{int((a != b).sum())} visbuffer pixels differ"
-            ca = rgba_a.cpu().numpy().view(np.uint8).reshape(-1, 4).astype(np.int16)
-            cb = rgba_b.cpu().numpy().view(np.uint8).reshape(-1, 4).astype(np.int16)
-            assert int(np.abs(ca - cb).max()) <= COLOR_TOL
+            ca = rgba_a.cpu().numpy().view(np.uint32)
+            cb = rgba_b.cpu().numpy().view(np.uint32)
+            assert np.array_equal(ca, cb), f"{int((ca != cb).sum())} RGBA8 pixels differ"
+
+
+def test_noalloc_empty_instance_list_writes_background(gpu):
+    """No instances: the visbuffer is cleared and the image is all
+    background, not whatever the buffers held before."""
+    import torch
+
+    W, H = 96, 40
+    vis = torch.zeros(W * H, dtype=torch.int64, device="cuda")
+    rgba = torch.zeros(W * H, dtype=torch.int32, device="cuda")
+    cam = pc.make_camera(scenes.identity(), scenes.perspective(60.0, W / H), W, H)
+    st = pc.render_noalloc(0, [], cam, vis.data_ptr(), rgba.data_ptr())
+    assert st == pc.CR_OK, pc.load().cr_last_error()
+    torch.cuda.synchronize()
+    assert (vis.cpu().numpy().view(np.uint64) == pc.CLEAR_PIXEL).all()
+    assert (rgba.cpu().numpy().view(np.uint32) == 0xFFFFFFFF).all()
 
 
 def test_noalloc_rejects_sizes_beyond_its_limits(gpu):
