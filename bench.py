@@ -349,6 +349,49 @@ def read_traffic(kernel, workload):
     return None
 
 
+def plain_algorithmic_bytes(wl, fstats, T):
+    """Algorithmic bytes per launch of the plain frame's kernels, from the
+    units the frame processed (its stats).  The frame cull (timed with the
+    vertex pass) reads a 24-byte box per vertex chunk and per work item and
+    writes 8 B per listed item; the vertex pass reads 12 B of position and
+    writes one record (4-byte cell records up to 4096 pixels a side, else 8)
+    per vertex of each chunk its box did not classify; stage 1 reads the
+    12-byte index triple of every triangle of each drawn work item and each
+    vertex record once, and writes and reads 8 B per survivor of the records.
+    Frames that draw a mesh more than once cull from box proofs and per-item
+    vertex lists (no per-vertex records in device memory).  Returns (bytes per
+    stage, triangles in drawn items, vertices evaluated)."""
+    mids = [m for m, _ in wl["instances"]]
+    direct = len(set(mids)) < len(mids)
+    rec = 4 if max(wl["W"], wl["H"]) <= 4096 else 8
+    items, items_drawn = int(fstats.work_items), int(fstats.work_items_drawn)
+    chunks, chunks_eval = int(fstats.vertex_chunks), int(fstats.vertex_chunks_evaluated)
+    surv = int(getattr(fstats, "stage1_survivors", 0))
+    nV_inst = sum(wl["meshes"][m][0].shape[0] for m, _ in wl["instances"])
+    if direct:
+        # frame cull: one 24-byte item box per item (the instance matrices
+        # stay in L1) and 8 B per listed item; stage 1: the 1408-byte vertex
+        # list block of each listed item and the positions of its distinct
+        # vertices (at most 128 x 12 B for these meshes)
+        v_eval, tri_drawn = 0, min(T, items_drawn * 128)
+        algo = {"vertex": 24 * items + 8 * items_drawn,
+                "stage1": (1408 + 12 * 128) * items_drawn, "boxes": True}
+    elif chunks:
+        v_eval = min(nV_inst, chunks_eval * 1024)
+        tri_drawn = min(T, items_drawn * 128)
+        algo = {"vertex": 24 * (chunks + items) + (12 + rec) * v_eval + 8 * items_drawn,
+                "stage1": 12 * tri_drawn + rec * v_eval + 16 * surv}
+    else:
+        v_eval, tri_drawn = nV_inst, T
+        algo = {"vertex": (12 + rec) * nV_inst, "stage1": 12 * T + rec * nV_inst + 16 * surv}
+    if wl.get("compressed"):
+        # compressed meshes: 6-byte positions, 3 x bits / 8 bytes of indices per triangle
+        ib = 3 * wl["compressed"][0].bits / 8.0
+        algo = {"vertex": 24 * (chunks + items) + (6 + rec) * v_eval + 8 * items_drawn,
+                "stage1": ib * tri_drawn + rec * v_eval + 16 * surv}
+    return algo, tri_drawn, v_eval
+
+
 def run_ours(args, rank, world, local):
     import torch
 
@@ -451,44 +494,9 @@ def run_ours(args, rank, world, local):
     if not args.no_parity:
         parity, oracle_s, parity_ok = frame_parity(wl, ctx, inst, vis, rgba)
     peak, peak_kind = load_peaks()
-    # Algorithmic bytes per launch, per unit processed.  The frame cull (timed
-    # with the vertex pass) reads a 24-byte box per vertex chunk and per work
-    # item; the vertex pass reads 12 B of position and writes one record
-    # (1 B outcode, or an 8-byte cell) per vertex of each chunk its box did
-    # not classify; stage 1 reads the 12-byte index triple of every triangle
-    # of each drawn work item and each vertex record once.  The whole-frame
-    # figure keeps the reference's 12T + 12V + 16P (+ 12P resolve), counting
-    # the geometry a full scan reads: culled groups are not read, so it can
-    # exceed the bandwidth peak.
-    # frames that draw a mesh more than once cull from box proofs and per-item
-    # vertex lists (no per-vertex records in device memory)
-    mids = [m for m, _ in wl["instances"]]
-    direct = len(set(mids)) < len(mids)
-    rec = 0 if direct else 1
+    algo, tri_drawn, v_eval = plain_algorithmic_bytes(wl, fstats, T)
     items, items_drawn = int(fstats.work_items), int(fstats.work_items_drawn)
     chunks, chunks_eval = int(fstats.vertex_chunks), int(fstats.vertex_chunks_evaluated)
-    nV_inst = sum(wl["meshes"][m][0].shape[0] for m, _ in wl["instances"])
-    if direct:
-        # frame cull: one 24-byte item box per item (the instance matrices
-        # stay in L1) and 8 B per listed item; stage 1: the 1408-byte vertex
-        # list block of each listed item and the positions of its distinct
-        # vertices (at most 128 x 12 B for these meshes)
-        v_eval, tri_drawn = 0, min(T, items_drawn * 128)
-        algo = {"vertex": 24 * items + 8 * items_drawn,
-                "stage1": (1408 + 12 * 128) * items_drawn}
-    elif chunks:
-        v_eval = min(nV_inst, chunks_eval * 1024)
-        tri_drawn = min(T, items_drawn * 128)
-        algo = {"vertex": 24 * (chunks + items) + (12 + rec) * v_eval + 8 * items_drawn,
-                "stage1": 12 * tri_drawn + rec * v_eval}
-    else:
-        v_eval, tri_drawn = nV_inst, T
-        algo = {"vertex": (12 + rec) * nV_inst, "stage1": 12 * T + rec * nV_inst}
-    if wl.get("compressed"):
-        # compressed meshes: 6-byte positions, 3 x bits / 8 bytes of indices per triangle
-        ib = 3 * wl["compressed"][0].bits / 8.0
-        algo = {"vertex": 24 * (chunks + items) + (6 + rec) * v_eval + 8 * items_drawn,
-                "stage1": ib * tri_drawn + rec * v_eval}
     dominant = max(("vertex", "stage1", "stage2", "stage3", "resolve", "clear"), key=lambda s: stage_ms[s])
     rk = "stage1" if dominant not in algo else dominant
     t_k = stage_ms[rk]
@@ -517,14 +525,17 @@ def run_ours(args, rank, world, local):
                    "nontrivial": int(fstats.nontrivial), "huge_tiles": int(fstats.huge_tiles),
                    "hierarchical_cull": {"work_items": items, "work_items_drawn": items_drawn,
                                          "vertex_chunks": chunks, "vertex_chunks_evaluated": chunks_eval,
-                                         "triangles_in_drawn_items": tri_drawn},
+                                         "triangles_in_drawn_items": tri_drawn,
+                                         "stage1_survivors": int(fstats.stage1_survivors)},
                    "frame_roofline": {"bytes": frame_bytes, "achieved_gbs": frame_gbs,
                                       "frac": frame_gbs / peak,
                                       "note": "reference formula 12T+12V+28P; provably culled groups are not "
                                               "read, so this can exceed 1"}},
         "e2e": {"value": world * T / (e2e * 1e-3) / 1e9, "unit": "Gtris/s", "ms_per_step": e2e,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 4 * W * H},
-        "roofline": {"kernel": "k_cull + k_vertex" if rk == "vertex" else f"k_{rk}", "bound": "hbm",
+        "roofline": {"kernel": {"vertex": "k_cull + k_vertex",
+                                "stage1": "k_stage1" if algo.get("boxes") else "k_s1cull + k_s1raster"}.get(
+                                    rk, f"k_{rk}"), "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "algorithmic_bytes": algo[rk], "kernel_ms": t_k,
@@ -544,8 +555,196 @@ def run_ours(args, rank, world, local):
                                               f"host threads (OpenMP), {oracle_s:.2f} s"}
         else:
             line["cpu_baseline"] = cpu_baseline(wl)
+    if args.sub_results and world == 1 and wl["name"] == DEFAULT_WORKLOAD:
+        # the same mesh seen whole from outside: its geometry must be read
+        orbit = sub_workload(wl, "planet_orbit_400m_1080p")
+        subs = [sub_plain(args, orbit, ctx, handles, True)]
+        ctx.close()
+        del wl, handles, orbit
+        torch.cuda.empty_cache()
+        subs += other_sub_results(args)
+        line["sub_results"] = subs
+        return line
     ctx.close()
     return line
+
+
+DEFAULT_WORKLOAD = "planet_400m_1080p"
+# the other benchmark configurations, timed after the default one when
+# --sub-results is on (the default), each against the reference arm's own
+SUB_WORKLOADS = ("planet_orbit_400m_1080p", "heightfield_1m_1080p", "instanced_3000x1m_1080p", "batched_64v_60m")
+
+
+def sub_workload(wl, name):
+    """A planet workload on the already built mesh with another camera."""
+    import scenes
+
+    out = dict(wl)
+    out["name"] = name
+    if "orbit" in name:
+        out["view"], out["proj"] = scenes.planet_orbit_camera(wl["W"], wl["H"])
+        out["desc"] = wl["desc"].replace("camera 0.035 radii above the surface",
+                                         "seen whole from 2.6 radii (about half of the triangles face the camera, "
+                                         "all of them in the frustum)")
+    return out
+
+
+def other_sub_results(args):
+    import torch
+
+    import pycurast as pc
+
+    subs = []
+    for name in SUB_WORKLOADS[1:]:
+        wl = build_workload(name)
+        if wl.get("batched"):
+            subs.append(sub_batched(args, wl))
+        else:
+            ctx = pc.Context()
+            handles = [ctx.mesh_from_device(p.data_ptr(), p.shape[0], i.data_ptr(), i.shape[0], c.data_ptr())
+                       if wl["device"] else ctx.mesh_from_host(p, i, c) for (p, i, c) in wl["meshes"]]
+            # the 3e9-triangle instanced frame's oracle takes tens of seconds:
+            # its parity is checked by the tests at the same size
+            subs.append(sub_plain(args, wl, ctx, handles, len(wl["instances"]) == 1))
+            ctx.close()
+        del wl
+        torch.cuda.empty_cache()
+    return subs
+
+
+def sub_plain(args, wl, ctx, handles, with_parity):
+    """A compact record of the plain frame of `wl` (meshes resident in HBM,
+    `handles` on `ctx`): device-timed steps, the per-stage split, the
+    dominant kernel's roofline and the parity of the last frame."""
+    import torch
+
+    import pycurast as pc
+
+    T, V, Tu = scene_counts(wl)
+    W, H = wl["W"], wl["H"]
+    inst = pc.make_instances([(handles[m], w) for m, w in wl["instances"]])
+    cam = pc.make_camera(wl["view"], wl["proj"], W, H)
+    vis = torch.empty(W * H, dtype=torch.int64, device="cuda")
+    rgba = torch.empty(W * H, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    flush = None
+    if 12 * Tu + 12 * V + 12 * W * H < 2 * L2_BYTES:
+        flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device="cuda")
+    ctx.render(inst, cam, vis.data_ptr(), rgba.data_ptr(), flags=pc.CR_RENDER_SYNC, stream=sh)
+    for _ in range(max(args.warmup - 1, 0)):
+        ctx.render(inst, cam, vis.data_ptr(), rgba.data_ptr(), flags=0, stream=sh)
+    ctx.sync()
+    _, fstats = ctx.stats()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        if flush is not None:
+            flush.fill_(k)
+        evs[k][0].record(stream)
+        ctx.render(inst, cam, vis.data_ptr(), rgba.data_ptr(), flags=0, stream=sh)
+        evs[k][1].record(stream)
+    torch.cuda.synchronize()
+    ctx.sync()
+    ms_steps = [a.elapsed_time(b) for a, b in evs]
+    ms = float(np.mean(ms_steps))
+    ctx.drain_stage_times()
+    for k in range(args.steps):
+        if flush is not None:
+            flush.fill_(k)
+        ctx.render(inst, cam, vis.data_ptr(), rgba.data_ptr(), flags=pc.CR_RENDER_TIMING, stream=sh)
+    torch.cuda.synchronize()
+    ctx.sync()
+    stage_ms, nframes = ctx.drain_stage_times()
+    stage_ms = {k: v / max(nframes, 1) for k, v in stage_ms.items()}
+    peak, peak_kind = load_peaks()
+    algo, tri_drawn, v_eval = plain_algorithmic_bytes(wl, fstats, T)
+    dominant = max(("vertex", "stage1", "stage2", "stage3", "resolve", "clear"), key=lambda x: stage_ms[x])
+    rk = "stage1" if dominant not in algo else dominant
+    achieved = algo[rk] / (stage_ms[rk] * 1e-3) / 1e9
+    frame_bytes = 12 * T + 12 * V + 28 * W * H
+    rec = {"workload": wl["name"], "desc": wl["desc"], "metric": "Gtris/s", "value": T / (ms * 1e-3) / 1e9,
+           "unit": "Gtris/s", "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup,
+           "step_ms": step_spread(ms_steps), "triangles": T, "width": W, "height": H,
+           "l2": "flushed between steps" if flush is not None else "inputs larger than L2",
+           "stage_ms": stage_ms, "dominant_stage": dominant,
+           "cull": {"work_items": int(fstats.work_items), "work_items_drawn": int(fstats.work_items_drawn),
+                    "vertex_chunks": int(fstats.vertex_chunks),
+                    "vertex_chunks_evaluated": int(fstats.vertex_chunks_evaluated),
+                    "stage1_survivors": int(fstats.stage1_survivors), "nontrivial": int(fstats.nontrivial),
+                    "huge_tiles": int(fstats.huge_tiles)},
+           "roofline": {"kernel": {"vertex": "k_cull + k_vertex",
+                                   "stage1": "k_stage1" if algo.get("boxes") else "k_s1cull + k_s1raster"}.get(
+                                       rk, f"k_{rk}"),
+                        "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "peak_kind": peak_kind, "algorithmic_bytes": algo[rk], "kernel_ms": stage_ms[rk]},
+           "frame_roofline": {"bytes": frame_bytes, "achieved_gbs": frame_bytes / (ms * 1e-3) / 1e9,
+                              "frac": frame_bytes / (ms * 1e-3) / 1e9 / peak,
+                              "note": "reference formula 12T+12V+28P"}}
+    if with_parity and not args.no_parity:
+        par, _, ok = frame_parity(wl, ctx, inst, vis, rgba)
+        rec["parity"] = "bit-exact" if ok else "MISMATCH"
+        rec["parity_detail"] = par
+    return rec
+
+
+def sub_batched(args, wl):
+    """A compact record of the batched frame (autotuned plan replayed as a
+    CUDA graph) beside the plain per-view loop at identical outputs."""
+    import torch
+
+    import pycurast as pc
+    import scenes
+
+    cams = wl["cams"]
+    nv = len(cams)
+    ctx = pc.Context()
+    p, i, c = wl["meshes"][0]
+    h = ctx.mesh_from_device(p.data_ptr(), p.shape[0], i.data_ptr(), i.shape[0], c.data_ptr())
+    inst = pc.make_instances([(h, scenes.identity())])
+    ccams = [pc.make_camera(*cam) for cam in cams]
+    vis = [torch.empty(W * H, dtype=torch.int64, device="cuda") for _, _, W, H in cams]
+    rgba = [torch.empty(W * H, dtype=torch.int32, device="cuda") for _, _, W, H in cams]
+    views = [(ccams[k], vis[k].data_ptr(), rgba[k].data_ptr(), 0) for k in range(nv)]
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    ctx.autotune_batch(inst, views)
+    plan = pc.BatchPlan(ctx, inst, views)
+    for _ in range(args.warmup):
+        plan.launch(sh)
+    plan.wait()
+
+    def timed(fn, steps):
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for k in range(steps):
+            evs[k][0].record(stream)
+            fn()
+            evs[k][1].record(stream)
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in evs]
+
+    steps = max(3, min(args.steps, 10))
+    ms_steps = timed(lambda: plan.launch(sh), steps)
+    plan.wait()
+    batched = [v.cpu().numpy() for v in vis]
+
+    def plain():
+        for j in range(nv):
+            ctx.render(inst, ccams[j], vis[j].data_ptr(), rgba[j].data_ptr(), 0, pc.CR_DISPLAY_VERTEX_COLORS, 0, sh)
+
+    for j in range(nv):  # synchronous frames first: they size the context's queues for every view
+        ctx.render(inst, ccams[j], vis[j].data_ptr(), rgba[j].data_ptr(), flags=pc.CR_RENDER_SYNC, stream=sh)
+    plain_steps = timed(plain, max(3, min(args.steps, 5)))
+    ctx.sync()
+    same = all(np.array_equal(a, v.cpu().numpy()) for a, v in zip(batched, vis))
+    plan.close()
+    ctx.close()
+    ms, plain_ms = float(np.mean(ms_steps)), float(np.mean(plain_steps))
+    return {"workload": wl["name"], "desc": wl["desc"], "metric": "views/s", "value": nv / (ms * 1e-3),
+            "unit": "views/s", "ms_per_step": ms, "steps": steps, "step_ms": step_spread(ms_steps),
+            "plain_loop": {"ms_per_step": plain_ms, "views_per_s": nv / (plain_ms * 1e-3)},
+            "speedup_vs_plain_loop": plain_ms / ms,
+            "parity": "bit-exact vs the plain loop" if same else "MISMATCH vs the plain loop"}
 
 
 POST_METRIC = "Mpx/s (EDL + SSAO + 2x supersampled display resolve of a 3840x2160 colorbuffer, per pass)"
@@ -1177,31 +1376,83 @@ def run_reference(args, rank, world, local):
                 "config": {"workload": wl["name"], "desc": wl["desc"], "parallelism": "single host thread"},
                 "cpu_baseline": base,
                 "e2e": {"value": base["value"], "unit": "Mtris/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    T, V, Tu = scene_counts(wl)
-    W, H = wl["W"], wl["H"]
     try:
         ref = ol.Reference("native", device=local)
     except Exception as e:  # noqa: BLE001
         return {"impl": "reference", "unavailable": f"reference kernels not loadable: {e}"}
-    if wl.get("compressed"):  # the reference's *_compressed kernels
-        ids = [ref.mesh_compressed_host(cp.packed, cp.positions, cp.num_triangles, dec[2], cp.aabb_min, cp.aabb_max,
-                                        cp.index_min, cp.index_max) for cp, dec in zip(wl["compressed"], wl["decoded"])]
-    elif wl["device"]:
-        ids = [ref.mesh_device(p.data_ptr(), p.shape[0], i.data_ptr(), i.shape[0], c.data_ptr())
-               for (p, i, c) in wl["meshes"]]
-    else:
-        ids = [ref.mesh_host(p, i, c) for (p, i, c) in wl["meshes"]]
+    r = ref_plain(args, wl, ref)
+    line = {
+        "impl": "reference",
+        "metric": "Gtris/s @1080p (plain 3-stage visbuffer + resolve, one frame per step)",
+        "value": r["value"],
+        "unit": "Gtris/s",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": r["ms_per_step"],
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": wl["name"], "desc": wl["desc"], "triangles": r["triangles"], "vertices": r["vertices"],
+                   "width": wl["W"], "height": wl["H"], "parallelism": "single GPU", "stage_ms": r["stage_ms"],
+                   "nontrivial": r["nontrivial"], "huge_tiles": r["huge_tiles"],
+                   "build": "CuRast NVRTC recipe (--use_fast_math, LTO) for sm_100a"},
+        "cpu_baseline": {"kind": "reference", "value": r["value"], "unit": "Gtris/s", "cores": 0,
+                         "sample": "not a CPU run: the reference has no CPU rasterizer, so its own CUDA kernels "
+                                   "are timed on this B200 (whole frame)"},
+        "e2e": {"value": r["value"], "unit": "Gtris/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    if args.sub_results and wl["name"] == DEFAULT_WORKLOAD:
+        import torch
+
+        subs = [ref_plain(args, sub_workload(wl, "planet_orbit_400m_1080p"), ref, ids=r["ids"])]
+        ref.reset()
+        del wl
+        torch.cuda.empty_cache()
+        for name in SUB_WORKLOADS[1:]:
+            sw = build_workload(name)
+            if sw.get("batched"):
+                b = run_reference_batched(args, sw, local, ref=ref)
+                subs.append({"workload": name, "desc": sw["desc"], "metric": "views/s", "value": b["value"],
+                             "unit": "views/s", "ms_per_step": b["ms_per_step"], "steps": b["steps"]})
+            else:
+                subs.append(ref_plain(args, sw, ref))
+            ref.reset()
+            del sw
+            torch.cuda.empty_cache()
+        for x in subs:
+            x.pop("ids", None)
+        line["sub_results"] = subs
+    return line
+
+
+def ref_plain(args, wl, ref, ids=None):
+    """The reference's own kernels (native build) on the plain frame of `wl`:
+    the mean device time of args.steps frames (clear + stages 1-3, then the
+    resolve), queues sized from the CPU oracle's exact counts with a margin
+    (the reference never checks its capacities)."""
+    import oracle_lib as ol
+
+    T, V, Tu = scene_counts(wl)
+    W, H = wl["W"], wl["H"]
+    if ids is None:
+        if wl.get("compressed"):  # the reference's *_compressed kernels
+            ids = [ref.mesh_compressed_host(cp.packed, cp.positions, cp.num_triangles, dec[2], cp.aabb_min,
+                                            cp.aabb_max, cp.index_min, cp.index_max)
+                   for cp, dec in zip(wl["compressed"], wl["decoded"])]
+        elif wl["device"]:
+            ids = [ref.mesh_device(p.data_ptr(), p.shape[0], i.data_ptr(), i.shape[0], c.data_ptr())
+                   for (p, i, c) in wl["meshes"]]
+        else:
+            ids = [ref.mesh_host(p, i, c) for (p, i, c) in wl["meshes"]]
     mids = [ids[m] for m, _ in wl["instances"]]
     worlds = np.stack([np.asarray(w, np.float32).reshape(16) for _, w in wl["instances"]])
-    # The reference never checks its queue capacities: size them from the CPU
-    # oracle's exact counts for this frame, with a wide margin (the fast-math
-    # build decides a handful of edge triangles differently).
-    items = []
-    for m, w in wl["instances"]:
-        p, i, c = wl["decoded"][m] if wl.get("compressed") else host_mesh(wl["meshes"][m])
-        items.append((p, i, c, w))
+    meshes = wl["decoded"] if wl.get("compressed") else [host_mesh(m) for m in wl["meshes"]]
+    items = [(*meshes[m], w) for m, w in wl["instances"]]
     _, ost = ol.raster(ol.Frame(items, wl["view"]), W, H, wl["proj"][5], nthreads=os.cpu_count() or 1)
-    del items
+    del items, meshes
     cap_nt = min(T, 2 * int(ost.nontrivial) + (1 << 20))
     cap_huge = 2 * int(ost.huge_tiles) + (1 << 20)
     ref.frame(mids, worlds, wl["view"], wl["proj"], W, H, instanced=True, cap_nontrivial=cap_nt,
@@ -1209,44 +1460,24 @@ def run_reference(args, rank, world, local):
     _, _, _, ms, counts = ref.frame(mids, worlds, wl["view"], wl["proj"], W, H, instanced=True,
                                     cap_nontrivial=cap_nt, cap_huge=cap_huge, frames=args.steps, want_color=False)
     step_ms = float(ms[0] + ms[1])
-    v = T / (step_ms * 1e-3) / 1e9
-    return {
-        "impl": "reference",
-        "metric": "Gtris/s @1080p (plain 3-stage visbuffer + resolve, one frame per step)",
-        "value": v,
-        "unit": "Gtris/s",
-        "n_gpus": 1,
-        "steps": args.steps,
-        "warmup": args.warmup,
-        "ms_per_step": step_ms,
-        "higher_is_better": True,
-        "scaling": "weak",
-        "vs_baseline": None,
-        "dtype": "f32",
-        "data": "synthetic (seeded)",
-        "config": {"workload": wl["name"], "desc": wl["desc"], "triangles": T, "vertices": V, "width": W,
-                   "height": H, "parallelism": "single GPU", "stage_ms": {"clear+raster": float(ms[0]),
-                                                                          "resolve": float(ms[1])},
-                   "nontrivial": int(counts[0]), "huge_tiles": int(counts[1]),
-                   "build": "CuRast NVRTC recipe (--use_fast_math, LTO) for sm_100a"},
-        "cpu_baseline": {"kind": "reference", "value": v, "unit": "Gtris/s", "cores": 0,
-                         "sample": "not a CPU run: the reference has no CPU rasterizer, so its own CUDA kernels "
-                                   "are timed on this B200 (whole frame)"},
-        "e2e": {"value": v, "unit": "Gtris/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
+    return {"workload": wl["name"], "desc": wl["desc"], "metric": "Gtris/s", "value": T / (step_ms * 1e-3) / 1e9,
+            "unit": "Gtris/s", "ms_per_step": step_ms, "steps": args.steps, "triangles": T, "vertices": V,
+            "stage_ms": {"clear+raster": float(ms[0]), "resolve": float(ms[1])},
+            "nontrivial": int(counts[0]), "huge_tiles": int(counts[1]), "ids": ids}
 
 
-def run_reference_batched(args, wl, local):
+def run_reference_batched(args, wl, local, ref=None):
     """The reference renders one view per CuRast::draw: its own kernels run
     once per view (same cameras, resolutions and mesh); a step is all views."""
     import oracle_lib as ol
 
     T, V, Tu = scene_counts(wl)
     cams = wl["cams"]
-    try:
-        ref = ol.Reference("native", device=local)
-    except Exception as e:  # noqa: BLE001
-        return {"impl": "reference", "unavailable": f"reference kernels not loadable: {e}"}
+    if ref is None:
+        try:
+            ref = ol.Reference("native", device=local)
+        except Exception as e:  # noqa: BLE001
+            return {"impl": "reference", "unavailable": f"reference kernels not loadable: {e}"}
     p, i, c = wl["meshes"][0]
     mid = ref.mesh_device(p.data_ptr(), p.shape[0], i.data_ptr(), i.shape[0], c.data_ptr())
     hp, hi, hc = host_mesh(wl["meshes"][0])
@@ -1331,13 +1562,15 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="planet_400m_1080p",
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD,
                     help="planet_400m_1080p (the 400M-triangle dense mesh), planet_<N>m_1080p, heightfield_1m_1080p, "
                          "instanced_<K>x<N>m_1080p, batched_<V>v_<N>m (V cameras over an N-million-triangle "
                          "terrain), served_<R>rps, post_2160p_ss2 (EDL + SSAO + supersampled resolve), glb_<N>m "
                          "(binary glTF ingest of N one-million-triangle primitives)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-parity", action="store_true", help="skip the oracle check of the last frame")
+    ap.add_argument("--no-sub-results", dest="sub_results", action="store_false",
+                    help="the default workload's line omits the other configurations")
     ap.add_argument("--ooc-nodes", type=int, default=247, help="out-of-core scene: nodes per side (served_*)")
     ap.add_argument("--serve-seconds", type=float, default=4.0, help="paced serving run length (served_*)")
     ap.add_argument("--capacity-requests", type=int, default=512, help="requests of the capacity run (served_*)")

@@ -237,6 +237,7 @@ cr_status assemble(cr_context* ctx, const cr_instance* instances, uint32_t count
         ci.outBase = A.outBytes;
         ci.vchunkBase = A.numVChunks;
         ci.chunkBoxes = m.chunkBoxes;
+        ci.id = A.order[r];  // the caller's list position: the MESH_ID display
         if (m.compressed) ci.codec = m.codec;
         A.outBytes += align_up(m.numVertices, 16);
         A.numVChunks += (m.numVertices + CR_VCHUNK - 1) / CR_VCHUNK;
@@ -277,6 +278,18 @@ cr_status assemble(cr_context* ctx, const cr_instance* instances, uint32_t count
     }
     A.totalTriangles = sum;
     A.numItems = items;
+    return CR_OK;
+}
+
+// The stage-1 survivor list of record-culled frames (grown like the queues).
+cr_status ensure_survivors(cr_context* ctx, uint64_t want) {
+    if (want <= ctx->s1Cap) return CR_OK;
+    ctx->dev_free(ctx->s1List, ctx->s1Cap * 8);
+    ctx->s1List = nullptr;
+    ctx->s1Cap = 0;
+    cr_status s = ctx->dev_alloc((void**)&ctx->s1List, want * 8, "stage-1 survivor list");
+    if (s) return s;
+    ctx->s1Cap = want;
     return CR_OK;
 }
 
@@ -450,6 +463,7 @@ void read_counters(cr_context* ctx) {
     ctx->last.overflow = c[CR_CTR_OVERFLOW];
     ctx->last.work_items_drawn = ctx->last.work_items ? c[CR_CTR_ITEMS] : 0;
     ctx->last.vertex_chunks_evaluated = ctx->last.vertex_chunks ? c[CR_CTR_CHUNKS] : 0;
+    ctx->last.stage1_survivors = c[CR_CTR_SURVIVORS];
 }
 
 cr_status run_frame(cr_context* ctx, uint32_t flags, cudaStream_t stream, uint64_t instances, uint64_t triangles,
@@ -500,6 +514,11 @@ cr_status run_frame(cr_context* ctx, uint32_t flags, cudaStream_t stream, uint64
         // the counters hold the exact demand of every queue that was fed in
         // full; re-issuing the frame is safe even without a clear, since every
         // fragment write is an atomic minimum (idempotent)
+        if (ctx->last.overflow & 4) {  // the survivor list: its counter holds the demand
+            const uint64_t sv = ctx->hCounters[CR_CTR_SURVIVORS];
+            s = ensure_survivors(ctx, std::max<uint64_t>(ctx->s1Cap, sv + sv / 8 + 1024));
+            if (s) return s;
+        }
         const uint64_t ntWant = std::max<uint64_t>(ctx->ntCap, ctx->last.nontrivial + ctx->last.nontrivial / 8 + 1024);
         const uint64_t huWant = (ctx->last.overflow & 1)
                                     ? ctx->hugeCap
@@ -605,6 +624,7 @@ cr_status cr_create(const cr_config* cfg, cr_context** out) {
     const uint64_t nt0 = c.max_nontrivial ? c.max_nontrivial : (1ull << 20);
     const uint64_t hu0 = c.max_huge ? c.max_huge : (1ull << 20);
     s = ensure_queues(ctx, nt0, hu0);
+    if (!s) s = ensure_survivors(ctx, 1ull << 22);
     if (s) {
         cr_destroy(ctx);
         return s;
@@ -631,6 +651,7 @@ cr_status cr_destroy(cr_context* ctx) {
     if (ctx->itemList) cudaFree(ctx->itemList);
     if (ctx->outcodes) cudaFree(ctx->outcodes);
     if (ctx->ntList) cudaFree(ctx->ntList);
+    if (ctx->s1List) cudaFree(ctx->s1List);
     if (ctx->hugeList) cudaFree(ctx->hugeList);
     if (ctx->counters) cudaFree(ctx->counters);
     if (ctx->dFrame) cudaFree(ctx->dFrame);
@@ -1060,10 +1081,11 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
                         : rec == CR_CULL_OUTCODES ? CR_REC_OUTCODES
                         : rec == CR_CULL_BOXES    ? CR_REC_BOXES
                         : instanced               ? CR_REC_BOXES
-                        : count > 1               ? CR_REC_CELLS
-                                                  : CR_REC_OUTCODES;
+                                                  : CR_REC_CELLS;
     if (cellMode == CR_REC_CELLS && (cam->width > 65535 || cam->height > 65535))
         cellMode = CR_REC_OUTCODES;  // cells hold 16-bit coordinates
+    else if (cellMode == CR_REC_CELLS && cam->width <= 4096 && cam->height <= 4096)
+        cellMode = CR_REC_CELLS32;  // 12-bit coordinates fit: half the record bytes
     const bool direct = cellMode == CR_REC_BOXES;
     if (direct && !(flags & kRenderResolveOnly))
         for (uint32_t i = 0; i < count; i++) {
@@ -1092,7 +1114,7 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
     CR_CUDA(cudaStreamWaitEvent(stream, ctx->frameDone, 0), "stream wait");
     const uint64_t numPixels = (uint64_t)cam->width * (uint64_t)cam->height;
 
-    s = ensure_records(ctx, direct ? 0 : A.outBytes * (cellMode == CR_REC_CELLS ? 8 : 1));
+    s = ensure_records(ctx, direct ? 0 : A.outBytes * (cellMode == CR_REC_CELLS ? 8 : cellMode == CR_REC_CELLS32 ? 4 : 1));
     if (s) return s;
     if (A.numItems > ctx->itemCap || A.numVChunks > ctx->chunkCap) {
         // item-cull survivors (at most every item) and one class per chunk
@@ -1102,13 +1124,14 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
         ctx->itemCap = ctx->chunkCap = ctx->itemBytes = 0;
         const uint64_t items = A.numItems + A.numItems / 8 + 1024;
         const uint64_t chunks = A.numVChunks + A.numVChunks / 8 + 1024;
-        const size_t bytes = align_up(items * 8, 256) + align_up(chunks * 4, 256);
+        const size_t bytes = align_up(items * 8, 256) + align_up(chunks * 4, 256) + align_up(chunks, 256);
         s = ctx->dev_alloc((void**)&ctx->itemList, bytes, "cull buffers");
         if (s) return s;
         ctx->itemCap = items;
         ctx->chunkCap = chunks;
         ctx->itemBytes = bytes;
         ctx->chunkList = (uint32_t*)((char*)ctx->itemList + align_up(items * 8, 256));
+        ctx->chunkClass = (uint8_t*)ctx->chunkList + align_up(chunks * 4, 256);
     }
     CrFrameParams fp{};
     CrResolveParams rp{};
@@ -1124,8 +1147,10 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
     fp.itemList = ctx->itemList;
     fp.itemCap = ctx->itemCap;
     fp.chunkList = ctx->chunkList;
+    fp.chunkClass = ctx->chunkClass;
     if (direct) {  // no vertex pass: no chunks to classify or evaluate
         fp.chunkList = nullptr;
+        fp.chunkClass = nullptr;
         fp.numVChunks = 0;
     }
     fp.fb = (uint64_t*)d_visbuffer;
@@ -1153,6 +1178,9 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
     rp.p00 = cam->proj[0];
     rp.p11 = cam->proj[5];
     rp.background = 0xffffffffu;  // HostDeviceInterface.h:37 BACKGROUND_COLOR
+    memcpy(rp.view, cam->view, 64);
+    rp.thrSmall = ctx->cfg.threshold_small;
+    rp.thrLarge = ctx->cfg.threshold_large;
     rp.idLo = resolveIdLo;
     rp.idHi = resolveIdHi;
     rp.writeBackground = resolveIdLo == 0 ? 1u : 0u;
@@ -1162,6 +1190,8 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
         fp.ntCap = ctx->ntCap;
         fp.hugeList = ctx->hugeList;
         fp.hugeCap = ctx->hugeCap;
+        fp.s1List = ctx->s1List;
+        fp.s1Cap = ctx->s1Cap;
         auto mark = [&](int i) -> cudaError_t { return tev ? cudaEventRecord(tev[i], stream) : cudaSuccess; };
         CR_CUDA(mark(0), "event");
         const bool raster = !(flags & kRenderResolveOnly);

@@ -122,6 +122,7 @@ void build_views(const cr_instance* instances, const Assembled& A, const cr_view
         cv.aspect = (float)cam.width / (float)cam.height;
         cv.fa = cv.f / cv.aspect;  // the kernels' target_of(p): p.f / p.aspect
         mat4_inverse(cam.view, cv.viewI);
+        memcpy(cv.view, cam.view, 64);
         for (int k = 0; k < 3; k++)  // viewI * (0,0,0,1)
             cv.origin[k] = (cv.viewI[0 + k] * 0.0f + cv.viewI[4 + k] * 0.0f) + (cv.viewI[8 + k] * 0.0f + cv.viewI[12 + k] * 1.0f);
         cv.p00 = cam.proj[0];
@@ -174,6 +175,8 @@ void base_params(const cr_context* ctx, int32_t display, CrFrameParams& fp, CrRe
     fp.debugFlags = ctx->cfg.debug_flags;
     rp.display = display;
     rp.background = 0xffffffffu;  // HostDeviceInterface.h:37 BACKGROUND_COLOR
+    rp.thrSmall = ctx->cfg.threshold_small;
+    rp.thrLarge = ctx->cfg.threshold_large;
     rp.writeBackground = 1u;
     rp.idLo = 0ull;
     rp.idHi = ~0ull;

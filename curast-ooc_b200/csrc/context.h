@@ -126,11 +126,14 @@ struct cr_context {
     uint64_t outCap = 0;
     uint64_t* ntList = nullptr;
     uint64_t ntCap = 0;
-    uint2* itemList = nullptr;    // item-cull survivors, then the chunk list
+    uint2* itemList = nullptr;    // item-cull survivors, then the chunk list and classes
     uint64_t itemCap = 0;
     uint32_t* chunkList = nullptr;
+    uint8_t* chunkClass = nullptr;
     uint64_t chunkCap = 0;
     size_t itemBytes = 0;
+    uint64_t* s1List = nullptr;   // stage-1 survivors of record-culled frames
+    uint64_t s1Cap = 0;
     CrTile* hugeList = nullptr;
     uint64_t hugeCap = 0;
     unsigned long long* counters = nullptr;
@@ -219,11 +222,14 @@ struct BatchScratch {
     size_t recordCap = 0;
     uint64_t* ntList = nullptr;
     uint64_t ntCap = 0;
-    uint2* itemList = nullptr;    // item-cull survivors, then the chunk list
+    uint2* itemList = nullptr;    // item-cull survivors, then the chunk list and classes
     uint64_t itemCap = 0;
     uint32_t* chunkList = nullptr;
+    uint8_t* chunkClass = nullptr;
     uint64_t chunkCap = 0;
     size_t itemBytes = 0;
+    uint64_t* s1List = nullptr;   // stage-1 survivors of record-culled frames
+    uint64_t s1Cap = 0;
     CrTile* hugeList = nullptr;
     uint64_t hugeCap = 0;
     unsigned long long* counters = nullptr;

@@ -32,10 +32,13 @@
 // counters[] slots
 #define CR_CTR_NONTRIVIAL 0     // entries appended to the stage-2 queue
 #define CR_CTR_HUGE 1           // tiles appended to the stage-3 queue
-#define CR_CTR_OVERFLOW 2       // bit 0: stage-2 queue, bit 1: stage-3 queue
+#define CR_CTR_OVERFLOW 2       // bit 0: stage-2 queue, bit 1: stage-3 queue,
+                                // bit 2: stage-1 survivor list
 #define CR_CTR_TIMEOUT 3        // nonzero if a bounded device wait gave up
 #define CR_CTR_ITEMS 4          // stage-1 work items that survive the item cull
 #define CR_CTR_CHUNKS 5         // vertex-pass chunks that need per-vertex records
+#define CR_CTR_SURVIVORS 6      // stage-1 triangles the records do not cull
+                                // (appended by k_s1cull for k_s1raster)
 #define CR_CTR_COUNT 8
 
 // Compressed geometry (the reference's IX_PU16 meshes, CMesh fields
@@ -62,7 +65,8 @@ struct alignas(16) CrInstance {
     uint64_t outBase;           // first outcode byte of this instance
     uint64_t vchunkBase;        // first vertex-pass chunk of this instance
     const float* chunkBoxes;    // per CR_VCHUNK vertices: min xyz, max xyz (or nullptr)
-    uint64_t pad1;
+    uint32_t id;                // the instance's place in the caller's list (MESH_ID display)
+    uint32_t pad1;
     CrCodec codec;              // compressed meshes: positions are uint16 xyz
 };
 
@@ -141,8 +145,9 @@ struct alignas(16) CrView {
     float fa;                   // f / aspect, rounded once in float
     uint32_t resolveBlockBase;  // first block of this view in the resolve grid
     uint32_t pad;
+    float view[16];             // the view matrix (the STAGE display)
 };
-static_assert(sizeof(CrView) == 144, "CrView layout");
+static_assert(sizeof(CrView) == 208, "CrView layout");
 
 // Multi-view vertex record (48 bytes, read as three 16-byte loads): per
 // frustum predicate of vertex_outcode one bit per view.  BEHIND bits are
@@ -213,13 +218,25 @@ struct CrFrameParams {
     CrItemViews* itemViews;
     CrViewMasks* chunkMasks;
     uint8_t* chunkUniform;
+    // record-culled single-view frames: per vertex-pass chunk the frame
+    // cull's class (CR_CHUNK_EVAL: the vertex pass writes its records; else
+    // the record every vertex of the chunk has); nullptr: every chunk has
+    // per-vertex records
+    uint8_t* chunkClass;
+    // stage-1 triangles the records do not cull, (instance << 32) | triangle,
+    // counted in counters[CR_CTR_SURVIVORS], at most s1Cap
+    uint64_t* s1List;
+    uint64_t s1Cap;
 };
+#define CR_CHUNK_EVAL 0xffu
 
 // CrFrameParams::cellMode
 #define CR_REC_OUTCODES 0u      // the vertex pass writes 1-byte outcodes
 #define CR_REC_CELLS 1u         // the vertex pass writes 8-byte cell records
 #define CR_REC_BOXES 2u         // no vertex pass: item and sub-box proofs of the
                                 // sample-miss cull, survivors evaluated directly
+#define CR_REC_CELLS32 3u       // the vertex pass writes 4-byte cell records
+                                // (vertex_cell32: W and H at most 4096)
 
 struct CrResolveParams {
     const CrInstance* instances;
@@ -236,6 +253,8 @@ struct CrResolveParams {
     uint32_t background;
     uint32_t writeBackground;   // 1: empty pixels get the background
     uint64_t idLo, idHi;        // covered pixels are written only for ids in [idLo, idHi)
+    float view[16];             // the view matrix (STAGE display)
+    uint32_t thrSmall, thrLarge;  // the stage thresholds (STAGE display)
 };
 
 // Post-processing of the colorbuffer (post.cu): the reference's EDL, SSAO and
@@ -263,9 +282,11 @@ int cr_launch_post(const CrPostParams& p, void* stream);
 struct CrLaunchShape {
     int numSMs;
     int vertexBlocks;
-    int stage1Blocks;
+    int stage1Blocks;           // k_stage1 (box-culled frames)
     int stage2Blocks;
     int stage3Blocks;
+    int s1CullBlocks;           // k_s1cull (record-culled frames)
+    int s1RasterBlocks;         // k_s1raster
 };
 
 int cr_query_launch_shape(int device, CrLaunchShape* out);

@@ -22,7 +22,7 @@
 #include "cr_device.h"
 #include "curast_b200.h"
 
-// The only scratch this entry point uses (CR_NOALLOC_SCRATCH_BYTES, ~12 MiB);
+// The only scratch this entry point uses (CR_NOALLOC_SCRATCH_BYTES, ~28 MiB);
 // every GPU that loads the library holds it until the process exits.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[CR_NOALLOC_SCRATCH_BYTES];
 
@@ -32,12 +32,17 @@ namespace {
 constexpr size_t kOffCounters = 0;
 constexpr size_t kOffFrame = 256;
 constexpr size_t kFrameBytes = 20u * 1024u - 256;
+// per-vertex records: 4-byte cell records (or 1-byte outcodes above 4096
+// pixels a side)
 constexpr size_t kOffOutcodes = kOffFrame + kFrameBytes;
-constexpr size_t kOffNontrivial = kOffOutcodes + CR_NOALLOC_MAX_VERTICES;
+constexpr size_t kOffNontrivial = kOffOutcodes + (size_t)CR_NOALLOC_MAX_VERTICES * 4;
 constexpr size_t kOffTiles = kOffNontrivial + (size_t)CR_NOALLOC_MAX_NONTRIVIAL * 8;
-constexpr size_t kEnd = kOffTiles + (size_t)CR_NOALLOC_MAX_TILES * sizeof(CrTile);
+constexpr size_t kOffSurvivors = kOffTiles + (size_t)CR_NOALLOC_MAX_TILES * sizeof(CrTile);
+constexpr size_t kEnd = kOffSurvivors + (size_t)CR_NOALLOC_MAX_SURVIVORS * 8;
 static_assert(kEnd <= CR_NOALLOC_SCRATCH_BYTES, "scratch layout exceeds the array");
-static_assert(kOffOutcodes % 256 == 0 && kOffNontrivial % 256 == 0 && kOffTiles % 256 == 0, "alignment");
+static_assert(kOffOutcodes % 256 == 0 && kOffNontrivial % 256 == 0 && kOffTiles % 256 == 0 &&
+                  kOffSurvivors % 256 == 0,
+              "alignment");
 
 // frame table of at most CR_NOALLOC_MAX_INSTANCES instances
 constexpr size_t kMaxI = CR_NOALLOC_MAX_INSTANCES;
@@ -154,6 +159,7 @@ cr_status render_on_device(int32_t device, const cr_noalloc_instance* instances,
         c.numVertices = in.num_vertices;
         c.outBase = outBase;
         c.vchunkBase = vchunks;
+        c.id = r;
         cr_mat4_mul(cam->view, in.world, wv + 16 * r);
         c.flip = cr_internal_det3(wv + 16 * r) < 0.0f ? 1u : 0u;
         memcpy(w + 16 * r, in.world, 64);
@@ -195,6 +201,9 @@ cr_status render_on_device(int32_t device, const cr_noalloc_instance* instances,
     fp.numItems = items;
     fp.numVChunks = vchunks;
     fp.outcodes = scratch + kOffOutcodes;
+    fp.cellMode = (cam->width <= 4096 && cam->height <= 4096) ? CR_REC_CELLS32 : CR_REC_OUTCODES;
+    fp.s1List = (uint64_t*)(scratch + kOffSurvivors);
+    fp.s1Cap = CR_NOALLOC_MAX_SURVIVORS;
     fp.fb = (uint64_t*)d_visbuffer;
     fp.W = cam->width;
     fp.H = cam->height;
@@ -226,6 +235,9 @@ cr_status render_on_device(int32_t device, const cr_noalloc_instance* instances,
     rp.p00 = cam->proj[0];
     rp.p11 = cam->proj[5];
     rp.background = 0xffffffffu;
+    memcpy(rp.view, cam->view, 64);
+    rp.thrSmall = 128;
+    rp.thrLarge = 4096;
     rp.writeBackground = 1u;
     rp.idLo = 0ull;
     rp.idHi = ~0ull;
@@ -245,7 +257,9 @@ cr_status render_on_device(int32_t device, const cr_noalloc_instance* instances,
     if (e != cudaSuccess) return fail(CR_ERR_CUDA, "cr_render_noalloc: %s", cudaGetErrorString(e));
     if (counters[CR_CTR_TIMEOUT]) return fail(CR_ERR_TIMEOUT, "cr_render_noalloc: a device-side wait timed out%s");
     if (counters[CR_CTR_OVERFLOW])
-        return fail(CR_ERR_QUEUE_OVERFLOW, "cr_render_noalloc: %squeues overflowed (stage 2: %lld entries, stage 3: %lld tiles)",
+        return fail(CR_ERR_QUEUE_OVERFLOW,
+                    "cr_render_noalloc: %squeues overflowed (stage 2: %lld entries, stage 3: %lld tiles, stage-1 "
+                    "survivors: see CR_NOALLOC_MAX_SURVIVORS)",
                     "", (long long)counters[CR_CTR_NONTRIVIAL], (long long)counters[CR_CTR_HUGE]);
     return CR_OK;
 }

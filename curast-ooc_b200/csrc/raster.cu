@@ -28,62 +28,135 @@
 
 namespace {
 
-#ifndef VX_UNROLL
-#define VX_UNROLL 4
+// The vertex pass: per listed chunk (CR_VCHUNK consecutive vertices of one
+// instance: the frame cull's CR_CHUNK_EVAL chunks, or every chunk) one block
+// writes each vertex's record -- the outcode byte or the cell record.  A
+// full chunk of a plain mesh whose positions are 16-byte aligned arrives in
+// shared memory as one 12 KB bulk copy (cp.async.bulk), issued VX_STAGES
+// chunks ahead of its use and signalled by an mbarrier (bounded wait), so
+// the pass streams positions instead of waiting on per-thread gathers; other
+// chunks (tails, compressed or unaligned meshes) are read directly.
+#ifndef VX_STAGES
+#define VX_STAGES 3
 #endif
+#ifndef VX_MIN_BLOCKS
+#define VX_MIN_BLOCKS 4
+#endif
+struct VxChunk {
+    const CrInstance* I;
+    uint32_t inst, v0, v1;
+    const float* src;  // bulk-copy source, or nullptr (direct reads)
+};
+
+__device__ __forceinline__ VxChunk vx_chunk(const CrFrameParams& p, uint64_t k) {
+    const uint64_t c = p.chunkList ? (uint64_t)__ldg(p.chunkList + k) : k;
+    uint32_t lo = 0, hi = p.numInstances - 1;  // instance holding chunk c
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (__ldg(&p.instances[mid].vchunkBase) <= c) lo = mid;
+        else hi = mid - 1;
+    }
+    VxChunk r;
+    r.I = p.instances + lo;
+    r.inst = lo;
+    r.v0 = (uint32_t)(c - __ldg(&r.I->vchunkBase)) * CR_VCHUNK;
+    r.v1 = min(r.v0 + (uint32_t)CR_VCHUNK, __ldg(&r.I->numVertices));
+    const float* pos = ldg_ptr(&r.I->positions);
+    const bool plain = (__ldg(&r.I->codec.bits) & CR_CODEC_IX_PU16) == 0u;
+    r.src = (plain && r.v1 - r.v0 == (uint32_t)CR_VCHUNK && ((uintptr_t)pos & 15u) == 0u) ? pos + 3ull * r.v0 : nullptr;
+    return r;
+}
+
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS) k_vertex(const CrFrameParams p) {
+__global__ void __launch_bounds__(THREADS, VX_MIN_BLOCKS) k_vertex(const CrFrameParams p) {
     pdl_enter();
+    constexpr int STAGES = VX_STAGES;
+    constexpr uint32_t BYTES = CR_VCHUNK * 12;
+    __shared__ __align__(128) float s_pos[STAGES][CR_VCHUNK * 3];
+    __shared__ __align__(8) uint64_t s_bar[STAGES];
     const float fa = p.f / p.aspect;
     const float Wf = (float)p.W, Hf = (float)p.H;
+    const float Wm1 = (float)(p.W - 1), Hm1 = (float)(p.H - 1);
     // the chunks the frame cull left for per-vertex records (or every chunk)
     const uint64_t nChunks = p.chunkList ? min((uint64_t)p.counters[CR_CTR_CHUNKS], p.numVChunks) : p.numVChunks;
-    for (uint64_t k = blockIdx.x; k < nChunks; k += gridDim.x) {
-        const uint64_t c = p.chunkList ? (uint64_t)__ldg(p.chunkList + k) : k;
-        uint32_t lo = 0, hi = p.numInstances - 1;  // instance holding chunk c
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi + 1) >> 1;
-            if (__ldg(&p.instances[mid].vchunkBase) <= c) lo = mid;
-            else hi = mid - 1;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) mbar_init(&s_bar[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    // `pending`: slots holding an issued, not yet consumed copy (every thread
+    // tracks it identically; thread 0 issues the copies)
+    uint32_t pending = 0, parity = 0;
+    for (int s = 0; s < STAGES; ++s) {
+        const uint64_t k = blockIdx.x + (uint64_t)s * gridDim.x;
+        if (k >= nChunks) break;
+        const VxChunk ch = vx_chunk(p, k);
+        if (ch.src) {
+            pending |= 1u << s;
+            if (threadIdx.x == 0) bulk_load(s_pos[s], ch.src, BYTES, &s_bar[s]);
         }
-        const CrInstance* I = p.instances + lo;
-        const uint32_t v0 = (uint32_t)(c - __ldg(&I->vchunkBase)) * CR_VCHUNK;
-        const uint32_t nV = __ldg(&I->numVertices);
-        const uint32_t v1 = min(v0 + (uint32_t)CR_VCHUNK, nV);
-        const GeomRef g = geom_of(I);
-        const Mat M = load_mat(p.world_view + 4ull * lo);
-        // each thread loads VX_UNROLL positions before transforming any:
-        // the pass is latency-bound on these gathers
-        constexpr int U = VX_UNROLL;
-        for (uint32_t v = v0 + threadIdx.x; v < v1; v += U * THREADS) {
-            V3 q[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-                if (v + u * THREADS < v1) q[u] = pos_of(g, v + u * THREADS);
-            if (p.cellMode == CR_REC_CELLS) {
-                uint64_t* out = reinterpret_cast<uint64_t*>(p.outcodes) + __ldg(&I->outBase);
-#pragma unroll
-                for (int u = 0; u < U; ++u)
-                    if (v + u * THREADS < v1)
-                        out[v + u * THREADS] = vertex_cell_record(M, q[u], fa, p.f, Wf, Hf, p.W, p.H);
+    }
+    uint32_t kk = 0;
+    for (uint64_t k = blockIdx.x; k < nChunks; k += gridDim.x, ++kk) {
+        const int slot = (int)(kk % STAGES);
+        const uint32_t bit = 1u << slot;
+        const VxChunk ch = vx_chunk(p, k);
+        if (ch.src) {
+            const bool ok = mbar_wait_bounded(&s_bar[slot], (parity & bit) ? 1u : 0u, p.waitTimeoutNs);
+            if (__syncthreads_or(!ok)) {  // record, stop the block, drain its copies below
+                if (threadIdx.x == 0) atomicOr(&p.counters[CR_CTR_TIMEOUT], 1ull);
+                break;
+            }
+            parity ^= bit;
+            pending &= ~bit;
+        }
+        const Mat M = load_mat(p.world_view + 4ull * ch.inst);
+        const GeomRef g = geom_of(ch.I);
+        const float* sp = s_pos[slot];
+        const uint64_t outBase = __ldg(&ch.I->outBase);
+        for (uint32_t v = ch.v0 + threadIdx.x; v < ch.v1; v += THREADS) {
+            V3 q;
+            if (ch.src) {
+                const uint32_t i = 3u * (v - ch.v0);  // stride-3 words: no bank conflicts
+                q = V3{sp[i], sp[i + 1], sp[i + 2]};
             } else {
-                uint8_t* out = p.outcodes + __ldg(&I->outBase);
-#pragma unroll
-                for (int u = 0; u < U; ++u)
-                    if (v + u * THREADS < v1) out[v + u * THREADS] = (uint8_t)vertex_outcode(M, q[u], fa, p.f);
+                q = pos_of(g, v);
+            }
+            if (p.cellMode == CR_REC_CELLS32)
+                reinterpret_cast<uint32_t*>(p.outcodes)[outBase + v] = vertex_cell32<true>(M, q, fa, p.f, Wf, Hf, Wm1, Hm1);
+            else if (p.cellMode == CR_REC_CELLS)
+                reinterpret_cast<uint64_t*>(p.outcodes)[outBase + v] = vertex_cell_record(M, q, fa, p.f, Wf, Hf, p.W, p.H);
+            else
+                p.outcodes[outBase + v] = (uint8_t)vertex_outcode(M, q, fa, p.f);
+        }
+        __syncthreads();  // every read of this slot is done: refill it
+        const uint64_t nk = k + (uint64_t)STAGES * gridDim.x;
+        if (nk < nChunks) {
+            const VxChunk nx = vx_chunk(p, nk);
+            if (nx.src) {
+                pending |= bit;
+                if (threadIdx.x == 0) {
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    bulk_load(s_pos[slot], nx.src, BYTES, &s_bar[slot]);
+                }
             }
         }
     }
+    // only after a timeout can copies still be in flight: wait for them
+    // (bounded) so none lands in shared memory after the block has exited
+    for (int s = 0; s < STAGES; ++s)
+        if (pending & (1u << s)) (void)mbar_wait_bounded(&s_bar[s], (parity >> s) & 1u, p.waitTimeoutNs);
 }
 
 // Frame cull, before the vertex pass; one thread per vertex-pass chunk, then
 // one per stage-1 work item.
 //   chunks  a chunk whose box proves CR_OC_* bits for every vertex
 //           (classify_chunk: exact "behind", a sound subset of the sides) gets
-//           those bits as its records here, without its positions being read;
-//           so does (with outcode records) a chunk wholly inside the frustum,
-//           whose every outcode is 0; the others are listed for the vertex
-//           pass.
+//           those bits as its class (chunkClass), the record all its vertices
+//           share, without its positions being read; so does (with outcode
+//           records) a chunk wholly inside the frustum, whose every outcode is
+//           0; the others get CR_CHUNK_EVAL and are listed for the vertex
+//           pass, which writes their per-vertex records.
 //   items   the item's box is classified for each instance of its chunk; an
 //           instance whose box is wholly behind or beyond one side has every
 //           triangle of the item culled by the reference's own tests
@@ -92,11 +165,11 @@ __global__ void __launch_bounds__(THREADS) k_vertex(const CrFrameParams p) {
 //           tv.cu:153-158).  Items with a surviving instance are appended
 //           (warp-aggregated) with the mask of those instances.
 // Skipping what the boxes prove cannot change the visbuffer.
-// A chunk class meaning "fill its records with 0" (wholly inside).
+// The class of a chunk whose every record is 0 (wholly inside).
 constexpr uint32_t CR_FILL_ZERO = 0x100u;
 
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS) k_cull(const CrFrameParams p) {
+__global__ void __launch_bounds__(THREADS, 3) k_cull(const CrFrameParams p) {
     pdl_enter();
     const int lane = threadIdx.x & 31;
     const float fa = p.f / p.aspect;
@@ -127,40 +200,9 @@ __global__ void __launch_bounds__(THREADS) k_cull(const CrFrameParams p) {
                 else if ((c & CH_INSIDE) && p.cellMode == CR_REC_OUTCODES) cls = CR_FILL_ZERO;
             }
         }
-        // classified chunks' records, written here by the whole warp (one
-        // chunk at a time, coalesced): their positions are never read
-        unsigned fillMask = __ballot_sync(FULL, cls != 0);
-        while (fillMask) {
-            const int j = __ffs(fillMask) - 1;
-            fillMask &= fillMask - 1;
-            const uint64_t gj = __shfl_sync(FULL, g, j);
-            const uint32_t cj = __shfl_sync(FULL, cls, j) & CR_OC_MASK;  // CR_FILL_ZERO fills 0
-            uint32_t lo = 0, hi = p.numInstances - 1;
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi + 1) >> 1;
-                if (__ldg(&p.instances[mid].vchunkBase) <= gj) lo = mid;
-                else hi = mid - 1;
-            }
-            const CrInstance* I = p.instances + lo;
-            const uint64_t cIdx = gj - __ldg(&I->vchunkBase);
-            const uint32_t nv = min((uint32_t)CR_VCHUNK, __ldg(&I->numVertices) - (uint32_t)cIdx * CR_VCHUNK);
-            const uint64_t v0 = __ldg(&I->outBase) + cIdx * CR_VCHUNK;
-            if (p.cellMode == CR_REC_CELLS) {  // 16-byte aligned: (outBase + k CR_VCHUNK) * 8
-                uint64_t* out = reinterpret_cast<uint64_t*>(p.outcodes) + v0;
-                for (uint32_t v = 2 * lane; v < nv; v += 64) {
-                    if (v + 1 < nv) *reinterpret_cast<ulonglong2*>(out + v) = make_ulonglong2(cj, cj);
-                    else out[v] = cj;
-                }
-            } else {  // 16-byte aligned: outBase and CR_VCHUNK are multiples of 16
-                uint8_t* out = p.outcodes + v0;
-                const uint32_t word = cj * 0x01010101u;
-                for (uint32_t v = 16 * lane; v < nv; v += 512) {
-                    if (v + 16 <= nv) *reinterpret_cast<uint4*>(out + v) = make_uint4(word, word, word, word);
-                    else
-                        for (uint32_t u = v; u < nv; ++u) out[u] = (uint8_t)cj;
-                }
-            }
-        }
+        // the chunk's class: the record every vertex of a classified chunk
+        // has (its positions are never read), or CR_CHUNK_EVAL
+        if (g < nChunks) p.chunkClass[g] = (uint8_t)(cls == 0 ? CR_CHUNK_EVAL : (cls & CR_OC_MASK));
         // chunks that need per-vertex records, listed for the vertex pass
         const bool eval = g < nChunks && cls == 0;
         const unsigned m = __ballot_sync(FULL, eval);
@@ -196,9 +238,17 @@ __global__ void __launch_bounds__(THREADS) k_cull(const CrFrameParams p) {
                     const uint32_t mc = __ldg(&p.instances[inst].meshClass);
                     if (mc & CR_OC_MASK) continue;
                     const Mat M = load_mat(p.world_view + 4ull * inst);
-                    if (!(mc & CR_MESH_INSIDE) && (classify_box(M, fa, p.f, blo, bhi) & CR_OC_MASK)) continue;
+                    bool inside = (mc & CR_MESH_INSIDE) != 0u;
+                    if (!inside) {
+                        const uint32_t c = classify_box(M, fa, p.f, blo, bhi);
+                        if (c & CR_OC_MASK) continue;
+                        inside = (c & CH_INSIDE) != 0u;
+                    }
                     if (samples && box_misses_samples(M, fa, p.f, p.W, p.H, invW, invH, blo, bhi)) continue;
-                    mask |= 1u << (inst - ib);
+                    // bit 16 + slot: every vertex of the item is in front of
+                    // the camera and inside every side (no chunk it touches
+                    // can have been classified culled)
+                    mask |= (1u << (inst - ib)) | (inside ? 1u << (16 + inst - ib) : 0u);
                 }
             }
         }
@@ -217,29 +267,56 @@ __global__ void __launch_bounds__(THREADS) k_cull(const CrFrameParams p) {
 }
 
 // Culls from the vertex pass's records (outcode bytes or cell records),
-// gathered per triangle corner.
-__device__ __forceinline__ void gather_culls(const CrFrameParams& p, uint32_t inst, const uint32_t (&ix)[S1_R][3],
-                                             const bool (&act)[S1_R], bool (&culledR)[S1_R]) {
-    if (p.cellMode == CR_REC_CELLS) {
-        const uint64_t* rec = reinterpret_cast<const uint64_t*>(p.outcodes) + __ldg(&p.instances[inst].outBase);
-        uint64_t o[S1_R][3];
+// gathered per triangle corner.  A corner whose vertex chunk the frame cull
+// classified from its box takes the chunk's class (the record every vertex
+// of the chunk has) instead of a per-vertex record, which was never written.
+// The class bytes of an item's corners sit in one or two cache lines, so
+// they are read first and the records gathered only where needed.
+template <typename Rec>
+__device__ __forceinline__ void gather_records(const CrFrameParams& p, const CrInstance* I, const uint32_t (&ix)[S1_R][3],
+                                               const bool (&act)[S1_R], Rec (&o)[S1_R][3]) {
+    const Rec* rec = reinterpret_cast<const Rec*>(p.outcodes) + __ldg(&I->outBase);
+    const uint8_t* cls = p.chunkClass ? p.chunkClass + __ldg(&I->vchunkBase) : nullptr;
 #pragma unroll
-        for (int r = 0; r < S1_R; ++r) {
-            o[r][0] = act[r] ? __ldg(rec + ix[r][0]) : 0ull;
-            o[r][1] = act[r] ? __ldg(rec + ix[r][1]) : 0ull;
-            o[r][2] = act[r] ? __ldg(rec + ix[r][2]) : 0ull;
+    for (int r = 0; r < S1_R; ++r)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const uint32_t c = (act[r] && cls) ? (uint32_t)__ldg(cls + (ix[r][k] / CR_VCHUNK)) : CR_CHUNK_EVAL;
+            o[r][k] = !act[r] ? (Rec)0 : c != CR_CHUNK_EVAL ? (Rec)c : __ldg(rec + ix[r][k]);
         }
+}
+
+// `inside`: the item's box is in front of the camera and inside every side
+// for this instance, so every corner's chunk has per-vertex records (cells)
+// or the outcode 0 (outcode records: nothing to cull from them).
+__device__ __forceinline__ void gather_culls(const CrFrameParams& p, uint32_t inst, const uint32_t (&ix)[S1_R][3],
+                                             const bool (&act)[S1_R], bool inside, bool (&culledR)[S1_R]) {
+    const CrInstance* I = p.instances + inst;
+    if (p.cellMode == CR_REC_CELLS32 && inside) {
+        const uint32_t* rec = reinterpret_cast<const uint32_t*>(p.outcodes) + __ldg(&I->outBase);
+        uint32_t o[S1_R][3];
+#pragma unroll
+        for (int r = 0; r < S1_R; ++r)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) o[r][k] = act[r] ? __ldg(rec + ix[r][k]) : 0u;
+#pragma unroll
+        for (int r = 0; r < S1_R; ++r) culledR[r] = cell32_culled(o[r][0], o[r][1], o[r][2]);
+    } else if (p.cellMode == CR_REC_OUTCODES && inside) {
+#pragma unroll
+        for (int r = 0; r < S1_R; ++r) culledR[r] = false;
+    } else if (p.cellMode == CR_REC_CELLS32) {
+        uint32_t o[S1_R][3];
+        gather_records(p, I, ix, act, o);
+#pragma unroll
+        for (int r = 0; r < S1_R; ++r) culledR[r] = cell32_culled(o[r][0], o[r][1], o[r][2]);
+    } else if (p.cellMode == CR_REC_CELLS) {
+        uint64_t o[S1_R][3];
+        gather_records(p, I, ix, act, o);
 #pragma unroll
         for (int r = 0; r < S1_R; ++r) culledR[r] = cell_culled(o[r][0], o[r][1], o[r][2]);
     } else {
-        const uint8_t* oc = p.outcodes + __ldg(&p.instances[inst].outBase);
-        uint32_t o[S1_R][3];
-#pragma unroll
-        for (int r = 0; r < S1_R; ++r) {
-            o[r][0] = act[r] ? __ldg(oc + ix[r][0]) : 0u;
-            o[r][1] = act[r] ? __ldg(oc + ix[r][1]) : 0u;
-            o[r][2] = act[r] ? __ldg(oc + ix[r][2]) : 0u;
-        }
+        uint8_t o[S1_R][3];
+        gather_records(p, I, ix, act, o);
         // all behind (tv.cu:119) or all beyond one side with none behind
         // (tv.cu:110-118)
 #pragma unroll
@@ -273,46 +350,260 @@ __device__ __forceinline__ TileSrc tile_source(const CrSegment* sg, uint32_t bat
     return TileSrc{nullptr, 0, false};
 }
 
-// A work item is CR_BATCH (128) consecutive triangles of one mesh x up to
-// CR_INST_CHUNK of its instances.  Per item a warp waits for the item's tile
-// (TMA ring, one 1D bulk copy per item issued STAGES items ahead), then per
-// instance decides which of its triangles can be culled without positions,
-// packs the others across the lanes and runs the reference's full
-// per-triangle path (stage1_triangle) on those.
-//   records (BOXES false)  the 1-byte outcodes or 8-byte cell records of the
-//                          vertex pass, gathered per triangle corner
-//   BOXES, vertex list     the item's distinct vertices (at most 256) get
-//                          cell records in shared memory per instance, the
-//                          same records the vertex pass would write; each
-//                          triangle reads its three from there
-//   BOXES, no list         sub-box proofs of the sample-miss cull, one per
-//                          (instance, 16 triangles), spread over the lanes
-// Nontrivial triangles are appended with one atomic per warp (ballot / popc).
-// a drain batch whose largest tiny raster has more fragments than this is
+// Warp-aggregated append of one stage-1 triangle per set lane to the
+// stage-2 queue (tv.cu:190-197).  All lanes of the warp call it.
+__device__ __forceinline__ void append_nontrivial(const CrFrameParams& p, bool queue, uint32_t inst, uint32_t tri) {
+    const int lane = threadIdx.x & 31;
+    const unsigned qmask = __ballot_sync(FULL, queue);
+    if (!qmask) return;
+    const int leader = __ffs(qmask) - 1;
+    unsigned long long b = 0;
+    if (lane == leader) b = atomicAdd(&p.counters[CR_CTR_NONTRIVIAL], (unsigned long long)__popc(qmask));
+    b = __shfl_sync(FULL, b, leader);
+    if (queue) {
+        const uint64_t q = b + __popc(qmask & ((1u << lane) - 1u));
+        if (q < p.ntCap) p.ntList[q] = ((uint64_t)inst << 32) | (uint64_t)tri;
+        else atomicOr(&p.counters[CR_CTR_OVERFLOW], 1ull);
+    }
+}
+
+// Record-culled frames, stage 1 in two kernels.
+//
+// k_s1cull: persistent warps over the work items (the frame cull's survivors,
+// or every item); a work item is CR_BATCH (128) consecutive triangles of one
+// mesh x up to CR_INST_CHUNK of its instances.  Its 1536-byte index tile
+// arrives by a 1D bulk copy (cp.async.bulk) in a per-warp shared-memory ring,
+// issued S1C_STAGES items ahead and signalled by an mbarrier (bounded wait).
+// Per live instance each lane gathers the records of its four triangles'
+// corners; a triangle no record culls is appended, with one atomic per
+// (warp, item, instance), to the survivor list as (instance << 32) | triangle.
+// The kernel holds no per-triangle raster state, so many warps fit on an SM
+// and keep the tiles and gathers of many items in flight.
+#ifndef S1C_STAGES
+#define S1C_STAGES 2
+#endif
+#ifndef S1C_MIN_BLOCKS
+#define S1C_MIN_BLOCKS 4
+#endif
+template <int WARPS, bool PACKED>
+__global__ void __launch_bounds__(WARPS * 32, S1C_MIN_BLOCKS) k_s1cull(const CrFrameParams p) {
+    pdl_enter();
+    constexpr int STAGES = S1C_STAGES;
+    __shared__ __align__(128) uint32_t s_idx[WARPS][STAGES][CR_BATCH * 3];
+    __shared__ __align__(8) uint64_t s_bar[WARPS][STAGES];
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    const uint64_t gw = (uint64_t)blockIdx.x * WARPS + w;
+    const uint64_t nw = (uint64_t)gridDim.x * WARPS;
+    if (lane == 0) {
+        for (int s = 0; s < STAGES; ++s) mbar_init(&s_bar[w][s], 1);
+        fence_barrier_init();
+    }
+    __syncwarp();
+    const uint64_t nItems = p.itemList ? min((uint64_t)p.counters[CR_CTR_ITEMS], p.itemCap) : p.numItems;
+    auto item_at = [&](uint64_t k) -> uint64_t { return p.itemList ? (uint64_t)__ldg(&p.itemList[k].x) : k; };
+    // `pending` marks ring slots holding an issued, not yet consumed tile
+    // copy; every lane tracks it identically, lane 0 issues the copies
+    uint32_t pending = 0;
+    for (int s = 0; s < STAGES; ++s) {
+        const uint64_t pk = gw + (uint64_t)s * nw;
+        if (pk >= nItems) break;
+        const Item it = decode_item(p, item_at(pk));
+        const TileSrc ts = tile_source<false>(p.segments + it.seg, it.batch, false);
+        if (ts.src) {
+            pending |= 1u << s;
+            // failure-detection test hook: the first copy is never issued, so
+            // its bounded wait must run out and report a timeout
+            const bool drop = (p.debugFlags & 1u) && gw == 0 && s == 0;
+            if (lane == 0 && !drop) bulk_load(s_idx[w][s], ts.src, ts.bytes, &s_bar[w][s]);
+        }
+    }
+    __syncwarp();
+    uint32_t parity = 0;
+    uint32_t k = 0;
+    for (uint64_t pk = gw; pk < nItems; pk += nw, ++k) {
+        const int slot = (int)(k % STAGES);
+        const uint32_t bit = 1u << slot;
+        // instance mask (bits 0..15) and wholly-inside mask (bits 16..31)
+        const uint32_t imask = p.itemList ? __ldg(&p.itemList[pk].y) : 0xffffu;
+        const Item it = decode_item(p, item_at(pk));
+        const CrSegment* sg = p.segments + it.seg;
+        const uint32_t numTri = __ldg(&sg->numTriangles);
+        const bool tma = item_uses_tma(sg, it.batch);
+        const uint32_t tri0 = it.batch * CR_BATCH;
+        if (tma) {
+            const bool ok =
+                __all_sync(FULL, mbar_wait_bounded(&s_bar[w][slot], (parity & bit) ? 1u : 0u, p.waitTimeoutNs));
+            if (!ok) {  // record, stop this warp, drain its copies below
+                if (lane == 0) atomicOr(&p.counters[CR_CTR_TIMEOUT], 1ull);
+                break;
+            }
+            parity ^= bit;
+            pending &= ~bit;
+        }
+        uint32_t ix[S1_R][3];
+        bool act[S1_R];
+        if (tma) {  // a full tile: every triangle of the item exists
+            const uint32_t* tile = s_idx[w][slot];
+#pragma unroll
+            for (int r = 0; r < S1_R; ++r) {
+                act[r] = true;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) ix[r][c] = tile[3 * (r * 32 + lane) + c];
+            }
+        } else {
+            const GeomRef geo = geom_of_t<PACKED>(sg);
+#pragma unroll
+            for (int r = 0; r < S1_R; ++r) {
+                const uint32_t pos = r * 32 + lane;
+                act[r] = tri0 + pos < numTri;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) ix[r][c] = act[r] ? geom_index(geo, 3ull * (tri0 + pos) + c) : 0u;
+            }
+        }
+        __syncwarp();
+        {  // every read of this slot is done: refill it with the item STAGES ahead
+            const uint64_t npk = pk + (uint64_t)STAGES * nw;
+            if (npk < nItems) {
+                const Item nt = decode_item(p, item_at(npk));
+                const TileSrc ns = tile_source<false>(p.segments + nt.seg, nt.batch, false);
+                if (ns.src) {
+                    pending |= bit;
+                    if (lane == 0) {
+                        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                        bulk_load(s_idx[w][slot], ns.src, ns.bytes, &s_bar[w][slot]);
+                    }
+                }
+            }
+        }
+        const uint32_t first = __ldg(&sg->firstInstance);
+        const uint32_t ib = first + it.chunk * CR_INST_CHUNK;
+        const uint32_t ie = min(ib + CR_INST_CHUNK, first + __ldg(&sg->instanceCount));
+        const uint32_t alive = imask & ((1u << (ie - ib)) - 1u);
+        for (uint32_t inst = ib; inst < ie; ++inst) {
+            if (!((alive >> (inst - ib)) & 1u)) continue;  // its box proved every triangle culled
+            bool culledR[S1_R];
+            gather_culls(p, inst, ix, act, ((imask >> (16 + inst - ib)) & 1u) != 0u, culledR);
+            unsigned m[S1_R];
+            uint32_t total = 0;
+#pragma unroll
+            for (int r = 0; r < S1_R; ++r) {
+                m[r] = __ballot_sync(FULL, act[r] && !culledR[r]);
+                total += __popc(m[r]);
+            }
+            if (total == 0) continue;
+            unsigned long long b = 0;
+            if (lane == 0) b = atomicAdd(&p.counters[CR_CTR_SURVIVORS], (unsigned long long)total);
+            b = __shfl_sync(FULL, b, 0);
+            const uint64_t hi = (uint64_t)inst << 32;
+#pragma unroll
+            for (int r = 0; r < S1_R; ++r) {
+                if ((m[r] >> lane) & 1u) {
+                    const uint64_t q = b + __popc(m[r] & ((1u << lane) - 1u));
+                    if (q < p.s1Cap) p.s1List[q] = hi | (uint64_t)(tri0 + r * 32 + lane);
+                    else atomicOr(&p.counters[CR_CTR_OVERFLOW], 4ull);
+                }
+                b += __popc(m[r]);
+            }
+        }
+    }
+    // only after a timeout can copies still be in flight: wait for them
+    // (bounded) so none lands in shared memory after the block has exited
+    for (int s = 0; s < STAGES; ++s)
+        if (pending & (1u << s)) (void)mbar_wait_bounded(&s_bar[w][s], (parity >> s) & 1u, p.waitTimeoutNs);
+}
+
+// a warp's tiny rasters whose largest has more fragments than this are
 // rasterized across the warp (stage1_coop_raster)
 #ifndef CR_COOP_MIN_FRAGMENTS
 #define CR_COOP_MIN_FRAGMENTS 8
 #endif
+
+// k_s1raster: persistent warps over the survivor list, one triangle per lane:
+// its indices and positions, then the reference's full per-triangle path
+// (stage1_triangle: transform, culls, the tiny raster or the stage-2 queue).
+// Survivors of one item are consecutive in the list, so a warp's gathers stay
+// within a few items.  COOP: frames of pixel-sized triangles spread the
+// lanes' tiny rasters over the warp.
+template <int WARPS, bool PACKED, bool COOP>
+__global__ void __launch_bounds__(WARPS * 32) k_s1raster(const CrFrameParams p) {
+    pdl_enter();
+    const int lane = threadIdx.x & 31;
+    const uint64_t gw = (uint64_t)blockIdx.x * WARPS + (threadIdx.x >> 5);
+    const uint64_t nw = (uint64_t)gridDim.x * WARPS;
+    const uint64_t n = min((uint64_t)p.counters[CR_CTR_SURVIVORS], p.s1Cap);
+    const Target tg = target_of(p);
+    const float fa = tg.fa;
+    for (uint64_t base = gw * 32; base < n; base += nw * 32) {
+        const uint64_t j = base + lane;
+        int res = S1_CULL;
+        uint32_t tri = 0, inst = 0;
+        S1Raster ras;
+        uint64_t rid = 0;
+        if (j < n) {
+            const uint64_t e = __ldg(p.s1List + j);
+            inst = (uint32_t)(e >> 32);
+            tri = (uint32_t)e;
+            const CrInstance* I = p.instances + inst;
+            const GeomRef g = geom_of_t<PACKED>(I);
+            const uint32_t i0 = geom_index(g, 3ull * tri + 0);
+            const uint32_t i1 = geom_index(g, 3ull * tri + 1);
+            const uint32_t i2 = geom_index(g, 3ull * tri + 2);
+            const V3 pa = pos_of(g, i0);
+            const V3 pb = pos_of(g, i1);
+            const V3 pc = pos_of(g, i2);
+            rid = __ldg(&I->cum) + tri;
+            res = stage1_triangle<COOP>(tg, fa, load_mat(p.world_view + 4ull * inst), __ldg(&I->flip), pa, pb, pc,
+                                        rid, &ras);
+        }
+        if constexpr (COOP) {
+            // the lanes' tiny rasters: spread over the warp when one of them
+            // would hold the others up, else each lane its own
+            const bool mine = res == S1_RASTER;
+            const int frags = mine ? max(ras.size_x, 0) * max(ras.size_y, 0) : 0;
+            if (__reduce_max_sync(FULL, (unsigned)frags) > CR_COOP_MIN_FRAGMENTS)
+                stage1_coop_raster(tg, mine, ras, rid);
+            else if (mine)
+                stage1_own_raster(tg, ras, rid);
+        }
+        append_nontrivial(p, res == S1_QUEUE, inst, tri);
+    }
+}
+
+// Box-culled frames (some mesh drawn more than once: no per-vertex records).
+// Persistent warps over the work items; per item a warp waits for the
+// item's vertex-list block (or its index tile) in the TMA ring, then per
+// instance decides which of its triangles can be culled without positions,
+// queues the others across the item's instances in a per-warp ring and runs
+// the reference's full per-triangle path (stage1_triangle) on them 32 at a
+// time.
+//   vertex list   the item's distinct vertices (at most 256) get cell
+//                 records in shared memory per instance, the same records
+//                 the vertex pass would write; each triangle reads its three
+//                 from there
+//   no list       sub-box proofs of the sample-miss cull, one per
+//                 (instance, 16 triangles), spread over the lanes
+// Nontrivial triangles are appended with one atomic per warp (ballot / popc).
 #ifndef CR_S1_BOXES_MIN_BLOCKS
 #define CR_S1_BOXES_MIN_BLOCKS 3
 #endif
 // PACKED: compiled for frames with compressed meshes (plain frames carry no
 // decoding code).
-template <int WARPS, bool BOXES, bool PACKED, bool COOP = false>
-__global__ void __launch_bounds__(WARPS * 32, BOXES ? CR_S1_BOXES_MIN_BLOCKS : 3) k_stage1(const CrFrameParams p) {
+template <int WARPS, bool PACKED>
+__global__ void __launch_bounds__(WARPS * 32, CR_S1_BOXES_MIN_BLOCKS) k_stage1(const CrFrameParams p) {
     pdl_enter();
-    constexpr int STAGES = BOXES ? 2 : S1_STAGES;
+    constexpr int STAGES = 2;
     static_assert(CR_LOCAL_BYTES <= CR_BATCH * 12, "a vertex-list block fits a ring slot");
     __shared__ __align__(128) uint32_t s_idx[WARPS][STAGES][CR_BATCH * 3];
     __shared__ __align__(8) uint64_t s_bar[WARPS][STAGES];
     __shared__ uint16_t s_ring[WARPS][S1_RING];
-    __shared__ __align__(16) uint32_t s_rec[BOXES ? WARPS : 1][BOXES ? CR_LOCAL_MAX : 1];
+    __shared__ __align__(16) uint32_t s_rec[WARPS][CR_LOCAL_MAX];
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
     const uint64_t gw = (uint64_t)blockIdx.x * WARPS + w;
     const uint64_t nw = (uint64_t)gridDim.x * WARPS;
     // shared-memory cell records hold 12-bit pixel cells
-    const bool lists = BOXES && p.W <= 4096 && p.H <= 4096;
+    const bool lists = p.W <= 4096 && p.H <= 4096;
 
     if (lane == 0) {
         for (int s = 0; s < STAGES; ++s) mbar_init(&s_bar[w][s], 1);
@@ -330,11 +621,9 @@ __global__ void __launch_bounds__(WARPS * 32, BOXES ? CR_S1_BOXES_MIN_BLOCKS : 3
         const uint64_t pk = gw + (uint64_t)s * nw;
         if (pk >= nItems) break;
         const Item it = decode_item(p, item_at(pk));
-        const TileSrc ts = tile_source<BOXES>(p.segments + it.seg, it.batch, lists);
+        const TileSrc ts = tile_source<true>(p.segments + it.seg, it.batch, lists);
         if (ts.src) {
             pending |= 1u << s;
-            // failure-detection test hook: the first copy is never issued, so
-            // its bounded wait must run out and report a timeout
             const bool drop = (p.debugFlags & 1u) && gw == 0 && s == 0;
             if (lane == 0 && !drop) bulk_load(s_idx[w][s], ts.src, ts.bytes, &s_bar[w][s]);
         }
@@ -355,9 +644,9 @@ __global__ void __launch_bounds__(WARPS * 32, BOXES ? CR_S1_BOXES_MIN_BLOCKS : 3
         const CrSegment* sg = p.segments + it.seg;
         const uint32_t numTri = __ldg(&sg->numTriangles);
         const GeomRef geo = geom_of_t<PACKED>(sg);
-        const TileSrc ts = tile_source<BOXES>(sg, it.batch, lists);
+        const TileSrc ts = tile_source<true>(sg, it.batch, lists);
         const bool tma = ts.src != nullptr;
-        const bool local = BOXES && ts.local;
+        const bool local = ts.local;
         const uint32_t tri0 = it.batch * CR_BATCH;
         if (tma) {
             const bool ok =
@@ -376,17 +665,9 @@ __global__ void __launch_bounds__(WARPS * 32, BOXES ? CR_S1_BOXES_MIN_BLOCKS : 3
             if (tma) return tile[3 * pos + c];
             return geom_index(geo, 3ull * (tri0 + pos) + c);
         };
-        uint32_t ix[S1_R][3];
         bool act[S1_R];
 #pragma unroll
-        for (int r = 0; r < S1_R; ++r) {
-            const uint32_t pos = r * 32 + lane;
-            act[r] = tri0 + pos < numTri;
-            if (BOXES) continue;  // box-culled frames gather no records by index
-            ix[r][0] = act[r] ? index_of(pos, 0) : 0;
-            ix[r][1] = act[r] ? index_of(pos, 1) : 0;
-            ix[r][2] = act[r] ? index_of(pos, 2) : 0;
-        }
+        for (int r = 0; r < S1_R; ++r) act[r] = tri0 + r * 32 + lane < numTri;
 
         const uint32_t first = __ldg(&sg->firstInstance);
         const uint32_t count = __ldg(&sg->instanceCount);
@@ -398,7 +679,7 @@ __global__ void __launch_bounds__(WARPS * 32, BOXES ? CR_S1_BOXES_MIN_BLOCKS : 3
         // bit 8 k + b of subw[k / 4] is set unless sub-box b of the k-th
         // surviving instance is proven to miss every sample
         uint32_t subw[4] = {~0u, ~0u, ~0u, ~0u};
-        if (BOXES && !local) {
+        if (!local) {
             const float* sbx = ldg_ptr(&sg->subBoxes);
             const int nsub = (int)min((uint32_t)(CR_BATCH / CR_SUB), (numTri - tri0 + CR_SUB - 1) / CR_SUB);
             const int pairs = __popc(alive) * (CR_BATCH / CR_SUB);
@@ -427,16 +708,12 @@ __global__ void __launch_bounds__(WARPS * 32, BOXES ? CR_S1_BOXES_MIN_BLOCKS : 3
         // and run through the reference's full path 32 at a time.
         uint16_t* ring = s_ring[w];
         uint32_t qh = 0, qt = 0;  // ring head / tail (warp-uniform)
-        // evaluates queued triangles 32 at a time (all: down to an empty
-        // ring); in record-culled frames the ring holds one instance's
-        // triangles, whose matrix, flip and first id the warp passes in
-        auto drain = [&](bool all, const Mat* Mu, uint32_t flipu, uint64_t cumu) {
+        // evaluates queued triangles 32 at a time (all: down to an empty ring)
+        auto drain = [&](bool all) {
             while (qt - qh >= 32u || (all && qt > qh)) {
                 const uint32_t j = qh + lane;
                 int res = S1_CULL;
                 uint32_t tri = 0, inst = 0;
-                S1Raster ras;
-                uint64_t rid = 0;
                 if (j < qt) {
                     const uint32_t e = ring[j & (S1_RING - 1)];
                     const uint32_t tp = e & 0xffu;
@@ -445,38 +722,12 @@ __global__ void __launch_bounds__(WARPS * 32, BOXES ? CR_S1_BOXES_MIN_BLOCKS : 3
                     const V3 pa = pos_of(geo, index_of(tp, 0));
                     const V3 pb = pos_of(geo, index_of(tp, 1));
                     const V3 pc = pos_of(geo, index_of(tp, 2));
-                    if (!BOXES) {
-                        rid = cumu + tri;
-                        res = stage1_triangle<COOP>(target_of(p), fa, *Mu, flipu, pa, pb, pc, rid, &ras);
-                    } else {
-                        res = stage1_triangle(target_of(p), fa, load_mat(p.world_view + 4ull * inst),
-                                              __ldg(&p.instances[inst].flip), pa, pb, pc,
-                                              __ldg(&p.instances[inst].cum) + tri);
-                    }
-                }
-                if constexpr (!BOXES && COOP) {
-                    // the lanes' tiny rasters: spread over the warp when one of
-                    // them would hold the others up, else each lane its own
-                    const bool mine = res == S1_RASTER;
-                    const int frags = mine ? max(ras.size_x, 0) * max(ras.size_y, 0) : 0;
-                    if (__reduce_max_sync(FULL, (unsigned)frags) > CR_COOP_MIN_FRAGMENTS)
-                        stage1_coop_raster(target_of(p), mine, ras, rid);
-                    else if (mine)
-                        stage1_own_raster(target_of(p), ras, rid);
+                    res = stage1_triangle(target_of(p), fa, load_mat(p.world_view + 4ull * inst),
+                                          __ldg(&p.instances[inst].flip), pa, pb, pc,
+                                          __ldg(&p.instances[inst].cum) + tri);
                 }
                 qh = min(qh + 32u, qt);
-                const unsigned qmask = __ballot_sync(FULL, res == S1_QUEUE);
-                if (qmask) {  // warp-aggregated append, tv.cu:190-197
-                    const int leader = __ffs(qmask) - 1;
-                    unsigned long long b = 0;
-                    if (lane == leader) b = atomicAdd(&p.counters[CR_CTR_NONTRIVIAL], (unsigned long long)__popc(qmask));
-                    b = __shfl_sync(FULL, b, leader);
-                    if (res == S1_QUEUE) {
-                        const uint64_t q = b + __popc(qmask & ((1u << lane) - 1u));
-                        if (q < p.ntCap) p.ntList[q] = ((uint64_t)inst << 32) | (uint64_t)tri;
-                        else atomicOr(&p.counters[CR_CTR_OVERFLOW], 1ull);
-                    }
-                }
+                append_nontrivial(p, res == S1_QUEUE, inst, tri);
                 __syncwarp();
             }
         };
@@ -485,9 +736,7 @@ __global__ void __launch_bounds__(WARPS * 32, BOXES ? CR_S1_BOXES_MIN_BLOCKS : 3
             if (!((alive >> (inst - ib)) & 1u)) continue;  // its box proved every triangle culled
             const int kk = rank++;
             bool culledR[S1_R];
-            if constexpr (!BOXES) {
-                gather_culls(p, inst, ix, act, culledR);
-            } else if (local) {
+            if (local) {
                 // cell records of the item's distinct vertices for this
                 // instance; an instance whose mesh box is inside the frustum
                 // has the outcode 0 at every vertex
@@ -531,21 +780,15 @@ __global__ void __launch_bounds__(WARPS * 32, BOXES ? CR_S1_BOXES_MIN_BLOCKS : 3
                 qt += __popc(m);
             }
             __syncwarp();
-            if constexpr (BOXES) {
-                drain(false, nullptr, 0u, 0ull);
-            } else {
-                if (qt == qh) continue;
-                const Mat M = load_mat(p.world_view + 4ull * inst);
-                drain(true, &M, __ldg(&p.instances[inst].flip), __ldg(&p.instances[inst].cum));
-            }
+            drain(false);
         }
-        if constexpr (BOXES) drain(true, nullptr, 0u, 0ull);
+        drain(true);
         __syncwarp();
         {  // every read of this slot is done: refill it with the item STAGES ahead
             const uint64_t npk = pk + (uint64_t)STAGES * nw;
             if (npk < nItems) {
                 const Item nt = decode_item(p, item_at(npk));
-                const TileSrc ns = tile_source<BOXES>(p.segments + nt.seg, nt.batch, lists);
+                const TileSrc ns = tile_source<true>(p.segments + nt.seg, nt.batch, lists);
                 if (ns.src) {
                     pending |= bit;
                     if (lane == 0) {
@@ -588,8 +831,12 @@ constexpr int VX_THREADS = 256;
 int cr_query_launch_shape(int device, CrLaunchShape* out) {
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return -1;
-    int b1 = 0, b2 = 0, b3 = 0, bv = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_stage1<S1_WARPS, false, false>, S1_WARPS * 32, 0) !=
+    int b1 = 0, b2 = 0, b3 = 0, bv = 0, bc = 0, br = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_stage1<S1_WARPS, false>, S1_WARPS * 32, 0) != cudaSuccess)
+        return -1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bc, k_s1cull<S1_WARPS, false>, S1_WARPS * 32, 0) != cudaSuccess)
+        return -1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&br, k_s1raster<S1_WARPS, false, true>, S1_WARPS * 32, 0) !=
         cudaSuccess)
         return -1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bv, k_vertex<VX_THREADS>, VX_THREADS, 0) != cudaSuccess)
@@ -601,6 +848,8 @@ int cr_query_launch_shape(int device, CrLaunchShape* out) {
         return -1;
     out->numSMs = sms;
     out->stage1Blocks = sms * (b1 > 0 ? b1 : 1);
+    out->s1CullBlocks = sms * (bc > 0 ? bc : 1);
+    out->s1RasterBlocks = sms * (br > 0 ? br : 1);
     out->stage2Blocks = sms * (b2 > 0 ? b2 : 1);
     out->stage3Blocks = sms * (b3 > 0 ? b3 : 1);
     return 0;
@@ -648,20 +897,27 @@ int cr_launch_cull(const CrFrameParams& p, const CrLaunchShape& s, void* stream)
     return launch_pdl(k_cull<256>, (unsigned)blocks, 256, stream, p);
 }
 
+// Box-culled frames: k_stage1.  Record-culled frames: k_s1cull (items ->
+// survivor list) then k_s1raster (survivors -> visbuffer / stage-2 queue).
 int cr_launch_stage1(const CrFrameParams& p, const CrLaunchShape& s, void* stream) {
     if (p.numItems == 0) return 0;
-    uint64_t warps = p.numItems;
-    uint64_t blocks = (warps + S1_WARPS - 1) / S1_WARPS;
-    if (blocks > (uint64_t)s.stage1Blocks) blocks = (uint64_t)s.stage1Blocks;
-    const unsigned b = (unsigned)blocks;
-    if (p.cellMode == CR_REC_BOXES)
-        return p.anyPacked ? launch_pdl(k_stage1<S1_WARPS, true, true>, b, S1_WARPS * 32, stream, p)
-                           : launch_pdl(k_stage1<S1_WARPS, true, false>, b, S1_WARPS * 32, stream, p);
+    const uint64_t itemBlocks = (p.numItems + S1_WARPS - 1) / S1_WARPS;
+    const unsigned T = S1_WARPS * 32;
+    if (p.cellMode == CR_REC_BOXES) {
+        const unsigned b = (unsigned)std::min<uint64_t>(itemBlocks, (uint64_t)s.stage1Blocks);
+        return p.anyPacked ? launch_pdl(k_stage1<S1_WARPS, true>, b, T, stream, p)
+                           : launch_pdl(k_stage1<S1_WARPS, false>, b, T, stream, p);
+    }
+    const unsigned bc = (unsigned)std::min<uint64_t>(itemBlocks, (uint64_t)s.s1CullBlocks);
+    if (p.anyPacked ? launch_pdl(k_s1cull<S1_WARPS, true>, bc, T, stream, p)
+                    : launch_pdl(k_s1cull<S1_WARPS, false>, bc, T, stream, p))
+        return -1;
+    const unsigned br = (unsigned)s.s1RasterBlocks;
     if (p.coopRaster)
-        return p.anyPacked ? launch_pdl(k_stage1<S1_WARPS, false, true, true>, b, S1_WARPS * 32, stream, p)
-                           : launch_pdl(k_stage1<S1_WARPS, false, false, true>, b, S1_WARPS * 32, stream, p);
-    return p.anyPacked ? launch_pdl(k_stage1<S1_WARPS, false, true>, b, S1_WARPS * 32, stream, p)
-                       : launch_pdl(k_stage1<S1_WARPS, false, false>, b, S1_WARPS * 32, stream, p);
+        return p.anyPacked ? launch_pdl(k_s1raster<S1_WARPS, true, true>, br, T, stream, p)
+                           : launch_pdl(k_s1raster<S1_WARPS, false, true>, br, T, stream, p);
+    return p.anyPacked ? launch_pdl(k_s1raster<S1_WARPS, true, false>, br, T, stream, p)
+                       : launch_pdl(k_s1raster<S1_WARPS, false, false>, br, T, stream, p);
 }
 
 int cr_launch_stage2(const CrFrameParams& p, const CrLaunchShape& s, void* stream) {

@@ -1053,9 +1053,20 @@ __device__ __forceinline__ void s2_row_span(const S2Span& P, float py, float asy
 
 // MULTI: entries carry their view (batched frames); otherwise view 0 is the
 // frame's single target.
+// One queued triangle's fragment-loop inputs, set up by its own lane and
+// read by the whole warp from shared memory (a broadcast).
+struct S2Tri {
+    S2Span sp;
+    uint64_t* fb;
+    float asx, asy, abx, aby, acx, acy, inv_det, iza, izb, izc, start_x, start_y;
+    int size_x, size_y, W, numPixels;
+    uint32_t id32;
+};
+
 template <int WARPS, bool MULTI>
 __global__ void __launch_bounds__(WARPS * 32) k_stage2(const CrFrameParams p) {
     pdl_enter();
+    __shared__ S2Tri s_tri[WARPS][32];
     const int lane = threadIdx.x & 31;
     const uint64_t gw = (uint64_t)blockIdx.x * WARPS + (threadIdx.x >> 5);
     const uint64_t nw = (uint64_t)gridDim.x * WARPS;
@@ -1125,37 +1136,53 @@ __global__ void __launch_bounds__(WARPS * 32) k_stage2(const CrFrameParams p) {
         }
 
         // ---- fragments: tv.cu:516-561, lanes stride each triangle ---------
+        // Each lane sets up its own triangle's row narrowing (s2_span_setup)
+        // and parks everything the fragment loop needs in shared memory; the
+        // warp then rasterizes the triangles one by one, reading them there.
+        S2Tri* const tris = s_tri[threadIdx.x >> 5];
+        if (kind == S2_RASTER) {
+            S2Tri& o = tris[lane];
+            o.start_x = floorf(su.min_x);
+            o.start_y = floorf(su.min_y);
+            o.size_x = su.size_x;
+            o.size_y = su.numFragments / su.size_x;
+            o.sp = s2_span_setup(o.start_x, o.start_y, o.size_x, o.size_y, su.asx, su.asy, su.abx, su.aby, su.acx,
+                                 su.acy, su.inv_det);
+            o.fb = MULTI ? tg.fb : p.fb;
+            o.asx = su.asx;
+            o.asy = su.asy;
+            o.abx = su.abx;
+            o.aby = su.aby;
+            o.acx = su.acx;
+            o.acy = su.acy;
+            o.inv_det = su.inv_det;
+            o.iza = su.iza;
+            o.izb = su.izb;
+            o.izc = su.izc;
+            o.W = MULTI ? tg.W : p.W;
+            o.numPixels = MULTI ? tg.W * tg.H : p.W * p.H;
+            o.id32 = su.id32;
+        }
+        __syncwarp();
         unsigned rmask = __ballot_sync(FULL, kind == S2_RASTER);
         while (rmask) {
             const int j = __ffs(rmask) - 1;
             rmask &= rmask - 1;
-            const float min_x = __shfl_sync(FULL, su.min_x, j);
-            const float min_y = __shfl_sync(FULL, su.min_y, j);
-            const float asx = __shfl_sync(FULL, su.asx, j);
-            const float asy = __shfl_sync(FULL, su.asy, j);
-            const float abx = __shfl_sync(FULL, su.abx, j);
-            const float aby = __shfl_sync(FULL, su.aby, j);
-            const float acx = __shfl_sync(FULL, su.acx, j);
-            const float acy = __shfl_sync(FULL, su.acy, j);
-            const float inv_det = __shfl_sync(FULL, su.inv_det, j);
-            const float iza = __shfl_sync(FULL, su.iza, j);
-            const float izb = __shfl_sync(FULL, su.izb, j);
-            const float izc = __shfl_sync(FULL, su.izc, j);
-            const int size_x = __shfl_sync(FULL, su.size_x, j);
-            const int nf = __shfl_sync(FULL, su.numFragments, j);
-            const uint64_t id = (uint64_t)__shfl_sync(FULL, su.id32, j);
-            uint64_t* const fbj = MULTI ? (uint64_t*)__shfl_sync(FULL, (unsigned long long)tg.fb, j) : p.fb;
-            const int Wj = MULTI ? __shfl_sync(FULL, tg.W, j) : p.W;
-            const int numPixels = Wj * (MULTI ? __shfl_sync(FULL, tg.H, j) : p.H);
-            const float start_x = floorf(min_x);
-            const float start_y = floorf(min_y);
-            const int size_y = nf / size_x;
+            const S2Tri& tr = tris[j];
+            const float asx = tr.asx, asy = tr.asy, abx = tr.abx, aby = tr.aby, acx = tr.acx, acy = tr.acy;
+            const float inv_det = tr.inv_det, iza = tr.iza, izb = tr.izb, izc = tr.izc;
+            const float start_x = tr.start_x, start_y = tr.start_y;
+            const int size_y = tr.size_y;
+            const uint64_t id = (uint64_t)tr.id32;
+            uint64_t* const fbj = tr.fb;
+            const int Wj = tr.W;
+            const int numPixels = tr.numPixels;
             // The reference tests every fragment of the bounding box.  Here each
             // row is first narrowed to the columns whose exact float test can
             // still pass (s2_row_span), the surviving spans of 32 rows are packed
             // across the lanes, and each fragment then runs the reference's
             // test unchanged -- so the same fragments are written.
-            const S2Span sp = s2_span_setup(start_x, start_y, size_x, size_y, asx, asy, abx, aby, acx, acy, inv_det);
+            const S2Span& sp = tr.sp;
             for (int r0 = 0; r0 < size_y; r0 += 32) {
                 int xlo = 0, len = 0;
                 if (r0 + lane < size_y) s2_row_span(sp, start_y + (float)(r0 + lane), asy, xlo, len);
@@ -1201,6 +1228,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_stage2(const CrFrameParams p) {
                 }
             }
         }
+        __syncwarp();  // the next group's setups overwrite this one's
     }
 }
 

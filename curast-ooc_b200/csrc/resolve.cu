@@ -3,8 +3,9 @@
 // One thread per pixel, 32x8 blocks so each warp reads 32 consecutive
 // visbuffer entries (256 B) and writes 32 consecutive RGBA8 values.  It fuses
 // the reference's two passes, kernel_resolve_visbuffer_to_colorbuffer2D
-// (src/kernels/resolve.cu:640-1141, DisplayAttribute NONE / TRIANGLE_ID /
-// VERTEX_COLORS) and kernel_resolve_colorbuffer_to_screenshot
+// (src/kernels/resolve.cu:640-1141, DisplayAttribute NONE / NORMAL /
+// VERTEX_COLORS / TRIANGLE_ID / MESH_ID / STAGE) and
+// kernel_resolve_colorbuffer_to_screenshot
 // (resolve.cu:1264-1313 with EDL and SSAO off), so the 64-bit colorbuffer is
 // written only when the caller asks for it and never read back.
 // inverse(view) is formed once on the host instead of once per pixel.
@@ -42,6 +43,12 @@ __device__ __forceinline__ V3 xform_f4(const float4* m, V3 p) {
     return V3{(c0.x * p.x + c1.x * p.y) + (c2.x * p.z + c3.x * 1.0f),
               (c0.y * p.x + c1.y * p.y) + (c2.y * p.z + c3.y * 1.0f),
               (c0.z * p.x + c1.z * p.y) + (c2.z * p.z + c3.z * 1.0f)};
+}
+
+// viewToNDC, helpers:95-101
+__device__ __forceinline__ V3 to_ndc(V3 v, float f, float aspect) {
+    const float depth = -v.z;
+    return V3{((f / aspect) * v.x) / depth, (f * v.y) / depth, depth};
 }
 
 __device__ __forceinline__ float clamp_ref(float v, float lo, float hi) {
@@ -87,12 +94,16 @@ __device__ __forceinline__ void resolve_pixel(const CrResolveParams& p, const in
         uint32_t tri = (uint32_t)(tid - __ldg(&I->cum));
         tri = min(tri, nT - 1u);
         const uint32_t* colors = ldg_ptr(&I->colors);
+        // the displays that refetch the triangle's vertices
+        const bool refetch = p.display == 3 || p.display == 7 || (p.display == 4 && colors);
         if (p.display == 0) {  // DisplayAttribute::NONE
             color = 0xffffffffu;
         } else if (p.display == 5) {  // DisplayAttribute::TRIANGLE_ID
             color = tri * 12345678u;
-        } else if (p.display == 4 && colors) {  // DisplayAttribute::VERTEX_COLORS
-            // resolve.cu:742-764: plain or compressed refetch (geom.cuh)
+        } else if (p.display == 6) {  // DisplayAttribute::MESH_ID (resolve.cu:878-879)
+            color = (__ldg(&I->id) + 1u) * 12345678u;
+        } else if (refetch) {
+            // resolve.cu:742-770: plain or compressed refetch (geom.cuh)
             const GeomRef g = geom_of(I);
             const uint32_t i0 = geom_index(g, 3ull * tri + 0);
             const uint32_t i1 = geom_index(g, 3ull * tri + 1);
@@ -101,47 +112,82 @@ __device__ __forceinline__ void resolve_pixel(const CrResolveParams& p, const in
             const V3 aw = xform_f4(W4, pos_of(g, i0));
             const V3 bw = xform_f4(W4, pos_of(g, i1));
             const V3 cw = xform_f4(W4, pos_of(g, i2));
-
-            // computeRayDir, resolve.cu:662-676
-            const V3 origin = {p.origin[0], p.origin[1], p.origin[2]};
-            const float u = 2.0f * ((float)x + 0.5f) / (float)p.W - 1.0f;
-            const float v = 2.0f * ((float)y + 0.5f) / (float)p.H - 1.0f;
-            const V3 rdv = normalize3(V3{1.0f / p.p00 * u, 1.0f / p.p11 * v, -1.0f});
-            const V3 rayDir = normalize3(sub3(xform_m(p.viewI, rdv), origin));
-
-            // intersectPlane (helpers:318-348) and barycentrics (resolve.cu:790-834)
             const V3 e1 = sub3(bw, aw);
             const V3 e2 = sub3(cw, aw);
             const V3 normal = normalize3(cross3(e1, e2));
-            const float d = dot3(aw, normal);
-            const float den = dot3(normal, rayDir);
-            float t = INFINITY;
-            if (den != 0.0f) {
-                const float tt = -(dot3(origin, normal) + -d) / den;
-                t = tt >= 0.0f ? tt : INFINITY;
-            }
-            const float d00 = dot3(e1, e1);
-            const float d01 = dot3(e1, e2);
-            const float d11 = dot3(e2, e2);
-            const float denomI = 1.0f / (d00 * d11 - d01 * d01);
-            const V3 ph = {origin.x + t * rayDir.x, origin.y + t * rayDir.y, origin.z + t * rayDir.z};
-            const V3 v2 = sub3(ph, aw);
-            const float d20 = dot3(v2, e1);
-            const float d21 = dot3(v2, e2);
-            const float sx = (d11 * d20 - d01 * d21) * denomI;
-            const float sy = (d00 * d21 - d01 * d20) * denomI;
-            const float w0 = 1.0f - sx - sy;
+            if (p.display == 4) {  // DisplayAttribute::VERTEX_COLORS
+                // computeRayDir, resolve.cu:662-676
+                const V3 origin = {p.origin[0], p.origin[1], p.origin[2]};
+                const float u = 2.0f * ((float)x + 0.5f) / (float)p.W - 1.0f;
+                const float v = 2.0f * ((float)y + 0.5f) / (float)p.H - 1.0f;
+                const V3 rdv = normalize3(V3{1.0f / p.p00 * u, 1.0f / p.p11 * v, -1.0f});
+                const V3 rayDir = normalize3(sub3(xform_m(p.viewI, rdv), origin));
 
-            const uint32_t Ca = __ldg(colors + i0), Cb = __ldg(colors + i1), Cc = __ldg(colors + i2);
-            color = Ca;
+                // intersectPlane (helpers:318-348) and barycentrics (resolve.cu:790-834)
+                const float d = dot3(aw, normal);
+                const float den = dot3(normal, rayDir);
+                float t = INFINITY;
+                if (den != 0.0f) {
+                    const float tt = -(dot3(origin, normal) + -d) / den;
+                    t = tt >= 0.0f ? tt : INFINITY;
+                }
+                const float d00 = dot3(e1, e1);
+                const float d01 = dot3(e1, e2);
+                const float d11 = dot3(e2, e2);
+                const float denomI = 1.0f / (d00 * d11 - d01 * d01);
+                const V3 ph = {origin.x + t * rayDir.x, origin.y + t * rayDir.y, origin.z + t * rayDir.z};
+                const V3 v2 = sub3(ph, aw);
+                const float d20 = dot3(v2, e1);
+                const float d21 = dot3(v2, e2);
+                const float sx = (d11 * d20 - d01 * d21) * denomI;
+                const float sy = (d00 * d21 - d01 * d20) * denomI;
+                const float w0 = 1.0f - sx - sy;
+
+                const uint32_t Ca = __ldg(colors + i0), Cb = __ldg(colors + i1), Cc = __ldg(colors + i2);
+                color = Ca;
 #pragma unroll
-            for (int ch = 0; ch < 3; ++ch) {
-                const float ca = (float)((Ca >> (8 * ch)) & 0xffu);
-                const float cb = (float)((Cb >> (8 * ch)) & 0xffu);
-                const float cc = (float)((Cc >> (8 * ch)) & 0xffu);
-                const float c = ca * w0 + cb * sx + cc * sy;
-                const uint32_t b8 = __float2uint_rz(clamp_ref(c, 0.0f, 255.0f)) & 0xffu;
-                color = (color & ~(0xffu << (8 * ch))) | (b8 << (8 * ch));
+                for (int ch = 0; ch < 3; ++ch) {
+                    const float ca = (float)((Ca >> (8 * ch)) & 0xffu);
+                    const float cb = (float)((Cb >> (8 * ch)) & 0xffu);
+                    const float cc = (float)((Cc >> (8 * ch)) & 0xffu);
+                    const float c = ca * w0 + cb * sx + cc * sy;
+                    const uint32_t b8 = __float2uint_rz(clamp_ref(c, 0.0f, 255.0f)) & 0xffu;
+                    color = (color & ~(0xffu << (8 * ch))) | (b8 << (8 * ch));
+                }
+            } else if (p.display == 3) {
+                // DisplayAttribute::NORMAL of a mesh without vertex normals:
+                // the face normal's components x 255, clamped (resolve.cu:944-951)
+                const float n[3] = {normal.x, normal.y, normal.z};
+                color = 0u;
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch)
+                    color |= (__float2uint_rz(clamp_ref(n[ch] * 255.0f, 0.0f, 255.0f)) & 0xffu) << (8 * ch);
+            } else {
+                // DisplayAttribute::STAGE (resolve.cu:974-1018): the stage the
+                // triangle's screen box and near-plane crossing imply
+                const float f = p.p11;
+                const float aspect = (float)p.W / (float)p.H;
+                const V3 an = to_ndc(xform_m(p.view, aw), f, aspect);
+                const V3 bn = to_ndc(xform_m(p.view, bw), f, aspect);
+                const V3 cn = to_ndc(xform_m(p.view, cw), f, aspect);
+                const bool nontrivial = an.z <= 0.0f || bn.z <= 0.0f || cn.z <= 0.0f;
+                const float Wf = (float)p.W, Hf = (float)p.H;
+                const float asx = (an.x * 0.5f + 0.5f) * Wf, asy = (an.y * 0.5f + 0.5f) * Hf;
+                const float bsx = (bn.x * 0.5f + 0.5f) * Wf, bsy = (bn.y * 0.5f + 0.5f) * Hf;
+                const float csx = (cn.x * 0.5f + 0.5f) * Wf, csy = (cn.y * 0.5f + 0.5f) * Hf;
+                float min_x = fminf(asx, fminf(bsx, csx)), max_x = fmaxf(asx, fmaxf(bsx, csx));
+                float min_y = fminf(asy, fminf(bsy, csy)), max_y = fmaxf(asy, fmaxf(bsy, csy));
+                min_x = fmaxf(min_x, 0.0f);
+                max_x = fminf(max_x, (float)(p.W - 1));
+                min_y = fmaxf(min_y, 0.0f);
+                max_y = fminf(max_y, (float)(p.H - 1));
+                const int size_x = (int)(ceilf(max_x) - floorf(min_x));
+                const int size_y = (int)(ceilf(max_y) - floorf(min_y));
+                const int numFragments = size_x * size_y;
+                int stage = numFragments <= (int)p.thrSmall ? 0 : numFragments <= (int)p.thrLarge ? 1 : 2;
+                if (nontrivial) stage = 2;
+                // SCHEME_SPECTRAL[9], [7], [3] (utils.cuh:21-33)
+                color = stage == 0 ? 0xffbd8832u : stage == 1 ? 0xffa4ddabu : 0xff61aefdu;
             }
         } else {
             color = 0xff0000ffu;
@@ -197,6 +243,7 @@ __global__ void __launch_bounds__(256) k_resolve_views(const CrResolveParams bas
         s_p.p11 = __ldg(&v->p11);
     }
     if (t < 16) s_p.viewI[t] = __ldg(&v->viewI[t]);
+    if (t >= 16 && t < 32) s_p.view[t - 16] = __ldg(&v->view[t - 16]);
     __syncthreads();
     const uint32_t b = blockIdx.x - __ldg(&v->resolveBlockBase);
     const uint32_t bx = (uint32_t)(W + 31) / 32;

@@ -28,8 +28,11 @@ CR_MEM_HOST = 0
 CR_MEM_DEVICE = 1
 
 CR_DISPLAY_NONE = 0
+CR_DISPLAY_NORMAL = 3
 CR_DISPLAY_VERTEX_COLORS = 4
 CR_DISPLAY_TRIANGLE_ID = 5
+CR_DISPLAY_MESH_ID = 6
+CR_DISPLAY_STAGE = 7
 
 CR_RENDER_SYNC = 1 << 0
 CR_RENDER_KEEP_ORDER = 1 << 1
@@ -145,6 +148,7 @@ class CrFrameStats(ctypes.Structure):
         ("work_items_drawn", _u64),
         ("vertex_chunks", _u64),
         ("vertex_chunks_evaluated", _u64),
+        ("stage1_survivors", _u64),
     ]
 
 
@@ -165,6 +169,7 @@ class CrNoallocInstance(ctypes.Structure):
 
 CR_NOALLOC_MAX_INSTANCES = 16
 CR_NOALLOC_MAX_VERTICES = 4 << 20
+CR_NOALLOC_MAX_SURVIVORS = 512 << 10
 
 CR_MAX_BATCH_VIEWS = 64
 CR_TUNE_THRESHOLDS = 1

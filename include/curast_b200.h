@@ -150,8 +150,14 @@ typedef struct cr_camera {
 
 typedef enum cr_display {
     CR_DISPLAY_NONE = 0,          /* DisplayAttribute::NONE: white                 */
+    CR_DISPLAY_NORMAL = 3,        /* DisplayAttribute::NORMAL: the face normal (the
+                                     meshes carry no vertex normals)               */
     CR_DISPLAY_VERTEX_COLORS = 4, /* DisplayAttribute::VERTEX_COLORS               */
-    CR_DISPLAY_TRIANGLE_ID = 5    /* DisplayAttribute::TRIANGLE_ID                 */
+    CR_DISPLAY_TRIANGLE_ID = 5,   /* DisplayAttribute::TRIANGLE_ID                 */
+    CR_DISPLAY_MESH_ID = 6,       /* DisplayAttribute::MESH_ID: the instance's place
+                                     in the caller's list stands for the node id   */
+    CR_DISPLAY_STAGE = 7          /* DisplayAttribute::STAGE: the raster stage the
+                                     triangle's screen box implies                 */
 } cr_display;
 
 enum cr_render_flags {
@@ -188,6 +194,9 @@ typedef struct cr_frame_stats {
     uint64_t work_items_drawn;
     uint64_t vertex_chunks;
     uint64_t vertex_chunks_evaluated;
+    /* record-culled frames: triangles the per-vertex records did not cull,
+     * which stage 1 ran through the reference's full per-triangle path */
+    uint64_t stage1_survivors;
 } cr_frame_stats;
 
 /* ---- context ---------------------------------------------------------- */
@@ -592,7 +601,7 @@ cr_status cr_server_destroy(cr_server* server);
  * device-wide synchronisation cudaMalloc/cudaFree imply in the middle of a
  * frame -- cr_render_noalloc renders one view without any context and calls
  * no allocating routine.  Its work queues, counters, outcodes and frame table
- * live in one static device array of CR_NOALLOC_SCRATCH_BYTES (about 12 MiB)
+ * live in one static device array of CR_NOALLOC_SCRATCH_BYTES (about 28 MiB)
  * that every GPU which loads the library holds until the process exits.
  *
  *   - instances[i] is one instance with its mesh's device arrays; ids follow
@@ -600,7 +609,9 @@ cr_status cr_server_destroy(cr_server* server);
  *     CR_NOALLOC_MAX_INSTANCES instances and CR_NOALLOC_MAX_VERTICES vertices
  *     summed over them, else CR_ERR_INVALID.  A frame needing more than
  *     CR_NOALLOC_MAX_NONTRIVIAL stage-2 or CR_NOALLOC_MAX_TILES stage-3
- *     entries returns CR_ERR_QUEUE_OVERFLOW (output incomplete).
+ *     entries, or more than CR_NOALLOC_MAX_SURVIVORS stage-1 triangles that
+ *     the per-vertex records cannot cull, returns CR_ERR_QUEUE_OVERFLOW
+ *     (output incomplete).
  *   - The call is synchronous on `stream`: it uploads the frame table from
  *     host memory and reads back the queue counters, then synchronises the
  *     stream.  So it must never be called on a stream that is being captured
@@ -618,7 +629,8 @@ cr_status cr_server_destroy(cr_server* server);
 #define CR_NOALLOC_MAX_VERTICES (4u << 20)
 #define CR_NOALLOC_MAX_NONTRIVIAL (512u << 10)
 #define CR_NOALLOC_MAX_TILES (256u << 10)
-#define CR_NOALLOC_SCRATCH_BYTES (12u * 1024u * 1024u + 20u * 1024u)
+#define CR_NOALLOC_MAX_SURVIVORS (512u << 10)
+#define CR_NOALLOC_SCRATCH_BYTES (28u * 1024u * 1024u + 20u * 1024u)
 
 typedef struct cr_noalloc_instance {
     const float* d_positions;   /* xyz per vertex, device                      */

@@ -30,7 +30,7 @@ class OrcInstance(ctypes.Structure):
         ("colors", _vp),
         ("cum", _u64),
         ("numTriangles", _u32),
-        ("pad", _u32),
+        ("id", _u32),
         ("world", _f32 * 16),
     ]
 
@@ -61,7 +61,7 @@ def oracle():
                                    ctypes.POINTER(OrcStats)]
         lib.orc_resolve.restype = _i32
         lib.orc_resolve.argtypes = [ctypes.POINTER(OrcInstance), _u32, _vp, _vp, _vp, _i32, _i32, _vp, _vp, _vp,
-                                    _u32, _i32, _i32]
+                                    _u32, _i32, _i32, _i32, _i32]
         lib.orc_clear.restype = None
         lib.orc_clear.argtypes = [_vp, _u64]
         lib.orc_mat4_mul.restype = None
@@ -81,9 +81,11 @@ def mat4_mul(a, b):
 
 
 class Frame:
-    """Instances in render order: list of (pos, idx, colors, world)."""
+    """Instances in render order: list of (pos, idx, colors, world).  ids:
+    each instance's mesh id for the MESH_ID display (default: its place in
+    `items`)."""
 
-    def __init__(self, items, view):
+    def __init__(self, items, view, ids=None):
         self.items = []
         self.keep = []
         n = len(items)
@@ -102,6 +104,7 @@ class Frame:
             r.colors = col.ctypes.data if col is not None else None
             r.cum = cum
             r.numTriangles = idx.shape[0] if idx is not None else pos.shape[0] // 3
+            r.id = int(ids[i]) if ids is not None else i
             r.world = (_f32 * 16)(*np.asarray(world, np.float32).reshape(16).tolist())
             self.world_view[i] = mat4_mul(view, world)
             self.prefix[i] = cum
@@ -122,7 +125,7 @@ def raster(frame, W, H, f, nthreads=0):
     return fb, st
 
 
-def resolve(frame, view, proj, W, H, fb, display=4, nthreads=0, background=0xFFFFFFFF):
+def resolve(frame, view, proj, W, H, fb, display=4, nthreads=0, background=0xFFFFFFFF, thresholds=(128, 4096)):
     cb = np.empty(W * H, np.uint64)
     rgba = np.empty(W * H, np.uint32)
     v = np.ascontiguousarray(np.asarray(view, np.float32).reshape(16))
@@ -130,7 +133,7 @@ def resolve(frame, view, proj, W, H, fb, display=4, nthreads=0, background=0xFFF
     fb = np.ascontiguousarray(fb, np.uint64)
     rc = oracle().orc_resolve(frame.inst, frame.n, frame.prefix.ctypes.data, v.ctypes.data, p.ctypes.data, W, H,
                               fb.ctypes.data, cb.ctypes.data, rgba.ctypes.data, background, int(display),
-                              int(nthreads))
+                              int(thresholds[0]), int(thresholds[1]), int(nthreads))
     if rc != 0:
         raise RuntimeError(f"orc_resolve failed: {rc}")
     return cb, rgba

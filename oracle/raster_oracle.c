@@ -43,7 +43,7 @@ typedef struct {
     const uint32_t* colors;    /* RGBA8 per vertex, may be NULL                */
     uint64_t cum;              /* CMesh::cummulativeTriangleCount               */
     uint32_t numTriangles;
-    uint32_t pad;
+    uint32_t id;               /* CMesh::id (the MESH_ID display)              */
     float world[16];           /* column-major object->world (CMesh::world)    */
 } orc_instance;
 
@@ -771,10 +771,12 @@ static inline float intersect_plane(v3 origin, v3 dir, v3 normal, float constant
 /* Resolves fb into a 64-bit colorbuffer (depth bits << 32 | RGBA8) and a
  * headless RGBA8 image.  prefix[i] == inst[i].cum.  display takes the
  * reference's DisplayAttribute values (HostDeviceInterface.h:277-286):
- * 0 NONE, 4 VERTEX_COLORS, 5 TRIANGLE_ID.  Either output may be NULL. */
+ * 0 NONE, 3 NORMAL (meshes without vertex normals), 4 VERTEX_COLORS,
+ * 5 TRIANGLE_ID, 6 MESH_ID, 7 STAGE (thrSmall / thrLarge: the raster's stage
+ * thresholds).  Either output may be NULL. */
 int orc_resolve(const orc_instance* inst, uint32_t nInst, const uint64_t* prefix, const float* view,
                 const float* proj, int W, int H, const uint64_t* fb, uint64_t* colorbuffer,
-                uint32_t* rgba, uint32_t background, int display, int nthreads) {
+                uint32_t* rgba, uint32_t background, int display, int thrSmall, int thrLarge, int nthreads) {
     nthreads = set_threads(nthreads);
     float viewI[16];
     mat4_inverse(view, viewI);
@@ -811,6 +813,60 @@ int orc_resolve(const orc_instance* inst, uint32_t nInst, const uint64_t* prefix
                     color = 0xffffffffu;
                 } else if (display == 5) {             /* DisplayAttribute::TRIANGLE_ID */
                     color = tri * 12345678u;
+                } else if (display == 6) {             /* DisplayAttribute::MESH_ID, resolve.cu:878-879 */
+                    color = (m->id + 1u) * 12345678u;
+                } else if (display == 3 || display == 7) {
+                    uint32_t i0, i1, i2;
+                    if (m->indices) {
+                        i0 = m->indices[3ull * tri + 0];
+                        i1 = m->indices[3ull * tri + 1];
+                        i2 = m->indices[3ull * tri + 2];
+                    } else {
+                        i0 = 3 * tri + 0; i1 = 3 * tri + 1; i2 = 3 * tri + 2;
+                    }
+                    v3 a_o = {m->positions[3ull * i0], m->positions[3ull * i0 + 1], m->positions[3ull * i0 + 2]};
+                    v3 b_o = {m->positions[3ull * i1], m->positions[3ull * i1 + 1], m->positions[3ull * i1 + 2]};
+                    v3 c_o = {m->positions[3ull * i2], m->positions[3ull * i2 + 1], m->positions[3ull * i2 + 2]};
+                    v3 a_w = xform_pt3(m->world, a_o);
+                    v3 b_w = xform_pt3(m->world, b_o);
+                    v3 c_w = xform_pt3(m->world, c_o);
+                    if (display == 3) {
+                        /* NORMAL without vertex normals, resolve.cu:944-951 */
+                        v3 N = normalize3(cross3(sub3(b_w, a_w), sub3(c_w, a_w)));
+                        float n[3] = {N.x, N.y, N.z};
+                        color = 0;
+                        for (int ch = 0; ch < 3; ch++) {
+                            float cl = clampf_ref(n[ch] * 255.0f, 0.0f, 255.0f);
+                            uint32_t b8 = (cl != cl) ? 0u : (uint32_t)(uint8_t)(int)cl;
+                            color |= b8 << (8 * ch);
+                        }
+                    } else {
+                        /* STAGE, resolve.cu:974-1018 */
+                        float f = proj[5];
+                        float aspect = (float)W / (float)H;
+                        v3 a_n = view_to_ndc(xform_pt3(view, a_w), f, aspect);
+                        v3 b_n = view_to_ndc(xform_pt3(view, b_w), f, aspect);
+                        v3 c_n = view_to_ndc(xform_pt3(view, c_w), f, aspect);
+                        int nontrivial = a_n.z <= 0.0f || b_n.z <= 0.0f || c_n.z <= 0.0f;
+                        v2 a_s = ndc_to_screen(a_n, (float)W, (float)H);
+                        v2 b_s = ndc_to_screen(b_n, (float)W, (float)H);
+                        v2 c_s = ndc_to_screen(c_n, (float)W, (float)H);
+                        float min_x = fminf(a_s.x, fminf(b_s.x, c_s.x));
+                        float max_x = fmaxf(a_s.x, fmaxf(b_s.x, c_s.x));
+                        float min_y = fminf(a_s.y, fminf(b_s.y, c_s.y));
+                        float max_y = fmaxf(a_s.y, fmaxf(b_s.y, c_s.y));
+                        min_x = fmaxf(min_x, 0.0f);
+                        max_x = fminf(max_x, (float)(W - 1));
+                        min_y = fmaxf(min_y, 0.0f);
+                        max_y = fminf(max_y, (float)(H - 1));
+                        int size_x = (int)(ceilf(max_x) - floorf(min_x));
+                        int size_y = (int)(ceilf(max_y) - floorf(min_y));
+                        int numFragments = size_x * size_y;
+                        int stage = numFragments <= thrSmall ? 0 : (numFragments <= thrLarge ? 1 : 2);
+                        if (nontrivial) stage = 2;
+                        /* SCHEME_SPECTRAL[9], [7], [3], utils.cuh:21-33 */
+                        color = stage == 0 ? 0xffbd8832u : (stage == 1 ? 0xffa4ddabu : 0xff61aefdu);
+                    }
                 } else if (display != 4 || !m->colors) {
                     color = 0xff0000ffu;
                 } else {                               /* DisplayAttribute::VERTEX_COLORS */

@@ -216,3 +216,15 @@ def test_autotune_thresholds_apply_to_plain_renders(gpu):
         tuning = c.autotune_batch(inst, Targets(cams).views(), pc.CR_TUNE_THRESHOLDS)
         assert tuning.threshold_small in (64, 128, 256)
         assert_views_equal(batched(c, inst, cams), plain_loop(c, inst, cams), "tuned thresholds")
+
+
+@pytest.mark.parametrize("display", [pc.CR_DISPLAY_NORMAL, pc.CR_DISPLAY_MESH_ID, pc.CR_DISPLAY_STAGE])
+def test_batched_displays_match_plain(ctx, display):
+    """The resolve's other displays in batched frames: each view's image (the
+    STAGE display reads the view's own matrix and size) equals cr_render's."""
+    h, keep = small_terrain(ctx, n=96)
+    hs = ctx.mesh_from_host(*scenes.triangle_soup(3000, seed=17, near_fraction=0.03))
+    inst = [(h, scenes.identity()), (hs, scenes.translate_scale(2.0, 0.5, 2.0, 0.8))]
+    cams = scenes.batch_cameras(7, seed=91, scale=0.1)
+    assert_views_equal(batched(ctx, inst, cams, display=display), plain_loop(ctx, inst, cams, display=display),
+                       f"display {display}")

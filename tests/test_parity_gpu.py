@@ -418,3 +418,33 @@ def test_async_render_on_torch_stream(ctx):
     s.synchronize()
     o = render_oracle([m], [(0, scenes.identity())], view, proj, W, H)[0]
     assert_same_vis(vis.cpu().numpy().view(np.uint64), o, "async render")
+
+
+@pytest.mark.parametrize("display", [pc.CR_DISPLAY_NONE, pc.CR_DISPLAY_NORMAL, pc.CR_DISPLAY_TRIANGLE_ID,
+                                     pc.CR_DISPLAY_MESH_ID, pc.CR_DISPLAY_STAGE])
+def test_resolve_displays(ctx, display):
+    """Every display of the reference's resolve that needs no textures:
+    against the oracle and the reference kernels (IEEE build).  Integer
+    colours (ids, stage colours) are exact; the face normal within 1."""
+    soup = scenes.triangle_soup(30000, seed=101, near_fraction=0.01)
+    hf = scenes.heightfield(nx=48, nz=24, seed=41)
+    meshes = [soup, hf]
+    inst = [(0, scenes.identity()), (1, scenes.translate_scale(-0.5, -0.8, -2.5, 1.5))]
+    W, H = 480, 270
+    view, proj = scenes.identity(), scenes.perspective(60.0, W / H)
+    vis, rgba, cb, stats = render_ours(ctx, meshes, inst, view, proj, W, H, display=display)
+    ovis, orgba, ocb, ost = render_oracle(meshes, inst, view, proj, W, H, display=display)
+    assert ost.stage1_direct > 0 and ost.nontrivial > 0 and ost.huge_tiles > 0
+    assert_same_vis(vis, ovis, "ours vs oracle")
+    tol = 1 if display == pc.CR_DISPLAY_NORMAL else 0
+    assert channel_diff(rgba, orgba) <= tol
+    if display != pc.CR_DISPLAY_NONE:  # NONE: white on the white background
+        assert len(np.unique(orgba)) > (3 if display == pc.CR_DISPLAY_STAGE else 1)
+    ref = reference()
+    ref.reset()
+    hs = [ref.mesh_host(p, i, c) for (p, i, c) in meshes]
+    worlds = np.stack([np.asarray(w, np.float32).reshape(16) for _, w in inst])
+    rvis, _, rrgba, _, _ = ref.frame([hs[m] for m, _ in inst], worlds, view, proj, W, H, instanced=True,
+                                     display=display, cap_nontrivial=1 << 22, cap_huge=1 << 22)
+    assert_same_vis(vis, rvis, "ours vs reference kernels")
+    assert channel_diff(rgba, rrgba) <= tol
