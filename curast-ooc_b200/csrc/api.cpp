@@ -237,6 +237,9 @@ cr_status assemble(cr_context* ctx, const cr_instance* instances, uint32_t count
         ci.outBase = A.outBytes;
         ci.vchunkBase = A.numVChunks;
         ci.chunkBoxes = m.chunkBoxes;
+        ci.chunkGroupBoxes = m.chunkGroupBoxes;
+        ci.cgBase = A.numChunkGroups;
+        A.numChunkGroups += ((m.numVertices + CR_VCHUNK - 1) / CR_VCHUNK + CR_GROUP - 1) / CR_GROUP;
         ci.id = A.order[r];  // the caller's list position: the MESH_ID display
         if (m.compressed) ci.codec = m.codec;
         A.outBytes += align_up(m.numVertices, 16);
@@ -261,6 +264,7 @@ cr_status assemble(cr_context* ctx, const cr_instance* instances, uint32_t count
             s.subBoxes = m.subBoxes;
             s.localLists = m.localLists;
             s.localCounts = m.localCounts;
+            s.groupBoxes = m.groupBoxes;
             A.seg.push_back(s);
         }
         A.seg.back().instanceCount++;
@@ -275,6 +279,8 @@ cr_status assemble(cr_context* ctx, const cr_instance* instances, uint32_t count
         s.numChunks = (s.instanceCount + CR_INST_CHUNK - 1) / CR_INST_CHUNK;
         s.itemBase = items;
         items += (uint64_t)s.numBatches * s.numChunks;
+        s.unitBase = A.numUnits;
+        A.numUnits += (uint64_t)((s.numBatches + CR_GROUP - 1) / CR_GROUP) * s.numChunks;
     }
     A.totalTriangles = sum;
     A.numItems = items;
@@ -318,18 +324,25 @@ cr_status launch_mesh_boxes(cr_context* ctx, MeshRec& m) {
     const size_t ib = align_up((size_t)((m.numTriangles + CR_BATCH - 1) / CR_BATCH) * 24, 256);
     const size_t cb = align_up((size_t)((m.numVertices + CR_VCHUNK - 1) / CR_VCHUNK) * 24, 256);
     const size_t sb = align_up((size_t)((m.numTriangles + CR_SUB - 1) / CR_SUB) * 24, 256);
+    const uint64_t nItems = (m.numTriangles + CR_BATCH - 1) / CR_BATCH;
+    const uint64_t nChunks = (m.numVertices + CR_VCHUNK - 1) / CR_VCHUNK;
+    const size_t gb = align_up((size_t)((nItems + CR_GROUP - 1) / CR_GROUP) * 24, 256);
+    const size_t cgb = align_up((size_t)((nChunks + CR_GROUP - 1) / CR_GROUP) * 24, 256);
     if (!m.itemBoxes) {
-        cr_status s = ctx->dev_alloc((void**)&m.itemBoxes, ib + cb + sb + 256, "mesh boxes");
+        cr_status s = ctx->dev_alloc((void**)&m.itemBoxes, ib + cb + sb + gb + cgb + 256, "mesh boxes");
         if (s) return s;
         m.chunkBoxes = (float*)((char*)m.itemBoxes + ib);
         m.subBoxes = (float*)((char*)m.itemBoxes + ib + cb);
-        m.boxBytes = ib + cb + sb + 256;
+        m.groupBoxes = (float*)((char*)m.itemBoxes + ib + cb + sb);
+        m.chunkGroupBoxes = (float*)((char*)m.itemBoxes + ib + cb + sb + gb);
+        m.boxBytes = ib + cb + sb + gb + cgb + 256;
     }
-    m.meshBox = (float*)((char*)m.itemBoxes + ib + cb + sb);
+    m.meshBox = (float*)((char*)m.itemBoxes + ib + cb + sb + gb + cgb);
     m.dCodec = (CrCodec*)((char*)m.meshBox + 64);
     CR_CUDA(cudaMemcpy(m.dCodec, &m.codec, sizeof(CrCodec), cudaMemcpyHostToDevice), "mesh codec");
     if (cr_launch_mesh_boxes(m.indices, m.positions, m.compressed ? m.dCodec : nullptr, m.numTriangles,
-                             m.numVertices, m.itemBoxes, m.chunkBoxes, m.subBoxes, m.meshBox, 0))
+                             m.numVertices, m.itemBoxes, m.chunkBoxes, m.subBoxes, m.meshBox, m.groupBoxes,
+                             m.chunkGroupBoxes, 0))
         return fail(CR_ERR_CUDA, "mesh box launch: %s", cudaGetErrorString(cudaGetLastError()));
     return CR_OK;
 }
@@ -422,6 +435,8 @@ cr_status upload_frame(cr_context* ctx, const Assembled& A, cudaStream_t stream,
     fp.numSegments = (uint32_t)m;
     fp.numItems = A.numItems;
     fp.numVChunks = A.numVChunks;
+    fp.numUnits = A.numUnits;
+    fp.numChunkGroups = A.numChunkGroups;
     rp.instances = fp.instances;
     rp.world = fp.world;
     rp.numInstances = (uint32_t)n;
@@ -1116,22 +1131,34 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
 
     s = ensure_records(ctx, direct ? 0 : A.outBytes * (cellMode == CR_REC_CELLS ? 8 : cellMode == CR_REC_CELLS32 ? 4 : 1));
     if (s) return s;
-    if (A.numItems > ctx->itemCap || A.numVChunks > ctx->chunkCap) {
-        // item-cull survivors (at most every item) and one class per chunk
+    if (A.numItems > ctx->itemCap || A.numVChunks > ctx->chunkCap || A.numUnits > ctx->unitCap ||
+        A.numChunkGroups > ctx->cgroupCap) {
+        // item-cull survivors (at most every item), the chunk list and one
+        // class per chunk, the group cull's lists (at most every unit / group)
         CR_CUDA(cudaDeviceSynchronize(), "cull buffer resize");
         ctx->dev_free(ctx->itemList, ctx->itemBytes);
         ctx->itemList = nullptr;
-        ctx->itemCap = ctx->chunkCap = ctx->itemBytes = 0;
+        ctx->itemCap = ctx->chunkCap = ctx->unitCap = ctx->cgroupCap = ctx->itemBytes = 0;
         const uint64_t items = A.numItems + A.numItems / 8 + 1024;
         const uint64_t chunks = A.numVChunks + A.numVChunks / 8 + 1024;
-        const size_t bytes = align_up(items * 8, 256) + align_up(chunks * 4, 256) + align_up(chunks, 256);
+        const uint64_t units = A.numUnits + A.numUnits / 8 + 1024;
+        const uint64_t cgroups = A.numChunkGroups + A.numChunkGroups / 8 + 1024;
+        const size_t oChunks = align_up(items * 8, 256);
+        const size_t oClass = oChunks + align_up(chunks * 4, 256);
+        const size_t oUnits = oClass + align_up(chunks, 256);
+        const size_t oGroups = oUnits + align_up(units * 8, 256);
+        const size_t bytes = oGroups + align_up(cgroups * 8, 256);
         s = ctx->dev_alloc((void**)&ctx->itemList, bytes, "cull buffers");
         if (s) return s;
         ctx->itemCap = items;
         ctx->chunkCap = chunks;
+        ctx->unitCap = units;
+        ctx->cgroupCap = cgroups;
         ctx->itemBytes = bytes;
-        ctx->chunkList = (uint32_t*)((char*)ctx->itemList + align_up(items * 8, 256));
-        ctx->chunkClass = (uint8_t*)ctx->chunkList + align_up(chunks * 4, 256);
+        ctx->chunkList = (uint32_t*)((char*)ctx->itemList + oChunks);
+        ctx->chunkClass = (uint8_t*)ctx->itemList + oClass;
+        ctx->unitList = (uint2*)((char*)ctx->itemList + oUnits);
+        ctx->cgroupList = (uint2*)((char*)ctx->itemList + oGroups);
     }
     CrFrameParams fp{};
     CrResolveParams rp{};
@@ -1148,10 +1175,13 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
     fp.itemCap = ctx->itemCap;
     fp.chunkList = ctx->chunkList;
     fp.chunkClass = ctx->chunkClass;
+    fp.unitList = ctx->unitList;
+    fp.cgroupList = ctx->cgroupList;
     if (direct) {  // no vertex pass: no chunks to classify or evaluate
         fp.chunkList = nullptr;
         fp.chunkClass = nullptr;
         fp.numVChunks = 0;
+        fp.numChunkGroups = 0;
     }
     fp.fb = (uint64_t*)d_visbuffer;
     fp.W = cam->width;

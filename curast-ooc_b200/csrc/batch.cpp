@@ -95,9 +95,61 @@ cr_status check_views(const cr_view* views, uint32_t nv, uint32_t flags) {
     return CR_OK;
 }
 
+// Several instance sets in one batched frame: the sets' instances one set
+// after the other, each set in cr_render's own order with its own ids (its
+// first instance's id is the set's base), and per view the set it renders.
+struct SetLayout {
+    std::vector<cr_instance> inst;
+    std::vector<uint64_t> firstIds;   // per instance: the set's base + the instance's id in the set
+    std::vector<uint32_t> instSet;    // per instance: its set
+    std::vector<uint64_t> setBase;    // per set: the id of its first triangle
+    const uint32_t* viewSets = nullptr;
+};
+
+cr_status layout_sets(cr_context* ctx, const cr_instance* instances, const uint32_t* setSizes, uint32_t numSets,
+                      const uint32_t* viewSets, uint32_t nv, uint32_t flags, SetLayout& S) {
+    uint64_t at = 0, base = 0;
+    for (uint32_t s = 0; s < numSets; s++) {
+        const uint32_t n = setSizes[s];
+        std::vector<uint32_t> mesh(n), tris(n), order(n);
+        std::vector<uint64_t> first(n);
+        for (uint32_t i = 0; i < n; i++) {
+            const uint32_t m = instances[at + i].mesh;
+            if (m >= ctx->meshes.size() || !ctx->meshes[m].live)
+                return fail(CR_ERR_NOT_FOUND, "set %u, instance %u: unknown mesh %u", s, i, m);
+            mesh[i] = m;
+            tris[i] = ctx->meshes[m].numTriangles;
+        }
+        if (n) {
+            cr_status st = cr_order_instances(mesh.data(), tris.data(), n, flags & CR_RENDER_KEEP_ORDER, order.data(),
+                                              first.data());
+            if (st) return st;
+        }
+        S.setBase.push_back(base);
+        uint64_t sum = 0;
+        for (uint32_t k = 0; k < n; k++) {
+            S.inst.push_back(instances[at + order[k]]);
+            S.firstIds.push_back(base + first[k]);
+            S.instSet.push_back(s);
+            sum += tris[order[k]];
+        }
+        at += n;
+        base += sum;
+    }
+    for (uint32_t v = 0; v < nv; v++)
+        if (viewSets[v] >= numSets) return fail(CR_ERR_INVALID, "view %u: instance set %u of %u", v, viewSets[v], numSets);
+    S.viewSets = viewSets;
+    return CR_OK;
+}
+
 // Per-view matrices, flips and targets; the same float operations cr_render
-// performs for one view.
-void build_views(const cr_instance* instances, const Assembled& A, const cr_view* views, uint32_t nv, BatchTables& B) {
+// performs for one view.  With instance sets, an instance outside a view's
+// set gets, in that view, a matrix that puts every finite vertex behind the
+// camera (so the box classes cull it) and flip bit 1 (stage 1 culls its
+// triangles whatever its positions), and the view's ids are relative to its
+// set's base.
+void build_views(const cr_instance* instances, const Assembled& A, const cr_view* views, uint32_t nv, BatchTables& B,
+                 const SetLayout* sets = nullptr) {
     const size_t n = A.inst.size();
     B.worldView.resize(16ull * n * nv);
     B.flips.resize((size_t)n * nv);
@@ -109,10 +161,18 @@ void build_views(const cr_instance* instances, const Assembled& A, const cr_view
         const cr_camera& cam = views[v].camera;
         for (size_t r = 0; r < n; r++) {
             float* wv = &B.worldView[16ull * (v * n + r)];
+            if (sets && sets->instSet[A.order[r]] != sets->viewSets[v]) {
+                memset(wv, 0, 64);
+                wv[14] = 1.0f;  // view-space z = +1: behind the camera
+                wv[15] = 1.0f;
+                B.flips[v * n + r] = 2u;
+                continue;
+            }
             mat4_mul(cam.view, instances[A.order[r]].world, wv);  // CuRast_render.h:409
             B.flips[v * n + r] = det3_glm(wv) < 0.0f ? 1u : 0u;
         }
         CrView& cv = B.views[v];
+        cv.idBase = sets ? sets->setBase[sets->viewSets[v]] : 0ull;
         cv.fb = (uint64_t*)views[v].d_visbuffer;
         cv.rgba = (uint32_t*)views[v].d_rgba;
         cv.colorbuffer = (uint64_t*)views[v].d_colorbuffer;
@@ -238,17 +298,20 @@ CrBatchShape shape_for(const cr_context* ctx, uint32_t sceneClass) {
 }
 
 cr_status render_batch(cr_context* ctx, const cr_instance* instances, uint32_t count, const cr_view* views, uint32_t nv,
-                       int32_t display, uint32_t flags, cudaStream_t stream, const CrBatchShape* forced) {
+                       int32_t display, uint32_t flags, cudaStream_t stream, const CrBatchShape* forced,
+                       const SetLayout* sets = nullptr) {
     if (!ctx || (!instances && count)) return fail(CR_ERR_INVALID, "cr_render_batch: NULL argument");
     cr_status s = check_views(views, nv, flags);
     if (s) return s;
     CR_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
     ensure_local_lists_for(ctx, instances, count);
     Assembled A;
-    s = assemble(ctx, instances, count, views[0].camera.view, flags, A);
+    s = sets ? assemble(ctx, instances, count, views[0].camera.view, flags | CR_RENDER_KEEP_ORDER, A,
+                        sets->firstIds.data())
+             : assemble(ctx, instances, count, views[0].camera.view, flags, A);
     if (s) return s;
     BatchTables B;
-    build_views(instances, A, views, nv, B);
+    build_views(instances, A, views, nv, B, sets);
     const uint32_t sceneClass = cr_scene_class(A.totalTriangles, B.sumPixels, nv);
     const CrBatchShape sh = forced ? *forced : shape_for(ctx, sceneClass);
     if (const cr_tuning* t = find_tuning(ctx, sceneClass)) {  // tuned queue sizes
@@ -456,6 +519,21 @@ extern "C" {
 
 uint32_t cr_scene_class(uint64_t triangles, uint64_t pixels, uint32_t num_views) {
     return (ceil_log2(triangles) << 16) | (ceil_log2(pixels) << 8) | ceil_log2(num_views);
+}
+
+cr_status cr_render_batch_sets(cr_context* ctx, const cr_instance* instances, const uint32_t* set_sizes,
+                               uint32_t num_sets, const cr_view* views, const uint32_t* view_sets, uint32_t num_views,
+                               int32_t display, uint32_t flags, void* stream) {
+    if (!ctx || !set_sizes || !view_sets || num_sets == 0) return fail(CR_ERR_INVALID, "cr_render_batch_sets: NULL argument");
+    uint64_t count = 0;
+    for (uint32_t k = 0; k < num_sets; k++) count += set_sizes[k];
+    if (count > 0xffffffffull || (count && !instances)) return fail(CR_ERR_INVALID, "cr_render_batch_sets: bad instance list");
+    CR_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    SetLayout S;
+    cr_status s = layout_sets(ctx, instances, set_sizes, num_sets, view_sets, num_views, flags, S);
+    if (s) return s;
+    return render_batch(ctx, S.inst.data(), (uint32_t)count, views, num_views, display, flags, (cudaStream_t)stream,
+                        nullptr, &S);
 }
 
 cr_status cr_render_batch(cr_context* ctx, const cr_instance* instances, uint32_t count, const cr_view* views,

@@ -44,6 +44,8 @@ struct MeshRec {
     float* itemBoxes = nullptr;   // per CR_BATCH triangles
     float* chunkBoxes = nullptr;  // per CR_VCHUNK vertices
     float* subBoxes = nullptr;    // per CR_SUB triangles
+    float* groupBoxes = nullptr;  // per CR_GROUP item boxes
+    float* chunkGroupBoxes = nullptr;  // per CR_GROUP chunk boxes
     float* meshBox = nullptr;     // the whole mesh's box (6 floats)
     size_t boxBytes = 0;
     float box[6] = {NAN, NAN, NAN, NAN, NAN, NAN};  // host copy of the mesh box
@@ -97,6 +99,8 @@ struct Assembled {
     uint64_t numItems = 0;
     uint64_t outBytes = 0;     // vertex-pass record slots of all instances
     uint64_t numVChunks = 0;   // vertex-pass chunks of all instances
+    uint64_t numUnits = 0;     // group-cull units (CR_GROUP items of one instance chunk)
+    uint64_t numChunkGroups = 0;  // group-cull chunk groups (CR_GROUP chunks of one instance)
 };
 
 }  // namespace cr
@@ -126,8 +130,12 @@ struct cr_context {
     uint64_t outCap = 0;
     uint64_t* ntList = nullptr;
     uint64_t ntCap = 0;
-    uint2* itemList = nullptr;    // item-cull survivors, then the chunk list and classes
+    uint2* itemList = nullptr;    // item-cull survivors, then the chunk list and classes,
+                                  // then the group cull's unit and chunk-group lists
     uint64_t itemCap = 0;
+    uint2* unitList = nullptr;
+    uint2* cgroupList = nullptr;
+    uint64_t unitCap = 0, cgroupCap = 0;
     uint32_t* chunkList = nullptr;
     uint8_t* chunkClass = nullptr;
     uint64_t chunkCap = 0;
@@ -222,8 +230,12 @@ struct BatchScratch {
     size_t recordCap = 0;
     uint64_t* ntList = nullptr;
     uint64_t ntCap = 0;
-    uint2* itemList = nullptr;    // item-cull survivors, then the chunk list and classes
+    uint2* itemList = nullptr;    // item-cull survivors, then the chunk list and classes,
+                                  // then the group cull's unit and chunk-group lists
     uint64_t itemCap = 0;
+    uint2* unitList = nullptr;
+    uint2* cgroupList = nullptr;
+    uint64_t unitCap = 0, cgroupCap = 0;
     uint32_t* chunkList = nullptr;
     uint8_t* chunkClass = nullptr;
     uint64_t chunkCap = 0;

@@ -39,7 +39,9 @@
 #define CR_CTR_CHUNKS 5         // vertex-pass chunks that need per-vertex records
 #define CR_CTR_SURVIVORS 6      // stage-1 triangles the records do not cull
                                 // (appended by k_s1cull for k_s1raster)
-#define CR_CTR_COUNT 8
+#define CR_CTR_UNITS 7          // item groups the group cull leaves for the item cull
+#define CR_CTR_CGROUPS 8        // chunk groups the group cull leaves for the chunk cull
+#define CR_CTR_COUNT 16
 
 // Compressed geometry (the reference's IX_PU16 meshes, CMesh fields
 // compressionFactor / index_min / aabb.min / bitsPerIndex / compressed,
@@ -68,6 +70,8 @@ struct alignas(16) CrInstance {
     uint32_t id;                // the instance's place in the caller's list (MESH_ID display)
     uint32_t pad1;
     CrCodec codec;              // compressed meshes: positions are uint16 xyz
+    const float* chunkGroupBoxes;  // per CR_GROUP chunk boxes: their union (or nullptr)
+    uint64_t cgBase;            // first chunk group of this instance
 };
 
 // Per-(instance, vertex) outcode bits written by the vertex pass.  They are
@@ -86,6 +90,7 @@ struct alignas(16) CrInstance {
 // beyond a frustum side, so no item box needs classifying; 0: unknown.
 #define CR_MESH_INSIDE 32u
 #define CR_VCHUNK 1024          // vertices per vertex-pass chunk
+#define CR_GROUP 32             // item boxes per group box, chunk boxes per chunk-group box
 
 // Cell records (8 bytes per (instance, vertex), CrFrameParams::cellMode):
 // the outcode byte plus the vertex's exact stage-1 screen position reduced to
@@ -98,7 +103,7 @@ struct alignas(16) CrInstance {
 #define CR_CELL_INSIDE (1ull << 8)
 #define CR_CELL_FRACX (1ull << 9)
 #define CR_CELL_FRACY (1ull << 10)
-static_assert(sizeof(CrInstance) == 112, "CrInstance layout");
+static_assert(sizeof(CrInstance) == 128, "CrInstance layout");
 
 struct alignas(16) CrSegment {
     const uint32_t* indices;
@@ -115,8 +120,10 @@ struct alignas(16) CrSegment {
     const uint8_t* localLists;  // per item, CR_LOCAL_BYTES (or nullptr)
     const uint32_t* localCounts;  // per item, distinct vertices or CR_LOCAL_NONE
     CrCodec codec;              // compressed meshes (flags bit 0 is then clear)
+    const float* groupBoxes;    // per CR_GROUP item boxes: their union (or nullptr)
+    uint64_t unitBase;          // first group-cull unit (item group x instance chunk)
 };
-static_assert(sizeof(CrSegment) == 112, "CrSegment layout");
+static_assert(sizeof(CrSegment) == 128, "CrSegment layout");
 
 struct alignas(16) CrTile {     // HugeTriangle, HostDeviceInterface.h:254-259
     int32_t instance;           // instance | view << 26 (view 0 in single-view frames)
@@ -146,8 +153,11 @@ struct alignas(16) CrView {
     uint32_t resolveBlockBase;  // first block of this view in the resolve grid
     uint32_t pad;
     float view[16];             // the view matrix (the STAGE display)
+    uint64_t idBase;            // first global id of the view's instance set: the
+                                // view's visbuffer holds ids relative to it
+    uint64_t pad2;
 };
-static_assert(sizeof(CrView) == 208, "CrView layout");
+static_assert(sizeof(CrView) == 224, "CrView layout");
 
 // Multi-view vertex record (48 bytes, read as three 16-byte loads): per
 // frustum predicate of vertex_outcode one bit per view.  BEHIND bits are
@@ -218,6 +228,12 @@ struct CrFrameParams {
     CrItemViews* itemViews;
     CrViewMasks* chunkMasks;
     uint8_t* chunkUniform;
+    // group cull: units (CR_GROUP consecutive items of one instance chunk)
+    // and chunk groups (CR_GROUP consecutive chunks of one instance) whose
+    // group box is not proven culled, listed for the item and chunk culls
+    uint64_t numUnits, numChunkGroups;
+    uint2* unitList;            // {unit, alive mask | inside mask << 16}
+    uint2* cgroupList;          // {chunk group, 1 if wholly inside}
     // record-culled single-view frames: per vertex-pass chunk the frame
     // cull's class (CR_CHUNK_EVAL: the vertex pass writes its records; else
     // the record every vertex of the chunk has); nullptr: every chunk has
@@ -255,6 +271,8 @@ struct CrResolveParams {
     uint64_t idLo, idHi;        // covered pixels are written only for ids in [idLo, idHi)
     float view[16];             // the view matrix (STAGE display)
     uint32_t thrSmall, thrLarge;  // the stage thresholds (STAGE display)
+    uint64_t idBase;            // added to a pixel's id to find its instance (batched
+                                // frames of several instance sets)
 };
 
 // Post-processing of the colorbuffer (post.cu): the reference's EDL, SSAO and
@@ -307,7 +325,7 @@ int cr_launch_resolve(const CrResolveParams& p, void* stream);
 // `codec`: device copy of a compressed mesh's codec, or nullptr.
 int cr_launch_mesh_boxes(const uint32_t* indices, const float* positions, const CrCodec* codec,
                          uint32_t numTriangles, uint32_t numVertices, float* itemBoxes, float* chunkBoxes,
-                         float* subBoxes, float* meshBox, void* stream);
+                         float* subBoxes, float* meshBox, float* groupBoxes, float* chunkGroupBoxes, void* stream);
 // Per-item vertex lists of an indexed mesh (see CR_LOCAL_BYTES).
 int cr_launch_local_lists(const uint32_t* indices, const CrCodec* codec, uint32_t numTriangles, uint8_t* lists,
                           uint32_t* counts, void* stream);

@@ -7,6 +7,9 @@
 //                proof of box_misses_samples
 //   chunk boxes  one per CR_VCHUNK (1024) consecutive vertices (a vertex-pass
 //                chunk)
+//   group boxes  one per CR_GROUP (32) consecutive item boxes and one per 32
+//                consecutive chunk boxes: their union, classified first by
+//                the group cull
 //   mesh box     the union of the item boxes, classified per instance on the
 //                host
 // Per view, a box classified by classify_chunk as wholly behind the camera
@@ -111,6 +114,30 @@ __global__ void __launch_bounds__(256) k_chunk_boxes(const float* pos, const CrC
         for (uint32_t v = c * CR_VCHUNK + lane; v < min(nV, (c + 1) * CR_VCHUNK); v += 32)
             extend(lo, hi, bad, g, v);
         warp_write_box(lo, hi, bad, boxes + 6ull * c, lane);
+    }
+}
+
+// One warp per group: the union of CR_GROUP consecutive boxes (item boxes or
+// chunk boxes), NaN if any of them is NaN.  The group cull classifies these
+// first, so a group proven culled skips its members' boxes.
+__global__ void __launch_bounds__(256) k_group_boxes(const float* boxes, uint32_t n, float* out) {
+    static_assert(CR_GROUP == 32, "one lane per member box");
+    const int lane = threadIdx.x & 31;
+    const uint32_t nGroups = (n + CR_GROUP - 1) / CR_GROUP;
+    for (uint32_t gi = blockIdx.x * 8 + (threadIdx.x >> 5); gi < nGroups; gi += gridDim.x * 8) {
+        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        bool bad = false;
+        const uint32_t b = gi * CR_GROUP + lane;
+        if (b < n) {
+            const float* q = boxes + 6ull * b;
+            for (int j = 0; j < 3; ++j) {
+                const float l = q[j], h = q[3 + j];
+                bad |= !(l <= h);  // NaN boxes
+                lo[j] = l;
+                hi[j] = h;
+            }
+        }
+        warp_write_box(lo, hi, bad, out + 6ull * gi, lane);
     }
 }
 
@@ -249,7 +276,7 @@ int cr_launch_local_lists(const uint32_t* indices, const CrCodec* codec, uint32_
 
 int cr_launch_mesh_boxes(const uint32_t* indices, const float* positions, const CrCodec* codec,
                          uint32_t numTriangles, uint32_t numVertices, float* itemBoxes, float* chunkBoxes,
-                         float* subBoxes, float* meshBox, void* stream) {
+                         float* subBoxes, float* meshBox, float* groupBoxes, float* chunkGroupBoxes, void* stream) {
     cudaStream_t st = (cudaStream_t)stream;
     const uint32_t nItems = (numTriangles + CR_BATCH - 1) / CR_BATCH;
     const uint32_t nChunks = (numVertices + CR_VCHUNK - 1) / CR_VCHUNK;
@@ -261,6 +288,14 @@ int cr_launch_mesh_boxes(const uint32_t* indices, const float* positions, const 
             indices, positions, codec, numTriangles, subBoxes);
     if (nChunks) k_chunk_boxes<<<(nChunks + 7) / 8 < 148 * 16 ? (nChunks + 7) / 8 : 148 * 16, 256, 0, st>>>(
         positions, codec, numVertices, chunkBoxes);
+    const uint32_t nGroups = (nItems + CR_GROUP - 1) / CR_GROUP;
+    const uint32_t nCGroups = (nChunks + CR_GROUP - 1) / CR_GROUP;
+    if (nGroups && groupBoxes)
+        k_group_boxes<<<(nGroups + 7) / 8 < 148 * 16 ? (nGroups + 7) / 8 : 148 * 16, 256, 0, st>>>(itemBoxes, nItems,
+                                                                                                 groupBoxes);
+    if (nCGroups && chunkGroupBoxes)
+        k_group_boxes<<<(nCGroups + 7) / 8 < 148 * 16 ? (nCGroups + 7) / 8 : 148 * 16, 256, 0, st>>>(
+            chunkBoxes, nChunks, chunkGroupBoxes);
     if (meshBox) k_mesh_box<<<1, 256, 0, st>>>(itemBoxes, nItems, meshBox);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

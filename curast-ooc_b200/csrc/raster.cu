@@ -74,33 +74,39 @@ __global__ void __launch_bounds__(THREADS, VX_MIN_BLOCKS) k_vertex(const CrFrame
     constexpr uint32_t BYTES = CR_VCHUNK * 12;
     __shared__ __align__(128) float s_pos[STAGES][CR_VCHUNK * 3];
     __shared__ __align__(8) uint64_t s_bar[STAGES];
+    // the chunk each slot holds, decoded once by thread 0 when it fills the slot
+    __shared__ VxChunk s_ch[STAGES];
     const float fa = p.f / p.aspect;
     const float Wf = (float)p.W, Hf = (float)p.H;
     const float Wm1 = (float)(p.W - 1), Hm1 = (float)(p.H - 1);
     // the chunks the frame cull left for per-vertex records (or every chunk)
     const uint64_t nChunks = p.chunkList ? min((uint64_t)p.counters[CR_CTR_CHUNKS], p.numVChunks) : p.numVChunks;
+    // thread 0 issues the copies; `pending` (its own) marks slots holding an
+    // issued, not yet consumed copy
+    uint32_t pending = 0, parity = 0;
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) mbar_init(&s_bar[s], 1);
         fence_barrier_init();
-    }
-    __syncthreads();
-    // `pending`: slots holding an issued, not yet consumed copy (every thread
-    // tracks it identically; thread 0 issues the copies)
-    uint32_t pending = 0, parity = 0;
-    for (int s = 0; s < STAGES; ++s) {
-        const uint64_t k = blockIdx.x + (uint64_t)s * gridDim.x;
-        if (k >= nChunks) break;
-        const VxChunk ch = vx_chunk(p, k);
-        if (ch.src) {
-            pending |= 1u << s;
-            if (threadIdx.x == 0) bulk_load(s_pos[s], ch.src, BYTES, &s_bar[s]);
+        for (int s = 0; s < STAGES; ++s) {
+            const uint64_t k = blockIdx.x + (uint64_t)s * gridDim.x;
+            if (k >= nChunks) break;
+            s_ch[s] = vx_chunk(p, k);
+            if (s_ch[s].src) {
+                pending |= 1u << s;
+                bulk_load(s_pos[s], s_ch[s].src, BYTES, &s_bar[s]);
+            }
         }
     }
+    __syncthreads();
+    uint32_t lastInst = 0xffffffffu;
+    Mat M;
+    uint64_t outBase = 0;
+    GeomRef g;
     uint32_t kk = 0;
     for (uint64_t k = blockIdx.x; k < nChunks; k += gridDim.x, ++kk) {
         const int slot = (int)(kk % STAGES);
         const uint32_t bit = 1u << slot;
-        const VxChunk ch = vx_chunk(p, k);
+        const VxChunk ch = s_ch[slot];
         if (ch.src) {
             const bool ok = mbar_wait_bounded(&s_bar[slot], (parity & bit) ? 1u : 0u, p.waitTimeoutNs);
             if (__syncthreads_or(!ok)) {  // record, stop the block, drain its copies below
@@ -110,10 +116,13 @@ __global__ void __launch_bounds__(THREADS, VX_MIN_BLOCKS) k_vertex(const CrFrame
             parity ^= bit;
             pending &= ~bit;
         }
-        const Mat M = load_mat(p.world_view + 4ull * ch.inst);
-        const GeomRef g = geom_of(ch.I);
+        if (ch.inst != lastInst) {  // the instance's matrix and records, once per run of its chunks
+            lastInst = ch.inst;
+            M = load_mat(p.world_view + 4ull * ch.inst);
+            outBase = __ldg(&ch.I->outBase);
+            g = geom_of(ch.I);
+        }
         const float* sp = s_pos[slot];
-        const uint64_t outBase = __ldg(&ch.I->outBase);
         for (uint32_t v = ch.v0 + threadIdx.x; v < ch.v1; v += THREADS) {
             V3 q;
             if (ch.src) {
@@ -130,69 +139,206 @@ __global__ void __launch_bounds__(THREADS, VX_MIN_BLOCKS) k_vertex(const CrFrame
                 p.outcodes[outBase + v] = (uint8_t)vertex_outcode(M, q, fa, p.f);
         }
         __syncthreads();  // every read of this slot is done: refill it
-        const uint64_t nk = k + (uint64_t)STAGES * gridDim.x;
-        if (nk < nChunks) {
-            const VxChunk nx = vx_chunk(p, nk);
-            if (nx.src) {
-                pending |= bit;
-                if (threadIdx.x == 0) {
+        if (threadIdx.x == 0) {
+            const uint64_t nk = k + (uint64_t)STAGES * gridDim.x;
+            if (nk < nChunks) {
+                s_ch[slot] = vx_chunk(p, nk);
+                if (s_ch[slot].src) {
+                    pending |= bit;
                     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                    bulk_load(s_pos[slot], nx.src, BYTES, &s_bar[slot]);
+                    bulk_load(s_pos[slot], s_ch[slot].src, BYTES, &s_bar[slot]);
                 }
             }
         }
     }
-    // only after a timeout can copies still be in flight: wait for them
-    // (bounded) so none lands in shared memory after the block has exited
-    for (int s = 0; s < STAGES; ++s)
-        if (pending & (1u << s)) (void)mbar_wait_bounded(&s_bar[s], (parity >> s) & 1u, p.waitTimeoutNs);
+    // only after a timeout can copies still be in flight: thread 0, which
+    // issued them, waits for them (bounded) so none lands in shared memory
+    // after the block has exited
+    if (threadIdx.x == 0)
+        for (int s = 0; s < STAGES; ++s)
+            if (pending & (1u << s)) (void)mbar_wait_bounded(&s_bar[s], (parity >> s) & 1u, p.waitTimeoutNs);
 }
 
-// Frame cull, before the vertex pass; one thread per vertex-pass chunk, then
-// one per stage-1 work item.
-//   chunks  a chunk whose box proves CR_OC_* bits for every vertex
-//           (classify_chunk: exact "behind", a sound subset of the sides) gets
-//           those bits as its class (chunkClass), the record all its vertices
-//           share, without its positions being read; so does (with outcode
-//           records) a chunk wholly inside the frustum, whose every outcode is
-//           0; the others get CR_CHUNK_EVAL and are listed for the vertex
-//           pass, which writes their per-vertex records.
-//   items   the item's box is classified for each instance of its chunk; an
-//           instance whose box is wholly behind or beyond one side has every
-//           triangle of the item culled by the reference's own tests
-//           (tv.cu:110-119); without vertex records (CR_REC_BOXES) so has one
-//           whose box provably misses every sample (box_misses_samples,
-//           tv.cu:153-158).  Items with a surviving instance are appended
-//           (warp-aggregated) with the mask of those instances.
-// Skipping what the boxes prove cannot change the visbuffer.
+// Frame cull, before the vertex pass, in two levels.  Every box is an
+// object-space box classified per instance for this view (classify_box:
+// exact "behind", a sound subset of the sides, and "wholly inside").
+//
+// k_cull_groups, one thread per group:
+//   chunk groups  CR_GROUP consecutive vertex-pass chunks of one instance; a
+//                 group box wholly behind or beyond one side gives every
+//                 chunk of the group those outcode bits as its class
+//                 (chunkClass: the record all its vertices share) without
+//                 any chunk box being read; the others are listed, with a
+//                 flag when the group box is wholly inside
+//   units         CR_GROUP consecutive work items of one instance chunk; the
+//                 unit lists the instances whose group box is not proven
+//                 culled (and those for which it is wholly inside)
+// k_cull, one warp per listed group (a lane per member):
+//   chunks        a chunk whose box proves CR_OC_* bits for every vertex gets
+//                 those bits as its class, without its positions being read;
+//                 so does (with outcode records) a chunk wholly inside the
+//                 frustum, whose every outcode is 0; the others get
+//                 CR_CHUNK_EVAL and are listed for the vertex pass, which
+//                 writes their per-vertex records
+//   items         the item's box is classified for each listed instance of
+//                 its unit; an instance whose box is wholly behind or beyond
+//                 one side has every triangle of the item culled by the
+//                 reference's own tests (tv.cu:110-119); so has one whose box
+//                 provably misses every sample (box_misses_samples,
+//                 tv.cu:153-158).  Items with a surviving instance are
+//                 appended (warp-aggregated) with the mask of those instances.
+// Skipping what the boxes prove cannot change the visbuffer; the two levels
+// let a frame whose camera sees a small part of a large mesh classify a box
+// per group of 32 instead of one per item and chunk.
 // The class of a chunk whose every record is 0 (wholly inside).
 constexpr uint32_t CR_FILL_ZERO = 0x100u;
+
+__device__ __forceinline__ uint32_t instance_of_cgroup(const CrFrameParams& p, uint64_t g) {
+    uint32_t lo = 0, hi = p.numInstances - 1;  // instance holding chunk group g
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (__ldg(&p.instances[mid].cgBase) <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+struct Unit {
+    uint32_t seg, chunk, group;
+};
+
+__device__ __forceinline__ Unit decode_unit(const CrFrameParams& p, uint64_t u) {
+    uint32_t lo = 0, hi = p.numSegments - 1;  // last segment whose unitBase <= u
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (__ldg(&p.segments[mid].unitBase) <= u) lo = mid;
+        else hi = mid - 1;
+    }
+    Unit r;
+    r.seg = lo;
+    const uint32_t ng = (__ldg(&p.segments[lo].numBatches) + CR_GROUP - 1) / CR_GROUP;
+    const uint64_t rem = u - __ldg(&p.segments[lo].unitBase);
+    r.chunk = (uint32_t)(rem / ng);
+    r.group = (uint32_t)(rem - (uint64_t)r.chunk * ng);
+    return r;
+}
+
+__device__ __forceinline__ void load_box(const float* bx, float (&lo)[3], float (&hi)[3]) {
+    lo[0] = __ldg(bx), lo[1] = __ldg(bx + 1), lo[2] = __ldg(bx + 2);
+    hi[0] = __ldg(bx + 3), hi[1] = __ldg(bx + 4), hi[2] = __ldg(bx + 5);
+}
+
+// Warp-aggregated append of `val` for the lanes with `want` to list[counter].
+template <typename T>
+__device__ __forceinline__ void list_append(unsigned long long* counter, T* list, uint64_t cap, bool want, T val) {
+    const int lane = threadIdx.x & 31;
+    const unsigned m = __ballot_sync(FULL, want);
+    if (!m) return;
+    const int leader = __ffs(m) - 1;
+    unsigned long long b = 0;
+    if (lane == leader) b = atomicAdd(counter, (unsigned long long)__popc(m));
+    b = __shfl_sync(FULL, b, leader);
+    if (want) {
+        const uint64_t q = b + __popc(m & ((1u << lane) - 1u));
+        if (q < cap) list[q] = val;
+    }
+}
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) k_cull_groups(const CrFrameParams p) {
+    pdl_enter();
+    const float fa = p.f / p.aspect;
+    const uint64_t stride = (uint64_t)gridDim.x * THREADS;
+    const uint64_t nGroups = p.chunkList ? p.numChunkGroups : 0;
+    for (uint64_t base = (uint64_t)blockIdx.x * THREADS; base < nGroups; base += stride) {
+        const uint64_t g = base + threadIdx.x;
+        bool keep = false, inside = false;
+        if (g < nGroups) {
+            const uint32_t inst = instance_of_cgroup(p, g);
+            const CrInstance* I = p.instances + inst;
+            const uint32_t c0 = (uint32_t)(g - __ldg(&I->cgBase)) * CR_GROUP;
+            const uint32_t nc = min((uint32_t)CR_GROUP, (__ldg(&I->numVertices) + CR_VCHUNK - 1) / CR_VCHUNK - c0);
+            const float* gb = ldg_ptr(&I->chunkGroupBoxes);
+            uint32_t c = 0;
+            if (gb) {
+                float lo[3], hi[3];
+                load_box(gb + 6ull * (g - __ldg(&I->cgBase)), lo, hi);
+                c = classify_box(load_mat(p.world_view + 4ull * inst), fa, p.f, lo, hi);
+            }
+            if (c & CR_OC_MASK) {  // every chunk of the group: the group's bits
+                uint8_t* cls = p.chunkClass + __ldg(&I->vchunkBase) + c0;
+                for (uint32_t j = 0; j < nc; ++j) cls[j] = (uint8_t)(c & CR_OC_MASK);
+            } else {
+                keep = true;
+                inside = (c & CH_INSIDE) != 0u;
+            }
+        }
+        list_append(&p.counters[CR_CTR_CGROUPS], p.cgroupList, p.numChunkGroups, keep,
+                    make_uint2((uint32_t)g, inside ? 1u : 0u));
+    }
+    if (!p.itemList) return;
+    for (uint64_t base = (uint64_t)blockIdx.x * THREADS; base < p.numUnits; base += stride) {
+        const uint64_t u = base + threadIdx.x;
+        uint32_t alive = 0, insideM = 0;
+        if (u < p.numUnits) {
+            const Unit un = decode_unit(p, u);
+            const CrSegment* sg = p.segments + un.seg;
+            const uint32_t first = __ldg(&sg->firstInstance);
+            const uint32_t ib = first + un.chunk * CR_INST_CHUNK;
+            const uint32_t ie = min(ib + CR_INST_CHUNK, first + __ldg(&sg->instanceCount));
+            const float* gbx = ldg_ptr(&sg->groupBoxes);
+            float lo[3], hi[3];
+            if (gbx) load_box(gbx + 6ull * un.group, lo, hi);
+            for (uint32_t inst = ib; inst < ie; ++inst) {
+                const uint32_t bit = 1u << (inst - ib);
+                // the instance's whole-mesh class, from the host, first
+                const uint32_t mc = __ldg(&p.instances[inst].meshClass);
+                if (mc & CR_OC_MASK) continue;
+                if (mc & CR_MESH_INSIDE) {
+                    alive |= bit;
+                    insideM |= bit;
+                    continue;
+                }
+                if (!gbx) {
+                    alive |= bit;
+                    continue;
+                }
+                const uint32_t c = classify_box(load_mat(p.world_view + 4ull * inst), fa, p.f, lo, hi);
+                if (c & CR_OC_MASK) continue;
+                alive |= bit;
+                if (c & CH_INSIDE) insideM |= bit;
+            }
+        }
+        list_append(&p.counters[CR_CTR_UNITS], p.unitList, p.numUnits, alive != 0u,
+                    make_uint2((uint32_t)u, alive | (insideM << 16)));
+    }
+}
 
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS, 3) k_cull(const CrFrameParams p) {
     pdl_enter();
+    constexpr int WARPS = THREADS / 32;
     const int lane = threadIdx.x & 31;
     const float fa = p.f / p.aspect;
-    const uint64_t stride = (uint64_t)gridDim.x * THREADS;
-    const uint64_t nChunks = p.chunkList ? p.numVChunks : 0;
-    for (uint64_t base = (uint64_t)blockIdx.x * THREADS; base < nChunks; base += stride) {
-        const uint64_t g = base + threadIdx.x;
+    const uint64_t gw = (uint64_t)blockIdx.x * WARPS + (threadIdx.x >> 5);
+    const uint64_t nw = (uint64_t)gridDim.x * WARPS;
+    // chunks of the listed chunk groups, a lane per chunk
+    const uint64_t nGroups = p.chunkList ? min((uint64_t)p.counters[CR_CTR_CGROUPS], p.numChunkGroups) : 0;
+    for (uint64_t k = gw; k < nGroups; k += nw) {
+        const uint2 e = __ldg(&p.cgroupList[k]);
+        const uint32_t inst = instance_of_cgroup(p, e.x);
+        const CrInstance* I = p.instances + inst;
+        const uint32_t cIdx = (uint32_t)(e.x - __ldg(&I->cgBase)) * CR_GROUP + lane;
+        const bool valid = cIdx < (__ldg(&I->numVertices) + CR_VCHUNK - 1) / CR_VCHUNK;
         uint32_t cls = 0;
-        if (g < nChunks) {
-            uint32_t lo = 0, hi = p.numInstances - 1;  // instance holding chunk g
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi + 1) >> 1;
-                if (__ldg(&p.instances[mid].vchunkBase) <= g) lo = mid;
-                else hi = mid - 1;
-            }
-            const CrInstance* I = p.instances + lo;
-            const uint64_t cIdx = g - __ldg(&I->vchunkBase);
+        if (valid) {
             const float* cb = ldg_ptr(&I->chunkBoxes);
-            if (cb) {
-                const float* bx = cb + 6ull * cIdx;
-                const float blo[3] = {__ldg(bx), __ldg(bx + 1), __ldg(bx + 2)};
-                const float bhi[3] = {__ldg(bx + 3), __ldg(bx + 4), __ldg(bx + 5)};
-                const uint32_t c = classify_box(load_mat(p.world_view + 4ull * lo), fa, p.f, blo, bhi);
+            if (e.y) {  // the group box is wholly inside: so is every chunk
+                if (p.cellMode == CR_REC_OUTCODES) cls = CR_FILL_ZERO;
+            } else if (cb) {
+                float lo[3], hi[3];
+                load_box(cb + 6ull * cIdx, lo, hi);
+                const uint32_t c = classify_box(load_mat(p.world_view + 4ull * inst), fa, p.f, lo, hi);
                 // wholly behind / beyond a side: those outcode bits at every
                 // vertex; wholly inside: outcode 0 at every vertex (1-byte
                 // records only: cell records also need each vertex's cell)
@@ -200,69 +346,55 @@ __global__ void __launch_bounds__(THREADS, 3) k_cull(const CrFrameParams p) {
                 else if ((c & CH_INSIDE) && p.cellMode == CR_REC_OUTCODES) cls = CR_FILL_ZERO;
             }
         }
-        // the chunk's class: the record every vertex of a classified chunk
-        // has (its positions are never read), or CR_CHUNK_EVAL
-        if (g < nChunks) p.chunkClass[g] = (uint8_t)(cls == 0 ? CR_CHUNK_EVAL : (cls & CR_OC_MASK));
+        const uint64_t g = __ldg(&I->vchunkBase) + cIdx;
+        if (valid) p.chunkClass[g] = (uint8_t)(cls == 0 ? CR_CHUNK_EVAL : (cls & CR_OC_MASK));
         // chunks that need per-vertex records, listed for the vertex pass
-        const bool eval = g < nChunks && cls == 0;
-        const unsigned m = __ballot_sync(FULL, eval);
-        if (m) {
-            const int leader = __ffs(m) - 1;
-            unsigned long long b = 0;
-            if (lane == leader) b = atomicAdd(&p.counters[CR_CTR_CHUNKS], (unsigned long long)__popc(m));
-            b = __shfl_sync(FULL, b, leader);
-            if (eval) p.chunkList[b + __popc(m & ((1u << lane) - 1u))] = (uint32_t)g;
-        }
+        list_append(&p.counters[CR_CTR_CHUNKS], p.chunkList, p.numVChunks, valid && cls == 0, (uint32_t)g);
     }
     if (!p.itemList) return;
+    // items of the listed units, a lane per item
     const double invW = 1.0 / (double)p.W, invH = 1.0 / (double)p.H;
-    for (uint64_t base = (uint64_t)blockIdx.x * THREADS; base < p.numItems; base += stride) {
-        const uint64_t item = base + threadIdx.x;
+    const uint64_t nUnits = min((uint64_t)p.counters[CR_CTR_UNITS], p.numUnits);
+    for (uint64_t k = gw; k < nUnits; k += nw) {
+        const uint2 e = __ldg(&p.unitList[k]);
+        const uint32_t alive = e.y & 0xffffu, insideU = e.y >> 16;
+        const Unit un = decode_unit(p, e.x);
+        const CrSegment* sg = p.segments + un.seg;
+        const uint32_t nb = __ldg(&sg->numBatches);
+        const uint32_t batch = un.group * CR_GROUP + lane;
+        const bool valid = batch < nb;
+        const uint32_t ib = __ldg(&sg->firstInstance) + un.chunk * CR_INST_CHUNK;
         uint32_t mask = 0;
-        if (item < p.numItems) {
-            const Item it = decode_item(p, item);
-            const CrSegment* sg = p.segments + it.seg;
-            const uint32_t first = __ldg(&sg->firstInstance);
-            const uint32_t ib = first + it.chunk * CR_INST_CHUNK;
-            const uint32_t ie = min(ib + CR_INST_CHUNK, first + __ldg(&sg->instanceCount));
+        if (valid) {
             const float* boxes = ldg_ptr(&sg->itemBoxes);
             if (!boxes) {
-                mask = (1u << (ie - ib)) - 1u;
+                mask = alive | (insideU << 16);
             } else {
-                const float* bx = boxes + 6ull * it.batch;
-                const float blo[3] = {__ldg(bx), __ldg(bx + 1), __ldg(bx + 2)};
-                const float bhi[3] = {__ldg(bx + 3), __ldg(bx + 4), __ldg(bx + 5)};
-                const bool samples = p.cellMode == CR_REC_BOXES;
-                for (uint32_t inst = ib; inst < ie; ++inst) {
-                    // the instance's whole-mesh class, from the host, first
-                    const uint32_t mc = __ldg(&p.instances[inst].meshClass);
-                    if (mc & CR_OC_MASK) continue;
+                float blo[3], bhi[3];
+                load_box(boxes + 6ull * batch, blo, bhi);
+                for (uint32_t rest = alive; rest; rest &= rest - 1) {
+                    const uint32_t slot = __ffs(rest) - 1;
+                    const uint32_t inst = ib + slot;
                     const Mat M = load_mat(p.world_view + 4ull * inst);
-                    bool inside = (mc & CR_MESH_INSIDE) != 0u;
+                    bool inside = ((insideU >> slot) & 1u) != 0u;
                     if (!inside) {
                         const uint32_t c = classify_box(M, fa, p.f, blo, bhi);
                         if (c & CR_OC_MASK) continue;
                         inside = (c & CH_INSIDE) != 0u;
                     }
-                    if (samples && box_misses_samples(M, fa, p.f, p.W, p.H, invW, invH, blo, bhi)) continue;
+                    // the sample-miss proof of the whole item box (for every
+                    // record mode: it culls items of sub-pixel triangles before
+                    // their indices are read)
+                    if (box_misses_samples(M, fa, p.f, p.W, p.H, invW, invH, blo, bhi)) continue;
                     // bit 16 + slot: every vertex of the item is in front of
                     // the camera and inside every side (no chunk it touches
                     // can have been classified culled)
-                    mask |= (1u << (inst - ib)) | (inside ? 1u << (16 + inst - ib) : 0u);
+                    mask |= (1u << slot) | (inside ? 1u << (16 + slot) : 0u);
                 }
             }
         }
-        const unsigned m = __ballot_sync(FULL, mask != 0);
-        if (m) {
-            const int leader = __ffs(m) - 1;
-            unsigned long long b = 0;
-            if (lane == leader) b = atomicAdd(&p.counters[CR_CTR_ITEMS], (unsigned long long)__popc(m));
-            b = __shfl_sync(FULL, b, leader);
-            if (mask) {
-                const uint64_t q = b + __popc(m & ((1u << lane) - 1u));
-                if (q < p.itemCap) p.itemList[q] = make_uint2((uint32_t)item, mask);
-            }
-        }
+        const uint64_t item = __ldg(&sg->itemBase) + (uint64_t)un.chunk * nb + batch;
+        list_append(&p.counters[CR_CTR_ITEMS], p.itemList, p.itemCap, mask != 0u, make_uint2((uint32_t)item, mask));
     }
 }
 
@@ -890,11 +1022,13 @@ int cr_launch_vertex(const CrFrameParams& p, const CrLaunchShape& s, void* strea
 
 int cr_launch_cull(const CrFrameParams& p, const CrLaunchShape& s, void* stream) {
     if (!p.itemList && !p.chunkList) return 0;
-    const uint64_t work = std::max<uint64_t>(p.numItems, p.chunkList ? p.numVChunks : 0);
+    const uint64_t work = std::max<uint64_t>(p.itemList ? p.numUnits : 0, p.chunkList ? p.numChunkGroups : 0);
     if (work == 0) return 0;
     uint64_t blocks = (work + 255) / 256;
     if (blocks > (uint64_t)s.numSMs * 8) blocks = (uint64_t)s.numSMs * 8;
-    return launch_pdl(k_cull<256>, (unsigned)blocks, 256, stream, p);
+    if (launch_pdl(k_cull_groups<256>, (unsigned)blocks, 256, stream, p)) return -1;
+    // one warp per listed group: as many warps as can be resident
+    return launch_pdl(k_cull<256>, (unsigned)(s.numSMs * 3), 256, stream, p);
 }
 
 // Box-culled frames: k_stage1.  Record-culled frames: k_s1cull (items ->

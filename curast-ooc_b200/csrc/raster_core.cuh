@@ -145,14 +145,17 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
         : "memory");
 }
 
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+// One wait of at most about suspend_ns: the thread is suspended (it issues
+// nothing) until the phase completes or the hint runs out, so waiting warps
+// leave the issue slots to the working ones.
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity, uint32_t suspend_ns = 20000u) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(smem_addr(bar)), "r"(parity)
+        : "r"(smem_addr(bar)), "r"(parity), "r"(suspend_ns)
         : "memory");
     return ok != 0;
 }
@@ -198,22 +201,26 @@ __device__ __forceinline__ bool ndc_beyond(float X, float d) {
 }
 
 // The render target of one view: visbuffer, size and projection.
+// idBase: the first global id of the view's instance set; the view's
+// visbuffer holds ids relative to it (0 in single-view frames).
 struct Target {
     uint64_t* fb;
     int32_t W, H;
     float f, fa;  // proj[1][1] and f / aspect
     uint32_t thrSmall;
+    uint64_t idBase;
 };
 
 __device__ __forceinline__ Target target_of(const CrFrameParams& p) {
-    return Target{p.fb, p.W, p.H, p.f, p.f / p.aspect, p.thrSmall};
+    return Target{p.fb, p.W, p.H, p.f, p.f / p.aspect, p.thrSmall, 0ull};
 }
 
 __device__ __forceinline__ Target target_of(const CrFrameParams& p, uint32_t view) {
     // fa is f / aspect rounded once in float on the host: the same value
     // target_of(p) forms on the device
     const CrView* v = p.views + view;
-    return Target{ldg_ptr(&v->fb), __ldg(&v->W), __ldg(&v->H), __ldg(&v->f), __ldg(&v->fa), p.thrSmall};
+    return Target{ldg_ptr(&v->fb), __ldg(&v->W), __ldg(&v->H), __ldg(&v->f), __ldg(&v->fa), p.thrSmall,
+                  __ldg(&v->idBase)};
 }
 
 // With COOP the tiny raster is not run here: its setup goes to *coop and
@@ -222,6 +229,9 @@ template <bool COOP = false>
 __device__ __forceinline__ int stage1_triangle(const Target& p, const float fa, const Mat& M,
                                                const uint32_t flip, const V3 pa, const V3 pb, const V3 pc,
                                                const uint64_t id, S1Raster* coop = nullptr) {
+    // flip bit 1: the instance is not drawn in this view (batched frames of
+    // several instance sets; its matrix also puts it behind the camera)
+    if (flip & 2u) return S1_CULL;
     const float f = p.f;
     const V3 av = xform(M, pa);
     const V3 bv = xform(M, pb);
@@ -234,7 +244,7 @@ __device__ __forceinline__ int stage1_triangle(const Target& p, const float fa, 
     {  // tv.cu:168-188
         const V3 N = cross3(sub3(bv, av), sub3(cv, av));
         float res = dot3(av, N);
-        if (flip) res = -res;
+        if (flip & 1u) res = -res;
         if (res >= 0.0f) return S1_CULL;
     }
     bool nontrivial = (da <= 0.0f || db <= 0.0f || dc <= 0.0f);
@@ -900,7 +910,7 @@ __device__ __forceinline__ int stage2_setup(const CrFrameParams& p, const Target
     const uint32_t tri = (uint32_t)(packed & 0xffffffffu);
     const CrInstance* I = p.instances + inst;
     // tv.cu:414,424,519: the cumulative count is held in 32 bits
-    const uint32_t cum32 = (uint32_t)__ldg(&I->cum);
+    const uint32_t cum32 = (uint32_t)(__ldg(&I->cum) - t.idBase);
     const Mat M = load_mat(p.world_view + 4ull * ((uint64_t)view * p.numInstances + inst));
     const float fa = t.fa;
     const GeomRef g = geom_of(I);
@@ -1380,7 +1390,7 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_stage3(const CrFrameParams p)
         const V3 cv = xform(M, pos_of(g, i2));
         const V3 e1 = sub3(bv, av);
         const V3 e2 = sub3(cv, av);
-        const uint64_t id = __ldg(&I->cum) + (uint64_t)tri;
+        const uint64_t id = __ldg(&I->cum) - tg.idBase + (uint64_t)tri;
 
         const float min_x = clamp_ref((float)(tile.tile_x * CR_TILE_SIZE), 0.0f, Wf);
         const float min_y = clamp_ref((float)(tile.tile_y * CR_TILE_SIZE), 0.0f, Hf);

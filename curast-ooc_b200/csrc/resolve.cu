@@ -77,7 +77,9 @@ __device__ __forceinline__ void resolve_pixel(const CrResolveParams& p, const in
     // cleared buffer unconditionally, resolve.cu:1134-1140)
     const uint32_t ud = (uint32_t)(pixel >> 33) & 0x7FFFFFF8u;
     const float depth = (ud == 0x7FFFFFF8u || p.numInstances == 0) ? INFINITY : __uint_as_float(ud);
-    const uint64_t tid = pixel & 0xFFFFFFFFFull;
+    // the pixel's id in the frame's global numbering (a batched view of one
+    // of several instance sets holds ids relative to its set's first)
+    const uint64_t tid = (pixel & 0xFFFFFFFFFull) + p.idBase;
 
     if (isinf(depth) ? !p.writeBackground : (tid < p.idLo || tid >= p.idHi)) return;  // another pass owns it
     uint32_t color = 0;
@@ -241,6 +243,7 @@ __global__ void __launch_bounds__(256) k_resolve_views(const CrResolveParams bas
         s_p.origin[2] = __ldg(&v->origin[2]);
         s_p.p00 = __ldg(&v->p00);
         s_p.p11 = __ldg(&v->p11);
+        s_p.idBase = __ldg(&v->idBase);
     }
     if (t < 16) s_p.viewI[t] = __ldg(&v->viewI[t]);
     if (t >= 16 && t < 32) s_p.view[t - 16] = __ldg(&v->view[t - 16]);

@@ -336,7 +336,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_stage1_views(const CrFrame
                         const V3 pa = pos_of(geo, index_of(tp, 0));
                         const V3 pb = pos_of(geo, index_of(tp, 1));
                         const V3 pc = pos_of(geo, index_of(tp, 2));
-                        res = stage1_triangle(tg, tg.fa, M, flip, pa, pb, pc, cum + tri);
+                        res = stage1_triangle(tg, tg.fa, M, flip, pa, pb, pc, cum - tg.idBase + tri);
                     }
                     const unsigned qmask = __ballot_sync(FULL, res == S1_QUEUE);
                     if (qmask) {  // warp-aggregated append, tv.cu:190-197, tagged with the view
@@ -734,7 +734,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_stage1_views_lists(const C
                     const V3 pb = pos_of(geo, index_of(tp, 1));
                     const V3 pc = pos_of(geo, index_of(tp, 2));
                     res = stage1_triangle(tg, tg.fa, load_mat(p.world_view + 4ull * vi), __ldg(p.flips + vi), pa, pb,
-                                          pc, __ldg(&p.instances[inst].cum) + tri);
+                                          pc, __ldg(&p.instances[inst].cum) - tg.idBase + tri);
                 }
                 qh = min(qh + 32u, qt);
                 const unsigned qmask = __ballot_sync(FULL, res == S1_QUEUE);
@@ -801,7 +801,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_stage1_views_lists(const C
                             const V3 pa = pos_of(geo, index_of(tp, 0));
                             const V3 pb = pos_of(geo, index_of(tp, 1));
                             const V3 pc = pos_of(geo, index_of(tp, 2));
-                            res = stage1_triangle(tg, tg.fa, M, flip, pa, pb, pc, cum + tri0 + tp);
+                            res = stage1_triangle(tg, tg.fa, M, flip, pa, pb, pc, cum - tg.idBase + tri0 + tp);
                         }
                         const unsigned qmask = __ballot_sync(FULL, res == S1_QUEUE);
                         if (qmask) {

@@ -320,6 +320,8 @@ EXPORTS = {
                                  _i32, ctypes.c_void_p]),
     "cr_render_batch": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrInstance), _u32, ctypes.POINTER(CrView), _u32, _i32,
                                _u32, ctypes.c_void_p]),
+    "cr_render_batch_sets": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrInstance), ctypes.c_void_p, _u32,
+                                    ctypes.POINTER(CrView), ctypes.c_void_p, _u32, _i32, _u32, ctypes.c_void_p]),
     "cr_batch_plan_create": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrInstance), _u32, ctypes.POINTER(CrView), _u32,
                                     _i32, _u32, ctypes.POINTER(ctypes.c_void_p)]),
     "cr_batch_plan_set_cameras": (_i32, [ctypes.c_void_p, ctypes.POINTER(CrCamera), _u32]),
@@ -866,6 +868,17 @@ class Context:
         varr, nv = make_views(views)
         _check(load().cr_render_batch(self.h, arr, n, varr, nv, int(display), int(flags),
                                       ctypes.c_void_p(int(stream))))
+
+    def render_batch_sets(self, sets, views, view_sets, display=CR_DISPLAY_VERTEX_COLORS, flags=CR_RENDER_SYNC,
+                          stream=0):
+        """sets: list of instance lists; view_sets[v]: the set view v renders."""
+        flat = [x for st in sets for x in st]
+        arr, n = make_instances(flat)
+        sizes = np.ascontiguousarray([len(st) for st in sets], np.uint32)
+        vs = np.ascontiguousarray(view_sets, np.uint32)
+        varr, nv = make_views(views)
+        _check(load().cr_render_batch_sets(self.h, arr, sizes.ctypes.data, len(sets), varr, vs.ctypes.data, nv,
+                                           int(display), int(flags), ctypes.c_void_p(int(stream))))
 
     def autotune_batch(self, instances, views, tune_flags=0):
         arr, n = make_instances(instances) if not isinstance(instances, tuple) else instances

@@ -334,6 +334,16 @@ cr_status cr_render_batch(cr_context* ctx, const cr_instance* instances, uint32_
                           const cr_view* views, uint32_t num_views, int32_t display,
                           uint32_t flags, void* stream);
 
+/* Several instance sets (scenes) in one batched frame, the same launches as
+ * cr_render_batch: `instances` holds set 0's set_sizes[0] instances, then
+ * set 1's, and so on; view v renders set view_sets[v] only, and its
+ * visbuffer and colour are bit-identical to cr_render of that set's
+ * instances alone (the set's own instance order and triangle ids).
+ * Geometry shared by several sets is read once. */
+cr_status cr_render_batch_sets(cr_context* ctx, const cr_instance* instances, const uint32_t* set_sizes,
+                               uint32_t num_sets, const cr_view* views, const uint32_t* view_sets,
+                               uint32_t num_views, int32_t display, uint32_t flags, void* stream);
+
 /* A batched frame captured once as a CUDA graph: frame-table upload, clear,
  * vertex pass, stages 1-3, resolve and counter readback replay with one
  * cudaGraphLaunch.  The plan owns its queues, records and tables, so plans

@@ -228,3 +228,28 @@ def test_batched_displays_match_plain(ctx, display):
     cams = scenes.batch_cameras(7, seed=91, scale=0.1)
     assert_views_equal(batched(ctx, inst, cams, display=display), plain_loop(ctx, inst, cams, display=display),
                        f"display {display}")
+
+
+def test_instance_sets_in_one_batch(ctx):
+    """Several instance sets (scenes) in one batched frame: every view
+    equals cr_render of its own set alone -- that set's instance order and
+    triangle ids, nothing of the other sets -- with views of every set
+    interleaved and a mesh shared by two sets."""
+    h, keep = small_terrain(ctx, n=80)
+    hs = ctx.mesh_from_host(*scenes.triangle_soup(3000, seed=19, near_fraction=0.03))
+    hh = ctx.mesh_from_host(*scenes.heightfield(nx=40, nz=20, seed=7))
+    sets = [[(h, scenes.identity())],
+            [(hs, scenes.translate_scale(2.0, 0.5, 2.0, 0.8)), (hh, scenes.translate_scale(1.0, 0.2, 1.0, 3.0)),
+             (hs, scenes.translate_scale(3.0, 0.4, 1.0, 0.5))],
+            [(hh, scenes.identity()), (h, scenes.translate_scale(0.5, 0.0, 0.5, 0.5))]]
+    cams = scenes.batch_cameras(9, seed=77, scale=0.1)
+    view_sets = [k % 3 for k in range(len(cams))]
+    t = Targets(cams, colorbuffer=True)
+    t.fill()
+    ctx.render_batch_sets(sets, t.views(), view_sets)
+    got = t.host()
+    for k in range(len(cams)):
+        alone = plain_loop(ctx, sets[view_sets[k]], [cams[k]], colorbuffer=True)
+        assert_views_equal(([got[0][k]], [got[1][k]], [got[2][k]]), alone, f"view {k} (set {view_sets[k]})")
+    covered = [(v != pc.CLEAR_PIXEL).mean() for v in got[0]]
+    assert min(covered) > 0.01

@@ -426,12 +426,13 @@ def test_resolve_displays(ctx, display):
     """Every display of the reference's resolve that needs no textures:
     against the oracle and the reference kernels (IEEE build).  Integer
     colours (ids, stage colours) are exact; the face normal within 1."""
-    soup = scenes.triangle_soup(30000, seed=101, near_fraction=0.01)
-    hf = scenes.heightfield(nx=48, nz=24, seed=41)
-    meshes = [soup, hf]
-    inst = [(0, scenes.identity()), (1, scenes.translate_scale(-0.5, -0.8, -2.5, 1.5))]
+    hf = scenes.heightfield(nx=96, nz=48, seed=41)
+    soup = scenes.triangle_soup(4000, seed=101, near_fraction=0.02)
+    meshes = [hf, soup]
+    inst = [(0, scenes.identity()), (1, scenes.translate_scale(0.5, 0.05, -0.3, 0.05)),
+            (0, scenes.translate_scale(0.55, 0.06, 0.15, 0.3))]
     W, H = 480, 270
-    view, proj = scenes.identity(), scenes.perspective(60.0, W / H)
+    view, proj = scenes.heightfield_camera(W, H)
     vis, rgba, cb, stats = render_ours(ctx, meshes, inst, view, proj, W, H, display=display)
     ovis, orgba, ocb, ost = render_oracle(meshes, inst, view, proj, W, H, display=display)
     assert ost.stage1_direct > 0 and ost.nontrivial > 0 and ost.huge_tiles > 0
