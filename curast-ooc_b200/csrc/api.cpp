@@ -795,13 +795,17 @@ cr_status upload_parallel(cr_context* ctx, const std::vector<CopyJob>& jobs) {
         char* dst;
         const char* src;
         size_t n;
+        const CopyJob* job;
+        uint64_t off;
     };
     std::vector<Piece> pieces;
-    for (const CopyJob& j : jobs)
-        for (size_t o = 0; o < j.bytes; o += kHalf)
-            pieces.push_back({(char*)j.dst + o, (const char*)j.src + o, std::min(kHalf, j.bytes - o)});
+    for (const CopyJob& j : jobs) {
+        const size_t step = kHalf - kHalf % std::max<size_t>(j.unit, 1);
+        for (size_t o = 0; o < j.bytes; o += step)
+            pieces.push_back({(char*)j.dst + o, (const char*)j.src + o, std::min(step, j.bytes - o), &j, o});
+    }
     std::atomic<size_t> next{0};
-    std::atomic<int> failed{0};
+    std::atomic<int> failed{0};  // 1: CUDA, 2: a source failed to convert
     auto worker = [&](cr_context::Stager& st) {
         if (cudaSetDevice(ctx->device) != cudaSuccess) failed = 1;
         bool used[2] = {false, false};
@@ -809,7 +813,14 @@ cr_status upload_parallel(cr_context* ctx, const std::vector<CopyJob>& jobs) {
         for (size_t k; !failed && (k = next.fetch_add(1)) < pieces.size(); half ^= 1) {
             uint8_t* buf = st.host + half * kHalf;
             if (used[half] && cudaEventSynchronize(st.done[half]) != cudaSuccess) failed = 1;
-            memcpy(buf, pieces[k].src, pieces[k].n);
+            if (pieces[k].job->fill) {
+                if (!pieces[k].job->fill(pieces[k].off, pieces[k].n, buf)) {
+                    failed = 2;
+                    break;
+                }
+            } else {
+                memcpy(buf, pieces[k].src, pieces[k].n);
+            }
             if (cudaMemcpyAsync(pieces[k].dst, buf, pieces[k].n, cudaMemcpyHostToDevice, st.stream) != cudaSuccess ||
                 cudaEventRecord(st.done[half], st.stream) != cudaSuccess)
                 failed = 1;
@@ -822,6 +833,7 @@ cr_status upload_parallel(cr_context* ctx, const std::vector<CopyJob>& jobs) {
     for (size_t i = 1; i < nw; i++) pool.emplace_back(worker, std::ref(ctx->stagers[i]));
     worker(ctx->stagers[0]);
     for (auto& t : pool) t.join();
+    if (failed == 2) return fail(CR_ERR_INVALID, "bulk upload: a source could not be converted");
     if (failed) return fail(CR_ERR_CUDA, "bulk upload: %s", cudaGetErrorString(cudaGetLastError()));
     return CR_OK;
 }

@@ -74,6 +74,11 @@ struct CopyJob {
     void* dst;
     const void* src;
     size_t bytes;
+    // a source produced on the fly (instead of src): fill(offset, n, buf)
+    // writes bytes [offset, offset + n) of the job into buf and returns false
+    // if the source cannot be converted; pieces are whole multiples of `unit`
+    std::function<bool(uint64_t, uint64_t, void*)> fill = nullptr;
+    size_t unit = 1;
 };
 // Device buffers of an owned mesh of nV vertices and nT triangles (positions,
 // indices padded to whole 384-byte tiles with the padding zeroed, colours),

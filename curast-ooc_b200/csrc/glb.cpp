@@ -279,6 +279,88 @@ bool vec3_of(const JVal* v, float* out) {
 
 cr_status glb_fail(const char* msg) { return fail(CR_ERR_INVALID, "glb: %s", msg); }
 
+// One primitive's validated accessors: what its conversion reads.
+struct GlbTask {
+    Acc pos, idx, col;
+    bool hasIdx = false;
+    int colMode = 0;  // 0 none, 1 stored RGBA8 bytes, 2 VEC3 float
+    bool hasBox = false;
+};
+
+// The conversions of one primitive, on element ranges so that a file can be
+// converted whole (cr_glb_open) or chunk by chunk into staging buffers
+// (cr_glb_open_file_streamed); both give the same values.
+// positions [v0, v1): float xyz, the bufferView's byteStride honoured
+void conv_positions(const GlbTask& t, uint64_t v0, uint64_t v1, float* dst) {
+    if (t.pos.stride == 12) {
+        memcpy(dst, t.pos.base + 12 * v0, 12 * (v1 - v0));
+    } else {
+        for (uint64_t v = v0; v < v1; v++) memcpy(dst + 3 * (v - v0), t.pos.base + v * t.pos.stride, 12);
+    }
+}
+
+// index positions [i0, i1), widened to 32 bits; false if one of them is not
+// below nv (an index beyond the primitive's vertices)
+bool conv_indices(const GlbTask& t, uint64_t i0, uint64_t i1, uint32_t nv, uint32_t* out) {
+    const uint8_t* q = t.idx.base;
+    const uint64_t n = i1 - i0;
+    uint32_t hi = 0;
+    if (t.idx.ct == CT_U32) {  // copied and range-checked in one pass
+        const uint64_t n8 = n & ~7ull;
+        uint32_t h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (uint64_t i = 0; i < n8; i += 8)
+            for (int l = 0; l < 8; l++) {
+                const uint32_t v = rd<uint32_t>(q + 4 * (i0 + i + l));
+                out[i + l] = v;
+                h[l] = std::max(h[l], v);
+            }
+        for (uint64_t i = n8; i < n; i++) {
+            out[i] = rd<uint32_t>(q + 4 * (i0 + i));
+            hi = std::max(hi, out[i]);
+        }
+        for (int l = 0; l < 8; l++) hi = std::max(hi, h[l]);
+    } else if (t.idx.ct == CT_U16) {
+        for (uint64_t i = 0; i < n; i++) {
+            out[i] = rd<uint16_t>(q + 2 * (i0 + i));
+            hi = std::max(hi, out[i]);
+        }
+    } else {
+        for (uint64_t i = 0; i < n; i++) {
+            out[i] = q[i0 + i];
+            hi = std::max(hi, out[i]);
+        }
+    }
+    return !(n && hi >= nv);
+}
+
+// colours [v0, v1) as the loader converts them
+void conv_colors(const GlbTask& t, uint64_t v0, uint64_t v1, uint32_t* out) {
+    if (t.colMode == 1) {
+        memcpy(out, t.col.base + 4 * v0, 4 * (v1 - v0));
+        return;
+    }
+    for (uint64_t v = v0; v < v1; v++) {
+        float c[3];
+        memcpy(c, t.col.base + v * t.col.stride, 12);
+        uint32_t rgba = 0xff000000u;
+        for (int ch = 0; ch < 3; ch++) {
+            float x = c[ch];
+            while (x > 1.0f) x = x / 256.0f;
+            rgba |= (uint32_t)byte_of(x) << (8 * ch);
+        }
+        out[v - v0] = rgba;
+    }
+}
+
+// the box of positions [v0, v1) merged into box (min xyz, max xyz)
+void extend_box(const float* pos, uint64_t n, float* box) {
+    for (uint64_t v = 0; v < n; v++)
+        for (int j = 0; j < 3; j++) {
+            box[j] = std::min(box[j], pos[3 * v + j]);
+            box[3 + j] = std::max(box[3 + j], pos[3 * v + j]);
+        }
+}
+
 }  // namespace
 
 // A vector whose resize leaves new elements uninitialised: every mesh array
@@ -342,6 +424,12 @@ struct cr_glb {
         float box[6];
     };
     std::vector<std::vector<Piece>> pieces;  // per mesh
+    // streamed files (cr_glb_open_file_streamed): the file stays mapped and
+    // each primitive's accessors are kept; nothing is converted up front
+    const uint8_t* map = nullptr;
+    size_t mapSize = 0;
+    std::vector<GlbTask> tasks;
+    bool streamed() const { return map != nullptr; }
     uint8_t* arena = nullptr;
     bool arenaPinned = false;
     uint32_t piecesMax = 0, piecesFlags = 0;
@@ -355,12 +443,17 @@ struct cr_glb {
         arenaPinned = false;
         pieces.clear();
     }
-    ~cr_glb() { free_arena(); }
+    ~cr_glb() {
+        free_arena();
+        if (map) munmap(const_cast<uint8_t*>(map), mapSize);
+    }
 };
 
 namespace {
 
-cr_status parse(cr_glb& g, const uint8_t* d, uint64_t size) {
+// convertNow false: validate and keep every primitive's accessors (the file
+// stays mapped: streamed); true: convert every primitive into host arrays.
+cr_status parse(cr_glb& g, const uint8_t* d, uint64_t size, bool convertNow = true) {
     if (size < 20 || rd<uint32_t>(d) != 0x46546C67u) return glb_fail("not a binary glTF (magic)");
     if (rd<uint32_t>(d + 4) != 2) return glb_fail("glTF version is not 2");
     const uint64_t total = std::min<uint64_t>(rd<uint32_t>(d + 8), size);
@@ -403,12 +496,7 @@ cr_status parse(cr_glb& g, const uint8_t* d, uint64_t size) {
 
     // ---- meshes: one per primitive --------------------------------------------
     // validated here, converted below in parallel (one primitive per task)
-    struct Task {
-        Acc pos, idx, col;
-        bool hasIdx = false;
-        int colMode = 0;  // 0 none, 1 stored RGBA8 bytes, 2 VEC3 float
-        bool hasBox = false;
-    };
+    using Task = GlbTask;
     std::vector<Task> tasks;
     std::vector<std::pair<uint32_t, uint32_t>> meshRange;  // glTF mesh -> [first, end)
     if (const JVal* ms = root.arrOf("meshes"))
@@ -466,74 +554,28 @@ cr_status parse(cr_glb& g, const uint8_t* d, uint64_t size) {
         cr_glb::Mesh& m = g.meshes[k];
         const uint64_t nv = m.numVertices;
         m.positions.resize(3 * nv);
-        if (t.pos.stride == 12) {
-            memcpy(m.positions.data(), t.pos.base, 12 * nv);
-        } else {
-            for (uint64_t v = 0; v < nv; v++) memcpy(&m.positions[3 * v], t.pos.base + v * t.pos.stride, 12);
-        }
+        conv_positions(t, 0, nv, m.positions.data());
         if (!t.hasBox) {
             for (int j = 0; j < 3; j++) {
                 m.box[j] = INFINITY;
                 m.box[3 + j] = -INFINITY;
             }
-            for (uint64_t v = 0; v < nv; v++)
-                for (int j = 0; j < 3; j++) {
-                    m.box[j] = std::min(m.box[j], m.positions[3 * v + j]);
-                    m.box[3 + j] = std::max(m.box[3 + j], m.positions[3 * v + j]);
-                }
+            extend_box(m.positions.data(), nv, m.box);
         }
         if (t.hasIdx) {
             const uint64_t n = 3ull * m.numTriangles;
             m.indices.resize(n);
-            uint32_t* out = m.indices.data();
-            const uint8_t* q = t.idx.base;
-            uint32_t hi = 0;
-            if (t.idx.ct == CT_U32) {  // copied and range-checked in one pass
-                const uint64_t n8 = n & ~7ull;
-                uint32_t h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-                for (uint64_t i = 0; i < n8; i += 8)
-                    for (int l = 0; l < 8; l++) {
-                        const uint32_t v = rd<uint32_t>(q + 4 * (i + l));
-                        out[i + l] = v;
-                        h[l] = std::max(h[l], v);
-                    }
-                for (uint64_t i = n8; i < n; i++) {
-                    out[i] = rd<uint32_t>(q + 4 * i);
-                    hi = std::max(hi, out[i]);
-                }
-                for (int l = 0; l < 8; l++) hi = std::max(hi, h[l]);
-            } else if (t.idx.ct == CT_U16) {
-                for (uint64_t i = 0; i < n; i++) {
-                    out[i] = rd<uint16_t>(q + 2 * i);
-                    hi = std::max(hi, out[i]);
-                }
-            } else {
-                for (uint64_t i = 0; i < n; i++) {
-                    out[i] = q[i];
-                    hi = std::max(hi, out[i]);
-                }
-            }
-            if (n && hi >= m.numVertices) return false;  // an index beyond the primitive's vertices
+            if (!conv_indices(t, 0, n, m.numVertices, m.indices.data())) return false;
         }
-        if (t.colMode == 1) {
+        if (t.colMode) {
             m.colors.resize(nv);
-            memcpy(m.colors.data(), t.col.base, 4 * nv);
-        } else if (t.colMode == 2) {
-            m.colors.resize(nv);
-            for (uint64_t v = 0; v < nv; v++) {
-                float c[3];
-                memcpy(c, t.col.base + v * t.col.stride, 12);
-                uint32_t rgba = 0xff000000u;
-                for (int ch = 0; ch < 3; ch++) {
-                    float x = c[ch];
-                    while (x > 1.0f) x = x / 256.0f;
-                    rgba |= (uint32_t)byte_of(x) << (8 * ch);
-                }
-                m.colors[v] = rgba;
-            }
+            conv_colors(t, 0, nv, m.colors.data());
         }
         return true;
     };
+    if (!convertNow) {
+        g.tasks = tasks;
+    } else
     {
         const size_t nthreads = std::min<size_t>({tasks.size(), 16, std::max(1u, std::thread::hardware_concurrency())});
         std::atomic<size_t> next{0};
@@ -758,6 +800,29 @@ cr_status cr_glb_open_file(const char* path, cr_glb** out) {
     return CR_OK;
 }
 
+cr_status cr_glb_open_file_streamed(const char* path, cr_glb** out) {
+    if (!path || !out) return fail(CR_ERR_INVALID, "cr_glb_open_file_streamed: NULL argument");
+    *out = nullptr;
+    const int fd = open(path, O_RDONLY);
+    if (fd < 0) return fail(CR_ERR_NOT_FOUND, "glb: cannot open %s", path);
+    struct stat st;
+    if (fstat(fd, &st) != 0 || st.st_size <= 0) {
+        close(fd);
+        return fail(CR_ERR_INVALID, "glb: cannot read %s", path);
+    }
+    const size_t n = (size_t)st.st_size;
+    void* map = mmap(nullptr, n, PROT_READ, MAP_PRIVATE, fd, 0);
+    close(fd);
+    if (map == MAP_FAILED) return fail(CR_ERR_INVALID, "glb: cannot map %s", path);
+    madvise(map, n, MADV_SEQUENTIAL);
+    std::unique_ptr<cr_glb> g(new cr_glb());
+    g->map = (const uint8_t*)map;  // unmapped by cr_glb_close
+    g->mapSize = n;
+    if (cr_status s = parse(*g, (const uint8_t*)map, n, false)) return s;
+    *out = g.release();
+    return CR_OK;
+}
+
 cr_status cr_glb_counts(const cr_glb* g, uint32_t* num_meshes, uint32_t* num_instances) {
     if (!g) return fail(CR_ERR_INVALID, "cr_glb_counts: NULL argument");
     if (num_meshes) *num_meshes = (uint32_t)g->meshes.size();
@@ -768,6 +833,8 @@ cr_status cr_glb_counts(const cr_glb* g, uint32_t* num_meshes, uint32_t* num_ins
 cr_status cr_glb_mesh_arrays(const cr_glb* g, uint32_t mesh, cr_glb_mesh* out) {
     if (!g || !out) return fail(CR_ERR_INVALID, "cr_glb_mesh_arrays: NULL argument");
     if (mesh >= g->meshes.size()) return fail(CR_ERR_NOT_FOUND, "cr_glb_mesh_arrays: no mesh %u", mesh);
+    if (g->streamed())
+        return fail(CR_ERR_UNSUPPORTED, "cr_glb_mesh_arrays: a streamed file keeps no host arrays");
     const cr_glb::Mesh& m = g->meshes[mesh];
     out->positions = m.positions.data();
     out->indices = m.indices.empty() ? nullptr : m.indices.data();
@@ -798,23 +865,51 @@ cr_status cr_glb_create_meshes(cr_context* ctx, const cr_glb* g, uint32_t flags,
     if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(CR_ERR_CUDA, "cr_glb_create_meshes: cudaSetDevice");
     // plain meshes: every buffer allocated first, then one parallel staged
     // upload of all of them, then their boxes
+    // a streamed file's primitives are converted straight from the mapped
+    // file into the staging buffers, chunk by chunk (no host copy of a
+    // primitive); compressed ones are converted one at a time
+    const bool streamed = g->streamed();
+    auto indexed = [&](size_t k) { return streamed ? g->tasks[k].hasIdx : !g->meshes[k].indices.empty(); };
+    auto colored = [&](size_t k) { return streamed ? g->tasks[k].colMode != 0 : !g->meshes[k].colors.empty(); };
     std::vector<size_t> plain;
     for (size_t k = 0; k < g->meshes.size(); k++)
-        if (!(flags & CR_GLB_COMPRESS) || g->meshes[k].indices.empty()) plain.push_back(k);
+        if (!(flags & CR_GLB_COMPRESS) || !indexed(k)) plain.push_back(k);
     std::vector<MeshRec> recs(plain.size());
     std::vector<CopyJob> jobs;
     cr_status s = CR_OK;
     size_t allocated = 0;
     for (; allocated < plain.size(); allocated++) {
-        const cr_glb::Mesh& m = g->meshes[plain[allocated]];
+        const size_t k = plain[allocated];
+        const cr_glb::Mesh& m = g->meshes[k];
         MeshRec& r = recs[allocated];
-        s = alloc_owned_mesh(ctx, m.numVertices, m.numTriangles, !m.indices.empty(), !m.colors.empty(), r);
+        s = alloc_owned_mesh(ctx, m.numVertices, m.numTriangles, indexed(k), colored(k), r);
         if (s) break;
-        jobs.push_back({r.positions, m.positions.data(), 12ull * m.numVertices});
-        if (!m.indices.empty()) jobs.push_back({r.indices, m.indices.data(), 12ull * m.numTriangles});
-        if (!m.colors.empty()) jobs.push_back({r.colors, m.colors.data(), 4ull * m.numVertices});
+        if (!streamed) {
+            jobs.push_back({r.positions, m.positions.data(), 12ull * m.numVertices});
+            if (indexed(k)) jobs.push_back({r.indices, m.indices.data(), 12ull * m.numTriangles});
+            if (colored(k)) jobs.push_back({r.colors, m.colors.data(), 4ull * m.numVertices});
+            continue;
+        }
+        const GlbTask* t = &g->tasks[k];
+        const uint32_t nv = m.numVertices;
+        jobs.push_back({r.positions, nullptr, 12ull * nv, [t](uint64_t o, uint64_t n, void* buf) {
+                            conv_positions(*t, o / 12, (o + n) / 12, (float*)buf);
+                            return true;
+                        }, 12});
+        if (indexed(k))
+            jobs.push_back({r.indices, nullptr, 12ull * m.numTriangles, [t, nv](uint64_t o, uint64_t n, void* buf) {
+                                return conv_indices(*t, o / 4, (o + n) / 4, nv, (uint32_t*)buf);
+                            }, 4});
+        if (colored(k))
+            jobs.push_back({r.colors, nullptr, 4ull * nv, [t](uint64_t o, uint64_t n, void* buf) {
+                                conv_colors(*t, o / 4, (o + n) / 4, (uint32_t*)buf);
+                                return true;
+                            }, 4});
     }
-    if (s == CR_OK) s = upload_parallel(ctx, jobs);
+    if (s == CR_OK) {
+        s = upload_parallel(ctx, jobs);
+        if (s == CR_ERR_INVALID) glb_fail("index beyond its primitive's vertices");
+    }
     if (s != CR_OK) {
         const std::string msg = cr_last_error();
         for (size_t k = 0; k < allocated; k++) {
@@ -832,8 +927,34 @@ cr_status cr_glb_create_meshes(cr_context* ctx, const cr_glb* g, uint32_t flags,
         }
     }
     for (size_t made = 0; made < g->meshes.size() && s == CR_OK; made++) {
-        const cr_glb::Mesh& m = g->meshes[made];
         if (done[made]) continue;  // compressed: packed on the host, as the loader packs
+        // a streamed primitive: its host arrays exist only while it is packed
+        cr_glb::Mesh tmp;
+        if (streamed) {
+            const GlbTask& t = g->tasks[made];
+            tmp.numVertices = g->meshes[made].numVertices;
+            tmp.numTriangles = g->meshes[made].numTriangles;
+            memcpy(tmp.box, g->meshes[made].box, sizeof(tmp.box));
+            tmp.positions.resize(3ull * tmp.numVertices);
+            conv_positions(t, 0, tmp.numVertices, tmp.positions.data());
+            if (!t.hasBox) {
+                for (int j = 0; j < 3; j++) {
+                    tmp.box[j] = INFINITY;
+                    tmp.box[3 + j] = -INFINITY;
+                }
+                extend_box(tmp.positions.data(), tmp.numVertices, tmp.box);
+            }
+            tmp.indices.resize(3ull * tmp.numTriangles);
+            if (!conv_indices(t, 0, 3ull * tmp.numTriangles, tmp.numVertices, tmp.indices.data())) {
+                s = glb_fail("index beyond its primitive's vertices");
+                break;
+            }
+            if (t.colMode) {
+                tmp.colors.resize(tmp.numVertices);
+                conv_colors(t, 0, tmp.numVertices, tmp.colors.data());
+            }
+        }
+        const cr_glb::Mesh& m = streamed ? tmp : g->meshes[made];
         const uint64_t n = 3ull * m.numTriangles;
         uint32_t lo = 0, hi = 0;
         if (n) {
@@ -872,6 +993,8 @@ cr_status cr_glb_ooc_nodes(cr_glb* g, uint32_t max_node_triangles, uint32_t flag
                            cr_ooc_node* nodes, uint32_t* count) {
     if (!g || !count) return fail(CR_ERR_INVALID, "cr_glb_ooc_nodes: NULL argument");
     if (flags & ~(uint32_t)CR_GLB_PIN_HOST) return fail(CR_ERR_INVALID, "cr_glb_ooc_nodes: unknown flags");
+    if (g->streamed())
+        return fail(CR_ERR_UNSUPPORTED, "cr_glb_ooc_nodes: a streamed file keeps no host arrays to build nodes from");
     const uint32_t maxT = max_node_triangles ? max_node_triangles : CR_OOC_MAX_NODE_TRIANGLES;
     if (maxT > CR_OOC_MAX_NODE_TRIANGLES)
         return fail(CR_ERR_INVALID, "cr_glb_ooc_nodes: at most %u triangles per node", CR_OOC_MAX_NODE_TRIANGLES);

@@ -977,12 +977,20 @@ __device__ __forceinline__ int stage2_setup(const CrFrameParams& p, const Target
 // condition bounds the column by an affine function of the row: the setup
 // folds everything per triangle into three (g0 + g1 sy) forms, and a row
 // costs a few double operations.  Non-finite setups keep every row whole.
+// When every bound is a small number of pixels (|g0| + |g1| (|sy| + 1) below
+// 2^12 over the box, and no condition is of kind 0), the rows are narrowed
+// in float: the float evaluation of g0 + g1 * sy, with g0, g1 and sy rounded
+// to float, is then within 2^-8 pixel of the double one, far inside the
+// whole pixel each span is widened by on both sides (s2_row_span), so the
+// float spans keep every column the double spans keep.
 struct S2Span {
     double g0[3], g1[3];  // per condition: bound (or emptiness test) = g0 + g1 * sy
     int kind[3];          // 1: lower bound on px, -1: upper bound, 0: empty if g0 + g1 * sy < 0
     double px0;
     int size_x;
     bool whole;
+    bool fast;            // the float copies below narrow the rows
+    float f0[3], f1[3];
 };
 
 __device__ __forceinline__ S2Span s2_span_setup(float start_x, float start_y, int size_x, int size_y, float asx,
@@ -1030,6 +1038,14 @@ __device__ __forceinline__ S2Span s2_span_setup(float start_x, float start_y, in
         fin = fin && isfinite(P.g0[k]) && isfinite(P.g1[k]);
     }
     P.whole = !fin;
+    const double SYmax = fmax(fabs(sy0), fabs(sy1)) + 1.0;
+    P.fast = fin;
+    for (int k = 0; k < 3; ++k) {
+        P.fast = P.fast && P.kind[k] != 0 && fabs(P.g0[k]) + fabs(P.g1[k]) * SYmax < 4096.0;
+        P.f0[k] = (float)P.g0[k];
+        P.f1[k] = (float)P.g1[k];
+    }
+    P.fast = P.fast && fabs(P.px0) + (double)size_x < 4096.0;
     return P;
 }
 
@@ -1037,6 +1053,28 @@ __device__ __forceinline__ void s2_row_span(const S2Span& P, float py, float asy
     xlo = 0;
     len = P.size_x;
     if (P.whole) return;
+    if (P.fast) {
+        const float sy = (py - asy) + 0.5f;
+        const float px0 = (float)P.px0;
+        float lo = px0, hi = px0 + (float)(P.size_x - 1);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float g = P.f0[k] + P.f1[k] * sy;
+            if (P.kind[k] > 0) lo = fmaxf(lo, g);
+            else hi = fminf(hi, g);
+        }
+        float flo = floorf(lo - px0) - 1.0f;
+        float fhi = ceilf(hi - px0) + 1.0f;
+        flo = fmaxf(flo, 0.0f);
+        fhi = fminf(fhi, (float)(P.size_x - 1));
+        if (!(flo <= fhi)) {
+            if (flo > fhi) len = 0;
+            return;
+        }
+        xlo = (int)flo;
+        len = (int)(fhi - flo) + 1;
+        return;
+    }
     const double sy = ((double)py - (double)asy) + 0.5;
     double lo = P.px0, hi = P.px0 + (double)(P.size_x - 1);
 #pragma unroll

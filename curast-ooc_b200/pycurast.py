@@ -340,6 +340,7 @@ EXPORTS = {
     "cr_ooc_destroy": (_i32, [ctypes.c_void_p]),
     "cr_glb_open": (_i32, [ctypes.c_void_p, _u64, ctypes.POINTER(ctypes.c_void_p)]),
     "cr_glb_open_file": (_i32, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "cr_glb_open_file_streamed": (_i32, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)]),
     "cr_glb_counts": (_i32, [ctypes.c_void_p, ctypes.POINTER(_u32), ctypes.POINTER(_u32)]),
     "cr_glb_mesh_arrays": (_i32, [ctypes.c_void_p, _u32, ctypes.POINTER(CrGlbMesh)]),
     "cr_glb_instances": (_i32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(CrInstance)]),
@@ -509,13 +510,17 @@ class OocScene:
 class Glb:
     """cr_glb: a binary glTF file read as the reference's loader reads it.
 
-    Glb(data=bytes) or Glb(path=...).  mesh(k) returns numpy copies of glb mesh
+    Glb(data=bytes) or Glb(path=...); Glb(path=..., streamed=True) keeps the
+    file mapped and converts its geometry only while uploading it
+    (cr_glb_open_file_streamed).  mesh(k) returns numpy copies of glb mesh
     k; instances(handles) the draw list; create_meshes(ctx) uploads every mesh;
     ooc_nodes() the out-of-core node array (valid while this object lives)."""
 
-    def __init__(self, data=None, path=None):
+    def __init__(self, data=None, path=None, streamed=False):
         h = ctypes.c_void_p()
-        if path is not None:
+        if path is not None and streamed:
+            _check(load().cr_glb_open_file_streamed(os.fsencode(path), ctypes.byref(h)))
+        elif path is not None:
             _check(load().cr_glb_open_file(os.fsencode(path), ctypes.byref(h)))
         else:
             buf = np.frombuffer(bytes(data), np.uint8)

@@ -511,6 +511,17 @@ typedef struct cr_glb_mesh {
  * cr_last_error) for anything malformed or outside the subset above. */
 cr_status cr_glb_open(const void* bytes, uint64_t size, cr_glb** out);
 cr_status cr_glb_open_file(const char* path, cr_glb** out);
+/* A file read as the reference's loader streams it (LargeGlbLoader.h:402-422,
+ * 504-521): the file stays memory-mapped until cr_glb_close and only its JSON
+ * structure is parsed here; cr_glb_create_meshes then converts each
+ * primitive straight from the mapped pages into the page-locked upload
+ * buffers, 8 MiB at a time on up to 8 host threads, so no host copy of the
+ * geometry is made and a file larger than host memory can be loaded
+ * (compressed primitives are converted and packed one at a time).  Indices
+ * are range-checked as they are converted (CR_ERR_INVALID from
+ * cr_glb_create_meshes, nothing created).  cr_glb_mesh_arrays and
+ * cr_glb_ooc_nodes need host arrays: CR_ERR_UNSUPPORTED for such a file. */
+cr_status cr_glb_open_file_streamed(const char* path, cr_glb** out);
 cr_status cr_glb_counts(const cr_glb* glb, uint32_t* num_meshes, uint32_t* num_instances);
 /* Host arrays of mesh k, owned by glb (valid until cr_glb_close). */
 cr_status cr_glb_mesh_arrays(const cr_glb* glb, uint32_t mesh, cr_glb_mesh* out);

@@ -89,6 +89,29 @@ def test_open_file_equals_open_bytes(mixed, tmp_path):
     assert e.value.status == pc.CR_ERR_NOT_FOUND
 
 
+def test_streamed_file_parses_the_same_scene(mixed, tmp_path):
+    """A streamed file (mapped, geometry converted only at upload) has the
+    same meshes, counts and draw list; it keeps no host arrays."""
+    p = tmp_path / "scene.glb"
+    p.write_bytes(mixed)
+    with pc.Glb(path=str(p), streamed=True) as a, pc.Glb(data=mixed) as b:
+        assert (a.num_meshes, a.num_instances) == (b.num_meshes, b.num_instances)
+        ia, na = a.instances()
+        ib, nb = b.instances()
+        assert na == nb
+        for k in range(na):
+            assert ia[k].mesh == ib[k].mesh and list(ia[k].world) == list(ib[k].world)
+        with pytest.raises(pc.CurastError) as e:
+            a.mesh(0)
+        assert e.value.status == pc.CR_ERR_UNSUPPORTED
+        with pytest.raises(pc.CurastError) as e:
+            a.ooc_nodes(100)
+        assert e.value.status == pc.CR_ERR_UNSUPPORTED
+    with pytest.raises(pc.CurastError) as e:
+        pc.Glb(path=str(tmp_path / "missing.glb"), streamed=True)
+    assert e.value.status == pc.CR_ERR_NOT_FOUND
+
+
 def test_oracle_known_answers(mixed):
     """Pins the restatement with values worked out by hand from the loader's
     source (LargeGlbLoader.h:784-803, :1275-1330)."""

@@ -138,3 +138,51 @@ def test_glb_ooc_nodes_render_like_resident(gpu, scene_file, pin):
     assert (ovis != CLEAR).mean() > 0.05
     assert_same_vis(got[0], ovis, "out-of-core glb nodes vs oracle of the selected pieces")
     assert channel_diff(got[1], orgba) <= COLOR_TOL
+
+
+@pytest.mark.parametrize("compress", [False, True])
+def test_streamed_file_renders_the_same(gpu, scene_file, tmp_path, compress):
+    """The file read streamed (geometry converted from the mapped file into
+    the upload buffers, never held on the host) gives the same meshes: its
+    frame equals the one of the file read whole, bit for bit."""
+    p = tmp_path / "scene.glb"
+    p.write_bytes(scene_file)
+    view, proj = _camera()
+    out = []
+    for streamed in (False, True):
+        with pc.Context() as ctx, pc.Glb(path=str(p), streamed=streamed) as g:
+            handles = g.create_meshes(ctx, compress=compress)
+            arr, n = g.instances(handles)
+            inst = [(arr[i].mesh, np.array(arr[i].world[:], np.float32)) for i in range(n)]
+            vis, rgba, _, _ = render_ours(ctx, None, [(k, w) for k, (_, w) in enumerate(inst)], view, proj, W, H,
+                                          handles=[h for h, _ in inst])
+            out.append((vis, rgba))
+    assert (out[0][0] != CLEAR).mean() > 0.05
+    assert_same_vis(out[1][0], out[0][0], "streamed vs whole file")
+    assert np.array_equal(out[1][1], out[0][1])
+
+
+def test_streamed_file_with_a_bad_index_creates_nothing(gpu, tmp_path):
+    """An index beyond its primitive's vertices is found while the streamed
+    primitive is converted: CR_ERR_INVALID and no mesh left behind."""
+    import json
+    import struct
+
+    meshes, nodes = gb.mixed_scene(grid=16, soup=200)
+    data = gb.build_glb(meshes, nodes)
+    n = struct.unpack_from("<I", data, 12)[0]
+    doc = json.loads(data[20:20 + n].decode())
+    a = doc["meshes"][0]["primitives"][0]["indices"]
+    doc["accessors"][a]["componentType"] = 5125  # u16 pairs read as u32: out of range
+    doc["accessors"][a]["count"] //= 2
+    js = json.dumps(doc).encode()
+    js += b" " * ((4 - len(js) % 4) % 4)
+    rest = data[20 + n:]
+    bad = struct.pack("<III", 0x46546C67, 2, 20 + len(js) + len(rest)) + struct.pack("<II", len(js), 0x4E4F534A) + js + rest
+    p = tmp_path / "bad.glb"
+    p.write_bytes(bad)
+    with pc.Context() as ctx, pc.Glb(path=str(p), streamed=True) as g:
+        with pytest.raises(pc.CurastError) as e:
+            g.create_meshes(ctx)
+        assert e.value.status == pc.CR_ERR_INVALID
+        assert b"beyond" in pc.load().cr_last_error()
