@@ -356,8 +356,10 @@ def plain_algorithmic_bytes(wl, fstats, T):
     writes 8 B per listed item; the vertex pass reads 12 B of position and
     writes one record (4-byte cell records up to 4096 pixels a side, else 8)
     per vertex of each chunk its box did not classify; stage 1 reads the
-    12-byte index triple of every triangle of each drawn work item and each
-    vertex record once, and writes and reads 8 B per survivor of the records.
+    12-byte index triple of every triangle of each drawn work item, the
+    record of each vertex those triangles use once (counted as one per two
+    triangles, as in a closed mesh, and at most the records written), and
+    writes and reads 8 B per survivor of the records.
     Frames that draw a mesh more than once cull from box proofs and per-item
     vertex lists (no per-vertex records in device memory).  Returns (bytes per
     stage, triangles in drawn items, vertices evaluated)."""
@@ -380,15 +382,15 @@ def plain_algorithmic_bytes(wl, fstats, T):
         v_eval = min(nV_inst, chunks_eval * 1024)
         tri_drawn = min(T, items_drawn * 128)
         algo = {"vertex": 24 * (chunks + items) + (12 + rec) * v_eval + 8 * items_drawn,
-                "stage1": 12 * tri_drawn + rec * v_eval + 16 * surv}
+                "stage1": 12 * tri_drawn + rec * min(v_eval, tri_drawn // 2) + 16 * surv}
     else:
         v_eval, tri_drawn = nV_inst, T
-        algo = {"vertex": (12 + rec) * nV_inst, "stage1": 12 * T + rec * nV_inst + 16 * surv}
+        algo = {"vertex": (12 + rec) * nV_inst, "stage1": 12 * T + rec * min(nV_inst, T // 2) + 16 * surv}
     if wl.get("compressed"):
         # compressed meshes: 6-byte positions, 3 x bits / 8 bytes of indices per triangle
         ib = 3 * wl["compressed"][0].bits / 8.0
         algo = {"vertex": 24 * (chunks + items) + (6 + rec) * v_eval + 8 * items_drawn,
-                "stage1": ib * tri_drawn + rec * v_eval + 16 * surv}
+                "stage1": ib * tri_drawn + rec * min(v_eval, tri_drawn // 2) + 16 * surv}
     return algo, tri_drawn, v_eval
 
 
@@ -540,7 +542,10 @@ def run_ours(args, rank, world, local):
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "algorithmic_bytes": algo[rk], "kernel_ms": t_k,
                      "traffic": read_traffic(rk, wl["name"])},
-        "gpu_launches": 6 * args.steps,
+        # clear, the two frame-cull kernels, the vertex pass (record-culled
+        # frames), stage 1 (two kernels when record-culled), stages 2 and 3,
+        # the resolve
+        "gpu_launches": (7 if algo.get("boxes") else 9) * args.steps,
         "clocks": clk,
     }
     if parity is not None:

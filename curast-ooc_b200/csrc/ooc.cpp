@@ -24,6 +24,10 @@ using namespace cr;
 namespace {
 
 constexpr int kPassRing = 32;  // in-flight raster passes tracked for slot reuse
+// Node uploads are issued in slices of about this many bytes with at most two
+// slices queued on the copy stream, so that other streams' copies (a
+// server's per-batch tables) never wait behind a whole pass of uploads.
+constexpr uint64_t kUploadSlice = 128ull << 20;
 
 struct NodeRec {
     cr_ooc_node desc;
@@ -59,6 +63,8 @@ struct cr_ooc {
     cudaStream_t copyStream = nullptr;
     cudaEvent_t uploadsDone = nullptr;
     cudaEvent_t passEv[kPassRing] = {};
+    cudaEvent_t sliceEv[2] = {};       // ends of the last two upload slices
+    uint64_t slices = 0;               // upload slices issued so far
     uint64_t ticket = 1;               // next raster-pass ticket
     uint64_t stamp = 1;                // next selection-pass stamp
 };
@@ -118,6 +124,15 @@ cr_status select_nodes(cr_ooc* o, const cr_camera* cam, cudaStream_t stream) {
     return CR_OK;
 }
 
+// Ends an upload slice on the copy stream and waits (on the host) until the
+// slice before it has been copied: at most two slices stay queued.
+cr_status end_upload_slice(cr_ooc* o) {
+    CR_CUDA(cudaEventRecord(o->sliceEv[o->slices & 1], o->copyStream), "upload slice");
+    o->slices++;
+    if (o->slices >= 2) CR_CUDA(cudaEventSynchronize(o->sliceEv[o->slices & 1]), "upload slice wait");
+    return CR_OK;
+}
+
 // Makes the nodes of one pass resident; the render stream then waits for
 // their copies.
 cr_status make_resident(cr_ooc* o, const std::vector<uint32_t>& pass, cudaStream_t renderStream, cr_ooc_stats& st) {
@@ -131,6 +146,7 @@ cr_status make_resident(cr_ooc* o, const std::vector<uint32_t>& pass, cudaStream
         }
     }
     bool copied = false;
+    uint64_t sliceBytes = 0;
     std::vector<uint64_t> waited;  // tickets this copy stream already waits for
     for (uint32_t n : pass) {
         NodeRec& nr = o->nodes[n];
@@ -160,8 +176,15 @@ cr_status make_resident(cr_ooc* o, const std::vector<uint32_t>& pass, cudaStream
             CR_CUDA(cudaMemcpyAsync(base + o->posBytes + o->idxBytes, d.colors, (size_t)d.num_vertices * 4,
                                     cudaMemcpyHostToDevice, o->copyStream),
                     "node colours upload");
-        st.uploaded_bytes += (uint64_t)d.num_vertices * (d.colors ? 16 : 12) + (uint64_t)d.num_triangles * 12;
+        const uint64_t nodeBytes = (uint64_t)d.num_vertices * (d.colors ? 16 : 12) + (uint64_t)d.num_triangles * 12;
+        st.uploaded_bytes += nodeBytes;
         st.uploaded_nodes++;
+        sliceBytes += nodeBytes;
+        if (sliceBytes >= kUploadSlice) {
+            sliceBytes = 0;
+            cr_status s = end_upload_slice(o);
+            if (s) return s;
+        }
         MeshRec& m = o->ctx->meshes[nr.mesh];
         m.positions = (float*)base;
         m.indices = (uint32_t*)(base + o->posBytes);
@@ -205,6 +228,8 @@ void release(cr_ooc* o) {
     if (o->hVisible) cudaFreeHost(o->hVisible);
     if (o->uploadsDone) cudaEventDestroy(o->uploadsDone);
     for (cudaEvent_t& e : o->passEv)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t& e : o->sliceEv)
         if (e) cudaEventDestroy(e);
     if (o->copyStream) cudaStreamDestroy(o->copyStream);
     delete o;
@@ -280,6 +305,11 @@ cr_status cr_ooc_create(cr_context* ctx, const cr_ooc_node* nodes, uint32_t coun
         return fail(CR_ERR_CUDA, "out-of-core scene setup");
     }
     for (cudaEvent_t& e : o->passEv)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+            release(o);
+            return fail(CR_ERR_CUDA, "out-of-core scene events");
+        }
+    for (cudaEvent_t& e : o->sliceEv)
         if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
             release(o);
             return fail(CR_ERR_CUDA, "out-of-core scene events");

@@ -11,15 +11,41 @@
 // triangle's coverage and depth are pure functions of the inputs, and the
 // visbuffer (an atomic 64-bit minimum over a fixed fragment set) is
 // independent of how the work is scheduled.
+//
+// CR_REF_MATH = 1 (raster_ref.cu): the file is compiled instead with
+// --use_fast_math, the recipe of the reference's own build
+// (CudaModularProgram.h:133-157), and follows that build's arithmetic: its
+// __fdividef calls are __fdividef, its other divisions and square roots are
+// the approximate ones that flag selects, products and sums contract to FMAs
+// as the compiler pairs them, and f / aspect and the mirror test are formed on
+// the device as the reference forms them.  The exact culling proofs of the
+// IEEE build (division-free frustum tests, row spans, tile pruning) do not
+// hold for approximate arithmetic and are left out.
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
 
 #include "cr_device.h"
 #include "geom.cuh"
+
+#ifndef CR_REF_MATH
+#define CR_REF_MATH 0
+#endif
+
 namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
+constexpr bool REF_MATH = CR_REF_MATH != 0;
+
+// The reference's __fdividef sites (tv.cu:206-211,249): the intrinsic in the
+// fast-math build, an IEEE division in this one.
+__device__ __forceinline__ float ref_fdiv(float a, float b) {
+#if CR_REF_MATH
+    return __fdividef(a, b);
+#else
+    return a / b;
+#endif
+}
 
 // Programmatic dependent launch.  The plain frame's kernels after the clear
 // are launched with cudaLaunchAttributeProgrammaticStreamSerialization: each
@@ -212,6 +238,11 @@ struct Target {
 };
 
 __device__ __forceinline__ Target target_of(const CrFrameParams& p) {
+    if constexpr (REF_MATH) {
+        // tv.cu:100-101: aspect and f / aspect in the build's own division
+        const float aspect = float(p.W) / float(p.H);
+        return Target{p.fb, p.W, p.H, p.f, p.f / aspect, p.thrSmall, 0ull};
+    }
     return Target{p.fb, p.W, p.H, p.f, p.f / p.aspect, p.thrSmall, 0ull};
 }
 
