@@ -682,7 +682,8 @@ def sub_plain(args, wl, ctx, handles, with_parity):
                                    "stage1": "k_stage1" if algo.get("boxes") else "k_s1cull + k_s1raster"}.get(
                                        rk, f"k_{rk}"),
                         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                        "peak_kind": peak_kind, "algorithmic_bytes": algo[rk], "kernel_ms": stage_ms[rk]},
+                        "peak_kind": peak_kind, "algorithmic_bytes": algo[rk], "kernel_ms": stage_ms[rk],
+                        "traffic": read_traffic(rk, wl["name"])},
            "frame_roofline": {"bytes": frame_bytes, "achieved_gbs": frame_bytes / (ms * 1e-3) / 1e9,
                               "frac": frame_bytes / (ms * 1e-3) / 1e9 / peak,
                               "note": "reference formula 12T+12V+28P"}}

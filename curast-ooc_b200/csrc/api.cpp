@@ -63,6 +63,42 @@ float det3_glm(const float* m) {
     return (x * c2[0] + y * c2[1]) + z * c2[2];
 }
 
+// The back-face proof's data of one instance (CR_BACK_DOUBLES) from its float
+// world-view matrix (column-major): R its 3x3 part, t its translation, all
+// exact in double.  e = -R^-1 t by cofactors; |det R| only when it exceeds
+// 1e-4 of the product of the columns' 1-norms, which bounds the float
+// det3_glm's error far below it, so the mirror flag the kernels use has the
+// exact sign (else 0: no proof for this instance).
+void back_face_data(const float* wv, double* o) {
+    double R[3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) R[i][j] = wv[j * 4 + i];
+    const double t[3] = {wv[12], wv[13], wv[14]};
+    const double a00 = R[1][1] * R[2][2] - R[1][2] * R[2][1], a01 = R[0][2] * R[2][1] - R[0][1] * R[2][2],
+                 a02 = R[0][1] * R[1][2] - R[0][2] * R[1][1], a10 = R[1][2] * R[2][0] - R[1][0] * R[2][2],
+                 a11 = R[0][0] * R[2][2] - R[0][2] * R[2][0], a12 = R[0][2] * R[1][0] - R[0][0] * R[1][2],
+                 a20 = R[1][0] * R[2][1] - R[1][1] * R[2][0], a21 = R[0][1] * R[2][0] - R[0][0] * R[2][1],
+                 a22 = R[0][0] * R[1][1] - R[0][1] * R[1][0];
+    const double det = R[0][0] * a00 + R[0][1] * a10 + R[0][2] * a20;
+    double had = 1.0, frob = 0.0, rowAbs = 0.0, tAbs = 0.0;
+    for (int j = 0; j < 3; j++) had *= fabs(R[0][j]) + fabs(R[1][j]) + fabs(R[2][j]);
+    for (int i = 0; i < 3; i++) {
+        rowAbs = std::max(rowAbs, fabs(R[i][0]) + fabs(R[i][1]) + fabs(R[i][2]));
+        tAbs = std::max(tAbs, fabs(t[i]));
+        for (int j = 0; j < 3; j++) frob += R[i][j] * R[i][j];
+    }
+    o[0] = -(a00 * t[0] + a01 * t[1] + a02 * t[2]) / det;
+    o[1] = -(a10 * t[0] + a11 * t[1] + a12 * t[2]) / det;
+    o[2] = -(a20 * t[0] + a21 * t[1] + a22 * t[2]) / det;
+    const bool ok = std::isfinite(det) && fabs(det) > 1e-4 * had && std::isfinite(o[0]) && std::isfinite(o[1]) &&
+                    std::isfinite(o[2]) && std::isfinite(tAbs) && std::isfinite(frob);
+    o[3] = ok ? fabs(det) : 0.0;
+    o[4] = sqrt(frob);
+    o[5] = rowAbs;
+    o[6] = tAbs;
+    o[7] = 0.0;
+}
+
 // glm::inverse for mat4 (libs/glm/glm/detail/func_matrix.inl:296-360)
 void mat4_inverse(const float* m, float* out) {
 #define M(c, r) m[(c) * 4 + (r)]
@@ -219,6 +255,7 @@ cr_status assemble(cr_context* ctx, const cr_instance* instances, uint32_t count
         count, firstIds ? (flags | CR_RENDER_KEEP_ORDER) : flags, [&](uint32_t i) { return instances[i].mesh; },
         [&](uint32_t i) { return ctx->meshes[instances[i].mesh].numTriangles; }, A.order);
     A.inst.assign(count, CrInstance{});
+    A.back.resize((size_t)CR_BACK_DOUBLES * count);
     A.worldView.resize(16ull * count);
     A.world.resize(16ull * count);
     A.seg.clear();
@@ -247,6 +284,7 @@ cr_status assemble(cr_context* ctx, const cr_instance* instances, uint32_t count
         float* wv = &A.worldView[16ull * r];
         mat4_mul(view, in.world, wv);  // CuRast_render.h:409
         ci.flip = det3_glm(wv) < 0.0f ? 1u : 0u;
+        back_face_data(wv, &A.back[(size_t)CR_BACK_DOUBLES * r]);
         memcpy(&A.world[16ull * r], in.world, 64);
         // CuRast_render.h:425-433: consecutive instances of one mesh form a segment
         if (A.seg.empty() || A.seg.back().positions != m.positions || A.seg.back().indices != m.indices ||
@@ -261,6 +299,7 @@ cr_status assemble(cr_context* ctx, const cr_instance* instances, uint32_t count
             s.flags = (!m.compressed && m.indices && ((uintptr_t)m.indices & 15u) == 0) ? 1u : 0u;
             if (m.compressed) s.codec = m.codec;
             s.itemBoxes = m.itemBoxes;
+            s.itemCones = m.itemCones;
             s.subBoxes = m.subBoxes;
             s.localLists = m.localLists;
             s.localCounts = m.localCounts;
@@ -328,21 +367,23 @@ cr_status launch_mesh_boxes(cr_context* ctx, MeshRec& m) {
     const uint64_t nChunks = (m.numVertices + CR_VCHUNK - 1) / CR_VCHUNK;
     const size_t gb = align_up((size_t)((nItems + CR_GROUP - 1) / CR_GROUP) * 24, 256);
     const size_t cgb = align_up((size_t)((nChunks + CR_GROUP - 1) / CR_GROUP) * 24, 256);
+    const size_t icb = align_up((size_t)nItems * CR_CONE_FLOATS * 4, 256);
     if (!m.itemBoxes) {
-        cr_status s = ctx->dev_alloc((void**)&m.itemBoxes, ib + cb + sb + gb + cgb + 256, "mesh boxes");
+        cr_status s = ctx->dev_alloc((void**)&m.itemBoxes, ib + cb + sb + gb + cgb + icb + 256, "mesh boxes");
         if (s) return s;
         m.chunkBoxes = (float*)((char*)m.itemBoxes + ib);
         m.subBoxes = (float*)((char*)m.itemBoxes + ib + cb);
         m.groupBoxes = (float*)((char*)m.itemBoxes + ib + cb + sb);
         m.chunkGroupBoxes = (float*)((char*)m.itemBoxes + ib + cb + sb + gb);
-        m.boxBytes = ib + cb + sb + gb + cgb + 256;
+        m.itemCones = (float*)((char*)m.itemBoxes + ib + cb + sb + gb + cgb);
+        m.boxBytes = ib + cb + sb + gb + cgb + icb + 256;
     }
-    m.meshBox = (float*)((char*)m.itemBoxes + ib + cb + sb + gb + cgb);
+    m.meshBox = (float*)((char*)m.itemBoxes + ib + cb + sb + gb + cgb + icb);
     m.dCodec = (CrCodec*)((char*)m.meshBox + 64);
     CR_CUDA(cudaMemcpy(m.dCodec, &m.codec, sizeof(CrCodec), cudaMemcpyHostToDevice), "mesh codec");
     if (cr_launch_mesh_boxes(m.indices, m.positions, m.compressed ? m.dCodec : nullptr, m.numTriangles,
                              m.numVertices, m.itemBoxes, m.chunkBoxes, m.subBoxes, m.meshBox, m.groupBoxes,
-                             m.chunkGroupBoxes, 0))
+                             m.chunkGroupBoxes, m.itemCones, 0))
         return fail(CR_ERR_CUDA, "mesh box launch: %s", cudaGetErrorString(cudaGetLastError()));
     return CR_OK;
 }
@@ -399,7 +440,8 @@ cr_status upload_frame(cr_context* ctx, const Assembled& A, cudaStream_t stream,
     const size_t oWV = align_up(oInst + n * sizeof(CrInstance), 256);
     const size_t oW = align_up(oWV + n * 64, 256);
     const size_t oSeg = align_up(oW + n * 64, 256);
-    const size_t total = align_up(oSeg + m * sizeof(CrSegment), 256);
+    const size_t oBack = align_up(oSeg + m * sizeof(CrSegment), 256);
+    const size_t total = align_up(oBack + n * CR_BACK_DOUBLES * 8, 256);
     // the previous frame's copy must have left the staging buffer
     CR_CUDA(cudaEventSynchronize(ctx->frameCopied), "frame staging");
     if (total > ctx->hFrameCap) {
@@ -424,6 +466,7 @@ cr_status upload_frame(cr_context* ctx, const Assembled& A, cudaStream_t stream,
     memcpy(h + oWV, A.worldView.data(), n * 64);
     memcpy(h + oW, A.world.data(), n * 64);
     memcpy(h + oSeg, A.seg.data(), m * sizeof(CrSegment));
+    memcpy(h + oBack, A.back.data(), n * CR_BACK_DOUBLES * 8);
     CR_CUDA(cudaMemcpyAsync(ctx->dFrame, h, total, cudaMemcpyHostToDevice, stream), "frame table upload");
     CR_CUDA(cudaEventRecord(ctx->frameCopied, stream), "frame event");
     char* d = (char*)ctx->dFrame;
@@ -431,6 +474,7 @@ cr_status upload_frame(cr_context* ctx, const Assembled& A, cudaStream_t stream,
     fp.world_view = (const float4*)(d + oWV);
     fp.world = (const float4*)(d + oW);
     fp.segments = (const CrSegment*)(d + oSeg);
+    fp.instBack = (const double*)(d + oBack);
     fp.numInstances = (uint32_t)n;
     fp.numSegments = (uint32_t)m;
     fp.numItems = A.numItems;
@@ -1097,14 +1141,17 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
     // (instance, vertex), or (no records) box proofs of the sample-miss cull
     // and per-item vertex lists; the choice changes speed only, never the output
     const uint32_t rec = ctx->cfg.cull_records;
+    // the reference build's arithmetic: no records, no culling proofs
+    const bool refMath = (flags & CR_RENDER_REF_MATH) != 0;
     bool instanced = false;  // some mesh drawn more than once
-    if (rec == CR_CULL_AUTO && count > 1) {
+    if (rec == CR_CULL_AUTO && count > 1 && !refMath) {
         std::vector<uint32_t> ms(count);
         for (uint32_t i = 0; i < count; i++) ms[i] = instances[i].mesh;
         std::sort(ms.begin(), ms.end());
         instanced = std::adjacent_find(ms.begin(), ms.end()) != ms.end();
     }
-    uint32_t cellMode = rec == CR_CULL_CELLS      ? CR_REC_CELLS
+    uint32_t cellMode = refMath                   ? CR_REC_BOXES
+                        : rec == CR_CULL_CELLS    ? CR_REC_CELLS
                         : rec == CR_CULL_OUTCODES ? CR_REC_OUTCODES
                         : rec == CR_CULL_BOXES    ? CR_REC_BOXES
                         : instanced               ? CR_REC_BOXES
@@ -1114,7 +1161,7 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
     else if (cellMode == CR_REC_CELLS && cam->width <= 4096 && cam->height <= 4096)
         cellMode = CR_REC_CELLS32;  // 12-bit coordinates fit: half the record bytes
     const bool direct = cellMode == CR_REC_BOXES;
-    if (direct && !(flags & kRenderResolveOnly))
+    if (direct && !refMath && !(flags & kRenderResolveOnly))
         for (uint32_t i = 0; i < count; i++) {
             const uint32_t m = instances[i].mesh;
             if (m < ctx->meshes.size() && ctx->meshes[m].live) ensure_local_lists(ctx, ctx->meshes[m]);
@@ -1243,6 +1290,19 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
             return fail(CR_ERR_CUDA, "clear launch: %s", cudaGetErrorString(cudaGetLastError()));
         }
         CR_CUDA(mark(1), "event");
+        if (refMath) {  // stages 1-3 in the reference build's arithmetic
+            CR_CUDA(mark(2), "event");
+            if (raster && count && cr_launch_ref_raster(fp, stream))
+                return fail(CR_ERR_CUDA, "raster launch: %s", cudaGetErrorString(cudaGetLastError()));
+            CR_CUDA(mark(3), "event");
+            CR_CUDA(mark(4), "event");
+            CR_CUDA(mark(5), "event");
+            if (rasterEnd) CR_CUDA(cudaEventRecord(rasterEnd, stream), "event");
+            if (!(flags & CR_RENDER_NO_RESOLVE) && cr_launch_resolve(rp, stream))
+                return fail(CR_ERR_CUDA, "resolve launch: %s", cudaGetErrorString(cudaGetLastError()));
+            CR_CUDA(mark(6), "event");
+            return CR_OK;
+        }
         if (raster && count && (cr_launch_cull(fp, ctx->shape, stream) || cr_launch_vertex(fp, ctx->shape, stream)))
             return fail(CR_ERR_CUDA, "vertex-pass launch: %s", cudaGetErrorString(cudaGetLastError()));
         CR_CUDA(mark(2), "event");
@@ -1262,7 +1322,7 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
         CR_CUDA(mark(6), "event");
         return CR_OK;
     };
-    const bool culled = fp.itemList && !(flags & kRenderResolveOnly);
+    const bool culled = fp.itemList && !refMath && !(flags & kRenderResolveOnly);
     return run_frame(ctx, flags, stream, count, A.totalTriangles, issue, culled ? A.numItems : 0,
                      culled ? fp.numVChunks : 0);
 }

@@ -46,6 +46,7 @@ struct MeshRec {
     float* subBoxes = nullptr;    // per CR_SUB triangles
     float* groupBoxes = nullptr;  // per CR_GROUP item boxes
     float* chunkGroupBoxes = nullptr;  // per CR_GROUP chunk boxes
+    float* itemCones = nullptr;   // per CR_BATCH triangles: CR_CONE_FLOATS normal cone
     float* meshBox = nullptr;     // the whole mesh's box (6 floats)
     size_t boxBytes = 0;
     float box[6] = {NAN, NAN, NAN, NAN, NAN, NAN};  // host copy of the mesh box
@@ -100,6 +101,7 @@ struct Assembled {
     std::vector<float> worldView;   // 16 per instance
     std::vector<float> world;       // 16 per instance
     std::vector<CrSegment> seg;
+    std::vector<double> back;       // CR_BACK_DOUBLES per instance (back-face proof)
     uint64_t totalTriangles = 0;
     uint64_t numItems = 0;
     uint64_t outBytes = 0;     // vertex-pass record slots of all instances

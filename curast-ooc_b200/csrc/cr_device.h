@@ -122,8 +122,19 @@ struct alignas(16) CrSegment {
     CrCodec codec;              // compressed meshes (flags bit 0 is then clear)
     const float* groupBoxes;    // per CR_GROUP item boxes: their union (or nullptr)
     uint64_t unitBase;          // first group-cull unit (item group x instance chunk)
+    const float* itemCones;     // per item, CR_CONE_FLOATS: its triangles' normal cone (or nullptr)
+    uint64_t pad;
 };
-static_assert(sizeof(CrSegment) == 128, "CrSegment layout");
+static_assert(sizeof(CrSegment) == 144, "CrSegment layout");
+// Per-item normal cone (object space), for the back-face proof of the frame
+// cull: axis m (float xyz, any length), cosT (every triangle's unit normal u
+// has u . m / |m| >= cosT; below -1: no cone), nMin (every triangle's
+// |(pb - pa) x (pc - pa)| >= nMin), edge (every |pb - pa|, |pc - pa| <= edge).
+#define CR_CONE_FLOATS 6
+// Per-instance data of the back-face proof (CrFrameParams::instBack, doubles):
+// the camera in object space (e = -R^-1 t, 3), |det R| (0: no proof), the
+// Frobenius norm of R, max_i sum_j |R_ij|, max_i |t_i|, and one spare.
+#define CR_BACK_DOUBLES 8
 
 struct alignas(16) CrTile {     // HugeTriangle, HostDeviceInterface.h:254-259
     int32_t instance;           // instance | view << 26 (view 0 in single-view frames)
@@ -243,6 +254,9 @@ struct CrFrameParams {
     // counted in counters[CR_CTR_SURVIVORS], at most s1Cap
     uint64_t* s1List;
     uint64_t s1Cap;
+    // CR_BACK_DOUBLES per instance for the item cull's back-face proof, or
+    // nullptr (no proof)
+    const double* instBack;
 };
 #define CR_CHUNK_EVAL 0xffu
 
@@ -317,15 +331,20 @@ int cr_launch_stage3(const CrFrameParams& p, const CrLaunchShape& s, void* strea
 // (runs before the vertex pass).
 int cr_launch_cull(const CrFrameParams& p, const CrLaunchShape& s, void* stream);
 int cr_launch_resolve(const CrResolveParams& p, void* stream);
+// Stages 1-3 of a frame in the reference build's fast-math arithmetic
+// (raster_ref.cu): every triangle through the per-triangle path.
+int cr_launch_ref_raster(const CrFrameParams& p, void* stream);
 
 // Mesh preparation (meshprep.cu): the box of the vertices of every CR_BATCH
 // and every CR_SUB consecutive triangles and of every CR_VCHUNK consecutive
 // vertices (a box
 // with a non-finite position is NaN and culls nothing).
 // `codec`: device copy of a compressed mesh's codec, or nullptr.
+// itemCones: per item CR_CONE_FLOATS (or nullptr).
 int cr_launch_mesh_boxes(const uint32_t* indices, const float* positions, const CrCodec* codec,
                          uint32_t numTriangles, uint32_t numVertices, float* itemBoxes, float* chunkBoxes,
-                         float* subBoxes, float* meshBox, float* groupBoxes, float* chunkGroupBoxes, void* stream);
+                         float* subBoxes, float* meshBox, float* groupBoxes, float* chunkGroupBoxes,
+                         float* itemCones, void* stream);
 // Per-item vertex lists of an indexed mesh (see CR_LOCAL_BYTES).
 int cr_launch_local_lists(const uint32_t* indices, const CrCodec* codec, uint32_t numTriangles, uint8_t* lists,
                           uint32_t* counts, void* stream);

@@ -70,6 +70,84 @@ __global__ void __launch_bounds__(256) k_item_boxes(const uint32_t* idx, const f
     }
 }
 
+// One warp per item: the normal cone of its triangles (CR_CONE_FLOATS, see
+// cr_device.h), computed in double from the float positions.  The axis is the
+// sum of the unit normals rounded to float; cosT is the least cosine between
+// a unit normal and that float axis, lowered by 1e-9 (far above the double
+// rounding of the computation) and rounded down to float; nMin is rounded
+// down and edge up.  A zero-area or non-finite triangle, or a cone wider than
+// acos(0.05), gives cosT = -2 (no proof).
+__global__ void __launch_bounds__(256) k_item_cones(const uint32_t* idx, const float* pos, const CrCodec* codec,
+                                                    uint32_t nT, float* cones) {
+    const int lane = threadIdx.x & 31;
+    const GeomRef g = geom_from(pos, idx, codec);
+    const uint32_t nItems = (nT + CR_BATCH - 1) / CR_BATCH;
+    for (uint32_t b = blockIdx.x * 8 + (threadIdx.x >> 5); b < nItems; b += gridDim.x * 8) {
+        double n[CR_BATCH / 32][3];
+        double len[CR_BATCH / 32];
+        bool live[CR_BATCH / 32];
+        double sx = 0.0, sy = 0.0, sz = 0.0, nMin = INFINITY, edge = 0.0;
+        bool bad = false;
+#pragma unroll
+        for (int r = 0; r < CR_BATCH / 32; ++r) {
+            const uint32_t t = b * CR_BATCH + r * 32 + lane;
+            live[r] = t < nT;
+            len[r] = 1.0;
+            n[r][0] = n[r][1] = n[r][2] = 0.0;
+            if (!live[r]) continue;
+            float a[3], bq[3], c[3];
+            geom_pos(g, geom_index(g, 3ull * t + 0), a[0], a[1], a[2]);
+            geom_pos(g, geom_index(g, 3ull * t + 1), bq[0], bq[1], bq[2]);
+            geom_pos(g, geom_index(g, 3ull * t + 2), c[0], c[1], c[2]);
+            const double u0 = (double)bq[0] - a[0], u1 = (double)bq[1] - a[1], u2 = (double)bq[2] - a[2];
+            const double v0 = (double)c[0] - a[0], v1 = (double)c[1] - a[1], v2 = (double)c[2] - a[2];
+            n[r][0] = u1 * v2 - u2 * v1;
+            n[r][1] = u2 * v0 - u0 * v2;
+            n[r][2] = u0 * v1 - u1 * v0;
+            len[r] = sqrt(n[r][0] * n[r][0] + n[r][1] * n[r][1] + n[r][2] * n[r][2]);
+            edge = fmax(edge, fmax(sqrt(u0 * u0 + u1 * u1 + u2 * u2), sqrt(v0 * v0 + v1 * v1 + v2 * v2)));
+            bad |= !(len[r] > 0.0) || !isfinite(len[r]) || !isfinite(edge);
+            nMin = fmin(nMin, len[r]);
+            if (len[r] > 0.0 && isfinite(len[r])) {
+                sx += n[r][0] / len[r];
+                sy += n[r][1] / len[r];
+                sz += n[r][2] / len[r];
+            }
+        }
+#pragma unroll
+        for (int d = 16; d >= 1; d >>= 1) {
+            sx += __shfl_xor_sync(FULL, sx, d);
+            sy += __shfl_xor_sync(FULL, sy, d);
+            sz += __shfl_xor_sync(FULL, sz, d);
+            nMin = fmin(nMin, __shfl_xor_sync(FULL, nMin, d));
+            edge = fmax(edge, __shfl_xor_sync(FULL, edge, d));
+        }
+        bad = __any_sync(FULL, bad);
+        // the axis as stored (float), renormalised in double as the proof does
+        const float mx = (float)sx, my = (float)sy, mz = (float)sz;
+        const double ml = sqrt((double)mx * mx + (double)my * my + (double)mz * mz);
+        double cosT = INFINITY;
+#pragma unroll
+        for (int r = 0; r < CR_BATCH / 32; ++r)
+            if (live[r] && len[r] > 0.0)
+                cosT = fmin(cosT, (n[r][0] * mx + n[r][1] * my + n[r][2] * mz) / (len[r] * ml));
+#pragma unroll
+        for (int d = 16; d >= 1; d >>= 1) cosT = fmin(cosT, __shfl_xor_sync(FULL, cosT, d));
+        cosT -= 1e-9;
+        if (bad || !(ml > 0.0) || !isfinite(ml) || !(cosT > 0.05)) cosT = -2.0;
+        if (lane < CR_CONE_FLOATS) {
+            float v;
+            if (lane == 0) v = mx;
+            else if (lane == 1) v = my;
+            else if (lane == 2) v = mz;
+            else if (lane == 3) v = __double2float_rd(cosT);
+            else if (lane == 4) v = bad ? 0.0f : __double2float_rd(nMin * (1.0 - 1e-9));
+            else v = bad ? INFINITY : __double2float_ru(edge * (1.0 + 1e-9));
+            cones[(uint64_t)CR_CONE_FLOATS * b + lane] = v;
+        }
+    }
+}
+
 // Half a warp per sub-box: lane t of the half is its triangle t.
 __global__ void __launch_bounds__(256) k_sub_boxes(const uint32_t* idx, const float* pos, const CrCodec* codec,
                                                    uint32_t nT, float* boxes) {
@@ -276,7 +354,8 @@ int cr_launch_local_lists(const uint32_t* indices, const CrCodec* codec, uint32_
 
 int cr_launch_mesh_boxes(const uint32_t* indices, const float* positions, const CrCodec* codec,
                          uint32_t numTriangles, uint32_t numVertices, float* itemBoxes, float* chunkBoxes,
-                         float* subBoxes, float* meshBox, float* groupBoxes, float* chunkGroupBoxes, void* stream) {
+                         float* subBoxes, float* meshBox, float* groupBoxes, float* chunkGroupBoxes,
+                         float* itemCones, void* stream) {
     cudaStream_t st = (cudaStream_t)stream;
     const uint32_t nItems = (numTriangles + CR_BATCH - 1) / CR_BATCH;
     const uint32_t nChunks = (numVertices + CR_VCHUNK - 1) / CR_VCHUNK;
@@ -296,6 +375,9 @@ int cr_launch_mesh_boxes(const uint32_t* indices, const float* positions, const 
     if (nCGroups && chunkGroupBoxes)
         k_group_boxes<<<(nCGroups + 7) / 8 < 148 * 16 ? (nCGroups + 7) / 8 : 148 * 16, 256, 0, st>>>(
             chunkBoxes, nChunks, chunkGroupBoxes);
+    if (nItems && itemCones)
+        k_item_cones<<<(nItems + 7) / 8 < 148 * 16 ? (nItems + 7) / 8 : 148 * 16, 256, 0, st>>>(
+            indices, positions, codec, numTriangles, itemCones);
     if (meshBox) k_mesh_box<<<1, 256, 0, st>>>(itemBoxes, nItems, meshBox);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

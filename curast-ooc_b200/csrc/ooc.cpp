@@ -347,8 +347,8 @@ cr_status cr_ooc_select(cr_ooc* o, const cr_camera* cam, uint8_t* visible) {
 cr_status cr_ooc_render(cr_ooc* o, const cr_camera* cam, uint64_t d_visbuffer, uint64_t d_rgba, int32_t display,
                         uint32_t flags, void* stream_, cr_ooc_stats* stats) {
     if (!o || !cam) return fail(CR_ERR_INVALID, "cr_ooc_render: NULL argument");
-    if (flags & (CR_RENDER_KEEP_ORDER | CR_RENDER_NO_CLEAR))
-        return fail(CR_ERR_INVALID, "cr_ooc_render: KEEP_ORDER and NO_CLEAR are not accepted");
+    if (flags & (CR_RENDER_KEEP_ORDER | CR_RENDER_NO_CLEAR | CR_RENDER_REF_MATH))
+        return fail(CR_ERR_INVALID, "cr_ooc_render: KEEP_ORDER, NO_CLEAR and REF_MATH are not accepted");
     cudaStream_t stream = (cudaStream_t)stream_;
     CR_CUDA(cudaSetDevice(o->ctx->device), "cudaSetDevice");
     cr_ooc_stats st{};

@@ -181,10 +181,12 @@ __global__ void __launch_bounds__(THREADS, VX_MIN_BLOCKS) k_vertex(const CrFrame
 //                 CR_CHUNK_EVAL and are listed for the vertex pass, which
 //                 writes their per-vertex records
 //   items         the item's box is classified for each listed instance of
-//                 its unit; an instance whose box is wholly behind or beyond
-//                 one side has every triangle of the item culled by the
-//                 reference's own tests (tv.cu:110-119); so has one whose box
-//                 provably misses every sample (box_misses_samples,
+//                 its unit; an instance for which every triangle of the item
+//                 provably faces away (item_back_facing: the item's normal
+//                 cone, tv.cu:168-188), or whose box is wholly behind or
+//                 beyond one side, has every triangle of the item culled by
+//                 the reference's own tests (tv.cu:110-119); so has one whose
+//                 box provably misses every sample (box_misses_samples,
 //                 tv.cu:153-158).  Items with a surviving instance are
 //                 appended (warp-aggregated) with the mask of those instances.
 // Skipping what the boxes prove cannot change the visbuffer; the two levels
@@ -367,6 +369,7 @@ __global__ void __launch_bounds__(THREADS, 3) k_cull(const CrFrameParams p) {
         uint32_t mask = 0;
         if (valid) {
             const float* boxes = ldg_ptr(&sg->itemBoxes);
+            const float* cones = p.instBack ? ldg_ptr(&sg->itemCones) : nullptr;
             if (!boxes) {
                 mask = alive | (insideU << 16);
             } else {
@@ -375,6 +378,10 @@ __global__ void __launch_bounds__(THREADS, 3) k_cull(const CrFrameParams p) {
                 for (uint32_t rest = alive; rest; rest &= rest - 1) {
                     const uint32_t slot = __ffs(rest) - 1;
                     const uint32_t inst = ib + slot;
+                    // every triangle of the item faces away from the camera
+                    if (cones && item_back_facing(p.instBack + (uint64_t)CR_BACK_DOUBLES * inst,
+                                                  cones + (uint64_t)CR_CONE_FLOATS * batch, blo, bhi))
+                        continue;
                     const Mat M = load_mat(p.world_view + 4ull * inst);
                     bool inside = ((insideU >> slot) & 1u) != 0u;
                     if (!inside) {

@@ -281,15 +281,25 @@ __device__ __forceinline__ int stage1_triangle(const Target& p, const float fa, 
     bool nontrivial = (da <= 0.0f || db <= 0.0f || dc <= 0.0f);
     const float Xa = fa * av.x, Xb = fa * bv.x, Xc = fa * cv.x;
     const float Ya = f * av.y, Yb = f * bv.y, Yc = f * cv.y;
-    if (!nontrivial) {  // tv.cu:113-118, on fl(X/d) without dividing
-        if (ndc_beyond(Xa, da) && ndc_beyond(Xb, db) && ndc_beyond(Xc, dc)) return S1_CULL;
-        if (ndc_beyond(-Xa, da) && ndc_beyond(-Xb, db) && ndc_beyond(-Xc, dc)) return S1_CULL;
-        if (ndc_beyond(Ya, da) && ndc_beyond(Yb, db) && ndc_beyond(Yc, dc)) return S1_CULL;
-        if (ndc_beyond(-Ya, da) && ndc_beyond(-Yb, db) && ndc_beyond(-Yc, dc)) return S1_CULL;
+    if constexpr (!REF_MATH) {
+        if (!nontrivial) {  // tv.cu:113-118, on fl(X/d) without dividing
+            if (ndc_beyond(Xa, da) && ndc_beyond(Xb, db) && ndc_beyond(Xc, dc)) return S1_CULL;
+            if (ndc_beyond(-Xa, da) && ndc_beyond(-Xb, db) && ndc_beyond(-Xc, dc)) return S1_CULL;
+            if (ndc_beyond(Ya, da) && ndc_beyond(Yb, db) && ndc_beyond(Yc, dc)) return S1_CULL;
+            if (ndc_beyond(-Ya, da) && ndc_beyond(-Yb, db) && ndc_beyond(-Yc, dc)) return S1_CULL;
+        }
     }
     const V3 an = {Xa / da, Ya / da, da};  // viewToNDC, helpers:95-101
     const V3 bn = {Xb / db, Yb / db, db};
     const V3 cn = {Xc / dc, Yc / dc, dc};
+    if constexpr (REF_MATH) {
+        if (!nontrivial) {  // tv.cu:113-118 on the build's own quotients
+            if (an.x > +1.0f && bn.x > +1.0f && cn.x > +1.0f) return S1_CULL;
+            if (an.x < -1.0f && bn.x < -1.0f && cn.x < -1.0f) return S1_CULL;
+            if (an.y > +1.0f && bn.y > +1.0f && cn.y > +1.0f) return S1_CULL;
+            if (an.y < -1.0f && bn.y < -1.0f && cn.y < -1.0f) return S1_CULL;
+        }
+    }
 
     const float Wf = (float)p.W, Hf = (float)p.H;
     V2 as = to_screen(an, Wf, Hf);
@@ -324,10 +334,10 @@ __device__ __forceinline__ int stage1_triangle(const Target& p, const float fa, 
 
     const V2 v_ab = {bs.x - as.x, bs.y - as.y};
     const V2 v_ac = {cs.x - as.x, cs.y - as.y};
-    const float factor = 1.0f / (v_ab.x * v_ac.y - v_ab.y * v_ac.x);
-    const float iza = 1.0f / an.z;
-    const float izb = 1.0f / bn.z;
-    const float izc = 1.0f / cn.z;
+    const float factor = ref_fdiv(1.0f, v_ab.x * v_ac.y - v_ab.y * v_ac.x);
+    const float iza = ref_fdiv(1.0f, an.z);
+    const float izb = ref_fdiv(1.0f, bn.z);
+    const float izc = ref_fdiv(1.0f, cn.z);
     const float ds_dx = v_ac.y * factor;
     const float ds_dy = -v_ac.x * factor;
     const float dt_dx = -v_ab.y * factor;
@@ -352,7 +362,7 @@ __device__ __forceinline__ int stage1_triangle(const Target& p, const float fa, 
             const float v = 1.0f - (s + t);
             if (s > 0.0f && t > 0.0f && v > 0.0f && (uint32_t)pid < numPixels) {
                 const float inv_depth = v * iza + s * izb + t * izc;
-                const float depth = 1.0f / inv_depth;
+                const float depth = ref_fdiv(1.0f, inv_depth);
                 fb_min(p.fb, (uint32_t)pid, pack_pixel(depth, id));
             }
             s += ds_dx;
@@ -381,7 +391,7 @@ __device__ __forceinline__ void stage1_own_raster(const Target& p, const S1Raste
             const float v = 1.0f - (s + t);
             if (s > 0.0f && t > 0.0f && v > 0.0f && (uint32_t)pid < numPixels) {
                 const float inv_depth = v * r.iza + s * r.izb + t * r.izc;
-                const float depth = 1.0f / inv_depth;
+                const float depth = ref_fdiv(1.0f, inv_depth);
                 fb_min(p.fb, (uint32_t)pid, pack_pixel(depth, id));
             }
             s += r.ds_dx;
@@ -448,7 +458,7 @@ __device__ __forceinline__ void stage1_coop_raster(const Target& p, const bool m
             const float v = 1.0f - (s + t);
             if (s > 0.0f && t > 0.0f && v > 0.0f && (uint32_t)pid < numPixels) {
                 const float inv_depth = v * iza + s * izb + t * izc;
-                const float depth = 1.0f / inv_depth;
+                const float depth = ref_fdiv(1.0f, inv_depth);
                 fb_min(p.fb, (uint32_t)pid, pack_pixel(depth, tid));
             }
             s += ds_dx;
@@ -695,6 +705,60 @@ __device__ bool box_misses_samples(const Mat& M, float fa, float f, int W, int H
     }
     return Sy < 1e30 &&
            axis_misses_samples(f, by, sty, bz, stz, invD, ED, fabs((double)f) * Sy, Sz, (double)H, invH);
+}
+
+// True if every triangle of an item is culled by stage 1's back-face test
+// (tv.cu:168-188) for this instance.  With the world-view matrix [R | t] and
+// the camera e = -R^-1 t in object space, the exact value of stage 1's
+// res = av . ((bv - av) x (cv - av)) is det R ((pa - e) . n), n the object-space
+// (pb - pa) x (pc - pa); with the mirror flip the test culls when
+// (pa - e) . n >= 0.  From the item's box (centre c, half-diagonal r) and
+// normal cone (axis m, every unit normal within acos cosT of it),
+// (pa - e) . n >= |n| G with G = |c - e| cos(phi + theta) - r, phi the angle
+// between c - e and m.  The float res differs from the exact one by at most
+// E: the transform's rounding (each view coordinate within gamma_3 T of the
+// exact one, T = sum_j |R_ij| |p_j| + |t_i|), the edge subtractions, the cross
+// and dot products (gamma_2 and gamma_3 of their magnitude bounds), with |av| <=
+// |R|_F (|c - e| + r) and edges <= |R|_F edge; E is doubled.  When
+// |det R| nMin G > E every triangle's float res has the sign that culls it.
+// B: CR_BACK_DOUBLES of the instance; cone: CR_CONE_FLOATS of the item.
+__device__ __noinline__ bool item_back_facing(const double* B, const float* cone, const float lo[3],
+                                                 const float hi[3]) {
+    const double detA = B[3];
+    const double cosT = (double)__ldg(cone + 3);
+    if (!(detA > 0.0) || !(cosT > 0.0)) return false;
+    double w[3], r2 = 0.0, P = 0.0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        const double c = 0.5 * ((double)lo[j] + (double)hi[j]);
+        const double h = 0.5 * ((double)hi[j] - (double)lo[j]);
+        w[j] = c - B[j];
+        r2 += h * h;
+        P = fmax(P, fmax(fabs((double)lo[j]), fabs((double)hi[j])));
+    }
+    const double r = sqrt(r2);
+    const double wl = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+    const double m0 = __ldg(cone), m1 = __ldg(cone + 1), m2 = __ldg(cone + 2);
+    const double ml = sqrt(m0 * m0 + m1 * m1 + m2 * m2);
+    if (!(wl > 0.0) || !(ml > 0.0)) return false;
+    const double cosPhi = fmin(1.0, fmax(-1.0, (w[0] * m0 + w[1] * m1 + w[2] * m2) / (wl * ml)));
+    const double sinPhi = sqrt(fmax(0.0, 1.0 - cosPhi * cosPhi));
+    const double sinT = sqrt(fmax(0.0, 1.0 - cosT * cosT));
+    // rounding of e, the centre and the angles in double: far below 1e-9 of
+    // the magnitudes involved
+    const double el = sqrt(B[0] * B[0] + B[1] * B[1] + B[2] * B[2]);
+    const double G = wl * (cosPhi * cosT - sinPhi * sinT) - r - 1e-9 * (wl + r + el + P);
+    if (!(G > 0.0)) return false;
+    const double u = 5.9604644775390625e-08;  // 2^-24
+    const double g2 = 2.0 * u / (1.0 - 2.0 * u), g3 = 3.0 * u / (1.0 - 3.0 * u);
+    const double a = B[4] * (wl + r);                // |av| bound
+    const double L = B[4] * (double)__ldg(cone + 5);  // edge length bound in view space
+    const double Delta = 1.7320508075688774 * g3 * (B[5] * P + B[6]);  // |av - A| bound
+    const double eta = 2.01 * Delta + u * L;         // |fl(bv - av) - (B - A)| bound
+    const double Lp = L + eta;
+    const double E = 2.0 * ((Delta + a * 3.4641016151377548 * g2 + g3 * (a + Delta)) * Lp * Lp * 1.01 +
+                            a * (2.0 * eta * L + eta * eta));
+    return isfinite(E) && detA * (double)__ldg(cone + 4) * G > E;
 }
 
 // Cell record of one vertex: the outcode plus stage 1's own screen position
@@ -1225,8 +1289,13 @@ __global__ void __launch_bounds__(WARPS * 32) k_stage2(const CrFrameParams p) {
             o.start_y = floorf(su.min_y);
             o.size_x = su.size_x;
             o.size_y = su.numFragments / su.size_x;
-            o.sp = s2_span_setup(o.start_x, o.start_y, o.size_x, o.size_y, su.asx, su.asy, su.abx, su.aby, su.acx,
-                                 su.acy, su.inv_det);
+            if constexpr (REF_MATH) {  // every fragment of the box is tested
+                o.sp.whole = true;
+                o.sp.size_x = o.size_x;
+            } else {
+                o.sp = s2_span_setup(o.start_x, o.start_y, o.size_x, o.size_y, su.asx, su.asy, su.abx, su.aby,
+                                     su.acx, su.acy, su.inv_det);
+            }
             o.fb = MULTI ? tg.fb : p.fb;
             o.asx = su.asx;
             o.asy = su.asy;
@@ -1468,8 +1537,8 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_stage3(const CrFrameParams p)
         // rows in two groups of 32: each lane finds the passing columns of
         // rows lane and lane + 32, then each group's spans are packed across
         // the lanes
-        int spanLo[2], spanLen[2];
-        {
+        int spanLo[2] = {0, 0}, spanLen[2] = {CR_TILE_SIZE, CR_TILE_SIZE};
+        if constexpr (!REF_MATH) {  // the fast-math build traces every pixel of the tile
             const S3Prune P = s3_prune_setup(av, e1, e2, fa, f);
 #pragma unroll
             for (int g = 0; g < 2; ++g)

@@ -165,7 +165,15 @@ enum cr_render_flags {
     CR_RENDER_KEEP_ORDER = 1u << 1,    /* do not sort instances (ids follow input) */
     CR_RENDER_NO_RESOLVE = 1u << 2,    /* visbuffer only                            */
     CR_RENDER_NO_CLEAR = 1u << 3,      /* accumulate into an existing visbuffer     */
-    CR_RENDER_TIMING = 1u << 4         /* record per-stage device times             */
+    CR_RENDER_TIMING = 1u << 4,        /* record per-stage device times             */
+    /* cr_render only: the arithmetic of the reference's own --use_fast_math
+     * build (its __fdividef calls, approximate divisions and square roots,
+     * contracted products), so that the visbuffer matches a CuRast built
+     * with its default recipe.  Every triangle takes the reference's
+     * per-triangle path (no exact culling proofs): a frame costs about what
+     * the reference's kernels cost.  Per-stage times report stages 1-3 as
+     * stage 1. */
+    CR_RENDER_REF_MATH = 1u << 5
 };
 
 /* Per-stage device time summed over the frames rendered with
