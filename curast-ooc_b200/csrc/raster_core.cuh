@@ -1075,9 +1075,11 @@ __device__ __forceinline__ int stage2_setup(const CrFrameParams& p, const Target
 // When every bound is a small number of pixels (|g0| + |g1| (|sy| + 1) below
 // 2^12 over the box, and no condition is of kind 0), the rows are narrowed
 // in float: the float evaluation of g0 + g1 * sy, with g0, g1 and sy rounded
-// to float, is then within 2^-8 pixel of the double one, far inside the
-// whole pixel each span is widened by on both sides (s2_row_span), so the
-// float spans keep every column the double spans keep.
+// to float (and the subtraction of the box's first column), is then within
+// 2^-8 pixel of the double one, inside the 2^-7 pixel each float span is
+// widened by on both sides (s2_row_span), so the float spans keep every column
+// the double spans keep.  A span is the columns between the bounds, nothing
+// more: the bounds hold the float test's error margins already.
 struct S2Span {
     double g0[3], g1[3];  // per condition: bound (or emptiness test) = g0 + g1 * sy
     int kind[3];          // 1: lower bound on px, -1: upper bound, 0: empty if g0 + g1 * sy < 0
@@ -1158,8 +1160,10 @@ __device__ __forceinline__ void s2_row_span(const S2Span& P, float py, float asy
             if (P.kind[k] > 0) lo = fmaxf(lo, g);
             else hi = fminf(hi, g);
         }
-        float flo = floorf(lo - px0) - 1.0f;
-        float fhi = ceilf(hi - px0) + 1.0f;
+        // the float bounds are within 2^-8 pixel of the double ones: keep
+        // every column within 2^-7 of the kept interval
+        float flo = ceilf(lo - px0 - 0.0078125f);
+        float fhi = floorf(hi - px0 + 0.0078125f);
         flo = fmaxf(flo, 0.0f);
         fhi = fminf(fhi, (float)(P.size_x - 1));
         if (!(flo <= fhi)) {
@@ -1182,8 +1186,11 @@ __device__ __forceinline__ void s2_row_span(const S2Span& P, float py, float asy
             return;
         }
     }
-    double flo = floor(lo - P.px0) - 1.0;
-    double fhi = ceil(hi - P.px0) + 1.0;
+    // the bounds hold the float test's error margins already; 1e-9 of
+    // their size covers the double rounding of g0 + g1 sy
+    const double eps = 1e-9 * (1.0 + fabs(lo) + fabs(hi) + fabs(P.px0));
+    double flo = ceil(lo - P.px0 - eps);
+    double fhi = floor(hi - P.px0 + eps);
     flo = fmax(flo, 0.0);
     fhi = fmin(fhi, (double)(P.size_x - 1));
     if (!(flo <= fhi)) {
