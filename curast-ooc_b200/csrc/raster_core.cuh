@@ -1513,8 +1513,16 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_stage3(const CrFrameParams p)
     const uint64_t gw = (uint64_t)blockIdx.x * WARPS + (threadIdx.x >> 5);
     const uint64_t nw = (uint64_t)gridDim.x * WARPS;
     const uint64_t count = min((uint64_t)p.counters[CR_CTR_HUGE], p.hugeCap);
+    // With fewer tiles than warps each tile is split into 2, 4 or 8 bands of
+    // rows, a warp per band, so that more warps share the frame's few tiles.
+    uint32_t nb = 1;
+    while (nb < 8 && count * (uint64_t)(2 * nb) <= nw) nb *= 2;
+    const int rpb = CR_TILE_SIZE / (int)nb;  // rows per band: 64, 32, 16 or 8
+    const uint64_t units = count * nb;
 
-    for (uint64_t ti = gw; ti < count; ti += nw) {
+    for (uint64_t wi = gw; wi < units; wi += nw) {
+        const uint64_t ti = wi / nb;
+        const int row0 = (int)(wi - ti * nb) * rpb;
         const CrTile tile = p.hugeList[ti];
         const uint32_t inst = (uint32_t)tile.instance & (uint32_t)CR_ENTRY_INST_MASK;
         const uint32_t view = MULTI ? ((uint32_t)tile.instance >> 26) : 0u;
@@ -1541,19 +1549,26 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_stage3(const CrFrameParams p)
         const float min_y = clamp_ref((float)(tile.tile_y * CR_TILE_SIZE), 0.0f, Hf);
         const float fx0 = floorf(min_x);
         const float fy0 = floorf(min_y);
-        // rows in two groups of 32: each lane finds the passing columns of
-        // rows lane and lane + 32, then each group's spans are packed across
-        // the lanes
-        int spanLo[2] = {0, 0}, spanLen[2] = {CR_TILE_SIZE, CR_TILE_SIZE};
+        // the band's rows in groups of 32: lane l of group g finds the
+        // passing columns of row row0 + 32 g + l, then each group's spans are
+        // packed across the lanes
+        const int groups = (rpb + 31) / 32;
+        int spanLo[2] = {0, 0}, spanLen[2] = {0, 0};
+#pragma unroll
+        for (int g = 0; g < 2; ++g)
+            if (g < groups && 32 * g + lane < rpb) spanLen[g] = CR_TILE_SIZE;
         if constexpr (!REF_MATH) {  // the fast-math build traces every pixel of the tile
             const S3Prune P = s3_prune_setup(av, e1, e2, fa, f);
 #pragma unroll
             for (int g = 0; g < 2; ++g)
-                s3_row_span(P, fx0, (float)(int)(fy0 + (float)(32 * g + lane)), Wf, Hf, fa, f, spanLo[g], spanLen[g]);
+                if (spanLen[g])
+                    s3_row_span(P, fx0, (float)(int)(fy0 + (float)(row0 + 32 * g + lane)), Wf, Hf, fa, f,
+                                spanLo[g], spanLen[g]);
         }
 #pragma unroll
         for (int g = 0; g < 2; ++g) {
-            const int r0 = 32 * g;
+            if (g >= groups) break;
+            const int r0 = row0 + 32 * g;
             const int xlo = spanLo[g], len = spanLen[g];
             int incl = len;
 #pragma unroll
