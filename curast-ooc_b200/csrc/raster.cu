@@ -123,6 +123,21 @@ __global__ void __launch_bounds__(THREADS, VX_MIN_BLOCKS) k_vertex(const CrFrame
             g = geom_of(ch.I);
         }
         const float* sp = s_pos[slot];
+        if (ch.src && p.cellMode == CR_REC_CELLS32 && ch.v1 - ch.v0 == (uint32_t)CR_VCHUNK) {
+            // a full chunk in shared memory, 4-byte records: each thread's
+            // four vertices as one straight-line block (independent work to
+            // overlap), records stored after all four are formed
+            static_assert(CR_VCHUNK % THREADS == 0, "whole vertices per thread");
+            uint32_t rec[CR_VCHUNK / THREADS];
+#pragma unroll
+            for (int k = 0; k < CR_VCHUNK / THREADS; ++k) {
+                const uint32_t i = 3u * (threadIdx.x + k * THREADS);
+                rec[k] = vertex_cell32<true>(M, V3{sp[i], sp[i + 1], sp[i + 2]}, fa, p.f, Wf, Hf, Wm1, Hm1);
+            }
+#pragma unroll
+            for (int k = 0; k < CR_VCHUNK / THREADS; ++k)
+                reinterpret_cast<uint32_t*>(p.outcodes)[outBase + ch.v0 + threadIdx.x + k * THREADS] = rec[k];
+        } else
         for (uint32_t v = ch.v0 + threadIdx.x; v < ch.v1; v += THREADS) {
             V3 q;
             if (ch.src) {
