@@ -1142,7 +1142,7 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
     // and per-item vertex lists; the choice changes speed only, never the output
     const uint32_t rec = ctx->cfg.cull_records;
     // the reference build's arithmetic: no records, no culling proofs
-    const bool refMath = (flags & CR_RENDER_REF_MATH) != 0;
+    const bool refMath = (flags & (CR_RENDER_REF_MATH | CR_RENDER_REF_MATH_NO_FMA)) != 0;
     bool instanced = false;  // some mesh drawn more than once
     if (rec == CR_CULL_AUTO && count > 1 && !refMath) {
         std::vector<uint32_t> ms(count);
@@ -1292,7 +1292,9 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
         CR_CUDA(mark(1), "event");
         if (refMath) {  // stages 1-3 in the reference build's arithmetic
             CR_CUDA(mark(2), "event");
-            if (raster && count && cr_launch_ref_raster(fp, stream))
+            if (raster && count &&
+                ((flags & CR_RENDER_REF_MATH_NO_FMA) ? cr_launch_ref_raster_nofma(fp, stream)
+                                                     : cr_launch_ref_raster(fp, stream)))
                 return fail(CR_ERR_CUDA, "raster launch: %s", cudaGetErrorString(cudaGetLastError()));
             CR_CUDA(mark(3), "event");
             CR_CUDA(mark(4), "event");

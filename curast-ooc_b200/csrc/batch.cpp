@@ -83,7 +83,8 @@ void use_lists(const BatchTables& B, CrFrameParams& fp) {
 cr_status check_views(const cr_view* views, uint32_t nv, uint32_t flags) {
     if (!views || nv == 0) return fail(CR_ERR_INVALID, "batched render: no views");
     if (nv > CR_MAX_BATCH_VIEWS) return fail(CR_ERR_INVALID, "batched render: %u views (at most %u)", nv, CR_MAX_BATCH_VIEWS);
-    if (flags & CR_RENDER_REF_MATH) return fail(CR_ERR_INVALID, "batched render: CR_RENDER_REF_MATH is cr_render's only");
+    if (flags & (CR_RENDER_REF_MATH | CR_RENDER_REF_MATH_NO_FMA))
+        return fail(CR_ERR_INVALID, "batched render: CR_RENDER_REF_MATH is cr_render's only");
     for (uint32_t v = 0; v < nv; v++) {
         const cr_camera& c = views[v].camera;
         if (c.width <= 0 || c.height <= 0 || (uint64_t)c.width * c.height >= (1ull << 31))

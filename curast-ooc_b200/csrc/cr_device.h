@@ -334,6 +334,8 @@ int cr_launch_resolve(const CrResolveParams& p, void* stream);
 // Stages 1-3 of a frame in the reference build's fast-math arithmetic
 // (raster_ref.cu): every triangle through the per-triangle path.
 int cr_launch_ref_raster(const CrFrameParams& p, void* stream);
+// The same without contracted products (raster_ref_nofma.cu).
+int cr_launch_ref_raster_nofma(const CrFrameParams& p, void* stream);
 
 // Mesh preparation (meshprep.cu): the box of the vertices of every CR_BATCH
 // and every CR_SUB consecutive triangles and of every CR_VCHUNK consecutive

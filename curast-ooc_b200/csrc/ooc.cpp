@@ -347,7 +347,7 @@ cr_status cr_ooc_select(cr_ooc* o, const cr_camera* cam, uint8_t* visible) {
 cr_status cr_ooc_render(cr_ooc* o, const cr_camera* cam, uint64_t d_visbuffer, uint64_t d_rgba, int32_t display,
                         uint32_t flags, void* stream_, cr_ooc_stats* stats) {
     if (!o || !cam) return fail(CR_ERR_INVALID, "cr_ooc_render: NULL argument");
-    if (flags & (CR_RENDER_KEEP_ORDER | CR_RENDER_NO_CLEAR | CR_RENDER_REF_MATH))
+    if (flags & (CR_RENDER_KEEP_ORDER | CR_RENDER_NO_CLEAR | CR_RENDER_REF_MATH | CR_RENDER_REF_MATH_NO_FMA))
         return fail(CR_ERR_INVALID, "cr_ooc_render: KEEP_ORDER, NO_CLEAR and REF_MATH are not accepted");
     cudaStream_t stream = (cudaStream_t)stream_;
     CR_CUDA(cudaSetDevice(o->ctx->device), "cudaSetDevice");

@@ -13,6 +13,12 @@
 #define CR_REF_MATH 1
 #include "raster_core.cuh"
 
+// The entry point's name: raster_ref_nofma.cu compiles this file again under
+// another name and flags.
+#ifndef CR_REF_RASTER_ENTRY
+#define CR_REF_RASTER_ENTRY cr_launch_ref_raster
+#endif
+
 namespace {
 
 constexpr int REF_WARPS = 8;
@@ -94,7 +100,7 @@ int blocks_for(Kernel k, int threads) {
 // Stages 1-3 of a CR_RENDER_REF_MATH frame (after the clear, before the
 // resolve).  The frame's segments, items and queues are those of an
 // ordinary frame; the record and cull fields of p are not read.
-int cr_launch_ref_raster(const CrFrameParams& p, void* stream) {
+int CR_REF_RASTER_ENTRY(const CrFrameParams& p, void* stream) {
     const cudaStream_t st = (cudaStream_t)stream;
     const unsigned T = REF_WARPS * 32;
     if (p.numItems) {

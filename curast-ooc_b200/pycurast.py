@@ -40,6 +40,7 @@ CR_RENDER_NO_RESOLVE = 1 << 2
 CR_RENDER_NO_CLEAR = 1 << 3
 CR_RENDER_TIMING = 1 << 4
 CR_RENDER_REF_MATH = 1 << 5
+CR_RENDER_REF_MATH_NO_FMA = 1 << 6
 STAGES = ("clear", "vertex", "stage1", "stage2", "stage3", "resolve")
 
 CLEAR_PIXEL = 0xFFFFFFF000000000

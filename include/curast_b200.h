@@ -173,7 +173,12 @@ enum cr_render_flags {
      * per-triangle path (no exact culling proofs): a frame costs about what
      * the reference's kernels cost.  Per-stage times report stages 1-3 as
      * stage 1. */
-    CR_RENDER_REF_MATH = 1u << 5
+    CR_RENDER_REF_MATH = 1u << 5,
+    /* cr_render only (implies CR_RENDER_REF_MATH): the arithmetic of the
+     * reference's recipe with --fmad=false added after --use_fast_math (no
+     * contracted products).  A CuRast built that way draws the same
+     * visbuffer bit for bit. */
+    CR_RENDER_REF_MATH_NO_FMA = 1u << 6
 };
 
 /* Per-stage device time summed over the frames rendered with

@@ -10,6 +10,11 @@ with NVRTC, for sm_100a, into `oracle/_ref/`:
       --dlink-time-opt, C++20; nvJitLink -lto -O3 at :365-374).  Used to
       time the reference implementation on the same GPU.
 
+  ref_tv_fastnofma.cubin / ref_resolve_fastnofma.cubin
+      The reference's recipe with --fmad=false added after --use_fast_math
+      (approximate divisions and square roots, no contracted products), as a
+      cubin without link-time optimisation.
+
   ref_tv_ieee.cubin / ref_resolve_ieee.cubin
       Same sources with IEEE float semantics: --fmad=false (no contraction),
       --prec-div=true, --prec-sqrt=true, --ftz=false, and every
@@ -148,6 +153,15 @@ def build(ref: str, force: bool = False) -> None:
                         "--relocatable-device-code=true", "--dlink-time-opt", "--split-compile=0"] + common
                 ltoir = _nvrtc_compile(src, os.path.basename(path), opts, want_ltoir=True)
                 cubin = _jitlink(ltoir, os.path.basename(path))
+                with open(out, "wb") as fh:
+                    fh.write(cubin)
+            # fastnofma: the reference's own recipe with --fmad=false added (its
+            # fast-math approximations without contracted products), built
+            # without link-time optimisation so nothing re-contracts at link
+            out = os.path.join(OUT, f"ref_{key}_fastnofma.cubin")
+            if force or not os.path.exists(out):
+                opts = [f"--gpu-architecture={ARCH}", "--use_fast_math", "--fmad=false"] + common
+                cubin = _nvrtc_compile(src, os.path.basename(path), opts, want_ltoir=False)
                 with open(out, "wb") as fh:
                     fh.write(cubin)
             # ieee: no contraction, IEEE div/sqrt, __fdividef -> IEEE division

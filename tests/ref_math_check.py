@@ -1,5 +1,7 @@
 """Compares CR_RENDER_REF_MATH frames with the reference's own kernels in
-their native --use_fast_math build.  Run in its own process by
+their native --use_fast_math build (argument "native", the default), or
+CR_RENDER_REF_MATH_NO_FMA frames with the reference built with --fmad=false
+added to that recipe (argument "fastnofma").  Run in its own process by
 tests/test_ref_math_gpu.py: the reference harness holds one build mode per
 process and the other parity tests use the IEEE one.  Prints one JSON line
 per scene: pixels whose visbuffer words differ, the covered pixels, and both
@@ -27,13 +29,15 @@ CLEAR = np.uint64(0xFFFFFFF000000000)
 STAGE_COLOURS = {0xffbd8832: 1, 0xffa4ddab: 2, 0xff61aefd: 3}
 
 
+FLAGS = pc.CR_RENDER_SYNC | pc.CR_RENDER_KEEP_ORDER | pc.CR_RENDER_REF_MATH
+
+
 def ours(ctx, handles, instances, view, proj, W, H):
     vis = torch.empty(W * H, dtype=torch.int64, device="cuda")
     rgba = torch.empty(W * H, dtype=torch.int32, device="cuda")
     cam = pc.make_camera(view, proj, W, H)
     ctx.render([(handles[m], w) for m, w in instances], cam, vis.data_ptr(), rgba.data_ptr(),
-               display=pc.CR_DISPLAY_STAGE,
-               flags=pc.CR_RENDER_SYNC | pc.CR_RENDER_KEEP_ORDER | pc.CR_RENDER_REF_MATH)
+               display=pc.CR_DISPLAY_STAGE, flags=FLAGS)
     torch.cuda.synchronize()
     st, stats = ctx.stats()
     assert st == pc.CR_OK
@@ -69,7 +73,13 @@ def compare(name, ctx, ref, meshes, instances, view, proj, W, H, cap=1 << 22):
 
 
 def main():
-    ref = ol.Reference("native")
+    # "native": the reference's own recipe against CR_RENDER_REF_MATH;
+    # "fastnofma": the recipe with --fmad=false against CR_RENDER_REF_MATH_NO_FMA
+    global FLAGS
+    mode = sys.argv[1] if len(sys.argv) > 1 else "native"
+    if mode == "fastnofma":
+        FLAGS |= pc.CR_RENDER_REF_MATH_NO_FMA
+    ref = ol.Reference(mode)
     with pc.Context() as ctx:
         for name in golden_cases.CASES:
             c = golden_cases.case(name)

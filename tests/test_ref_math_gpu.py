@@ -1,5 +1,6 @@
 """CR_RENDER_REF_MATH: frames in the arithmetic of the reference's own
---use_fast_math build, compared with the reference's kernels in that build
+--use_fast_math build, compared with the reference's kernels in that build;
+CR_RENDER_REF_MATH_NO_FMA: the same recipe with --fmad=false added, bit-exact
 (tests/ref_math_check.py, run in its own process because the reference
 harness holds one build mode per process)."""
 import json
@@ -44,6 +45,24 @@ def test_ref_math_matches_the_fast_math_reference(gpu):
         # build's code does not reproduce
         assert c["differ"] - c["same_triangle_other_depth"] <= 2, c
         assert c["differ"] <= 0.005 * c["covered"], c
+
+
+def test_ref_math_without_contraction_is_bit_exact(gpu):
+    """CR_RENDER_REF_MATH_NO_FMA against the reference built with its own
+    recipe plus --fmad=false: every pixel of every scene, all three stages."""
+    if not os.path.exists(ol.HARNESS_SO):
+        pytest.skip("reference harness not built")
+    script = os.path.join(HERE, "ref_math_check.py")
+    res = subprocess.run([sys.executable, script, "fastnofma"], capture_output=True, text=True, timeout=900)
+    assert res.returncode == 0, res.stderr[-2000:]
+    cases = [json.loads(line) for line in res.stdout.splitlines() if line.startswith("{")]
+    assert len(cases) >= 9
+    for c in cases:
+        assert c["covered"] > 0, c
+        assert c["differ"] == 0, c
+        assert c["nontrivial"][0] == c["nontrivial"][1] and c["huge_tiles"][0] == c["huge_tiles"][1], c
+    # the scenes reach every stage
+    assert sum(c["huge_tiles"][0] for c in cases) > 0 and sum(c["nontrivial"][0] for c in cases) > 0
 
 
 def test_ref_math_is_cr_render_only(gpu):
