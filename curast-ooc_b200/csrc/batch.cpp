@@ -757,6 +757,7 @@ cr_status cr_autotune_batch(cr_context* ctx, const cr_instance* instances, uint3
     auto total = [](const float ms[6]) { return ms[0] + ms[1] + ms[2] + ms[3] + ms[4]; };
 
     CrBatchShape best = ctx->bshape;
+    const uint32_t keepSmall = ctx->cfg.threshold_small;
     float ms[6];
     s = measure(best, ms);  // also grows the queues to the frame's demand
     if (s) return s;
@@ -850,8 +851,17 @@ cr_status cr_autotune_batch(cr_context* ctx, const cr_instance* instances, uint3
         }
         ctx->cfg.threshold_small = bestThr;
     }
-    float after[6];
+    // keep the tuned shapes only where they beat the occupancy defaults
+    // clearly (by 2 %, above run-to-run noise), timed again side by side;
+    // else the defaults (and the default thresholds) stay
+    float after[6], again[6];
     if ((s = measure(best, after))) return s;
+    if ((s = measure(ctx->bshape, again))) return s;
+    if (!(total(after) < 0.98f * std::min(before, total(again)))) {
+        best = ctx->bshape;
+        ctx->cfg.threshold_small = keepSmall;
+        if ((s = measure(best, after))) return s;
+    }
     cr_tuning t{};
     t.scene_class = sceneClass;
     t.threshold_small = ctx->cfg.threshold_small;

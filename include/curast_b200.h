@@ -408,7 +408,8 @@ typedef struct cr_tuning {
     uint64_t nontrivial_cap;
     uint64_t huge_cap;
     float ms_before;           /* default shapes, device ms per batched frame  */
-    float ms_after;            /* tuned shapes                                 */
+    float ms_after;            /* the shapes kept: the tuned ones when they beat
+                                  the defaults by 2 %, else the defaults      */
     uint32_t candidates;       /* configurations timed                         */
     uint32_t reserved[3];
 } cr_tuning;
