@@ -373,6 +373,7 @@ def plain_algorithmic_bytes(wl, fstats, T):
     rec = 4 if max(wl["W"], wl["H"]) <= 4096 else 8
     items, items_drawn = int(fstats.work_items), int(fstats.work_items_drawn)
     chunks, chunks_eval = int(fstats.vertex_chunks), int(fstats.vertex_chunks_evaluated)
+    slices_eval = int(getattr(fstats, "vertex_slices_evaluated", 0))
     surv = int(getattr(fstats, "stage1_survivors", 0))
     nV_inst = sum(wl["meshes"][m][0].shape[0] for m, _ in wl["instances"])
     if direct:
@@ -384,7 +385,9 @@ def plain_algorithmic_bytes(wl, fstats, T):
         algo = {"vertex": 24 * items + 8 * items_drawn,
                 "stage1": (1408 + 12 * 128) * items_drawn, "boxes": True}
     elif chunks:
-        v_eval = min(nV_inst, chunks_eval * 1024)
+        # the vertex pass evaluates the slices (128 vertices) of its listed
+        # chunks that hold a vertex of a drawn item
+        v_eval = min(nV_inst, slices_eval * 128 if slices_eval else chunks_eval * 1024)
         tri_drawn = min(T, items_drawn * 128)
         algo = {"vertex": 24 * (chunks + items) + (12 + rec) * v_eval + 8 * items_drawn,
                 "stage1": 12 * tri_drawn + rec * min(v_eval, tri_drawn // 2) + 16 * surv}
@@ -568,6 +571,7 @@ def run_ours(args, rank, world, local):
                    "nontrivial": int(fstats.nontrivial), "huge_tiles": int(fstats.huge_tiles),
                    "hierarchical_cull": {"work_items": items, "work_items_drawn": items_drawn,
                                          "vertex_chunks": chunks, "vertex_chunks_evaluated": chunks_eval,
+                                         "vertex_slices_evaluated": int(getattr(fstats, "vertex_slices_evaluated", 0)),
                                          "triangles_in_drawn_items": tri_drawn,
                                          "stage1_survivors": int(fstats.stage1_survivors)},
                    "frame_roofline": {"bytes": frame_bytes, "achieved_gbs": frame_gbs,
@@ -588,7 +592,7 @@ def run_ours(args, rank, world, local):
         # clear, the two frame-cull kernels, the vertex pass (record-culled
         # frames), stage 1 (two kernels when record-culled), stages 2 and 3,
         # the resolve
-        "gpu_launches": (7 if algo.get("boxes") else 9) * args.steps,
+        "gpu_launches": (7 if algo.get("boxes") else 10) * args.steps,
         "clocks": clk,
     }
     if parity is not None:
@@ -719,6 +723,7 @@ def sub_plain(args, wl, ctx, handles, with_parity):
            "cull": {"work_items": int(fstats.work_items), "work_items_drawn": int(fstats.work_items_drawn),
                     "vertex_chunks": int(fstats.vertex_chunks),
                     "vertex_chunks_evaluated": int(fstats.vertex_chunks_evaluated),
+                    "vertex_slices_evaluated": int(getattr(fstats, "vertex_slices_evaluated", 0)),
                     "stage1_survivors": int(fstats.stage1_survivors), "nontrivial": int(fstats.nontrivial),
                     "huge_tiles": int(fstats.huge_tiles)},
            "roofline": {"kernel": {"vertex": "k_cull + k_vertex",

@@ -300,6 +300,7 @@ cr_status assemble(cr_context* ctx, const cr_instance* instances, uint32_t count
             if (m.compressed) s.codec = m.codec;
             s.itemBoxes = m.itemBoxes;
             s.itemCones = m.itemCones;
+            s.itemSlices = m.itemSlices;
             s.subBoxes = m.subBoxes;
             s.localLists = m.localLists;
             s.localCounts = m.localCounts;
@@ -368,22 +369,24 @@ cr_status launch_mesh_boxes(cr_context* ctx, MeshRec& m) {
     const size_t gb = align_up((size_t)((nItems + CR_GROUP - 1) / CR_GROUP) * 24, 256);
     const size_t cgb = align_up((size_t)((nChunks + CR_GROUP - 1) / CR_GROUP) * 24, 256);
     const size_t icb = align_up((size_t)nItems * CR_CONE_FLOATS * 4, 256);
+    const size_t isb = align_up((size_t)nItems * 32, 256);
     if (!m.itemBoxes) {
-        cr_status s = ctx->dev_alloc((void**)&m.itemBoxes, ib + cb + sb + gb + cgb + icb + 256, "mesh boxes");
+        cr_status s = ctx->dev_alloc((void**)&m.itemBoxes, ib + cb + sb + gb + cgb + icb + isb + 256, "mesh boxes");
         if (s) return s;
         m.chunkBoxes = (float*)((char*)m.itemBoxes + ib);
         m.subBoxes = (float*)((char*)m.itemBoxes + ib + cb);
         m.groupBoxes = (float*)((char*)m.itemBoxes + ib + cb + sb);
         m.chunkGroupBoxes = (float*)((char*)m.itemBoxes + ib + cb + sb + gb);
         m.itemCones = (float*)((char*)m.itemBoxes + ib + cb + sb + gb + cgb);
-        m.boxBytes = ib + cb + sb + gb + cgb + icb + 256;
+        m.itemSlices = (uint4*)((char*)m.itemBoxes + ib + cb + sb + gb + cgb + icb);
+        m.boxBytes = ib + cb + sb + gb + cgb + icb + isb + 256;
     }
-    m.meshBox = (float*)((char*)m.itemBoxes + ib + cb + sb + gb + cgb + icb);
+    m.meshBox = (float*)((char*)m.itemBoxes + ib + cb + sb + gb + cgb + icb + isb);
     m.dCodec = (CrCodec*)((char*)m.meshBox + 64);
     CR_CUDA(cudaMemcpy(m.dCodec, &m.codec, sizeof(CrCodec), cudaMemcpyHostToDevice), "mesh codec");
     if (cr_launch_mesh_boxes(m.indices, m.positions, m.compressed ? m.dCodec : nullptr, m.numTriangles,
                              m.numVertices, m.itemBoxes, m.chunkBoxes, m.subBoxes, m.meshBox, m.groupBoxes,
-                             m.chunkGroupBoxes, m.itemCones, 0))
+                             m.chunkGroupBoxes, m.itemCones, m.itemSlices, 0))
         return fail(CR_ERR_CUDA, "mesh box launch: %s", cudaGetErrorString(cudaGetLastError()));
     return CR_OK;
 }
@@ -522,6 +525,8 @@ void read_counters(cr_context* ctx) {
     ctx->last.overflow = c[CR_CTR_OVERFLOW];
     ctx->last.work_items_drawn = ctx->last.work_items ? c[CR_CTR_ITEMS] : 0;
     ctx->last.vertex_chunks_evaluated = ctx->last.vertex_chunks ? c[CR_CTR_CHUNKS] : 0;
+    ctx->last.vertex_slices_evaluated =
+        !ctx->last.vertex_chunks ? 0 : ctx->lastStamps ? c[CR_CTR_VSLICES] : c[CR_CTR_CHUNKS] * (CR_VCHUNK / CR_VSLICE);
     ctx->last.stage1_survivors = c[CR_CTR_SURVIVORS];
 }
 
@@ -1197,6 +1202,7 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
         CR_CUDA(cudaDeviceSynchronize(), "cull buffer resize");
         ctx->dev_free(ctx->itemList, ctx->itemBytes);
         ctx->itemList = nullptr;
+        ctx->sliceNeed = nullptr;
         ctx->itemCap = ctx->chunkCap = ctx->unitCap = ctx->cgroupCap = ctx->itemBytes = 0;
         const uint64_t items = A.numItems + A.numItems / 8 + 1024;
         const uint64_t chunks = A.numVChunks + A.numVChunks / 8 + 1024;
@@ -1206,9 +1212,13 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
         const size_t oClass = oChunks + align_up(chunks * 4, 256);
         const size_t oUnits = oClass + align_up(chunks, 256);
         const size_t oGroups = oUnits + align_up(units * 8, 256);
-        const size_t bytes = oGroups + align_up(cgroups * 8, 256);
+        const size_t oNeed = oGroups + align_up(cgroups * 8, 256);
+        const size_t bytes = oNeed + align_up(chunks * (CR_VCHUNK / CR_VSLICE) * 4, 256);
         s = ctx->dev_alloc((void**)&ctx->itemList, bytes, "cull buffers");
         if (s) return s;
+        ctx->sliceNeed = (uint32_t*)((char*)ctx->itemList + oNeed);
+        CR_CUDA(cudaMemset(ctx->sliceNeed, 0, chunks * (CR_VCHUNK / CR_VSLICE) * 4), "slice stamps");
+        ctx->needStamp = 0;
         ctx->itemCap = items;
         ctx->chunkCap = chunks;
         ctx->unitCap = units;
@@ -1236,6 +1246,20 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
     fp.chunkClass = ctx->chunkClass;
     fp.unitList = ctx->unitList;
     fp.cgroupList = ctx->cgroupList;
+    // the vertex pass evaluates only the slices that hold a vertex of a drawn
+    // item, when every mesh of the frame has its items' slices
+    bool stamps = !direct && !refMath && count > 0 && ctx->sliceNeed != nullptr;
+    for (const CrSegment& sg : A.seg) stamps = stamps && sg.itemSlices != nullptr;
+    if (stamps) {
+        if (++ctx->needStamp == 0) {  // the stamps wrapped: clear them
+            CR_CUDA(cudaMemsetAsync(ctx->sliceNeed, 0, ctx->chunkCap * (CR_VCHUNK / CR_VSLICE) * 4, stream),
+                    "slice stamps");
+            ctx->needStamp = 1;
+        }
+        fp.sliceNeed = ctx->sliceNeed;
+        fp.needStamp = ctx->needStamp;
+    }
+    ctx->lastStamps = stamps;
     if (direct) {  // no vertex pass: no chunks to classify or evaluate
         fp.chunkList = nullptr;
         fp.chunkClass = nullptr;

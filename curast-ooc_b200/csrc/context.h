@@ -47,6 +47,7 @@ struct MeshRec {
     float* groupBoxes = nullptr;  // per CR_GROUP item boxes
     float* chunkGroupBoxes = nullptr;  // per CR_GROUP chunk boxes
     float* itemCones = nullptr;   // per CR_BATCH triangles: CR_CONE_FLOATS normal cone
+    uint4* itemSlices = nullptr;  // per CR_BATCH triangles: two uint4, the slices they use
     float* meshBox = nullptr;     // the whole mesh's box (6 floats)
     size_t boxBytes = 0;
     float box[6] = {NAN, NAN, NAN, NAN, NAN, NAN};  // host copy of the mesh box
@@ -146,6 +147,10 @@ struct cr_context {
     uint32_t* chunkList = nullptr;
     uint8_t* chunkClass = nullptr;
     uint64_t chunkCap = 0;
+    uint32_t* sliceNeed = nullptr;  // per slice of chunkCap chunks: the stamp of the last
+                                    // frame a drawn item used one of its vertices
+    uint32_t needStamp = 0;         // the last frame's stamp (0 is never issued)
+    bool lastStamps = false;        // the last frame's vertex pass evaluated stamped slices only
     size_t itemBytes = 0;
     uint64_t* s1List = nullptr;   // stage-1 survivors of record-culled frames
     uint64_t s1Cap = 0;

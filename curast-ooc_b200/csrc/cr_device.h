@@ -9,7 +9,7 @@
 // Work queues (library-owned, grown on demand):
 //   uint64_t    nontrivial[cap]   (instance << 32 | triangle), tv.cu:192-197
 //   CrTile      huge[cap]         {instance, triangle, tile_x, tile_y}, HostDeviceInterface.h:254-259
-//   unsigned long long counters[8]  see CR_CTR_*
+//   unsigned long long counters[CR_CTR_COUNT]  see CR_CTR_*
 #pragma once
 #include <cstdint>
 
@@ -41,6 +41,7 @@
                                 // (appended by k_s1cull for k_s1raster)
 #define CR_CTR_UNITS 7          // item groups the group cull leaves for the item cull
 #define CR_CTR_CGROUPS 8        // chunk groups the group cull leaves for the chunk cull
+#define CR_CTR_VSLICES 9        // slices the vertex pass evaluated (frames with slice stamps)
 #define CR_CTR_COUNT 16
 
 // Compressed geometry (the reference's IX_PU16 meshes, CMesh fields
@@ -90,6 +91,15 @@ struct alignas(16) CrInstance {
 // beyond a frustum side, so no item box needs classifying; 0: unknown.
 #define CR_MESH_INSIDE 32u
 #define CR_VCHUNK 1024          // vertices per vertex-pass chunk
+#define CR_VSLICE 128           // vertices per slice (8 per chunk): the unit of the
+                                // vertex pass's slice stamps
+// CrSegment::itemSlices, per item q0, q1: the slices its triangles' vertices
+// lie in (an index past the mesh's vertices counts as its last slice), as two
+// windows of 64 slices -- A from q0.x (the least slice), B from q0.y (the
+// least slice at or past q0.x + 64) -- with bit masks q0.z | q0.w << 32 (A)
+// and q1.x | q1.y << 32 (B); q1.z and q1.w & 0x7fffffff are the least and
+// greatest slice, and bit 31 of q1.w says some slice lies past both windows:
+// then every slice from the least to the greatest counts.
 #define CR_GROUP 32             // item boxes per group box, chunk boxes per chunk-group box
 
 // Cell records (8 bytes per (instance, vertex), CrFrameParams::cellMode):
@@ -123,7 +133,8 @@ struct alignas(16) CrSegment {
     const float* groupBoxes;    // per CR_GROUP item boxes: their union (or nullptr)
     uint64_t unitBase;          // first group-cull unit (item group x instance chunk)
     const float* itemCones;     // per item, CR_CONE_FLOATS: its triangles' normal cone (or nullptr)
-    uint64_t pad;
+    const uint4* itemSlices;    // per item, two: the vertex-pass slices its vertices lie in
+                                // (CR_VSLICE; or nullptr)
 };
 static_assert(sizeof(CrSegment) == 144, "CrSegment layout");
 // Per-item normal cone (object space), for the back-face proof of the frame
@@ -257,6 +268,14 @@ struct CrFrameParams {
     // CR_BACK_DOUBLES per instance for the item cull's back-face proof, or
     // nullptr (no proof)
     const double* instBack;
+    // record-culled frames: per vertex-pass slice (CrInstance::vchunkBase *
+    // CR_VCHUNK / CR_VSLICE + slice), needStamp when a drawn item uses one of
+    // its vertices (k_stamp, from CrSegment::itemSlices, after the item cull);
+    // the vertex pass evaluates only those slices of its listed chunks -- the
+    // records stage 1 reads.  nullptr: every slice of a listed chunk.
+    uint32_t* sliceNeed;
+    uint32_t needStamp;
+    uint32_t pad3;
 };
 #define CR_CHUNK_EVAL 0xffu
 
@@ -342,11 +361,12 @@ int cr_launch_ref_raster_nofma(const CrFrameParams& p, void* stream);
 // vertices (a box
 // with a non-finite position is NaN and culls nothing).
 // `codec`: device copy of a compressed mesh's codec, or nullptr.
-// itemCones: per item CR_CONE_FLOATS (or nullptr).
+// itemCones: per item CR_CONE_FLOATS (or nullptr); itemSlices: per item two
+// uint4 (CrSegment::itemSlices, or nullptr).
 int cr_launch_mesh_boxes(const uint32_t* indices, const float* positions, const CrCodec* codec,
                          uint32_t numTriangles, uint32_t numVertices, float* itemBoxes, float* chunkBoxes,
                          float* subBoxes, float* meshBox, float* groupBoxes, float* chunkGroupBoxes,
-                         float* itemCones, void* stream);
+                         float* itemCones, uint4* itemSlices, void* stream);
 // Per-item vertex lists of an indexed mesh (see CR_LOCAL_BYTES).
 int cr_launch_local_lists(const uint32_t* indices, const CrCodec* codec, uint32_t numTriangles, uint8_t* lists,
                           uint32_t* counts, void* stream);

@@ -70,6 +70,69 @@ __global__ void __launch_bounds__(256) k_item_boxes(const uint32_t* idx, const f
     }
 }
 
+// One warp per item: the vertex-pass slices its triangles' vertices lie in
+// (CrSegment::itemSlices: two windows of 64 slices, or the whole range).
+__global__ void __launch_bounds__(256) k_item_slices(const uint32_t* idx, const float* pos, const CrCodec* codec,
+                                                     uint32_t nT, uint32_t nSlices, uint4* out) {
+    const int lane = threadIdx.x & 31;
+    const GeomRef g = geom_from(pos, idx, codec);
+    const uint32_t nItems = (nT + CR_BATCH - 1) / CR_BATCH;
+    constexpr uint32_t NONE = 0xffffffffu;
+    for (uint32_t b = blockIdx.x * 8 + (threadIdx.x >> 5); b < nItems; b += gridDim.x * 8) {
+        uint32_t sl[CR_BATCH / 32][3];
+        uint32_t lo = NONE, hi = 0;
+#pragma unroll
+        for (int r = 0; r < CR_BATCH / 32; ++r) {
+            const uint32_t t = b * CR_BATCH + r * 32 + lane;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                sl[r][k] = t < nT ? min(geom_index(g, 3ull * t + k) / (uint32_t)CR_VSLICE, nSlices - 1) : NONE;
+                if (sl[r][k] != NONE) {
+                    lo = min(lo, sl[r][k]);
+                    hi = max(hi, sl[r][k]);
+                }
+            }
+        }
+        lo = __reduce_min_sync(FULL, lo);
+        hi = __reduce_max_sync(FULL, hi);
+        // window B starts at the least slice past window A
+        uint32_t b0 = NONE;
+#pragma unroll
+        for (int r = 0; r < CR_BATCH / 32; ++r)
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                if (sl[r][k] != NONE && sl[r][k] - lo >= 64u) b0 = min(b0, sl[r][k]);
+        b0 = __reduce_min_sync(FULL, b0);
+        if (b0 == NONE) b0 = lo + 64u;
+        uint32_t a0m = 0, a1m = 0, b0m = 0, b1m = 0;
+        bool past = false;
+#pragma unroll
+        for (int r = 0; r < CR_BATCH / 32; ++r)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                if (sl[r][k] == NONE) continue;
+                const uint32_t d = sl[r][k] - lo;
+                if (d < 32u) a0m |= 1u << d;
+                else if (d < 64u) a1m |= 1u << (d - 32u);
+                else {
+                    const uint32_t e = sl[r][k] - b0;
+                    if (e < 32u) b0m |= 1u << e;
+                    else if (e < 64u) b1m |= 1u << (e - 32u);
+                    else past = true;
+                }
+            }
+        a0m = __reduce_or_sync(FULL, a0m);
+        a1m = __reduce_or_sync(FULL, a1m);
+        b0m = __reduce_or_sync(FULL, b0m);
+        b1m = __reduce_or_sync(FULL, b1m);
+        past = __any_sync(FULL, past);
+        if (lane == 0) {
+            out[2ull * b] = make_uint4(lo, b0, a0m, a1m);
+            out[2ull * b + 1] = make_uint4(b0m, b1m, lo, hi | (past ? 0x80000000u : 0u));
+        }
+    }
+}
+
 // One warp per item: the normal cone of its triangles (CR_CONE_FLOATS, see
 // cr_device.h), computed in double from the float positions.  The axis is the
 // sum of the unit normals rounded to float; cosT is the least cosine between
@@ -355,7 +418,7 @@ int cr_launch_local_lists(const uint32_t* indices, const CrCodec* codec, uint32_
 int cr_launch_mesh_boxes(const uint32_t* indices, const float* positions, const CrCodec* codec,
                          uint32_t numTriangles, uint32_t numVertices, float* itemBoxes, float* chunkBoxes,
                          float* subBoxes, float* meshBox, float* groupBoxes, float* chunkGroupBoxes,
-                         float* itemCones, void* stream) {
+                         float* itemCones, uint4* itemSlices, void* stream) {
     cudaStream_t st = (cudaStream_t)stream;
     const uint32_t nItems = (numTriangles + CR_BATCH - 1) / CR_BATCH;
     const uint32_t nChunks = (numVertices + CR_VCHUNK - 1) / CR_VCHUNK;
@@ -378,6 +441,10 @@ int cr_launch_mesh_boxes(const uint32_t* indices, const float* positions, const 
     if (nItems && itemCones)
         k_item_cones<<<(nItems + 7) / 8 < 148 * 16 ? (nItems + 7) / 8 : 148 * 16, 256, 0, st>>>(
             indices, positions, codec, numTriangles, itemCones);
+    const uint32_t nSlices = (numVertices + CR_VSLICE - 1) / CR_VSLICE;
+    if (nItems && nSlices && itemSlices)
+        k_item_slices<<<(nItems + 7) / 8 < 148 * 16 ? (nItems + 7) / 8 : 148 * 16, 256, 0, st>>>(
+            indices, positions, codec, numTriangles, nSlices, itemSlices);
     if (meshBox) k_mesh_box<<<1, 256, 0, st>>>(itemBoxes, nItems, meshBox);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

@@ -28,150 +28,94 @@
 
 namespace {
 
-// The vertex pass: per listed chunk (CR_VCHUNK consecutive vertices of one
-// instance: the frame cull's CR_CHUNK_EVAL chunks, or every chunk) one block
-// writes each vertex's record -- the outcode byte or the cell record.  A
-// full chunk of a plain mesh whose positions are 16-byte aligned arrives in
-// shared memory as one 12 KB bulk copy (cp.async.bulk), issued VX_STAGES
-// chunks ahead of its use and signalled by an mbarrier (bounded wait), so
-// the pass streams positions instead of waiting on per-thread gathers; other
-// chunks (tails, compressed or unaligned meshes) are read directly.
-#ifndef VX_STAGES
-#define VX_STAGES 3
-#endif
+// The vertex pass writes each vertex's record -- the outcode byte or the cell
+// record -- of the listed chunks (CR_VCHUNK consecutive vertices of one
+// instance: the frame cull's CR_CHUNK_EVAL chunks, or every chunk).  The
+// grid's warps stride over tasks: a chunk, or with few chunks a share of its
+// slices (CR_VSLICE vertices; G = 2, 4 or 8 tasks per chunk, task j taking
+// the slices s = j mod G), so that every warp has several.  With slice stamps
+// (CrFrameParams::sliceNeed) only the slices that hold a vertex of a drawn
+// item are evaluated -- the records stage 1 reads.  A slice is four rounds of
+// 32 consecutive vertices: the warp issues the position loads of all four,
+// then forms the four records (independent work to overlap), each round's
+// loads and stores coalesced.  No block-wide step: warps take tasks
+// independently.
 #ifndef VX_MIN_BLOCKS
 #define VX_MIN_BLOCKS 4
 #endif
-struct VxChunk {
-    const CrInstance* I;
-    uint32_t inst, v0, v1;
-    const float* src;  // bulk-copy source, or nullptr (direct reads)
-};
-
-__device__ __forceinline__ VxChunk vx_chunk(const CrFrameParams& p, uint64_t k) {
-    const uint64_t c = p.chunkList ? (uint64_t)__ldg(p.chunkList + k) : k;
-    uint32_t lo = 0, hi = p.numInstances - 1;  // instance holding chunk c
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi + 1) >> 1;
-        if (__ldg(&p.instances[mid].vchunkBase) <= c) lo = mid;
-        else hi = mid - 1;
-    }
-    VxChunk r;
-    r.I = p.instances + lo;
-    r.inst = lo;
-    r.v0 = (uint32_t)(c - __ldg(&r.I->vchunkBase)) * CR_VCHUNK;
-    r.v1 = min(r.v0 + (uint32_t)CR_VCHUNK, __ldg(&r.I->numVertices));
-    const float* pos = ldg_ptr(&r.I->positions);
-    const bool plain = (__ldg(&r.I->codec.bits) & CR_CODEC_IX_PU16) == 0u;
-    r.src = (plain && r.v1 - r.v0 == (uint32_t)CR_VCHUNK && ((uintptr_t)pos & 15u) == 0u) ? pos + 3ull * r.v0 : nullptr;
-    return r;
-}
+constexpr uint32_t VX_SLICES = CR_VCHUNK / CR_VSLICE;
+static_assert(VX_SLICES <= 8 && CR_VSLICE == 128, "a lane per slice stamp, a byte of slice bits; four rounds of 32 per slice");
 
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS, VX_MIN_BLOCKS) k_vertex(const CrFrameParams p) {
     pdl_enter();
-    constexpr int STAGES = VX_STAGES;
-    constexpr uint32_t BYTES = CR_VCHUNK * 12;
-    __shared__ __align__(128) float s_pos[STAGES][CR_VCHUNK * 3];
-    __shared__ __align__(8) uint64_t s_bar[STAGES];
-    // the chunk each slot holds, decoded once by thread 0 when it fills the slot
-    __shared__ VxChunk s_ch[STAGES];
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t gw = (uint64_t)blockIdx.x * (THREADS / 32) + (threadIdx.x >> 5);
+    const uint64_t nw = (uint64_t)gridDim.x * (THREADS / 32);
     const float fa = p.f / p.aspect;
     const float Wf = (float)p.W, Hf = (float)p.H;
     const float Wm1 = (float)(p.W - 1), Hm1 = (float)(p.H - 1);
     // the chunks the frame cull left for per-vertex records (or every chunk)
     const uint64_t nChunks = p.chunkList ? min((uint64_t)p.counters[CR_CTR_CHUNKS], p.numVChunks) : p.numVChunks;
-    // thread 0 issues the copies; `pending` (its own) marks slots holding an
-    // issued, not yet consumed copy
-    uint32_t pending = 0, parity = 0;
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < STAGES; ++s) mbar_init(&s_bar[s], 1);
-        fence_barrier_init();
-        for (int s = 0; s < STAGES; ++s) {
-            const uint64_t k = blockIdx.x + (uint64_t)s * gridDim.x;
-            if (k >= nChunks) break;
-            s_ch[s] = vx_chunk(p, k);
-            if (s_ch[s].src) {
-                pending |= 1u << s;
-                bulk_load(s_pos[s], s_ch[s].src, BYTES, &s_bar[s]);
-            }
-        }
-    }
-    __syncthreads();
     uint32_t lastInst = 0xffffffffu;
     Mat M;
     uint64_t outBase = 0;
     GeomRef g;
-    uint32_t kk = 0;
-    for (uint64_t k = blockIdx.x; k < nChunks; k += gridDim.x, ++kk) {
-        const int slot = (int)(kk % STAGES);
-        const uint32_t bit = 1u << slot;
-        const VxChunk ch = s_ch[slot];
-        if (ch.src) {
-            const bool ok = mbar_wait_bounded(&s_bar[slot], (parity & bit) ? 1u : 0u, p.waitTimeoutNs);
-            if (__syncthreads_or(!ok)) {  // record, stop the block, drain its copies below
-                if (threadIdx.x == 0) atomicOr(&p.counters[CR_CTR_TIMEOUT], 1ull);
-                break;
-            }
-            parity ^= bit;
-            pending &= ~bit;
+    // tasks per chunk: the least power of two up to VX_SLICES giving every
+    // warp at least four
+    uint32_t lg = 0;
+    while ((1u << lg) < VX_SLICES && (nChunks << lg) < 4 * nw) ++lg;
+    uint32_t run = 0;  // slices evaluated by this warp
+    for (uint64_t t = gw; t < (nChunks << lg); t += nw) {
+        const uint64_t k = t >> lg;
+        const uint32_t part = (uint32_t)(t & ((1u << lg) - 1u));
+        const uint64_t c = p.chunkList ? (uint64_t)__ldg(p.chunkList + k) : k;
+        // this task's slices: s = part mod 2^lg
+        uint32_t slices = 0;
+        for (uint32_t s = part; s < VX_SLICES; s += 1u << lg) slices |= 1u << s;
+        if (p.sliceNeed) {
+            const bool need = lane < VX_SLICES && __ldg(p.sliceNeed + (uint64_t)VX_SLICES * c + lane) == p.needStamp;
+            slices &= __ballot_sync(FULL, need);
         }
-        if (ch.inst != lastInst) {  // the instance's matrix and records, once per run of its chunks
-            lastInst = ch.inst;
-            M = load_mat(p.world_view + 4ull * ch.inst);
-            outBase = __ldg(&ch.I->outBase);
-            g = geom_of(ch.I);
+        if (!slices) continue;  // no drawn item uses its vertices
+        run += (uint32_t)__popc(slices);
+        uint32_t lo = 0, hi = p.numInstances - 1;  // instance holding chunk c
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (__ldg(&p.instances[mid].vchunkBase) <= c) lo = mid;
+            else hi = mid - 1;
         }
-        const float* sp = s_pos[slot];
-        if (ch.src && p.cellMode == CR_REC_CELLS32 && ch.v1 - ch.v0 == (uint32_t)CR_VCHUNK) {
-            // a full chunk in shared memory, 4-byte records: each thread's
-            // four vertices as one straight-line block (independent work to
-            // overlap), records stored after all four are formed
-            static_assert(CR_VCHUNK % THREADS == 0, "whole vertices per thread");
-            uint32_t rec[CR_VCHUNK / THREADS];
+        const CrInstance* I = p.instances + lo;
+        if (lo != lastInst) {  // the instance's matrix and records, once per run of its chunks
+            lastInst = lo;
+            M = load_mat(p.world_view + 4ull * lo);
+            outBase = __ldg(&I->outBase);
+            g = geom_of(I);
+        }
+        const uint32_t v0 = (uint32_t)(c - __ldg(&I->vchunkBase)) * CR_VCHUNK;
+        const uint32_t v1 = min(v0 + (uint32_t)CR_VCHUNK, __ldg(&I->numVertices));
+        for (uint32_t m = slices; m; m &= m - 1) {
+            const uint32_t sv = v0 + (uint32_t)(__ffs(m) - 1) * CR_VSLICE + lane;
+            V3 q[4];
 #pragma unroll
-            for (int k = 0; k < CR_VCHUNK / THREADS; ++k) {
-                const uint32_t i = 3u * (threadIdx.x + k * THREADS);
-                rec[k] = vertex_cell32<true>(M, V3{sp[i], sp[i + 1], sp[i + 2]}, fa, p.f, Wf, Hf, Wm1, Hm1);
-            }
+            for (int r = 0; r < 4; ++r)
+                if (sv + 32u * r < v1) q[r] = pos_of(g, sv + 32u * r);
 #pragma unroll
-            for (int k = 0; k < CR_VCHUNK / THREADS; ++k)
-                reinterpret_cast<uint32_t*>(p.outcodes)[outBase + ch.v0 + threadIdx.x + k * THREADS] = rec[k];
-        } else
-        for (uint32_t v = ch.v0 + threadIdx.x; v < ch.v1; v += THREADS) {
-            V3 q;
-            if (ch.src) {
-                const uint32_t i = 3u * (v - ch.v0);  // stride-3 words: no bank conflicts
-                q = V3{sp[i], sp[i + 1], sp[i + 2]};
-            } else {
-                q = pos_of(g, v);
-            }
-            if (p.cellMode == CR_REC_CELLS32)
-                reinterpret_cast<uint32_t*>(p.outcodes)[outBase + v] = vertex_cell32<true>(M, q, fa, p.f, Wf, Hf, Wm1, Hm1);
-            else if (p.cellMode == CR_REC_CELLS)
-                reinterpret_cast<uint64_t*>(p.outcodes)[outBase + v] = vertex_cell_record(M, q, fa, p.f, Wf, Hf, p.W, p.H);
-            else
-                p.outcodes[outBase + v] = (uint8_t)vertex_outcode(M, q, fa, p.f);
-        }
-        __syncthreads();  // every read of this slot is done: refill it
-        if (threadIdx.x == 0) {
-            const uint64_t nk = k + (uint64_t)STAGES * gridDim.x;
-            if (nk < nChunks) {
-                s_ch[slot] = vx_chunk(p, nk);
-                if (s_ch[slot].src) {
-                    pending |= bit;
-                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                    bulk_load(s_pos[slot], s_ch[slot].src, BYTES, &s_bar[slot]);
-                }
+            for (int r = 0; r < 4; ++r) {
+                const uint32_t v = sv + 32u * r;
+                if (v >= v1) continue;
+                if (p.cellMode == CR_REC_CELLS32)
+                    reinterpret_cast<uint32_t*>(p.outcodes)[outBase + v] =
+                        vertex_cell32<true>(M, q[r], fa, p.f, Wf, Hf, Wm1, Hm1);
+                else if (p.cellMode == CR_REC_CELLS)
+                    reinterpret_cast<uint64_t*>(p.outcodes)[outBase + v] =
+                        vertex_cell_record(M, q[r], fa, p.f, Wf, Hf, p.W, p.H);
+                else
+                    p.outcodes[outBase + v] = (uint8_t)vertex_outcode(M, q[r], fa, p.f);
             }
         }
     }
-    // only after a timeout can copies still be in flight: thread 0, which
-    // issued them, waits for them (bounded) so none lands in shared memory
-    // after the block has exited
-    if (threadIdx.x == 0)
-        for (int s = 0; s < STAGES; ++s)
-            if (pending & (1u << s)) (void)mbar_wait_bounded(&s_bar[s], (parity >> s) & 1u, p.waitTimeoutNs);
+    if (p.sliceNeed && lane == 0 && run) atomicAdd(&p.counters[CR_CTR_VSLICES], (unsigned long long)run);
 }
 
 // Frame cull, before the vertex pass, in two levels.  Every box is an
@@ -417,6 +361,45 @@ __global__ void __launch_bounds__(THREADS, 3) k_cull(const CrFrameParams p) {
         }
         const uint64_t item = __ldg(&sg->itemBase) + (uint64_t)un.chunk * nb + batch;
         list_append(&p.counters[CR_CTR_ITEMS], p.itemList, p.itemCap, mask != 0u, make_uint2((uint32_t)item, mask));
+    }
+}
+
+// Slice stamps, between the item cull and the vertex pass of frames with
+// CrFrameParams::sliceNeed: a thread per listed (drawn) item stamps, for each
+// instance it is drawn for, the slices its vertices lie in (CrSegment::
+// itemSlices; an item whose slices do not fit the two windows stamps the
+// slice of each of its triangles' vertices).  Every writer of a slice stores
+// the same value, so plain stores suffice.
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) k_stamp(const CrFrameParams p) {
+    pdl_enter();
+    const uint64_t n = min((uint64_t)p.counters[CR_CTR_ITEMS], p.itemCap);
+    const uint32_t stamp = p.needStamp;
+    for (uint64_t k = (uint64_t)blockIdx.x * THREADS + threadIdx.x; k < n; k += (uint64_t)gridDim.x * THREADS) {
+        const uint2 e = p.itemList[k];
+        const Item it = decode_item(p, e.x);
+        const CrSegment* sg = p.segments + it.seg;
+        const uint4* sl = ldg_ptr(&sg->itemSlices) + 2ull * it.batch;
+        const uint4 q0 = __ldg(sl), q1 = __ldg(sl + 1);
+        const uint64_t winA = (uint64_t)q0.z | ((uint64_t)q0.w << 32);
+        const uint64_t winB = (uint64_t)q1.x | ((uint64_t)q1.y << 32);
+        const bool spread = (q1.w >> 31) != 0u;
+        const uint32_t ib = __ldg(&sg->firstInstance) + it.chunk * CR_INST_CHUNK;
+        for (uint32_t rest = e.y & 0xffffu; rest; rest &= rest - 1) {
+            const CrInstance* I = p.instances + ib + (uint32_t)(__ffs(rest) - 1);
+            uint32_t* need = p.sliceNeed + (uint64_t)VX_SLICES * __ldg(&I->vchunkBase);
+            if (spread) {
+                const GeomRef g = geom_of(I);
+                const uint32_t last = (__ldg(&I->numVertices) + CR_VSLICE - 1) / CR_VSLICE - 1;
+                const uint32_t t0 = it.batch * CR_BATCH;
+                const uint32_t t1 = min(t0 + (uint32_t)CR_BATCH, __ldg(&sg->numTriangles));
+                for (uint32_t t = t0; t < t1; ++t)
+                    for (int c = 0; c < 3; ++c) need[min(geom_index(g, 3ull * t + c) / (uint32_t)CR_VSLICE, last)] = stamp;
+            } else {
+                for (uint64_t b = winA; b; b &= b - 1) need[q0.x + (uint32_t)(__ffsll((long long)b) - 1)] = stamp;
+                for (uint64_t b = winB; b; b &= b - 1) need[q0.y + (uint32_t)(__ffsll((long long)b) - 1)] = stamp;
+            }
+        }
     }
 }
 
@@ -1050,7 +1033,9 @@ int cr_launch_cull(const CrFrameParams& p, const CrLaunchShape& s, void* stream)
     if (blocks > (uint64_t)s.numSMs * 8) blocks = (uint64_t)s.numSMs * 8;
     if (launch_pdl(k_cull_groups<256>, (unsigned)blocks, 256, stream, p)) return -1;
     // one warp per listed group: as many warps as can be resident
-    return launch_pdl(k_cull<256>, (unsigned)(s.numSMs * 3), 256, stream, p);
+    if (launch_pdl(k_cull<256>, (unsigned)(s.numSMs * 3), 256, stream, p)) return -1;
+    if (!p.sliceNeed || !p.itemList || !p.chunkList) return 0;
+    return launch_pdl(k_stamp<256>, (unsigned)(s.numSMs * 4), 256, stream, p);
 }
 
 // Box-culled frames: k_stage1.  Record-culled frames: k_s1cull (items ->

@@ -770,9 +770,13 @@ __device__ __forceinline__ uint64_t vertex_cell_record(const Mat& M, V3 p, float
     const float d = -q.z;
     if (d <= 0.0f) return CR_OC_BEHIND;
     const float X = fa * q.x, Y = f * q.y;
-    uint64_t rec = (ndc_beyond(X, d) ? CR_OC_RIGHT : 0u) | (ndc_beyond(-X, d) ? CR_OC_LEFT : 0u) |
-                   (ndc_beyond(Y, d) ? CR_OC_TOP : 0u) | (ndc_beyond(-Y, d) ? CR_OC_BOTTOM : 0u);
-    const V2 s = to_screen(V3{X / d, Y / d, d}, Wf, Hf);
+    const float qx = X / d, qy = Y / d;
+    // the sides from the quotients themselves: ndc_beyond(X, d) is fl(X / d)
+    // > 1, and ndc_beyond(-X, d) is fl(X / d) < -1 (rounding to nearest is
+    // symmetric)
+    uint64_t rec = (qx > 1.0f ? CR_OC_RIGHT : 0u) | (qx < -1.0f ? CR_OC_LEFT : 0u) |
+                   (qy > 1.0f ? CR_OC_TOP : 0u) | (qy < -1.0f ? CR_OC_BOTTOM : 0u);
+    const V2 s = to_screen(V3{qx, qy, d}, Wf, Hf);
     const float sx = s.x - 0.5f, sy = s.y - 0.5f;
     if (sx >= 0.0f && sx <= (float)(W - 1) && sy >= 0.0f && sy <= (float)(H - 1)) {
         const float fx = floorf(sx), fy = floorf(sy);
@@ -797,7 +801,8 @@ __device__ __forceinline__ uint32_t vertex_cell32(const Mat& M, V3 p, float fa, 
     const float d = -q.z;
     const float X = fa * q.x, Y = f * q.y;
     if (SIDES && d <= 0.0f) return CR_OC_BEHIND;
-    const V2 s = to_screen(V3{X / d, Y / d, d}, Wf, Hf);
+    const float qx = X / d, qy = Y / d;
+    const V2 s = to_screen(V3{qx, qy, d}, Wf, Hf);
     const float sx = s.x - 0.5f, sy = s.y - 0.5f;
     if (sx >= 0.0f && sx <= Wm1 && sy >= 0.0f && sy <= Hm1) {
         // on screen, so beyond no side: ndc_beyond(X, d) is fl(X / d) > 1,
@@ -808,8 +813,11 @@ __device__ __forceinline__ uint32_t vertex_cell32(const Mat& M, V3 p, float fa, 
                ((uint32_t)(int)fx << 8) | ((uint32_t)(int)fy << 20);
     }
     if (!SIDES) return 0u;
-    return (ndc_beyond(X, d) ? CR_OC_RIGHT : 0u) | (ndc_beyond(-X, d) ? CR_OC_LEFT : 0u) |
-           (ndc_beyond(Y, d) ? CR_OC_TOP : 0u) | (ndc_beyond(-Y, d) ? CR_OC_BOTTOM : 0u);
+    // the sides from the quotients themselves: ndc_beyond(X, d) is fl(X / d)
+    // > 1, and ndc_beyond(-X, d) is fl(X / d) < -1 (rounding to nearest is
+    // symmetric)
+    return (qx > 1.0f ? CR_OC_RIGHT : 0u) | (qx < -1.0f ? CR_OC_LEFT : 0u) | (qy > 1.0f ? CR_OC_TOP : 0u) |
+           (qy < -1.0f ? CR_OC_BOTTOM : 0u);
 }
 
 // cell_culled on 32-bit records.

@@ -151,6 +151,7 @@ class CrFrameStats(ctypes.Structure):
         ("vertex_chunks", _u64),
         ("vertex_chunks_evaluated", _u64),
         ("stage1_survivors", _u64),
+        ("vertex_slices_evaluated", _u64),
     ]
 
 

@@ -210,6 +210,10 @@ typedef struct cr_frame_stats {
     /* record-culled frames: triangles the per-vertex records did not cull,
      * which stage 1 ran through the reference's full per-triangle path */
     uint64_t stage1_survivors;
+    /* record-culled frames: 128-vertex slices of the evaluated chunks whose
+     * records the vertex pass wrote -- those holding a vertex of a drawn
+     * work item (8 per evaluated chunk where the slices are not tracked) */
+    uint64_t vertex_slices_evaluated;
 } cr_frame_stats;
 
 /* ---- context ---------------------------------------------------------- */
