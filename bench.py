@@ -358,9 +358,12 @@ def plain_algorithmic_bytes(wl, fstats, T):
     """Algorithmic bytes per launch of the plain frame's kernels, from the
     units the frame processed (its stats).  The frame cull (timed with the
     vertex pass) reads a 24-byte box per vertex chunk and per work item and
-    writes 8 B per listed item; the vertex pass reads 12 B of position and
-    writes one record (4-byte cell records up to 4096 pixels a side, else 8)
-    per vertex of each chunk its box did not classify; stage 1 reads the
+    writes 8 B per listed item; the slice stamps read each listed item's
+    entry and slice windows (8 + 32 B) and write a few 4-byte stamps (16 B
+    counted); the vertex pass reads 12 B of position and writes one record
+    (4-byte cell records up to 4096 pixels a side, else 8) per vertex of each
+    slice it evaluates (the 128-vertex slices of the chunks its box did not
+    classify that hold a vertex of a drawn item); stage 1 reads the
     12-byte index triple of every triangle of each drawn work item, the
     record of each vertex those triangles use once (counted as one per two
     triangles, as in a closed mesh, and at most the records written), and
@@ -376,6 +379,7 @@ def plain_algorithmic_bytes(wl, fstats, T):
     slices_eval = int(getattr(fstats, "vertex_slices_evaluated", 0))
     surv = int(getattr(fstats, "stage1_survivors", 0))
     nV_inst = sum(wl["meshes"][m][0].shape[0] for m, _ in wl["instances"])
+    stamps = 56 * items_drawn if slices_eval else 0
     if direct:
         # frame cull: one 24-byte item box per item (the instance matrices
         # stay in L1) and 8 B per listed item; stage 1: the 1408-byte vertex
@@ -389,7 +393,7 @@ def plain_algorithmic_bytes(wl, fstats, T):
         # chunks that hold a vertex of a drawn item
         v_eval = min(nV_inst, slices_eval * 128 if slices_eval else chunks_eval * 1024)
         tri_drawn = min(T, items_drawn * 128)
-        algo = {"vertex": 24 * (chunks + items) + (12 + rec) * v_eval + 8 * items_drawn,
+        algo = {"vertex": 24 * (chunks + items) + (12 + rec) * v_eval + 8 * items_drawn + stamps,
                 "stage1": 12 * tri_drawn + rec * min(v_eval, tri_drawn // 2) + 16 * surv}
     else:
         v_eval, tri_drawn = nV_inst, T
@@ -397,7 +401,7 @@ def plain_algorithmic_bytes(wl, fstats, T):
     if wl.get("compressed"):
         # compressed meshes: 6-byte positions, 3 x bits / 8 bytes of indices per triangle
         ib = 3 * wl["compressed"][0].bits / 8.0
-        algo = {"vertex": 24 * (chunks + items) + (6 + rec) * v_eval + 8 * items_drawn,
+        algo = {"vertex": 24 * (chunks + items) + (6 + rec) * v_eval + 8 * items_drawn + stamps,
                 "stage1": ib * tri_drawn + rec * min(v_eval, tri_drawn // 2) + 16 * surv}
     return algo, tri_drawn, v_eval
 
