@@ -96,7 +96,7 @@ void back_face_data(const float* wv, double* o) {
     o[4] = sqrt(frob);
     o[5] = rowAbs;
     o[6] = tAbs;
-    o[7] = 0.0;
+    o[7] = sqrt(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
 }
 
 // glm::inverse for mat4 (libs/glm/glm/detail/func_matrix.inl:296-360)

@@ -138,13 +138,15 @@ struct alignas(16) CrSegment {
 };
 static_assert(sizeof(CrSegment) == 144, "CrSegment layout");
 // Per-item normal cone (object space), for the back-face proof of the frame
-// cull: axis m (float xyz, any length), cosT (every triangle's unit normal u
-// has u . m / |m| >= cosT; below -1: no cone), nMin (every triangle's
-// |(pb - pa) x (pc - pa)| >= nMin), edge (every |pb - pa|, |pc - pa| <= edge).
-#define CR_CONE_FLOATS 6
+// cull: axis m (float xyz, unit length within 2^-23), cosT (every triangle's
+// unit normal u has u . m / |m| >= cosT; below -1: no cone), nMin (every
+// triangle's |(pb - pa) x (pc - pa)| >= nMin), edge (every |pb - pa|,
+// |pc - pa| <= edge), sinT >= sqrt(1 - cosT^2), and r >= half the diagonal of
+// the item's box.
+#define CR_CONE_FLOATS 8
 // Per-instance data of the back-face proof (CrFrameParams::instBack, doubles):
 // the camera in object space (e = -R^-1 t, 3), |det R| (0: no proof), the
-// Frobenius norm of R, max_i sum_j |R_ij|, max_i |t_i|, and one spare.
+// Frobenius norm of R, max_i sum_j |R_ij|, max_i |t_i|, and |e|.
 #define CR_BACK_DOUBLES 8
 
 struct alignas(16) CrTile {     // HugeTriangle, HostDeviceInterface.h:254-259

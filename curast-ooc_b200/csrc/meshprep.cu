@@ -135,11 +135,12 @@ __global__ void __launch_bounds__(256) k_item_slices(const uint32_t* idx, const 
 
 // One warp per item: the normal cone of its triangles (CR_CONE_FLOATS, see
 // cr_device.h), computed in double from the float positions.  The axis is the
-// sum of the unit normals rounded to float; cosT is the least cosine between
-// a unit normal and that float axis, lowered by 1e-9 (far above the double
-// rounding of the computation) and rounded down to float; nMin is rounded
-// down and edge up.  A zero-area or non-finite triangle, or a cone wider than
-// acos(0.05), gives cosT = -2 (no proof).
+// sum of the unit normals, normalised and rounded to float; cosT is the least
+// cosine between a unit normal and that float axis, lowered by 1e-9 (far
+// above the double rounding of the computation) and rounded down to float;
+// nMin is rounded down, edge, sinT (from the stored cosT) and r (half the
+// diagonal of the box of the item's vertices) up.  A zero-area or non-finite
+// triangle, or a cone wider than acos(0.05), gives cosT = -2 (no proof).
 __global__ void __launch_bounds__(256) k_item_cones(const uint32_t* idx, const float* pos, const CrCodec* codec,
                                                     uint32_t nT, float* cones) {
     const int lane = threadIdx.x & 31;
@@ -150,6 +151,7 @@ __global__ void __launch_bounds__(256) k_item_cones(const uint32_t* idx, const f
         double len[CR_BATCH / 32];
         bool live[CR_BATCH / 32];
         double sx = 0.0, sy = 0.0, sz = 0.0, nMin = INFINITY, edge = 0.0;
+        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
         bool bad = false;
 #pragma unroll
         for (int r = 0; r < CR_BATCH / 32; ++r) {
@@ -162,6 +164,11 @@ __global__ void __launch_bounds__(256) k_item_cones(const uint32_t* idx, const f
             geom_pos(g, geom_index(g, 3ull * t + 0), a[0], a[1], a[2]);
             geom_pos(g, geom_index(g, 3ull * t + 1), bq[0], bq[1], bq[2]);
             geom_pos(g, geom_index(g, 3ull * t + 2), c[0], c[1], c[2]);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                lo[j] = fminf(lo[j], fminf(a[j], fminf(bq[j], c[j])));
+                hi[j] = fmaxf(hi[j], fmaxf(a[j], fmaxf(bq[j], c[j])));
+            }
             const double u0 = (double)bq[0] - a[0], u1 = (double)bq[1] - a[1], u2 = (double)bq[2] - a[2];
             const double v0 = (double)c[0] - a[0], v1 = (double)c[1] - a[1], v2 = (double)c[2] - a[2];
             n[r][0] = u1 * v2 - u2 * v1;
@@ -184,10 +191,17 @@ __global__ void __launch_bounds__(256) k_item_cones(const uint32_t* idx, const f
             sz += __shfl_xor_sync(FULL, sz, d);
             nMin = fmin(nMin, __shfl_xor_sync(FULL, nMin, d));
             edge = fmax(edge, __shfl_xor_sync(FULL, edge, d));
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                lo[j] = fminf(lo[j], __shfl_xor_sync(FULL, lo[j], d));
+                hi[j] = fmaxf(hi[j], __shfl_xor_sync(FULL, hi[j], d));
+            }
         }
         bad = __any_sync(FULL, bad);
-        // the axis as stored (float), renormalised in double as the proof does
-        const float mx = (float)sx, my = (float)sy, mz = (float)sz;
+        // the axis as stored (float, normalised in double first), renormalised
+        // in double as the cone's cosine is measured
+        const double sl = sqrt(sx * sx + sy * sy + sz * sz);
+        const float mx = (float)(sx / sl), my = (float)(sy / sl), mz = (float)(sz / sl);
         const double ml = sqrt((double)mx * mx + (double)my * my + (double)mz * mz);
         double cosT = INFINITY;
 #pragma unroll
@@ -197,15 +211,24 @@ __global__ void __launch_bounds__(256) k_item_cones(const uint32_t* idx, const f
 #pragma unroll
         for (int d = 16; d >= 1; d >>= 1) cosT = fmin(cosT, __shfl_xor_sync(FULL, cosT, d));
         cosT -= 1e-9;
-        if (bad || !(ml > 0.0) || !isfinite(ml) || !(cosT > 0.05)) cosT = -2.0;
+        if (bad || !(sl > 0.0) || !isfinite(sl) || !(ml > 0.0) || !isfinite(ml) || !(cosT > 0.05)) cosT = -2.0;
+        const float cosTf = __double2float_rd(cosT);
+        double r2 = 0.0;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const double h = 0.5 * ((double)hi[j] - (double)lo[j]);
+            r2 += h * h;
+        }
         if (lane < CR_CONE_FLOATS) {
             float v;
             if (lane == 0) v = mx;
             else if (lane == 1) v = my;
             else if (lane == 2) v = mz;
-            else if (lane == 3) v = __double2float_rd(cosT);
+            else if (lane == 3) v = cosTf;
             else if (lane == 4) v = bad ? 0.0f : __double2float_rd(nMin * (1.0 - 1e-9));
-            else v = bad ? INFINITY : __double2float_ru(edge * (1.0 + 1e-9));
+            else if (lane == 5) v = bad ? INFINITY : __double2float_ru(edge * (1.0 + 1e-9));
+            else if (lane == 6) v = __double2float_ru(sqrt(fmax(0.0, 1.0 - (double)cosTf * cosTf)) * (1.0 + 1e-12));
+            else v = __double2float_ru(sqrt(r2) * (1.0 + 1e-12));
             cones[(uint64_t)CR_CONE_FLOATS * b + lane] = v;
         }
     }

@@ -715,7 +715,10 @@ __device__ bool box_misses_samples(const Mat& M, float fa, float f, int W, int H
 // (pa - e) . n >= 0.  From the item's box (centre c, half-diagonal r) and
 // normal cone (axis m, every unit normal within acos cosT of it),
 // (pa - e) . n >= |n| G with G = |c - e| cos(phi + theta) - r, phi the angle
-// between c - e and m.  The float res differs from the exact one by at most
+// between c - e and m, evaluated without dividing as ((c - e) . m cos theta -
+// |(c - e) x m| sin theta) / |m| with |m| = 1 (the stored unit axis is within
+// 2^-23 of it, a relative error that the 1e-6 slack covers with the double
+// rounding).  The float res differs from the exact one by at most
 // E: the transform's rounding (each view coordinate within gamma_3 T of the
 // exact one, T = sum_j |R_ij| |p_j| + |t_i|), the edge subtractions, the cross
 // and dot products (gamma_2 and gamma_3 of their magnitude bounds), with |av| <=
@@ -727,27 +730,22 @@ __device__ __noinline__ bool item_back_facing(const double* B, const float* cone
     const double detA = B[3];
     const double cosT = (double)__ldg(cone + 3);
     if (!(detA > 0.0) || !(cosT > 0.0)) return false;
-    double w[3], r2 = 0.0, P = 0.0;
+    const double m0 = __ldg(cone), m1 = __ldg(cone + 1), m2 = __ldg(cone + 2);
+    const double sinT = __ldg(cone + 6), r = __ldg(cone + 7);
+    double w[3], P = 0.0;
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-        const double c = 0.5 * ((double)lo[j] + (double)hi[j]);
-        const double h = 0.5 * ((double)hi[j] - (double)lo[j]);
-        w[j] = c - B[j];
-        r2 += h * h;
+        w[j] = 0.5 * ((double)lo[j] + (double)hi[j]) - B[j];
         P = fmax(P, fmax(fabs((double)lo[j]), fabs((double)hi[j])));
     }
-    const double r = sqrt(r2);
     const double wl = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
-    const double m0 = __ldg(cone), m1 = __ldg(cone + 1), m2 = __ldg(cone + 2);
-    const double ml = sqrt(m0 * m0 + m1 * m1 + m2 * m2);
-    if (!(wl > 0.0) || !(ml > 0.0)) return false;
-    const double cosPhi = fmin(1.0, fmax(-1.0, (w[0] * m0 + w[1] * m1 + w[2] * m2) / (wl * ml)));
-    const double sinPhi = sqrt(fmax(0.0, 1.0 - cosPhi * cosPhi));
-    const double sinT = sqrt(fmax(0.0, 1.0 - cosT * cosT));
-    // rounding of e, the centre and the angles in double: far below 1e-9 of
-    // the magnitudes involved
-    const double el = sqrt(B[0] * B[0] + B[1] * B[1] + B[2] * B[2]);
-    const double G = wl * (cosPhi * cosT - sinPhi * sinT) - r - 1e-9 * (wl + r + el + P);
+    if (!(wl > 0.0)) return false;
+    const double dm = w[0] * m0 + w[1] * m1 + w[2] * m2;
+    const double cx = w[1] * m2 - w[2] * m1, cy = w[2] * m0 - w[0] * m2, cz = w[0] * m1 - w[1] * m0;
+    const double cr = sqrt(cx * cx + cy * cy + cz * cz);
+    // rounding of e, the centre and the products in double, and |m| = 1
+    // within 2^-23: far below 1e-6 of the magnitudes involved (B[7] = |e|)
+    const double G = (dm * cosT - cr * sinT) - r - 1e-6 * (wl + r + B[7] + P);
     if (!(G > 0.0)) return false;
     const double u = 5.9604644775390625e-08;  // 2^-24
     const double g2 = 2.0 * u / (1.0 - 2.0 * u), g3 = 3.0 * u / (1.0 - 3.0 * u);

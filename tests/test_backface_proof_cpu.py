@@ -45,7 +45,8 @@ def back_face_data(M):
     had = np.prod(np.abs(R).sum(0))
     e = -np.linalg.solve(R, t)
     ok = np.isfinite(det) and abs(det) > 1e-4 * had
-    return e, (abs(det) if ok else 0.0), np.sqrt((R * R).sum()), np.abs(R).sum(1).max(), np.abs(t).max()
+    return e, (abs(det) if ok else 0.0), np.sqrt((R * R).sum()), np.abs(R).sum(1).max(), np.abs(t).max(), \
+        np.linalg.norm(e)
 
 
 def item_cone(pa, pb, pc):
@@ -55,33 +56,35 @@ def item_cone(pa, pb, pc):
     ln = np.linalg.norm(n, axis=1)
     if not (ln > 0).all():
         return None
-    m = (n / ln[:, None]).sum(0).astype(F).astype(np.float64)
+    s = (n / ln[:, None]).sum(0)
+    m = (s / np.linalg.norm(s)).astype(F).astype(np.float64)  # unit axis, rounded to float
     ml = np.linalg.norm(m)
     cosT = ((n @ m) / (ln * ml)).min() - 1e-9
     if not cosT > 0.05:
         return None
+    cosTf = np.nextafter(F(cosT), F(-np.inf))
     edge = max(np.linalg.norm(u, axis=1).max(), np.linalg.norm(v, axis=1).max())
-    return m, np.nextafter(F(cosT), F(-np.inf)), np.nextafter(F(ln.min() * (1 - 1e-9)), F(-np.inf)), \
-        np.nextafter(F(edge * (1 + 1e-9)), F(np.inf))
+    allp = np.concatenate([pa, pb, pc]).astype(np.float64)
+    r = 0.5 * np.linalg.norm(allp.max(0) - allp.min(0))
+    up = lambda x: np.nextafter(F(x), F(np.inf))  # noqa: E731
+    return m, cosTf, np.nextafter(F(ln.min() * (1 - 1e-9)), F(-np.inf)), up(edge * (1 + 1e-9)), \
+        up(np.sqrt(max(0.0, 1.0 - float(cosTf) ** 2)) * (1 + 1e-12)), up(r * (1 + 1e-12))
 
 
 def proof(M, lo, hi, cone):
-    e, detA, frob, rowAbs, tAbs = back_face_data(M)
-    m, cosT, nMin, edge = cone
-    cosT = float(cosT)
+    e, detA, frob, rowAbs, tAbs, el = back_face_data(M)
+    m, cosT, nMin, edge, sinT, r = cone
+    cosT, sinT, r = float(cosT), float(sinT), float(r)
     if not (detA > 0 and cosT > 0):
         return False
     lo64, hi64 = lo.astype(np.float64), hi.astype(np.float64)
-    c = 0.5 * (lo64 + hi64)
-    r = np.linalg.norm(0.5 * (hi64 - lo64))
     P = max(np.abs(lo64).max(), np.abs(hi64).max())
-    w = c - e
+    w = 0.5 * (lo64 + hi64) - e
     wl = np.linalg.norm(w)
-    ml = np.linalg.norm(m)
-    cosPhi = min(1.0, max(-1.0, float(w @ m) / (wl * ml)))
-    sinPhi = np.sqrt(max(0.0, 1 - cosPhi * cosPhi))
-    sinT = np.sqrt(max(0.0, 1 - cosT * cosT))
-    G = wl * (cosPhi * cosT - sinPhi * sinT) - r - 1e-9 * (wl + r + np.linalg.norm(e) + P)
+    if not wl > 0:
+        return False
+    # |c - e| cos(phi + theta) = ((c - e) . m cos theta - |(c - e) x m| sin theta) / |m|, |m| = 1
+    G = (float(w @ m) * cosT - np.linalg.norm(np.cross(w, m)) * sinT) - r - 1e-6 * (wl + r + el + P)
     if not G > 0:
         return False
     g2, g3 = 2 * U / (1 - 2 * U), 3 * U / (1 - 3 * U)
