@@ -743,6 +743,9 @@ def sub_plain(args, wl, ctx, handles, with_parity):
         par, _, ok = frame_parity(wl, ctx, inst, vis, rgba)
         rec["parity"] = "bit-exact" if ok else "MISMATCH"
         rec["parity_detail"] = par
+    elif not args.no_parity:
+        rec["parity"] = ("not checked in this run (the CPU oracle takes tens of seconds on this frame); "
+                         "tests/test_bench_sizes_gpu.py checks the same frame bit for bit")
     return rec
 
 
