@@ -548,11 +548,13 @@ cr_status run_frame(cr_context* ctx, uint32_t flags, cudaStream_t stream, uint64
             ctx->ringCount++;
         }
         if (sync) CR_CUDA(cudaEventRecord(ctx->ev[0], stream), "event");
+        ctx->countersPublished = false;
         cr_status s = issue(tev, sync ? ctx->ev[1] : nullptr);
         if (s) return s;
-        CR_CUDA(cudaMemcpyAsync(ctx->hCounters, ctx->counters, CR_CTR_COUNT * sizeof(unsigned long long),
-                                cudaMemcpyDeviceToHost, stream),
-                "counters readback");
+        if (!ctx->countersPublished)
+            CR_CUDA(cudaMemcpyAsync(ctx->hCounters, ctx->counters, CR_CTR_COUNT * sizeof(unsigned long long),
+                                    cudaMemcpyDeviceToHost, stream),
+                    "counters readback");
         ctx->last = cr_frame_stats{};
         ctx->last.instances = instances;
         ctx->last.triangles = triangles;
@@ -1297,6 +1299,9 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
     rp.idLo = resolveIdLo;
     rp.idHi = resolveIdHi;
     rp.writeBackground = resolveIdLo == 0 ? 1u : 0u;
+    // the resolve, the frame's last kernel, hands the counters to the host
+    rp.counters = ctx->counters;
+    rp.hostCounters = ctx->hCounters;
 
     auto issue = [&](cudaEvent_t* tev, cudaEvent_t rasterEnd) -> cr_status {
         fp.ntList = ctx->ntList;
@@ -1306,6 +1311,15 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
         fp.s1List = ctx->s1List;
         fp.s1Cap = ctx->s1Cap;
         auto mark = [&](int i) -> cudaError_t { return tev ? cudaEventRecord(tev[i], stream) : cudaSuccess; };
+        // the resolve (unless NO_RESOLVE) also copies the frame's counters to
+        // the host buffer, so run_frame issues no read-back of its own
+        auto resolve = [&]() -> cr_status {
+            if (flags & CR_RENDER_NO_RESOLVE) return CR_OK;
+            if (cr_launch_resolve(rp, stream))
+                return fail(CR_ERR_CUDA, "resolve launch: %s", cudaGetErrorString(cudaGetLastError()));
+            ctx->countersPublished = true;
+            return CR_OK;
+        };
         CR_CUDA(mark(0), "event");
         const bool raster = !(flags & kRenderResolveOnly);
         if ((flags & CR_RENDER_NO_CLEAR) || !raster) {
@@ -1324,8 +1338,7 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
             CR_CUDA(mark(4), "event");
             CR_CUDA(mark(5), "event");
             if (rasterEnd) CR_CUDA(cudaEventRecord(rasterEnd, stream), "event");
-            if (!(flags & CR_RENDER_NO_RESOLVE) && cr_launch_resolve(rp, stream))
-                return fail(CR_ERR_CUDA, "resolve launch: %s", cudaGetErrorString(cudaGetLastError()));
+            if (cr_status rs = resolve()) return rs;
             CR_CUDA(mark(6), "event");
             return CR_OK;
         }
@@ -1343,8 +1356,7 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
         CR_CUDA(mark(5), "event");
         if (rasterEnd) CR_CUDA(cudaEventRecord(rasterEnd, stream), "event");
         // an empty frame still resolves: its image is all background
-        if (!(flags & CR_RENDER_NO_RESOLVE) && cr_launch_resolve(rp, stream))
-            return fail(CR_ERR_CUDA, "resolve launch: %s", cudaGetErrorString(cudaGetLastError()));
+        if (cr_status rs = resolve()) return rs;
         CR_CUDA(mark(6), "event");
         return CR_OK;
     };

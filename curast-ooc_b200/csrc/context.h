@@ -151,6 +151,8 @@ struct cr_context {
                                     // frame a drawn item used one of its vertices
     uint32_t needStamp = 0;         // the last frame's stamp (0 is never issued)
     bool lastStamps = false;        // the last frame's vertex pass evaluated stamped slices only
+    bool countersPublished = false; // the frame being issued has its resolve copy the counters
+                                    // to hCounters (no separate read-back)
     size_t itemBytes = 0;
     uint64_t* s1List = nullptr;   // stage-1 survivors of record-culled frames
     uint64_t s1Cap = 0;

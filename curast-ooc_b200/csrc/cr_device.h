@@ -308,6 +308,12 @@ struct CrResolveParams {
     uint32_t thrSmall, thrLarge;  // the stage thresholds (STAGE display)
     uint64_t idBase;            // added to a pixel's id to find its instance (batched
                                 // frames of several instance sets)
+    // plain frames: the frame's counters (CR_CTR_COUNT, final once the raster
+    // stages are done) and a page-locked host buffer the resolve copies them
+    // to, in place of a device-to-host copy that would queue behind image
+    // read-backs on the copy engine (hostCounters nullptr: no copy)
+    const unsigned long long* counters;
+    unsigned long long* hostCounters;
 };
 
 // Post-processing of the colorbuffer (post.cu): the reference's EDL, SSAO and

@@ -208,6 +208,8 @@ __global__ void __launch_bounds__(256) k_resolve(const CrResolveParams p) {
     // launched after the raster stages with programmatic stream
     // serialization: wait for them before reading the visbuffer
     asm volatile("griddepcontrol.wait;" ::: "memory");
+    if (p.hostCounters && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.y == 0 && threadIdx.x < CR_CTR_COUNT)
+        p.hostCounters[threadIdx.x] = p.counters[threadIdx.x];
     const int x = blockIdx.x * 32 + threadIdx.x;
     const int y = blockIdx.y * 8 + threadIdx.y;
     if (x >= p.W || y >= p.H) return;
