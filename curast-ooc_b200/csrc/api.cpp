@@ -521,6 +521,7 @@ cr_status fold_oldest(cr_context* ctx) {
 void read_counters(cr_context* ctx) {
     const unsigned long long* c = ctx->hCounters;
     ctx->last.nontrivial = c[CR_CTR_NONTRIVIAL];
+    ctx->lastNontrivial = c[CR_CTR_NONTRIVIAL];
     ctx->last.huge_tiles = c[CR_CTR_HUGE];
     ctx->last.overflow = c[CR_CTR_OVERFLOW];
     ctx->last.work_items_drawn = ctx->last.work_items ? c[CR_CTR_ITEMS] : 0;
@@ -1242,6 +1243,9 @@ cr_status cr::render_impl(cr_context* ctx, const cr_instance* instances, uint32_
     // frames whose triangles cover pixels (not mostly sub-pixel ones) keep
     // many lanes rasterizing in stage 1: spread those rasters over the warp
     fp.coopRaster = pxPerTriangle >= 0.5f ? 1u : 0u;
+    // frames that queue many triangles for stage 2 (judged from the last
+    // measured frame) run it at 4 blocks per SM
+    fp.dense2 = ctx->lastNontrivial >= 65536 ? 1u : 0u;
     fp.itemList = ctx->itemList;
     fp.itemCap = ctx->itemCap;
     fp.chunkList = ctx->chunkList;

@@ -151,6 +151,7 @@ struct cr_context {
                                     // frame a drawn item used one of its vertices
     uint32_t needStamp = 0;         // the last frame's stamp (0 is never issued)
     bool lastStamps = false;        // the last frame's vertex pass evaluated stamped slices only
+    uint64_t lastNontrivial = 0;    // stage-2 queue entries of the last frame whose counters were read
     bool countersPublished = false; // the frame being issued has its resolve copy the counters
                                     // to hCounters (no separate read-back)
     size_t itemBytes = 0;

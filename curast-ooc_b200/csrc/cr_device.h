@@ -277,7 +277,9 @@ struct CrFrameParams {
     // records stage 1 reads.  nullptr: every slice of a listed chunk.
     uint32_t* sliceNeed;
     uint32_t needStamp;
-    uint32_t pad3;
+    // 1: stage 2 runs as k_stage2_dense (the host's estimate from the
+    // context's last measured frame: many queued triangles)
+    uint32_t dense2;
 };
 #define CR_CHUNK_EVAL 0xffu
 
@@ -346,6 +348,7 @@ struct CrLaunchShape {
     int stage3Blocks;
     int s1CullBlocks;           // k_s1cull (record-culled frames)
     int s1RasterBlocks;         // k_s1raster
+    int stage2DenseBlocks;      // k_stage2_dense
 };
 
 int cr_query_launch_shape(int device, CrLaunchShape* out);

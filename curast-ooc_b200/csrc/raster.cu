@@ -988,6 +988,10 @@ int cr_query_launch_shape(int device, CrLaunchShape* out) {
     out->s1CullBlocks = sms * (bc > 0 ? bc : 1);
     out->s1RasterBlocks = sms * (br > 0 ? br : 1);
     out->stage2Blocks = sms * (b2 > 0 ? b2 : 1);
+    int b2d = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2d, k_stage2_dense<S2_WARPS>, S2_WARPS * 32, 0) != cudaSuccess)
+        return -1;
+    out->stage2DenseBlocks = sms * (b2d > 0 ? b2d : 1);
     out->stage3Blocks = sms * (b3 > 0 ? b3 : 1);
     return 0;
 }
@@ -1062,6 +1066,8 @@ int cr_launch_stage1(const CrFrameParams& p, const CrLaunchShape& s, void* strea
 }
 
 int cr_launch_stage2(const CrFrameParams& p, const CrLaunchShape& s, void* stream) {
+    if (p.dense2 && s.stage2DenseBlocks > 0)
+        return launch_pdl(k_stage2_dense<S2_WARPS>, (unsigned)s.stage2DenseBlocks, S2_WARPS * 32, stream, p);
     return launch_pdl(k_stage2<S2_WARPS, false>, (unsigned)s.stage2Blocks, S2_WARPS * 32, stream, p);
 }
 

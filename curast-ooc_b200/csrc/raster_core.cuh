@@ -1220,7 +1220,7 @@ struct S2Tri {
 };
 
 template <int WARPS, bool MULTI>
-__global__ void __launch_bounds__(WARPS * 32) k_stage2(const CrFrameParams p) {
+__device__ __forceinline__ void stage2_run(const CrFrameParams& p) {
     pdl_enter();
     __shared__ S2Tri s_tri[WARPS][32];
     const int lane = threadIdx.x & 31;
@@ -1391,6 +1391,19 @@ __global__ void __launch_bounds__(WARPS * 32) k_stage2(const CrFrameParams p) {
         }
         __syncwarp();  // the next group's setups overwrite this one's
     }
+}
+
+template <int WARPS, bool MULTI>
+__global__ void __launch_bounds__(WARPS * 32) k_stage2(const CrFrameParams p) {
+    stage2_run<WARPS, MULTI>(p);
+}
+
+// Stage 2 for frames with many queued triangles (CrFrameParams::dense2): the
+// same work held to 4 blocks per SM (64 registers, a few spilled), which the
+// 1M heightfield's 383K queued slivers prefer; frames with few take k_stage2.
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, 4) k_stage2_dense(const CrFrameParams p) {
+    stage2_run<WARPS, false>(p);
 }
 
 // ---------------------------------------------------------------------------
