@@ -442,8 +442,47 @@ __device__ __forceinline__ void gather_culls(const CrFrameParams& p, uint32_t in
 #pragma unroll
         for (int r = 0; r < S1_R; ++r) culledR[r] = false;
     } else if (p.cellMode == CR_REC_CELLS32) {
+        // The records are loaded at once (every vertex has a record slot, so
+        // the loads stay in bounds) while the warp reads the class bytes of
+        // the item's chunk range, a lane per chunk: when every chunk has
+        // per-vertex records (the usual case) they are used as they are;
+        // else each corner takes its chunk's class where it has one.
+        const uint32_t* rec = reinterpret_cast<const uint32_t*>(p.outcodes) + __ldg(&I->outBase);
+        const uint8_t* cls = p.chunkClass ? p.chunkClass + __ldg(&I->vchunkBase) : nullptr;
         uint32_t o[S1_R][3];
-        gather_records(p, I, ix, act, o);
+        uint32_t lo = 0xffffffffu, hi = 0;
+#pragma unroll
+        for (int r = 0; r < S1_R; ++r)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                o[r][k] = act[r] ? __ldg(rec + ix[r][k]) : 0u;
+                if (act[r]) {
+                    lo = min(lo, ix[r][k] / CR_VCHUNK);
+                    hi = max(hi, ix[r][k] / CR_VCHUNK);
+                }
+            }
+        bool allEval = true;
+        if (cls) {
+            lo = __reduce_min_sync(FULL, lo);
+            hi = __reduce_max_sync(FULL, hi);
+            const int lane = threadIdx.x & 31;
+            if (lo <= hi && hi - lo < 32u) {
+                const bool mine = lo + (uint32_t)lane <= hi;
+                allEval = __all_sync(FULL, !mine || __ldg(cls + lo + lane) == CR_CHUNK_EVAL);
+            } else {
+                allEval = lo > hi;  // no active corner: nothing to read
+            }
+        }
+        if (!allEval) {
+#pragma unroll
+            for (int r = 0; r < S1_R; ++r)
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                    if (act[r]) {
+                        const uint32_t c = __ldg(cls + ix[r][k] / CR_VCHUNK);
+                        if (c != CR_CHUNK_EVAL) o[r][k] = c;
+                    }
+        }
 #pragma unroll
         for (int r = 0; r < S1_R; ++r) culledR[r] = cell32_culled(o[r][0], o[r][1], o[r][2]);
     } else if (p.cellMode == CR_REC_CELLS) {
