@@ -586,7 +586,7 @@ def run_ours(args, rank, world, local):
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 4 * W * H,
                 "mode": "steps back to back, each image read back while the next step renders",
                 "latency_ms_per_step": e2e_latency},
-        "roofline": {"kernel": {"vertex": "k_cull + k_vertex",
+        "roofline": {"kernel": {"vertex": "k_cull_groups + k_cull + k_stamp + k_vertex",
                                 "stage1": "k_stage1" if algo.get("boxes") else "k_s1cull + k_s1raster"}.get(
                                     rk, f"k_{rk}"), "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -730,7 +730,7 @@ def sub_plain(args, wl, ctx, handles, with_parity):
                     "vertex_slices_evaluated": int(getattr(fstats, "vertex_slices_evaluated", 0)),
                     "stage1_survivors": int(fstats.stage1_survivors), "nontrivial": int(fstats.nontrivial),
                     "huge_tiles": int(fstats.huge_tiles)},
-           "roofline": {"kernel": {"vertex": "k_cull + k_vertex",
+           "roofline": {"kernel": {"vertex": "k_cull_groups + k_cull + k_stamp + k_vertex",
                                    "stage1": "k_stage1" if algo.get("boxes") else "k_s1cull + k_s1raster"}.get(
                                        rk, f"k_{rk}"),
                         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
