@@ -1,25 +1,33 @@
-// raster.cu -- single-view kernels for sm_100a: the vertex pass, stage 1
-// and the clear, plus the launchers of every single-view stage (stages 2 and
-// 3 live in raster_core.cuh, shared with the batched kernels of views.cu).
+// raster.cu -- single-view kernels for sm_100a: the frame cull, the slice
+// stamps, the vertex pass, stage 1 and the clear, plus the launchers of every
+// single-view stage (stages 2 and 3 live in raster_core.cuh, shared with the
+// batched kernels of views.cu).
 //
 // Work decomposition (differs from the reference, same fragment set):
-//   vertex   one thread per (instance, vertex): transform + exact per-vertex
-//            cull predicates (behind / beyond each frustum side) into a byte.
-//   stage 1  persistent warps; a work item is 128 consecutive triangles of
-//            one mesh x up to 16 of its instances.  The item's 1536-byte index
-//            tile is fetched by a 1D bulk TMA copy (cp.async.bulk) into a
-//            3-deep per-warp shared-memory ring, signalled by an mbarrier, so
-//            index loads are coalesced bursts issued ahead of use.  Triangles
-//            whose three outcodes prove them culled stop there; survivors are
-//            packed across the lanes and run the reference's full path.
-//            Nontrivial triangles are appended with one atomic per warp
-//            (ballot / popc).                         reference: tv.cu:274-384
+//   cull     k_cull_groups / k_cull: exact box, sample-miss and back-face
+//            proofs over groups of 32 items or vertex chunks, then over the
+//            surviving items per instance; drawn items and the vertex chunks
+//            that need per-vertex records are listed.
+//   stamps   k_stamp: per drawn (item, instance), the 128-vertex slices its
+//            vertices lie in.
+//   vertex   k_vertex: warps over the listed chunks' stamped slices; per
+//            vertex the exact stage-1 screen cell and outcode in a record.
+//   stage 1  record-culled frames: k_s1cull (persistent warps over work items
+//            of 128 consecutive triangles x up to 16 instances; the 1536-byte
+//            index tile arrives by a 1D bulk copy (cp.async.bulk) in a 2-deep
+//            per-warp shared-memory ring signalled by an mbarrier; triangles
+//            whose three records prove them culled stop there) and
+//            k_s1raster (the reference's full path on the survivors, one per
+//            lane).  Box-culled frames: k_stage1 (per-item vertex lists and
+//            shared-memory records per instance).  Nontrivial triangles are
+//            appended with one atomic per warp.     reference: tv.cu:274-384
 //   stage 2  persistent warps; every lane sets up one queued triangle at once
-//            (the reference: lane 0 sets up while 31 lanes wait), then the
-//            warp rasterises each in turn, lanes striding over fragments.
-//            Tile appends are one atomic per warp.    reference: tv.cu:388-563
-//   stage 3  one warp per 64x64 tile (the reference: one 64-thread block),
-//            each lane ray-traces two columns.        reference: tv.cu:568-745
+//            (the reference: lane 0 sets up while 31 lanes wait), then per
+//            triangle rows are narrowed to the columns that can pass and
+//            packed across the lanes.               reference: tv.cu:388-563
+//   stage 3  a warp per 64x64 tile or band of its rows (the reference: one
+//            64-thread block per tile), rows narrowed likewise.
+//                                                   reference: tv.cu:568-745
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cstdint>
