@@ -347,8 +347,9 @@ struct CrLaunchShape {
     int stage2Blocks;
     int stage3Blocks;
     int s1CullBlocks;           // k_s1cull (record-culled frames)
-    int s1RasterBlocks;         // k_s1raster
+    int s1RasterBlocks;         // k_s1raster, warp-wide tiny rasters
     int stage2DenseBlocks;      // k_stage2_dense
+    int s1RasterOwnBlocks;      // k_s1raster, each lane its own tiny raster
 };
 
 int cr_query_launch_shape(int device, CrLaunchShape* out);

@@ -1039,6 +1039,11 @@ int cr_query_launch_shape(int device, CrLaunchShape* out) {
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2d, k_stage2_dense<S2_WARPS>, S2_WARPS * 32, 0) != cudaSuccess)
         return -1;
     out->stage2DenseBlocks = sms * (b2d > 0 ? b2d : 1);
+    int bo = 0;  // the one-lane-raster variant carries fewer registers: more blocks fit
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bo, k_s1raster<S1_WARPS, false, false>, S1_WARPS * 32, 0) !=
+        cudaSuccess)
+        return -1;
+    out->s1RasterOwnBlocks = sms * (bo > 0 ? bo : 1);
     out->stage3Blocks = sms * (b3 > 0 ? b3 : 1);
     return 0;
 }
@@ -1104,7 +1109,7 @@ int cr_launch_stage1(const CrFrameParams& p, const CrLaunchShape& s, void* strea
     if (p.anyPacked ? launch_pdl(k_s1cull<S1_WARPS, true>, bc, T, stream, p)
                     : launch_pdl(k_s1cull<S1_WARPS, false>, bc, T, stream, p))
         return -1;
-    const unsigned br = (unsigned)s.s1RasterBlocks;
+    const unsigned br = (unsigned)(p.coopRaster || s.s1RasterOwnBlocks <= 0 ? s.s1RasterBlocks : s.s1RasterOwnBlocks);
     if (p.coopRaster)
         return p.anyPacked ? launch_pdl(k_s1raster<S1_WARPS, true, true>, br, T, stream, p)
                            : launch_pdl(k_s1raster<S1_WARPS, false, true>, br, T, stream, p);
